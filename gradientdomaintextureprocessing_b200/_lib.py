@@ -1,0 +1,89 @@
+"""ctypes binding of the C ABI declared in include/gdtp.h.
+
+The shared library is built in-tree (``libgdtp.so`` next to this file) by
+``gradientdomaintextureprocessing_b200.build``.  Nothing here falls back to
+Python: a missing library or a failing call raises ``GDTPError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("GDTP_LIB", os.path.join(_HERE, "libgdtp.so"))
+
+GDTP_OK = 0
+_ERRORS = {-1: "invalid argument", -2: "setup failed", -3: "CUDA error", -4: "not converged", -5: "HBM budget exceeded",
+           -6: "call out of order", -7: "numerical failure"}
+
+
+class GDTPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gdtp error {code} ({_ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Report(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("vcycles", C.c_int), ("rel_residual_max", C.c_double), ("seconds", C.c_double)]
+
+
+_lib = None
+
+_P = C.c_void_p
+_SIGS = {
+    "gdtp_last_error": (C.c_char_p, []),
+    "gdtp_version": (C.c_int, []),
+    "gdtp_hierarchy_build": (C.c_int, [_P, C.c_int64, _P, C.c_int64, _P, C.c_int, C.c_int, C.c_int, _P, C.POINTER(_P)]),
+    "gdtp_hierarchy_free": (None, [_P]),
+    "gdtp_hierarchy_levels": (C.c_int, [_P]),
+    "gdtp_hierarchy_charts": (C.c_int, [_P]),
+    "gdtp_hierarchy_counts": (C.c_int, [_P, C.c_int, _P]),
+    "gdtp_hierarchy_array": (C.c_int, [_P, C.c_char_p, C.c_int, _P, C.POINTER(C.c_int64)]),
+    "gdtp_system_create": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, C.c_int64, C.POINTER(_P)]),
+    "gdtp_system_free": (None, [_P]),
+    "gdtp_system_array": (C.c_int, [_P, C.c_char_p, C.c_int, _P, C.POINTER(C.c_int64)]),
+    "gdtp_system_update": (C.c_int, [_P, C.c_double, C.c_double]),
+    "gdtp_apply": (C.c_int, [_P, C.c_int, _P, _P, C.c_int]),
+    "gdtp_vcycle": (C.c_int, [_P, _P, _P, C.c_int]),
+    "gdtp_solve": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.POINTER(Report)]),
+    "gdtp_solve_device": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, _P, C.POINTER(Report)]),
+    "gdtp_solve_fp64": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.POINTER(Report)]),
+    "gdtp_residual": (C.c_int, [_P, _P, _P, C.c_int, _P]),
+    "gdtp_system_set": (C.c_int, [_P, C.c_char_p, C.c_double]),
+    "gdtp_system_device_bytes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+}
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GDTPError(-3, f"{LIB_PATH} not built; run gradientdomaintextureprocessing_b200.build")
+        L = C.CDLL(LIB_PATH)
+        missing = []
+        for name, (res, args) in _SIGS.items():
+            try:
+                f = getattr(L, name)
+            except AttributeError:
+                missing.append(name)
+                continue
+            f.restype = res
+            f.argtypes = args
+        L.gdtp_missing_symbols = missing
+        _lib = L
+    return _lib
+
+
+def check(code: int) -> None:
+    if code != GDTP_OK:
+        raise GDTPError(code, lib().gdtp_last_error().decode())
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)

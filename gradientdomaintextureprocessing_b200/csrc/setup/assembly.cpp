@@ -1,0 +1,248 @@
+// Host side of the FP64 assembly: parameter metric, device work lists, and the
+// sparse boundary blocks built from element matrices computed on the device.
+//
+//   embedding metric                 Src/Metric.inl:248-276
+//   parameter metric g = J^-T G J^-1 Src/Metric.inl:415-446
+//   interior / boundary cell loops   Src/MassAndStiffness.h:31-284
+//   deep coefficient scatter         Src/MassAndStiffness.h:287-346
+//   boundary triplets and P^T B P    Src/MassAndStiffness.h:348-405, 490-549
+#include <cmath>
+
+#include "setup.h"
+
+namespace gdtp {
+
+bool embedding_metric(const Mesh& mesh, const Atlas& A, ChartMetrics& out) {
+  const int nt = mesh.nt();
+  std::vector<M2> G(nt);
+  double total = 0;
+  for (int t = 0; t < nt; t++) {
+    const double* p0 = &mesh.vertices[3 * mesh.triangles[3 * t]];
+    const double* p1 = &mesh.vertices[3 * mesh.triangles[3 * t + 1]];
+    const double* p2 = &mesh.vertices[3 * mesh.triangles[3 * t + 2]];
+    double d[2][3] = {{p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]}, {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]}};
+    M2 g;
+    for (int k = 0; k < 2; k++)
+      for (int l = 0; l < 2; l++) g.c[k][l] = d[k][0] * d[l][0] + d[k][1] * d[l][1] + d[k][2] * d[l][2];
+    total += std::sqrt(g.det()) / 2;
+    G[t] = g;
+  }
+  if (!(total > 0)) return false;
+  for (auto& g : G)
+    for (int k = 0; k < 2; k++)
+      for (int l = 0; l < 2; l++) g.c[k][l] /= total;
+  out.assign(A.charts.size(), {});
+  for (size_t c = 0; c < A.charts.size(); c++) {
+    const AtlasChart& ac = A.charts[c];
+    out[c].resize(ac.meshTriangleIndices.size());
+    for (size_t k = 0; k < ac.meshTriangleIndices.size(); k++) {
+      int t = ac.meshTriangleIndices[k];
+      V2 q0 = mesh.corner(t, 0), q1 = mesh.corner(t, 1), q2 = mesh.corner(t, 2);
+      M2 J;
+      J.c[0][0] = q1.x - q0.x; J.c[0][1] = q1.y - q0.y;
+      J.c[1][0] = q2.x - q0.x; J.c[1][1] = q2.y - q0.y;
+      M2 Ji = J.inverse();
+      out[c][k] = (Ji.transpose() * G[t]) * Ji;
+    }
+  }
+  return true;
+}
+
+static void bbox_cells(const V2* p, double cw, double ch, int mn[2], int mx[2]) {
+  double fminx = std::max(std::min(std::min(p[0].x, p[1].x), p[2].x), 0.0);
+  double fminy = std::max(std::min(std::min(p[0].y, p[1].y), p[2].y), 0.0);
+  double fmaxx = std::min(std::max(std::max(p[0].x, p[1].x), p[2].x), 1.0);
+  double fmaxy = std::min(std::max(std::max(p[0].y, p[1].y), p[2].y), 1.0);
+  double iw = 1.0 / cw, ih = 1.0 / ch;
+  mn[0] = int(std::floor(fminx * iw)); mn[1] = int(std::floor(fminy * ih));
+  mx[0] = int(std::ceil(fmaxx * iw)); mx[1] = int(std::ceil(fmaxy * ih));
+}
+
+void build_assembly_work(const Hierarchy& h, const BoundaryElements& be, const ChartMetrics& g, AssemblyWork& w) {
+  const GridLevel& L = h.levels[0];
+  const Atlas& A = h.atlas;
+  w = AssemblyWork();
+  // triangle table (chart-major) with grid-corner-relative positions and metric
+  std::vector<int> triBase(A.charts.size() + 1, 0);
+  for (size_t c = 0; c < A.charts.size(); c++) triBase[c + 1] = triBase[c] + (int)A.charts[c].triangles.size();
+  w.numTriangles = triBase.back();
+  w.triPos.resize(6 * size_t(w.numTriangles));
+  w.triMetric.resize(4 * size_t(w.numTriangles));
+  w.triMetricInv.resize(4 * size_t(w.numTriangles));
+  w.triScale.resize(w.numTriangles);
+  for (size_t c = 0; c < A.charts.size(); c++) {
+    const AtlasChart& ac = A.charts[c];
+    const GridChart& gc = L.charts[c];
+    for (size_t t = 0; t < ac.triangles.size(); t++) {
+      size_t e = triBase[c] + t;
+      for (int k = 0; k < 3; k++) {
+        V2 p = ac.vertices[ac.triangles[t][k]] - gc.corner;
+        w.triPos[6 * e + 2 * k] = p.x;
+        w.triPos[6 * e + 2 * k + 1] = p.y;
+      }
+      const M2& m = g[c][t];
+      M2 mi = m.inverse();
+      double gm[4] = {m.c[0][0], m.c[0][1], m.c[1][0], m.c[1][1]};
+      double gi[4] = {mi.c[0][0], mi.c[0][1], mi.c[1][0], mi.c[1][1]};
+      for (int q = 0; q < 4; q++) { w.triMetric[4 * e + q] = gm[q]; w.triMetricInv[4 * e + q] = gi[q]; }
+      w.triScale[e] = std::sqrt(m.det());
+    }
+  }
+  // interior cells: global order = chart order, then interior cell order
+  std::vector<int> icBase(L.charts.size() + 1, 0), btBase(L.charts.size() + 1, 0);
+  for (size_t c = 0; c < L.charts.size(); c++) icBase[c + 1] = icBase[c] + L.charts[c].numInteriorCells;
+  w.numInteriorCells = icBase.back();
+  w.cellIJ.resize(2 * size_t(w.numInteriorCells));
+  w.cellChart.resize(w.numInteriorCells);
+  for (size_t c = 0; c < L.charts.size(); c++) {
+    const GridChart& gc = L.charts[c];
+    for (int j = 0; j < gc.height - 1; j++)
+      for (int i = 0; i < gc.width - 1; i++) {
+        int ic = gc.localInteriorCell[gc.cat(i, j)];
+        if (ic < 0) continue;
+        w.cellIJ[2 * (icBase[c] + ic)] = i;
+        w.cellIJ[2 * (icBase[c] + ic) + 1] = j;
+        w.cellChart[icBase[c] + ic] = (int)c;
+      }
+  }
+  w.chartCellSize.resize(2 * L.charts.size());
+  for (size_t c = 0; c < L.charts.size(); c++) {
+    w.chartCellSize[2 * c] = L.charts[c].cellSizeW;
+    w.chartCellSize[2 * c + 1] = L.charts[c].cellSizeH;
+  }
+  // boundary triangles: global order = chart order, boundary cell order, triangle order
+  for (size_t c = 0; c < L.charts.size(); c++) {
+    int n = 0;
+    for (auto& v : be.charts[c].cellTriangles) n += (int)v.size();
+    btBase[c + 1] = btBase[c] + n;
+  }
+  w.numBoundaryTriangles = btBase.back();
+  w.btPos.resize(6 * size_t(w.numBoundaryTriangles));
+  w.btIdx.resize(6 * size_t(w.numBoundaryTriangles));
+  std::vector<std::vector<int>> cellFirstBt(L.charts.size());
+  for (size_t c = 0; c < L.charts.size(); c++) {
+    int b = btBase[c];
+    cellFirstBt[c].resize(be.charts[c].cellTriangles.size() + 1);
+    for (size_t cell = 0; cell < be.charts[c].cellTriangles.size(); cell++) {
+      cellFirstBt[c][cell] = b;
+      for (const BoundaryTriangle& bt : be.charts[c].cellTriangles[cell]) {
+        for (int k = 0; k < 3; k++) { w.btPos[6 * size_t(b) + 2 * k] = bt.v[k].x; w.btPos[6 * size_t(b) + 2 * k + 1] = bt.v[k].y; }
+        for (int k = 0; k < 6; k++) w.btIdx[6 * size_t(b) + k] = be.fineBoundaryIndex[bt.idx[k]];
+        b++;
+      }
+    }
+    cellFirstBt[c][be.charts[c].cellTriangles.size()] = b;
+  }
+  // (cell or boundary triangle, chart triangle) pairs in chart-triangle order, bucketed
+  std::vector<std::pair<int, int>> icPairs, btPairs;
+  for (size_t c = 0; c < L.charts.size(); c++) {
+    const AtlasChart& ac = A.charts[c];
+    const GridChart& gc = L.charts[c];
+    for (size_t t = 0; t < ac.triangles.size(); t++) {
+      V2 p[3];
+      for (int k = 0; k < 3; k++) p[k] = ac.vertices[ac.triangles[t][k]] - gc.corner;
+      int mn[2], mx[2];
+      bbox_cells(p, gc.cellSizeW, gc.cellSizeH, mn, mx);
+      for (int j = mn[1]; j < mx[1]; j++)
+        for (int i = mn[0]; i < mx[0]; i++) {
+          int ic = gc.localInteriorCell[gc.cat(i, j)];
+          if (ic >= 0) { icPairs.push_back({icBase[c] + ic, triBase[c] + (int)t}); continue; }
+          int bc = gc.localBoundaryCell[gc.cat(i, j)];
+          if (bc >= 0)
+            for (int b = cellFirstBt[c][bc]; b < cellFirstBt[c][bc + 1]; b++) btPairs.push_back({b, triBase[c] + (int)t});
+        }
+    }
+  }
+  auto bucket = [](int n, const std::vector<std::pair<int, int>>& pairs, std::vector<int>& ptr, std::vector<int>& idx) {
+    ptr.assign(n + 1, 0);
+    for (auto& p : pairs) ptr[p.first + 1]++;
+    for (int i = 0; i < n; i++) ptr[i + 1] += ptr[i];
+    idx.resize(pairs.size());
+    std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+    for (auto& p : pairs) idx[fill[p.first]++] = p.second;  // stable: chart-triangle order kept
+  };
+  bucket(w.numInteriorCells, icPairs, w.cellPtr, w.cellTri);
+  bucket(w.numBoundaryTriangles, btPairs, w.btPtr, w.btTri);
+
+  // deep texels: the four surrounding interior cells (raster order) and the
+  // texel's corner slot in each
+  w.deepCells.resize(4 * size_t(L.numDeep));
+  for (size_t c = 0; c < L.charts.size(); c++) {
+    const GridChart& gc = L.charts[c];
+    for (int j = 0; j < gc.height; j++)
+      for (int i = 0; i < gc.width; i++) {
+        int d = gc.deepTexel[gc.at(i, j)];
+        if (d < 0) continue;
+        const int ci[4] = {i - 1, i, i - 1, i}, cj[4] = {j - 1, j - 1, j, j};
+        for (int q = 0; q < 4; q++) w.deepCells[4 * size_t(d) + q] = icBase[c] + gc.localInteriorCell[gc.cat(ci[q], cj[q])];
+      }
+  }
+  // interior cells touching a boundary texel (their boundary rows are built on the host)
+  for (int ic = 0; ic < w.numInteriorCells; ic++) {
+    const GridChart& gc = L.charts[w.cellChart[ic]];
+    int i = w.cellIJ[2 * ic], j = w.cellIJ[2 * ic + 1];
+    int q[4] = {gc.at(i, j), gc.at(i + 1, j), gc.at(i + 1, j + 1), gc.at(i, j + 1)};
+    for (int k = 0; k < 4; k++)
+      if (gc.nodeType[q[k]] != 2) { w.boundaryAdjacentCells.push_back(ic); break; }
+  }
+}
+
+// Deep coefficient of texel slot k (corner of a cell) toward neighbour slot l.
+static inline int neighbour_offset(int k, int l) {
+  static const int oi[4] = {0, 1, 1, 0}, oj[4] = {0, 0, 1, 1};
+  return (oj[l] - oj[k] + 1) * 3 + (oi[l] - oi[k] + 1);
+}
+
+bool assemble_boundary_blocks(const Hierarchy& h, const BoundaryElements& be, const AssemblyWork& w,
+                              const std::vector<double>& adjCellMass, const std::vector<double>& adjCellStiffness,
+                              const std::vector<double>& btMass, const std::vector<double>& btStiffness, FineSystem& fs,
+                              std::string& err) {
+  const GridLevel& L = h.levels[0];
+  std::vector<Triplet> bbM, bbS, bdM, bdS;
+  for (size_t a = 0; a < w.boundaryAdjacentCells.size(); a++) {
+    int ic = w.boundaryAdjacentCells[a];
+    const GridChart& gc = L.charts[w.cellChart[ic]];
+    int i = w.cellIJ[2 * ic], j = w.cellIJ[2 * ic + 1];
+    int pos[4] = {gc.at(i, j), gc.at(i + 1, j), gc.at(i + 1, j + 1), gc.at(i, j + 1)};
+    const double* M = &adjCellMass[16 * a];
+    const double* S = &adjCellStiffness[16 * a];
+    for (int k = 0; k < 4; k++) {
+      int node = gc.texel[pos[k]];
+      int bd = L.boundaryAndDeep[node];
+      if (bd < 0) continue;  // deep rows come from the device gather
+      int b = bd - 1;
+      for (int l = 0; l < 4; l++) {
+        int nb = gc.texel[pos[l]];
+        if (L.boundaryAndDeep[nb] < 0) {
+          bdM.push_back({b, nb, M[4 * k + l]});
+          bdS.push_back({b, nb, S[4 * k + l]});
+        } else {
+          int fk = be.fineBoundaryIndex[gc.interiorTexel[pos[k]]], fl = be.fineBoundaryIndex[gc.interiorTexel[pos[l]]];
+          if (fk < 0 || fl < 0) { err = "interior cell corner without fine boundary index"; return false; }
+          bbM.push_back({fk, fl, M[4 * k + l]});
+          bbS.push_back({fk, fl, S[4 * k + l]});
+        }
+      }
+    }
+  }
+  for (int b = 0; b < w.numBoundaryTriangles; b++) {
+    const int* f = &w.btIdx[6 * size_t(b)];
+    const double* M = &btMass[36 * size_t(b)];
+    const double* S = &btStiffness[36 * size_t(b)];
+    for (int k = 0; k < 6; k++)
+      for (int l = 0; l < 6; l++) {
+        bbM.push_back({f[k], f[l], M[6 * l + k]});
+        bbS.push_back({f[k], f[l], S[6 * l + k]});
+      }
+  }
+  Csr fineBBM = csr_from_triplets(be.numFineBoundary, be.numFineBoundary, bbM);
+  Csr fineBBS = csr_from_triplets(be.numFineBoundary, be.numFineBoundary, bbS);
+  Csr R = csr_transpose(be.prolongation);
+  fs.bbMass = csr_multiply(R, csr_multiply(fineBBM, be.prolongation));
+  fs.bbStiffness = csr_multiply(R, csr_multiply(fineBBS, be.prolongation));
+  fs.bdMass = csr_from_triplets(L.numBoundary, L.numTexels, bdM);
+  fs.bdStiffness = csr_from_triplets(L.numBoundary, L.numTexels, bdS);
+  return true;
+}
+
+}  // namespace gdtp

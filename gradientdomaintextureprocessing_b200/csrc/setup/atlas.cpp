@@ -1,0 +1,213 @@
+// Atlas construction from per-corner texture coordinates.
+//
+// Follows the reference's chart decomposition and atlas indexing so that every
+// downstream index (charts, chart vertices, atlas edges, boundary half-edges)
+// is identical:
+//   chart components           Src/ChartDecomposition.h:30-73
+//   atlas vertices / edges     Src/AtlasMesh.inl:3-101
+//   boundary half-edges        Src/AtlasMesh.inl:103-163
+//   boundary vertices          Src/AtlasMesh.inl:165-184
+//   chart tables, grid origin  Src/AtlasCharts.inl:3-76
+#include <cmath>
+#include <cstring>
+#include <queue>
+#include <unordered_map>
+
+#include "setup.h"
+
+namespace gdtp {
+
+static inline uint64_t edge_key(uint32_t a, uint32_t b) { return (uint64_t(a) << 32) | uint64_t(b); }
+
+static bool same_uv(const V2& a, const V2& b) { return a.x == b.x && a.y == b.y; }
+
+bool build_atlas(const Mesh& mesh, int width, int height, Atlas& A, std::string& err) {
+  const int nt = mesh.nt();
+  A.width = width;
+  A.height = height;
+  const int* T = mesh.triangles.data();
+
+  // directed half-edge table of the input mesh
+  std::unordered_map<uint64_t, int> half;
+  half.reserve(size_t(nt) * 4);
+  for (int t = 0; t < nt; t++)
+    for (int k = 0; k < 3; k++) {
+      uint64_t key = edge_key(T[3 * t + k], T[3 * t + (k + 1) % 3]);
+      if (!half.emplace(key, 3 * t + k).second) { err = "non-manifold mesh (repeated directed edge)"; return false; }
+    }
+  auto opposite = [&](int t, int k) -> int {
+    auto it = half.find(edge_key(T[3 * t + (k + 1) % 3], T[3 * t + k]));
+    return it == half.end() ? -1 : it->second;
+  };
+  // an edge is interior to a chart when its twin carries the same texture coordinates
+  auto uv_continuous = [&](int t, int k, int o) {
+    int s = o / 3, m = o % 3;
+    return same_uv(mesh.corner(t, (k + 1) % 3), mesh.corner(s, m)) && same_uv(mesh.corner(t, k), mesh.corner(s, (m + 1) % 3));
+  };
+
+  // ---- charts: edge-connected components with continuous texture coordinates
+  A.triangleChart.assign(nt, -1);
+  int comp = -1;
+  std::vector<int> nb;
+  for (int seed = 0; seed < nt; seed++) {
+    if (A.triangleChart[seed] != -1) continue;
+    comp++;
+    std::queue<int> q;
+    A.triangleChart[seed] = comp;
+    q.push(seed);
+    while (!q.empty()) {
+      int t = q.front();
+      q.pop();
+      for (int k = 0; k < 3; k++) {
+        int o = opposite(t, k);
+        if (o < 0 || !uv_continuous(t, k, o)) continue;
+        int s = o / 3;
+        if (A.triangleChart[s] == -1) { A.triangleChart[s] = comp; q.push(s); }
+        else if (A.triangleChart[s] != comp) { err = "inconsistent chart components"; return false; }
+      }
+    }
+  }
+  A.numCharts = comp + 1;
+
+  // ---- atlas vertices: one per distinct (texture coordinate, mesh vertex) pair, first-seen order
+  struct Key { uint64_t u, v; int m; bool operator==(const Key& o) const { return u == o.u && v == o.v && m == o.m; } };
+  struct KeyHash { size_t operator()(const Key& k) const { return std::hash<uint64_t>()(k.u * 0x9E3779B97F4A7C15ull ^ (k.v + 0x7F4A7C15ull * (uint64_t)k.m)); } };
+  std::unordered_map<Key, int, KeyHash> vmap;
+  vmap.reserve(size_t(nt) * 2);
+  A.triangles.resize(nt);
+  for (int t = 0; t < nt; t++)
+    for (int k = 0; k < 3; k++) {
+      V2 p = mesh.corner(t, k);
+      Key key;
+      std::memcpy(&key.u, &p.x, 8);
+      std::memcpy(&key.v, &p.y, 8);
+      key.m = T[3 * t + k];
+      auto it = vmap.find(key);
+      int id;
+      if (it == vmap.end()) {
+        id = (int)A.vertices.size();
+        vmap.emplace(key, id);
+        A.vertices.push_back(p);
+        A.vertexMap.push_back(T[3 * t + k]);
+      } else {
+        id = it->second;
+      }
+      A.triangles[t][k] = id;
+    }
+
+  // ---- vertices within 1e-6 texel of a texel-centre line are moved off it
+  // (the reference does this with rand(); a deterministic offset keeps the atlas
+  // reproducible -- inputs from the bundled generators never need it)
+  const double precision = 1e-6;
+  for (size_t i = 0; i < A.vertices.size(); i++)
+    for (int c = 0; c < 2; c++) {
+      double dim = c == 0 ? double(width) : double(height);
+      double scaled = A.vertices[i][c] * dim - 0.5;
+      double off = scaled - double(std::round(scaled));
+      if (std::fabs(off) < precision) {
+        double h = 1.0 + double((i * 2654435761u + c) % 1000) / 1000.0;
+        scaled = off > 0 ? std::round(scaled) + precision * h : std::round(scaled) - precision * h;
+        A.vertices[i][c] = (scaled + 0.5) / dim;
+        A.gridJitterCount++;
+      }
+    }
+
+  // ---- atlas edge indices
+  std::unordered_map<uint64_t, int> ahalf;
+  ahalf.reserve(size_t(nt) * 4);
+  for (int t = 0; t < nt; t++)
+    for (int k = 0; k < 3; k++) {
+      uint64_t key = edge_key(A.triangles[t][k], A.triangles[t][(k + 1) % 3]);
+      if (!ahalf.emplace(key, 3 * t + k).second) { err = "non-oriented-manifold atlas"; return false; }
+    }
+  const int res = std::max(width, height);
+  int nextEdge = 2 * res * res * A.numCharts;
+  A.halfEdgeToEdgeIndex.assign(3 * nt, -1);
+  for (int t = 0; t < nt; t++)
+    for (int k = 0; k < 3; k++) {
+      int cur = 3 * t + k;
+      auto it = ahalf.find(edge_key(A.triangles[t][(k + 1) % 3], A.triangles[t][k]));
+      if (it != ahalf.end()) {
+        if (cur < it->second) A.halfEdgeToEdgeIndex[cur] = A.halfEdgeToEdgeIndex[it->second] = nextEdge++;
+      } else {
+        A.halfEdgeToEdgeIndex[cur] = nextEdge++;
+      }
+    }
+
+  // ---- boundary half-edges of the input mesh (open edges and texture seams)
+  A.oppositeHalfEdge.assign(3 * nt, -1);
+  A.isBoundaryHalfEdge.assign(3 * nt, 0);
+  A.isClosed = true;
+  std::vector<int> boundaryHalfEdges;
+  for (int t = 0; t < nt; t++)
+    for (int k = 0; k < 3; k++) {
+      int cur = 3 * t + k;
+      int o = opposite(t, k);
+      if (o >= 0) {
+        if (cur < o) { A.oppositeHalfEdge[cur] = o; A.oppositeHalfEdge[o] = cur; }
+        if (!uv_continuous(t, k, o) && cur < o) {
+          boundaryHalfEdges.push_back(cur);
+          boundaryHalfEdges.push_back(o);
+          A.isBoundaryHalfEdge[cur] = A.isBoundaryHalfEdge[o] = 1;
+        }
+      } else {
+        A.isClosed = false;
+        boundaryHalfEdges.push_back(cur);
+        A.isBoundaryHalfEdge[cur] = 1;
+      }
+    }
+  A.boundaryVertexIndex.assign(mesh.nv(), -1);
+  A.numBoundaryVertices = 0;
+  for (int he : boundaryHalfEdges) {
+    int t = he / 3, k = he % 3;
+    for (int e = 0; e < 2; e++) {
+      int v = T[3 * t + (k + e) % 3];
+      if (A.boundaryVertexIndex[v] == -1) A.boundaryVertexIndex[v] = A.numBoundaryVertices++;
+    }
+  }
+
+  // ---- chart tables
+  A.charts.assign(A.numCharts, AtlasChart());
+  for (auto& c : A.charts) { c.minCorner = V2(1, 1); c.maxCorner = V2(0, 0); }
+  std::vector<int> chartVertex(A.vertices.size(), -1), chartVertexCount(A.numCharts, 0);
+  for (int t = 0; t < nt; t++) {
+    AtlasChart& C = A.charts[A.triangleChart[t]];
+    C.meshTriangleIndices.push_back(t);
+    I3 tri;
+    for (int k = 0; k < 3; k++) {
+      C.atlasEdgeIndices.push_back(A.halfEdgeToEdgeIndex[3 * t + k]);
+      int av = A.triangles[t][k];
+      if (chartVertex[av] == -1) {
+        chartVertex[av] = chartVertexCount[A.triangleChart[t]]++;
+        V2 p = A.vertices[av];
+        for (int c = 0; c < 2; c++) {
+          C.minCorner[c] = std::min(p[c], C.minCorner[c]);
+          C.maxCorner[c] = std::max(p[c], C.maxCorner[c]);
+        }
+        C.vertices.push_back(p);
+        C.meshVertexIndices.push_back(A.vertexMap[av]);
+      }
+      tri[k] = chartVertex[av];
+    }
+    C.triangles.push_back(tri);
+  }
+  for (auto& C : A.charts) {
+    V2 mid = (C.minCorner + C.maxCorner) / 2.0;
+    mid.x *= double(width);
+    mid.y *= double(height);
+    mid = mid - V2(0.5, 0.5);
+    mid = V2(std::floor(mid.x), std::floor(mid.y));
+    C.originCoords[0] = int(std::round(mid.x));
+    C.originCoords[1] = int(std::round(mid.y));
+    mid = mid + V2(0.5, 0.5);
+    mid.x /= double(width);
+    mid.y /= double(height);
+    C.gridOrigin = mid;
+    for (size_t t = 0; t < C.meshTriangleIndices.size(); t++)
+      for (int k = 0; k < 3; k++)
+        if (A.isBoundaryHalfEdge[3 * C.meshTriangleIndices[t] + k]) C.boundaryHalfEdges.push_back(3 * int(t) + k);
+  }
+  return true;
+}
+
+}  // namespace gdtp

@@ -1,0 +1,135 @@
+/*
+ * gdtp.h -- C ABI of the B200 texel-FEM solve path (gradient-domain texture
+ * processing: atlas-clipped texel grid, multigrid V-cycle, coarse direct solve).
+ *
+ * Plain pointers and sizes only.  Every function returns a gdtp status (0 = ok,
+ * negative = error); gdtp_last_error() returns the message of the calling
+ * thread's last failure.  Arrays are row-major; "host" pointers are ordinary
+ * CPU memory, "device" pointers are CUDA device memory of the handle's device.
+ *
+ * Texel vectors use the reference's layout: one entry per active texel in the
+ * reference's global texel order (chart by chart, raster order), k channels
+ * interleaved (x[texel * k + channel]).
+ *
+ * Each entry point names the reference interface it replaces (path:line in
+ * fabianprada/GradientDomainTextureProcessing).
+ */
+#ifndef GDTP_H
+#define GDTP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GDTP_OK 0
+#define GDTP_ERR_INVALID (-1)       /* bad argument */
+#define GDTP_ERR_SETUP (-2)         /* mesh / atlas / hierarchy construction failed */
+#define GDTP_ERR_CUDA (-3)          /* CUDA runtime error or no usable device */
+#define GDTP_ERR_NOT_CONVERGED (-4) /* solve stopped at max_iters above tolerance */
+#define GDTP_ERR_BUDGET (-5)        /* HBM admission budget exceeded */
+#define GDTP_ERR_STATE (-6)         /* call out of order (e.g. solve before update) */
+#define GDTP_ERR_NUMERIC (-7)       /* coarse factorisation not positive definite */
+
+typedef struct gdtp_hierarchy gdtp_hierarchy;
+typedef struct gdtp_system gdtp_system;
+
+const char* gdtp_last_error(void);
+int gdtp_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Hierarchy (host).  Replaces InitializeHierarchy
+ * (include/Src/HierarchyConstruction.inl:799-849) and, for the finest level,
+ * InitializeBoundaryTriangulation (include/Src/BoundaryQuadraticElements.inl:619)
+ * and InitializeBoundaryProlongationData (BoundaryQuadraticElements.inl:775).
+ * vertices: nv*3, triangles: nt*3, uv: nt*3*2 per-corner coordinates.
+ * block_info: {blockWidth, blockHeight, paddingWidth, paddingHeight,
+ * boundaryDilation} as MultigridBlockInfo (include/Src/Hierarchy.h:61-76), or NULL.
+ * ------------------------------------------------------------------------- */
+int gdtp_hierarchy_build(const double* vertices, int64_t nv, const int32_t* triangles, int64_t nt, const double* uv,
+                         int width, int height, int levels, const int32_t* block_info, gdtp_hierarchy** out);
+void gdtp_hierarchy_free(gdtp_hierarchy* h);
+int gdtp_hierarchy_levels(const gdtp_hierarchy* h);
+int gdtp_hierarchy_charts(const gdtp_hierarchy* h);
+/* counts[8] = {texels, deep, boundary, cells, boundaryCells, interiorCells, interiorTexels, charts}
+ * (GridAtlas counters, include/Src/Hierarchy.h:241-252) */
+int gdtp_hierarchy_counts(const gdtp_hierarchy* h, int level, int64_t* counts);
+/* Named host arrays of one level (int32 unless noted).  With out == NULL only
+ * *count (elements) is written.  Names and row widths:
+ *   "nodeinfo"(4: chart,ci,cj,type)  GridAtlas::nodeInfo           Hierarchy.h:236
+ *   "boundaryAndDeep" "boundaryGlobal" "deepGlobal"                Hierarchy.h:233-235
+ *   "rasterLines"(5) "restrictionLines"(5) "deepLines"(5)          Hierarchy.h:239-241
+ *   "prolongationLines"(6)                                         Hierarchy.h:242
+ *   "charts"(12) chart grid ints, "chartsd"(4, float64) corner+cell size   Hierarchy.h:146-161
+ *   "nodeType" "cellType" concatenated per-chart images
+ *   "textureNodes"(5: ci,cj,chart,tId,isInterior) level 0 only     Basis.h:4-28
+ *   "textureBary"(2, float64) level 0 only
+ *   "boundaryRestriction.ptr/.col/.val(float64)"  HierarchicalSystem::boundaryRestriction
+ *   "boundaryNodes"(4: boundaryNodes, midPoints, fineNodes, fineBoundaryNodes) level 0
+ *   "boundaryProlongation.ptr/.col/.val(float64)" level 0 (coarseBoundaryFineBoundaryProlongation) */
+int gdtp_hierarchy_array(const gdtp_hierarchy* h, const char* name, int level, void* out, int64_t* count);
+
+/* ---------------------------------------------------------------------------
+ * System (device).  gdtp_system_create binds a hierarchy to a CUDA device and
+ * assembles the FP64 mass and stiffness matrices: replaces InitializeMetric
+ * (include/Src/Metric.inl:448; metric_mode 0 = embedding) and
+ * InitializeMassAndStiffness (include/Src/MassAndStiffness.h:490-549).
+ * parameter_metric: optional per mesh triangle 2x2 metric (nt*4, column-major
+ * g(0,0),g(0,1),g(1,0),g(1,1) in texture coordinates, as InitializeParameterMetric
+ * produces, Metric.inl:415-446); NULL selects metric_mode.
+ * ------------------------------------------------------------------------- */
+int gdtp_system_create(gdtp_hierarchy* h, int device, int metric_mode, const double* parameter_metric,
+                       const double* vertices, int64_t nv, gdtp_system** out);
+void gdtp_system_free(gdtp_system* s);
+/* Named host copies of the assembled FP64 system (level 0 unless noted):
+ *   "deepMass" "deepStiffness" (10 per deep texel)
+ *   "bbMass.ptr/.col/.val" "bbStiffness.*" "bdMass.*" "bdStiffness.*"
+ *   after gdtp_system_update: "coef.deep"(level l, raw, 10 per deep texel), "coef.bb.*", "coef.bd.*" */
+int gdtp_system_array(const gdtp_system* s, const char* name, int level, void* out, int64_t* count);
+
+/* Combine and coarsen: A = screen*M + stiffness*S, Galerkin hierarchy, coarse
+ * Cholesky.  Replaces UpdateLinearSystem (include/Src/UpdateCoefficients.inl:463-513),
+ * UpdateMultigridCoefficients (:285-399) and UpdateMultigridSolvers (:402-439). */
+int gdtp_system_update(gdtp_system* s, double stiffness_weight, double screen_weight);
+
+/* y = A x with the raw FP64 operator (which: 0 = A, 1 = M, 2 = S).  Replaces
+ * MultiplyBySystemMatrix_NoReciprocals (include/Src/IterativeSolvers.inl:881-950).
+ * Host float64 buffers of numTexels*k. */
+int gdtp_apply(gdtp_system* s, int which, const double* x, double* y, int k);
+
+/* One FP32 V-cycle on level-0 vectors (host float32, numTexels*k), x updated in
+ * place.  Replaces VCycle (include/Src/IterativeSolvers.inl:1211-1333). */
+int gdtp_vcycle(gdtp_system* s, float* x, const float* rhs, int k);
+
+typedef struct gdtp_report {
+  int iterations;          /* outer FP64 refinement steps (or V-cycles for the plain FP64 path) */
+  int vcycles;             /* total V-cycles */
+  double rel_residual_max; /* max over RHS of ||b - A x||_2 / ||b||_2 with the FP64 operator */
+  double seconds;          /* device time of the solve */
+} gdtp_report;
+
+/* Mixed-precision solve A x = b: FP32 V-cycles (all k right-hand sides at once)
+ * inside FP64 iterative refinement, until every RHS reaches tol.  x holds the
+ * initial guess on entry.  Host float64 numTexels*k.  Replaces the app loop of
+ * VCycle calls (TextureFiltering.cpp:562-579) and, for accuracy, the
+ * --useDirectSolver path (TextureFiltering.cpp:651-655, 704-707). */
+int gdtp_solve(gdtp_system* s, const double* b, double* x, int k, double tol, int max_iters, gdtp_report* report);
+/* Same on device float64 buffers (no host copies); stream = cudaStream_t or NULL. */
+int gdtp_solve_device(gdtp_system* s, const double* b_dev, double* x_dev, int k, double tol, int max_iters,
+                      void* stream, gdtp_report* report);
+/* Plain FP64 V-cycles (no mixed precision) until tol: the comparator path. */
+int gdtp_solve_fp64(gdtp_system* s, const double* b, double* x, int k, double tol, int max_iters, gdtp_report* report);
+
+/* Relative residuals ||b - A x|| / ||b|| per RHS (FP64 operator), host buffers. */
+int gdtp_residual(gdtp_system* s, const double* b, const double* x, int k, double* rel);
+
+/* Solver knobs: "pre_sweeps" "post_sweeps" "vcycles_per_refinement" "levels_used"; value as double. */
+int gdtp_system_set(gdtp_system* s, const char* knob, double value);
+/* Device bytes held by the system (coefficients, vectors, coarse factor). */
+int gdtp_system_device_bytes(const gdtp_system* s, int64_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GDTP_H */

@@ -1,0 +1,369 @@
+// Oracle harness: drives the UNMODIFIED reference solve path (compiled from the
+// reference's own headers, never copied) and dumps every structure the B200
+// implementation must reproduce.  Test infrastructure only: nothing in the
+// product links or runs this program.
+//
+// Call sequence mirrors the TextureFiltering app (TextureFiltering/TextureFiltering.cpp:581-718):
+//   InitializeHierarchy            include/Src/HierarchyConstruction.inl:799
+//   InitializeBoundaryProlongationData include/Src/BoundaryQuadraticElements.inl:775
+//   InitializeMetric (embedding)   include/Src/Metric.inl:448
+//   InitializeMassAndStiffness     include/Src/MassAndStiffness.h:490
+//   FullMatrixConstruction         include/Src/UpdateCoefficients.inl:137
+//   UpdateLinearSystem             include/Src/UpdateCoefficients.inl:463
+//   MultiplyBySystemMatrix_NoReciprocals include/Src/IterativeSolvers.inl:881
+//   VCycle                         include/Src/IterativeSolvers.inl:1211
+//   solve(EigenCholeskySolver3)    include/Src/Solver.h:191   (the --useDirectSolver FP64 ground truth)
+//
+// Usage: gdtp_ref <mesh.gdm> <out.gdd> [levels] [stiffness] [sharpness] [vcycles] [mode]
+//   mode "dump": everything (small meshes); "solve": counts + rhs + exact solution + V-cycle timing.
+//   The RHS is  M f + stiffness*sharpness * S f  and the operator  M + stiffness*S.
+#ifndef USE_FLOAT
+#define USE_FLOAT 0
+#endif
+#define PNG_INCLUDED 1
+void PNGWriteColor(const char*, const unsigned char*, int, int) {}
+unsigned char* PNGReadColor(const char*, int&, int&) { return nullptr; }
+
+#include <Src/VectorPrecisionType.inl>
+#include <Misha/CmdLineParser.h>
+#include <Src/SimpleMesh.h>
+#include <Src/Basis.h>
+#include <Misha/FEM.h>
+#include <Src/Solver.h>
+#include <Src/Hierarchy.h>
+#include <Src/MassAndStiffness.h>
+
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <omp.h>
+
+// ---------------------------------------------------------------------------
+// named-array container ("GDTPDMP1"): name, dtype code, ndim, dims, raw bytes
+// dtype codes: 1=int32 2=float64 3=float32 4=int64
+// ---------------------------------------------------------------------------
+struct Dump {
+  FILE* f = nullptr;
+  explicit Dump(const char* path) {
+    f = fopen(path, "wb");
+    if (!f) { fprintf(stderr, "cannot open %s\n", path); exit(2); }
+    fwrite("GDTPDMP1", 1, 8, f);
+  }
+  ~Dump() { if (f) fclose(f); }
+  void put(const std::string& name, int code, const std::vector<int64_t>& dims, const void* data, size_t bytes) {
+    uint32_t n = (uint32_t)name.size();
+    fwrite(&n, 4, 1, f);
+    fwrite(name.data(), 1, n, f);
+    uint8_t c = (uint8_t)code;
+    fwrite(&c, 1, 1, f);
+    uint32_t nd = (uint32_t)dims.size();
+    fwrite(&nd, 4, 1, f);
+    fwrite(dims.data(), 8, nd, f);
+    if (bytes) fwrite(data, 1, bytes, f);
+  }
+  void i32(const std::string& name, const std::vector<int>& v, int64_t cols = 1) {
+    put(name, 1, cols == 1 ? std::vector<int64_t>{(int64_t)v.size()} : std::vector<int64_t>{(int64_t)v.size() / cols, cols}, v.data(), v.size() * 4);
+  }
+  void f64(const std::string& name, const std::vector<double>& v, int64_t cols = 1) {
+    put(name, 2, cols == 1 ? std::vector<int64_t>{(int64_t)v.size()} : std::vector<int64_t>{(int64_t)v.size() / cols, cols}, v.data(), v.size() * 8);
+  }
+  template <class T>
+  void csr(const std::string& name, const SparseMatrix<T, int>& M) {
+    std::vector<int> ptr(M.rows + 1, 0), col;
+    std::vector<double> val;
+    for (size_t i = 0; i < M.rows; i++) {
+      ptr[i + 1] = ptr[i] + (int)M.RowSize(i);
+      for (size_t j = 0; j < M.RowSize(i); j++) { col.push_back(M[i][j].N); val.push_back((double)M[i][j].Value); }
+    }
+    i32(name + "/ptr", ptr);
+    i32(name + "/col", col);
+    f64(name + "/val", val);
+  }
+};
+
+static bool ReadGDM(const char* path, TexturedMesh& mesh) {
+  FILE* f = fopen(path, "rb");
+  if (!f) return false;
+  char magic[8];
+  if (fread(magic, 1, 8, f) != 8 || memcmp(magic, "GDTPMSH1", 8)) { fclose(f); return false; }
+  int64_t hdr[5];
+  if (fread(hdr, 8, 5, f) != 5) { fclose(f); return false; }
+  int64_t nv = hdr[0], nt = hdr[1], w = hdr[2], h = hdr[3], c = hdr[4];
+  std::vector<double> v(nv * 3), uv(nt * 6);
+  std::vector<int> t(nt * 3);
+  std::vector<float> tex(w * h * c);
+  size_t ok = fread(v.data(), 8, v.size(), f) + fread(t.data(), 4, t.size(), f) + fread(uv.data(), 8, uv.size(), f) +
+              fread(tex.data(), 4, tex.size(), f);
+  fclose(f);
+  if (ok != v.size() + t.size() + uv.size() + tex.size()) return false;
+  mesh.vertices.resize(nv);
+  for (int64_t i = 0; i < nv; i++) mesh.vertices[i] = Point3D<double>(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+  mesh.triangles.resize(nt);
+  for (int64_t i = 0; i < nt; i++) mesh.triangles[i] = TriangleIndex(t[3 * i], t[3 * i + 1], t[3 * i + 2]);
+  mesh.textureCoordinates.resize(nt * 3);
+  for (int64_t i = 0; i < nt * 3; i++) mesh.textureCoordinates[i] = Point2D<double>(uv[2 * i], uv[2 * i + 1]);
+  mesh.texture.resize((int)w, (int)h);
+  for (int64_t j = 0; j < h; j++)
+    for (int64_t i = 0; i < w; i++) {
+      const float* p = &tex[(j * w + i) * c];
+      mesh.texture(i, j) = Point3D<float>(p[0], c > 1 ? p[1] : p[0], c > 2 ? p[2] : p[0]);
+    }
+  return true;
+}
+
+typedef VECTOR_TYPE Vec;
+typedef REAL_TYPE Real;
+
+static double ResidualNorm(const std::vector<MultigridLevelCoefficients<Real>>&, const std::vector<double>& deepA,
+                           const SparseMatrix<double, int>& BD, const SparseMatrix<double, int>& BB,
+                           const GridAtlas& atlas, const std::vector<Vec>& x, const std::vector<Vec>& b,
+                           double bnorm2[3], double rnorm2[3]) {
+  std::vector<Vec> Ax(x.size());
+  MultiplyBySystemMatrix_NoReciprocals(deepA, BD, BB, atlas.boundaryGlobalIndex, atlas.rasterLines, x, Ax);
+  double worst = 0;
+  for (int c = 0; c < 3; c++) { bnorm2[c] = 0; rnorm2[c] = 0; }
+  for (size_t i = 0; i < x.size(); i++)
+    for (int c = 0; c < 3; c++) {
+      double r = (double)b[i][c] - (double)Ax[i][c];
+      rnorm2[c] += r * r;
+      bnorm2[c] += (double)b[i][c] * (double)b[i][c];
+    }
+  for (int c = 0; c < 3; c++) worst = std::max(worst, sqrt(rnorm2[c] / std::max(bnorm2[c], 1e-300)));
+  return worst;
+}
+
+int main(int argc, char** argv) {
+  if (argc < 3) {
+    fprintf(stderr, "usage: %s mesh.gdm out.gdd [levels] [stiffness] [sharpness] [vcycles] [dump|solve]\n", argv[0]);
+    return 2;
+  }
+  const int levels = argc > 3 ? atoi(argv[3]) : 4;
+  const double stiffnessWeight = argc > 4 ? atof(argv[4]) : 1e-3;
+  const double sharpnessWeight = argc > 5 ? atof(argv[5]) : 2.0;
+  const int vcycles = argc > 6 ? atoi(argv[6]) : 12;
+  const std::string mode = argc > 7 ? argv[7] : "dump";
+  const bool full = (mode == "dump");
+
+  TexturedMesh mesh;
+  if (!ReadGDM(argv[1], mesh)) { fprintf(stderr, "cannot read %s\n", argv[1]); return 2; }
+  const int width = mesh.texture.width(), height = mesh.texture.height();
+  Dump out(argv[2]);
+
+  auto T0 = std::chrono::steady_clock::now();
+  auto secs = [](std::chrono::steady_clock::time_point a) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
+  };
+
+  // ---------------- hierarchy -------------------------------------------------------------
+  MultigridBlockInfo blockInfo(128, 16, 2, 0, 0);  // app defaults TextureFiltering.cpp:25-28
+  std::vector<TextureNodeInfo> textureNodes;
+  std::vector<CellIndex> cellIndices;
+  HierarchicalSystem hierarchy;
+  std::vector<AtlasChart> atlasCharts;
+  if (!InitializeHierarchy(mesh, width, height, levels, textureNodes, cellIndices, hierarchy, atlasCharts, blockInfo, false, false)) {
+    fprintf(stderr, "InitializeHierarchy failed\n");
+    return 3;
+  }
+  double tHierarchy = secs(T0);
+  auto T1 = std::chrono::steady_clock::now();
+  BoundaryProlongationData boundaryProlongation;
+  if (!InitializeBoundaryProlongationData(hierarchy.gridAtlases[0], boundaryProlongation)) return 3;
+  std::vector<std::vector<SquareMatrix<double, 2>>> parameterMetric;
+  if (!InitializeMetric(mesh, EMBEDDING_METRIC, atlasCharts, parameterMetric)) return 3;
+
+  const GridAtlas& fine = hierarchy.gridAtlases[0];
+  std::vector<Point3D<double>> inputSignal(textureNodes.size());
+  std::vector<Vec> f0(textureNodes.size());
+  for (size_t i = 0; i < textureNodes.size(); i++) {
+    Point3D<float> t = mesh.texture(textureNodes[i].ci, textureNodes[i].cj);
+    inputSignal[i] = Point3D<double>(t[0], t[1], t[2]);
+    f0[i] = SetData(t[0], t[1], t[2]);
+  }
+
+  std::vector<double> deepMass, deepStiffness, texelToCell;
+  SparseMatrix<double, int> bbM, bbS, bdM, bdS, cellRHS[3];
+  if (!InitializeMassAndStiffness(deepMass, deepStiffness, bbM, bbS, bdM, bdS, hierarchy, parameterMetric, atlasCharts,
+                                  boundaryProlongation, false, inputSignal, texelToCell, cellRHS)) {
+    fprintf(stderr, "InitializeMassAndStiffness failed\n");
+    return 3;
+  }
+  double tAssembly = secs(T1);
+
+  // ---------------- system ---------------------------------------------------------------
+  auto T2 = std::chrono::steady_clock::now();
+  SparseMatrix<double, int> mass, stiffness, A;
+  FullMatrixConstruction(fine, deepMass, bbM, bdM, mass);
+  FullMatrixConstruction(fine, deepStiffness, bbS, bdS, stiffness);
+  A = mass + stiffness * stiffnessWeight;
+
+  std::vector<MultigridLevelCoefficients<Real>> coeffs;
+  EigenCholeskySolver3<Real> coarseSolver;
+  std::vector<EigenCholeskySolver3<Real>> boundarySolvers;
+  EigenCholeskySolver3<Real> directSolver;
+  if (!UpdateLinearSystem(stiffnessWeight, 1.0, hierarchy, coeffs, deepMass, deepStiffness, bbM, bbS, bdM, bdS, coarseSolver,
+                          boundarySolvers, directSolver, A, false, true, false)) {
+    fprintf(stderr, "UpdateLinearSystem failed\n");
+    return 3;
+  }
+  double tSystem = secs(T2);
+
+  std::vector<Vec> mf(f0.size()), sf(f0.size()), rhs(f0.size());
+  MultiplyBySystemMatrix_NoReciprocals(deepMass, bdM, bbM, fine.boundaryGlobalIndex, fine.rasterLines, f0, mf);
+  MultiplyBySystemMatrix_NoReciprocals(deepStiffness, bdS, bbS, fine.boundaryGlobalIndex, fine.rasterLines, f0, sf);
+  for (size_t i = 0; i < f0.size(); i++) rhs[i] = mf[i] + sf[i] * (Real)(sharpnessWeight * stiffnessWeight);
+
+  // combined FP64 operator (no reciprocals) for residual checks
+  std::vector<double> deepA(deepMass.size());
+  for (size_t i = 0; i < deepA.size(); i++) deepA[i] = deepMass[i] + stiffnessWeight * deepStiffness[i];
+  SparseMatrix<double, int> BBA = bbM + bbS * stiffnessWeight;
+  SparseMatrix<double, int> BDA = bdM + bdS * stiffnessWeight;
+
+  // ---------------- FP64 direct solve (the accuracy oracle) ------------------------------
+  auto T3 = std::chrono::steady_clock::now();
+  std::vector<Vec> exact(f0.size(), ZeroData());
+#if !USE_FLOAT  // the FP32 build only reproduces the shipped V-cycle; ground truth needs FP64
+  directSolver.init(A);
+  directSolver.update(A);
+  solve(directSolver, exact, rhs);
+#endif
+  double tDirect = secs(T3);
+
+  // ---------------- V-cycles ------------------------------------------------------------
+  std::vector<MultigridLevelIndices<Real>> indices(levels);
+  for (int l = 0; l < levels; l++) {
+    const GridAtlas& g = hierarchy.gridAtlases[l];
+    indices[l].threadTasks = g.threadTasks;
+    indices[l].boundaryGlobalIndex = g.boundaryGlobalIndex;
+    indices[l].segmentedLines = g.segmentedLines;
+    indices[l].rasterLines = g.rasterLines;
+    indices[l].restrictionLines = g.restrictionLines;
+    indices[l].prolongationLines = g.prolongationLines;
+    if (l < levels - 1) indices[l].boundaryRestriction = hierarchy.boundaryRestriction[l];
+  }
+  std::vector<MultigridLevelVariables<Vec>> vars(levels);
+  for (int l = 0; l < levels; l++) {
+    const GridAtlas& g = hierarchy.gridAtlases[l];
+    vars[l].x.assign(g.numTexels, ZeroData());
+    vars[l].rhs.assign(g.numTexels, ZeroData());
+    vars[l].residual.assign(g.numTexels, ZeroData());
+    vars[l].boundary_rhs.assign(g.boundaryGlobalIndex.size(), ZeroData());
+    vars[l].boundary_value.assign(g.boundaryGlobalIndex.size(), ZeroData());
+    vars[l].variable_boundary_value.assign(g.boundaryGlobalIndex.size(), ZeroData());
+  }
+  for (size_t i = 0; i < f0.size(); i++) vars[0].rhs[i] = rhs[i];
+  std::vector<double> history, cycleTimes;
+  double bn[3], rn[3];
+  history.push_back(ResidualNorm(coeffs, deepA, BDA, BBA, fine, vars[0].x, rhs, bn, rn));
+  std::vector<double> firstIterate;
+  for (int it = 0; it < vcycles; it++) {
+    auto Tc = std::chrono::steady_clock::now();
+    VCycle(vars, coeffs, indices, boundarySolvers, coarseSolver, false, false);
+    cycleTimes.push_back(secs(Tc));
+    history.push_back(ResidualNorm(coeffs, deepA, BDA, BBA, fine, vars[0].x, rhs, bn, rn));
+    if (it == 0 && full)
+      for (size_t i = 0; i < f0.size(); i++)
+        for (int c = 0; c < 3; c++) firstIterate.push_back((double)vars[0].x[i][c]);
+  }
+
+  // ---------------- output --------------------------------------------------------------
+  out.i32("meta/size", {width, height, levels, (int)atlasCharts.size(), omp_get_max_threads()});
+  out.f64("meta/weights", {stiffnessWeight, sharpnessWeight});
+  out.f64("time/setup", {tHierarchy, tAssembly, tSystem, tDirect});
+  out.f64("time/vcycle", cycleTimes);
+  out.f64("vcycle/history", history);
+  auto vec3 = [&](const std::vector<Vec>& v) {
+    std::vector<double> o(v.size() * 3);
+    for (size_t i = 0; i < v.size(); i++)
+      for (int c = 0; c < 3; c++) o[3 * i + c] = (double)v[i][c];
+    return o;
+  };
+  out.f64("solve/f", vec3(f0), 3);
+  out.f64("solve/rhs", vec3(rhs), 3);
+  out.f64("solve/exact", vec3(exact), 3);
+  out.f64("solve/vcycle_x", vec3(vars[0].x), 3);
+  if (full) out.f64("solve/vcycle_x1", firstIterate, 3);
+
+  for (int l = 0; l < levels; l++) {
+    const GridAtlas& g = hierarchy.gridAtlases[l];
+    std::string p = "L" + std::to_string(l) + "/";
+    out.i32(p + "counts", {g.numTexels, g.numDeepTexels, g.numBoundaryTexels, g.numCells, g.numBoundaryCells, g.numInteriorCells,
+                           g.numInteriorTexels});
+    if (!full) continue;
+    std::vector<int> ni;
+    for (auto& n : g.nodeInfo) { ni.push_back(n.chartId); ni.push_back(n.ci); ni.push_back(n.cj); ni.push_back(n.nodeType); }
+    out.i32(p + "nodeinfo", ni, 4);
+    out.i32(p + "boundaryGlobalIndex", g.boundaryGlobalIndex);
+    out.i32(p + "deepGlobalIndex", g.deepGlobalIndex);
+    out.i32(p + "boundaryAndDeepIndex", g.boundaryAndDeepIndex);
+    std::vector<int> rl;
+    for (auto& r : g.rasterLines) { rl.insert(rl.end(), {r.lineStartIndex, r.lineEndIndex, r.prevLineIndex, r.nextLineIndex, r.coeffStartIndex}); }
+    out.i32(p + "rasterLines", rl, 5);
+    rl.clear();
+    for (auto& r : g.restrictionLines) { rl.insert(rl.end(), {r.lineStartIndex, r.lineEndIndex, r.prevLineIndex, r.nextLineIndex, r.coeffStartIndex}); }
+    out.i32(p + "restrictionLines", rl, 5);
+    rl.clear();
+    for (auto& r : g.deepLines) { rl.insert(rl.end(), {r.coarseLineStartIndex, r.coarseLineEndIndex, r.finePrevLineIndex, r.fineCurrentLineIndex, r.fineNextLineIndex}); }
+    out.i32(p + "deepLines", rl, 5);
+    rl.clear();
+    for (auto& r : g.prolongationLines) { rl.insert(rl.end(), {r.startIndex, r.length, r.centerLineIndex, r.prevLineIndex, r.nextLineIndex, (int)r.alignedStart}); }
+    out.i32(p + "prolongationLines", rl, 6);
+    std::vector<int> ci;
+    std::vector<double> cd;
+    std::vector<int> ctype, ntype;
+    for (auto& c : g.gridCharts) {
+      ci.insert(ci.end(), {c.cornerCoords[0], c.cornerCoords[1], c.centerOffset[0], c.centerOffset[1], c.width, c.height,
+                           c.globalIndexTexelOffset, c.globalTexelDeepOffset, c.globalTexelBoundaryOffset, c.globalIndexCellOffset,
+                           c.numInteriorCells, c.numBoundaryCells});
+      cd.insert(cd.end(), {c.corner[0], c.corner[1], c.cellSizeW, c.cellSizeH});
+      for (int k = 0; k < c.cellType.size(); k++) ctype.push_back(c.cellType[k]);
+      for (int k = 0; k < c.nodeType.size(); k++) ntype.push_back(c.nodeType[k]);
+    }
+    out.i32(p + "charts_i", ci, 12);
+    out.f64(p + "charts_d", cd, 4);
+    out.i32(p + "cellType", ctype);
+    out.i32(p + "nodeType", ntype);
+    // multigrid coefficients (reciprocal form for l < levels-1)
+    std::vector<double> dc(coeffs[l].deepCoefficients.begin(), coeffs[l].deepCoefficients.end());
+    out.f64(p + "coef/deep", dc, 10);
+    out.csr(p + "coef/BB", coeffs[l].boundaryBoundaryMatrix);
+    out.csr(p + "coef/BD", coeffs[l].boundaryDeepMatrix);
+    if (l < levels - 1) out.csr(p + "boundaryRestriction", hierarchy.boundaryRestriction[l]);
+  }
+  if (full) {
+    std::vector<int> tn;
+    std::vector<double> tb;
+    for (auto& n : textureNodes) {
+      tn.insert(tn.end(), {n.ci, n.cj, n.chartId, n.tId, (int)n.isInterior});
+      tb.insert(tb.end(), {n.baricentricCoords[0], n.baricentricCoords[1]});
+    }
+    out.i32("fine/textureNodes", tn, 5);
+    out.f64("fine/textureBary", tb, 2);
+    out.f64("fine/deepMass", deepMass, 10);
+    out.f64("fine/deepStiffness", deepStiffness, 10);
+    out.csr("fine/BBmass", bbM);
+    out.csr("fine/BBstiffness", bbS);
+    out.csr("fine/BDmass", bdM);
+    out.csr("fine/BDstiffness", bdS);
+    out.csr("fine/A", A);
+    out.i32("fine/boundaryNodes", {fine.numBoundaryNodes, fine.numMidPoints, fine.numFineNodes, boundaryProlongation.numFineBoundarNodes});
+    out.csr("fine/boundaryProlongation", boundaryProlongation.coarseBoundaryFineBoundaryProlongation);
+    std::vector<int> ac;
+    std::vector<double> ad;
+    for (auto& c : atlasCharts) {
+      ac.insert(ac.end(), {c.originCoords[0], c.originCoords[1], (int)c.triangles.size(), (int)c.vertices.size(), (int)c.boundaryHalfEdges.size()});
+      ad.insert(ad.end(), {c.minCorner[0], c.minCorner[1], c.maxCorner[0], c.maxCorner[1], c.gridOrigin[0], c.gridOrigin[1]});
+    }
+    out.i32("atlas/charts_i", ac, 5);
+    out.f64("atlas/charts_d", ad, 6);
+    for (int l = 1; l < levels; l++) {
+      std::string p = "L" + std::to_string(l) + "/";
+      out.csr(p + "boundaryCoarseFineProlongation", hierarchy.boundaryCoarseFineProlongation[l]);
+    }
+  }
+  fprintf(stderr, "ok: %d texels, %d levels, hierarchy %.3fs assembly %.3fs system %.3fs direct %.3fs, vcycle %.4fs, resid %g -> %g\n",
+          fine.numTexels, levels, tHierarchy, tAssembly, tSystem, tDirect,
+          cycleTimes.empty() ? 0.0 : cycleTimes.back(), history.front(), history.back());
+  return 0;
+}
