@@ -1,0 +1,304 @@
+"""Benchmark: mixed-precision texel-FEM solve on the B200.
+
+Workload (the icosphere configuration): icosphere subdivided 6x (81,920
+triangles, vertices jittered N(0, 1e-3)), 16 latitude/longitude charts packed
+with 8-texel gutters, 2048x2048 RGB texture of seeded value noise + U(-0.1, 0.1).
+Operator M + 1e-3 S (screened Poisson / TextureFiltering form), right-hand side
+M f + 1e-3 * 2 * S f, 3 right-hand sides solved together.
+
+One step = one solve of all 3 right-hand sides from x = 0 to relative residual
+<= 1e-6 (FP64 operator, every RHS): FP32 V-cycles inside FP64 refinement.
+
+  value  Mtexels/s = texels x RHS / solve time / 1e6, inputs resident in HBM
+         (device API gdtp_solve_device), device-timed with CUDA events.
+  e2e    same through the host API gdtp_solve with pinned host buffers
+         (H2D of b and x0, D2H of x inside every step).
+  --impl reference: the reference's own CPU solver (oracle/_ref/gdtp_ref: the
+         reference headers compiled unmodified) on the host cores, same mesh,
+         texture, operator and tolerance; its V-cycles are timed.
+
+Multi-GPU (torchrun): every rank solves its own copy (replicas, no collective on
+the solve path); value = total texels x RHS of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mtexels solved/s at 1e-6 rel. residual, mixed vs FP64; p50/p99 latency"
+WIDTH = 2048
+LAMBDA, SHARP, TOL, K = 1e-3, 2.0, 1e-6, 3
+
+
+def workload():
+    from gradientdomaintextureprocessing_b200 import meshgen
+    return meshgen.icosphere_atlas(WIDTH, WIDTH, subdiv=6, seed=0)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[3 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(self.samples[0][1]),
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local, dist
+
+
+def run_reference(args, rank: int) -> dict:
+    """Times the reference's CPU V-cycle loop (oracle/_ref/gdtp_ref, time mode)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "gdtp_ref")
+    cores = os.cpu_count() or 1
+    if not os.path.exists(exe):
+        return {"impl": "reference", "unavailable": "oracle/_ref/gdtp_ref not built (needs the reference sources at build time)"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from gdd import read_dump
+    from gradientdomaintextureprocessing_b200 import meshgen
+    mesh = workload()
+    with tempfile.TemporaryDirectory() as tmp:
+        gdm = os.path.join(tmp, "mesh.gdm")
+        meshgen.write_gdm(gdm, mesh)
+        per_step, hist, counts = [], None, None
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+        for step in range(args.warmup + args.steps):
+            out = os.path.join(tmp, f"r{step}.gdd")
+            subprocess.run([exe, gdm, out, "4", str(LAMBDA), str(SHARP), "60", "time", str(TOL)], check=True,
+                           capture_output=True, env=env)
+            d = read_dump(out)
+            hist, counts = d["vcycle/history"], d["L0/counts"]
+            if step >= args.warmup:
+                per_step.append(float(d["time/vcycle"].sum()))
+    n0 = int(counts[0])
+    t = float(np.mean(per_step))
+    value = n0 * K / t / 1e6
+    return {"metric": METRIC, "value": value, "unit": "Mtexels/s (texels x RHS)", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "icosphere6 2048x2048 RGB, 16 charts, screened Poisson 1e-3, 3 RHS, tol 1e-6",
+                       "texels": n0, "rhs": K, "levels": 4, "vcycles": len(hist) - 1,
+                       "final_rel_residual": float(hist[-1]), "solver": "reference FP64 V-cycle (Vec4d), OpenMP"},
+            "cpu_baseline": {"value": value, "unit": "Mtexels/s (texels x RHS)", "cores": cores, "kind": "reference",
+                             "sample": "full workload: the reference V-cycles to 1e-6, set-up excluded"},
+            "e2e": {"value": value, "unit": "Mtexels/s (texels x RHS)", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, rank)), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    from gradientdomaintextureprocessing_b200 import build as _build
+    _build.build()
+    from gradientdomaintextureprocessing_b200 import _lib
+    from gradientdomaintextureprocessing_b200.hierarchy import InitializeHierarchy
+    from gradientdomaintextureprocessing_b200.system import System, texel_signal, texture_filtering_rhs
+    import ctypes as C
+
+    t0 = time.time()
+    mesh = workload()
+    h = InitializeHierarchy(mesh, levels=4)
+    s = System(h, device=local)
+    s.update(LAMBDA, 1.0)
+    f = texel_signal(h, mesh["texture"])
+    b_host = texture_filtering_rhs(s, f, LAMBDA, SHARP)
+    setup_s = time.time() - t0
+    n0 = b_host.shape[0]
+    L = _lib.lib()
+
+    # device-resident inputs
+    b_dev = torch.from_numpy(b_host).to("cuda")
+    x_dev = torch.zeros_like(b_dev)
+    stream = torch.cuda.current_stream()
+    rep = _lib.Report()
+
+    def device_step():
+        x_dev.zero_()
+        code = L.gdtp_solve_device(s.handle, C.c_void_p(b_dev.data_ptr()), C.c_void_p(x_dev.data_ptr()), K, TOL, 60,
+                                   C.c_void_p(stream.cuda_stream), C.byref(rep))
+        if code != 0:
+            _lib.check(code)
+        return rep.iterations, rep.rel_residual_max
+
+    for _ in range(args.warmup):
+        device_step()
+    C.c_int64()
+    prof_reset = C.c_int64()
+    L.gdtp_system_array(s.handle, b"profile.reset", 0, None, C.byref(prof_reset))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    lat, iters, resid = [], [], []
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clocks:
+        ev[0].record(stream)
+        for i in range(args.steps):
+            it, r = device_step()
+            ev[i + 1].record(stream)
+            iters.append(it)
+            resid.append(r)
+        torch.cuda.synchronize()
+    for i in range(args.steps):
+        lat.append(ev[i].elapsed_time(ev[i + 1]))
+    total_ms = ev[0].elapsed_time(ev[-1])
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    prof = np.zeros(4)
+    cnt = C.c_int64()
+    L.gdtp_system_array(s.handle, b"profile", 0, prof.ctypes.data_as(C.c_void_p), C.byref(cnt))
+    value = world * n0 * K * args.steps / (total_ms * 1e-3) / 1e6
+
+    # end to end through the host API with pinned buffers
+    b_pin = torch.from_numpy(b_host).pin_memory().numpy()
+    x_pin = torch.zeros(b_host.shape, dtype=torch.float64).pin_memory().numpy()
+
+    def host_step():
+        x_pin[:] = 0.0
+        code = L.gdtp_solve(s.handle, b_pin.ctypes.data_as(C.c_void_p), x_pin.ctypes.data_as(C.c_void_p), K, TOL, 60, C.byref(rep))
+        if code != 0:
+            _lib.check(code)
+
+    host_step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        host_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * n0 * K * args.steps / (e2e_ms * 1e-3) / 1e6
+    rel_final = float(s.residual(b_host, x_pin).max())
+
+    # plain FP64 GPU V-cycle on the same problem (the comparator path), one solve
+    x64, rep64 = s.solve(b_host, tol=TOL, precision="fp64")
+    t64 = rep64["seconds"]
+    # dominant kernel: level-0 colour Gauss-Seidel sweep (4 colour passes), timed
+    # by events recorded inside the captured refinement graph
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    sweep_ms = prof[1] / max(prof[0], 1)
+    texels = prof[2]
+    # algorithmic bytes of one 4-colour sweep on level 0 (FP32, 4 channels): per
+    # deep texel 10 coefficients (40 B) + rhs (16 B) + x written once (16 B) +
+    # x read once per colour pass for the 3 other colours' values (3 x 16 B)
+    sweep_bytes = texels * (40 + 16 + 16 + 48)
+    achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9 if sweep_ms > 0 else None
+    launches = int(sum(iters) * prof[3] + args.steps * 2)
+
+    out = {"metric": METRIC, "value": value, "unit": "Mtexels/s (texels x RHS)", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 V-cycle + f64 refinement", "data": "synthetic",
+           "config": {"workload": "icosphere6 2048x2048 RGB, 16 charts, screened Poisson 1e-3, 3 RHS, tol 1e-6",
+                      "texels": n0, "rhs": K, "levels_used": s.levels_used, "l2": "inputs larger than L2 (>126 MB resident)",
+                      "parallelism": f"replicas x{world}", "setup_s": round(setup_s, 2)},
+           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+           "refinement_steps": {"mean": float(np.mean(iters)), "max": int(max(iters))},
+           "rel_residual": {"device_path_max": float(max(resid)), "host_path_final": rel_final},
+           "fp64_vcycle": {"value": n0 * K / t64 / 1e6, "unit": "Mtexels/s (texels x RHS)", "vcycles": rep64["vcycles"],
+                           "rel_residual": rep64["rel_residual_max"]},
+           "e2e": {"value": e2e_value, "unit": "Mtexels/s (texels x RHS)", "h2d_bytes_per_step": int(b_host.nbytes * 2),
+                   "d2h_bytes_per_step": int(b_host.nbytes)},
+           "roofline": {"bound": "hbm", "kernel": "level-0 4-colour Gauss-Seidel sweep (k_gs_colour x4)",
+                        "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": (achieved / peak) if achieved else None, "traffic": None,
+                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                        "bytes_per_launch": sweep_bytes, "ms_per_launch": sweep_ms},
+           "gpu_launches": launches,
+           "clocks": clocks.summary()}
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        ref = run_reference(argparse.Namespace(gpus=1, steps=1, warmup=0), 0)
+        out["cpu_baseline"] = ref.get("cpu_baseline", {"unavailable": ref.get("unavailable")})
+        if "config" in ref:
+            out["cpu_baseline"]["vcycles"] = ref["config"]["vcycles"]
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -40,7 +40,9 @@ extern "C" int gdtp_hierarchy_build(const double* vertices, int64_t nv, const in
   }
   h->width = width;
   h->height = height;
-  if (!build_hierarchy(h->mesh, width, height, levels, info, h->h)) return fail(GDTP_ERR_SETUP, "hierarchy: " + h->h.error);
+  // levels beyond the requested ones are added until the coarsest level is small
+  // enough for the dense direct solve of the device V-cycle
+  if (!build_hierarchy(h->mesh, width, height, levels, info, h->h, 2600, 12)) return fail(GDTP_ERR_SETUP, "hierarchy: " + h->h.error);
   std::string err;
   if (!build_boundary_elements(h->h, h->be, err)) return fail(GDTP_ERR_SETUP, "boundary elements: " + err);
   *out = h.release();

@@ -1,0 +1,170 @@
+// C ABI: device system (assembly, update, apply, V-cycle, solves).
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/gdtp.h"
+#include "capi_internal.h"
+#include "system.h"
+
+using namespace gdtp;
+
+struct gdtp_system {
+  gdtp_hierarchy* h = nullptr;
+  std::unique_ptr<DeviceSystem> sys;
+};
+
+#define GDTP_SYS_CHECK(s)                                                       \
+  do {                                                                          \
+    if (!(s) || !(s)->sys) return fail(GDTP_ERR_INVALID, "null system handle"); \
+  } while (0)
+
+static int sys_fail(gdtp_system* s, int code) { return fail(code, s->sys->error()); }
+
+extern "C" int gdtp_system_create(gdtp_hierarchy* h, int device, int metric_mode, const double* parameter_metric,
+                                  const double* vertices, int64_t nv, gdtp_system** out) {
+  if (!h || !out) return fail(GDTP_ERR_INVALID, "gdtp_system_create: null argument");
+  if (metric_mode != 0 && !parameter_metric) return fail(GDTP_ERR_INVALID, "gdtp_system_create: unknown metric mode");
+  *out = nullptr;
+  std::unique_ptr<gdtp_system> s(new gdtp_system());
+  s->h = h;
+  Mesh mesh = h->mesh;
+  if (vertices) {
+    if (nv != mesh.nv()) return fail(GDTP_ERR_INVALID, "gdtp_system_create: vertex count differs from the hierarchy's mesh");
+    mesh.vertices.assign(vertices, vertices + nv * 3);
+  }
+  s->sys.reset(new DeviceSystem(h->h, h->be, device));
+  if (!s->sys->ok()) return fail(GDTP_ERR_CUDA, s->sys->error());
+  if (!s->sys->assemble(mesh, parameter_metric)) return fail(GDTP_ERR_CUDA, s->sys->error());
+  *out = s.release();
+  return GDTP_OK;
+}
+
+extern "C" void gdtp_system_free(gdtp_system* s) { delete s; }
+
+extern "C" int gdtp_system_update(gdtp_system* s, double stiffness_weight, double screen_weight) {
+  GDTP_SYS_CHECK(s);
+  if (!(screen_weight >= 0) || !(stiffness_weight >= 0) || screen_weight + stiffness_weight == 0)
+    return fail(GDTP_ERR_INVALID, "gdtp_system_update: weights must be non-negative and not both zero");
+  if (!s->sys->update(stiffness_weight, screen_weight)) return sys_fail(s, GDTP_ERR_NUMERIC);
+  return GDTP_OK;
+}
+
+extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int level, void* out, int64_t* count) {
+  if (!s || !s->sys || !cname) return fail(GDTP_ERR_INVALID, "gdtp_system_array: bad arguments");
+  const std::string name(cname);
+  const FineSystem& f = s->sys->fine();
+  auto vec = [&](const std::vector<double>& v) {
+    if (count) *count = (int64_t)v.size();
+    if (out && !v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(double));
+    return GDTP_OK;
+  };
+  if (name == "deepMass") return vec(f.deepMass);
+  if (name == "deepStiffness") return vec(f.deepStiffness);
+  auto part = [&](const std::string& prefix) { return name.substr(prefix.size()); };
+  if (name.rfind("bbMass.", 0) == 0) return emit_csr(f.bbMass, part("bbMass."), out, count);
+  if (name.rfind("bbStiffness.", 0) == 0) return emit_csr(f.bbStiffness, part("bbStiffness."), out, count);
+  if (name.rfind("bdMass.", 0) == 0) return emit_csr(f.bdMass, part("bdMass."), out, count);
+  if (name.rfind("bdStiffness.", 0) == 0) return emit_csr(f.bdStiffness, part("bdStiffness."), out, count);
+  const auto& co = s->sys->coefficients();
+  if (name.rfind("coef.", 0) == 0) {
+    if (level < 0 || level >= (int)co.size()) return fail(GDTP_ERR_STATE, "coefficients not available for this level (update first)");
+    if (name == "coef.deep") return vec(co[level].deep);
+    if (name.rfind("coef.bb.", 0) == 0) return emit_csr(co[level].bb, part("coef.bb."), out, count);
+    if (name.rfind("coef.bd.", 0) == 0) return emit_csr(co[level].bd, part("coef.bd."), out, count);
+  }
+  if (name == "profile") {  // {timed groups, total ms, deep texels per group, kernels per refinement graph}
+    double v[4] = {s->sys->profCount, s->sys->profMs, s->sys->profTexels, double(s->sys->graphKernels)};
+    if (count) *count = 4;
+    if (out) std::memcpy(out, v, sizeof(v));
+    return GDTP_OK;
+  }
+  if (name == "profile.reset") {
+    const_cast<DeviceSystem*>(s->sys.get())->profCount = 0;
+    const_cast<DeviceSystem*>(s->sys.get())->profMs = 0;
+    if (count) *count = 0;
+    return GDTP_OK;
+  }
+  if (name == "levelsUsed") {
+    if (count) *count = 1;
+    if (out) *static_cast<int32_t*>(out) = s->sys->levelsUsed();
+    return GDTP_OK;
+  }
+  return fail(GDTP_ERR_INVALID, "gdtp_system_array: unknown array " + name);
+}
+
+extern "C" int gdtp_apply(gdtp_system* s, int which, const double* x, double* y, int k) {
+  GDTP_SYS_CHECK(s);
+  if (!x || !y || which < 0 || which > 2) return fail(GDTP_ERR_INVALID, "gdtp_apply: bad arguments");
+  return s->sys->apply(which, x, y, k) ? GDTP_OK : sys_fail(s, GDTP_ERR_CUDA);
+}
+
+extern "C" int gdtp_vcycle(gdtp_system* s, float* x, const float* rhs, int k) {
+  GDTP_SYS_CHECK(s);
+  if (!x || !rhs) return fail(GDTP_ERR_INVALID, "gdtp_vcycle: null vector");
+  return s->sys->vcycle_host(x, rhs, k) ? GDTP_OK : sys_fail(s, GDTP_ERR_CUDA);
+}
+
+static void fill_report(gdtp_report* r, const SolveReport& rep) {
+  if (!r) return;
+  r->iterations = rep.iterations;
+  r->vcycles = rep.vcycles;
+  r->rel_residual_max = rep.relMax;
+  r->seconds = rep.seconds;
+}
+
+extern "C" int gdtp_solve(gdtp_system* s, const double* b, double* x, int k, double tol, int max_iters, gdtp_report* report) {
+  GDTP_SYS_CHECK(s);
+  if (!b || !x || !(tol > 0) || max_iters < 0) return fail(GDTP_ERR_INVALID, "gdtp_solve: bad arguments");
+  SolveReport rep;
+  if (!s->sys->solve_mixed(b, x, nullptr, nullptr, k, tol, max_iters, nullptr, rep)) return sys_fail(s, GDTP_ERR_CUDA);
+  fill_report(report, rep);
+  return rep.relMax <= tol ? GDTP_OK : fail(GDTP_ERR_NOT_CONVERGED, "relative residual above tolerance after max_iters");
+}
+
+extern "C" int gdtp_solve_device(gdtp_system* s, const double* b_dev, double* x_dev, int k, double tol, int max_iters, void* stream,
+                                 gdtp_report* report) {
+  GDTP_SYS_CHECK(s);
+  if (!b_dev || !x_dev || !(tol > 0) || max_iters < 0) return fail(GDTP_ERR_INVALID, "gdtp_solve_device: bad arguments");
+  SolveReport rep;
+  if (!s->sys->solve_mixed(nullptr, nullptr, b_dev, x_dev, k, tol, max_iters, static_cast<cudaStream_t>(stream), rep))
+    return sys_fail(s, GDTP_ERR_CUDA);
+  fill_report(report, rep);
+  return rep.relMax <= tol ? GDTP_OK : fail(GDTP_ERR_NOT_CONVERGED, "relative residual above tolerance after max_iters");
+}
+
+extern "C" int gdtp_solve_fp64(gdtp_system* s, const double* b, double* x, int k, double tol, int max_iters, gdtp_report* report) {
+  GDTP_SYS_CHECK(s);
+  if (!b || !x || !(tol > 0) || max_iters < 0) return fail(GDTP_ERR_INVALID, "gdtp_solve_fp64: bad arguments");
+  SolveReport rep;
+  if (!s->sys->solve_fp64(b, x, k, tol, max_iters, rep)) return sys_fail(s, GDTP_ERR_CUDA);
+  fill_report(report, rep);
+  return rep.relMax <= tol ? GDTP_OK : fail(GDTP_ERR_NOT_CONVERGED, "relative residual above tolerance after max_iters");
+}
+
+extern "C" int gdtp_residual(gdtp_system* s, const double* b, const double* x, int k, double* rel) {
+  GDTP_SYS_CHECK(s);
+  if (!b || !x || !rel) return fail(GDTP_ERR_INVALID, "gdtp_residual: null argument");
+  return s->sys->residual_host(b, x, k, rel) ? GDTP_OK : sys_fail(s, GDTP_ERR_CUDA);
+}
+
+extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
+  GDTP_SYS_CHECK(s);
+  if (!knob) return fail(GDTP_ERR_INVALID, "gdtp_system_set: null knob");
+  const std::string k(knob);
+  SolverKnobs& kn = s->sys->knobs;
+  const int v = int(value);
+  if (k == "pre_sweeps" && v >= 0 && v <= 16) kn.preSweeps = v;
+  else if (k == "post_sweeps" && v >= 0 && v <= 16) kn.postSweeps = v;
+  else if (k == "max_block" && v >= 16 && v <= 1024) kn.maxBlock = v;
+  else if (k == "max_coarse" && v >= 16 && v <= 12000) kn.maxCoarse = v;
+  else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
+  s->sys->invalidate_graph();
+  return GDTP_OK;
+}
+
+extern "C" int gdtp_system_device_bytes(const gdtp_system* s, int64_t* bytes) {
+  if (!s || !s->sys || !bytes) return fail(GDTP_ERR_INVALID, "gdtp_system_device_bytes: bad arguments");
+  *bytes = (int64_t)s->sys->deviceBytes();
+  return GDTP_OK;
+}

@@ -1,0 +1,68 @@
+// Host-callable launchers of the V-cycle kernels (vcycle_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace gdtp {
+namespace dev {
+
+struct ColourRun;
+struct RestrictRun;
+struct ProlongRun;
+
+// Device view of one level's exact boundary solver (see setup/bsolve.cpp).
+template <typename T>
+struct BoundaryDev {
+  int nb = 0, nSub = 0, nI = 0, nS = 0, maxBlock = 0;
+  const int* subPtr = nullptr;
+  const long long* invOff = nullptr;
+  const T* inv = nullptr;
+  const int* posGlobal = nullptr;   // position -> global texel
+  const T* scale = nullptr;
+  const int *bdPtr = nullptr, *bdCol = nullptr;
+  const T* bdVal = nullptr;
+  const int *aisPtr = nullptr, *aisCol = nullptr;
+  const T* aisVal = nullptr;
+  const int *asiPtr = nullptr, *asiCol = nullptr;
+  const T* asiVal = nullptr;
+  const T* sinv = nullptr;
+  T *y = nullptr, *t = nullptr, *xs = nullptr;  // work vectors (nI, nS, nS rows of KP)
+};
+
+template <typename T, int W>
+void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP, cudaStream_t s);
+template <typename T, int W>
+void launch_residual(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const int* bPtr, const int* bCol,
+                     const T* bVal, const int* bGlobal, int nB, const T* rhs, const T* x, T* res, int KP, cudaStream_t s);
+template <typename T, int W>
+void launch_restrict(const RestrictRun* runs, int nRuns, const int* rPtr, const int* rCol, const T* rVal, const int* rOut,
+                     int nB, const T* res, T* coarseRhs, int KP, cudaStream_t s);
+template <typename T, int W>
+void launch_prolong_add(const ProlongRun* runs, int nRuns, const T* coarse, T* fine, int KP, cudaStream_t s);
+template <typename T, int W>
+void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s);
+template <typename T, int W>
+cudaError_t configure_boundary_smem(size_t bytes);
+template <typename T, int W>
+void launch_coarse_solve(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, cudaStream_t s);
+
+void launch_raw_operator(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr, const int* bCol,
+                         const double* bVal, const int* bGlobal, int nB, const double* b, const double* x, double* out, int K,
+                         int mode, double* partials, double* sums, cudaStream_t s);
+int raw_operator_blocks(int nRuns, int nB, int K);
+template <typename T>
+void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s);
+template <typename T>
+void launch_add_correction(double* x, const T* e, long long n, int K, int KP, cudaStream_t s);
+
+// assembly (assembly_kernels.cu)
+void launch_interior_cells(int n, const int* cellPtr, const int* cellTri, const int* cellIJ, const int* cellChart,
+                           const double* chartCellSize, const double* triPos, const double* triMetricInv, const double* triScale,
+                           double* mass, double* stiff, cudaStream_t s);
+void launch_deep_gather(int nDeep, const int* deepCells, const double* cellMass, const double* cellStiff, double* deepMass,
+                        double* deepStiff, cudaStream_t s);
+void launch_boundary_triangles(int n, const int* btPtr, const int* btTri, const double* btPos, const double* triPos,
+                               const double* triMetric, const double* triMetricInv, double* mass, double* stiff, cudaStream_t s);
+void launch_gather_cells(int n, const int* idx, const double* src, double* dst, cudaStream_t s);
+
+}  // namespace dev
+}  // namespace gdtp

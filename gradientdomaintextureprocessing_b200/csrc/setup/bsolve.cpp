@@ -1,0 +1,236 @@
+// Exact solve of the boundary block BB of one level, set up for the device.
+//
+// The reference relaxes boundary texels by a sparse LDLT of BB at every
+// smoothing step (IterativeSolvers.inl:193-209, 414-430; factorised in
+// UpdateCoefficients.inl:402-439 with Eigen SimplicialLDLT, Solver.h:144-203).
+// Boundary rows include texels whose support barely meets the chart (diagonals
+// down to 1e-17 of the typical one), and pointwise relaxation of them stalls, so
+// the exactness matters.  A sparse triangular solve is a long sequential chain
+// on a GPU; instead the boundary graph is split into subdomains of at most
+// `maxBlock` texels plus a vertex separator, and
+//     BB^-1 r  =  [interiors: A_II^-1 (r_I - A_IS x_S)] , x_S = S^-1 (r_S - A_SI A_II^-1 r_I)
+// with S = A_SS - A_SI A_II^-1 A_IS, is applied with dense block inverses only:
+// every step is a batch of independent dense products.  All inverses are of the
+// Jacobi-scaled block D^-1/2 BB D^-1/2 (unit diagonal), which keeps the FP32
+// copies well scaled; they are computed here in FP64.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <queue>
+
+#include "setup.h"
+
+namespace gdtp {
+
+// In-place inverse of a dense SPD matrix (row-major, n x n) via Cholesky.
+// Returns false if not positive definite.
+bool dense_spd_inverse(double* A, int n, bool parallel) {
+  // Cholesky, lower triangle: A = L L^T
+  for (int k = 0; k < n; k++) {
+    double d = A[size_t(k) * n + k];
+    for (int p = 0; p < k; p++) d -= A[size_t(k) * n + p] * A[size_t(k) * n + p];
+    if (!(d > 0)) return false;
+    d = std::sqrt(d);
+    A[size_t(k) * n + k] = d;
+    const double inv = 1.0 / d;
+#pragma omp parallel for schedule(static) if (parallel && n - k > 256)
+    for (int i = k + 1; i < n; i++) {
+      double s = A[size_t(i) * n + k];
+      const double* ri = &A[size_t(i) * n];
+      const double* rk = &A[size_t(k) * n];
+      for (int p = 0; p < k; p++) s -= ri[p] * rk[p];
+      A[size_t(i) * n + k] = s * inv;
+    }
+  }
+  // W = L^-1 (lower), column by column
+  std::vector<double> W(size_t(n) * n, 0.0);
+#pragma omp parallel for schedule(dynamic, 8) if (parallel)
+  for (int j = 0; j < n; j++) {
+    W[size_t(j) * n + j] = 1.0 / A[size_t(j) * n + j];
+    for (int i = j + 1; i < n; i++) {
+      double s = 0;
+      const double* ri = &A[size_t(i) * n];
+      for (int p = j; p < i; p++) s -= ri[p] * W[size_t(p) * n + j];
+      W[size_t(i) * n + j] = s / A[size_t(i) * n + i];
+    }
+  }
+  // A^-1 = W^T W
+#pragma omp parallel for schedule(dynamic, 8) if (parallel)
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j <= i; j++) {
+      double s = 0;
+      for (int p = i; p < n; p++) s += W[size_t(p) * n + i] * W[size_t(p) * n + j];
+      A[size_t(i) * n + j] = A[size_t(j) * n + i] = s;
+    }
+  return true;
+}
+
+bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, BoundarySolverSetup& bs, std::string& err) {
+  const int nb = BB.rows;
+  bs = BoundarySolverSetup();
+  bs.nb = nb;
+  if (nb == 0) return true;
+  std::vector<double> diag(nb, 0.0);
+  for (int i = 0; i < nb; i++)
+    for (int k = BB.ptr[i]; k < BB.ptr[i + 1]; k++)
+      if (BB.col[k] == i) diag[i] = BB.val[k];
+  for (int i = 0; i < nb; i++)
+    if (!(diag[i] > 0)) { err = "boundary block has a non-positive diagonal"; return false; }
+
+  // ---- subdomains: breadth-first growth from the lowest unassigned row
+  std::vector<int> part(nb, -1);
+  int nSub = 0;
+  if (nb <= maxBlock) {
+    std::fill(part.begin(), part.end(), 0);
+    nSub = 1;
+  } else {
+    for (int seed = 0; seed < nb; seed++) {
+      if (part[seed] != -1) continue;
+      std::queue<int> q;
+      q.push(seed);
+      part[seed] = nSub;
+      int size = 1;
+      while (!q.empty() && size < maxBlock) {
+        int u = q.front();
+        q.pop();
+        for (int k = BB.ptr[u]; k < BB.ptr[u + 1] && size < maxBlock; k++) {
+          int v = BB.col[k];
+          if (part[v] == -1) { part[v] = nSub; size++; q.push(v); }
+        }
+      }
+      nSub++;
+    }
+  }
+  // ---- vertex separator: for every cut edge the endpoint in the higher subdomain
+  std::vector<char> sep(nb, 0);
+  for (int u = 0; u < nb; u++)
+    for (int k = BB.ptr[u]; k < BB.ptr[u + 1]; k++) {
+      int v = BB.col[k];
+      if (part[u] != part[v]) sep[part[u] > part[v] ? u : v] = 1;
+    }
+  // order: interiors grouped by subdomain, then separators
+  std::vector<std::vector<int>> members(nSub);
+  for (int u = 0; u < nb; u++)
+    if (!sep[u]) members[part[u]].push_back(u);
+  bs.subPtr.assign(1, 0);
+  for (int p = 0; p < nSub; p++) {
+    if (members[p].empty()) continue;
+    bs.order.insert(bs.order.end(), members[p].begin(), members[p].end());
+    bs.subPtr.push_back((int)bs.order.size());
+  }
+  bs.nSub = (int)bs.subPtr.size() - 1;
+  bs.nI = (int)bs.order.size();
+  for (int u = 0; u < nb; u++)
+    if (sep[u]) bs.order.push_back(u);
+  bs.nS = nb - bs.nI;
+  std::vector<int> pos(nb);
+  for (int k = 0; k < nb; k++) pos[bs.order[k]] = k;
+  bs.scale.resize(nb);
+  for (int k = 0; k < nb; k++) bs.scale[k] = 1.0 / std::sqrt(diag[bs.order[k]]);
+  auto scaled = [&](int i, int kk) { return BB.val[kk] * bs.scale[pos[i]] * bs.scale[pos[BB.col[kk]]]; };
+
+  // ---- subdomain inverses (scaled), and the interior/separator couplings
+  bs.invOff.assign(bs.nSub + 1, 0);
+  for (int p = 0; p < bs.nSub; p++) {
+    int64_t m = bs.subPtr[p + 1] - bs.subPtr[p];
+    bs.invOff[p + 1] = bs.invOff[p] + m * m;
+  }
+  bs.inv.assign(size_t(bs.invOff[bs.nSub]), 0.0);
+  bool ok = true;
+#pragma omp parallel for schedule(dynamic, 1) reduction(&& : ok)
+  for (int p = 0; p < bs.nSub; p++) {
+    const int b0 = bs.subPtr[p], m = bs.subPtr[p + 1] - b0;
+    double* D = &bs.inv[size_t(bs.invOff[p])];
+    for (int a = 0; a < m; a++) {
+      int i = bs.order[b0 + a];
+      for (int kk = BB.ptr[i]; kk < BB.ptr[i + 1]; kk++) {
+        int c = pos[BB.col[kk]] - b0;
+        if (c >= 0 && c < m) D[size_t(a) * m + c] = scaled(i, kk);
+      }
+    }
+    ok = dense_spd_inverse(D, m, false) && ok;
+  }
+  if (!ok) { err = "boundary subdomain block is not positive definite"; return false; }
+  std::vector<Triplet> tIS;
+  for (int k = 0; k < bs.nI; k++) {
+    int i = bs.order[k];
+    for (int kk = BB.ptr[i]; kk < BB.ptr[i + 1]; kk++) {
+      int c = pos[BB.col[kk]];
+      if (c >= bs.nI) tIS.push_back({k, c - bs.nI, scaled(i, kk)});
+    }
+  }
+  bs.AIS = csr_from_triplets(bs.nI, bs.nS, tIS);
+  bs.ASI = csr_transpose(bs.AIS);
+
+  // ---- Schur complement on the separator, S = A_SS - A_SI A_II^-1 A_IS (scaled)
+  if (bs.nS > 0) {
+    const int nS = bs.nS;
+    bs.Sinv.assign(size_t(nS) * nS, 0.0);
+    for (int s = 0; s < nS; s++) {
+      int i = bs.order[bs.nI + s];
+      for (int kk = BB.ptr[i]; kk < BB.ptr[i + 1]; kk++) {
+        int c = pos[BB.col[kk]];
+        if (c >= bs.nI) bs.Sinv[size_t(s) * nS + (c - bs.nI)] = scaled(i, kk);
+      }
+    }
+    // per subdomain: the separator columns it touches
+#pragma omp parallel
+    {
+      std::vector<double> local;
+#pragma omp for schedule(dynamic, 1)
+      for (int p = 0; p < bs.nSub; p++) {
+        const int b0 = bs.subPtr[p], m = bs.subPtr[p + 1] - b0;
+        std::vector<int> touch;
+        for (int a = 0; a < m; a++)
+          for (int kk = bs.AIS.ptr[b0 + a]; kk < bs.AIS.ptr[b0 + a + 1]; kk++) touch.push_back(bs.AIS.col[kk]);
+        std::sort(touch.begin(), touch.end());
+        touch.erase(std::unique(touch.begin(), touch.end()), touch.end());
+        const int t = (int)touch.size();
+        if (!t) continue;
+        // C = A_IS restricted (m x t), then G = Inv C, contribution C^T G
+        std::vector<double> C(size_t(m) * t, 0.0), G(size_t(m) * t, 0.0);
+        for (int a = 0; a < m; a++)
+          for (int kk = bs.AIS.ptr[b0 + a]; kk < bs.AIS.ptr[b0 + a + 1]; kk++) {
+            int c = int(std::lower_bound(touch.begin(), touch.end(), bs.AIS.col[kk]) - touch.begin());
+            C[size_t(a) * t + c] = bs.AIS.val[kk];
+          }
+        const double* Inv = &bs.inv[size_t(bs.invOff[p])];
+        for (int a = 0; a < m; a++)
+          for (int q = 0; q < m; q++) {
+            double w = Inv[size_t(a) * m + q];
+            if (w == 0.0) continue;
+            const double* cq = &C[size_t(q) * t];
+            double* ga = &G[size_t(a) * t];
+            for (int c = 0; c < t; c++) ga[c] += w * cq[c];
+          }
+        local.assign(size_t(t) * t, 0.0);
+        for (int a = 0; a < m; a++)
+          for (int c1 = 0; c1 < t; c1++) {
+            double cv = C[size_t(a) * t + c1];
+            if (cv == 0.0) continue;
+            for (int c2 = 0; c2 < t; c2++) local[size_t(c1) * t + c2] += cv * G[size_t(a) * t + c2];
+          }
+#pragma omp critical
+        for (int c1 = 0; c1 < t; c1++)
+          for (int c2 = 0; c2 < t; c2++) bs.Sinv[size_t(touch[c1]) * nS + touch[c2]] -= local[size_t(c1) * t + c2];
+      }
+    }
+    // symmetrise against rounding, then invert
+    for (int a = 0; a < nS; a++)
+      for (int c = 0; c < a; c++) {
+        double v = 0.5 * (bs.Sinv[size_t(a) * nS + c] + bs.Sinv[size_t(c) * nS + a]);
+        bs.Sinv[size_t(a) * nS + c] = bs.Sinv[size_t(c) * nS + a] = v;
+      }
+    if (!dense_spd_inverse(bs.Sinv.data(), nS, true)) { err = "boundary Schur complement is not positive definite"; return false; }
+  }
+  // ---- boundary-deep coupling rows in solver order (unscaled, global texel columns)
+  std::vector<Triplet> tBD;
+  for (int k = 0; k < nb; k++) {
+    int i = bs.order[k];
+    for (int kk = BD.ptr[i]; kk < BD.ptr[i + 1]; kk++) tBD.push_back({k, BD.col[kk], BD.val[kk]});
+  }
+  bs.BD = csr_from_triplets(nb, BD.cols, tBD);
+  return true;
+}
+
+}  // namespace gdtp

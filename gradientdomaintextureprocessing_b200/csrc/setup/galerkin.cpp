@@ -42,9 +42,9 @@ static int prolong_row(const GridLevel& F, const GridLevel& C, int q, int cols[4
   return m;
 }
 
-bool galerkin_hierarchy(const Hierarchy& h, const std::vector<double>& deep0, const Csr& bb0, const Csr& bd0,
+bool galerkin_hierarchy(const Hierarchy& h, int L, const std::vector<double>& deep0, const Csr& bb0, const Csr& bd0,
                         std::vector<LevelCoefficients>& out, std::string& err) {
-  const int L = (int)h.levels.size();
+  if (L <= 0 || L > (int)h.levels.size()) L = (int)h.levels.size();
   out.assign(L, LevelCoefficients());
   out[0].deep = deep0;
   out[0].bb = bb0;

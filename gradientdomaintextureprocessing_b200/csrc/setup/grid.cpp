@@ -352,16 +352,27 @@ static bool build_prolongation(GridLevel& F, const GridLevel& C, std::string& er
   return true;
 }
 
-bool build_hierarchy(const Mesh& mesh, int width, int height, int levels, const BlockInfo& info, Hierarchy& h) {
+bool build_hierarchy(const Mesh& mesh, int width, int height, int levels, const BlockInfo& info, Hierarchy& h,
+                     int extendToTexels, int maxLevels) {
   h.error.clear();
   if (levels < 1) { h.error = "levels must be >= 1"; return false; }
   if (!build_atlas(mesh, width, height, h.atlas, h.error)) return false;
-  h.levels.assign(levels, GridLevel());
-  for (int l = 0; l < levels; l++)
+  h.levels.clear();
+  h.requestedLevels = levels;
+  for (int l = 0;; l++) {
+    if (l >= levels && (extendToTexels <= 0 || h.levels.back().numTexels <= extendToTexels || l >= maxLevels)) break;
+    h.levels.emplace_back();
     if (!build_level(h.atlas, l, width, height, info, h.levels[l], h.error)) {
+      if (l >= levels) {  // an optional extra level that does not exist: stop coarsening
+        h.levels.pop_back();
+        h.error.clear();
+        break;
+      }
       h.error = "level " + std::to_string(l) + ": " + h.error;
       return false;
     }
+  }
+  levels = (int)h.levels.size();
   for (int l = 0; l + 1 < levels; l++)
     if (!build_restriction(h.levels[l], h.levels[l + 1], h.error) || !build_prolongation(h.levels[l], h.levels[l + 1], h.error)) {
       h.error = "level " + std::to_string(l) + ": " + h.error;

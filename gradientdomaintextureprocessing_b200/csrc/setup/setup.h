@@ -165,6 +165,7 @@ struct GridLevel {
 };
 
 struct Hierarchy {
+  int requestedLevels = 0;              // levels asked for; more may be built for the coarse direct solve
   Atlas atlas;
   std::vector<GridLevel> levels;
   std::string error;
@@ -175,7 +176,10 @@ struct BlockInfo { int blockWidth = 128, blockHeight = 16, paddingWidth = 2, pad
 // atlas.cpp
 bool build_atlas(const Mesh& mesh, int width, int height, Atlas& atlas, std::string& err);
 // grid.cpp
-bool build_hierarchy(const Mesh& mesh, int width, int height, int levels, const BlockInfo& info, Hierarchy& h);
+// Builds `levels` levels, then keeps coarsening while the coarsest level holds
+// more than extendToTexels texels (0: never), up to maxLevels.
+bool build_hierarchy(const Mesh& mesh, int width, int height, int levels, const BlockInfo& info, Hierarchy& h,
+                     int extendToTexels = 0, int maxLevels = 12);
 
 // ----------------------------------------------------------------------------
 // boundary elements and assembly
@@ -243,8 +247,24 @@ struct LevelCoefficients {
   Csr bb, bd;                           // boundary x boundary, boundary x global
 };
 // Galerkin hierarchy A_{l+1} = P^T A_l P; coarsest also as a dense matrix.
-bool galerkin_hierarchy(const Hierarchy& h, const std::vector<double>& deep0, const Csr& bb0, const Csr& bd0,
+bool galerkin_hierarchy(const Hierarchy& h, int levels, const std::vector<double>& deep0, const Csr& bb0, const Csr& bd0,
                         std::vector<LevelCoefficients>& out, std::string& err);
 void full_matrix(const GridLevel& g, const LevelCoefficients& c, Csr& full);
+
+// Exact boundary-block solve by subdomain inverses + separator Schur complement
+// (bsolve.cpp).  Positions k index `order` (interiors by subdomain, then separators).
+struct BoundarySolverSetup {
+  int nb = 0, nSub = 0, nI = 0, nS = 0;
+  std::vector<int> order;               // position -> boundary index
+  std::vector<int> subPtr;              // subdomain -> [subPtr[p], subPtr[p+1]) positions
+  std::vector<double> scale;            // per position: 1/sqrt(BB_ii)
+  std::vector<int64_t> invOff;          // per subdomain offset into inv
+  std::vector<double> inv;              // scaled dense inverses, row-major m x m
+  Csr AIS, ASI;                         // scaled couplings: interior positions x separator, and transpose
+  std::vector<double> Sinv;             // scaled nS x nS inverse Schur complement
+  Csr BD;                               // positions x global texels (unscaled boundary-deep rows)
+};
+bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, BoundarySolverSetup& bs, std::string& err);
+bool dense_spd_inverse(double* A, int n, bool parallel);
 
 }  // namespace gdtp

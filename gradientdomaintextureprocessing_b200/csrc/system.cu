@@ -1,0 +1,678 @@
+// Device-resident texel-FEM system (see system.h).
+//
+// Solve path (mixed precision, every RHS at once):
+//   r = b - A x            FP64 operator, FP64 vectors, per-RHS norms
+//   e = V(r)               one FP32 V-cycle from e = 0
+//   x += e                 FP64
+// repeated until max_k ||r_k|| / ||b_k|| <= tol.  The V-cycle follows the
+// reference's schedule (IterativeSolvers.inl:1211-1333): on the way down each
+// level relaxes (boundary block solved exactly, then deep texels by colour-run
+// Gauss-Seidel), forms the residual and restricts it; the coarsest level is
+// solved directly; on the way up the correction is prolongated and relaxed
+// again.  The sequence of launches of one refinement step is captured once into
+// a CUDA graph and replayed.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "system.h"
+
+namespace gdtp {
+
+static inline int kp_for(int k) {
+  if (k <= 1) return 1;
+  int kp = 4;
+  while (kp < k) kp *= 2;
+  return kp;
+}
+
+DeepRuns build_deep_runs(const GridLevel& L) {
+  DeepRuns R;
+  R.texel.reserve(L.numDeep);
+  for (int c = 0; c < 4; c++) {
+    R.runStart[c] = (int)R.runs.size();
+    const int ci = c & 1, cj = c >> 1;
+    for (const Line& l : L.rasterLines) {
+      const NodeInfo& n = L.nodes[l.start];
+      if ((n.cj & 1) != cj) continue;
+      const int len = l.end - l.start + 1;
+      const int o = (ci - (n.ci & 1)) & 1;
+      for (int p = o; p < len; p += 64) {
+        dev::ColourRun r;
+        r.pos0 = l.start + p;
+        r.prev0 = l.prev + p;
+        r.next0 = l.next + p;
+        r.coef0 = R.count;
+        r.len = std::min(32, (len - p + 1) / 2);
+        for (int m = 0; m < r.len; m++) R.texel.push_back(l.coeff + p + 2 * m);
+        R.count += r.len;
+        R.runs.push_back(r);
+      }
+    }
+  }
+  R.runStart[4] = (int)R.runs.size();
+  return R;
+}
+
+DeviceSystem::DeviceSystem(const Hierarchy& h, const BoundaryElements& be, int device) : h_(h), be_(be), device_(device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { err_ = "no CUDA device"; return; }
+  if (device < 0 || device >= n) { err_ = "invalid CUDA device"; return; }
+  if (!check(cudaSetDevice(device), "cudaSetDevice")) return;
+  if (!check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate")) return;
+}
+
+DeviceSystem::~DeviceSystem() {
+  cudaSetDevice(device_);
+  if (iterGraph_) cudaGraphExecDestroy(iterGraph_);
+  if (profEv_[0]) { cudaEventDestroy(profEv_[0]); cudaEventDestroy(profEv_[1]); }
+  if (sumsHost_) cudaFreeHost(sumsHost_);
+  mg32_.reset();
+  mg64_.reset();
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void DeviceSystem::invalidate_graph() {
+  cudaSetDevice(device_);
+  if (iterGraph_) cudaGraphExecDestroy(iterGraph_);
+  iterGraph_ = nullptr;
+  iterGraphK_ = -1;
+}
+
+bool DeviceSystem::check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  err_ = std::string(what) + ": " + cudaGetErrorString(e);
+  return false;
+}
+
+size_t DeviceSystem::deviceBytes() const {
+  size_t b = rawArena_.total + workArena_.total;
+  if (mg32_) b += mg32_->arena.total;
+  if (mg64_) b += mg64_->arena.total;
+  return b;
+}
+
+// ----------------------------------------------------------------------------
+// assembly
+// ----------------------------------------------------------------------------
+bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  ChartMetrics g;
+  if (parameterMetric) {
+    g.assign(h_.atlas.charts.size(), {});
+    for (size_t c = 0; c < h_.atlas.charts.size(); c++)
+      for (int t : h_.atlas.charts[c].meshTriangleIndices) {
+        M2 m;
+        m.c[0][0] = parameterMetric[4 * t]; m.c[0][1] = parameterMetric[4 * t + 1];
+        m.c[1][0] = parameterMetric[4 * t + 2]; m.c[1][1] = parameterMetric[4 * t + 3];
+        g[c].push_back(m);
+      }
+  } else if (!embedding_metric(mesh, h_.atlas, g)) {
+    err_ = "degenerate mesh (zero area)";
+    return false;
+  }
+  AssemblyWork w;
+  build_assembly_work(h_, be_, g, w);
+  DeviceArena A;
+  int* cellPtr = A.upload(w.cellPtr);
+  int* cellTri = A.upload(w.cellTri);
+  int* cellIJ = A.upload(w.cellIJ);
+  int* cellChart = A.upload(w.cellChart);
+  double* cellSize = A.upload(w.chartCellSize);
+  double* triPos = A.upload(w.triPos);
+  double* triMetric = A.upload(w.triMetric);
+  double* triInv = A.upload(w.triMetricInv);
+  double* triScale = A.upload(w.triScale);
+  int* deepCells = A.upload(w.deepCells);
+  int* adj = A.upload(w.boundaryAdjacentCells);
+  int* btPtr = A.upload(w.btPtr);
+  int* btTri = A.upload(w.btTri);
+  double* btPos = A.upload(w.btPos);
+  double* cm = A.zeros<double>(16 * size_t(w.numInteriorCells));
+  double* cs = A.zeros<double>(16 * size_t(w.numInteriorCells));
+  const int nd = h_.levels[0].numDeep;
+  double* dm = A.zeros<double>(10 * size_t(nd));
+  double* ds = A.zeros<double>(10 * size_t(nd));
+  const size_t na = w.boundaryAdjacentCells.size();
+  double* am = A.zeros<double>(16 * na);
+  double* as = A.zeros<double>(16 * na);
+  double* bm = A.zeros<double>(36 * size_t(w.numBoundaryTriangles));
+  double* bs = A.zeros<double>(36 * size_t(w.numBoundaryTriangles));
+  if (!check(A.last, "assembly upload")) return false;
+  dev::launch_interior_cells(w.numInteriorCells, cellPtr, cellTri, cellIJ, cellChart, cellSize, triPos, triInv, triScale, cm, cs,
+                             stream_);
+  dev::launch_deep_gather(nd, deepCells, cm, cs, dm, ds, stream_);
+  dev::launch_gather_cells((int)na, adj, cm, am, stream_);
+  dev::launch_gather_cells((int)na, adj, cs, as, stream_);
+  dev::launch_boundary_triangles(w.numBoundaryTriangles, btPtr, btTri, btPos, triPos, triMetric, triInv, bm, bs, stream_);
+  if (!check(cudaGetLastError(), "assembly launch")) return false;
+  fine_ = FineSystem();
+  fine_.deepMass.resize(10 * size_t(nd));
+  fine_.deepStiffness.resize(10 * size_t(nd));
+  std::vector<double> ham(16 * na), has(16 * na), hbm(36 * size_t(w.numBoundaryTriangles)), hbs(hbm.size());
+  bool ok = check(cudaMemcpyAsync(fine_.deepMass.data(), dm, fine_.deepMass.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
+            check(cudaMemcpyAsync(fine_.deepStiffness.data(), ds, fine_.deepStiffness.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
+            check(cudaMemcpyAsync(ham.data(), am, ham.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
+            check(cudaMemcpyAsync(has.data(), as, has.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
+            check(cudaMemcpyAsync(hbm.data(), bm, hbm.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
+            check(cudaMemcpyAsync(hbs.data(), bs, hbs.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
+            check(cudaStreamSynchronize(stream_), "assembly");
+  if (!ok) return false;
+  if (!assemble_boundary_blocks(h_, be_, w, ham, has, hbm, hbs, fine_, err_)) return false;
+
+  // raw FP64 operators of M and S on level 0 (deep planes in colour-run order)
+  runs0_ = build_deep_runs(h_.levels[0]);
+  const GridLevel& L0 = h_.levels[0];
+  auto make_raw = [&](const std::vector<double>& deep, const Csr& bb, const Csr& bd, RawOperator& op) {
+    const int cnt = runs0_.count;
+    std::vector<double> planes(size_t(9) * cnt);
+    for (int i = 0; i < cnt; i++)
+      for (int k = 0; k < 9; k++) planes[size_t(k) * cnt + i] = deep[10 * size_t(runs0_.texel[i]) + k];
+    std::vector<int> ptr(1, 0), col;
+    std::vector<double> val;
+    for (int b = 0; b < L0.numBoundary; b++) {
+      for (int k = bd.ptr[b]; k < bd.ptr[b + 1]; k++) { col.push_back(bd.col[k]); val.push_back(bd.val[k]); }
+      for (int k = bb.ptr[b]; k < bb.ptr[b + 1]; k++) { col.push_back(L0.boundaryGlobal[bb.col[k]]); val.push_back(bb.val[k]); }
+      ptr.push_back((int)col.size());
+    }
+    op.runs = rawArena_.upload(runs0_.runs);
+    op.nRuns = (int)runs0_.runs.size();
+    op.coef = rawArena_.upload(planes);
+    op.planeStride = cnt;
+    op.bPtr = rawArena_.upload(ptr);
+    op.bCol = rawArena_.upload(col);
+    op.bVal = rawArena_.upload(val);
+    op.bGlobal = rawArena_.upload(L0.boundaryGlobal);
+    op.nB = L0.numBoundary;
+  };
+  make_raw(fine_.deepMass, fine_.bbMass, fine_.bdMass, rawM_);
+  make_raw(fine_.deepStiffness, fine_.bbStiffness, fine_.bdStiffness, rawS_);
+  return check(rawArena_.last, "operator upload");
+}
+
+// ----------------------------------------------------------------------------
+// coefficient hierarchy + device multigrid
+// ----------------------------------------------------------------------------
+bool DeviceSystem::update(double stiffness, double screen) {
+  if (!err_.empty()) return false;
+  if (fine_.deepMass.empty() && h_.levels[0].numDeep > 0) { err_ = "update before assembly"; return false; }
+  cudaSetDevice(device_);
+  const GridLevel& L0 = h_.levels[0];
+  std::vector<double> deep(fine_.deepMass.size());
+  for (size_t i = 0; i < deep.size(); i++) deep[i] = screen * fine_.deepMass[i] + stiffness * fine_.deepStiffness[i];
+  Csr bb = csr_axpby(screen, fine_.bbMass, stiffness, fine_.bbStiffness);
+  Csr bd = csr_axpby(screen, fine_.bdMass, stiffness, fine_.bdStiffness);
+  bd.cols = L0.numTexels;
+  // levels used: stop once the coarsest fits the dense direct solve
+  int L = (int)h_.levels.size();
+  for (int l = 0; l < (int)h_.levels.size(); l++)
+    if (h_.levels[l].numTexels <= knobs.maxCoarse) { L = l + 1; break; }
+  if (h_.levels[L - 1].numTexels > 12000) { err_ = "coarsest level too large for the dense direct solve; build more levels"; return false; }
+  std::vector<LevelCoefficients> co;
+  if (!galerkin_hierarchy(h_, L, deep, bb, bd, co, err_)) return false;
+  coeffs_ = std::move(co);
+  levelsUsed_ = L;
+  stiffness_ = stiffness;
+  screen_ = screen;
+  // raw FP64 A on level 0
+  {
+    const int cnt = runs0_.count;
+    std::vector<double> planes(size_t(9) * cnt);
+    for (int i = 0; i < cnt; i++)
+      for (int k = 0; k < 9; k++) planes[size_t(k) * cnt + i] = deep[10 * size_t(runs0_.texel[i]) + k];
+    std::vector<int> ptr(1, 0), col;
+    std::vector<double> val;
+    for (int b = 0; b < L0.numBoundary; b++) {
+      for (int k = bd.ptr[b]; k < bd.ptr[b + 1]; k++) { col.push_back(bd.col[k]); val.push_back(bd.val[k]); }
+      for (int k = bb.ptr[b]; k < bb.ptr[b + 1]; k++) { col.push_back(L0.boundaryGlobal[bb.col[k]]); val.push_back(bb.val[k]); }
+      ptr.push_back((int)col.size());
+    }
+    rawA_ = RawOperator();
+    rawA_.runs = rawM_.runs;
+    rawA_.nRuns = rawM_.nRuns;
+    rawA_.coef = rawArena_.upload(planes);
+    rawA_.planeStride = cnt;
+    rawA_.bPtr = rawArena_.upload(ptr);
+    rawA_.bCol = rawArena_.upload(col);
+    rawA_.bVal = rawArena_.upload(val);
+    rawA_.bGlobal = rawM_.bGlobal;
+    rawA_.nB = L0.numBoundary;
+    if (!check(rawArena_.last, "operator upload")) return false;
+  }
+  mg32_.reset();
+  mg64_.reset();
+  if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; iterGraphK_ = -1; }
+  updated_ = true;
+  return true;
+}
+
+template <typename T>
+bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
+  const int L = levelsUsed_;
+  DeviceArena& A = mg.arena;
+  mg.levels.assign(L, LevelDev<T>());
+  mg.KP = KP;
+  int maxBlockAll = 0;
+  for (int l = 0; l < L; l++) {
+    const GridLevel& G = h_.levels[l];
+    const LevelCoefficients& C = coeffs_[l];
+    LevelDev<T>& D = mg.levels[l];
+    D.n = G.numTexels;
+    D.nDeep = G.numDeep;
+    D.nB = G.numBoundary;
+    D.x = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
+    D.b = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
+    D.r = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
+    if (l == L - 1) {
+      // coarsest: scaled dense inverse (FP64)
+      Csr full;
+      full_matrix(G, C, full);
+      const int n = G.numTexels;
+      std::vector<double> dense(size_t(n) * n, 0.0), scale(n);
+      for (int i = 0; i < n; i++)
+        for (int k = full.ptr[i]; k < full.ptr[i + 1]; k++)
+          if (full.col[k] == i) scale[i] = 1.0 / std::sqrt(full.val[k]);
+      for (int i = 0; i < n; i++)
+        for (int k = full.ptr[i]; k < full.ptr[i + 1]; k++) dense[size_t(i) * n + full.col[k]] = full.val[k] * scale[i] * scale[full.col[k]];
+      if (!dense_spd_inverse(dense.data(), n, true)) { err_ = "coarsest operator is not positive definite"; return false; }
+      mg.coarseN = n;
+      mg.coarseInv = A.upload(dense);
+      mg.coarseScale = A.upload(scale);
+      continue;
+    }
+    // deep runs + reciprocal coefficient planes
+    DeepRuns R = build_deep_runs(G);
+    std::vector<T> planes(size_t(10) * std::max(1, R.count));
+    for (int i = 0; i < R.count; i++) {
+      const double* c = &C.deep[10 * size_t(R.texel[i])];
+      const double c4 = c[4], inv = 1.0 / c4;
+      for (int k = 0; k < 9; k++) planes[size_t(k) * R.count + i] = T(k == 4 ? inv : c[k] * inv);
+      planes[size_t(9) * R.count + i] = T(c4);
+    }
+    D.runs = A.upload(R.runs);
+    D.nRuns = (int)R.runs.size();
+    std::copy(R.runStart, R.runStart + 5, D.runStart);
+    D.coef = A.upload(planes);
+    D.planeStride = R.count;
+    // boundary rows (merged BD + BB, global columns)
+    {
+      std::vector<int> ptr(1, 0), col;
+      std::vector<T> val;
+      for (int b = 0; b < G.numBoundary; b++) {
+        for (int k = C.bd.ptr[b]; k < C.bd.ptr[b + 1]; k++) { col.push_back(C.bd.col[k]); val.push_back(T(C.bd.val[k])); }
+        for (int k = C.bb.ptr[b]; k < C.bb.ptr[b + 1]; k++) { col.push_back(G.boundaryGlobal[C.bb.col[k]]); val.push_back(T(C.bb.val[k])); }
+        ptr.push_back((int)col.size());
+      }
+      D.bPtr = A.upload(ptr);
+      D.bCol = A.upload(col);
+      D.bVal = A.upload(val);
+      D.bGlobal = A.upload(G.boundaryGlobal);
+    }
+    // exact boundary solver
+    {
+      BoundarySolverSetup bs;
+      if (!build_boundary_solver(C.bb, C.bd, knobs.maxBlock, bs, err_)) { err_ = "level " + std::to_string(l) + ": " + err_; return false; }
+      dev::BoundaryDev<T>& B = D.B;
+      B.nb = bs.nb;
+      B.nSub = bs.nSub;
+      B.nI = bs.nI;
+      B.nS = bs.nS;
+      int mb = 0;
+      for (int p = 0; p < bs.nSub; p++) mb = std::max(mb, bs.subPtr[p + 1] - bs.subPtr[p]);
+      B.maxBlock = mb;
+      maxBlockAll = std::max(maxBlockAll, mb);
+      std::vector<long long> off(bs.invOff.begin(), bs.invOff.end());
+      std::vector<T> inv(bs.inv.begin(), bs.inv.end()), scale(bs.scale.begin(), bs.scale.end()), sinv(bs.Sinv.begin(), bs.Sinv.end());
+      std::vector<int> pg(bs.nb);
+      for (int k = 0; k < bs.nb; k++) pg[k] = G.boundaryGlobal[bs.order[k]];
+      auto upT = [&](const std::vector<double>& v) { std::vector<T> t(v.begin(), v.end()); return (const T*)A.upload(t); };
+      B.subPtr = A.upload(bs.subPtr);
+      B.invOff = A.upload(off);
+      B.inv = A.upload(inv);
+      B.posGlobal = A.upload(pg);
+      B.scale = A.upload(scale);
+      B.bdPtr = A.upload(bs.BD.ptr);
+      B.bdCol = A.upload(bs.BD.col);
+      B.bdVal = upT(bs.BD.val);
+      B.aisPtr = A.upload(bs.AIS.ptr);
+      B.aisCol = A.upload(bs.AIS.col);
+      B.aisVal = upT(bs.AIS.val);
+      B.asiPtr = A.upload(bs.ASI.ptr);
+      B.asiCol = A.upload(bs.ASI.col);
+      B.asiVal = upT(bs.ASI.val);
+      B.sinv = A.upload(sinv);
+      B.y = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nI)) * KP * sizeof(T)));
+      B.t = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * KP * sizeof(T)));
+      B.xs = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * KP * sizeof(T)));
+    }
+    // transfers to / from level l+1
+    {
+      const GridLevel& Cg = h_.levels[l + 1];
+      std::vector<dev::RestrictRun> rr;
+      for (const Line& ln : Cg.restrictionLines) {
+        const int len = (ln.end - ln.start) / 2 + 1;
+        for (int p = 0; p < len; p += 32) rr.push_back({ln.coeff + p, ln.start + 2 * p, ln.prev + 2 * p, ln.next + 2 * p, std::min(32, len - p)});
+      }
+      D.rruns = A.upload(rr);
+      D.nRRuns = (int)rr.size();
+      const Csr& Rb = G.boundaryRestriction;
+      std::vector<T> rv(Rb.val.begin(), Rb.val.end());
+      D.rbPtr = A.upload(Rb.ptr);
+      D.rbCol = A.upload(Rb.col);
+      D.rbVal = A.upload(rv);
+      D.rbOut = A.upload(Cg.boundaryGlobal);
+      D.nRB = Rb.rows;
+      std::vector<dev::ProlongRun> pr;
+      for (const ProlongationLine& pl : G.prolongationLines)
+        for (int p = 0; p < pl.length; p += 32)
+          pr.push_back({pl.start + p, p, std::min(32, pl.length - p), pl.center, pl.prev, pl.next, pl.aligned});
+      D.pruns = A.upload(pr);
+      D.nPRuns = (int)pr.size();
+    }
+  }
+  if (!check(A.last, "multigrid upload")) return false;
+  // dynamic shared memory of the boundary subdomain kernels
+  const size_t smem = size_t(maxBlockAll) * KP * sizeof(T);
+  if (smem > 220 * 1024) { err_ = "boundary subdomain too large for shared memory at this RHS count"; return false; }
+  if (KP == 1) return check(dev::configure_boundary_smem<T, 1>(smem), "boundary smem");
+  return check(dev::configure_boundary_smem<T, 4>(smem), "boundary smem");
+}
+
+template bool DeviceSystem::build_multigrid<float>(Multigrid<float>&, int);
+template bool DeviceSystem::build_multigrid<double>(Multigrid<double>&, int);
+
+// ----------------------------------------------------------------------------
+// V-cycle
+// ----------------------------------------------------------------------------
+template <typename T, int W>
+void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
+  const int L = (int)mg.levels.size();
+  const int KP = mg.KP;
+  for (int l = 0; l + 1 < L; l++) {
+    LevelDev<T>& D = mg.levels[l];
+    LevelDev<T>& C = mg.levels[l + 1];
+    if (l > 0) cudaMemsetAsync(D.x, 0, size_t(D.n) * KP * sizeof(T), s);
+    dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
+    for (int sw = 0; sw < knobs.preSweeps; sw++) {
+      const bool prof = profiling_ && l == 0 && sw == 0;
+      if (prof) cudaEventRecord(profEv_[0], s);
+      for (int c = 0; c < 4; c++)
+        dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
+      if (prof) cudaEventRecord(profEv_[1], s);
+    }
+    dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
+    dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, D.r, C.b, KP, s);
+  }
+  dev::launch_coarse_solve<T, W>(mg.coarseN, mg.coarseInv, mg.coarseScale, mg.levels[L - 1].b, mg.levels[L - 1].x, KP, s);
+  for (int l = L - 2; l >= 0; l--) {
+    LevelDev<T>& D = mg.levels[l];
+    dev::launch_prolong_add<T, W>(D.pruns, D.nPRuns, mg.levels[l + 1].x, D.x, KP, s);
+    dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
+    for (int sw = 0; sw < knobs.postSweeps; sw++)
+      for (int c = 3; c >= 0; c--)
+        dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
+  }
+}
+
+template void DeviceSystem::vcycle<float, 1>(Multigrid<float>&, cudaStream_t);
+template void DeviceSystem::vcycle<float, 4>(Multigrid<float>&, cudaStream_t);
+template void DeviceSystem::vcycle<double, 1>(Multigrid<double>&, cudaStream_t);
+template void DeviceSystem::vcycle<double, 4>(Multigrid<double>&, cudaStream_t);
+
+// ----------------------------------------------------------------------------
+// solve work and drivers
+// ----------------------------------------------------------------------------
+bool DeviceSystem::ensure_work(int k) {
+  if (k <= workK_) return true;
+  workArena_ = DeviceArena();
+  const size_t n = h_.levels[0].numTexels;
+  b64_ = workArena_.zeros<double>(n * k);
+  x64_ = workArena_.zeros<double>(n * k);
+  r64_ = workArena_.zeros<double>(n * k);
+  const int blocks = dev::raw_operator_blocks(rawM_.nRuns, h_.levels[0].numBoundary, k);
+  partials_ = workArena_.zeros<double>(size_t(blocks) * 2 * k);
+  sums_ = workArena_.zeros<double>(2 * size_t(k));
+  if (sumsHost_) cudaFreeHost(sumsHost_);
+  if (!check(cudaMallocHost(&sumsHost_, 2 * size_t(k) * sizeof(double)), "cudaMallocHost")) return false;
+  if (!check(workArena_.last, "work allocation")) return false;
+  workK_ = k;
+  if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; iterGraphK_ = -1; }
+  return true;
+}
+
+bool DeviceSystem::raw_apply_dev(const RawOperator& op, const double* b, const double* x, double* out, int k, int mode,
+                                 cudaStream_t s, double* sumsHost) {
+  dev::launch_raw_operator(op.runs, op.nRuns, op.coef, op.planeStride, op.bPtr, op.bCol, op.bVal, op.bGlobal, op.nB, b, x, out, k,
+                           mode, partials_, sums_, s);
+  if (!sumsHost) return check(cudaGetLastError(), "raw operator");
+  return check(cudaMemcpyAsync(sumsHost, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") &&
+         check(cudaStreamSynchronize(s), "raw operator");
+}
+
+bool DeviceSystem::apply(int which, const double* x, double* y, int k) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
+  const RawOperator* op = which == 1 ? &rawM_ : which == 2 ? &rawS_ : &rawA_;
+  if (which == 0 && !updated_) { err_ = "apply(A) before update"; return false; }
+  if (!ensure_work(k)) return false;
+  const size_t n = h_.levels[0].numTexels;
+  return check(cudaMemcpyAsync(x64_, x, n * k * 8, cudaMemcpyHostToDevice, stream_), "h2d") &&
+         raw_apply_dev(*op, nullptr, x64_, r64_, k, 1, stream_, nullptr) &&
+         check(cudaMemcpyAsync(y, r64_, n * k * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
+         check(cudaStreamSynchronize(stream_), "apply");
+}
+
+bool DeviceSystem::residual_host(const double* b, const double* x, int k, double* rel) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (!updated_) { err_ = "residual before update"; return false; }
+  if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
+  if (!ensure_work(k)) return false;
+  const size_t n = h_.levels[0].numTexels;
+  if (!check(cudaMemcpyAsync(b64_, b, n * k * 8, cudaMemcpyHostToDevice, stream_), "h2d") ||
+      !check(cudaMemcpyAsync(x64_, x, n * k * 8, cudaMemcpyHostToDevice, stream_), "h2d") ||
+      !raw_apply_dev(rawA_, b64_, x64_, r64_, k, 0, stream_, sumsHost_))
+    return false;
+  for (int c = 0; c < k; c++) rel[c] = std::sqrt(sumsHost_[c] / std::max(sumsHost_[k + c], 1e-300));
+  return true;
+}
+
+bool DeviceSystem::vcycle_host(float* x, const float* rhs, int k) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (!updated_) { err_ = "vcycle before update"; return false; }
+  if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
+  const int KP = kp_for(k);
+  if (!mg32_ || mg32_->KP < KP) {
+    mg32_.reset(new Multigrid<float>());
+    if (!build_multigrid(*mg32_, KP)) return false;
+  }
+  Multigrid<float>& mg = *mg32_;
+  const size_t n = h_.levels[0].numTexels;
+  std::vector<float> px(n * mg.KP, 0.f), pb(n * mg.KP, 0.f);
+  for (size_t i = 0; i < n; i++)
+    for (int c = 0; c < k; c++) { px[i * mg.KP + c] = x[i * k + c]; pb[i * mg.KP + c] = rhs[i * k + c]; }
+  LevelDev<float>& D0 = mg.levels[0];
+  if (!check(cudaMemcpyAsync(D0.x, px.data(), px.size() * 4, cudaMemcpyHostToDevice, stream_), "h2d") ||
+      !check(cudaMemcpyAsync(D0.b, pb.data(), pb.size() * 4, cudaMemcpyHostToDevice, stream_), "h2d"))
+    return false;
+  if (mg.KP == 1) vcycle<float, 1>(mg, stream_); else vcycle<float, 4>(mg, stream_);
+  if (!check(cudaGetLastError(), "vcycle") ||
+      !check(cudaMemcpyAsync(px.data(), D0.x, px.size() * 4, cudaMemcpyDeviceToHost, stream_), "d2h") ||
+      !check(cudaStreamSynchronize(stream_), "vcycle"))
+    return false;
+  for (size_t i = 0; i < n; i++)
+    for (int c = 0; c < k; c++) x[i * k + c] = px[i * mg.KP + c];
+  return true;
+}
+
+bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const double* b_dev, double* x_dev, int k, double tol,
+                               int maxIters, cudaStream_t userStream, SolveReport& rep) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (!updated_) { err_ = "solve before update"; return false; }
+  if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
+  const int KP = kp_for(k);
+  if (!mg32_ || mg32_->KP < KP) {
+    mg32_.reset(new Multigrid<float>());
+    if (!build_multigrid(*mg32_, KP)) return false;
+    if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; iterGraphK_ = -1; }
+  }
+  if (!ensure_work(k)) return false;
+  Multigrid<float>& mg = *mg32_;
+  const size_t n = h_.levels[0].numTexels;
+  cudaStream_t s = stream_;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  if (userStream) {
+    cudaEventRecord(e0, userStream);
+    cudaStreamWaitEvent(s, e0, 0);
+  }
+  cudaEventRecord(e0, s);
+  const double* B = b_dev ? b_dev : b64_;
+  double* X = x_dev ? x_dev : x64_;
+  if (b_host && !check(cudaMemcpyAsync(b64_, b_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d b")) return false;
+  if (x_host && !check(cudaMemcpyAsync(x64_, x_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d x")) return false;
+  // refinement step graph: rhs <- r, e <- V(rhs), x += e, r <- b - A x (+ norms)
+  if (!iterGraph_ || iterGraphK_ != k || iterGraphB_ != B || iterGraphX_ != X) {
+    if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; }
+    cudaGraph_t g;
+    if (!profEv_[0]) {
+      cudaEventCreate(&profEv_[0]);
+      cudaEventCreate(&profEv_[1]);
+    }
+    profiling_ = true;
+    if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
+    LevelDev<float>& D0 = mg.levels[0];
+    dev::launch_pack_rhs<float>(r64_, D0.b, (long long)n, k, mg.KP, s);
+    cudaMemsetAsync(D0.x, 0, n * mg.KP * sizeof(float), s);
+    if (mg.KP == 1) vcycle<float, 1>(mg, s); else vcycle<float, 4>(mg, s);
+    dev::launch_add_correction<float>(X, D0.x, (long long)n, k, mg.KP, s);
+    dev::launch_raw_operator(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
+                             rawA_.bGlobal, rawA_.nB, B, X, r64_, k, 0, partials_, sums_, s);
+    profiling_ = false;
+    if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
+    {
+      size_t nn = 0;
+      cudaGraphGetNodes(g, nullptr, &nn);
+      std::vector<cudaGraphNode_t> nodes(nn);
+      cudaGraphGetNodes(g, nodes.data(), &nn);
+      graphKernels = 0;
+      for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(nd, &t);
+        if (t == cudaGraphNodeTypeKernel) graphKernels++;
+      }
+    }
+    if (!check(cudaGraphInstantiate(&iterGraph_, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
+    cudaGraphDestroy(g);
+    iterGraphK_ = k;
+    iterGraphB_ = B;
+    iterGraphX_ = X;
+  }
+  // initial residual
+  if (!raw_apply_dev(rawA_, B, X, r64_, k, 0, s, sumsHost_)) return false;
+  rep = SolveReport();
+  rep.rel.assign(k, 0.0);
+  auto rel_max = [&]() {
+    double m = 0;
+    for (int c = 0; c < k; c++) {
+      rep.rel[c] = std::sqrt(sumsHost_[c] / std::max(sumsHost_[k + c], 1e-300));
+      m = std::max(m, rep.rel[c]);
+    }
+    return m;
+  };
+  double rm = rel_max();
+  int it = 0;
+  while (rm > tol && it < maxIters) {
+    if (!check(cudaGraphLaunch(iterGraph_, s), "graph launch") ||
+        !check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
+        !check(cudaStreamSynchronize(s), "refinement step"))
+      return false;
+    it++;
+    rm = rel_max();
+    float pm = 0;
+    if (cudaEventElapsedTime(&pm, profEv_[0], profEv_[1]) == cudaSuccess) {
+      profCount += 1;
+      profMs += pm;
+      profTexels = mg.levels[0].nDeep;
+    }
+  }
+  if (x_host && !check(cudaMemcpyAsync(x_host, x64_, n * k * 8, cudaMemcpyDeviceToHost, s), "d2h x")) return false;
+  cudaEventRecord(e1, s);
+  if (userStream) cudaStreamWaitEvent(userStream, e1, 0);
+  if (!check(cudaEventSynchronize(e1), "solve")) return false;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  rep.iterations = it;
+  rep.vcycles = it;
+  rep.relMax = rm;
+  rep.seconds = ms * 1e-3;
+  return true;
+}
+
+bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, int k, double tol, int maxIters, SolveReport& rep) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (!updated_) { err_ = "solve before update"; return false; }
+  if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
+  const int KP = kp_for(k);
+  if (!mg64_ || mg64_->KP < KP) {
+    mg64_.reset(new Multigrid<double>());
+    if (!build_multigrid(*mg64_, KP)) return false;
+  }
+  if (!ensure_work(k)) return false;
+  Multigrid<double>& mg = *mg64_;
+  const size_t n = h_.levels[0].numTexels;
+  cudaStream_t s = stream_;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, s);
+  if (!check(cudaMemcpyAsync(b64_, b_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d b") ||
+      !check(cudaMemcpyAsync(x64_, x_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d x") ||
+      !raw_apply_dev(rawA_, b64_, x64_, r64_, k, 0, s, sumsHost_))
+    return false;
+  rep = SolveReport();
+  rep.rel.assign(k, 0.0);
+  auto rel_max = [&]() {
+    double m = 0;
+    for (int c = 0; c < k; c++) {
+      rep.rel[c] = std::sqrt(sumsHost_[c] / std::max(sumsHost_[k + c], 1e-300));
+      m = std::max(m, rep.rel[c]);
+    }
+    return m;
+  };
+  double rm = rel_max();
+  int it = 0;
+  LevelDev<double>& D0 = mg.levels[0];
+  while (rm > tol && it < maxIters) {
+    dev::launch_pack_rhs<double>(r64_, D0.b, (long long)n, k, mg.KP, s);
+    cudaMemsetAsync(D0.x, 0, n * mg.KP * sizeof(double), s);
+    if (mg.KP == 1) vcycle<double, 1>(mg, s); else vcycle<double, 4>(mg, s);
+    dev::launch_add_correction<double>(x64_, D0.x, (long long)n, k, mg.KP, s);
+    if (!raw_apply_dev(rawA_, b64_, x64_, r64_, k, 0, s, sumsHost_)) return false;
+    it++;
+    rm = rel_max();
+  }
+  if (!check(cudaMemcpyAsync(x_host, x64_, n * k * 8, cudaMemcpyDeviceToHost, s), "d2h x")) return false;
+  cudaEventRecord(e1, s);
+  if (!check(cudaEventSynchronize(e1), "solve")) return false;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  rep.iterations = it;
+  rep.vcycles = it;
+  rep.relMax = rm;
+  rep.seconds = ms * 1e-3;
+  return true;
+}
+
+}  // namespace gdtp

@@ -1,0 +1,194 @@
+// Device-resident texel-FEM system: FP64 operators, multigrid levels (FP32 for
+// the mixed-precision path, FP64 for the plain comparator), exact boundary
+// solvers, coarsest dense inverse, and the solve drivers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels/vcycle.cuh"
+#include "kernels/vcycle_kernels.h"
+#include "setup/setup.h"
+
+namespace gdtp {
+
+// Owning device allocation.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept { std::swap(p, o.p); std::swap(bytes, o.bytes); return *this; }
+  ~DevBuf() { if (p) cudaFree(p); }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct DeviceArena {
+  std::vector<DevBuf> bufs;
+  size_t total = 0;
+  cudaError_t last = cudaSuccess;
+  void* alloc(size_t bytes) {
+    DevBuf b;
+    if (bytes == 0) bytes = 16;
+    last = cudaMalloc(&b.p, bytes);
+    if (last != cudaSuccess) return nullptr;
+    b.bytes = bytes;
+    total += bytes;
+    void* p = b.p;
+    bufs.push_back(std::move(b));
+    return p;
+  }
+  template <class T> T* upload(const std::vector<T>& v) {
+    T* p = static_cast<T*>(alloc(v.size() * sizeof(T)));
+    if (p && !v.empty()) last = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return p;
+  }
+  template <class T> T* zeros(size_t n) {
+    T* p = static_cast<T*>(alloc(n * sizeof(T)));
+    if (p) last = cudaMemset(p, 0, n * sizeof(T));
+    return p;
+  }
+};
+
+// Colour runs and raw FP64 stencil planes of one level's deep texels.
+struct DeepRuns {
+  std::vector<dev::ColourRun> runs;
+  int runStart[5] = {0, 0, 0, 0, 0};
+  std::vector<int> texel;       // run texel -> deep index (plane order)
+  int count = 0;                // run texels = deep texels
+};
+DeepRuns build_deep_runs(const GridLevel& L);
+
+// One multigrid level on the device, value type T.
+template <typename T>
+struct LevelDev {
+  int n = 0, nDeep = 0, nB = 0;
+  const dev::ColourRun* runs = nullptr;
+  int nRuns = 0, runStart[5] = {0, 0, 0, 0, 0};
+  const T* coef = nullptr;      // 10 planes, reciprocal form
+  int planeStride = 0;
+  const int *bPtr = nullptr, *bCol = nullptr, *bGlobal = nullptr;
+  const T* bVal = nullptr;      // boundary rows: BD + BB with global columns
+  dev::BoundaryDev<T> B;
+  const dev::RestrictRun* rruns = nullptr;  // to the next level
+  int nRRuns = 0;
+  const int *rbPtr = nullptr, *rbCol = nullptr, *rbOut = nullptr;
+  const T* rbVal = nullptr;
+  int nRB = 0;
+  const dev::ProlongRun* pruns = nullptr;   // from the next level
+  int nPRuns = 0;
+  T *x = nullptr, *b = nullptr, *r = nullptr;
+};
+
+template <typename T>
+struct Multigrid {
+  std::vector<LevelDev<T>> levels;
+  int coarseN = 0;
+  const double* coarseInv = nullptr;    // scaled dense inverse of the coarsest operator
+  const double* coarseScale = nullptr;
+  int KP = 0;                           // channel stride the vectors were sized for
+  DeviceArena arena;
+};
+
+// Raw FP64 operator on level 0 (no reciprocals): y = A x.
+struct RawOperator {
+  const dev::ColourRun* runs = nullptr;
+  int nRuns = 0;
+  const double* coef = nullptr;         // 9 planes used
+  int planeStride = 0;
+  const int *bPtr = nullptr, *bCol = nullptr, *bGlobal = nullptr;
+  const double* bVal = nullptr;
+  int nB = 0;
+};
+
+struct SolverKnobs {
+  int preSweeps = 2, postSweeps = 2;
+  int maxBlock = 384;                   // boundary subdomain size
+  int maxCoarse = 2600;                 // coarsest level size limit (texels)
+};
+
+struct SolveReport {
+  int iterations = 0, vcycles = 0;
+  double relMax = 0, seconds = 0;
+  std::vector<double> rel;
+};
+
+class DeviceSystem {
+ public:
+  DeviceSystem(const Hierarchy& h, const BoundaryElements& be, int device);
+  ~DeviceSystem();
+  int device() const { return device_; }
+  bool ok() const { return err_.empty(); }
+  const std::string& error() const { return err_; }
+
+  // assembly (FP64 on device) -> fine M and S
+  bool assemble(const Mesh& mesh, const double* parameterMetric);
+  const FineSystem& fine() const { return fine_; }
+
+  // A = screen*M + stiffness*S, Galerkin hierarchy, boundary solvers, coarse inverse
+  bool update(double stiffness, double screen);
+  const std::vector<LevelCoefficients>& coefficients() const { return coeffs_; }
+  int levelsUsed() const { return levelsUsed_; }
+
+  // host in/out, k right-hand sides (tight n x k)
+  bool apply(int which, const double* x, double* y, int k);
+  bool solve_mixed(const double* b_host, double* x_host, const double* b_dev, double* x_dev, int k, double tol, int maxIters,
+                   cudaStream_t userStream, SolveReport& rep);
+  bool solve_fp64(const double* b_host, double* x_host, int k, double tol, int maxIters, SolveReport& rep);
+  bool vcycle_host(float* x, const float* rhs, int k);
+  bool residual_host(const double* b, const double* x, int k, double* rel);
+
+  SolverKnobs knobs;
+  size_t deviceBytes() const;
+  // knobs that change the launch sequence take effect on the next solve
+  void invalidate_graph();
+  // live timing of the level-0 pre-smoothing colour passes inside the captured
+  // refinement graph: {launch groups timed, total ms, texels updated per group}
+  double profCount = 0, profMs = 0, profTexels = 0;
+  int graphKernels = 0;         // kernel nodes in the refinement-step graph
+
+ private:
+  template <typename T>
+  bool build_multigrid(Multigrid<T>& mg, int KP);
+  template <typename T, int W>
+  void vcycle(Multigrid<T>& mg, cudaStream_t s);
+  bool ensure_work(int k);
+  bool raw_apply_dev(const RawOperator& op, const double* b, const double* x, double* out, int k, int mode, cudaStream_t s,
+                     double* sumsHost);
+  bool check(cudaError_t e, const char* what);
+
+  const Hierarchy& h_;
+  const BoundaryElements& be_;
+  int device_ = 0;
+  std::string err_;
+  cudaStream_t stream_ = nullptr;
+  FineSystem fine_;
+  std::vector<LevelCoefficients> coeffs_;
+  int levelsUsed_ = 0;
+  double stiffness_ = 0, screen_ = 0;
+  bool updated_ = false;
+  bool profiling_ = false;
+
+  DeviceArena rawArena_;
+  RawOperator rawM_, rawS_, rawA_;
+  DeepRuns runs0_;
+
+  std::unique_ptr<Multigrid<float>> mg32_;
+  std::unique_ptr<Multigrid<double>> mg64_;
+
+  // solve work (tight n x k FP64)
+  DeviceArena workArena_;
+  int workK_ = 0;
+  double *b64_ = nullptr, *x64_ = nullptr, *r64_ = nullptr, *partials_ = nullptr, *sums_ = nullptr;
+  double* sumsHost_ = nullptr;  // pinned
+  cudaGraphExec_t iterGraph_ = nullptr;
+  cudaEvent_t profEv_[2] = {nullptr, nullptr};
+  int iterGraphK_ = -1;
+  const double *iterGraphB_ = nullptr, *iterGraphX_ = nullptr;
+};
+
+}  // namespace gdtp

@@ -1,0 +1,153 @@
+"""Host mirror of the reference's system-level interface for the solve path.
+
+The names follow the reference so callers read the same:
+
+* ``InitializeMassAndStiffness(hierarchy)``  -> ``System`` (FP64 assembly on the
+  device; ``include/Src/MassAndStiffness.h:490``), metric from
+  ``InitializeMetric`` (``include/Src/Metric.inl:448``) unless one is given.
+* ``UpdateLinearSystem(stiffness, screen, system)``
+  (``include/Src/UpdateCoefficients.inl:463``).
+* ``MultiplyBySystemMatrix_NoReciprocals(system, x, which)``
+  (``include/Src/IterativeSolvers.inl:881``).
+* ``VCycle(system, x, rhs)`` (``include/Src/IterativeSolvers.inl:1211``).
+* ``solve(system, b, x0, tol)``: mixed-precision solve (FP32 V-cycles inside FP64
+  refinement), the device replacement for the app's loop of V-cycles.
+
+All work runs in ``libgdtp.so``; every call raises ``GDTPError`` on failure
+(no CUDA device included).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .hierarchy import Hierarchy
+
+MASS, STIFFNESS, SYSTEM = 1, 2, 0
+
+
+class System:
+    def __init__(self, hierarchy: Hierarchy, device: int = 0, parameter_metric: np.ndarray | None = None,
+                 vertices: np.ndarray | None = None):
+        self.hierarchy = hierarchy  # keeps the hierarchy alive for the system's lifetime
+        self.n = hierarchy.counts(0)["numTexels"]
+        pm = None if parameter_metric is None else np.ascontiguousarray(parameter_metric, dtype=np.float64)
+        vv = None if vertices is None else np.ascontiguousarray(vertices, dtype=np.float64)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().gdtp_system_create(hierarchy.handle, int(device), 0 if pm is None else 1, _lib.ptr(pm),
+                                                 _lib.ptr(vv), 0 if vv is None else len(vv), C.byref(h)))
+        self._s = h
+
+    def __del__(self):
+        s, self._s = getattr(self, "_s", None), None
+        if s:
+            _lib.lib().gdtp_system_free(s)
+
+    @property
+    def handle(self):
+        return self._s
+
+    # -- set-up -----------------------------------------------------------------
+    def update(self, stiffness_weight: float, screen_weight: float = 1.0) -> None:
+        _lib.check(_lib.lib().gdtp_system_update(self._s, float(stiffness_weight), float(screen_weight)))
+
+    def set(self, knob: str, value: float) -> None:
+        _lib.check(_lib.lib().gdtp_system_set(self._s, knob.encode(), float(value)))
+
+    def device_bytes(self) -> int:
+        b = C.c_int64()
+        _lib.check(_lib.lib().gdtp_system_device_bytes(self._s, C.byref(b)))
+        return b.value
+
+    def array(self, name: str, level: int = 0) -> np.ndarray:
+        L = _lib.lib()
+        n = C.c_int64()
+        _lib.check(L.gdtp_system_array(self._s, name.encode(), level, None, C.byref(n)))
+        if name in ("levelsUsed",) or name.endswith((".ptr", ".col")):
+            out = np.empty(n.value, dtype=np.int32)
+        else:
+            out = np.empty(n.value, dtype=np.float64)
+        _lib.check(L.gdtp_system_array(self._s, name.encode(), level, _lib.ptr(out), C.byref(n)))
+        if name in ("deepMass", "deepStiffness", "coef.deep"):
+            return out.reshape(-1, 10)
+        return out
+
+    def csr(self, name: str, level: int = 0, shape=None):
+        import scipy.sparse as sp
+        ptr, col, val = (self.array(f"{name}.{p}", level) for p in ("ptr", "col", "val"))
+        ncol = shape[1] if shape else (int(col.max()) + 1 if len(col) else 0)
+        return sp.csr_matrix((val, col, ptr), shape=(len(ptr) - 1, ncol))
+
+    @property
+    def levels_used(self) -> int:
+        return int(self.array("levelsUsed")[0])
+
+    # -- operators and solves -----------------------------------------------------
+    def _vec(self, a: np.ndarray, dtype) -> tuple[np.ndarray, int]:
+        a = np.ascontiguousarray(a, dtype=dtype)
+        if a.ndim == 1:
+            a = a[:, None]
+        if a.shape[0] != self.n:
+            raise ValueError(f"vector has {a.shape[0]} texels, system has {self.n}")
+        return a, a.shape[1]
+
+    def apply(self, x: np.ndarray, which: int = SYSTEM) -> np.ndarray:
+        x, k = self._vec(x, np.float64)
+        y = np.empty_like(x)
+        _lib.check(_lib.lib().gdtp_apply(self._s, int(which), _lib.ptr(x), _lib.ptr(y), k))
+        return y
+
+    def vcycle(self, x: np.ndarray, rhs: np.ndarray) -> np.ndarray:
+        x, k = self._vec(x, np.float32)
+        x = x.copy()
+        rhs, _ = self._vec(rhs, np.float32)
+        _lib.check(_lib.lib().gdtp_vcycle(self._s, _lib.ptr(x), _lib.ptr(rhs), k))
+        return x
+
+    def residual(self, b: np.ndarray, x: np.ndarray) -> np.ndarray:
+        b, k = self._vec(b, np.float64)
+        x, _ = self._vec(x, np.float64)
+        rel = np.empty(k)
+        _lib.check(_lib.lib().gdtp_residual(self._s, _lib.ptr(b), _lib.ptr(x), k, _lib.ptr(rel)))
+        return rel
+
+    def solve(self, b: np.ndarray, x0: np.ndarray | None = None, tol: float = 1e-6, max_iters: int = 60,
+              precision: str = "mixed", check: bool = True):
+        b, k = self._vec(b, np.float64)
+        x = np.zeros_like(b) if x0 is None else self._vec(x0, np.float64)[0].copy()
+        rep = _lib.Report()
+        fn = _lib.lib().gdtp_solve if precision == "mixed" else _lib.lib().gdtp_solve_fp64
+        code = fn(self._s, _lib.ptr(b), _lib.ptr(x), k, float(tol), int(max_iters), C.byref(rep))
+        if code != 0 and (check or code != -4):
+            _lib.check(code)
+        return x, {"iterations": rep.iterations, "vcycles": rep.vcycles, "rel_residual_max": rep.rel_residual_max,
+                   "seconds": rep.seconds, "converged": code == 0}
+
+
+def InitializeMassAndStiffness(hierarchy: Hierarchy, device: int = 0, parameter_metric=None) -> System:
+    return System(hierarchy, device=device, parameter_metric=parameter_metric)
+
+
+def UpdateLinearSystem(stiffness_weight: float, screen_weight: float, system: System) -> None:
+    system.update(stiffness_weight, screen_weight)
+
+
+def MultiplyBySystemMatrix_NoReciprocals(system: System, x: np.ndarray, which: int = SYSTEM) -> np.ndarray:
+    return system.apply(x, which)
+
+
+def VCycle(system: System, x: np.ndarray, rhs: np.ndarray) -> np.ndarray:
+    return system.vcycle(x, rhs)
+
+
+def texture_filtering_rhs(system: System, f: np.ndarray, stiffness: float, sharpness: float) -> np.ndarray:
+    """``M f + stiffness * sharpness * S f`` (TextureFiltering.cpp:693-700)."""
+    return system.apply(f, MASS) + stiffness * sharpness * system.apply(f, STIFFNESS)
+
+
+def texel_signal(hierarchy: Hierarchy, texture: np.ndarray) -> np.ndarray:
+    """Texture value of every active texel, in texel order (TextureFiltering.cpp:603-608)."""
+    tn = hierarchy.array("textureNodes")
+    return np.ascontiguousarray(texture[tn[:, 1], tn[:, 0]], dtype=np.float64)

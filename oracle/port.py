@@ -1,0 +1,101 @@
+"""Oracle port: numpy/scipy restatement of the reference's solve-path operators.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the product imports this module; tests
+use it as the checker.  It is pinned against the compiled reference
+(``oracle/_ref``, fixtures in ``tests/golden``) by ``tests/test_oracle_port.py``.
+
+Every function restates one reference operator on the reference's data layout
+(texel order, 10-slot deep coefficients, boundary CSR blocks):
+
+* ``full_matrix``             FullMatrixConstruction   include/Src/UpdateCoefficients.inl:137-219
+* ``multiply_no_reciprocals`` MultiplyBySystemMatrix_NoReciprocals include/Src/IterativeSolvers.inl:881-950
+* ``prolongation``            InitializeProlongationMatrix include/Src/ProlongationAndRestriction.inl:218-263
+* ``reciprocal_form``         UpdateMultigridCoefficients include/Src/UpdateCoefficients.inl:374-397
+* ``direct_solve``            the --useDirectSolver FP64 solve (TextureFiltering.cpp:651-655, 704-707;
+                              Eigen SimplicialLDLT in include/Src/Solver.h:144-203, here scipy's LU)
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+
+def full_matrix(nodeinfo: np.ndarray, deep_global: np.ndarray, boundary_global: np.ndarray, deep: np.ndarray,
+                bb: sp.csr_matrix, bd: sp.csr_matrix) -> sp.csr_matrix:
+    """Global operator from deep 9-point rows and the BB / BD boundary blocks."""
+    n = len(nodeinfo)
+    key = {(int(c), int(i), int(j)): g for g, (c, i, j, _) in enumerate(nodeinfo)}
+    rows, cols, vals = [], [], []
+    for d, g in enumerate(deep_global):
+        c, i, j, _ = nodeinfo[g]
+        for oy in (-1, 0, 1):
+            for ox in (-1, 0, 1):
+                rows.append(g)
+                cols.append(key[(int(c), int(i) + ox, int(j) + oy)])
+                vals.append(deep[d, (oy + 1) * 3 + ox + 1])
+    bbc, bdc = bb.tocoo(), bd.tocoo()
+    rows += list(boundary_global[bbc.row]) + list(boundary_global[bdc.row])
+    cols += list(boundary_global[bbc.col]) + list(bdc.col)
+    vals += list(bbc.data) + list(bdc.data)
+    return sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+
+
+def multiply_no_reciprocals(A: sp.csr_matrix, x: np.ndarray) -> np.ndarray:
+    """y = A x with the raw (non-reciprocal) operator."""
+    return A @ x
+
+
+def prolongation(fine_nodeinfo: np.ndarray, fine_charts: np.ndarray, coarse_nodeinfo: np.ndarray,
+                 coarse_charts: np.ndarray) -> sp.csr_matrix:
+    """Bilinear per-chart prolongation: even offsets from the chart centre sit on a
+    coarse texel (weight 1), odd ones between two (1/2 per axis)."""
+    key = {(int(c), int(i), int(j)): g for g, (c, i, j, _) in enumerate(coarse_nodeinfo)}
+    rows, cols, vals = [], [], []
+    for g, (c, i, j, _) in enumerate(fine_nodeinfo):
+        ri, rj = int(i) - fine_charts[c, 2], int(j) - fine_charts[c, 3]
+        for a in ((0,) if ri % 2 == 0 else (0, 1)):
+            for b in ((0,) if rj % 2 == 0 else (0, 1)):
+                rows.append(g)
+                cols.append(key[(int(c), ri // 2 + a + coarse_charts[c, 2], rj // 2 + b + coarse_charts[c, 3])])
+                vals.append((1.0 if ri % 2 == 0 else 0.5) * (1.0 if rj % 2 == 0 else 0.5))
+    return sp.csr_matrix((vals, (rows, cols)), shape=(len(fine_nodeinfo), len(coarse_nodeinfo)))
+
+
+def deep_rows(A: sp.csr_matrix, nodeinfo: np.ndarray, deep_global: np.ndarray) -> np.ndarray:
+    """10-slot deep coefficients (slot (dj+1)*3+(di+1)) read back from a global operator."""
+    key = {(int(c), int(i), int(j)): g for g, (c, i, j, _) in enumerate(nodeinfo)}
+    out = np.zeros((len(deep_global), 10))
+    A = A.tocsr()
+    for d, g in enumerate(deep_global):
+        c, i, j, _ = nodeinfo[g]
+        for oy in (-1, 0, 1):
+            for ox in (-1, 0, 1):
+                out[d, (oy + 1) * 3 + ox + 1] = A[g, key[(int(c), int(i) + ox, int(j) + oy)]]
+    return out
+
+
+def reciprocal_form(deep: np.ndarray) -> np.ndarray:
+    """c_k /= c4 (k != 4), c4 = 1/c4, c9 = c4 (the smoother's stored form)."""
+    out = deep.copy()
+    c4 = deep[:, 4].copy()
+    out[:, :9] = deep[:, :9] / c4[:, None]
+    out[:, 4] = 1.0 / c4
+    out[:, 9] = c4
+    return out
+
+
+def direct_solve(A: sp.csr_matrix, b: np.ndarray) -> np.ndarray:
+    return spla.splu(A.tocsc()).solve(np.asarray(b, dtype=np.float64))
+
+
+def relative_residual(A: sp.csr_matrix, b: np.ndarray, x: np.ndarray) -> np.ndarray:
+    return np.linalg.norm(b - A @ x, axis=0) / np.linalg.norm(b, axis=0)
+
+
+def energy_error(A: sp.csr_matrix, x: np.ndarray, x_ref: np.ndarray) -> np.ndarray:
+    """Relative error in the operator's energy norm, per right-hand side.  Texels
+    whose support barely meets a chart have tiny diagonals and are not pinned by
+    the residual; the energy norm weighs every texel by its support."""
+    e = x - x_ref
+    return np.sqrt(np.einsum("ik,ik->k", e, A @ e) / np.einsum("ik,ik->k", x_ref, A @ x_ref))

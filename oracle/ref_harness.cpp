@@ -145,6 +145,8 @@ int main(int argc, char** argv) {
   const int vcycles = argc > 6 ? atoi(argv[6]) : 12;
   const std::string mode = argc > 7 ? argv[7] : "dump";
   const bool full = (mode == "dump");
+  const bool timeOnly = (mode == "time");  // V-cycles to `tol` (argv[8]) only: no dumps, no direct solve
+  const double tol = argc > 8 ? atof(argv[8]) : 1e-6;
 
   TexturedMesh mesh;
   if (!ReadGDM(argv[1], mesh)) { fprintf(stderr, "cannot read %s\n", argv[1]); return 2; }
@@ -223,11 +225,13 @@ int main(int argc, char** argv) {
   // ---------------- FP64 direct solve (the accuracy oracle) ------------------------------
   auto T3 = std::chrono::steady_clock::now();
   std::vector<Vec> exact(f0.size(), ZeroData());
+  if (!timeOnly) {
 #if !USE_FLOAT  // the FP32 build only reproduces the shipped V-cycle; ground truth needs FP64
   directSolver.init(A);
   directSolver.update(A);
   solve(directSolver, exact, rhs);
 #endif
+  }
   double tDirect = secs(T3);
 
   // ---------------- V-cycles ------------------------------------------------------------
@@ -258,6 +262,7 @@ int main(int argc, char** argv) {
   history.push_back(ResidualNorm(coeffs, deepA, BDA, BBA, fine, vars[0].x, rhs, bn, rn));
   std::vector<double> firstIterate;
   for (int it = 0; it < vcycles; it++) {
+    if (timeOnly && history.back() <= tol) break;
     auto Tc = std::chrono::steady_clock::now();
     VCycle(vars, coeffs, indices, boundarySolvers, coarseSolver, false, false);
     cycleTimes.push_back(secs(Tc));
@@ -356,6 +361,19 @@ int main(int argc, char** argv) {
       ad.insert(ad.end(), {c.minCorner[0], c.minCorner[1], c.maxCorner[0], c.maxCorner[1], c.gridOrigin[0], c.gridOrigin[1]});
     }
     out.i32("atlas/charts_i", ac, 5);
+    // boundary-cell triangulation: per triangle chart, cell, corner node indices, corner positions
+    std::vector<int> bti;
+    std::vector<double> btd;
+    for (size_t c = 0; c < fine.gridCharts.size(); c++) {
+      const GridChart& g = fine.gridCharts[c];
+      for (size_t cell = 0; cell < g.boundaryTriangles.size(); cell++)
+        for (const BoundaryIndexedTriangle& t : g.boundaryTriangles[cell]) {
+          bti.insert(bti.end(), {(int)c, (int)cell, (int)t.indices[0], (int)t.indices[1], (int)t.indices[2]});
+          for (int k = 0; k < 3; k++) { btd.push_back(t.vertices[k][0]); btd.push_back(t.vertices[k][1]); }
+        }
+    }
+    out.i32("fine/boundaryTriangles", bti, 5);
+    out.f64("fine/boundaryTrianglePos", btd, 6);
     out.f64("atlas/charts_d", ad, 6);
     for (int l = 1; l < levels; l++) {
       std::string p = "L" + std::to_string(l) + "/";

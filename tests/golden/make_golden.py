@@ -1,0 +1,75 @@
+"""Regenerates the golden fixtures in this directory from the reference itself.
+
+Runs the oracle harness (``oracle/_ref/gdtp_ref``: the reference solve path
+compiled from its own sources by ``oracle/Makefile``) on seeded meshes from
+``gradientdomaintextureprocessing_b200.meshgen`` and keeps the arrays the tests
+compare against.  Needs the reference checkout (only this script does):
+
+    make -C oracle && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from gdd import read_dump  # noqa: E402
+from gradientdomaintextureprocessing_b200 import meshgen  # noqa: E402
+
+CASES = {
+    # name: (mesh factory, levels, stiffness, sharpness, keep coefficients)
+    "torus128": (lambda: meshgen.torus_atlas(128, 128), 4, 1e-3, 2.0, True),
+    "torus256": (lambda: meshgen.torus_atlas(256, 256), 4, 1e-3, 2.0, False),
+    "ico256": (lambda: meshgen.icosphere_atlas(256, 256, subdiv=5), 4, 1e-3, 2.0, True),
+}
+INDEX_KEYS = ["counts", "nodeinfo", "boundaryGlobalIndex", "deepGlobalIndex", "boundaryAndDeepIndex", "rasterLines",
+              "restrictionLines", "deepLines", "prolongationLines", "charts_i", "charts_d"]
+
+
+def make(name: str) -> None:
+    factory, levels, lam, sharp, coefs = CASES[name]
+    mesh = factory()
+    exe = os.path.join(ROOT, "oracle", "_ref", "gdtp_ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        gdm, out = os.path.join(tmp, "m.gdm"), os.path.join(tmp, "o.gdd")
+        meshgen.write_gdm(gdm, mesh)
+        subprocess.run([exe, gdm, out, str(levels), str(lam), str(sharp), "12", "dump"], check=True, capture_output=True)
+        d = read_dump(out)
+    keep = {"mesh/vertices": mesh["vertices"], "mesh/triangles": mesh["triangles"], "mesh/uv": mesh["uv"],
+            "mesh/texture": mesh["texture"], "meta/size": d["meta/size"], "meta/weights": d["meta/weights"]}
+    for k in ("solve/f", "solve/rhs", "solve/exact", "vcycle/history", "fine/textureNodes", "fine/textureBary",
+              "fine/boundaryNodes"):
+        keep[k] = d[k]
+    for l in range(levels):
+        for k in INDEX_KEYS:
+            if f"L{l}/{k}" in d:
+                keep[f"L{l}/{k}"] = d[f"L{l}/{k}"]
+        for part in ("ptr", "col", "val"):
+            if f"L{l}/boundaryRestriction/{part}" in d:
+                keep[f"L{l}/boundaryRestriction/{part}"] = d[f"L{l}/boundaryRestriction/{part}"]
+    if coefs:
+        for k in ("fine/deepMass", "fine/deepStiffness"):
+            keep[k] = d[k]
+        for m in ("BBmass", "BBstiffness", "BDmass", "BDstiffness"):
+            for part in ("ptr", "col", "val"):
+                keep[f"fine/{m}/{part}"] = d[f"fine/{m}/{part}"]
+        for l in range(levels):
+            keep[f"L{l}/coef/deep"] = d[f"L{l}/coef/deep"]
+            for m in ("BB", "BD"):
+                for part in ("ptr", "col", "val"):
+                    keep[f"L{l}/coef/{m}/{part}"] = d[f"L{l}/coef/{m}/{part}"]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k.replace("/", "__"): v for k, v in keep.items()})
+    print(name, sum(v.nbytes for v in keep.values()) / 1e6, "MB raw")
+
+
+if __name__ == "__main__":
+    for name in (sys.argv[1:] or CASES):
+        make(name)

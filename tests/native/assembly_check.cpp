@@ -6,7 +6,9 @@
 //
 // usage: assembly_check mesh.gdm out.gdd levels
 #include <cstdio>
+#include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -97,12 +99,56 @@ int main(int argc, char** argv) {
   for (size_t i = 0; i < deepA.size(); i++) deepA[i] = fs.deepMass[i] + lam * fs.deepStiffness[i];
   Csr bbA = csr_axpby(1.0, fs.bbMass, lam, fs.bbStiffness), bdA = csr_axpby(1.0, fs.bdMass, lam, fs.bdStiffness);
   std::vector<LevelCoefficients> lc;
-  if (!galerkin_hierarchy(h, deepA, bbA, bdA, lc, err)) { fprintf(stderr, "%s\n", err.c_str()); return 3; }
+  if (!galerkin_hierarchy(h, 0, deepA, bbA, bdA, lc, err)) { fprintf(stderr, "%s\n", err.c_str()); return 3; }
   for (size_t l = 0; l < lc.size(); l++) {
     std::string p = "L" + std::to_string(l) + "/mine/";
     out.f64(p + "deep", lc[l].deep, 10);
     out.csr(p + "BB", lc[l].bb);
     out.csr(p + "BD", lc[l].bd);
+  }
+  // exact boundary solver: apply to r = BB * ones-ish vector and report the error
+  for (size_t l = 0; l < lc.size(); l++) {
+    BoundarySolverSetup bs;
+    int maxBlock = argc > 5 ? atoi(argv[5]) : 384;
+    if (!build_boundary_solver(lc[l].bb, lc[l].bd, maxBlock, bs, err)) { fprintf(stderr, "bsolve: %s\n", err.c_str()); return 3; }
+    const Csr& BB = lc[l].bb;
+    std::vector<double> xt(bs.nb), r(bs.nb, 0.0), x(bs.nb, 0.0);
+    for (int i = 0; i < bs.nb; i++) xt[i] = std::sin(0.37 * i) + 0.1 * std::cos(1.3 * i);
+    for (int i = 0; i < bs.nb; i++)
+      for (int k = BB.ptr[i]; k < BB.ptr[i + 1]; k++) r[i] += BB.val[k] * xt[BB.col[k]];
+    // scaled solve
+    std::vector<double> rh(bs.nb), y(bs.nI, 0.0), t(bs.nS), xs(bs.nS, 0.0), xh(bs.nb);
+    for (int k = 0; k < bs.nb; k++) rh[k] = r[bs.order[k]] * bs.scale[k];
+    for (int p = 0; p < bs.nSub; p++) {
+      int b0 = bs.subPtr[p], m = bs.subPtr[p + 1] - b0;
+      const double* Inv = &bs.inv[bs.invOff[p]];
+      for (int a = 0; a < m; a++) { double s2 = 0; for (int q = 0; q < m; q++) s2 += Inv[size_t(a) * m + q] * rh[b0 + q]; y[b0 + a] = s2; }
+    }
+    for (int s2 = 0; s2 < bs.nS; s2++) {
+      double v = rh[bs.nI + s2];
+      for (int k = bs.ASI.ptr[s2]; k < bs.ASI.ptr[s2 + 1]; k++) v -= bs.ASI.val[k] * y[bs.ASI.col[k]];
+      t[s2] = v;
+    }
+    for (int a = 0; a < bs.nS; a++) { double v = 0; for (int c = 0; c < bs.nS; c++) v += bs.Sinv[size_t(a) * bs.nS + c] * t[c]; xs[a] = v; }
+    for (int p = 0; p < bs.nSub; p++) {
+      int b0 = bs.subPtr[p], m = bs.subPtr[p + 1] - b0;
+      std::vector<double> z(m, 0.0);
+      for (int a = 0; a < m; a++)
+        for (int k = bs.AIS.ptr[b0 + a]; k < bs.AIS.ptr[b0 + a + 1]; k++) z[a] += bs.AIS.val[k] * xs[bs.AIS.col[k]];
+      const double* Inv = &bs.inv[bs.invOff[p]];
+      for (int a = 0; a < m; a++) { double s2 = 0; for (int q = 0; q < m; q++) s2 += Inv[size_t(a) * m + q] * z[q]; xh[b0 + a] = y[b0 + a] - s2; }
+    }
+    for (int s2 = 0; s2 < bs.nS; s2++) xh[bs.nI + s2] = xs[s2];
+    for (int k = 0; k < bs.nb; k++) x[bs.order[k]] = xh[k] * bs.scale[k];
+    double emax = 0, xmax = 0, rres = 0, rn = 0;
+    for (int i = 0; i < bs.nb; i++) { emax = std::max(emax, std::fabs(x[i] - xt[i])); xmax = std::max(xmax, std::fabs(xt[i])); }
+    for (int i = 0; i < bs.nb; i++) {
+      double v = r[i];
+      for (int k = BB.ptr[i]; k < BB.ptr[i + 1]; k++) v -= BB.val[k] * x[BB.col[k]];
+      rres += v * v; rn += r[i] * r[i];
+    }
+    fprintf(stderr, "level %zu boundary %d: %d subdomains, %d separator, rel residual %.2e, max err %.2e\n", l, bs.nb, bs.nSub, bs.nS,
+            std::sqrt(rres / rn), emax / xmax);
   }
   out.f64("fine/deepMass", fs.deepMass, 10);
   out.f64("fine/deepStiffness", fs.deepStiffness, 10);
@@ -110,9 +156,22 @@ int main(int argc, char** argv) {
   out.csr("fine/BBstiffness", fs.bbStiffness);
   out.csr("fine/BDmass", fs.bdMass);
   out.csr("fine/BDstiffness", fs.bdStiffness);
+  {
+    std::vector<int> bti;
+    std::vector<double> btd;
+    for (size_t c = 0; c < be.charts.size(); c++)
+      for (size_t cell = 0; cell < be.charts[c].cellTriangles.size(); cell++)
+        for (const BoundaryTriangle& t : be.charts[c].cellTriangles[cell]) {
+          bti.insert(bti.end(), {(int)c, (int)cell, t.idx[0], t.idx[1], t.idx[2]});
+          for (int k = 0; k < 3; k++) { btd.push_back(t.v[k].x); btd.push_back(t.v[k].y); }
+        }
+    out.put("fine/boundaryTriangles", 1, bti.size(), 5, bti.data(), 4);
+    out.f64("fine/boundaryTrianglePos", btd, 6);
+  }
   std::vector<int> info = {be.numBoundaryNodes, be.numMidPoints, be.numFineNodes, be.numFineBoundary, be.degenerateTriangulations};
   out.i32("fine/boundaryNodes", info);
   fprintf(stderr, "assembly_check: %d interior cells, %d boundary triangles, %d degenerate triangulations\n", w.numInteriorCells,
           w.numBoundaryTriangles, be.degenerateTriangulations);
   return 0;
 }
+// (appended) exact boundary solver check: BB x = r via the subdomain/Schur path, FP64
