@@ -180,145 +180,174 @@ __global__ void __launch_bounds__(256) k_prolong_add(const ProlongRun* __restric
 }
 
 // ----------------------------------------------------------------------------
-// Exact boundary-block solve  x_B = BB^-1 (rhs_B - BD x), in four steps over
-// the subdomain / separator split (scaled by s = BB_ii^-1/2).
+// Exact boundary-block solve  x_B = BB^-1 (rhs_B - BD x) over the subdomain /
+// separator split (scaled by s = BB_ii^-1/2):
+//   r^ = s (rhs - BD x)                       k_bs_rhs        (sparse, all rows)
+//   y  = Inv_p r^_I                           k_bs_gemv mode 0 (dense, batched)
+//   t  = r^_S - A_SI y                        k_bs_sep_rhs    (sparse)
+//   xs = Sinv t                               k_bs_gemv mode 1 (dense, j-chunked) + k_bs_sep_sum
+//   z  = A_IS xs                              k_bs_coupling   (sparse)
+//   x_I = s (y - Inv_p z)                     k_bs_gemv mode 2 (dense, scatter)
+// The dense products are memory-bound: every inverse is symmetric and stored
+// row-major with rows padded to a multiple of 4, so lane l of a warp reads rows
+// 4l..4l+3 of matrix row j with one vector load and a warp reads contiguous
+// memory; the 8 warps of a block take interleaved j and are reduced in shared
+// memory in a fixed order (deterministic).
 // ----------------------------------------------------------------------------
-// step 1 (block per subdomain): r^ = s (rhs - BD x) for the interior rows, y = Inv r^
 template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bsolve_interior(const int* __restrict__ subPtr, const long long* __restrict__ invOff,
-                                                         const T* __restrict__ inv, const int* __restrict__ posGlobal,
-                                                         const T* __restrict__ scale, const int* __restrict__ bdPtr,
-                                                         const int* __restrict__ bdCol, const T* __restrict__ bdVal,
-                                                         const T* __restrict__ rhs, const T* __restrict__ x, T* __restrict__ y,
-                                                         int KP, int G) {
-  extern __shared__ unsigned char smem_raw[];
-  T* rs = reinterpret_cast<T*>(smem_raw);  // m * KP
-  const int p = blockIdx.x;
-  const int b0 = subPtr[p], m = subPtr[p + 1] - b0;
-  for (int e = threadIdx.x; e < m * G; e += blockDim.x) {
-    const int a = e / G, q = e - a * G, off = q * W, k = b0 + a;
-    const int g = posGlobal[k];
-    Vec<T, W> acc = vload<T, W>(rhs + (long long)g * KP + off);
-    for (int j = bdPtr[k]; j < bdPtr[k + 1]; j++) axpy(acc, -bdVal[j], vload<T, W>(x + (long long)bdCol[j] * KP + off));
-    const T s = scale[k];
-#pragma unroll
-    for (int c = 0; c < W; c++) acc.v[c] *= s;
-    vstore<T, W>(rs + a * KP + off, acc);
-  }
-  __syncthreads();
-  const T* Inv = inv + invOff[p];
-  // warp per output row; lanes stride the row (coalesced), reduce by shuffles
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int a = warp; a < m; a += nw) {
-    const T* row = Inv + (long long)a * m;
-    for (int q = 0; q < G; q++) {
-      const int off = q * W;
-      Vec<T, W> acc;
-#pragma unroll
-      for (int c = 0; c < W; c++) acc.v[c] = 0;
-      for (int j = lane; j < m; j += 32) axpy(acc, row[j], vload<T, W>(rs + j * KP + off));
-#pragma unroll
-      for (int c = 0; c < W; c++)
-        for (int s = 16; s > 0; s >>= 1) acc.v[c] += __shfl_xor_sync(0xffffffffu, acc.v[c], s);
-      if (lane == 0) vstore<T, W>(y + (long long)(b0 + a) * KP + off, acc);
-    }
-  }
-}
-
-// step 2 (thread per separator row): t = s (rhs - BD x) - A_SI y
-template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bsolve_separator_rhs(int nI, int nS, const int* __restrict__ posGlobal,
-                                                              const T* __restrict__ scale, const int* __restrict__ bdPtr,
-                                                              const int* __restrict__ bdCol, const T* __restrict__ bdVal,
-                                                              const int* __restrict__ asiPtr, const int* __restrict__ asiCol,
-                                                              const T* __restrict__ asiVal, const T* __restrict__ rhs,
-                                                              const T* __restrict__ x, const T* __restrict__ y, T* __restrict__ t,
-                                                              int KP, int G) {
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long s = tid / G;
-  if (s >= nS) return;
-  const int q = int(tid - s * G), off = q * W, k = nI + int(s);
-  const int g = posGlobal[k];
-  Vec<T, W> acc = vload<T, W>(rhs + (long long)g * KP + off);
+__global__ void __launch_bounds__(256) k_bs_rhs(int nb, const int* __restrict__ posGlobal, const T* __restrict__ scale,
+                                                const int* __restrict__ bdPtr, const int* __restrict__ bdCol,
+                                                const T* __restrict__ bdVal, const T* __restrict__ rhs, const T* __restrict__ x,
+                                                T* __restrict__ rhat, int KP, int G) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long k = t / G;
+  if (k >= nb) return;
+  const int q = int(t - k * G), off = q * W;
+  Vec<T, W> acc = vload<T, W>(rhs + (long long)posGlobal[k] * KP + off);
   for (int j = bdPtr[k]; j < bdPtr[k + 1]; j++) axpy(acc, -bdVal[j], vload<T, W>(x + (long long)bdCol[j] * KP + off));
   const T sc = scale[k];
 #pragma unroll
   for (int c = 0; c < W; c++) acc.v[c] *= sc;
+  vstore<T, W>(rhat + k * KP + off, acc);
+}
+
+template <typename T>
+struct Quad;
+template <>
+struct __align__(16) Quad<float> {
+  float v[4];
+};
+template <>
+struct __align__(32) Quad<double> {
+  double v[4];
+};
+
+// task = {matrix, first row quad, j begin, j end}; rows of the block's matrix
+// start at rowPtr[matrix] in the vectors.  mode:
+//   0: out[row] = sum_j M[j][row] vin[j]
+//   1: out[chunk = blockIdx.y][row] = partial sum over this task's j range
+//   2: x[posGlobal[row]] = scale[row] * (y[row] - sum)
+template <typename T, int W>
+__global__ void __launch_bounds__(256) k_bs_gemv(const int4* __restrict__ tasks, const int* __restrict__ rowPtr,
+                                                 const long long* __restrict__ matOff, const T* __restrict__ mat,
+                                                 const T* __restrict__ vin, T* __restrict__ out, int mode, int nRowsTotal,
+                                                 int chunkLen, const int* __restrict__ posGlobal, const T* __restrict__ scale,
+                                                 const T* __restrict__ y, T* __restrict__ x, int KP, int G) {
+  __shared__ T red[8][32][4 * W];
+  const int4 task = tasks[blockIdx.x];
+  const int p = task.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rq = task.y + lane;
+  const int r0 = rowPtr[p], m = rowPtr[p + 1] - r0, mp = (m + 3) & ~3;
+  int j0 = task.z, j1 = task.w;
+  if (mode == 1) {  // chunk of the j range taken by this grid row
+    j0 = task.z + blockIdx.y * chunkLen;
+    j1 = min(task.w, j0 + chunkLen);
+  }
+  const T* M = mat + matOff[p];
+  const bool active = 4 * rq < m;
+  for (int q = 0; q < G; q++) {
+    const int off = q * W;
+    T acc[4][W];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int c = 0; c < W; c++) acc[a][c] = 0;
+    if (active) {
+#pragma unroll 4
+      for (int j = j0 + warp; j < j1; j += 8) {
+        const Quad<T> mq = *reinterpret_cast<const Quad<T>*>(M + (long long)j * mp + 4 * rq);
+        const Vec<T, W> v = vload<T, W>(vin + (long long)(r0 + j) * KP + off);
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int c = 0; c < W; c++) acc[a][c] += mq.v[a] * v.v[c];
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int c = 0; c < W; c++) red[warp][lane][a * W + c] = acc[a][c];
+    __syncthreads();
+    if (warp == 0 && active) {
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int row = 4 * rq + a;
+        if (row < m) {
+          Vec<T, W> sum;
+#pragma unroll
+          for (int c = 0; c < W; c++) {
+            T v = 0;
+            for (int w = 0; w < 8; w++) v += red[w][lane][a * W + c];
+            sum.v[c] = v;
+          }
+          if (mode == 0) {
+            vstore<T, W>(out + (long long)(r0 + row) * KP + off, sum);
+          } else if (mode == 1) {
+            vstore<T, W>(out + ((long long)blockIdx.y * nRowsTotal + (r0 + row)) * KP + off, sum);
+          } else {
+            const Vec<T, W> yy = vload<T, W>(y + (long long)(r0 + row) * KP + off);
+            const T sc = scale[r0 + row];
+            Vec<T, W> o;
+#pragma unroll
+            for (int c = 0; c < W; c++) o.v[c] = (yy.v[c] - sum.v[c]) * sc;
+            vstore<T, W>(x + (long long)posGlobal[r0 + row] * KP + off, o);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// t = r^_S - A_SI y
+template <typename T, int W>
+__global__ void __launch_bounds__(256) k_bs_sep_rhs(int nI, int nS, const int* __restrict__ asiPtr, const int* __restrict__ asiCol,
+                                                    const T* __restrict__ asiVal, const T* __restrict__ rhat,
+                                                    const T* __restrict__ y, T* __restrict__ t, int KP, int G) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long s = tid / G;
+  if (s >= nS) return;
+  const int q = int(tid - s * G), off = q * W;
+  Vec<T, W> acc = vload<T, W>(rhat + (long long)(nI + s) * KP + off);
   for (int j = asiPtr[s]; j < asiPtr[s + 1]; j++) axpy(acc, -asiVal[j], vload<T, W>(y + (long long)asiCol[j] * KP + off));
   vstore<T, W>(t + s * KP + off, acc);
 }
 
-// step 3 (warp per separator row): xs = Sinv t ; x[g] = s * xs
+// xs = sum of the chunk partials (fixed order); x[posGlobal[base + s]] = scale * xs
 template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bsolve_separator(int nI, int nS, const T* __restrict__ sinv, const T* __restrict__ t,
-                                                          const int* __restrict__ posGlobal, const T* __restrict__ scale,
-                                                          T* __restrict__ xs, T* __restrict__ x, int KP, int G) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= nS) return;
-  const T* row = sinv + (long long)warp * nS;
-  for (int q = 0; q < G; q++) {
-    const int off = q * W;
-    Vec<T, W> acc;
+__global__ void __launch_bounds__(256) k_bs_sep_sum(int base, int n, int chunks, const T* __restrict__ part,
+                                                    const int* __restrict__ posGlobal, const T* __restrict__ scale,
+                                                    T* __restrict__ xs, T* __restrict__ x, int KP, int G) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long s = tid / G;
+  if (s >= n) return;
+  const int q = int(tid - s * G), off = q * W;
+  Vec<T, W> acc = vload<T, W>(part + s * KP + off);
+  for (int c = 1; c < chunks; c++) {
+    const Vec<T, W> v = vload<T, W>(part + ((long long)c * n + s) * KP + off);
 #pragma unroll
-    for (int c = 0; c < W; c++) acc.v[c] = 0;
-    for (int j = lane; j < nS; j += 32) axpy(acc, row[j], vload<T, W>(t + (long long)j * KP + off));
-#pragma unroll
-    for (int c = 0; c < W; c++)
-      for (int s = 16; s > 0; s >>= 1) acc.v[c] += __shfl_xor_sync(0xffffffffu, acc.v[c], s);
-    if (lane == 0) {
-      vstore<T, W>(xs + (long long)warp * KP + off, acc);
-      const T sc = scale[nI + warp];
-#pragma unroll
-      for (int c = 0; c < W; c++) acc.v[c] *= sc;
-      vstore<T, W>(x + (long long)posGlobal[nI + warp] * KP + off, acc);
-    }
+    for (int k = 0; k < W; k++) acc.v[k] += v.v[k];
   }
+  if (xs) vstore<T, W>(xs + s * KP + off, acc);
+  const T sc = scale[base + s];
+#pragma unroll
+  for (int k = 0; k < W; k++) acc.v[k] *= sc;
+  vstore<T, W>(x + (long long)posGlobal[base + s] * KP + off, acc);
 }
 
-// step 4 (block per subdomain): x_I = s (y - Inv (A_IS xs))
+// z = A_IS xs for every interior position
 template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bsolve_back(const int* __restrict__ subPtr, const long long* __restrict__ invOff,
-                                                     const T* __restrict__ inv, const int* __restrict__ posGlobal,
-                                                     const T* __restrict__ scale, const int* __restrict__ aisPtr,
-                                                     const int* __restrict__ aisCol, const T* __restrict__ aisVal,
-                                                     const T* __restrict__ xs, const T* __restrict__ y, T* __restrict__ x, int KP,
-                                                     int G) {
-  extern __shared__ unsigned char smem_raw[];
-  T* zs = reinterpret_cast<T*>(smem_raw);
-  const int p = blockIdx.x;
-  const int b0 = subPtr[p], m = subPtr[p + 1] - b0;
-  for (int e = threadIdx.x; e < m * G; e += blockDim.x) {
-    const int a = e / G, q = e - a * G, off = q * W, k = b0 + a;
-    Vec<T, W> acc;
+__global__ void __launch_bounds__(256) k_bs_coupling(int nI, const int* __restrict__ aisPtr, const int* __restrict__ aisCol,
+                                                     const T* __restrict__ aisVal, const T* __restrict__ xs, T* __restrict__ z,
+                                                     int KP, int G) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long k = tid / G;
+  if (k >= nI) return;
+  const int q = int(tid - k * G), off = q * W;
+  Vec<T, W> acc;
 #pragma unroll
-    for (int c = 0; c < W; c++) acc.v[c] = 0;
-    for (int j = aisPtr[k]; j < aisPtr[k + 1]; j++) axpy(acc, aisVal[j], vload<T, W>(xs + (long long)aisCol[j] * KP + off));
-    vstore<T, W>(zs + a * KP + off, acc);
-  }
-  __syncthreads();
-  const T* Inv = inv + invOff[p];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int a = warp; a < m; a += nw) {
-    const T* row = Inv + (long long)a * m;
-    for (int q = 0; q < G; q++) {
-      const int off = q * W;
-      Vec<T, W> acc;
-#pragma unroll
-      for (int c = 0; c < W; c++) acc.v[c] = 0;
-      for (int j = lane; j < m; j += 32) axpy(acc, row[j], vload<T, W>(zs + j * KP + off));
-#pragma unroll
-      for (int c = 0; c < W; c++)
-        for (int s = 16; s > 0; s >>= 1) acc.v[c] += __shfl_xor_sync(0xffffffffu, acc.v[c], s);
-      if (lane == 0) {
-        const Vec<T, W> yy = vload<T, W>(y + (long long)(b0 + a) * KP + off);
-        const T sc = scale[b0 + a];
-        Vec<T, W> out;
-#pragma unroll
-        for (int c = 0; c < W; c++) out.v[c] = (yy.v[c] - acc.v[c]) * sc;
-        vstore<T, W>(x + (long long)posGlobal[b0 + a] * KP + off, out);
-      }
-    }
-  }
+  for (int c = 0; c < W; c++) acc.v[c] = 0;
+  for (int j = aisPtr[k]; j < aisPtr[k + 1]; j++) axpy(acc, aisVal[j], vload<T, W>(xs + (long long)aisCol[j] * KP + off));
+  vstore<T, W>(z + k * KP + off, acc);
 }
 
 // ----------------------------------------------------------------------------
@@ -361,21 +390,23 @@ __global__ void __launch_bounds__(256) k_coarse_solve(int n, const double* __res
 // and b^2 per channel go to `partials` for a deterministic norm reduction.
 // ----------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restrict__ runs, int nRuns, const double* __restrict__ coef,
-                                                      int planeStride, int deepBlocks, const int* __restrict__ bPtr,
-                                                      const int* __restrict__ bCol, const double* __restrict__ bVal,
-                                                      const int* __restrict__ bGlobal, int nB, const double* __restrict__ b,
-                                                      const double* __restrict__ x, double* __restrict__ out, int K, int G, int mode,
-                                                      double* __restrict__ partials) {
-  double acc[4] = {0, 0, 0, 0};
-  int g = -1, q = 0;
-  if ((int)blockIdx.x < deepBlocks) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int per = 32 * G;
-    const long long r = t / per;
-    const int rem = int(t - r * per);
-    const int m = rem / G;
-    q = rem - m * G;
-    if (r < nRuns) {
+                                                      int planeStride, const int* __restrict__ bPtr, const int* __restrict__ bCol,
+                                                      const double* __restrict__ bVal, const int* __restrict__ bGlobal, int nB,
+                                                      const double* __restrict__ b, const double* __restrict__ x,
+                                                      double* __restrict__ out, int K, int G, int mode, double* __restrict__ partials) {
+  // grid-stride over deep items (runs x 32 x G) then boundary items (rows x G);
+  // the stride is a multiple of G, so every thread keeps one channel group q
+  const long long nDeepItems = (long long)nRuns * 32 * G, nItems = nDeepItems + (long long)nB * G;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = int(t0 % G);
+  double rr[4] = {0, 0, 0, 0}, bb[4] = {0, 0, 0, 0};
+  for (long long t = t0; t < nItems; t += stride) {
+    double acc[4] = {0, 0, 0, 0};
+    int g = -1;
+    if (t < nDeepItems) {
+      const long long r = t / (32 * G);
+      const int m = int(t - r * 32 * G) / G;
       const ColourRun R = runs[r];
       if (m < R.len) {
         const int pos = R.pos0 + 2 * m, pp = R.prev0 + 2 * m, pn = R.next0 + 2 * m;
@@ -391,12 +422,8 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
         }
         g = pos;
       }
-    }
-  } else {
-    const long long t = (long long)(blockIdx.x - deepBlocks) * blockDim.x + threadIdx.x;
-    const long long row = t / G;
-    q = int(t - row * G);
-    if (row < nB) {
+    } else {
+      const long long row = (t - nDeepItems) / G;
       for (int k = bPtr[row]; k < bPtr[row + 1]; k++) {
         const double w = bVal[k];
         const double* xs = x + (long long)bCol[k] * K + 4 * q;
@@ -406,18 +433,17 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
       }
       g = bGlobal[row];
     }
-  }
-  double rr[4] = {0, 0, 0, 0}, bb[4] = {0, 0, 0, 0};
-  if (g >= 0) {
+    if (g >= 0) {
 #pragma unroll
-    for (int ch = 0; ch < 4; ch++) {
-      const int c = 4 * q + ch;
-      if (c >= K) continue;
-      const double bv = b ? b[(long long)g * K + c] : 0.0;
-      const double v = mode == 0 ? bv - acc[ch] : acc[ch];
-      out[(long long)g * K + c] = v;
-      rr[ch] = v * v;
-      bb[ch] = bv * bv;
+      for (int ch = 0; ch < 4; ch++) {
+        const int c = 4 * q + ch;
+        if (c >= K) continue;
+        const double bv = b ? b[(long long)g * K + c] : 0.0;
+        const double v = mode == 0 ? bv - acc[ch] : acc[ch];
+        out[(long long)g * K + c] = v;
+        rr[ch] += v * v;
+        bb[ch] += bv * bv;
+      }
     }
   }
   if (!partials) return;
@@ -517,27 +543,28 @@ template <typename T, int W>
 void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s) {
   if (B.nb == 0) return;
   const int G = KP / W;
-  const size_t smem = size_t(B.maxBlock) * KP * sizeof(T);
-  if (B.nSub > 0)
-    k_bsolve_interior<T, W><<<B.nSub, 256, smem, s>>>(B.subPtr, B.invOff, B.inv, B.posGlobal, B.scale, B.bdPtr, B.bdCol, B.bdVal,
-                                                      rhs, x, B.y, KP, G);
+  k_bs_rhs<T, W><<<nblk((long long)B.nb * G), 256, 0, s>>>(B.nb, B.posGlobal, B.scale, B.bdPtr, B.bdCol, B.bdVal, rhs, x, B.rhat,
+                                                            KP, G);
+  if (B.nSubTasks > 0)
+    k_bs_gemv<T, W><<<B.nSubTasks, 256, 0, s>>>(B.subTasks, B.subPtr, B.invOff, B.inv, B.rhat, B.y, 0, B.nI, 0, nullptr, nullptr,
+                                                nullptr, nullptr, KP, G);
   if (B.nS > 0) {
-    k_bsolve_separator_rhs<T, W><<<nblk((long long)B.nS * G), 256, 0, s>>>(B.nI, B.nS, B.posGlobal, B.scale, B.bdPtr, B.bdCol,
-                                                                         B.bdVal, B.asiPtr, B.asiCol, B.asiVal, rhs, x, B.y,
-                                                                         B.t, KP, G);
-    k_bsolve_separator<T, W><<<nblk((long long)B.nS * 32), 256, 0, s>>>(B.nI, B.nS, B.sinv, B.t, B.posGlobal, B.scale, B.xs, x,
-                                                                      KP, G);
+    k_bs_sep_rhs<T, W><<<nblk((long long)B.nS * G), 256, 0, s>>>(B.nI, B.nS, B.asiPtr, B.asiCol, B.asiVal, B.rhat, B.y, B.t, KP, G);
+    const int chunkLen = (B.nS + B.schurChunks - 1) / B.schurChunks;
+    dim3 grid(B.nSchurTasks, B.schurChunks);
+    k_bs_gemv<T, W><<<grid, 256, 0, s>>>(B.schurTasks, B.schurPtr, B.schurOff, B.sinv, B.t, B.part, 1, B.nS, chunkLen, nullptr,
+                                         nullptr, nullptr, nullptr, KP, G);
+    k_bs_sep_sum<T, W><<<nblk((long long)B.nS * G), 256, 0, s>>>(B.nI, B.nS, B.schurChunks, B.part, B.posGlobal, B.scale, B.xs, x,
+                                                                  KP, G);
+    if (B.nI > 0) {
+      k_bs_coupling<T, W><<<nblk((long long)B.nI * G), 256, 0, s>>>(B.nI, B.aisPtr, B.aisCol, B.aisVal, B.xs, B.z, KP, G);
+      k_bs_gemv<T, W><<<B.nSubTasks, 256, 0, s>>>(B.subTasks, B.subPtr, B.invOff, B.inv, B.z, nullptr, 2, B.nI, 0, B.posGlobal,
+                                                  B.scale, B.y, x, KP, G);
+    }
+  } else if (B.nI > 0) {
+    // no separator: x_I = s * y
+    k_bs_sep_sum<T, W><<<nblk((long long)B.nI * G), 256, 0, s>>>(0, B.nI, 1, B.y, B.posGlobal, B.scale, nullptr, x, KP, G);
   }
-  if (B.nSub > 0)
-    k_bsolve_back<T, W><<<B.nSub, 256, smem, s>>>(B.subPtr, B.invOff, B.inv, B.posGlobal, B.scale, B.aisPtr, B.aisCol, B.aisVal,
-                                                  B.xs, B.y, x, KP, G);
-}
-template <typename T, int W>
-cudaError_t configure_boundary_smem(size_t bytes) {
-  const int b = int(std::max<size_t>(bytes, 48 * 1024));
-  cudaError_t e = cudaFuncSetAttribute(k_bsolve_interior<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_bsolve_back<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 template <typename T, int W>
 void launch_coarse_solve(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, cudaStream_t s) {
@@ -546,20 +573,20 @@ void launch_coarse_solve(int n, const double* ainv, const double* scale, const T
 }
 
 static inline int raw_groups(int K) { int G = 1; while (4 * G < K) G *= 2; return G; }
+// fixed grid (grid-stride): bounded number of partial sums, launch-shape-independent order
+static const int kRawBlocks = 148 * 8;
 void launch_raw_operator(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr, const int* bCol,
                          const double* bVal, const int* bGlobal, int nB, const double* b, const double* x, double* out, int K,
                          int mode, double* partials, double* sums, cudaStream_t s) {
   const int G = raw_groups(K);
-  const int db = nblk((long long)nRuns * 32 * G), bb = nblk((long long)nB * G);
-  if (db + bb == 0) return;
-  k_raw_operator<<<db + bb, 256, 0, s>>>(runs, nRuns, coef, planeStride, db, bPtr, bCol, bVal, bGlobal, nB, b, x, out, K, G,
-                                         mode, partials);
-  if (partials && sums) k_sum_partials<<<1, 256, 0, s>>>(partials, db + bb, K, sums);
+  const long long items = (long long)nRuns * 32 * G + (long long)nB * G;
+  if (items == 0) return;
+  const int blocks = int(std::min<long long>(kRawBlocks, nblk(items)));
+  k_raw_operator<<<blocks, 256, 0, s>>>(runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, out, K, G, mode,
+                                        partials);
+  if (partials && sums) k_sum_partials<<<1, 256, 0, s>>>(partials, blocks, K, sums);
 }
-int raw_operator_blocks(int nRuns, int nB, int K) {
-  const int G = raw_groups(K);
-  return nblk((long long)nRuns * 32 * G) + nblk((long long)nB * G);
-}
+int raw_operator_blocks(int nRuns, int nB, int K) { return kRawBlocks; }
 
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s) {
@@ -578,8 +605,7 @@ void launch_add_correction(double* x, const T* e, long long n, int K, int KP, cu
                                       const T*, T*, int, cudaStream_t);                                                  \
   template void launch_prolong_add<T, W>(const ProlongRun*, int, const T*, T*, int, cudaStream_t);                       \
   template void launch_boundary_solve<T, W>(const BoundaryDev<T>&, const T*, T*, int, cudaStream_t);                     \
-  template void launch_coarse_solve<T, W>(int, const double*, const double*, const T*, T*, int, cudaStream_t);     \
-  template cudaError_t configure_boundary_smem<T, W>(size_t);
+  template void launch_coarse_solve<T, W>(int, const double*, const double*, const T*, T*, int, cudaStream_t);
 GDTP_INSTANTIATE(float, 1)
 GDTP_INSTANTIATE(float, 4)
 GDTP_INSTANTIATE(double, 1)

@@ -10,13 +10,22 @@ struct RestrictRun;
 struct ProlongRun;
 
 // Device view of one level's exact boundary solver (see setup/bsolve.cpp).
+// Dense inverses are symmetric, stored row-major with rows padded to a multiple
+// of 4 entries; tasks are {matrix, first row quad, j begin, j end}, one per block.
 template <typename T>
 struct BoundaryDev {
-  int nb = 0, nSub = 0, nI = 0, nS = 0, maxBlock = 0;
-  const int* subPtr = nullptr;
+  int nb = 0, nSub = 0, nI = 0, nS = 0;
+  const int* subPtr = nullptr;          // subdomain row ranges (positions)
   const long long* invOff = nullptr;
   const T* inv = nullptr;
-  const int* posGlobal = nullptr;   // position -> global texel
+  const int4* subTasks = nullptr;
+  int nSubTasks = 0;
+  const int* schurPtr = nullptr;        // {0, nS}
+  const long long* schurOff = nullptr;  // {0}
+  const T* sinv = nullptr;
+  const int4* schurTasks = nullptr;
+  int nSchurTasks = 0, schurChunks = 1;
+  const int* posGlobal = nullptr;       // position -> global texel
   const T* scale = nullptr;
   const int *bdPtr = nullptr, *bdCol = nullptr;
   const T* bdVal = nullptr;
@@ -24,8 +33,7 @@ struct BoundaryDev {
   const T* aisVal = nullptr;
   const int *asiPtr = nullptr, *asiCol = nullptr;
   const T* asiVal = nullptr;
-  const T* sinv = nullptr;
-  T *y = nullptr, *t = nullptr, *xs = nullptr;  // work vectors (nI, nS, nS rows of KP)
+  T *rhat = nullptr, *y = nullptr, *z = nullptr, *t = nullptr, *xs = nullptr, *part = nullptr;  // work
 };
 
 template <typename T, int W>
@@ -40,8 +48,6 @@ template <typename T, int W>
 void launch_prolong_add(const ProlongRun* runs, int nRuns, const T* coarse, T* fine, int KP, cudaStream_t s);
 template <typename T, int W>
 void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s);
-template <typename T, int W>
-cudaError_t configure_boundary_smem(size_t bytes);
 template <typename T, int W>
 void launch_coarse_solve(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, cudaStream_t s);
 

@@ -254,7 +254,6 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
   DeviceArena& A = mg.arena;
   mg.levels.assign(L, LevelDev<T>());
   mg.KP = KP;
-  int maxBlockAll = 0;
   for (int l = 0; l < L; l++) {
     const GridLevel& G = h_.levels[l];
     const LevelCoefficients& C = coeffs_[l];
@@ -319,18 +318,45 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       B.nSub = bs.nSub;
       B.nI = bs.nI;
       B.nS = bs.nS;
-      int mb = 0;
-      for (int p = 0; p < bs.nSub; p++) mb = std::max(mb, bs.subPtr[p + 1] - bs.subPtr[p]);
-      B.maxBlock = mb;
-      maxBlockAll = std::max(maxBlockAll, mb);
-      std::vector<long long> off(bs.invOff.begin(), bs.invOff.end());
-      std::vector<T> inv(bs.inv.begin(), bs.inv.end()), scale(bs.scale.begin(), bs.scale.end()), sinv(bs.Sinv.begin(), bs.Sinv.end());
-      std::vector<int> pg(bs.nb);
-      for (int k = 0; k < bs.nb; k++) pg[k] = G.boundaryGlobal[bs.order[k]];
-      auto upT = [&](const std::vector<double>& v) { std::vector<T> t(v.begin(), v.end()); return (const T*)A.upload(t); };
+      // subdomain inverses, rows padded to a multiple of 4
+      std::vector<long long> off(bs.nSub + 1, 0);
+      std::vector<int4> tasks;
+      for (int p = 0; p < bs.nSub; p++) {
+        const int m = bs.subPtr[p + 1] - bs.subPtr[p], mp = (m + 3) & ~3;
+        off[p + 1] = off[p] + (long long)m * mp;
+        for (int rq = 0; rq < mp / 4; rq += 32) tasks.push_back(make_int4(p, rq, 0, m));
+      }
+      std::vector<T> inv(size_t(off[bs.nSub]), T(0));
+      for (int p = 0; p < bs.nSub; p++) {
+        const int m = bs.subPtr[p + 1] - bs.subPtr[p], mp = (m + 3) & ~3;
+        const double* src = &bs.inv[size_t(bs.invOff[p])];
+        for (int j = 0; j < m; j++)
+          for (int a = 0; a < m; a++) inv[size_t(off[p]) + size_t(j) * mp + a] = T(src[size_t(j) * m + a]);
+      }
       B.subPtr = A.upload(bs.subPtr);
       B.invOff = A.upload(off);
       B.inv = A.upload(inv);
+      B.subTasks = A.upload(tasks);
+      B.nSubTasks = (int)tasks.size();
+      // separator Schur complement inverse, same layout, j range split in chunks
+      if (bs.nS > 0) {
+        const int nS = bs.nS, nSp = (nS + 3) & ~3;
+        std::vector<T> sinv(size_t(nS) * nSp, T(0));
+        for (int j = 0; j < nS; j++)
+          for (int a = 0; a < nS; a++) sinv[size_t(j) * nSp + a] = T(bs.Sinv[size_t(j) * nS + a]);
+        std::vector<int4> st;
+        for (int rq = 0; rq < nSp / 4; rq += 32) st.push_back(make_int4(0, rq, 0, nS));
+        B.sinv = A.upload(sinv);
+        B.schurTasks = A.upload(st);
+        B.nSchurTasks = (int)st.size();
+        B.schurChunks = std::max(1, std::min(64, std::min(nS / 32 + 1, 600 / std::max(1, B.nSchurTasks))));
+        B.schurPtr = A.upload(std::vector<int>{0, nS});
+        B.schurOff = A.upload(std::vector<long long>{0});
+      }
+      std::vector<T> scale(bs.scale.begin(), bs.scale.end());
+      std::vector<int> pg(bs.nb);
+      for (int k = 0; k < bs.nb; k++) pg[k] = G.boundaryGlobal[bs.order[k]];
+      auto upT = [&](const std::vector<double>& v) { std::vector<T> t(v.begin(), v.end()); return (const T*)A.upload(t); };
       B.posGlobal = A.upload(pg);
       B.scale = A.upload(scale);
       B.bdPtr = A.upload(bs.BD.ptr);
@@ -342,10 +368,12 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       B.asiPtr = A.upload(bs.ASI.ptr);
       B.asiCol = A.upload(bs.ASI.col);
       B.asiVal = upT(bs.ASI.val);
-      B.sinv = A.upload(sinv);
+      B.rhat = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nb)) * KP * sizeof(T)));
       B.y = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nI)) * KP * sizeof(T)));
+      B.z = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nI)) * KP * sizeof(T)));
       B.t = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * KP * sizeof(T)));
       B.xs = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * KP * sizeof(T)));
+      B.part = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * B.schurChunks * KP * sizeof(T)));
     }
     // transfers to / from level l+1
     {
@@ -373,11 +401,7 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     }
   }
   if (!check(A.last, "multigrid upload")) return false;
-  // dynamic shared memory of the boundary subdomain kernels
-  const size_t smem = size_t(maxBlockAll) * KP * sizeof(T);
-  if (smem > 220 * 1024) { err_ = "boundary subdomain too large for shared memory at this RHS count"; return false; }
-  if (KP == 1) return check(dev::configure_boundary_smem<T, 1>(smem), "boundary smem");
-  return check(dev::configure_boundary_smem<T, 4>(smem), "boundary smem");
+  return true;
 }
 
 template bool DeviceSystem::build_multigrid<float>(Multigrid<float>&, int);
@@ -397,10 +421,10 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
     dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
     for (int sw = 0; sw < knobs.preSweeps; sw++) {
       const bool prof = profiling_ && l == 0 && sw == 0;
-      if (prof) cudaEventRecord(profEv_[0], s);
+      if (prof) cudaEventRecordWithFlags(profEv_[0], s, cudaEventRecordExternal);
       for (int c = 0; c < 4; c++)
         dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
-      if (prof) cudaEventRecord(profEv_[1], s);
+      if (prof) cudaEventRecordWithFlags(profEv_[1], s, cudaEventRecordExternal);
     }
     dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
     dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, D.r, C.b, KP, s);
@@ -600,6 +624,8 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
       profCount += 1;
       profMs += pm;
       profTexels = mg.levels[0].nDeep;
+    } else {
+      cudaGetLastError();  // timing unavailable: do not leave the error for the next caller
     }
   }
   if (x_host && !check(cudaMemcpyAsync(x_host, x64_, n * k * 8, cudaMemcpyDeviceToHost, s), "d2h x")) return false;
