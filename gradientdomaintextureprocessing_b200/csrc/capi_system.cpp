@@ -168,3 +168,10 @@ extern "C" int gdtp_system_device_bytes(const gdtp_system* s, int64_t* bytes) {
   *bytes = (int64_t)s->sys->deviceBytes();
   return GDTP_OK;
 }
+
+// Internal accessor for entry points compiled in other translation units (not exported).
+extern "C" __attribute__((visibility("hidden"))) int gdtp_system_device_view(const gdtp_system* s, const void** sys) {
+  if (!s || !s->sys || !sys) return fail(GDTP_ERR_INVALID, "null system handle");
+  *sys = s->sys.get();
+  return GDTP_OK;
+}

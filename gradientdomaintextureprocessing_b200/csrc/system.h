@@ -149,6 +149,10 @@ class DeviceSystem {
   // live timing of the level-0 pre-smoothing colour passes inside the captured
   // refinement graph: {launch groups timed, total ms, texels updated per group}
   double profCount = 0, profMs = 0, profTexels = 0;
+  // read-only views for entry points that bring their own buffers
+  const RawOperator& raw_system_operator() const { return rawA_; }
+  bool is_updated() const { return updated_; }
+  int num_texels() const { return h_.levels[0].numTexels; }
   int graphKernels = 0;         // kernel nodes in the refinement-step graph
 
  private:

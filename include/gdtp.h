@@ -124,6 +124,21 @@ int gdtp_solve_fp64(gdtp_system* s, const double* b, double* x, int k, double to
 /* Relative residuals ||b - A x|| / ||b|| per RHS (FP64 operator), host buffers. */
 int gdtp_residual(gdtp_system* s, const double* b, const double* x, int k, double* rel);
 
+/* Residual check that allocates nothing, for callers that may not allocate
+ * device memory when they need it (pre-planned render/simulation loops,
+ * stream-ordered pools that must not grow, hosts where cudaMalloc would stall
+ * their own work).  No counterpart in the reference.  Device buffers b_dev,
+ * x_dev (inputs) and r_dev (output residual b - A x), float64 numTexels*k;
+ * rel_host receives ||b - A x|| / ||b|| per right-hand side.  k <= 64: the
+ * norm reduction's scratch is a fixed ~1.2 MB static device array that every
+ * device loading the library holds until exit.  The first call on a device
+ * resolves that array's address (cudaGetSymbolAddress) and must come before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race; the call waits on `stream` before returning.  Calls no cudaMalloc or
+ * cudaFree. */
+int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_dev, double* r_dev, int k, double* rel_host,
+                         void* stream);
+
 /* Solver knobs: "pre_sweeps" "post_sweeps" "vcycles_per_refinement" "levels_used"; value as double. */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
 /* Device bytes held by the system (coefficients, vectors, coarse factor). */
