@@ -42,9 +42,9 @@ WIDTH = 2048
 LAMBDA, SHARP, TOL, K = 1e-3, 2.0, 1e-6, 3
 
 
-def workload():
+def workload(width: int = WIDTH):
     from gradientdomaintextureprocessing_b200 import meshgen
-    return meshgen.icosphere_atlas(WIDTH, WIDTH, subdiv=6, seed=0)
+    return meshgen.icosphere_atlas(width, width, subdiv=6, seed=0)
 
 
 class ClockSampler:
@@ -147,6 +147,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-solves", type=int, default=0,
+                    help="profiling run: build the workload, run this many solves and exit (for ncu launch lists)")
+    ap.add_argument("--width", type=int, default=WIDTH, help="texture resolution (profiling of smaller cases)")
     args = ap.parse_args()
 
     rank, world, local, dist = dist_setup(args.gpus)
@@ -167,13 +170,18 @@ def main():
     import ctypes as C
 
     t0 = time.time()
-    mesh = workload()
+    mesh = workload(args.width)
     h = InitializeHierarchy(mesh, levels=4)
     s = System(h, device=local)
     s.update(LAMBDA, 1.0)
     f = texel_signal(h, mesh["texture"])
     b_host = texture_filtering_rhs(s, f, LAMBDA, SHARP)
     setup_s = time.time() - t0
+    if args.profile_solves:
+        for _ in range(args.profile_solves):
+            x, r = s.solve(b_host, tol=TOL)
+            print(json.dumps(r), flush=True)
+        return
     n0 = b_host.shape[0]
     L = _lib.lib()
 
