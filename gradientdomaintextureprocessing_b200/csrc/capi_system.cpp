@@ -122,6 +122,17 @@ extern "C" int gdtp_solve(gdtp_system* s, const double* b, double* x, int k, dou
   return rep.relMax <= tol ? GDTP_OK : fail(GDTP_ERR_NOT_CONVERGED, "relative residual above tolerance after max_iters");
 }
 
+extern "C" int gdtp_solve_ex(gdtp_system* s, const double* b, double* x, int k, double tol, int max_iters, int flags,
+                             gdtp_report* report) {
+  GDTP_SYS_CHECK(s);
+  if (!b || !x || !(tol > 0) || max_iters < 0 || (flags & ~GDTP_ZERO_GUESS)) return fail(GDTP_ERR_INVALID, "gdtp_solve_ex: bad arguments");
+  SolveReport rep;
+  if (!s->sys->solve_mixed(b, x, nullptr, nullptr, k, tol, max_iters, nullptr, rep, (flags & GDTP_ZERO_GUESS) != 0))
+    return sys_fail(s, GDTP_ERR_CUDA);
+  fill_report(report, rep);
+  return rep.relMax <= tol ? GDTP_OK : fail(GDTP_ERR_NOT_CONVERGED, "relative residual above tolerance after max_iters");
+}
+
 extern "C" int gdtp_solve_device(gdtp_system* s, const double* b_dev, double* x_dev, int k, double tol, int max_iters, void* stream,
                                  gdtp_report* report) {
   GDTP_SYS_CHECK(s);
@@ -156,10 +167,28 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
   const int v = int(value);
   if (k == "pre_sweeps" && v >= 0 && v <= 16) kn.preSweeps = v;
   else if (k == "post_sweeps" && v >= 0 && v <= 16) kn.postSweeps = v;
+  else if (k == "pre_boundary" && (v == 0 || v == 1)) kn.preBoundary = v;
+  else if (k == "post_boundary" && (v == 0 || v == 1)) kn.postBoundary = v;
   else if (k == "max_block" && v >= 16 && v <= 1024) kn.maxBlock = v;
   else if (k == "max_coarse" && v >= 16 && v <= 12000) kn.maxCoarse = v;
   else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
   s->sys->invalidate_graph();
+  return GDTP_OK;
+}
+
+extern "C" int gdtp_system_autotune(gdtp_system* s, const double* b, int k, double tol, double* knobs_out) {
+  GDTP_SYS_CHECK(s);
+  if (!b || !(tol > 0)) return fail(GDTP_ERR_INVALID, "gdtp_system_autotune: bad arguments");
+  SolverKnobs best;
+  double secs = 0;
+  if (!s->sys->autotune(b, k, tol, best, secs)) return sys_fail(s, GDTP_ERR_CUDA);
+  if (knobs_out) {
+    knobs_out[0] = best.preSweeps;
+    knobs_out[1] = best.postSweeps;
+    knobs_out[2] = best.preBoundary;
+    knobs_out[3] = best.postBoundary;
+    knobs_out[4] = secs;
+  }
   return GDTP_OK;
 }
 

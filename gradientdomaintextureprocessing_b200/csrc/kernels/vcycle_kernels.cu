@@ -393,7 +393,8 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
                                                       int planeStride, const int* __restrict__ bPtr, const int* __restrict__ bCol,
                                                       const double* __restrict__ bVal, const int* __restrict__ bGlobal, int nB,
                                                       const double* __restrict__ b, const double* __restrict__ x,
-                                                      double* __restrict__ out, int K, int G, int mode, double* __restrict__ partials) {
+                                                      double* __restrict__ out, int K, int G, int mode, double* __restrict__ partials,
+                                                      float* __restrict__ out32 = nullptr, int KP = 0) {
   // grid-stride over deep items (runs x 32 x G) then boundary items (rows x G);
   // the stride is a multiple of G, so every thread keeps one channel group q
   const long long nDeepItems = (long long)nRuns * 32 * G, nItems = nDeepItems + (long long)nB * G;
@@ -440,10 +441,13 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
         if (c >= K) continue;
         const double bv = b ? b[(long long)g * K + c] : 0.0;
         const double v = mode == 0 ? bv - acc[ch] : acc[ch];
-        out[(long long)g * K + c] = v;
+        if (out32) out32[(long long)g * KP + c] = float(v);
+        else out[(long long)g * K + c] = v;
         rr[ch] += v * v;
         bb[ch] += bv * bv;
       }
+      if (out32)  // zero the padding channels of this group
+        for (int c = max(K, 4 * q); c < min(KP, 4 * q + 4); c++) out32[(long long)g * KP + c] = 0.f;
     }
   }
   if (!partials) return;
@@ -587,6 +591,17 @@ void launch_raw_operator(const ColourRun* runs, int nRuns, const double* coef, i
   if (partials && sums) k_sum_partials<<<1, 256, 0, s>>>(partials, blocks, K, sums);
 }
 int raw_operator_blocks(int nRuns, int nB, int K) { return kRawBlocks; }
+void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr,
+                             const int* bCol, const double* bVal, const int* bGlobal, int nB, const double* b, const double* x,
+                             float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s) {
+  const int G = raw_groups(K);
+  const long long items = (long long)nRuns * 32 * G + (long long)nB * G;
+  if (items == 0) return;
+  const int blocks = int(std::min<long long>(kRawBlocks, nblk(items)));
+  k_raw_operator<<<blocks, 256, 0, s>>>(runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, nullptr, K, G, 0,
+                                        partials, rhs32, KP);
+  if (partials && sums) k_sum_partials<<<1, 256, 0, s>>>(partials, blocks, K, sums);
+}
 
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s) {

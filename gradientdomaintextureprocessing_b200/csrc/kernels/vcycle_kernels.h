@@ -55,6 +55,10 @@ void launch_raw_operator(const ColourRun* runs, int nRuns, const double* coef, i
                          const double* bVal, const int* bGlobal, int nB, const double* b, const double* x, double* out, int K,
                          int mode, double* partials, double* sums, cudaStream_t s);
 int raw_operator_blocks(int nRuns, int nB, int K);
+// r = b - A x written as the padded FP32 right-hand side (n x KP), plus norms
+void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr,
+                             const int* bCol, const double* bVal, const int* bGlobal, int nB, const double* b, const double* x,
+                             float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s);
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s);
 template <typename T>

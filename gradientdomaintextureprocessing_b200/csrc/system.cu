@@ -418,7 +418,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
     LevelDev<T>& D = mg.levels[l];
     LevelDev<T>& C = mg.levels[l + 1];
     if (l > 0) cudaMemsetAsync(D.x, 0, size_t(D.n) * KP * sizeof(T), s);
-    dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
+    if (knobs.preBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
     for (int sw = 0; sw < knobs.preSweeps; sw++) {
       const bool prof = profiling_ && l == 0 && sw == 0;
       if (prof) cudaEventRecordWithFlags(profEv_[0], s, cudaEventRecordExternal);
@@ -433,7 +433,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
   for (int l = L - 2; l >= 0; l--) {
     LevelDev<T>& D = mg.levels[l];
     dev::launch_prolong_add<T, W>(D.pruns, D.nPRuns, mg.levels[l + 1].x, D.x, KP, s);
-    dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
+    if (knobs.postBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
     for (int sw = 0; sw < knobs.postSweeps; sw++)
       for (int c = 3; c >= 0; c--)
         dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
@@ -534,7 +534,7 @@ bool DeviceSystem::vcycle_host(float* x, const float* rhs, int k) {
 }
 
 bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const double* b_dev, double* x_dev, int k, double tol,
-                               int maxIters, cudaStream_t userStream, SolveReport& rep) {
+                               int maxIters, cudaStream_t userStream, SolveReport& rep, bool zeroGuess) {
   if (!err_.empty()) return false;
   cudaSetDevice(device_);
   if (!updated_) { err_ = "solve before update"; return false; }
@@ -560,7 +560,8 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
   const double* B = b_dev ? b_dev : b64_;
   double* X = x_dev ? x_dev : x64_;
   if (b_host && !check(cudaMemcpyAsync(b64_, b_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d b")) return false;
-  if (x_host && !check(cudaMemcpyAsync(x64_, x_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d x")) return false;
+  if (x_host && !zeroGuess && !check(cudaMemcpyAsync(x64_, x_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d x")) return false;
+  if (zeroGuess && !check(cudaMemsetAsync(X, 0, n * k * 8, s), "zero x")) return false;
   // refinement step graph: rhs <- r, e <- V(rhs), x += e, r <- b - A x (+ norms)
   if (!iterGraph_ || iterGraphK_ != k || iterGraphB_ != B || iterGraphX_ != X) {
     if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; }
@@ -572,12 +573,12 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     profiling_ = true;
     if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
     LevelDev<float>& D0 = mg.levels[0];
-    dev::launch_pack_rhs<float>(r64_, D0.b, (long long)n, k, mg.KP, s);
     cudaMemsetAsync(D0.x, 0, n * mg.KP * sizeof(float), s);
     if (mg.KP == 1) vcycle<float, 1>(mg, s); else vcycle<float, 4>(mg, s);
     dev::launch_add_correction<float>(X, D0.x, (long long)n, k, mg.KP, s);
-    dev::launch_raw_operator(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
-                             rawA_.bGlobal, rawA_.nB, B, X, r64_, k, 0, partials_, sums_, s);
+    // r = b - A x, written straight into the FP32 right-hand side of the next V-cycle
+    dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
+                                 rawA_.bGlobal, rawA_.nB, B, X, D0.b, k, mg.KP, partials_, sums_, s);
     profiling_ = false;
     if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
     {
@@ -598,8 +599,12 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     iterGraphB_ = B;
     iterGraphX_ = X;
   }
-  // initial residual
-  if (!raw_apply_dev(rawA_, B, X, r64_, k, 0, s, sumsHost_)) return false;
+  // initial residual, straight into the FP32 right-hand side
+  dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
+                               rawA_.bGlobal, rawA_.nB, B, X, mg.levels[0].b, k, mg.KP, partials_, sums_, s);
+  if (!check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
+      !check(cudaStreamSynchronize(s), "initial residual"))
+    return false;
   rep = SolveReport();
   rep.rel.assign(k, 0.0);
   auto rel_max = [&]() {
@@ -640,6 +645,40 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
   rep.vcycles = it;
   rep.relMax = rm;
   rep.seconds = ms * 1e-3;
+  return true;
+}
+
+bool DeviceSystem::autotune(const double* b, int k, double tol, SolverKnobs& best, double& bestSeconds) {
+  if (!err_.empty()) return false;
+  const size_t n = h_.levels[0].numTexels;
+  std::vector<double> x(n * k);
+  const SolverKnobs base = knobs;
+  bestSeconds = 1e300;
+  best = base;
+  // candidates: deep sweeps before / after the coarse correction and where the
+  // exact boundary solve goes (after the correction is required for accuracy
+  // on the way up; before it is optional)
+  const int cand[][4] = {{1, 1, 0, 1}, {1, 2, 0, 1}, {2, 1, 0, 1}, {2, 2, 0, 1}, {2, 3, 0, 1}, {3, 3, 0, 1},
+                         {2, 2, 1, 1}, {1, 1, 1, 1}};
+  for (const auto& c : cand) {
+    knobs = base;
+    knobs.preSweeps = c[0];
+    knobs.postSweeps = c[1];
+    knobs.preBoundary = c[2];
+    knobs.postBoundary = c[3];
+    invalidate_graph();
+    double t = 1e300;
+    for (int rep = 0; rep < 3; rep++) {  // first run captures the graph
+      std::fill(x.begin(), x.end(), 0.0);
+      SolveReport r;
+      if (!solve_mixed(b, x.data(), nullptr, nullptr, k, tol, 60, nullptr, r)) return false;
+      if (r.relMax > tol) { t = 1e300; break; }
+      if (rep > 0) t = std::min(t, r.seconds);
+    }
+    if (t < bestSeconds) { bestSeconds = t; best = knobs; }
+  }
+  knobs = best;
+  invalidate_graph();
   return true;
 }
 

@@ -107,6 +107,7 @@ struct RawOperator {
 
 struct SolverKnobs {
   int preSweeps = 2, postSweeps = 2;
+  int preBoundary = 0, postBoundary = 1;  // exact boundary solve before the pre / post sweeps
   int maxBlock = 384;                   // boundary subdomain size
   int maxCoarse = 2600;                 // coarsest level size limit (texels)
 };
@@ -137,9 +138,12 @@ class DeviceSystem {
   // host in/out, k right-hand sides (tight n x k)
   bool apply(int which, const double* x, double* y, int k);
   bool solve_mixed(const double* b_host, double* x_host, const double* b_dev, double* x_dev, int k, double tol, int maxIters,
-                   cudaStream_t userStream, SolveReport& rep);
+                   cudaStream_t userStream, SolveReport& rep, bool zeroGuess = false);
   bool solve_fp64(const double* b_host, double* x_host, int k, double tol, int maxIters, SolveReport& rep);
   bool vcycle_host(float* x, const float* rhs, int k);
+  // times full solves of b (host, n x k) for a grid of smoother settings and
+  // keeps the fastest that converges; returns the chosen knobs
+  bool autotune(const double* b, int k, double tol, SolverKnobs& best, double& bestSeconds);
   bool residual_host(const double* b, const double* x, int k, double* rel);
 
   SolverKnobs knobs;

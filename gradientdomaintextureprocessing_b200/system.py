@@ -56,6 +56,14 @@ class System:
     def set(self, knob: str, value: float) -> None:
         _lib.check(_lib.lib().gdtp_system_set(self._s, knob.encode(), float(value)))
 
+    def autotune(self, b: np.ndarray, tol: float = 1e-6) -> dict:
+        """Picks the fastest converging smoother setting for solves like ``b``."""
+        b, k = self._vec(b, np.float64)
+        out = np.zeros(5)
+        _lib.check(_lib.lib().gdtp_system_autotune(self._s, _lib.ptr(b), k, float(tol), _lib.ptr(out)))
+        return {"pre_sweeps": int(out[0]), "post_sweeps": int(out[1]), "pre_boundary": int(out[2]),
+                "post_boundary": int(out[3]), "seconds": float(out[4])}
+
     def device_bytes(self) -> int:
         b = C.c_int64()
         _lib.check(_lib.lib().gdtp_system_device_bytes(self._s, C.byref(b)))

@@ -115,6 +115,10 @@ typedef struct gdtp_report {
  * VCycle calls (TextureFiltering.cpp:562-579) and, for accuracy, the
  * --useDirectSolver path (TextureFiltering.cpp:651-655, 704-707). */
 int gdtp_solve(gdtp_system* s, const double* b, double* x, int k, double tol, int max_iters, gdtp_report* report);
+/* As gdtp_solve with flags: GDTP_ZERO_GUESS starts from x = 0 and treats x as
+ * output only (no host-to-device copy of x). */
+#define GDTP_ZERO_GUESS 1
+int gdtp_solve_ex(gdtp_system* s, const double* b, double* x, int k, double tol, int max_iters, int flags, gdtp_report* report);
 /* Same on device float64 buffers (no host copies); stream = cudaStream_t or NULL. */
 int gdtp_solve_device(gdtp_system* s, const double* b_dev, double* x_dev, int k, double tol, int max_iters,
                       void* stream, gdtp_report* report);
@@ -139,8 +143,16 @@ int gdtp_residual(gdtp_system* s, const double* b, const double* x, int k, doubl
 int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_dev, double* r_dev, int k, double* rel_host,
                          void* stream);
 
-/* Solver knobs: "pre_sweeps" "post_sweeps" "vcycles_per_refinement" "levels_used"; value as double. */
+/* Solver knobs (value as double): "pre_sweeps", "post_sweeps" (deep colour sweeps
+ * per smoothing, default 2/2), "pre_boundary", "post_boundary" (exact boundary
+ * solve before the pre / post sweeps, default 0/1), "max_block" (boundary
+ * subdomain size, next update), "max_coarse" (coarsest level size, next update). */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
+/* Autotuner: times complete solves of b (host float64 numTexels*k) to tol for a
+ * set of smoother settings (sweeps and boundary-solve placement), keeps the
+ * fastest that converges.  knobs_out (optional, 5 doubles): pre sweeps, post
+ * sweeps, pre boundary, post boundary, best solve seconds. */
+int gdtp_system_autotune(gdtp_system* s, const double* b, int k, double tol, double* knobs_out);
 /* Device bytes held by the system (coefficients, vectors, coarse factor). */
 int gdtp_system_device_bytes(const gdtp_system* s, int64_t* bytes);
 
