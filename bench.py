@@ -40,6 +40,9 @@ sys.path.insert(0, ROOT)
 METRIC = "Mtexels solved/s at 1e-6 rel. residual, mixed vs FP64; p50/p99 latency"
 WIDTH = 2048
 LAMBDA, SHARP, TOL, K = 1e-3, 2.0, 1e-6, 3
+# DRAM bytes (read + write) per deep texel of one level-0 4-colour sweep, from an
+# ncu capture of k_gs_colour on this workload (cold L2; profiles/gs_colour_icosphere2048.md)
+NCU_SWEEP_BYTES_PER_DEEP_TEXEL = 4 * 48.68e6 / 1432006
 
 
 def workload(width: int = WIDTH):
@@ -52,17 +55,21 @@ class ClockSampler:
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.samples = []   # (host time, fields)
         self.proc = None
+        self.window = None
 
     def __enter__(self):
         q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t_end = time.time() + 10.0   # the timed region starts once sampling runs
+            while not self.samples and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.02)
         except FileNotFoundError:
             self.proc = None
         return self
@@ -71,10 +78,17 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 7:
-                self.samples.append(parts)
+                self.samples.append((time.time(), parts))
+
+    def mark(self, t0: float, t1: float):
+        """Host-time window of the timed region."""
+        self.window = (t0, t1)
 
     def __exit__(self, *a):
         if self.proc:
+            t_end = time.time() + 0.5   # let the sample that follows the region arrive
+            while self.window and time.time() < t_end and not any(t > self.window[1] for t, _ in self.samples):
+                time.sleep(0.02)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -82,13 +96,21 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.samples:
+        samples = self.samples
+        if self.window and samples:
+            # samples inside the timed region, widened by one sampling period on
+            # each side so that a region shorter than the period still has one
+            t0, t1 = self.window
+            inside = [s for s in samples if t0 - 0.1 <= s[0] <= t1 + 0.1]
+            samples = inside or sorted(samples, key=lambda s: min(abs(s[0] - t0), abs(s[0] - t1)))[:2]
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        f = [p for _, p in samples]
+        sm = [float(p[0]) for p in f if p[0].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].strip() == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(self.samples[0][1]),
-                "reasons": reasons, "samples": len(self.samples)}
+        reasons = sorted({names[i] for p in f for i in range(4) if p[3 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(f[0][1]),
+                "reasons": reasons, "samples": len(f)}
 
 
 def dist_setup(n_gpus: int):
@@ -211,6 +233,7 @@ def main():
     lat, iters, resid = [], [], []
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     with ClockSampler(local) as clocks:
+        t_host0 = time.time()
         ev[0].record(stream)
         for i in range(args.steps):
             it, r = device_step()
@@ -218,6 +241,7 @@ def main():
             iters.append(it)
             resid.append(r)
         torch.cuda.synchronize()
+        clocks.mark(t_host0, time.time())
     for i in range(args.steps):
         lat.append(ev[i].elapsed_time(ev[i + 1]))
     total_ms = ev[0].elapsed_time(ev[-1])
@@ -295,7 +319,9 @@ def main():
                    "d2h_bytes_per_step": int(b_host.nbytes), "api": "gdtp_solve_ex (zero initial guess, pinned host buffers)"},
            "roofline": {"bound": "hbm", "kernel": "level-0 4-colour Gauss-Seidel sweep (k_gs_colour x4)",
                         "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": (achieved / peak) if achieved else None, "traffic": None,
+                        "frac": (achieved / peak) if achieved else None,
+                        "traffic": texels * NCU_SWEEP_BYTES_PER_DEEP_TEXEL if texels else None,
+                        "traffic_source": "ncu dram__bytes_read+write per deep texel x deep texels (cold L2)",
                         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                         "bytes_per_launch": sweep_bytes, "ms_per_launch": sweep_ms},
            "gpu_launches": launches,
