@@ -24,7 +24,8 @@ static int sys_fail(gdtp_system* s, int code) { return fail(code, s->sys->error(
 extern "C" int gdtp_system_create(gdtp_hierarchy* h, int device, int metric_mode, const double* parameter_metric,
                                   const double* vertices, int64_t nv, gdtp_system** out) {
   if (!h || !out) return fail(GDTP_ERR_INVALID, "gdtp_system_create: null argument");
-  if (metric_mode != 0 && !parameter_metric) return fail(GDTP_ERR_INVALID, "gdtp_system_create: unknown metric mode");
+  if (metric_mode != 0 && metric_mode != 1 && !parameter_metric)
+    return fail(GDTP_ERR_INVALID, "gdtp_system_create: unknown metric mode");
   *out = nullptr;
   std::unique_ptr<gdtp_system> s(new gdtp_system());
   s->h = h;
@@ -32,6 +33,18 @@ extern "C" int gdtp_system_create(gdtp_hierarchy* h, int device, int metric_mode
   if (vertices) {
     if (nv != mesh.nv()) return fail(GDTP_ERR_INVALID, "gdtp_system_create: vertex count differs from the hierarchy's mesh");
     mesh.vertices.assign(vertices, vertices + nv * 3);
+  }
+  std::vector<double> uniform;
+  if (!parameter_metric && metric_mode == 1) {  // uniform metric, per mesh triangle
+    std::vector<M2> G, P;
+    if (!surface_metric(mesh, 1, true, G) || !gdtp::parameter_metric(mesh, G, P))
+      return fail(GDTP_ERR_SETUP, "gdtp_system_create: degenerate texture triangles");
+    uniform.resize(4 * P.size());
+    for (size_t t = 0; t < P.size(); t++) {
+      uniform[4 * t] = P[t].c[0][0]; uniform[4 * t + 1] = P[t].c[0][1];
+      uniform[4 * t + 2] = P[t].c[1][0]; uniform[4 * t + 3] = P[t].c[1][1];
+    }
+    parameter_metric = uniform.data();
   }
   s->sys.reset(new DeviceSystem(h->h, h->be, device));
   if (!s->sys->ok()) return fail(GDTP_ERR_CUDA, s->sys->error());
@@ -169,7 +182,7 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
   else if (k == "post_sweeps" && v >= 0 && v <= 16) kn.postSweeps = v;
   else if (k == "pre_boundary" && (v == 0 || v == 1)) kn.preBoundary = v;
   else if (k == "post_boundary" && (v == 0 || v == 1)) kn.postBoundary = v;
-  else if (k == "max_block" && v >= 16 && v <= 1024) kn.maxBlock = v;
+  else if (k == "max_block" && v >= 16 && v <= dev::kBoundaryChunkMax) kn.maxBlock = v;
   else if (k == "max_coarse" && v >= 16 && v <= 12000) kn.maxCoarse = v;
   else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
   s->sys->invalidate_graph();

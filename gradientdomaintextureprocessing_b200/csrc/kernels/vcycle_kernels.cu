@@ -181,36 +181,20 @@ __global__ void __launch_bounds__(256) k_prolong_add(const ProlongRun* __restric
 
 // ----------------------------------------------------------------------------
 // Exact boundary-block solve  x_B = BB^-1 (rhs_B - BD x) over the subdomain /
-// separator split (scaled by s = BB_ii^-1/2):
-//   r^ = s (rhs - BD x)                       k_bs_rhs        (sparse, all rows)
-//   y  = Inv_p r^_I                           k_bs_gemv mode 0 (dense, batched)
-//   t  = r^_S - A_SI y                        k_bs_sep_rhs    (sparse)
-//   xs = Sinv t                               k_bs_gemv mode 1 (dense, j-chunked) + k_bs_sep_sum
-//   z  = A_IS xs                              k_bs_coupling   (sparse)
-//   x_I = s (y - Inv_p z)                     k_bs_gemv mode 2 (dense, scatter)
-// The dense products are memory-bound: every inverse is symmetric and stored
-// row-major with rows padded to a multiple of 4, so lane l of a warp reads rows
-// 4l..4l+3 of matrix row j with one vector load and a warp reads contiguous
-// memory; the 8 warps of a block take interleaved j and are reduced in shared
-// memory in a fixed order (deterministic).
+// separator split (scaled by s = BB_ii^-1/2), three launches per level:
+//   k_bs_dense mode 0:  y  = Inv_p r^_I,  r^ = s (rhs - BD x) built in the prologue
+//   k_bs_dense mode 1:  xs = Sinv t,      t  = r^_S - A_SI y built in the prologue;
+//                       x_S = s xs
+//   k_bs_back:          x_I = s (y - W_p xs),  W_p = Inv_p A_{I_p,S} (m x t_p)
+// The dense products are memory-bound streams of the symmetric inverses,
+// stored row-major with rows padded to a multiple of 4: lane l of a warp reads
+// rows 4l..4l+3 of matrix row j with one vector load, so a warp reads
+// contiguous memory.  A block takes 128 rows of one matrix and a chunk of its
+// j range (8 warps interleave j); the chunks of a row group (blockIdx.y) write
+// partial sums and the last block to finish adds them in chunk order, so the
+// result does not depend on scheduling.  Chunking keeps the dependent-load
+// chain of each warp short on the small coarse levels.
 // ----------------------------------------------------------------------------
-template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bs_rhs(int nb, const int* __restrict__ posGlobal, const T* __restrict__ scale,
-                                                const int* __restrict__ bdPtr, const int* __restrict__ bdCol,
-                                                const T* __restrict__ bdVal, const T* __restrict__ rhs, const T* __restrict__ x,
-                                                T* __restrict__ rhat, int KP, int G) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long k = t / G;
-  if (k >= nb) return;
-  const int q = int(t - k * G), off = q * W;
-  Vec<T, W> acc = vload<T, W>(rhs + (long long)posGlobal[k] * KP + off);
-  for (int j = bdPtr[k]; j < bdPtr[k + 1]; j++) axpy(acc, -bdVal[j], vload<T, W>(x + (long long)bdCol[j] * KP + off));
-  const T sc = scale[k];
-#pragma unroll
-  for (int c = 0; c < W; c++) acc.v[c] *= sc;
-  vstore<T, W>(rhat + k * KP + off, acc);
-}
-
 template <typename T>
 struct Quad;
 template <>
@@ -222,40 +206,46 @@ struct __align__(32) Quad<double> {
   double v[4];
 };
 
-// task = {matrix, first row quad, j begin, j end}; rows of the block's matrix
-// start at rowPtr[matrix] in the vectors.  mode:
-//   0: out[row] = sum_j M[j][row] vin[j]
-//   1: out[chunk = blockIdx.y][row] = partial sum over this task's j range
-//   2: x[posGlobal[row]] = scale[row] * (y[row] - sum)
 template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bs_gemv(const int4* __restrict__ tasks, const int* __restrict__ rowPtr,
-                                                 const long long* __restrict__ matOff, const T* __restrict__ mat,
-                                                 const T* __restrict__ vin, T* __restrict__ out, int mode, int nRowsTotal,
-                                                 int chunkLen, const int* __restrict__ posGlobal, const T* __restrict__ scale,
-                                                 const T* __restrict__ y, T* __restrict__ x, int KP, int G) {
+__global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode, const T* __restrict__ rhs, T* __restrict__ x, int KP,
+                                                  int G) {
   __shared__ T red[8][32][4 * W];
-  const int4 task = tasks[blockIdx.x];
-  const int p = task.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rq = task.y + lane;
-  const int r0 = rowPtr[p], m = rowPtr[p + 1] - r0, mp = (m + 3) & ~3;
-  int j0 = task.z, j1 = task.w;
-  if (mode == 1) {  // chunk of the j range taken by this grid row
-    j0 = task.z + blockIdx.y * chunkLen;
-    j1 = min(task.w, j0 + chunkLen);
-  }
-  const T* M = mat + matOff[p];
+  __shared__ Vec<T, W> vin[kBoundaryChunkMax];
+  __shared__ int lastFlag;
+  const int4 task = (mode == 0 ? B.subTasks : B.schurTasks)[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rq = task.y + lane;
+  const int r0 = mode == 0 ? B.subPtr[task.x] : 0;
+  const int m = mode == 0 ? B.subPtr[task.x + 1] - r0 : B.nS, mp = (m + 3) & ~3;
+  const T* M = mode == 0 ? B.inv + B.invOff[task.x] : B.sinv;
+  const int nch = gridDim.y, chunk = blockIdx.y;
+  const int clen = (m + nch - 1) / nch, j0 = min(m, chunk * clen), j1 = min(m, j0 + clen);
   const bool active = 4 * rq < m;
+  T* part = mode == 0 ? B.subPart : B.schurPart;
   for (int q = 0; q < G; q++) {
     const int off = q * W;
+    // prologue: the chunk's input vector (scaled boundary right-hand side)
+    for (int j = j0 + (int)threadIdx.x; j < j1; j += blockDim.x) {
+      const int k = (mode == 0 ? r0 : B.nI) + j;  // solver position
+      Vec<T, W> acc = vload<T, W>(rhs + (long long)B.posGlobal[k] * KP + off);
+      for (int e = B.bdPtr[k]; e < B.bdPtr[k + 1]; e++) axpy(acc, -B.bdVal[e], vload<T, W>(x + (long long)B.bdCol[e] * KP + off));
+      const T sc = B.scale[k];
+#pragma unroll
+      for (int c = 0; c < W; c++) acc.v[c] *= sc;
+      if (mode == 1)
+        for (int e = B.asiPtr[j]; e < B.asiPtr[j + 1]; e++) axpy(acc, -B.asiVal[e], vload<T, W>(B.y + (long long)B.asiCol[e] * KP + off));
+      vin[j - j0] = acc;
+    }
+    __syncthreads();
     T acc[4][W];
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
       for (int c = 0; c < W; c++) acc[a][c] = 0;
     if (active) {
-#pragma unroll 4
+#pragma unroll 8
       for (int j = j0 + warp; j < j1; j += 8) {
         const Quad<T> mq = *reinterpret_cast<const Quad<T>*>(M + (long long)j * mp + 4 * rq);
-        const Vec<T, W> v = vload<T, W>(vin + (long long)(r0 + j) * KP + off);
+        const Vec<T, W> v = vin[j - j0];
 #pragma unroll
         for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -271,83 +261,82 @@ __global__ void __launch_bounds__(256) k_bs_gemv(const int4* __restrict__ tasks,
 #pragma unroll
       for (int a = 0; a < 4; a++) {
         const int row = 4 * rq + a;
-        if (row < m) {
-          Vec<T, W> sum;
+        if (row >= m) continue;
+        Vec<T, W> sum;
 #pragma unroll
-          for (int c = 0; c < W; c++) {
-            T v = 0;
-            for (int w = 0; w < 8; w++) v += red[w][lane][a * W + c];
-            sum.v[c] = v;
-          }
-          if (mode == 0) {
-            vstore<T, W>(out + (long long)(r0 + row) * KP + off, sum);
-          } else if (mode == 1) {
-            vstore<T, W>(out + ((long long)blockIdx.y * nRowsTotal + (r0 + row)) * KP + off, sum);
-          } else {
-            const Vec<T, W> yy = vload<T, W>(y + (long long)(r0 + row) * KP + off);
-            const T sc = scale[r0 + row];
-            Vec<T, W> o;
+        for (int c = 0; c < W; c++) {
+          T v = 0;
+          for (int w = 0; w < 8; w++) v += red[w][lane][a * W + c];
+          sum.v[c] = v;
+        }
+        if (nch > 1) {
+          vstore<T, W>(part + (((long long)blockIdx.x * nch + chunk) * 128 + 4 * lane + a) * KP + off, sum);
+        } else if (mode == 0) {
+          vstore<T, W>(B.y + (long long)(r0 + row) * KP + off, sum);
+        } else {
+          vstore<T, W>(B.xs + (long long)row * KP + off, sum);
+          const T sc = B.scale[B.nI + row];
 #pragma unroll
-            for (int c = 0; c < W; c++) o.v[c] = (yy.v[c] - sum.v[c]) * sc;
-            vstore<T, W>(x + (long long)posGlobal[r0 + row] * KP + off, o);
-          }
+          for (int c = 0; c < W; c++) sum.v[c] *= sc;
+          vstore<T, W>(x + (long long)B.posGlobal[B.nI + row] * KP + off, sum);
         }
       }
     }
     __syncthreads();
   }
-}
-
-// t = r^_S - A_SI y
-template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bs_sep_rhs(int nI, int nS, const int* __restrict__ asiPtr, const int* __restrict__ asiCol,
-                                                    const T* __restrict__ asiVal, const T* __restrict__ rhat,
-                                                    const T* __restrict__ y, T* __restrict__ t, int KP, int G) {
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long s = tid / G;
-  if (s >= nS) return;
-  const int q = int(tid - s * G), off = q * W;
-  Vec<T, W> acc = vload<T, W>(rhat + (long long)(nI + s) * KP + off);
-  for (int j = asiPtr[s]; j < asiPtr[s + 1]; j++) axpy(acc, -asiVal[j], vload<T, W>(y + (long long)asiCol[j] * KP + off));
-  vstore<T, W>(t + s * KP + off, acc);
-}
-
-// xs = sum of the chunk partials (fixed order); x[posGlobal[base + s]] = scale * xs
-template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bs_sep_sum(int base, int n, int chunks, const T* __restrict__ part,
-                                                    const int* __restrict__ posGlobal, const T* __restrict__ scale,
-                                                    T* __restrict__ xs, T* __restrict__ x, int KP, int G) {
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long s = tid / G;
-  if (s >= n) return;
-  const int q = int(tid - s * G), off = q * W;
-  Vec<T, W> acc = vload<T, W>(part + s * KP + off);
-  for (int c = 1; c < chunks; c++) {
-    const Vec<T, W> v = vload<T, W>(part + ((long long)c * n + s) * KP + off);
-#pragma unroll
-    for (int k = 0; k < W; k++) acc.v[k] += v.v[k];
+  if (nch == 1) return;
+  // the last chunk of this row group to finish adds the partials in chunk order
+  __threadfence();
+  __syncthreads();
+  int* counter = (mode == 0 ? B.subCount : B.schurCount) + blockIdx.x;
+  if (threadIdx.x == 0) {
+    const int prev = atomicAdd(counter, 1);
+    lastFlag = prev == nch - 1;
+    if (lastFlag) *counter = 0;  // ready for the next launch
   }
-  if (xs) vstore<T, W>(xs + s * KP + off, acc);
-  const T sc = scale[base + s];
+  __syncthreads();
+  if (!lastFlag) return;
+  __threadfence();
+  for (int it = threadIdx.x; it < 128 * G; it += blockDim.x) {
+    const int rt = it / G, q = it - rt * G, row = 4 * task.y + rt, off = q * W;
+    if (row >= m) continue;
+    Vec<T, W> sum;
 #pragma unroll
-  for (int k = 0; k < W; k++) acc.v[k] *= sc;
-  vstore<T, W>(x + (long long)posGlobal[base + s] * KP + off, acc);
+    for (int c = 0; c < W; c++) sum.v[c] = 0;
+    for (int ch = 0; ch < nch; ch++) {
+      const T* src = part + (((long long)blockIdx.x * nch + ch) * 128 + rt) * KP + off;
+#pragma unroll
+      for (int c = 0; c < W; c++) sum.v[c] += __ldcg(src + c);
+    }
+    if (mode == 0) {
+      vstore<T, W>(B.y + (long long)(r0 + row) * KP + off, sum);
+    } else {
+      vstore<T, W>(B.xs + (long long)row * KP + off, sum);
+      const T sc = B.scale[B.nI + row];
+#pragma unroll
+      for (int c = 0; c < W; c++) sum.v[c] *= sc;
+      vstore<T, W>(x + (long long)B.posGlobal[B.nI + row] * KP + off, sum);
+    }
+  }
 }
 
-// z = A_IS xs for every interior position
+// x_I = s (y - W_p xs[touch_p]) for every interior position (W_p column-major,
+// so a warp reads consecutive rows of one column)
 template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bs_coupling(int nI, const int* __restrict__ aisPtr, const int* __restrict__ aisCol,
-                                                     const T* __restrict__ aisVal, const T* __restrict__ xs, T* __restrict__ z,
-                                                     int KP, int G) {
+__global__ void __launch_bounds__(256) k_bs_back(BoundaryDev<T> B, T* __restrict__ x, int KP, int G) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long k = tid / G;
-  if (k >= nI) return;
-  const int q = int(tid - k * G), off = q * W;
-  Vec<T, W> acc;
+  const long long i = tid / G;
+  if (i >= B.nI) return;
+  const int q = int(tid - i * G), off = q * W;
+  const int p = B.rowSub[i], b0 = B.subPtr[p], m = B.subPtr[p + 1] - b0, a = int(i) - b0;
+  Vec<T, W> acc = vload<T, W>(B.y + i * KP + off);
+  const T* Wp = B.wt + B.wOff[p] + a;
+  for (int e = B.touchPtr[p]; e < B.touchPtr[p + 1]; e++, Wp += m)
+    axpy(acc, -*Wp, vload<T, W>(B.xs + (long long)B.touch[e] * KP + off));
+  const T sc = B.scale[i];
 #pragma unroll
-  for (int c = 0; c < W; c++) acc.v[c] = 0;
-  for (int j = aisPtr[k]; j < aisPtr[k + 1]; j++) axpy(acc, aisVal[j], vload<T, W>(xs + (long long)aisCol[j] * KP + off));
-  vstore<T, W>(z + k * KP + off, acc);
+  for (int c = 0; c < W; c++) acc.v[c] *= sc;
+  vstore<T, W>(x + (long long)B.posGlobal[i] * KP + off, acc);
 }
 
 // ----------------------------------------------------------------------------
@@ -547,28 +536,9 @@ template <typename T, int W>
 void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s) {
   if (B.nb == 0) return;
   const int G = KP / W;
-  k_bs_rhs<T, W><<<nblk((long long)B.nb * G), 256, 0, s>>>(B.nb, B.posGlobal, B.scale, B.bdPtr, B.bdCol, B.bdVal, rhs, x, B.rhat,
-                                                            KP, G);
-  if (B.nSubTasks > 0)
-    k_bs_gemv<T, W><<<B.nSubTasks, 256, 0, s>>>(B.subTasks, B.subPtr, B.invOff, B.inv, B.rhat, B.y, 0, B.nI, 0, nullptr, nullptr,
-                                                nullptr, nullptr, KP, G);
-  if (B.nS > 0) {
-    k_bs_sep_rhs<T, W><<<nblk((long long)B.nS * G), 256, 0, s>>>(B.nI, B.nS, B.asiPtr, B.asiCol, B.asiVal, B.rhat, B.y, B.t, KP, G);
-    const int chunkLen = (B.nS + B.schurChunks - 1) / B.schurChunks;
-    dim3 grid(B.nSchurTasks, B.schurChunks);
-    k_bs_gemv<T, W><<<grid, 256, 0, s>>>(B.schurTasks, B.schurPtr, B.schurOff, B.sinv, B.t, B.part, 1, B.nS, chunkLen, nullptr,
-                                         nullptr, nullptr, nullptr, KP, G);
-    k_bs_sep_sum<T, W><<<nblk((long long)B.nS * G), 256, 0, s>>>(B.nI, B.nS, B.schurChunks, B.part, B.posGlobal, B.scale, B.xs, x,
-                                                                  KP, G);
-    if (B.nI > 0) {
-      k_bs_coupling<T, W><<<nblk((long long)B.nI * G), 256, 0, s>>>(B.nI, B.aisPtr, B.aisCol, B.aisVal, B.xs, B.z, KP, G);
-      k_bs_gemv<T, W><<<B.nSubTasks, 256, 0, s>>>(B.subTasks, B.subPtr, B.invOff, B.inv, B.z, nullptr, 2, B.nI, 0, B.posGlobal,
-                                                  B.scale, B.y, x, KP, G);
-    }
-  } else if (B.nI > 0) {
-    // no separator: x_I = s * y
-    k_bs_sep_sum<T, W><<<nblk((long long)B.nI * G), 256, 0, s>>>(0, B.nI, 1, B.y, B.posGlobal, B.scale, nullptr, x, KP, G);
-  }
+  if (B.nSubTasks > 0) k_bs_dense<T, W><<<dim3(B.nSubTasks, B.subChunks), 256, 0, s>>>(B, 0, rhs, x, KP, G);
+  if (B.nS > 0) k_bs_dense<T, W><<<dim3(B.nSchurTasks, B.schurChunks), 256, 0, s>>>(B, 1, rhs, x, KP, G);
+  if (B.nI > 0) k_bs_back<T, W><<<nblk((long long)B.nI * G), 256, 0, s>>>(B, x, KP, G);
 }
 template <typename T, int W>
 void launch_coarse_solve(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, cudaStream_t s) {

@@ -9,31 +9,39 @@ struct ColourRun;
 struct RestrictRun;
 struct ProlongRun;
 
-// Device view of one level's exact boundary solver (see setup/bsolve.cpp).
-// Dense inverses are symmetric, stored row-major with rows padded to a multiple
-// of 4 entries; tasks are {matrix, first row quad, j begin, j end}, one per block.
+// Longest j chunk of a boundary dense product (its input vector is staged in
+// shared memory): subdomains hold at most this many rows, and the separator
+// product is split into at least ceil(nS / kBoundaryChunkMax) chunks.
+constexpr int kBoundaryChunkMax = 384;
+
+// Device view of one level's exact boundary solver (setup/bsolve.cpp).  Solver
+// positions: interior rows of the subdomains first (subdomain by subdomain),
+// then the separator.  Dense inverses are symmetric, stored row-major with rows
+// padded to a multiple of 4 entries; a task {matrix, first row quad, -, -} is
+// one 128-row group, launched as `chunks` blocks over the j range.
 template <typename T>
 struct BoundaryDev {
   int nb = 0, nSub = 0, nI = 0, nS = 0;
   const int* subPtr = nullptr;          // subdomain row ranges (positions)
+  const int* rowSub = nullptr;          // interior position -> subdomain
   const long long* invOff = nullptr;
   const T* inv = nullptr;
   const int4* subTasks = nullptr;
-  int nSubTasks = 0;
-  const int* schurPtr = nullptr;        // {0, nS}
-  const long long* schurOff = nullptr;  // {0}
-  const T* sinv = nullptr;
+  int nSubTasks = 0, subChunks = 1;
+  const T* sinv = nullptr;              // separator Schur complement inverse (nS x nSp)
   const int4* schurTasks = nullptr;
   int nSchurTasks = 0, schurChunks = 1;
   const int* posGlobal = nullptr;       // position -> global texel
   const T* scale = nullptr;
   const int *bdPtr = nullptr, *bdCol = nullptr;
   const T* bdVal = nullptr;
-  const int *aisPtr = nullptr, *aisCol = nullptr;
-  const T* aisVal = nullptr;
-  const int *asiPtr = nullptr, *asiCol = nullptr;
+  const int *asiPtr = nullptr, *asiCol = nullptr;  // separator x interior coupling (scaled)
   const T* asiVal = nullptr;
-  T *rhat = nullptr, *y = nullptr, *z = nullptr, *t = nullptr, *xs = nullptr, *part = nullptr;  // work
+  const int *touchPtr = nullptr, *touch = nullptr; // per subdomain: separator columns
+  const long long* wOff = nullptr;
+  const T* wt = nullptr;                // Inv_p A_{I_p,touch}, column-major m x t_p
+  T *y = nullptr, *xs = nullptr, *subPart = nullptr, *schurPart = nullptr;  // work
+  int *subCount = nullptr, *schurCount = nullptr;                            // chunk arrival counters (zero between launches)
 };
 
 template <typename T, int W>

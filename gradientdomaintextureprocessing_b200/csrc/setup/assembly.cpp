@@ -13,37 +13,13 @@
 namespace gdtp {
 
 bool embedding_metric(const Mesh& mesh, const Atlas& A, ChartMetrics& out) {
-  const int nt = mesh.nt();
-  std::vector<M2> G(nt);
-  double total = 0;
-  for (int t = 0; t < nt; t++) {
-    const double* p0 = &mesh.vertices[3 * mesh.triangles[3 * t]];
-    const double* p1 = &mesh.vertices[3 * mesh.triangles[3 * t + 1]];
-    const double* p2 = &mesh.vertices[3 * mesh.triangles[3 * t + 2]];
-    double d[2][3] = {{p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]}, {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]}};
-    M2 g;
-    for (int k = 0; k < 2; k++)
-      for (int l = 0; l < 2; l++) g.c[k][l] = d[k][0] * d[l][0] + d[k][1] * d[l][1] + d[k][2] * d[l][2];
-    total += std::sqrt(g.det()) / 2;
-    G[t] = g;
-  }
-  if (!(total > 0)) return false;
-  for (auto& g : G)
-    for (int k = 0; k < 2; k++)
-      for (int l = 0; l < 2; l++) g.c[k][l] /= total;
+  std::vector<M2> G, P;
+  if (!surface_metric(mesh, 0, true, G) || !parameter_metric(mesh, G, P)) return false;
   out.assign(A.charts.size(), {});
   for (size_t c = 0; c < A.charts.size(); c++) {
     const AtlasChart& ac = A.charts[c];
     out[c].resize(ac.meshTriangleIndices.size());
-    for (size_t k = 0; k < ac.meshTriangleIndices.size(); k++) {
-      int t = ac.meshTriangleIndices[k];
-      V2 q0 = mesh.corner(t, 0), q1 = mesh.corner(t, 1), q2 = mesh.corner(t, 2);
-      M2 J;
-      J.c[0][0] = q1.x - q0.x; J.c[0][1] = q1.y - q0.y;
-      J.c[1][0] = q2.x - q0.x; J.c[1][1] = q2.y - q0.y;
-      M2 Ji = J.inverse();
-      out[c][k] = (Ji.transpose() * G[t]) * Ji;
-    }
+    for (size_t k = 0; k < ac.meshTriangleIndices.size(); k++) out[c][k] = P[ac.meshTriangleIndices[k]];
   }
   return true;
 }

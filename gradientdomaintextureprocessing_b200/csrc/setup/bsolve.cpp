@@ -162,6 +162,28 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, BoundaryS
   bs.AIS = csr_from_triplets(bs.nI, bs.nS, tIS);
   bs.ASI = csr_transpose(bs.AIS);
 
+  // ---- separator columns each subdomain touches, and W_p = Inv_p A_{I_p,S}
+  // restricted to them (m x t, stored column-major): the back substitution
+  // x_I = Inv_p (r_I - A_IS x_S) = y_p - W_p x_S reads W_p instead of Inv_p.
+  bs.touchPtr.assign(bs.nSub + 1, 0);
+  std::vector<std::vector<int>> touches(bs.nSub);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int p = 0; p < bs.nSub; p++) {
+    std::vector<int>& touch = touches[p];
+    for (int a = bs.subPtr[p]; a < bs.subPtr[p + 1]; a++)
+      for (int kk = bs.AIS.ptr[a]; kk < bs.AIS.ptr[a + 1]; kk++) touch.push_back(bs.AIS.col[kk]);
+    std::sort(touch.begin(), touch.end());
+    touch.erase(std::unique(touch.begin(), touch.end()), touch.end());
+  }
+  bs.wOff.assign(bs.nSub + 1, 0);
+  for (int p = 0; p < bs.nSub; p++) {
+    bs.touchPtr[p + 1] = bs.touchPtr[p] + (int)touches[p].size();
+    bs.wOff[p + 1] = bs.wOff[p] + int64_t(bs.subPtr[p + 1] - bs.subPtr[p]) * (int64_t)touches[p].size();
+  }
+  bs.touch.resize(bs.touchPtr[bs.nSub]);
+  for (int p = 0; p < bs.nSub; p++) std::copy(touches[p].begin(), touches[p].end(), bs.touch.begin() + bs.touchPtr[p]);
+  bs.W.assign(size_t(bs.wOff[bs.nSub]), 0.0);
+
   // ---- Schur complement on the separator, S = A_SS - A_SI A_II^-1 A_IS (scaled)
   if (bs.nS > 0) {
     const int nS = bs.nS;
@@ -173,18 +195,15 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, BoundaryS
         if (c >= bs.nI) bs.Sinv[size_t(s) * nS + (c - bs.nI)] = scaled(i, kk);
       }
     }
-    // per subdomain: the separator columns it touches
+    // per-subdomain contributions, subtracted afterwards in subdomain order so
+    // that the complement is bit-identical from run to run
+    std::vector<std::vector<double>> contrib(bs.nSub);
 #pragma omp parallel
     {
-      std::vector<double> local;
 #pragma omp for schedule(dynamic, 1)
       for (int p = 0; p < bs.nSub; p++) {
         const int b0 = bs.subPtr[p], m = bs.subPtr[p + 1] - b0;
-        std::vector<int> touch;
-        for (int a = 0; a < m; a++)
-          for (int kk = bs.AIS.ptr[b0 + a]; kk < bs.AIS.ptr[b0 + a + 1]; kk++) touch.push_back(bs.AIS.col[kk]);
-        std::sort(touch.begin(), touch.end());
-        touch.erase(std::unique(touch.begin(), touch.end()), touch.end());
+        const std::vector<int>& touch = touches[p];
         const int t = (int)touch.size();
         if (!t) continue;
         // C = A_IS restricted (m x t), then G = Inv C, contribution C^T G
@@ -203,6 +222,10 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, BoundaryS
             double* ga = &G[size_t(a) * t];
             for (int c = 0; c < t; c++) ga[c] += w * cq[c];
           }
+        double* Wp = &bs.W[size_t(bs.wOff[p])];
+        for (int a = 0; a < m; a++)
+          for (int c = 0; c < t; c++) Wp[size_t(c) * m + a] = G[size_t(a) * t + c];
+        std::vector<double>& local = contrib[p];
         local.assign(size_t(t) * t, 0.0);
         for (int a = 0; a < m; a++)
           for (int c1 = 0; c1 < t; c1++) {
@@ -210,10 +233,13 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, BoundaryS
             if (cv == 0.0) continue;
             for (int c2 = 0; c2 < t; c2++) local[size_t(c1) * t + c2] += cv * G[size_t(a) * t + c2];
           }
-#pragma omp critical
-        for (int c1 = 0; c1 < t; c1++)
-          for (int c2 = 0; c2 < t; c2++) bs.Sinv[size_t(touch[c1]) * nS + touch[c2]] -= local[size_t(c1) * t + c2];
       }
+    }
+    for (int p = 0; p < bs.nSub; p++) {
+      const std::vector<int>& touch = touches[p];
+      const int t = (int)touch.size();
+      for (int c1 = 0; c1 < t; c1++)
+        for (int c2 = 0; c2 < t; c2++) bs.Sinv[size_t(touch[c1]) * nS + touch[c2]] -= contrib[p][size_t(c1) * t + c2];
     }
     // symmetrise against rounding, then invert
     for (int a = 0; a < nS; a++)

@@ -207,6 +207,16 @@ bool build_boundary_elements(const Hierarchy& h, BoundaryElements& be, std::stri
 // per chart, per chart triangle: 2x2 parameter metric g (column-major c[col][row])
 typedef std::vector<std::vector<M2>> ChartMetrics;
 bool embedding_metric(const Mesh& mesh, const Atlas& atlas, ChartMetrics& g);
+// Per mesh triangle metrics (metric.cpp), in the basis of the triangle's edges:
+// mode 0 = embedding (edges in space), 1 = uniform (edges in texture space);
+// optionally divided by the total area they measure.
+bool surface_metric(const Mesh& mesh, int mode, bool normalizeArea, std::vector<M2>& G);
+// Tangent-field metric: g B diag(0, across) B^-1 + isotropic g, with B the
+// g-orthonormal frame (field, field rotated); vf = nt x 2 edge-basis vectors.
+bool vector_field_metric(const std::vector<M2>& G, const double* vf, double across, double isotropic, bool normalizeArea,
+                         std::vector<M2>& out);
+// Pull-back to texture coordinates: J^-T G J^-1 with J the texture-space edges.
+bool parameter_metric(const Mesh& mesh, const std::vector<M2>& G, std::vector<M2>& out);
 
 // Work lists of the device assembly.  Interior cells: for every interior cell
 // (chart order, then interior-cell order) the chart triangles overlapping it,
@@ -261,6 +271,9 @@ struct BoundarySolverSetup {
   std::vector<int64_t> invOff;          // per subdomain offset into inv
   std::vector<double> inv;              // scaled dense inverses, row-major m x m
   Csr AIS, ASI;                         // scaled couplings: interior positions x separator, and transpose
+  std::vector<int> touchPtr, touch;     // per subdomain: the separator columns its rows couple to
+  std::vector<int64_t> wOff;            // per subdomain offset into W
+  std::vector<double> W;                // Inv_p A_{I_p,touch}, m x t column-major (scaled)
   std::vector<double> Sinv;             // scaled nS x nS inverse Schur complement
   Csr BD;                               // positions x global texels (unscaled boundary-deep rows)
 };

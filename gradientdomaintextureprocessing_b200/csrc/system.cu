@@ -318,14 +318,17 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       B.nSub = bs.nSub;
       B.nI = bs.nI;
       B.nS = bs.nS;
-      // subdomain inverses, rows padded to a multiple of 4
+      // subdomain inverses, rows padded to a multiple of 4; one task per 128 rows
       std::vector<long long> off(bs.nSub + 1, 0);
       std::vector<int4> tasks;
+      int maxM = 0;
       for (int p = 0; p < bs.nSub; p++) {
         const int m = bs.subPtr[p + 1] - bs.subPtr[p], mp = (m + 3) & ~3;
         off[p + 1] = off[p] + (long long)m * mp;
+        maxM = std::max(maxM, m);
         for (int rq = 0; rq < mp / 4; rq += 32) tasks.push_back(make_int4(p, rq, 0, m));
       }
+      if (maxM > dev::kBoundaryChunkMax) { err_ = "boundary subdomain larger than the device chunk limit"; return false; }
       std::vector<T> inv(size_t(off[bs.nSub]), T(0));
       for (int p = 0; p < bs.nSub; p++) {
         const int m = bs.subPtr[p + 1] - bs.subPtr[p], mp = (m + 3) & ~3;
@@ -333,12 +336,26 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
         for (int j = 0; j < m; j++)
           for (int a = 0; a < m; a++) inv[size_t(off[p]) + size_t(j) * mp + a] = T(src[size_t(j) * m + a]);
       }
+      // blocks per row group: enough chunks for one wave of 3 resident blocks
+      // on each of the 148 SMs, each warp still taking >= 4 j steps
+      auto chunks_for = [](int tasks, int m, int minChunks) {
+        int c = (3 * 148 + std::max(1, tasks) - 1) / std::max(1, tasks);
+        c = std::min(c, std::max(1, m / 32));
+        return std::max(c, std::max(1, minChunks));
+      };
+      std::vector<int> rowSub(std::max(1, bs.nI));
+      for (int p = 0; p < bs.nSub; p++)
+        for (int k = bs.subPtr[p]; k < bs.subPtr[p + 1]; k++) rowSub[k] = p;
       B.subPtr = A.upload(bs.subPtr);
+      B.rowSub = A.upload(rowSub);
       B.invOff = A.upload(off);
       B.inv = A.upload(inv);
       B.subTasks = A.upload(tasks);
       B.nSubTasks = (int)tasks.size();
-      // separator Schur complement inverse, same layout, j range split in chunks
+      B.subChunks = chunks_for(B.nSubTasks, maxM, 1);
+      B.subPart = static_cast<T*>(A.alloc(size_t(std::max(1, B.nSubTasks)) * B.subChunks * 128 * KP * sizeof(T)));
+      B.subCount = A.zeros<int>(std::max(1, B.nSubTasks));
+      // separator Schur complement inverse, same layout
       if (bs.nS > 0) {
         const int nS = bs.nS, nSp = (nS + 3) & ~3;
         std::vector<T> sinv(size_t(nS) * nSp, T(0));
@@ -349,10 +366,17 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
         B.sinv = A.upload(sinv);
         B.schurTasks = A.upload(st);
         B.nSchurTasks = (int)st.size();
-        B.schurChunks = std::max(1, std::min(64, std::min(nS / 32 + 1, 600 / std::max(1, B.nSchurTasks))));
-        B.schurPtr = A.upload(std::vector<int>{0, nS});
-        B.schurOff = A.upload(std::vector<long long>{0});
+        B.schurChunks = chunks_for(B.nSchurTasks, nS, (nS + dev::kBoundaryChunkMax - 1) / dev::kBoundaryChunkMax);
+        B.schurPart = static_cast<T*>(A.alloc(size_t(B.nSchurTasks) * B.schurChunks * 128 * KP * sizeof(T)));
+        B.schurCount = A.zeros<int>(B.nSchurTasks);
       }
+      // back substitution: W_p column-major with its separator columns
+      std::vector<long long> wOff(bs.wOff.begin(), bs.wOff.end());
+      std::vector<T> wt(bs.W.begin(), bs.W.end());
+      B.touchPtr = A.upload(bs.touchPtr);
+      B.touch = A.upload(bs.touch);
+      B.wOff = A.upload(wOff);
+      B.wt = A.upload(wt);
       std::vector<T> scale(bs.scale.begin(), bs.scale.end());
       std::vector<int> pg(bs.nb);
       for (int k = 0; k < bs.nb; k++) pg[k] = G.boundaryGlobal[bs.order[k]];
@@ -362,18 +386,11 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       B.bdPtr = A.upload(bs.BD.ptr);
       B.bdCol = A.upload(bs.BD.col);
       B.bdVal = upT(bs.BD.val);
-      B.aisPtr = A.upload(bs.AIS.ptr);
-      B.aisCol = A.upload(bs.AIS.col);
-      B.aisVal = upT(bs.AIS.val);
       B.asiPtr = A.upload(bs.ASI.ptr);
       B.asiCol = A.upload(bs.ASI.col);
       B.asiVal = upT(bs.ASI.val);
-      B.rhat = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nb)) * KP * sizeof(T)));
       B.y = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nI)) * KP * sizeof(T)));
-      B.z = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nI)) * KP * sizeof(T)));
-      B.t = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * KP * sizeof(T)));
       B.xs = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * KP * sizeof(T)));
-      B.part = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * B.schurChunks * KP * sizeof(T)));
     }
     // transfers to / from level l+1
     {

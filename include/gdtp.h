@@ -71,13 +71,33 @@ int gdtp_hierarchy_counts(const gdtp_hierarchy* h, int level, int64_t* counts);
 int gdtp_hierarchy_array(const gdtp_hierarchy* h, const char* name, int level, void* out, int64_t* count);
 
 /* ---------------------------------------------------------------------------
+ * Metrics (host).  Per mesh triangle parameter metric (nt*4, the layout of
+ * gdtp_system_create's parameter_metric), area-normalised as the reference's.
+ * gdtp_surface_metric: mode 0 = embedding (InitializeEmbeddingMetric,
+ * Metric.inl:248-275), 1 = uniform (InitializeUniformMetric, :277-303), pulled
+ * back to texture space (InitializeParameterMetric, :415-446).
+ * gdtp_anisotropic_metric: tangent-field metric for line-integral convolution
+ * (InitializeVectorFieldMetric, Metric.inl:12-67, as InitializeAnisotropicMetric
+ * :468-486 applies it to a given field): g B diag(0, across) B^-1 + isotropic*g
+ * with B the g-orthonormal frame {field, field rotated by 90 degrees}.  vf: nt*2,
+ * the field on each triangle in the basis of its edges (p1 - p0, p2 - p0), the
+ * per-triangle layout of the reference's vector-field files.  The reference uses
+ * across = 0.1 and isotropic = 1e-5 (Metric.inl:45-55).
+ * ------------------------------------------------------------------------- */
+int gdtp_surface_metric(const double* vertices, int64_t nv, const int32_t* triangles, int64_t nt, const double* uv, int mode,
+                        double* metric_out);
+int gdtp_anisotropic_metric(const double* vertices, int64_t nv, const int32_t* triangles, int64_t nt, const double* uv,
+                            const double* vf, double across, double isotropic, double* metric_out);
+
+/* ---------------------------------------------------------------------------
  * System (device).  gdtp_system_create binds a hierarchy to a CUDA device and
  * assembles the FP64 mass and stiffness matrices: replaces InitializeMetric
  * (include/Src/Metric.inl:448; metric_mode 0 = embedding) and
  * InitializeMassAndStiffness (include/Src/MassAndStiffness.h:490-549).
  * parameter_metric: optional per mesh triangle 2x2 metric (nt*4, column-major
  * g(0,0),g(0,1),g(1,0),g(1,1) in texture coordinates, as InitializeParameterMetric
- * produces, Metric.inl:415-446); NULL selects metric_mode.
+ * produces, Metric.inl:415-446); NULL selects metric_mode (0 = embedding,
+ * 1 = uniform: InitializeMetric, Metric.inl:448-466).
  * ------------------------------------------------------------------------- */
 int gdtp_system_create(gdtp_hierarchy* h, int device, int metric_mode, const double* parameter_metric,
                        const double* vertices, int64_t nv, gdtp_system** out);
