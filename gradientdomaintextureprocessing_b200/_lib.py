@@ -41,6 +41,8 @@ _SIGS = {
     "gdtp_hierarchy_charts": (C.c_int, [_P]),
     "gdtp_hierarchy_counts": (C.c_int, [_P, C.c_int, _P]),
     "gdtp_hierarchy_array": (C.c_int, [_P, C.c_char_p, C.c_int, _P, C.POINTER(C.c_int64)]),
+    "gdtp_surface_metric": (C.c_int, [_P, C.c_int64, _P, C.c_int64, _P, C.c_int, _P]),
+    "gdtp_anisotropic_metric": (C.c_int, [_P, C.c_int64, _P, C.c_int64, _P, _P, C.c_double, C.c_double, _P]),
     "gdtp_system_create": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, C.c_int64, C.POINTER(_P)]),
     "gdtp_system_free": (None, [_P]),
     "gdtp_system_array": (C.c_int, [_P, C.c_char_p, C.c_int, _P, C.POINTER(C.c_int64)]),

@@ -49,6 +49,16 @@ struct __align__(32) Vec<double, 4> {
   double v[4];
 };
 
+// Programmatic dependent launch.  Every V-cycle kernel starts with
+// grid_dependency_wait(): it returns once the grids this launch depends on have
+// completed and their writes are visible (immediately when the launch carries
+// no programmatic dependency).  grid_launch_dependents() then lets the next
+// kernel in the stream be scheduled while this one still runs, so its launch
+// latency overlaps this kernel's tail; the next kernel in turn waits before it
+// touches memory.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <typename T, int W>
 __device__ __forceinline__ Vec<T, W> vload(const T* p) {
   return *reinterpret_cast<const Vec<T, W>*>(p);

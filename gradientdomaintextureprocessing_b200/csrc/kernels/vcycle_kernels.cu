@@ -28,6 +28,8 @@ __device__ __forceinline__ void axpy(Vec<T, W>& acc, T a, const Vec<T, W>& v) {
 template <typename T, int W>
 __global__ void __launch_bounds__(256) k_gs_colour(const ColourRun* __restrict__ runs, int nRuns, const T* __restrict__ coef,
                                                    int planeStride, const T* __restrict__ rhs, T* __restrict__ x, int KP, int G) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int per = 32 * G;
   const long long r = t / per;
@@ -68,6 +70,8 @@ __global__ void __launch_bounds__(256) k_residual(const ColourRun* __restrict__ 
                                                   const int* __restrict__ bCol, const T* __restrict__ bVal,
                                                   const int* __restrict__ bGlobal, int nB, const T* __restrict__ rhs,
                                                   const T* __restrict__ x, T* __restrict__ res, int KP, int G) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   if ((int)blockIdx.x < deepBlocks) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int per = 32 * G;
@@ -114,7 +118,13 @@ template <typename T, int W>
 __global__ void __launch_bounds__(256) k_restrict(const RestrictRun* __restrict__ runs, int nRuns, int deepBlocks,
                                                   const int* __restrict__ rPtr, const int* __restrict__ rCol,
                                                   const T* __restrict__ rVal, const int* __restrict__ rOut, int nB,
-                                                  const T* __restrict__ res, T* __restrict__ coarseRhs, int KP, int G) {
+                                                  const T* __restrict__ res, T* __restrict__ coarseRhs, T* __restrict__ coarseX,
+                                                  long long coarseVals, int KP, int G) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  // the coarse iterate starts from zero: cleared here (grid-stride)
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < coarseVals; i += (long long)gridDim.x * blockDim.x)
+    coarseX[i] = T(0);
   if ((int)blockIdx.x < deepBlocks) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int per = 32 * G;
@@ -154,6 +164,8 @@ __global__ void __launch_bounds__(256) k_restrict(const RestrictRun* __restrict_
 template <typename T, int W>
 __global__ void __launch_bounds__(256) k_prolong_add(const ProlongRun* __restrict__ runs, int nRuns, const T* __restrict__ coarse,
                                                      T* __restrict__ fine, int KP, int G) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int per = 32 * G;
   const long long r = t / per;
@@ -209,6 +221,8 @@ struct __align__(32) Quad<double> {
 template <typename T, int W>
 __global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode, const T* __restrict__ rhs, T* __restrict__ x, int KP,
                                                   int G) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   __shared__ T red[8][32][4 * W];
   __shared__ Vec<T, W> vin[kBoundaryChunkMax];
   __shared__ int lastFlag;
@@ -324,6 +338,8 @@ __global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode,
 // so a warp reads consecutive rows of one column)
 template <typename T, int W>
 __global__ void __launch_bounds__(256) k_bs_back(BoundaryDev<T> B, T* __restrict__ x, int KP, int G) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long i = tid / G;
   if (i >= B.nI) return;
@@ -345,6 +361,8 @@ __global__ void __launch_bounds__(256) k_bs_back(BoundaryDev<T> B, T* __restrict
 template <typename T, int W>
 __global__ void __launch_bounds__(256) k_coarse_solve(int n, const double* __restrict__ ainv, const double* __restrict__ scale,
                                                       const T* __restrict__ rhs, T* __restrict__ x, int KP, int G) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= n) return;
   const double* row = ainv + (long long)warp * n;
@@ -384,6 +402,8 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
                                                       const double* __restrict__ b, const double* __restrict__ x,
                                                       double* __restrict__ out, int K, int G, int mode, double* __restrict__ partials,
                                                       float* __restrict__ out32 = nullptr, int KP = 0) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   // grid-stride over deep items (runs x 32 x G) then boundary items (rows x G);
   // the stride is a multiple of G, so every thread keeps one channel group q
   const long long nDeepItems = (long long)nRuns * 32 * G, nItems = nDeepItems + (long long)nB * G;
@@ -464,6 +484,8 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
 
 // Sum of per-block partials in a fixed order (one block): sums[2K]
 __global__ void k_sum_partials(const double* __restrict__ partials, int nBlocks, int K, double* __restrict__ sums) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   __shared__ double sh[256];
   for (int c = 0; c < 2 * K; c++) {
     double s = 0;
@@ -482,20 +504,26 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int nBlocks,
 // FP64 residual (n*K, tight) -> FP32 right-hand side (n*KP, padded)
 template <typename T>
 __global__ void k_pack_rhs(const double* __restrict__ r, T* __restrict__ rhs, long long n, int K, int KP) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * KP) return;
   const long long i = t / KP;
   const int c = int(t - i * KP);
   rhs[t] = c < K ? T(r[i * K + c]) : T(0);
 }
-// x64 += e (padded FP32/FP64 correction)
+// x64 += e (padded FP32/FP64 correction); e is cleared for the next V-cycle
+// (its padding lanes stay zero through the V-cycle)
 template <typename T>
-__global__ void k_add_correction(double* __restrict__ x, const T* __restrict__ e, long long n, int K, int KP) {
+__global__ void k_add_correction(double* __restrict__ x, T* __restrict__ e, long long n, int K, int KP) {
+  grid_dependency_wait();
+  grid_launch_dependents();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * K) return;
   const long long i = t / K;
   const int c = int(t - i * K);
   x[t] += double(e[i * KP + c]);
+  e[i * KP + c] = T(0);
 }
 
 // ----------------------------------------------------------------------------
@@ -503,12 +531,35 @@ __global__ void k_add_correction(double* __restrict__ x, const T* __restrict__ e
 // ----------------------------------------------------------------------------
 static inline int nblk(long long threads) { return int((threads + 255) / 256); }
 
+static bool g_programmatic = true;
+void set_programmatic_launch(bool on) { g_programmatic = on; }
+bool programmatic_launch() { return g_programmatic; }
+
+// Every V-cycle kernel is launched with programmatic stream serialization:
+// inside a captured graph consecutive kernels get programmatic edges, so a
+// kernel is scheduled while its predecessor drains (each kernel waits in
+// grid_dependency_wait() before touching memory).
+template <typename... P, typename... A>
+static void launch(void (*kernel)(P...), dim3 grid, cudaStream_t s, A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = g_programmatic ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<P>(args)...);
+}
+
 template <typename T, int W>
 void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP,
                       cudaStream_t s) {
   if (nRuns == 0) return;
   const int G = KP / W;
-  k_gs_colour<T, W><<<nblk((long long)nRuns * 32 * G), 256, 0, s>>>(runs, nRuns, coef, planeStride, rhs, x, KP, G);
+  launch(k_gs_colour<T, W>, dim3(nblk((long long)nRuns * 32 * G)), s, runs, nRuns, coef, planeStride, rhs, x, KP, G);
 }
 template <typename T, int W>
 void launch_residual(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const int* bPtr, const int* bCol,
@@ -516,34 +567,35 @@ void launch_residual(const ColourRun* runs, int nRuns, const T* coef, int planeS
   const int G = KP / W;
   const int db = nblk((long long)nRuns * 32 * G), bb = nblk((long long)nB * G);
   if (db + bb == 0) return;
-  k_residual<T, W><<<db + bb, 256, 0, s>>>(runs, nRuns, coef, planeStride, db, bPtr, bCol, bVal, bGlobal, nB, rhs, x, res, KP, G);
+  launch(k_residual<T, W>, dim3(db + bb), s, runs, nRuns, coef, planeStride, db, bPtr, bCol, bVal, bGlobal, nB, rhs, x, res, KP, G);
 }
 template <typename T, int W>
 void launch_restrict(const RestrictRun* runs, int nRuns, const int* rPtr, const int* rCol, const T* rVal, const int* rOut,
-                     int nB, const T* res, T* coarseRhs, int KP, cudaStream_t s) {
+                     int nB, const T* res, T* coarseRhs, T* coarseX, long long coarseTexels, int KP, cudaStream_t s) {
   const int G = KP / W;
   const int db = nblk((long long)nRuns * 32 * G), bb = nblk((long long)nB * G);
-  if (db + bb == 0) return;
-  k_restrict<T, W><<<db + bb, 256, 0, s>>>(runs, nRuns, db, rPtr, rCol, rVal, rOut, nB, res, coarseRhs, KP, G);
+  if (db + bb == 0 && coarseTexels == 0) return;
+  launch(k_restrict<T, W>, dim3(std::max(1, db + bb)), s, runs, nRuns, db, rPtr, rCol, rVal, rOut, nB, res, coarseRhs, coarseX,
+         coarseTexels * KP, KP, G);
 }
 template <typename T, int W>
 void launch_prolong_add(const ProlongRun* runs, int nRuns, const T* coarse, T* fine, int KP, cudaStream_t s) {
   if (nRuns == 0) return;
   const int G = KP / W;
-  k_prolong_add<T, W><<<nblk((long long)nRuns * 32 * G), 256, 0, s>>>(runs, nRuns, coarse, fine, KP, G);
+  launch(k_prolong_add<T, W>, dim3(nblk((long long)nRuns * 32 * G)), s, runs, nRuns, coarse, fine, KP, G);
 }
 template <typename T, int W>
 void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s) {
   if (B.nb == 0) return;
   const int G = KP / W;
-  if (B.nSubTasks > 0) k_bs_dense<T, W><<<dim3(B.nSubTasks, B.subChunks), 256, 0, s>>>(B, 0, rhs, x, KP, G);
-  if (B.nS > 0) k_bs_dense<T, W><<<dim3(B.nSchurTasks, B.schurChunks), 256, 0, s>>>(B, 1, rhs, x, KP, G);
-  if (B.nI > 0) k_bs_back<T, W><<<nblk((long long)B.nI * G), 256, 0, s>>>(B, x, KP, G);
+  if (B.nSubTasks > 0) launch(k_bs_dense<T, W>, dim3(B.nSubTasks, B.subChunks), s, B, 0, rhs, x, KP, G);
+  if (B.nS > 0) launch(k_bs_dense<T, W>, dim3(B.nSchurTasks, B.schurChunks), s, B, 1, rhs, x, KP, G);
+  if (B.nI > 0) launch(k_bs_back<T, W>, dim3(nblk((long long)B.nI * G)), s, B, x, KP, G);
 }
 template <typename T, int W>
 void launch_coarse_solve(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, cudaStream_t s) {
   if (n == 0) return;
-  k_coarse_solve<T, W><<<nblk((long long)n * 32), 256, 0, s>>>(n, ainv, scale, rhs, x, KP, KP / W);
+  launch(k_coarse_solve<T, W>, dim3(nblk((long long)n * 32)), s, n, ainv, scale, rhs, x, KP, KP / W);
 }
 
 static inline int raw_groups(int K) { int G = 1; while (4 * G < K) G *= 2; return G; }
@@ -556,9 +608,9 @@ void launch_raw_operator(const ColourRun* runs, int nRuns, const double* coef, i
   const long long items = (long long)nRuns * 32 * G + (long long)nB * G;
   if (items == 0) return;
   const int blocks = int(std::min<long long>(kRawBlocks, nblk(items)));
-  k_raw_operator<<<blocks, 256, 0, s>>>(runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, out, K, G, mode,
-                                        partials);
-  if (partials && sums) k_sum_partials<<<1, 256, 0, s>>>(partials, blocks, K, sums);
+  launch(k_raw_operator, dim3(blocks), s, runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, out, K, G, mode,
+         partials, (float*)nullptr, 0);
+  if (partials && sums) launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
 }
 int raw_operator_blocks(int nRuns, int nB, int K) { return kRawBlocks; }
 void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr,
@@ -568,18 +620,18 @@ void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coe
   const long long items = (long long)nRuns * 32 * G + (long long)nB * G;
   if (items == 0) return;
   const int blocks = int(std::min<long long>(kRawBlocks, nblk(items)));
-  k_raw_operator<<<blocks, 256, 0, s>>>(runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, nullptr, K, G, 0,
-                                        partials, rhs32, KP);
-  if (partials && sums) k_sum_partials<<<1, 256, 0, s>>>(partials, blocks, K, sums);
+  launch(k_raw_operator, dim3(blocks), s, runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, (double*)nullptr, K,
+         G, 0, partials, rhs32, KP);
+  if (partials && sums) launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
 }
 
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s) {
-  k_pack_rhs<T><<<nblk(n * KP), 256, 0, s>>>(r, rhs, n, K, KP);
+  launch(k_pack_rhs<T>, dim3(nblk(n * KP)), s, r, rhs, n, K, KP);
 }
 template <typename T>
-void launch_add_correction(double* x, const T* e, long long n, int K, int KP, cudaStream_t s) {
-  k_add_correction<T><<<nblk(n * K), 256, 0, s>>>(x, e, n, K, KP);
+void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s) {
+  launch(k_add_correction<T>, dim3(nblk(n * K)), s, x, e, n, K, KP);
 }
 
 #define GDTP_INSTANTIATE(T, W)                                                                                             \
@@ -587,7 +639,7 @@ void launch_add_correction(double* x, const T* e, long long n, int K, int KP, cu
   template void launch_residual<T, W>(const ColourRun*, int, const T*, int, const int*, const int*, const T*, const int*, \
                                       int, const T*, const T*, T*, int, cudaStream_t);                                   \
   template void launch_restrict<T, W>(const RestrictRun*, int, const int*, const int*, const T*, const int*, int,        \
-                                      const T*, T*, int, cudaStream_t);                                                  \
+                                      const T*, T*, T*, long long, int, cudaStream_t);                                   \
   template void launch_prolong_add<T, W>(const ProlongRun*, int, const T*, T*, int, cudaStream_t);                       \
   template void launch_boundary_solve<T, W>(const BoundaryDev<T>&, const T*, T*, int, cudaStream_t);                     \
   template void launch_coarse_solve<T, W>(int, const double*, const double*, const T*, T*, int, cudaStream_t);
@@ -597,8 +649,8 @@ GDTP_INSTANTIATE(double, 1)
 GDTP_INSTANTIATE(double, 4)
 template void launch_pack_rhs<float>(const double*, float*, long long, int, int, cudaStream_t);
 template void launch_pack_rhs<double>(const double*, double*, long long, int, int, cudaStream_t);
-template void launch_add_correction<float>(double*, const float*, long long, int, int, cudaStream_t);
-template void launch_add_correction<double>(double*, const double*, long long, int, int, cudaStream_t);
+template void launch_add_correction<float>(double*, float*, long long, int, int, cudaStream_t);
+template void launch_add_correction<double>(double*, double*, long long, int, int, cudaStream_t);
 
 }  // namespace dev
 }  // namespace gdtp

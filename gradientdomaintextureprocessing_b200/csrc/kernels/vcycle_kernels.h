@@ -49,9 +49,10 @@ void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int plane
 template <typename T, int W>
 void launch_residual(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const int* bPtr, const int* bCol,
                      const T* bVal, const int* bGlobal, int nB, const T* rhs, const T* x, T* res, int KP, cudaStream_t s);
+// also clears the coarse iterate coarseX (coarseTexels x KP values)
 template <typename T, int W>
 void launch_restrict(const RestrictRun* runs, int nRuns, const int* rPtr, const int* rCol, const T* rVal, const int* rOut,
-                     int nB, const T* res, T* coarseRhs, int KP, cudaStream_t s);
+                     int nB, const T* res, T* coarseRhs, T* coarseX, long long coarseTexels, int KP, cudaStream_t s);
 template <typename T, int W>
 void launch_prolong_add(const ProlongRun* runs, int nRuns, const T* coarse, T* fine, int KP, cudaStream_t s);
 template <typename T, int W>
@@ -69,8 +70,12 @@ void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coe
                              float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s);
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s);
+// x += e, then e = 0
 template <typename T>
-void launch_add_correction(double* x, const T* e, long long n, int K, int KP, cudaStream_t s);
+void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s);
+// Programmatic dependent launch of the V-cycle kernels (process-wide, default on)
+void set_programmatic_launch(bool on);
+bool programmatic_launch();
 
 // assembly (assembly_kernels.cu)
 void launch_interior_cells(int n, const int* cellPtr, const int* cellTri, const int* cellIJ, const int* cellChart,

@@ -434,7 +434,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
   for (int l = 0; l + 1 < L; l++) {
     LevelDev<T>& D = mg.levels[l];
     LevelDev<T>& C = mg.levels[l + 1];
-    if (l > 0) cudaMemsetAsync(D.x, 0, size_t(D.n) * KP * sizeof(T), s);
+    // D.x of levels > 0 was cleared by the restriction into this level
     if (knobs.preBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
     for (int sw = 0; sw < knobs.preSweeps; sw++) {
       const bool prof = profiling_ && l == 0 && sw == 0;
@@ -444,7 +444,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
       if (prof) cudaEventRecordWithFlags(profEv_[1], s, cudaEventRecordExternal);
     }
     dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
-    dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, D.r, C.b, KP, s);
+    dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, D.r, C.b, C.x, C.n, KP, s);
   }
   dev::launch_coarse_solve<T, W>(mg.coarseN, mg.coarseInv, mg.coarseScale, mg.levels[L - 1].b, mg.levels[L - 1].x, KP, s);
   for (int l = L - 2; l >= 0; l--) {
@@ -589,8 +589,9 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     }
     profiling_ = true;
     if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
+    // D0.x (the correction) is zero on entry: cleared before the first step
+    // and by the correction update of every step
     LevelDev<float>& D0 = mg.levels[0];
-    cudaMemsetAsync(D0.x, 0, n * mg.KP * sizeof(float), s);
     if (mg.KP == 1) vcycle<float, 1>(mg, s); else vcycle<float, 4>(mg, s);
     dev::launch_add_correction<float>(X, D0.x, (long long)n, k, mg.KP, s);
     // r = b - A x, written straight into the FP32 right-hand side of the next V-cycle
@@ -616,7 +617,8 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     iterGraphB_ = B;
     iterGraphX_ = X;
   }
-  // initial residual, straight into the FP32 right-hand side
+  // zero correction, initial residual straight into the FP32 right-hand side
+  if (!check(cudaMemsetAsync(mg.levels[0].x, 0, n * mg.KP * sizeof(float), s), "zero correction")) return false;
   dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
                                rawA_.bGlobal, rawA_.nB, B, X, mg.levels[0].b, k, mg.KP, partials_, sums_, s);
   if (!check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||

@@ -10,6 +10,9 @@ path, so the workloads are generated here from a seed:
                           vertex positions jittered N(0, 1e-3), 16 latitude /
                           longitude band charts (8 polar pie slices, 8
                           equatorial rectangles) packed on a 4x4 grid.
+* ``genus2_atlas``     -- two tori joined by a tube (genus 2, ~200k
+                          triangles), 32 charts packed on an 8x4 grid, with
+                          ``gaussian_bump_field`` as its tangent field.
 
 Every chart is separated from its neighbours and from the border of the unit
 square by a gutter of at least ``gutter`` texels.  A mesh is a dict of numpy
@@ -31,8 +34,8 @@ import struct
 
 import numpy as np
 
-__all__ = ["torus_atlas", "icosphere_atlas", "value_noise", "write_gdm",
-           "read_gdm", "chart_ids"]
+__all__ = ["torus_atlas", "icosphere_atlas", "genus2_atlas", "gaussian_bump_field", "value_noise", "write_gdm",
+           "read_gdm", "write_vf", "read_vf", "chart_ids"]
 
 
 # ----------------------------------------------------------------------------
@@ -297,6 +300,199 @@ def icosphere_atlas(width: int = 2048, height: int = 2048, subdiv: int = 6, seed
     tex = value_noise(rng, width, height, channels) + rng.uniform(-0.1, 0.1, size=(height, width, channels))
     return {"vertices": v, "triangles": f.astype(np.int32), "uv": uv,
             "texture": tex.astype(np.float32), "name": f"icosphere{subdiv}_{width}x{height}"}
+
+
+# ----------------------------------------------------------------------------
+# genus 2: two tori joined by a straight tube, 32 charts
+# ----------------------------------------------------------------------------
+
+def _signed_uv_area(uv: np.ndarray) -> np.ndarray:
+    return ((uv[:, 1, 0] - uv[:, 0, 0]) * (uv[:, 2, 1] - uv[:, 0, 1]) -
+            (uv[:, 2, 0] - uv[:, 0, 0]) * (uv[:, 1, 1] - uv[:, 0, 1]))
+
+
+def genus2_atlas(width: int = 4096, height: int = 4096, nu: int = 352, nv: int = 144, R: float = 1.0,
+                 r: float = 0.4, gap: float = 0.3, seed: int = 0, gutter: int = 8, jitter: float = 0.3,
+                 channels: int = 1) -> dict:
+    """Genus-2 surface: two tori side by side, each opened by one block of its
+    (u, v) grid where it faces the other, the two openings joined by a straight
+    tube (a surface of genus 2).
+
+    Torus A is centred at x = -(R + r + gap), torus B is its mirror image.  The
+    grid of each torus is cut into 4 x 4 blocks of 90 x 90 degrees, block (0, 0)
+    (facing the other torus, outer equator) is removed, and each remaining block
+    is one chart (rectangle in (u (R + r cos v_mid), v r)).  The tube is the
+    extrusion along x of the opening's rim and is split into 2 charts
+    (developed: rim arc length x extrusion length).  32 charts, about
+    4 nu nv triangles; vertices of the removed blocks are dropped.  Texture: ``channels`` of uniform noise in [0, 1)."""
+    if nu % 4 or nv % 4:
+        raise ValueError("nu and nv must be multiples of 4")
+    rng = np.random.default_rng(seed)
+    cx = R + r + gap
+    bu, bv = nu // 4, nv // 4
+    ii, jj = np.meshgrid(np.arange(nu), np.arange(nv), indexing="xy")
+    u = 2 * np.pi * ii / nu - np.pi / 4
+    v = 2 * np.pi * jj / nv - np.pi / 4
+    rad = R + r * np.cos(v)
+    posA = np.stack([-cx + rad * np.cos(u), rad * np.sin(u), r * np.sin(v)], -1).reshape(-1, 3)
+    nA = nu * nv
+
+    def vid(i, j):
+        return (j % nv) * nu + (i % nu)
+
+    # torus quads outside the removed block, two triangles each, grouped by block
+    tA, cA, blk = [], [], []
+    for j in range(nv):
+        for i in range(nu):
+            b = (i // bu, j // bv)
+            if b == (0, 0):
+                continue
+            a_, b_, c_, d_ = (i, j), (i + 1, j), (i + 1, j + 1), (i, j + 1)
+            for tri in ((a_, b_, c_), (a_, c_, d_)):
+                tA.append([vid(*q) for q in tri])
+                cA.append(tri)
+                blk.append(b[1] * 4 + b[0])
+    tA = np.array(tA, dtype=np.int64)
+    cA = np.array(cA, dtype=np.float64)
+    blk = np.array(blk, dtype=np.int64)
+    # rim of the opening, counter-clockwise in (i, j)
+    rim = ([(i, 0) for i in range(0, bu)] + [(bu, j) for j in range(0, bv)] +
+           [(i, bv) for i in range(bu, 0, -1)] + [(0, j) for j in range(bv, 0, -1)])
+    rim_ids = np.array([vid(i, j) for i, j in rim], dtype=np.int64)
+    nr = len(rim_ids)
+    # tube rings between rim A (x < 0) and its mirror: x runs from x_A to -x_A
+    rimA = posA[rim_ids]
+    h = 2 * np.pi * r / nv
+    m = max(2, int(np.ceil(2 * np.abs(rimA[:, 0]).max() / h)))
+    s = np.arange(1, m) / m
+    rings = np.empty((m - 1, nr, 3))
+    rings[:, :, 0] = rimA[None, :, 0] * (1 - 2 * s[:, None])
+    rings[:, :, 1:] = rimA[None, :, 1:]
+    nRing = (m - 1) * nr
+    # vertex array: torus A, torus B (mirror), tube rings
+    posB = posA * np.array([-1.0, 1.0, 1.0])
+    verts = np.concatenate([posA, posB, rings.reshape(-1, 3)], 0)
+    ring_vid = np.empty((m + 1, nr), dtype=np.int64)
+    ring_vid[0] = rim_ids
+    ring_vid[m] = nA + rim_ids
+    ring_vid[1:m] = 2 * nA + np.arange(nRing).reshape(m - 1, nr)
+    tB = nA + tA[:, ::-1]            # mirror image: reversed winding
+    cB = cA[:, ::-1]
+    # tube quads (k, q) -> (k+1, q) ... oriented below
+    tT, cT, qT = [], [], []
+    for k in range(m):
+        for q in range(nr):
+            a_, b_ = ring_vid[k, q], ring_vid[k, (q + 1) % nr]
+            c_, d_ = ring_vid[k + 1, (q + 1) % nr], ring_vid[k + 1, q]
+            for tri, cc in (((a_, b_, c_), ((q, k), (q + 1, k), (q + 1, k + 1))),
+                            ((a_, c_, d_), ((q, k), (q + 1, k + 1), (q, k + 1)))):
+                tT.append(tri)
+                cT.append(cc)
+                qT.append(q)
+    tT = np.array(tT, dtype=np.int64)
+    cT = np.array(cT, dtype=np.float64)
+    qT = np.array(qT, dtype=np.int64)
+    # orient the tube outwards (away from the rim's centroid axis, parallel to x)
+    axis = rimA[:, 1:].mean(0)
+    p0, p1, p2 = verts[tT[:, 0]], verts[tT[:, 1]], verts[tT[:, 2]]
+    nrm = np.cross(p1 - p0, p2 - p0)
+    out = (p0 + p1 + p2)[:, 1:] / 3 - axis
+    if np.median((nrm[:, 1:] * out).sum(1)) < 0:
+        tT = tT[:, [0, 2, 1]]
+        cT = cT[:, [0, 2, 1]]
+    tris = np.concatenate([tA, tB, tT], 0)
+    used = np.zeros(len(verts), dtype=bool)
+    used[tris.reshape(-1)] = True
+    remap = np.cumsum(used) - 1
+    verts = verts[used]
+    tris = remap[tris]
+    # charts: 15 blocks per torus, 2 tube halves
+    chart = np.concatenate([blk, 16 + blk, 32 + (qT * 2) // nr], 0)
+    corners = np.concatenate([cA, cB, cT], 0)
+    kind = np.concatenate([np.zeros(len(tA)), np.ones(len(tB)), 2 * np.ones(len(tT))]).astype(np.int64)
+    # rim arc length (tube development)
+    seg = np.linalg.norm(np.roll(rimA[:, 1:], -1, 0) - rimA[:, 1:], axis=1)
+    arc = np.concatenate([[0.0], np.cumsum(seg)])
+    chart_uv, groups = [], []
+    for c in np.unique(chart):
+        tids = np.nonzero(chart == c)[0]
+        cc = corners[tids]
+        if kind[tids[0]] < 2:       # torus block: (u * (R + r cos v_mid), v * r)
+            uu = 2 * np.pi * cc[..., 0] / nu
+            vv = 2 * np.pi * cc[..., 1] / nv
+            vmid = 2 * np.pi * ((c % 16) // 4 + 0.5) / 4 - np.pi / 4
+            p = np.stack([uu * (R + r * np.cos(vmid)), vv * r], -1)
+        else:                       # tube half: (arc length along the rim, x)
+            q = cc[..., 0].astype(np.int64)
+            k = cc[..., 1]
+            xA = np.abs(rimA[q % nr, 0])
+            p = np.stack([arc[q], -xA + 2 * xA * k / m], -1)
+        if np.median(_signed_uv_area(p)) < 0:
+            p[..., 0] *= -1
+        chart_uv.append(p)
+        groups.append(tids)
+    placed = _pack_charts(chart_uv, (8, 4), width, height, gutter)
+    uv = np.empty((len(tris), 3, 2))
+    for tids, p in zip(groups, placed):
+        uv[tids] = p
+    # per chart-vertex texture jitter (same for every corner of one chart vertex),
+    # at most a tenth of the shortest texture-space edge
+    scale = np.array([width, height])
+    edge = np.linalg.norm((np.roll(uv, -1, 1) - uv) * scale, axis=-1).min()
+    amp = min(jitter, 0.1 * edge)
+    ckey = chart[:, None] * (len(verts) + 1) + tris
+    ukeys, inv = np.unique(ckey.reshape(-1), return_inverse=True)
+    jit = rng.uniform(-amp, amp, size=(len(ukeys), 2)) / scale
+    uv = uv + jit[inv].reshape(uv.shape)
+    bad = int((_signed_uv_area(uv) <= 0).sum())
+    if bad:
+        raise RuntimeError(f"genus-2 atlas has {bad} flipped triangles")
+    uv = _keep_off_texel_grid(uv, width, height)
+    tex = rng.uniform(0.0, 1.0, size=(height, width, channels))
+    return {"vertices": verts.astype(np.float64), "triangles": tris.astype(np.int32), "uv": uv,
+            "texture": tex.astype(np.float32), "name": f"genus2_{nu}x{nv}_{width}x{height}"}
+
+
+def gaussian_bump_field(mesh: dict, bumps: int = 8, seed: int = 0, sigma: float = 0.5) -> np.ndarray:
+    """Tangent field per triangle: the surface gradient of a seeded sum of
+    Gaussians, rotated by 90 degrees about the normal.  Returned in each
+    triangle's edge basis (coefficients of p1 - p0 and p2 - p0), the layout of
+    the reference's vector-field files."""
+    rng = np.random.default_rng(seed)
+    v = mesh["vertices"]
+    t = mesh["triangles"].astype(np.int64)
+    centres = v[rng.choice(len(v), size=bumps, replace=False)]
+    amp = rng.uniform(0.5, 1.5, size=bumps) * rng.choice([-1.0, 1.0], size=bumps)
+    d2 = ((v[:, None, :] - centres[None]) ** 2).sum(-1)
+    phi = (amp * np.exp(-d2 / (2 * sigma * sigma))).sum(1)
+    e1 = v[t[:, 1]] - v[t[:, 0]]
+    e2 = v[t[:, 2]] - v[t[:, 0]]
+    n = np.cross(e1, e2)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    # gradient of the linear interpolant: G [e1 e2] = [phi1 - phi0, phi2 - phi0], G in the plane
+    E = np.stack([e1, e2], 1)                          # (nt, 2, 3)
+    gram = np.einsum("tai,tbi->tab", E, E)
+    dphi = np.stack([phi[t[:, 1]] - phi[t[:, 0]], phi[t[:, 2]] - phi[t[:, 0]]], -1)
+    coef = np.linalg.solve(gram, dphi[..., None])[..., 0]
+    grad = np.einsum("ta,tai->ti", coef, E)
+    rot = np.cross(n, grad)
+    # rotated vector in the edge basis
+    rhs = np.einsum("tai,ti->ta", E, rot)
+    return np.linalg.solve(gram, rhs[..., None])[..., 0]
+
+
+def write_vf(path: str, vf: np.ndarray) -> None:
+    """Reference vector file: int32 count, then count Point2D<double> (Src/VectorIO.h:9-32)."""
+    vf = np.ascontiguousarray(vf, dtype=np.float64).reshape(-1, 2)
+    with open(path, "wb") as fh:
+        fh.write(struct.pack("<i", len(vf)))
+        fh.write(vf.tobytes())
+
+
+def read_vf(path: str) -> np.ndarray:
+    with open(path, "rb") as fh:
+        (n,) = struct.unpack("<i", fh.read(4))
+        return np.frombuffer(fh.read(16 * n), dtype=np.float64).reshape(n, 2).copy()
 
 
 # ----------------------------------------------------------------------------

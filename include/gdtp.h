@@ -166,7 +166,9 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
 /* Solver knobs (value as double): "pre_sweeps", "post_sweeps" (deep colour sweeps
  * per smoothing, default 2/2), "pre_boundary", "post_boundary" (exact boundary
  * solve before the pre / post sweeps, default 0/1), "max_block" (boundary
- * subdomain size, next update), "max_coarse" (coarsest level size, next update). */
+ * subdomain size, 16..384, next update), "max_coarse" (coarsest level size, next
+ * update), "programmatic_launch" (0/1, default 1: V-cycle kernels overlap their
+ * launch with the previous kernel's tail; process-wide). */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
 /* Autotuner: times complete solves of b (host float64 numTexels*k) to tol for a
  * set of smoother settings (sweeps and boundary-solve placement), keeps the

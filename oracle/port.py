@@ -13,6 +13,12 @@ Every function restates one reference operator on the reference's data layout
 * ``reciprocal_form``         UpdateMultigridCoefficients include/Src/UpdateCoefficients.inl:374-397
 * ``direct_solve``            the --useDirectSolver FP64 solve (TextureFiltering.cpp:651-655, 704-707;
                               Eigen SimplicialLDLT in include/Src/Solver.h:144-203, here scipy's LU)
+* ``embedding_metric``        InitializeEmbeddingMetric include/Src/Metric.inl:248-275
+* ``vector_field_metric``     InitializeVectorFieldMetric include/Src/Metric.inl:12-67
+* ``parameter_metric``        InitializeParameterMetric include/Src/Metric.inl:415-446
+
+Metrics are (nt, 2, 2) arrays in ordinary row/column order (m[t, i, j]); the
+reference's SquareMatrix g(c, r) is column c, row r, so g(c, r) = m[t, r, c].
 """
 from __future__ import annotations
 
@@ -99,3 +105,49 @@ def energy_error(A: sp.csr_matrix, x: np.ndarray, x_ref: np.ndarray) -> np.ndarr
     the residual; the energy norm weighs every texel by its support."""
     e = x - x_ref
     return np.sqrt(np.einsum("ik,ik->k", e, A @ e) / np.einsum("ik,ik->k", x_ref, A @ x_ref))
+
+
+# ----------------------------------------------------------------------------
+# metrics (per mesh triangle, in the basis of the triangle's edges)
+# ----------------------------------------------------------------------------
+
+def embedding_metric(vertices: np.ndarray, triangles: np.ndarray, normalize: bool = True) -> np.ndarray:
+    """g_kl = e_k . e_l with e_0 = p1 - p0, e_1 = p2 - p0, divided by the total area."""
+    p = vertices[triangles]
+    e = np.stack([p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]], 1)
+    g = np.einsum("tki,tli->tkl", e, e)
+    if normalize:
+        g = g / (np.sqrt(np.linalg.det(g)) / 2).sum()
+    return g
+
+
+def vector_field_metric(g: np.ndarray, vf: np.ndarray, across: float = 0.1, isotropic: float = 1e-5,
+                        normalize: bool = True) -> np.ndarray:
+    """g B diag(0, across) B^-1 + isotropic g, B = g-orthonormal {vf, rotated g vf}."""
+    out = np.empty_like(g)
+    for t in range(len(g)):
+        G = g[t]
+        v0 = vf[t]
+        u = np.zeros((2, 2))
+        if v0 @ G @ v0 > 0:
+            gv = G @ v0
+            e = [v0.copy(), np.array([-gv[1], gv[0]])]
+            e = [x / np.sqrt(x @ G @ x) for x in e]
+            B = np.stack(e, 1)
+            u = G @ B @ np.diag([0.0, across]) @ np.linalg.inv(B)
+        out[t] = u + G * isotropic
+    if normalize:
+        out = out / (np.sqrt(np.linalg.det(out)) / 2).sum()
+    return out
+
+
+def parameter_metric(uv: np.ndarray, g: np.ndarray) -> np.ndarray:
+    """Pull-back to texture coordinates: J^-T g J^-1, J = [q1 - q0, q2 - q0] as columns."""
+    J = np.stack([uv[:, 1] - uv[:, 0], uv[:, 2] - uv[:, 0]], 2)
+    Ji = np.linalg.inv(J)
+    return np.einsum("tki,tkl,tlj->tij", Ji, g, Ji)
+
+
+def metric_entries(m: np.ndarray) -> np.ndarray:
+    """(nt, 4) entries g(0,0), g(0,1), g(1,0), g(1,1) in the reference's (column, row) indexing."""
+    return np.stack([m[:, 0, 0], m[:, 1, 0], m[:, 0, 1], m[:, 1, 1]], 1)

@@ -7,6 +7,7 @@
 //   InitializeHierarchy            include/Src/HierarchyConstruction.inl:799
 //   InitializeBoundaryProlongationData include/Src/BoundaryQuadraticElements.inl:775
 //   InitializeMetric (embedding)   include/Src/Metric.inl:448
+//   InitializeAnisotropicMetric    include/Src/Metric.inl:468  (with a .vf tangent field, as the LIC app)
 //   InitializeMassAndStiffness     include/Src/MassAndStiffness.h:490
 //   FullMatrixConstruction         include/Src/UpdateCoefficients.inl:137
 //   UpdateLinearSystem             include/Src/UpdateCoefficients.inl:463
@@ -14,9 +15,11 @@
 //   VCycle                         include/Src/IterativeSolvers.inl:1211
 //   solve(EigenCholeskySolver3)    include/Src/Solver.h:191   (the --useDirectSolver FP64 ground truth)
 //
-// Usage: gdtp_ref <mesh.gdm> <out.gdd> [levels] [stiffness] [sharpness] [vcycles] [mode]
+// Usage: gdtp_ref <mesh.gdm> <out.gdd> [levels] [stiffness] [sharpness] [vcycles] [mode] [tol] [field.vf]
 //   mode "dump": everything (small meshes); "solve": counts + rhs + exact solution + V-cycle timing.
 //   The RHS is  M f + stiffness*sharpness * S f  and the operator  M + stiffness*S.
+//   With field.vf (the reference's vector file: int32 count + per-triangle Point2D<double> in the
+//   triangle's edge basis, read by its own ReadVector) M and S use the anisotropic metric instead.
 #ifndef USE_FLOAT
 #define USE_FLOAT 0
 #endif
@@ -32,6 +35,7 @@ unsigned char* PNGReadColor(const char*, int&, int&) { return nullptr; }
 #include <Src/Solver.h>
 #include <Src/Hierarchy.h>
 #include <Src/MassAndStiffness.h>
+#include <Src/VectorIO.h>
 
 #include <chrono>
 #include <cstdint>
@@ -173,7 +177,24 @@ int main(int argc, char** argv) {
   BoundaryProlongationData boundaryProlongation;
   if (!InitializeBoundaryProlongationData(hierarchy.gridAtlases[0], boundaryProlongation)) return 3;
   std::vector<std::vector<SquareMatrix<double, 2>>> parameterMetric;
-  if (!InitializeMetric(mesh, EMBEDDING_METRIC, atlasCharts, parameterMetric)) return 3;
+  const char* vfPath = argc > 9 ? argv[9] : nullptr;
+  if (vfPath && *vfPath) {
+    std::vector<Point2D<double>> vf;
+    if (!ReadVector(vf, vfPath) || vf.size() != mesh.triangles.size()) { fprintf(stderr, "bad vector field %s\n", vfPath); return 2; }
+    if (!InitializeAnisotropicMetric(mesh, atlasCharts, parameterMetric, vf, false)) return 3;
+  } else if (!InitializeMetric(mesh, EMBEDDING_METRIC, atlasCharts, parameterMetric)) {
+    return 3;
+  }
+  if (full) {  // parameter metric in mesh triangle order, entries g(0,0) g(0,1) g(1,0) g(1,1)
+    std::vector<double> pm(4 * mesh.triangles.size(), 0.0);
+    for (size_t c = 0; c < atlasCharts.size(); c++)
+      for (size_t k = 0; k < atlasCharts[c].meshTriangleIndices.size(); k++) {
+        const int t = atlasCharts[c].meshTriangleIndices[k];
+        const SquareMatrix<double, 2>& g = parameterMetric[c][k];
+        pm[4 * t] = g(0, 0); pm[4 * t + 1] = g(0, 1); pm[4 * t + 2] = g(1, 0); pm[4 * t + 3] = g(1, 1);
+      }
+    out.f64("metric/parameter", pm, 4);
+  }
 
   const GridAtlas& fine = hierarchy.gridAtlases[0];
   std::vector<Point3D<double>> inputSignal(textureNodes.size());

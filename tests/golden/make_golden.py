@@ -29,7 +29,12 @@ CASES = {
     "torus128": (lambda: meshgen.torus_atlas(128, 128), 4, 1e-3, 2.0, True),
     "torus256": (lambda: meshgen.torus_atlas(256, 256), 4, 1e-3, 2.0, False),
     "ico256": (lambda: meshgen.icosphere_atlas(256, 256, subdiv=5), 4, 1e-3, 2.0, True),
+    # line-integral convolution: anisotropic metric of a tangent field, operator
+    # M + 1e-4 S (the LIC app's default licStiffness), right-hand side M f
+    "genus2lic512": (lambda: meshgen.genus2_atlas(512, 512, nu=64, nv=32), 4, 1e-4, 0.0, True),
 }
+# tangent fields (reference .vf files) of the anisotropic cases
+FIELDS = {"genus2lic512": lambda mesh: meshgen.gaussian_bump_field(mesh, bumps=8, seed=0)}
 INDEX_KEYS = ["counts", "nodeinfo", "boundaryGlobalIndex", "deepGlobalIndex", "boundaryAndDeepIndex", "rasterLines",
               "restrictionLines", "deepLines", "prolongationLines", "charts_i", "charts_d"]
 
@@ -38,13 +43,21 @@ def make(name: str) -> None:
     factory, levels, lam, sharp, coefs = CASES[name]
     mesh = factory()
     exe = os.path.join(ROOT, "oracle", "_ref", "gdtp_ref")
+    vf = FIELDS[name](mesh) if name in FIELDS else None
     with tempfile.TemporaryDirectory() as tmp:
-        gdm, out = os.path.join(tmp, "m.gdm"), os.path.join(tmp, "o.gdd")
+        gdm, out, vfp = os.path.join(tmp, "m.gdm"), os.path.join(tmp, "o.gdd"), os.path.join(tmp, "f.vf")
         meshgen.write_gdm(gdm, mesh)
-        subprocess.run([exe, gdm, out, str(levels), str(lam), str(sharp), "12", "dump"], check=True, capture_output=True)
+        args = [exe, gdm, out, str(levels), str(lam), str(sharp), "12", "dump", "1e-6"]
+        if vf is not None:
+            meshgen.write_vf(vfp, vf)
+            args.append(vfp)
+        subprocess.run(args, check=True, capture_output=True)
         d = read_dump(out)
     keep = {"mesh/vertices": mesh["vertices"], "mesh/triangles": mesh["triangles"], "mesh/uv": mesh["uv"],
-            "mesh/texture": mesh["texture"], "meta/size": d["meta/size"], "meta/weights": d["meta/weights"]}
+            "mesh/texture": mesh["texture"], "meta/size": d["meta/size"], "meta/weights": d["meta/weights"],
+            "metric/parameter": d["metric/parameter"]}
+    if vf is not None:
+        keep["mesh/field"] = vf
     for k in ("solve/f", "solve/rhs", "solve/exact", "vcycle/history", "fine/textureNodes", "fine/textureBary",
               "fine/boundaryNodes"):
         keep[k] = d[k]

@@ -2,11 +2,17 @@
 from the compiled reference, tests/golden).  Tolerances:
 
 * deep mass/stiffness and boundary-deep rows: 1e-12 relative (FP64 quadrature,
-  same accumulation order; only rounding/FMA differs);
+  same accumulation order; only rounding/FMA differs).  With the anisotropic
+  LIC metric the metric itself is ill-conditioned (ratio 1e4 between its
+  eigenvalues): its rounding (1e-16) reaches the coefficients amplified by that
+  ratio, so the bound is 1e-12 x 1e4 (measured 1e-11);
 * boundary-boundary block: 1e-6 of its largest entry.  The reference moves the
   seam nodes it inserts by a rand()-driven 1e-10 relative offset before its
   Delaunay step (BoundaryQuadraticElements.inl:433-436); the device path keeps
-  them on the segment.  Measured difference ~1e-8;
+  them on the segment.  Measured difference ~1e-8 (mass), 6e-7 (stiffness).
+  The anisotropic stiffness amplifies that perturbation: 1e-4 bound, measured
+  1.4e-5 of the largest entry, 5e-5 of the largest entry of any row, no row
+  differing structurally;
 * solves: relative residual <= requested tolerance with the FP64 operator, and
   energy-norm error against the reference's FP64 direct solution <= 1e-5
   (texels whose support barely meets a chart have diagonals down to 1e-17 of
@@ -21,15 +27,24 @@ from conftest import golden_csr, golden_mesh, load_golden
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module", params=["torus128", "ico256"])
+# genus2lic512: line-integral convolution, anisotropic metric of a tangent field
+# (stiffness ratio 1e4 across / along the field), operator M + 1e-4 S
+@pytest.fixture(scope="module", params=["torus128", "ico256", "genus2lic512"])
 def setup(request, built_lib):
     from gradientdomaintextureprocessing_b200.hierarchy import InitializeHierarchy
+    from gradientdomaintextureprocessing_b200.metric import InitializeAnisotropicMetric
     from gradientdomaintextureprocessing_b200.system import System
     g = load_golden(request.param)
-    h = InitializeHierarchy(golden_mesh(g), levels=int(g["meta/size"][2]))
-    s = System(h)
+    mesh = golden_mesh(g)
+    h = InitializeHierarchy(mesh, levels=int(g["meta/size"][2]))
+    pm = InitializeAnisotropicMetric(mesh, g["mesh/field"]) if "mesh/field" in g else None
+    s = System(h, parameter_metric=pm)
     s.update(float(g["meta/weights"][0]), 1.0)
     return g, h, s
+
+
+# anisotropic V-cycles contract slowly (point smoother across a 1e4 ratio)
+MAX_ITERS = 400
 
 
 def ref_full(g):
@@ -50,18 +65,27 @@ def rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
+def coef_tol(g):
+    return 1e-12 * (1e4 if "mesh/field" in g else 1.0)
+
+
+def bb_tol(g):
+    return 1e-4 if "mesh/field" in g else 1e-6
+
+
 def test_deep_coefficients_match_reference(setup):
     g, _, s = setup
-    assert rel(s.array("deepMass"), g["fine/deepMass"]) < 1e-12
-    assert rel(s.array("deepStiffness"), g["fine/deepStiffness"]) < 1e-12
+    assert rel(s.array("deepMass"), g["fine/deepMass"]) < coef_tol(g)
+    assert rel(s.array("deepStiffness"), g["fine/deepStiffness"]) < coef_tol(g)
 
 
 def test_boundary_blocks_match_reference(setup):
     g, _, s = setup
     n = len(g["L0/nodeinfo"])
     nb = len(g["L0/boundaryGlobalIndex"])
-    for mine, ref, shape, tol in (("bdMass", "BDmass", (nb, n), 1e-12), ("bdStiffness", "BDstiffness", (nb, n), 1e-12),
-                                  ("bbMass", "BBmass", (nb, nb), 1e-6), ("bbStiffness", "BBstiffness", (nb, nb), 1e-6)):
+    t = coef_tol(g)
+    for mine, ref, shape, tol in (("bdMass", "BDmass", (nb, n), t), ("bdStiffness", "BDstiffness", (nb, n), t),
+                                  ("bbMass", "BBmass", (nb, nb), 1e-6), ("bbStiffness", "BBstiffness", (nb, nb), bb_tol(g))):
         A = s.csr(mine, shape=shape)
         B = golden_csr(g, f"fine/{ref}", shape)
         assert abs(A - B).max() <= tol * abs(B).max(), mine
@@ -84,7 +108,7 @@ def test_coefficient_hierarchy_matches_reference(setup):
         n = len(g[f"L{l}/nodeinfo"])
         assert abs(s.csr("coef.bd", l, (nb, n)) - golden_csr(g, f"L{l}/coef/BD", (nb, n))).max() <= 1e-10 * abs(golden_csr(g, f"L{l}/coef/BD", (nb, n))).max()
         BB = golden_csr(g, f"L{l}/coef/BB", (nb, nb))
-        assert abs(s.csr("coef.bb", l, (nb, nb)) - BB).max() <= 1e-6 * abs(BB).max(), l
+        assert abs(s.csr("coef.bb", l, (nb, nb)) - BB).max() <= bb_tol(g) * abs(BB).max(), l
 
 
 def test_filtering_rhs_matches_reference(setup):
@@ -92,6 +116,8 @@ def test_filtering_rhs_matches_reference(setup):
     g, h, s = setup
     lam, sharp = g["meta/weights"]
     f = texel_signal(h, golden_mesh(g)["texture"])
+    if f.shape[1] == 1:  # single-channel texture: the harness replicates it into RGB
+        f = np.repeat(f, 3, axis=1)
     np.testing.assert_array_equal(f, g["solve/f"])
     b = texture_filtering_rhs(s, f, lam, sharp)
     assert rel(b, g["solve/rhs"]) < 2e-6  # the BB block differs at ~1e-8 of its largest entry (module docstring)
@@ -102,7 +128,7 @@ def test_vcycle_contracts_residual(setup):
     b = g["solve/rhs"]
     x = s.vcycle(np.zeros_like(b, dtype=np.float32), b.astype(np.float32))
     r = s.residual(b, x.astype(np.float64))
-    assert r.max() < 0.2, r
+    assert r.max() < (0.9 if "mesh/field" in g else 0.2), r
 
 
 @pytest.mark.parametrize("precision,tol", [("mixed", 1e-6), ("mixed", 1e-8), ("fp64", 1e-8)])
@@ -110,7 +136,7 @@ def test_solve_matches_reference_solution(setup, precision, tol):
     import port
     g, _, s = setup
     b = g["solve/rhs"]
-    x, rep = s.solve(b, tol=tol, precision=precision)
+    x, rep = s.solve(b, tol=tol, precision=precision, max_iters=MAX_ITERS)
     assert rep["converged"] and rep["rel_residual_max"] <= tol
     assert s.residual(b, x).max() <= tol
     A = ref_full(g)
@@ -120,16 +146,16 @@ def test_solve_matches_reference_solution(setup, precision, tol):
 def test_batched_and_single_rhs_agree(setup):
     g, _, s = setup
     b = g["solve/rhs"]
-    xb, _ = s.solve(b, tol=1e-8)
+    xb, _ = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
     for c in range(b.shape[1]):
-        xc, _ = s.solve(b[:, c], tol=1e-8)
+        xc, _ = s.solve(b[:, c], tol=1e-8, max_iters=MAX_ITERS)
         assert rel(xc[:, 0], xb[:, c]) < 1e-4 or np.abs(xc[:, 0] - xb[:, c]).max() < 1e-5 * np.abs(xb).max()
 
 
 def test_solve_is_deterministic(setup):
     g, _, s = setup
     b = g["solve/rhs"]
-    x1, r1 = s.solve(b, tol=1e-6)
-    x2, r2 = s.solve(b, tol=1e-6)
+    x1, r1 = s.solve(b, tol=1e-6, max_iters=MAX_ITERS)
+    x2, r2 = s.solve(b, tol=1e-6, max_iters=MAX_ITERS)
     assert r1["iterations"] == r2["iterations"]
     np.testing.assert_array_equal(x1, x2)

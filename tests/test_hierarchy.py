@@ -6,7 +6,7 @@ import pytest
 
 from conftest import golden_csr, golden_mesh, load_golden
 
-CASES = ["torus128", "torus256", "ico256"]
+CASES = ["torus128", "torus256", "ico256", "genus2lic512"]
 NAMES = {"nodeinfo": "nodeinfo", "boundaryGlobalIndex": "boundaryGlobal", "deepGlobalIndex": "deepGlobal",
          "boundaryAndDeepIndex": "boundaryAndDeep", "rasterLines": "rasterLines", "restrictionLines": "restrictionLines",
          "deepLines": "deepLines", "prolongationLines": "prolongationLines", "charts_i": "charts"}
