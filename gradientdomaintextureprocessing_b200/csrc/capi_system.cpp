@@ -92,9 +92,22 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
     if (out) std::memcpy(out, v, sizeof(v));
     return GDTP_OK;
   }
+  if (name == "profile.levels") {  // {steps timed, levels L, down ms x (L-1), coarse ms, up ms x (L-1)}
+    const DeviceSystem& d = *s->sys;
+    std::vector<double> v{d.traceCount, double(d.traceDownMs.size() + 1)};
+    v.insert(v.end(), d.traceDownMs.begin(), d.traceDownMs.end());
+    v.push_back(d.traceCoarseMs);
+    v.insert(v.end(), d.traceUpMs.begin(), d.traceUpMs.end());
+    return vec(v);
+  }
   if (name == "profile.reset") {
-    const_cast<DeviceSystem*>(s->sys.get())->profCount = 0;
-    const_cast<DeviceSystem*>(s->sys.get())->profMs = 0;
+    DeviceSystem* d = const_cast<DeviceSystem*>(s->sys.get());
+    d->profCount = 0;
+    d->profMs = 0;
+    d->traceCount = 0;
+    d->traceCoarseMs = 0;
+    d->traceDownMs.clear();
+    d->traceUpMs.clear();
     if (count) *count = 0;
     return GDTP_OK;
   }
@@ -185,6 +198,7 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
   else if (k == "max_block" && v >= 16 && v <= dev::kBoundaryChunkMax) kn.maxBlock = v;
   else if (k == "max_coarse" && v >= 16 && v <= 12000) kn.maxCoarse = v;
   else if (k == "programmatic_launch" && (v == 0 || v == 1)) dev::set_programmatic_launch(v != 0);
+  else if (k == "trace_levels" && (v == 0 || v == 1)) kn.traceLevels = v;
   else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
   s->sys->invalidate_graph();
   return GDTP_OK;

@@ -67,6 +67,7 @@ DeviceSystem::~DeviceSystem() {
   cudaSetDevice(device_);
   if (iterGraph_) cudaGraphExecDestroy(iterGraph_);
   if (profEv_[0]) { cudaEventDestroy(profEv_[0]); cudaEventDestroy(profEv_[1]); }
+  for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
   if (sumsHost_) cudaFreeHost(sumsHost_);
   mg32_.reset();
   mg64_.reset();
@@ -427,10 +428,16 @@ template bool DeviceSystem::build_multigrid<double>(Multigrid<double>&, int);
 // ----------------------------------------------------------------------------
 // V-cycle
 // ----------------------------------------------------------------------------
+void DeviceSystem::trace_mark(int i, cudaStream_t s) {
+  if (!profiling_ || !knobs.traceLevels || i >= (int)traceEv_.size()) return;
+  cudaEventRecordWithFlags(traceEv_[i], s, cudaEventRecordExternal);
+}
+
 template <typename T, int W>
 void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
   const int L = (int)mg.levels.size();
   const int KP = mg.KP;
+  trace_mark(0, s);
   for (int l = 0; l + 1 < L; l++) {
     LevelDev<T>& D = mg.levels[l];
     LevelDev<T>& C = mg.levels[l + 1];
@@ -445,8 +452,10 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
     }
     dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
     dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, D.r, C.b, C.x, C.n, KP, s);
+    trace_mark(l + 1, s);
   }
   dev::launch_coarse_solve<T, W>(mg.coarseN, mg.coarseInv, mg.coarseScale, mg.levels[L - 1].b, mg.levels[L - 1].x, KP, s);
+  trace_mark(L, s);
   for (int l = L - 2; l >= 0; l--) {
     LevelDev<T>& D = mg.levels[l];
     dev::launch_prolong_add<T, W>(D.pruns, D.nPRuns, mg.levels[l + 1].x, D.x, KP, s);
@@ -454,6 +463,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
     for (int sw = 0; sw < knobs.postSweeps; sw++)
       for (int c = 3; c >= 0; c--)
         dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
+    trace_mark(L + 1 + (L - 2 - l), s);
   }
 }
 
@@ -588,6 +598,11 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
       cudaEventCreate(&profEv_[1]);
     }
     profiling_ = true;
+    if (knobs.traceLevels && traceEv_.size() != size_t(2 * mg.levels.size())) {
+      for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
+      traceEv_.assign(2 * mg.levels.size(), nullptr);
+      for (cudaEvent_t& e : traceEv_) cudaEventCreate(&e);
+    }
     if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
     // D0.x (the correction) is zero on entry: cleared before the first step
     // and by the correction update of every step
@@ -643,6 +658,22 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
       return false;
     it++;
     rm = rel_max();
+    if (knobs.traceLevels && traceEv_.size() == size_t(2 * mg.levels.size())) {
+      const int L = (int)mg.levels.size();
+      std::vector<float> t(2 * L, 0.f);
+      bool okT = true;
+      for (int i = 1; i < 2 * L; i++) okT = okT && cudaEventElapsedTime(&t[i], traceEv_[i - 1], traceEv_[i]) == cudaSuccess;
+      if (okT) {
+        traceDownMs.resize(L - 1, 0.0);
+        traceUpMs.resize(L - 1, 0.0);
+        for (int l = 0; l + 1 < L; l++) traceDownMs[l] += t[l + 1];
+        traceCoarseMs += t[L];
+        for (int l = L - 2; l >= 0; l--) traceUpMs[l] += t[L + 1 + (L - 2 - l)];
+        traceCount += 1;
+      } else {
+        cudaGetLastError();
+      }
+    }
     float pm = 0;
     if (cudaEventElapsedTime(&pm, profEv_[0], profEv_[1]) == cudaSuccess) {
       profCount += 1;

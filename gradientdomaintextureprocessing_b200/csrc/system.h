@@ -110,6 +110,7 @@ struct SolverKnobs {
   int preBoundary = 0, postBoundary = 1;  // exact boundary solve before the pre / post sweeps
   int maxBlock = 384;                   // boundary subdomain size
   int maxCoarse = 2600;                 // coarsest level size limit (texels)
+  int traceLevels = 0;                  // time every level's down / up leg (events in the graph)
 };
 
 struct SolveReport {
@@ -153,6 +154,12 @@ class DeviceSystem {
   // live timing of the level-0 pre-smoothing colour passes inside the captured
   // refinement graph: {launch groups timed, total ms, texels updated per group}
   double profCount = 0, profMs = 0, profTexels = 0;
+  // level trace (knob traceLevels): refinement steps timed, then per level l the
+  // summed ms of its down leg (smoothing, residual, restriction), the coarse
+  // solve, then per level its up leg (prolongation, boundary solve, smoothing)
+  double traceCount = 0;
+  std::vector<double> traceDownMs, traceUpMs;
+  double traceCoarseMs = 0;
   // read-only views for entry points that bring their own buffers
   const RawOperator& raw_system_operator() const { return rawA_; }
   bool is_updated() const { return updated_; }
@@ -195,6 +202,8 @@ class DeviceSystem {
   double* sumsHost_ = nullptr;  // pinned
   cudaGraphExec_t iterGraph_ = nullptr;
   cudaEvent_t profEv_[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> traceEv_;   // 2 L markers of the captured V-cycle (traceLevels)
+  void trace_mark(int i, cudaStream_t s);
   int iterGraphK_ = -1;
   const double *iterGraphB_ = nullptr, *iterGraphX_ = nullptr;
 };
