@@ -55,6 +55,7 @@ _SIGS = {
     "gdtp_solve_fp64": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.POINTER(Report)]),
     "gdtp_residual": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "gdtp_system_set": (C.c_int, [_P, C.c_char_p, C.c_double]),
+    "gdtp_system_get": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_double)]),
     "gdtp_system_autotune": (C.c_int, [_P, _P, C.c_int, C.c_double, _P]),
     "gdtp_residual_static": (C.c_int, [_P, _P, _P, _P, C.c_int, _P, _P]),
     "gdtp_system_device_bytes": (C.c_int, [_P, C.POINTER(C.c_int64)]),

@@ -100,6 +100,12 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
     v.insert(v.end(), d.traceUpMs.begin(), d.traceUpMs.end());
     return vec(v);
   }
+  if (name == "profile.cluster") {  // {code, ns} pairs of the last traced cluster launch, start at [1022]
+    std::vector<unsigned long long> t;
+    if (!const_cast<DeviceSystem*>(s->sys.get())->cluster_timeline(t)) return fail(GDTP_ERR_CUDA, s->sys->error());
+    std::vector<double> v(t.begin(), t.end());
+    return vec(v);
+  }
   if (name == "profile.reset") {
     DeviceSystem* d = const_cast<DeviceSystem*>(s->sys.get());
     d->profCount = 0;
@@ -199,8 +205,32 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
   else if (k == "max_coarse" && v >= 16 && v <= 12000) kn.maxCoarse = v;
   else if (k == "programmatic_launch" && (v == 0 || v == 1)) dev::set_programmatic_launch(v != 0);
   else if (k == "trace_levels" && (v == 0 || v == 1)) kn.traceLevels = v;
+  else if (k == "cluster_texels" && v >= 0) kn.clusterTexels = v;
+  else if (k == "coarse_pre_sweeps" && v >= -1 && v <= 16) kn.coarsePreSweeps = v;
+  else if (k == "coarse_post_sweeps" && v >= -1 && v <= 16) kn.coarsePostSweeps = v;
+  else if (k == "coarse_from" && v >= 1 && v <= 16) kn.coarseFrom = v;
   else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
   s->sys->invalidate_graph();
+  return GDTP_OK;
+}
+
+extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* value) {
+  if (!s || !s->sys || !knob || !value) return fail(GDTP_ERR_INVALID, "gdtp_system_get: bad arguments");
+  const std::string k(knob);
+  const SolverKnobs& kn = s->sys->knobs;
+  if (k == "pre_sweeps") *value = kn.preSweeps;
+  else if (k == "post_sweeps") *value = kn.postSweeps;
+  else if (k == "pre_boundary") *value = kn.preBoundary;
+  else if (k == "post_boundary") *value = kn.postBoundary;
+  else if (k == "max_block") *value = kn.maxBlock;
+  else if (k == "max_coarse") *value = kn.maxCoarse;
+  else if (k == "programmatic_launch") *value = dev::programmatic_launch() ? 1 : 0;
+  else if (k == "trace_levels") *value = kn.traceLevels;
+  else if (k == "cluster_texels") *value = kn.clusterTexels;
+  else if (k == "coarse_pre_sweeps") *value = kn.coarsePreSweeps;
+  else if (k == "coarse_post_sweeps") *value = kn.coarsePostSweeps;
+  else if (k == "coarse_from") *value = kn.coarseFrom;
+  else return fail(GDTP_ERR_INVALID, "gdtp_system_get: unknown knob " + k);
   return GDTP_OK;
 }
 

@@ -12,15 +12,10 @@
 
 #include "vcycle.cuh"
 #include "vcycle_kernels.h"
+#include "vcycle_ops.cuh"
 
 namespace gdtp {
 namespace dev {
-
-template <typename T, int W>
-__device__ __forceinline__ void axpy(Vec<T, W>& acc, T a, const Vec<T, W>& v) {
-#pragma unroll
-  for (int c = 0; c < W; c++) acc.v[c] += a * v.v[c];
-}
 
 // ----------------------------------------------------------------------------
 // Gauss-Seidel on one colour: x = rhs*c4 - sum_{k!=4} c_k x_k
@@ -30,34 +25,7 @@ __global__ void __launch_bounds__(256) k_gs_colour(const ColourRun* __restrict__
                                                    int planeStride, const T* __restrict__ rhs, T* __restrict__ x, int KP, int G) {
   grid_dependency_wait();
   grid_launch_dependents();
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int per = 32 * G;
-  const long long r = t / per;
-  if (r >= nRuns) return;
-  const int rem = int(t - r * per);
-  const int m = rem / G, q = rem - m * G;
-  const ColourRun R = runs[r];
-  if (m >= R.len) return;
-  const int pos = R.pos0 + 2 * m, pp = R.prev0 + 2 * m, pn = R.next0 + 2 * m;
-  const T* c = coef + R.coef0 + m;
-  const int off = q * W;
-  Vec<T, W> acc;
-#pragma unroll
-  for (int k = 0; k < W; k++) acc.v[k] = 0;
-  axpy(acc, c[0 * planeStride], vload<T, W>(x + (long long)(pp - 1) * KP + off));
-  axpy(acc, c[1 * planeStride], vload<T, W>(x + (long long)(pp)*KP + off));
-  axpy(acc, c[2 * planeStride], vload<T, W>(x + (long long)(pp + 1) * KP + off));
-  axpy(acc, c[3 * planeStride], vload<T, W>(x + (long long)(pos - 1) * KP + off));
-  axpy(acc, c[5 * planeStride], vload<T, W>(x + (long long)(pos + 1) * KP + off));
-  axpy(acc, c[6 * planeStride], vload<T, W>(x + (long long)(pn - 1) * KP + off));
-  axpy(acc, c[7 * planeStride], vload<T, W>(x + (long long)(pn)*KP + off));
-  axpy(acc, c[8 * planeStride], vload<T, W>(x + (long long)(pn + 1) * KP + off));
-  const T c4 = c[4 * planeStride];
-  const Vec<T, W> b = vload<T, W>(rhs + (long long)pos * KP + off);
-  Vec<T, W> out;
-#pragma unroll
-  for (int k = 0; k < W; k++) out.v[k] = b.v[k] * c4 - acc.v[k];
-  vstore<T, W>(x + (long long)pos * KP + off, out);
+  gs_item<T, W, LoadDefault>(runs, nRuns, coef, planeStride, rhs, x, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ----------------------------------------------------------------------------
@@ -72,43 +40,12 @@ __global__ void __launch_bounds__(256) k_residual(const ColourRun* __restrict__ 
                                                   const T* __restrict__ x, T* __restrict__ res, int KP, int G) {
   grid_dependency_wait();
   grid_launch_dependents();
-  if ((int)blockIdx.x < deepBlocks) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int per = 32 * G;
-    const long long r = t / per;
-    if (r >= nRuns) return;
-    const int rem = int(t - r * per);
-    const int m = rem / G, q = rem - m * G;
-    const ColourRun R = runs[r];
-    if (m >= R.len) return;
-    const int pos = R.pos0 + 2 * m, pp = R.prev0 + 2 * m, pn = R.next0 + 2 * m;
-    const T* c = coef + R.coef0 + m;
-    const int off = q * W;
-    Vec<T, W> acc = vload<T, W>(x + (long long)pos * KP + off);
-    axpy(acc, c[0 * planeStride], vload<T, W>(x + (long long)(pp - 1) * KP + off));
-    axpy(acc, c[1 * planeStride], vload<T, W>(x + (long long)(pp)*KP + off));
-    axpy(acc, c[2 * planeStride], vload<T, W>(x + (long long)(pp + 1) * KP + off));
-    axpy(acc, c[3 * planeStride], vload<T, W>(x + (long long)(pos - 1) * KP + off));
-    axpy(acc, c[5 * planeStride], vload<T, W>(x + (long long)(pos + 1) * KP + off));
-    axpy(acc, c[6 * planeStride], vload<T, W>(x + (long long)(pn - 1) * KP + off));
-    axpy(acc, c[7 * planeStride], vload<T, W>(x + (long long)(pn)*KP + off));
-    axpy(acc, c[8 * planeStride], vload<T, W>(x + (long long)(pn + 1) * KP + off));
-    const T c9 = c[9 * planeStride];
-    const Vec<T, W> b = vload<T, W>(rhs + (long long)pos * KP + off);
-    Vec<T, W> out;
-#pragma unroll
-    for (int k = 0; k < W; k++) out.v[k] = b.v[k] - acc.v[k] * c9;
-    vstore<T, W>(res + (long long)pos * KP + off, out);
-  } else {
-    const long long t = (long long)(blockIdx.x - deepBlocks) * blockDim.x + threadIdx.x;
-    const long long row = t / G;
-    if (row >= nB) return;
-    const int q = int(t - row * G), off = q * W;
-    const int g = bGlobal[row];
-    Vec<T, W> acc = vload<T, W>(rhs + (long long)g * KP + off);
-    for (int k = bPtr[row]; k < bPtr[row + 1]; k++) axpy(acc, -bVal[k], vload<T, W>(x + (long long)bCol[k] * KP + off));
-    vstore<T, W>(res + (long long)g * KP + off, acc);
-  }
+  if ((int)blockIdx.x < deepBlocks)
+    residual_deep_item<T, W, LoadDefault>(runs, nRuns, coef, planeStride, rhs, x, res, KP, G,
+                                          (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  else
+    residual_boundary_item<T, W, LoadDefault>(bPtr, bCol, bVal, bGlobal, nB, rhs, x, res, KP, G,
+                                              (long long)(blockIdx.x - deepBlocks) * blockDim.x + threadIdx.x);
 }
 
 // ----------------------------------------------------------------------------
@@ -125,37 +62,11 @@ __global__ void __launch_bounds__(256) k_restrict(const RestrictRun* __restrict_
   // the coarse iterate starts from zero: cleared here (grid-stride)
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < coarseVals; i += (long long)gridDim.x * blockDim.x)
     coarseX[i] = T(0);
-  if ((int)blockIdx.x < deepBlocks) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int per = 32 * G;
-    const long long r = t / per;
-    if (r >= nRuns) return;
-    const int rem = int(t - r * per);
-    const int m = rem / G, q = rem - m * G;
-    const RestrictRun R = runs[r];
-    if (m >= R.len) return;
-    const int f = R.f0 + 2 * m, fp = R.fp0 + 2 * m, fn = R.fn0 + 2 * m, off = q * W;
-    const Vec<T, W> a0 = vload<T, W>(res + (long long)f * KP + off);
-    const Vec<T, W> e1 = vload<T, W>(res + (long long)fp * KP + off), e2 = vload<T, W>(res + (long long)(f - 1) * KP + off),
-                    e3 = vload<T, W>(res + (long long)(f + 1) * KP + off), e4 = vload<T, W>(res + (long long)fn * KP + off);
-    const Vec<T, W> d1 = vload<T, W>(res + (long long)(fp - 1) * KP + off), d2 = vload<T, W>(res + (long long)(fp + 1) * KP + off),
-                    d3 = vload<T, W>(res + (long long)(fn - 1) * KP + off), d4 = vload<T, W>(res + (long long)(fn + 1) * KP + off);
-    Vec<T, W> out;
-#pragma unroll
-    for (int k = 0; k < W; k++)
-      out.v[k] = a0.v[k] + (e1.v[k] + e2.v[k] + e3.v[k] + e4.v[k]) * T(0.5) + (d1.v[k] + d2.v[k] + d3.v[k] + d4.v[k]) * T(0.25);
-    vstore<T, W>(coarseRhs + (long long)(R.out0 + m) * KP + off, out);
-  } else {
-    const long long t = (long long)(blockIdx.x - deepBlocks) * blockDim.x + threadIdx.x;
-    const long long row = t / G;
-    if (row >= nB) return;
-    const int q = int(t - row * G), off = q * W;
-    Vec<T, W> acc;
-#pragma unroll
-    for (int k = 0; k < W; k++) acc.v[k] = 0;
-    for (int k = rPtr[row]; k < rPtr[row + 1]; k++) axpy(acc, rVal[k], vload<T, W>(res + (long long)rCol[k] * KP + off));
-    vstore<T, W>(coarseRhs + (long long)rOut[row] * KP + off, acc);
-  }
+  if ((int)blockIdx.x < deepBlocks)
+    restrict_deep_item<T, W, LoadDefault>(runs, nRuns, res, coarseRhs, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  else
+    restrict_boundary_item<T, W, LoadDefault>(rPtr, rCol, rVal, rOut, nB, res, coarseRhs, KP, G,
+                                              (long long)(blockIdx.x - deepBlocks) * blockDim.x + threadIdx.x);
 }
 
 // ----------------------------------------------------------------------------
@@ -166,29 +77,7 @@ __global__ void __launch_bounds__(256) k_prolong_add(const ProlongRun* __restric
                                                      T* __restrict__ fine, int KP, int G) {
   grid_dependency_wait();
   grid_launch_dependents();
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int per = 32 * G;
-  const long long r = t / per;
-  if (r >= nRuns) return;
-  const int rem = int(t - r * per);
-  const int m = rem / G, q = rem - m * G;
-  const ProlongRun R = runs[r];
-  if (m >= R.len) return;
-  const int i = R.i0 + m, o = R.aligned ? 0 : 1, off = q * W;
-  const int p = (i + o) / 2, n = (i + o + 1) / 2;
-  T* dst = fine + (long long)(R.f0 + m) * KP + off;
-  Vec<T, W> acc = vload<T, W>(dst);
-  if (R.center >= 0) {
-    const Vec<T, W> a = vload<T, W>(coarse + (long long)(R.center + p) * KP + off), b = vload<T, W>(coarse + (long long)(R.center + n) * KP + off);
-#pragma unroll
-    for (int k = 0; k < W; k++) acc.v[k] += (a.v[k] + b.v[k]) * T(0.5);
-  } else {
-    const Vec<T, W> a = vload<T, W>(coarse + (long long)(R.prev + p) * KP + off), b = vload<T, W>(coarse + (long long)(R.prev + n) * KP + off),
-                    c = vload<T, W>(coarse + (long long)(R.next + p) * KP + off), d = vload<T, W>(coarse + (long long)(R.next + n) * KP + off);
-#pragma unroll
-    for (int k = 0; k < W; k++) acc.v[k] += (a.v[k] + b.v[k] + c.v[k] + d.v[k]) * T(0.25);
-  }
-  vstore<T, W>(dst, acc);
+  prolong_item<T, W, LoadDefault>(runs, nRuns, coarse, fine, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ----------------------------------------------------------------------------
@@ -207,16 +96,6 @@ __global__ void __launch_bounds__(256) k_prolong_add(const ProlongRun* __restric
 // result does not depend on scheduling.  Chunking keeps the dependent-load
 // chain of each warp short on the small coarse levels.
 // ----------------------------------------------------------------------------
-template <typename T>
-struct Quad;
-template <>
-struct __align__(16) Quad<float> {
-  float v[4];
-};
-template <>
-struct __align__(32) Quad<double> {
-  double v[4];
-};
 
 template <typename T, int W>
 __global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode, const T* __restrict__ rhs, T* __restrict__ x, int KP,
@@ -238,17 +117,7 @@ __global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode,
   for (int q = 0; q < G; q++) {
     const int off = q * W;
     // prologue: the chunk's input vector (scaled boundary right-hand side)
-    for (int j = j0 + (int)threadIdx.x; j < j1; j += blockDim.x) {
-      const int k = (mode == 0 ? r0 : B.nI) + j;  // solver position
-      Vec<T, W> acc = vload<T, W>(rhs + (long long)B.posGlobal[k] * KP + off);
-      for (int e = B.bdPtr[k]; e < B.bdPtr[k + 1]; e++) axpy(acc, -B.bdVal[e], vload<T, W>(x + (long long)B.bdCol[e] * KP + off));
-      const T sc = B.scale[k];
-#pragma unroll
-      for (int c = 0; c < W; c++) acc.v[c] *= sc;
-      if (mode == 1)
-        for (int e = B.asiPtr[j]; e < B.asiPtr[j + 1]; e++) axpy(acc, -B.asiVal[e], vload<T, W>(B.y + (long long)B.asiCol[e] * KP + off));
-      vin[j - j0] = acc;
-    }
+    for (int j = j0 + (int)threadIdx.x; j < j1; j += blockDim.x) vin[j - j0] = bs_input<T, W, LoadDefault>(B, mode, r0, j, rhs, x, KP, off);
     __syncthreads();
     T acc[4][W];
 #pragma unroll
@@ -340,19 +209,7 @@ template <typename T, int W>
 __global__ void __launch_bounds__(256) k_bs_back(BoundaryDev<T> B, T* __restrict__ x, int KP, int G) {
   grid_dependency_wait();
   grid_launch_dependents();
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long i = tid / G;
-  if (i >= B.nI) return;
-  const int q = int(tid - i * G), off = q * W;
-  const int p = B.rowSub[i], b0 = B.subPtr[p], m = B.subPtr[p + 1] - b0, a = int(i) - b0;
-  Vec<T, W> acc = vload<T, W>(B.y + i * KP + off);
-  const T* Wp = B.wt + B.wOff[p] + a;
-  for (int e = B.touchPtr[p]; e < B.touchPtr[p + 1]; e++, Wp += m)
-    axpy(acc, -*Wp, vload<T, W>(B.xs + (long long)B.touch[e] * KP + off));
-  const T sc = B.scale[i];
-#pragma unroll
-  for (int c = 0; c < W; c++) acc.v[c] *= sc;
-  vstore<T, W>(x + (long long)B.posGlobal[i] * KP + off, acc);
+  bs_back_item<T, W, LoadDefault>(B, x, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ----------------------------------------------------------------------------
@@ -365,28 +222,7 @@ __global__ void __launch_bounds__(256) k_coarse_solve(int n, const double* __res
   grid_launch_dependents();
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= n) return;
-  const double* row = ainv + (long long)warp * n;
-  for (int q = 0; q < G; q++) {
-    const int off = q * W;
-    double acc[W];
-#pragma unroll
-    for (int c = 0; c < W; c++) acc[c] = 0;
-    for (int j = lane; j < n; j += 32) {
-      const Vec<T, W> v = vload<T, W>(rhs + (long long)j * KP + off);
-      const double w = row[j] * scale[j];
-#pragma unroll
-      for (int c = 0; c < W; c++) acc[c] += w * double(v.v[c]);
-    }
-#pragma unroll
-    for (int c = 0; c < W; c++)
-      for (int s = 16; s > 0; s >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], s);
-    if (lane == 0) {
-      Vec<T, W> out;
-#pragma unroll
-      for (int c = 0; c < W; c++) out.v[c] = T(acc[c] * scale[warp]);
-      vstore<T, W>(x + (long long)warp * KP + off, out);
-    }
-  }
+  coarse_row<T, W, LoadDefault>(n, ainv, scale, rhs, x, KP, G, warp, lane);
 }
 
 // ----------------------------------------------------------------------------

@@ -44,6 +44,28 @@ struct BoundaryDev {
   int *subCount = nullptr, *schurCount = nullptr;                            // chunk arrival counters (zero between launches)
 };
 
+// One multigrid level on the device, value type T (plain pointers and counts;
+// also read by the cluster kernel from a device-side array).
+template <typename T>
+struct LevelDev {
+  int n = 0, nDeep = 0, nB = 0;
+  const ColourRun* runs = nullptr;
+  int nRuns = 0, runStart[5] = {0, 0, 0, 0, 0};
+  const T* coef = nullptr;      // 10 planes, reciprocal form
+  int planeStride = 0;
+  const int *bPtr = nullptr, *bCol = nullptr, *bGlobal = nullptr;
+  const T* bVal = nullptr;      // boundary rows: BD + BB with global columns
+  BoundaryDev<T> B;
+  const RestrictRun* rruns = nullptr;  // to the next level
+  int nRRuns = 0;
+  const int *rbPtr = nullptr, *rbCol = nullptr, *rbOut = nullptr;
+  const T* rbVal = nullptr;
+  int nRB = 0;
+  const ProlongRun* pruns = nullptr;   // from the next level
+  int nPRuns = 0;
+  T *x = nullptr, *b = nullptr, *r = nullptr;
+};
+
 template <typename T, int W>
 void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP, cudaStream_t s);
 template <typename T, int W>
@@ -73,6 +95,18 @@ void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaSt
 // x += e, then e = 0
 template <typename T>
 void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s);
+// Coarse levels l0 .. L-1 in one thread-block cluster (coarse_cycle.cu).
+// leg 0: down leg of levels l0..L-2 (pre-smoothing, residual, restriction);
+// leg 1: up leg (prolongation, boundary solve, post-smoothing); leg 2: both with
+// the coarsest dense solve in between.  lvDev: device array of all levels.
+// timeline (optional, 1024 entries): {phase code, globaltimer ns} pairs after each
+// phase, start time in [1022].  Returns false when no cluster can run.
+template <typename T, int W>
+bool launch_coarse_cycle(const LevelDev<T>* lvDev, int l0, int L, int leg, int preSweeps, int postSweeps, int preBoundary,
+                         int postBoundary, int KP, int coarseN, const double* coarseInv, const double* coarseScale,
+                         unsigned long long* timeline, cudaStream_t s);
+// CTAs of the coarse-level cluster on this device (0: clusters unavailable)
+int coarse_cycle_cluster_ctas(bool fp64, int W);
 // Programmatic dependent launch of the V-cycle kernels (process-wide, default on)
 void set_programmatic_launch(bool on);
 bool programmatic_launch();

@@ -1,0 +1,284 @@
+// Per-item bodies of the V-cycle operators, shared by the one-launch-per-phase
+// kernels (vcycle_kernels.cu) and the cluster-resident coarse-level kernel
+// (coarse_cycle.cu), so both run the same arithmetic in the same order.
+//
+// An "item" is one texel (or boundary row) and one group of W channels; a
+// launch or a cluster loop hands out item indices.  LD selects how mutable
+// vectors (x, rhs, residual, boundary work) are read: LoadDefault for kernels
+// that only read data written by earlier launches, LoadL2 (ld.global.cg, L2
+// only) for the cluster kernel, whose phases read what other CTAs wrote in the
+// previous phase of the same launch.
+#pragma once
+#include "vcycle.cuh"
+#include "vcycle_kernels.h"
+
+namespace gdtp {
+namespace dev {
+
+struct LoadDefault {
+  template <typename T, int W>
+  static __device__ __forceinline__ Vec<T, W> ld(const T* p) { return vload<T, W>(p); }
+};
+
+struct LoadL2 {
+  template <typename T, int W>
+  static __device__ __forceinline__ Vec<T, W> ld(const T* p);
+};
+template <>
+__device__ __forceinline__ Vec<float, 4> LoadL2::ld<float, 4>(const float* p) {
+  const float4 v = __ldcg(reinterpret_cast<const float4*>(p));
+  Vec<float, 4> r;
+  r.v[0] = v.x; r.v[1] = v.y; r.v[2] = v.z; r.v[3] = v.w;
+  return r;
+}
+template <>
+__device__ __forceinline__ Vec<float, 1> LoadL2::ld<float, 1>(const float* p) {
+  Vec<float, 1> r;
+  r.v[0] = __ldcg(p);
+  return r;
+}
+template <>
+__device__ __forceinline__ Vec<double, 4> LoadL2::ld<double, 4>(const double* p) {
+  const double2 a = __ldcg(reinterpret_cast<const double2*>(p)), b = __ldcg(reinterpret_cast<const double2*>(p + 2));
+  Vec<double, 4> r;
+  r.v[0] = a.x; r.v[1] = a.y; r.v[2] = b.x; r.v[3] = b.y;
+  return r;
+}
+template <>
+__device__ __forceinline__ Vec<double, 1> LoadL2::ld<double, 1>(const double* p) {
+  Vec<double, 1> r;
+  r.v[0] = __ldcg(p);
+  return r;
+}
+
+// Four consecutive entries of a dense-inverse row (one vector load).
+template <typename T>
+struct Quad;
+template <>
+struct __align__(16) Quad<float> {
+  float v[4];
+};
+template <>
+struct __align__(32) Quad<double> {
+  double v[4];
+};
+
+template <typename T, int W>
+__device__ __forceinline__ void axpy(Vec<T, W>& acc, T a, const Vec<T, W>& v) {
+#pragma unroll
+  for (int c = 0; c < W; c++) acc.v[c] += a * v.v[c];
+}
+
+// Gauss-Seidel update of one colour-run texel: x = rhs*c4 - sum_{k!=4} c_k x_k
+// (IterativeSolvers.inl:449-463).  Items: runs x 32 x G.
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void gs_item(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x,
+                                        int KP, int G, long long t) {
+  const int per = 32 * G;
+  const long long r = t / per;
+  if (r >= nRuns) return;
+  const int rem = int(t - r * per);
+  const int m = rem / G, q = rem - m * G;
+  const ColourRun R = runs[r];
+  if (m >= R.len) return;
+  const int pos = R.pos0 + 2 * m, pp = R.prev0 + 2 * m, pn = R.next0 + 2 * m;
+  const T* c = coef + R.coef0 + m;
+  const int off = q * W;
+  Vec<T, W> acc;
+#pragma unroll
+  for (int k = 0; k < W; k++) acc.v[k] = 0;
+  axpy(acc, c[0 * planeStride], LD::template ld<T, W>(x + (long long)(pp - 1) * KP + off));
+  axpy(acc, c[1 * planeStride], LD::template ld<T, W>(x + (long long)(pp)*KP + off));
+  axpy(acc, c[2 * planeStride], LD::template ld<T, W>(x + (long long)(pp + 1) * KP + off));
+  axpy(acc, c[3 * planeStride], LD::template ld<T, W>(x + (long long)(pos - 1) * KP + off));
+  axpy(acc, c[5 * planeStride], LD::template ld<T, W>(x + (long long)(pos + 1) * KP + off));
+  axpy(acc, c[6 * planeStride], LD::template ld<T, W>(x + (long long)(pn - 1) * KP + off));
+  axpy(acc, c[7 * planeStride], LD::template ld<T, W>(x + (long long)(pn)*KP + off));
+  axpy(acc, c[8 * planeStride], LD::template ld<T, W>(x + (long long)(pn + 1) * KP + off));
+  const T c4 = c[4 * planeStride];
+  const Vec<T, W> b = LD::template ld<T, W>(rhs + (long long)pos * KP + off);
+  Vec<T, W> out;
+#pragma unroll
+  for (int k = 0; k < W; k++) out.v[k] = b.v[k] * c4 - acc.v[k];
+  vstore<T, W>(x + (long long)pos * KP + off, out);
+}
+
+// Deep residual r = rhs - (sum_{k!=4} c_k x_k + x) * c9 (IterativeSolvers.inl:479-493).
+// Items: runs x 32 x G (all colours).
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void residual_deep_item(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs,
+                                                   const T* x, T* res, int KP, int G, long long t) {
+  const int per = 32 * G;
+  const long long r = t / per;
+  if (r >= nRuns) return;
+  const int rem = int(t - r * per);
+  const int m = rem / G, q = rem - m * G;
+  const ColourRun R = runs[r];
+  if (m >= R.len) return;
+  const int pos = R.pos0 + 2 * m, pp = R.prev0 + 2 * m, pn = R.next0 + 2 * m;
+  const T* c = coef + R.coef0 + m;
+  const int off = q * W;
+  Vec<T, W> acc = LD::template ld<T, W>(x + (long long)pos * KP + off);
+  axpy(acc, c[0 * planeStride], LD::template ld<T, W>(x + (long long)(pp - 1) * KP + off));
+  axpy(acc, c[1 * planeStride], LD::template ld<T, W>(x + (long long)(pp)*KP + off));
+  axpy(acc, c[2 * planeStride], LD::template ld<T, W>(x + (long long)(pp + 1) * KP + off));
+  axpy(acc, c[3 * planeStride], LD::template ld<T, W>(x + (long long)(pos - 1) * KP + off));
+  axpy(acc, c[5 * planeStride], LD::template ld<T, W>(x + (long long)(pos + 1) * KP + off));
+  axpy(acc, c[6 * planeStride], LD::template ld<T, W>(x + (long long)(pn - 1) * KP + off));
+  axpy(acc, c[7 * planeStride], LD::template ld<T, W>(x + (long long)(pn)*KP + off));
+  axpy(acc, c[8 * planeStride], LD::template ld<T, W>(x + (long long)(pn + 1) * KP + off));
+  const T c9 = c[9 * planeStride];
+  const Vec<T, W> b = LD::template ld<T, W>(rhs + (long long)pos * KP + off);
+  Vec<T, W> out;
+#pragma unroll
+  for (int k = 0; k < W; k++) out.v[k] = b.v[k] - acc.v[k] * c9;
+  vstore<T, W>(res + (long long)pos * KP + off, out);
+}
+
+// Boundary residual r_B = rhs_B - [BD BB] x (IterativeSolvers.inl:549-555).  Items: rows x G.
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void residual_boundary_item(const int* bPtr, const int* bCol, const T* bVal, const int* bGlobal, int nB,
+                                                       const T* rhs, const T* x, T* res, int KP, int G, long long t) {
+  const long long row = t / G;
+  if (row >= nB) return;
+  const int q = int(t - row * G), off = q * W;
+  const int g = bGlobal[row];
+  Vec<T, W> acc = LD::template ld<T, W>(rhs + (long long)g * KP + off);
+  for (int k = bPtr[row]; k < bPtr[row + 1]; k++) axpy(acc, -bVal[k], LD::template ld<T, W>(x + (long long)bCol[k] * KP + off));
+  vstore<T, W>(res + (long long)g * KP + off, acc);
+}
+
+// Full-weighting restriction of deep lines (IterativeSolvers.inl:1037-1053).  Items: runs x 32 x G.
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void restrict_deep_item(const RestrictRun* runs, int nRuns, const T* res, T* coarseRhs, int KP, int G,
+                                                   long long t) {
+  const int per = 32 * G;
+  const long long r = t / per;
+  if (r >= nRuns) return;
+  const int rem = int(t - r * per);
+  const int m = rem / G, q = rem - m * G;
+  const RestrictRun R = runs[r];
+  if (m >= R.len) return;
+  const int f = R.f0 + 2 * m, fp = R.fp0 + 2 * m, fn = R.fn0 + 2 * m, off = q * W;
+  const Vec<T, W> a0 = LD::template ld<T, W>(res + (long long)f * KP + off);
+  const Vec<T, W> e1 = LD::template ld<T, W>(res + (long long)fp * KP + off), e2 = LD::template ld<T, W>(res + (long long)(f - 1) * KP + off),
+                  e3 = LD::template ld<T, W>(res + (long long)(f + 1) * KP + off), e4 = LD::template ld<T, W>(res + (long long)fn * KP + off);
+  const Vec<T, W> d1 = LD::template ld<T, W>(res + (long long)(fp - 1) * KP + off),
+                  d2 = LD::template ld<T, W>(res + (long long)(fp + 1) * KP + off),
+                  d3 = LD::template ld<T, W>(res + (long long)(fn - 1) * KP + off),
+                  d4 = LD::template ld<T, W>(res + (long long)(fn + 1) * KP + off);
+  Vec<T, W> out;
+#pragma unroll
+  for (int k = 0; k < W; k++)
+    out.v[k] = a0.v[k] + (e1.v[k] + e2.v[k] + e3.v[k] + e4.v[k]) * T(0.5) + (d1.v[k] + d2.v[k] + d3.v[k] + d4.v[k]) * T(0.25);
+  vstore<T, W>(coarseRhs + (long long)(R.out0 + m) * KP + off, out);
+}
+
+// Sparse boundary restriction rows.  Items: rows x G.
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void restrict_boundary_item(const int* rPtr, const int* rCol, const T* rVal, const int* rOut, int nB,
+                                                       const T* res, T* coarseRhs, int KP, int G, long long t) {
+  const long long row = t / G;
+  if (row >= nB) return;
+  const int q = int(t - row * G), off = q * W;
+  Vec<T, W> acc;
+#pragma unroll
+  for (int k = 0; k < W; k++) acc.v[k] = 0;
+  for (int k = rPtr[row]; k < rPtr[row + 1]; k++) axpy(acc, rVal[k], LD::template ld<T, W>(res + (long long)rCol[k] * KP + off));
+  vstore<T, W>(coarseRhs + (long long)rOut[row] * KP + off, acc);
+}
+
+// Bilinear prolongation added to the fine iterate (IterativeSolvers.inl:1128-1151).  Items: runs x 32 x G.
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void prolong_item(const ProlongRun* runs, int nRuns, const T* coarse, T* fine, int KP, int G, long long t) {
+  const int per = 32 * G;
+  const long long r = t / per;
+  if (r >= nRuns) return;
+  const int rem = int(t - r * per);
+  const int m = rem / G, q = rem - m * G;
+  const ProlongRun R = runs[r];
+  if (m >= R.len) return;
+  const int i = R.i0 + m, o = R.aligned ? 0 : 1, off = q * W;
+  const int p = (i + o) / 2, n = (i + o + 1) / 2;
+  T* dst = fine + (long long)(R.f0 + m) * KP + off;
+  Vec<T, W> acc = LD::template ld<T, W>(dst);
+  if (R.center >= 0) {
+    const Vec<T, W> a = LD::template ld<T, W>(coarse + (long long)(R.center + p) * KP + off),
+                    b = LD::template ld<T, W>(coarse + (long long)(R.center + n) * KP + off);
+#pragma unroll
+    for (int k = 0; k < W; k++) acc.v[k] += (a.v[k] + b.v[k]) * T(0.5);
+  } else {
+    const Vec<T, W> a = LD::template ld<T, W>(coarse + (long long)(R.prev + p) * KP + off),
+                    b = LD::template ld<T, W>(coarse + (long long)(R.prev + n) * KP + off),
+                    c = LD::template ld<T, W>(coarse + (long long)(R.next + p) * KP + off),
+                    d = LD::template ld<T, W>(coarse + (long long)(R.next + n) * KP + off);
+#pragma unroll
+    for (int k = 0; k < W; k++) acc.v[k] += (a.v[k] + b.v[k] + c.v[k] + d.v[k]) * T(0.25);
+  }
+  vstore<T, W>(dst, acc);
+}
+
+// Boundary back substitution x_I = s (y - W_p xs[touch_p]).  Items: interior positions x G.
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void bs_back_item(const BoundaryDev<T>& B, T* x, int KP, int G, long long tid) {
+  const long long i = tid / G;
+  if (i >= B.nI) return;
+  const int q = int(tid - i * G), off = q * W;
+  const int p = B.rowSub[i], b0 = B.subPtr[p], m = B.subPtr[p + 1] - b0, a = int(i) - b0;
+  Vec<T, W> acc = LD::template ld<T, W>(B.y + i * KP + off);
+  const T* Wp = B.wt + B.wOff[p] + a;
+  for (int e = B.touchPtr[p]; e < B.touchPtr[p + 1]; e++, Wp += m)
+    axpy(acc, -*Wp, LD::template ld<T, W>(B.xs + (long long)B.touch[e] * KP + off));
+  const T sc = B.scale[i];
+#pragma unroll
+  for (int c = 0; c < W; c++) acc.v[c] *= sc;
+  vstore<T, W>(x + (long long)B.posGlobal[i] * KP + off, acc);
+}
+
+// Input of a boundary dense product at position j of a subdomain (mode 0,
+// r^ = s (rhs - BD x)) or of the separator (mode 1, t = r^_S - A_SI y).
+template <typename T, int W, typename LD>
+__device__ __forceinline__ Vec<T, W> bs_input(const BoundaryDev<T>& B, int mode, int r0, int j, const T* rhs, const T* x, int KP,
+                                              int off) {
+  const int k = (mode == 0 ? r0 : B.nI) + j;  // solver position
+  Vec<T, W> acc = LD::template ld<T, W>(rhs + (long long)B.posGlobal[k] * KP + off);
+  for (int e = B.bdPtr[k]; e < B.bdPtr[k + 1]; e++) axpy(acc, -B.bdVal[e], LD::template ld<T, W>(x + (long long)B.bdCol[e] * KP + off));
+  const T sc = B.scale[k];
+#pragma unroll
+  for (int c = 0; c < W; c++) acc.v[c] *= sc;
+  if (mode == 1)
+    for (int e = B.asiPtr[j]; e < B.asiPtr[j + 1]; e++)
+      axpy(acc, -B.asiVal[e], LD::template ld<T, W>(B.y + (long long)B.asiCol[e] * KP + off));
+  return acc;
+}
+
+// Coarsest level, one row per warp: x = D Ainv^ D rhs (FP64 accumulation).
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void coarse_row(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, int G, int row,
+                                           int lane) {
+  const double* arow = ainv + (long long)row * n;
+  for (int q = 0; q < G; q++) {
+    const int off = q * W;
+    double acc[W];
+#pragma unroll
+    for (int c = 0; c < W; c++) acc[c] = 0;
+    for (int j = lane; j < n; j += 32) {
+      const Vec<T, W> v = LD::template ld<T, W>(rhs + (long long)j * KP + off);
+      const double w = arow[j] * scale[j];
+#pragma unroll
+      for (int c = 0; c < W; c++) acc[c] += w * double(v.v[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < W; c++)
+      for (int s = 16; s > 0; s >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], s);
+    if (lane == 0) {
+      Vec<T, W> out;
+#pragma unroll
+      for (int c = 0; c < W; c++) out.v[c] = T(acc[c] * scale[row]);
+      vstore<T, W>(x + (long long)row * KP + off, out);
+    }
+  }
+}
+
+}  // namespace dev
+}  // namespace gdtp

@@ -20,6 +20,9 @@
 
 namespace gdtp {
 
+// coarsest levels up to this size are solved inside the coarse-level cluster
+static const int kClusterCoarseMax = 1024;
+
 static inline int kp_for(int k) {
   if (k <= 1) return 1;
   int kp = 4;
@@ -419,7 +422,10 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     }
   }
   if (!check(A.last, "multigrid upload")) return false;
-  return true;
+  // whether this device can run the coarse-level cluster (queried outside any capture)
+  mg.clusterOK = dev::coarse_cycle_cluster_ctas(sizeof(T) == 8, (KP % 4 == 0) ? 4 : 1) > 0;
+  mg.levelsDev = A.upload(mg.levels);
+  return check(A.last, "multigrid upload");
 }
 
 template bool DeviceSystem::build_multigrid<float>(Multigrid<float>&, int);
@@ -428,6 +434,18 @@ template bool DeviceSystem::build_multigrid<double>(Multigrid<double>&, int);
 // ----------------------------------------------------------------------------
 // V-cycle
 // ----------------------------------------------------------------------------
+bool DeviceSystem::cluster_timeline(std::vector<unsigned long long>& out) {
+  out.clear();
+  if (!timeline_) return true;
+  out.resize(1024);
+  return check(cudaMemcpy(out.data(), timeline_, 1024 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "timeline");
+}
+
+unsigned long long* DeviceSystem::clusterTimeline() {
+  // allocated before the refinement graph is captured (solve_mixed)
+  return (profiling_ && knobs.traceLevels) ? timeline_ : nullptr;
+}
+
 void DeviceSystem::trace_mark(int i, cudaStream_t s) {
   if (!profiling_ || !knobs.traceLevels || i >= (int)traceEv_.size()) return;
   cudaEventRecordWithFlags(traceEv_[i], s, cudaEventRecordExternal);
@@ -437,13 +455,19 @@ template <typename T, int W>
 void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
   const int L = (int)mg.levels.size();
   const int KP = mg.KP;
+  // levels [lc, L) run in the coarse-level cluster when it is enabled: from the
+  // first level below the finest with at most clusterTexels texels
+  int lc = L - 1;
+  if (knobs.clusterTexels > 0 && mg.clusterOK)
+    for (int l = 1; l + 1 < L; l++)
+      if (mg.levels[l].n <= knobs.clusterTexels) { lc = l; break; }
   trace_mark(0, s);
-  for (int l = 0; l + 1 < L; l++) {
+  for (int l = 0; l < lc; l++) {
     LevelDev<T>& D = mg.levels[l];
     LevelDev<T>& C = mg.levels[l + 1];
     // D.x of levels > 0 was cleared by the restriction into this level
     if (knobs.preBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
-    for (int sw = 0; sw < knobs.preSweeps; sw++) {
+    for (int sw = 0; sw < pre_sweeps(l); sw++) {
       const bool prof = profiling_ && l == 0 && sw == 0;
       if (prof) cudaEventRecordWithFlags(profEv_[0], s, cudaEventRecordExternal);
       for (int c = 0; c < 4; c++)
@@ -454,13 +478,29 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
     dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, D.r, C.b, C.x, C.n, KP, s);
     trace_mark(l + 1, s);
   }
-  dev::launch_coarse_solve<T, W>(mg.coarseN, mg.coarseInv, mg.coarseScale, mg.levels[L - 1].b, mg.levels[L - 1].x, KP, s);
-  trace_mark(L, s);
-  for (int l = L - 2; l >= 0; l--) {
+  if (lc < L - 1) {
+    // coarse levels in one cluster; a large coarsest level is solved by the whole GPU in between
+    const bool whole = mg.coarseN <= kClusterCoarseMax;
+    if (whole) {
+      dev::launch_coarse_cycle<T, W>(mg.levelsDev, lc, L, 2, pre_sweeps(lc), post_sweeps(lc), knobs.preBoundary,
+                                     knobs.postBoundary, KP, mg.coarseN, mg.coarseInv, mg.coarseScale, clusterTimeline(), s);
+    } else {
+      dev::launch_coarse_cycle<T, W>(mg.levelsDev, lc, L, 0, pre_sweeps(lc), post_sweeps(lc), knobs.preBoundary,
+                                     knobs.postBoundary, KP, mg.coarseN, mg.coarseInv, mg.coarseScale, clusterTimeline(), s);
+      dev::launch_coarse_solve<T, W>(mg.coarseN, mg.coarseInv, mg.coarseScale, mg.levels[L - 1].b, mg.levels[L - 1].x, KP, s);
+      dev::launch_coarse_cycle<T, W>(mg.levelsDev, lc, L, 1, pre_sweeps(lc), post_sweeps(lc), knobs.preBoundary,
+                                     knobs.postBoundary, KP, mg.coarseN, mg.coarseInv, mg.coarseScale, clusterTimeline(), s);
+    }
+    for (int i = lc + 1; i <= L + 1 + (L - 2 - lc); i++) trace_mark(i, s);  // the cluster's levels count as one segment
+  } else {
+    dev::launch_coarse_solve<T, W>(mg.coarseN, mg.coarseInv, mg.coarseScale, mg.levels[L - 1].b, mg.levels[L - 1].x, KP, s);
+    trace_mark(L, s);
+  }
+  for (int l = std::min(lc, L - 1) - 1; l >= 0; l--) {
     LevelDev<T>& D = mg.levels[l];
     dev::launch_prolong_add<T, W>(D.pruns, D.nPRuns, mg.levels[l + 1].x, D.x, KP, s);
     if (knobs.postBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
-    for (int sw = 0; sw < knobs.postSweeps; sw++)
+    for (int sw = 0; sw < post_sweeps(l); sw++)
       for (int c = 3; c >= 0; c--)
         dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
     trace_mark(L + 1 + (L - 2 - l), s);
@@ -597,6 +637,11 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
       cudaEventCreate(&profEv_[0]);
       cudaEventCreate(&profEv_[1]);
     }
+    if (knobs.traceLevels && !timeline_) {
+      timeline_ = static_cast<unsigned long long*>(rawArena_.alloc(1024 * sizeof(unsigned long long)));
+      if (!check(rawArena_.last, "timeline") || !check(cudaMemset(timeline_, 0, 1024 * sizeof(unsigned long long)), "timeline"))
+        return false;
+    }
     profiling_ = true;
     if (knobs.traceLevels && traceEv_.size() != size_t(2 * mg.levels.size())) {
       for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
@@ -700,33 +745,42 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
 
 bool DeviceSystem::autotune(const double* b, int k, double tol, SolverKnobs& best, double& bestSeconds) {
   if (!err_.empty()) return false;
+  cudaSetDevice(device_);
   const size_t n = h_.levels[0].numTexels;
-  std::vector<double> x(n * k);
+  // b and x stay on the device: only the solve itself is timed
+  DeviceArena tune;
+  double* bDev = tune.upload(std::vector<double>(b, b + n * k));
+  double* xDev = static_cast<double*>(tune.alloc(n * k * sizeof(double)));
+  if (!check(tune.last, "autotune buffers")) return false;
   const SolverKnobs base = knobs;
   bestSeconds = 1e300;
   best = base;
-  // candidates: deep sweeps before / after the coarse correction and where the
-  // exact boundary solve goes (after the correction is required for accuracy
-  // on the way up; before it is optional)
-  const int cand[][4] = {{1, 1, 0, 1}, {1, 2, 0, 1}, {2, 1, 0, 1}, {2, 2, 0, 1}, {2, 3, 0, 1}, {3, 3, 0, 1},
-                         {2, 2, 1, 1}, {1, 1, 1, 1}};
-  for (const auto& c : cand) {
-    knobs = base;
-    knobs.preSweeps = c[0];
-    knobs.postSweeps = c[1];
-    knobs.preBoundary = c[2];
-    knobs.postBoundary = c[3];
-    invalidate_graph();
-    double t = 1e300;
-    for (int rep = 0; rep < 3; rep++) {  // first run captures the graph
-      std::fill(x.begin(), x.end(), 0.0);
-      SolveReport r;
-      if (!solve_mixed(b, x.data(), nullptr, nullptr, k, tol, 60, nullptr, r)) return false;
-      if (r.relMax > tol) { t = 1e300; break; }
-      if (rep > 0) t = std::min(t, r.seconds);
+  // candidates: deep sweeps before / after the coarse correction on the finer
+  // levels, and on the levels from `coarseFrom` on (-1: same as the finer
+  // ones); the exact boundary solve follows the coarse correction
+  const int fine[][2] = {{1, 1}, {2, 2}, {2, 3}, {3, 3}, {3, 4}, {4, 4}};
+  const int coarse[][3] = {{-1, -1, 2}, {0, 1, 2}, {0, 2, 2}, {0, 3, 2}, {1, 1, 2}, {1, 2, 2},
+                           {0, 2, 1}, {0, 3, 1}, {1, 2, 1}, {0, 2, 3}};
+  for (const auto& f : fine)
+    for (const auto& c : coarse) {
+      knobs = base;
+      knobs.preSweeps = f[0];
+      knobs.postSweeps = f[1];
+      knobs.preBoundary = 0;
+      knobs.postBoundary = 1;
+      knobs.coarsePreSweeps = c[0];
+      knobs.coarsePostSweeps = c[1];
+      knobs.coarseFrom = c[2];
+      invalidate_graph();
+      double t = 1e300;
+      for (int rep = 0; rep < 3; rep++) {  // the first run captures the graph
+        SolveReport r;
+        if (!solve_mixed(nullptr, nullptr, bDev, xDev, k, tol, 60, nullptr, r, true)) return false;
+        if (r.relMax > tol) { t = 1e300; break; }
+        if (rep > 0) t = std::min(t, r.seconds);
+      }
+      if (t < bestSeconds) { bestSeconds = t; best = knobs; }
     }
-    if (t < bestSeconds) { bestSeconds = t; best = knobs; }
-  }
   knobs = best;
   invalidate_graph();
   return true;

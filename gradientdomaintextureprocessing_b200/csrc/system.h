@@ -63,26 +63,8 @@ struct DeepRuns {
 };
 DeepRuns build_deep_runs(const GridLevel& L);
 
-// One multigrid level on the device, value type T.
 template <typename T>
-struct LevelDev {
-  int n = 0, nDeep = 0, nB = 0;
-  const dev::ColourRun* runs = nullptr;
-  int nRuns = 0, runStart[5] = {0, 0, 0, 0, 0};
-  const T* coef = nullptr;      // 10 planes, reciprocal form
-  int planeStride = 0;
-  const int *bPtr = nullptr, *bCol = nullptr, *bGlobal = nullptr;
-  const T* bVal = nullptr;      // boundary rows: BD + BB with global columns
-  dev::BoundaryDev<T> B;
-  const dev::RestrictRun* rruns = nullptr;  // to the next level
-  int nRRuns = 0;
-  const int *rbPtr = nullptr, *rbCol = nullptr, *rbOut = nullptr;
-  const T* rbVal = nullptr;
-  int nRB = 0;
-  const dev::ProlongRun* pruns = nullptr;   // from the next level
-  int nPRuns = 0;
-  T *x = nullptr, *b = nullptr, *r = nullptr;
-};
+using LevelDev = dev::LevelDev<T>;
 
 template <typename T>
 struct Multigrid {
@@ -91,6 +73,8 @@ struct Multigrid {
   const double* coarseInv = nullptr;    // scaled dense inverse of the coarsest operator
   const double* coarseScale = nullptr;
   int KP = 0;                           // channel stride the vectors were sized for
+  const dev::LevelDev<T>* levelsDev = nullptr;  // copy of `levels` in device memory (cluster kernel)
+  bool clusterOK = false;               // the device can run the coarse-level cluster
   DeviceArena arena;
 };
 
@@ -111,6 +95,9 @@ struct SolverKnobs {
   int maxBlock = 384;                   // boundary subdomain size
   int maxCoarse = 2600;                 // coarsest level size limit (texels)
   int traceLevels = 0;                  // time every level's down / up leg (events in the graph)
+  int clusterTexels = 0;                // levels up to this size run in one thread-block cluster (0: off)
+  int coarsePreSweeps = -1, coarsePostSweeps = -1;  // sweeps on levels >= coarseFrom (-1: as level 0)
+  int coarseFrom = 2;
 };
 
 struct SolveReport {
@@ -148,6 +135,12 @@ class DeviceSystem {
   bool residual_host(const double* b, const double* x, int k, double* rel);
 
   SolverKnobs knobs;
+  int pre_sweeps(int level) const {
+    return (level >= knobs.coarseFrom && knobs.coarsePreSweeps >= 0) ? knobs.coarsePreSweeps : knobs.preSweeps;
+  }
+  int post_sweeps(int level) const {
+    return (level >= knobs.coarseFrom && knobs.coarsePostSweeps >= 0) ? knobs.coarsePostSweeps : knobs.postSweeps;
+  }
   size_t deviceBytes() const;
   // knobs that change the launch sequence take effect on the next solve
   void invalidate_graph();
@@ -204,6 +197,12 @@ class DeviceSystem {
   cudaEvent_t profEv_[2] = {nullptr, nullptr};
   std::vector<cudaEvent_t> traceEv_;   // 2 L markers of the captured V-cycle (traceLevels)
   void trace_mark(int i, cudaStream_t s);
+  unsigned long long* timeline_ = nullptr;  // cluster phase timeline (traceLevels)
+  unsigned long long* clusterTimeline();
+ public:
+  // last cluster timeline: {code, ns} pairs (empty when not traced)
+  bool cluster_timeline(std::vector<unsigned long long>& out);
+ private:
   int iterGraphK_ = -1;
   const double *iterGraphB_ = nullptr, *iterGraphX_ = nullptr;
 };

@@ -56,13 +56,20 @@ class System:
     def set(self, knob: str, value: float) -> None:
         _lib.check(_lib.lib().gdtp_system_set(self._s, knob.encode(), float(value)))
 
+    def get(self, knob: str) -> float:
+        v = C.c_double()
+        _lib.check(_lib.lib().gdtp_system_get(self._s, knob.encode(), C.byref(v)))
+        return v.value
+
     def autotune(self, b: np.ndarray, tol: float = 1e-6) -> dict:
         """Picks the fastest converging smoother setting for solves like ``b``."""
         b, k = self._vec(b, np.float64)
         out = np.zeros(5)
         _lib.check(_lib.lib().gdtp_system_autotune(self._s, _lib.ptr(b), k, float(tol), _lib.ptr(out)))
-        return {"pre_sweeps": int(out[0]), "post_sweeps": int(out[1]), "pre_boundary": int(out[2]),
-                "post_boundary": int(out[3]), "seconds": float(out[4])}
+        knobs = {name: int(self.get(name)) for name in ("pre_sweeps", "post_sweeps", "pre_boundary", "post_boundary",
+                                                         "coarse_pre_sweeps", "coarse_post_sweeps", "coarse_from")}
+        knobs["seconds"] = float(out[4])
+        return knobs
 
     def device_bytes(self) -> int:
         b = C.c_int64()

@@ -164,15 +164,22 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
                          void* stream);
 
 /* Solver knobs (value as double): "pre_sweeps", "post_sweeps" (deep colour sweeps
- * per smoothing, default 2/2), "pre_boundary", "post_boundary" (exact boundary
- * solve before the pre / post sweeps, default 0/1), "max_block" (boundary
- * subdomain size, 16..384, next update), "max_coarse" (coarsest level size, next
- * update), "programmatic_launch" (0/1, default 1: V-cycle kernels overlap their
- * launch with the previous kernel's tail; process-wide). */
+ * per smoothing, default 2/2), "coarse_pre_sweeps", "coarse_post_sweeps" (the
+ * same on levels >= "coarse_from", default -1 = as the finer levels; coarse_from
+ * default 2), "pre_boundary", "post_boundary" (exact boundary solve before the
+ * pre / post sweeps, default 0/1), "max_block" (boundary subdomain size, 16..384,
+ * next update), "max_coarse" (coarsest level size, next update),
+ * "programmatic_launch" (0/1, default 1: V-cycle kernels overlap their launch
+ * with the previous kernel's tail; process-wide), "cluster_texels" (levels up to
+ * this many texels run in one thread-block cluster; default 0 = off),
+ * "trace_levels" (0/1: time every level's legs, arrays "profile.levels" and
+ * "profile.cluster"). */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
-/* Autotuner: times complete solves of b (host float64 numTexels*k) to tol for a
- * set of smoother settings (sweeps and boundary-solve placement), keeps the
- * fastest that converges.  knobs_out (optional, 5 doubles): pre sweeps, post
+int gdtp_system_get(const gdtp_system* s, const char* knob, double* value);
+/* Autotuner: times complete solves of b (host float64 numTexels*k, uploaded
+ * once; device time only) to tol for a grid of smoother settings (sweeps on the
+ * finer and on the coarser levels), keeps the fastest that converges (read the
+ * choice back with gdtp_system_get).  knobs_out (optional, 5 doubles): pre sweeps, post
  * sweeps, pre boundary, post boundary, best solve seconds. */
 int gdtp_system_autotune(gdtp_system* s, const double* b, int k, double tol, double* knobs_out);
 /* Device bytes held by the system (coefficients, vectors, coarse factor). */

@@ -159,3 +159,23 @@ def test_solve_is_deterministic(setup):
     x2, r2 = s.solve(b, tol=1e-6, max_iters=MAX_ITERS)
     assert r1["iterations"] == r2["iterations"]
     np.testing.assert_array_equal(x1, x2)
+
+
+def test_cluster_coarse_levels_match_launch_path(setup):
+    """The coarse levels run in one thread-block cluster give the same bits as
+    one launch per phase (same per-item arithmetic and summation order)."""
+    g, _, s = setup
+    b = g["solve/rhs"]
+    x0 = np.zeros_like(b, dtype=np.float32)
+    s.set("cluster_texels", 0)
+    try:
+        ref = s.vcycle(x0, b.astype(np.float32))
+        xr, rr = s.solve(b, tol=1e-6, max_iters=MAX_ITERS)
+    finally:
+        s.set("cluster_texels", 1 << 30)
+    got = s.vcycle(x0, b.astype(np.float32))
+    xg, rg = s.solve(b, tol=1e-6, max_iters=MAX_ITERS)
+    s.set("cluster_texels", 131072)
+    np.testing.assert_array_equal(got, ref)
+    assert rg["iterations"] == rr["iterations"]
+    np.testing.assert_array_equal(xg, xr)
