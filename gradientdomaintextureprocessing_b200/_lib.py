@@ -59,6 +59,13 @@ _SIGS = {
     "gdtp_system_autotune": (C.c_int, [_P, _P, C.c_int, C.c_double, _P]),
     "gdtp_residual_static": (C.c_int, [_P, _P, _P, _P, C.c_int, _P, _P]),
     "gdtp_system_device_bytes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "gdtp_geodesics_create": (C.c_int, [_P, C.POINTER(_P)]),
+    "gdtp_geodesics_free": (None, [_P]),
+    "gdtp_geodesics_counts": (C.c_int, [_P, _P]),
+    "gdtp_geodesics_array": (C.c_int, [_P, C.c_char_p, _P, C.POINTER(C.c_int64)]),
+    "gdtp_geodesic_rhs": (C.c_int, [_P, _P, _P, C.c_int]),
+    "gdtp_geodesic_rhs_device": (C.c_int, [_P, _P, _P, C.c_int, _P]),
+    "gdtp_geodesic_distance": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_double, C.c_int, _P, C.POINTER(Report)]),
 }
 
 

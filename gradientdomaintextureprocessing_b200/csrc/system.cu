@@ -117,6 +117,7 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
     err_ = "degenerate mesh (zero area)";
     return false;
   }
+  metric_ = g;
   AssemblyWork w;
   build_assembly_work(h_, be_, g, w);
   DeviceArena A;

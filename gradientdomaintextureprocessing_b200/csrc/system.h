@@ -117,6 +117,11 @@ class DeviceSystem {
   // assembly (FP64 on device) -> fine M and S
   bool assemble(const Mesh& mesh, const double* parameterMetric);
   const FineSystem& fine() const { return fine_; }
+  // what the assembly was built from (for the geodesic integration samples)
+  const Hierarchy& hierarchy() const { return h_; }
+  const BoundaryElements& boundary_elements() const { return be_; }
+  const ChartMetrics& metric() const { return metric_; }
+  cudaStream_t stream() const { return stream_; }
 
   // A = screen*M + stiffness*S, Galerkin hierarchy, boundary solvers, coarse inverse
   bool update(double stiffness, double screen);
@@ -175,6 +180,7 @@ class DeviceSystem {
   std::string err_;
   cudaStream_t stream_ = nullptr;
   FineSystem fine_;
+  ChartMetrics metric_;
   std::vector<LevelCoefficients> coeffs_;
   int levelsUsed_ = 0;
   double stiffness_ = 0, screen_ = 0;

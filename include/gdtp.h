@@ -182,6 +182,40 @@ int gdtp_system_get(const gdtp_system* s, const char* knob, double* value);
  * choice back with gdtp_system_get).  knobs_out (optional, 5 doubles): pre sweeps, post
  * sweeps, pre boundary, post boundary, best solve seconds. */
 int gdtp_system_autotune(gdtp_system* s, const double* b, int k, double tol, double* knobs_out);
+/* ---------------------------------------------------------------------------
+ * Heat-method geodesics (device).  gdtp_geodesics_create builds, for the
+ * system's mesh, atlas and metric, the integration samples of the Geodesics
+ * app: replaces InitializeGridAtladInteriorCellLines and
+ * InitializeNormalizedVectorFieldIntegration (include/Src/VectorFieldIntergration.inl:68-73,
+ * 428-437; samples per interior cell / boundary element and chart triangle,
+ * computed in FP64, stored in FP32).
+ * gdtp_geodesic_rhs: rhs = integral of X . grad(phi_i), X = -grad u / |grad u|
+ * in the metric, boundary terms through the fine boundary nodes (prolong u,
+ * integrate, restrict): replaces IntergrateNormalizedVectorFieldFromSamples
+ * (VectorFieldIntergration.inl:453-582) with the boundary prolongation and
+ * restriction around it (Geodesics/Geodesics.cpp:519-532).  Host float64
+ * numTexels*k in and out (or device buffers, stream-ordered, for _device).
+ * gdtp_geodesic_distance: the whole pipeline for k source texels (k right-hand
+ * sides): (M + t S) u = delta on `smooth`, rhs, (eps M + S) d = rhs on
+ * `distance` (both systems updated by the caller; the app uses eps = 1e-6,
+ * Geodesics.cpp:642), d shifted to 0 at each source (Geodesics.cpp:536-547).
+ * report: iterations and V-cycles of both solves summed, worst residual.
+ * ------------------------------------------------------------------------- */
+typedef struct gdtp_geodesics gdtp_geodesics;
+int gdtp_geodesics_create(gdtp_system* s, gdtp_geodesics** out);
+void gdtp_geodesics_free(gdtp_geodesics* g);
+/* counts[2] = {interior-cell samples, boundary-element samples} */
+int gdtp_geodesics_counts(const gdtp_geodesics* g, int64_t* counts);
+/* Host copies of the samples (as float64; with out == NULL only *count):
+ * "cellSamples" 16 per (interior cell, chart triangle) slot: pos(2), tensor(4),
+ * v_0..v_3(8), 0, 0; "hexSamples" 20 per (boundary element, chart triangle)
+ * slot: pos(2), tensor(4), v_0..v_5(12), 0, 0; "cellPtr", "corners", "slotBt", "btIdx". */
+int gdtp_geodesics_array(gdtp_geodesics* g, const char* name, double* out, int64_t* count);
+int gdtp_geodesic_rhs(gdtp_geodesics* g, const double* potential, double* rhs, int k);
+int gdtp_geodesic_rhs_device(gdtp_geodesics* g, const double* potential_dev, double* rhs_dev, int k, void* stream);
+int gdtp_geodesic_distance(gdtp_geodesics* g, gdtp_system* smooth, gdtp_system* distance, const int32_t* sources, int k, double tol,
+                           int max_iters, double* distance_out, gdtp_report* report);
+
 /* Device bytes held by the system (coefficients, vectors, coarse factor). */
 int gdtp_system_device_bytes(const gdtp_system* s, int64_t* bytes);
 

@@ -14,8 +14,13 @@
 //   MultiplyBySystemMatrix_NoReciprocals include/Src/IterativeSolvers.inl:881
 //   VCycle                         include/Src/IterativeSolvers.inl:1211
 //   solve(EigenCholeskySolver3)    include/Src/Solver.h:191   (the --useDirectSolver FP64 ground truth)
+// Mode "geodesic" follows the Geodesics app instead (Geodesics/Geodesics.cpp:257-300, 552-760):
+//   (M + stiffness S) u = delta_source, InitializeGridAtladInteriorCellLines /
+//   InitializeNormalizedVectorFieldIntegration (VectorFieldIntergration.inl:68-73, 428-437),
+//   boundary prolongation, IntergrateNormalizedVectorFieldFromSamples (:453-582), boundary
+//   restriction, (1e-6 M + S) d = rhs with exact solves, d shifted to 0 at the source.
 //
-// Usage: gdtp_ref <mesh.gdm> <out.gdd> [levels] [stiffness] [sharpness] [vcycles] [mode] [tol] [field.vf]
+// Usage: gdtp_ref <mesh.gdm> <out.gdd> [levels] [stiffness] [sharpness] [vcycles] [mode] [tol] [field.vf] [source]
 //   mode "dump": everything (small meshes); "solve": counts + rhs + exact solution + V-cycle timing.
 //   The RHS is  M f + stiffness*sharpness * S f  and the operator  M + stiffness*S.
 //   With field.vf (the reference's vector file: int32 count + per-triangle Point2D<double> in the
@@ -36,6 +41,8 @@ unsigned char* PNGReadColor(const char*, int&, int&) { return nullptr; }
 #include <Src/Hierarchy.h>
 #include <Src/MassAndStiffness.h>
 #include <Src/VectorIO.h>
+#include <Src/VectorFieldIntergration.inl>
+#include <algorithm>
 
 #include <chrono>
 #include <cstdint>
@@ -292,6 +299,75 @@ int main(int argc, char** argv) {
       for (size_t i = 0; i < f0.size(); i++)
         for (int c = 0; c < 3; c++) firstIterate.push_back((double)vars[0].x[i][c]);
   }
+
+  // ---------------- heat-method geodesics (mode "geodesic", FP64 build) -------------------
+#if !USE_FLOAT
+  if (mode == "geodesic") {
+    const int n = (int)textureNodes.size();
+    const int src = argc > 10 ? atoi(argv[10]) : n / 3;
+    EigenCholeskySolver1<double> smoothSolver, distSolver;
+    smoothSolver.init(A);
+    smoothSolver.update(A);
+    std::vector<double> delta(n, 0.0), u(n, 0.0), d(n, 0.0);
+    delta[src] = 1.0;
+    solve(smoothSolver, u, delta);
+    std::vector<InteriorCellLine> lines;
+    std::vector<std::pair<int, int>> lineIndex;
+    InitializeGridAtladInteriorCellLines(atlasCharts, fine.gridCharts, lines, lineIndex);
+    std::vector<std::vector<CellLineSampleInfo<double>>> cellSamples(lines.size());
+    std::vector<HexagonalSampleInfo<double>> hexSamples;
+    if (!InitializeNormalizedVectorFieldIntegration<double>(parameterMetric, atlasCharts, fine.gridCharts, lineIndex,
+                                                            boundaryProlongation.fineBoundaryIndex, cellSamples, hexSamples)) {
+      fprintf(stderr, "InitializeNormalizedVectorFieldIntegration failed\n");
+      return 3;
+    }
+    for (auto& v : cellSamples) std::sort(v.begin(), v.end(), CellLineSampleCompare<double>);
+    const std::vector<int>& bgi = fine.boundaryGlobalIndex;
+    const int nf = boundaryProlongation.numFineBoundarNodes;
+    std::vector<double> cbv(bgi.size()), cbr(bgi.size()), fbv(nf), fbr(nf), grhs(n, 0.0);
+    for (size_t i = 0; i < bgi.size(); i++) cbv[i] = u[bgi[i]];
+    boundaryProlongation.coarseBoundaryFineBoundaryProlongation.Multiply(&cbv[0], &fbv[0]);
+    omp_set_num_threads(1);  // its line-parallel scatter races at range boundaries
+    IntergrateNormalizedVectorFieldFromSamples<double>(double(width), double(height), lines, cellSamples, hexSamples, u, grhs, fbv, fbr);
+    std::vector<double> interiorRhs = grhs;
+    boundaryProlongation.fineBoundaryCoarseBoundaryRestriction.Multiply(&fbr[0], &cbr[0]);
+    for (size_t i = 0; i < bgi.size(); i++) grhs[bgi[i]] += cbr[i];
+    SparseMatrix<double, int> G = mass * 1e-6 + stiffness;
+    distSolver.init(G);
+    distSolver.update(G);
+    solve(distSolver, d, grhs);
+    const double d0 = d[src];
+    for (auto& v : d) v -= d0;
+    size_t nCellSamples = 0;
+    for (auto& v : cellSamples) nCellSamples += v.size();
+    // samples: hex {pos(2), tensor(4: (0,0) (0,1) (1,0) (1,1)), v(12), fine nodes(6)}; cell {line, cellOffset, pos, tensor, v(8)}
+    std::vector<double> hx, cl;
+    for (const auto& h : hexSamples) {
+      hx.insert(hx.end(), {h.pos[0], h.pos[1], h.tensor(0, 0), h.tensor(0, 1), h.tensor(1, 0), h.tensor(1, 1)});
+      for (int k = 0; k < 6; k++) { hx.push_back(h.v[k][0]); hx.push_back(h.v[k][1]); }
+      for (int k = 0; k < 6; k++) hx.push_back(h.fineNodes[k]);
+    }
+    for (size_t r = 0; r < cellSamples.size(); r++)
+      for (const auto& c : cellSamples[r]) {
+        cl.insert(cl.end(), {double(r), double(c.cellOffset), c.pos[0], c.pos[1], c.tensor(0, 0), c.tensor(0, 1), c.tensor(1, 0), c.tensor(1, 1)});
+        for (int k = 0; k < 4; k++) { cl.push_back(c.v[k][0]); cl.push_back(c.v[k][1]); }
+      }
+    out.f64("geo/hex_samples", hx, 24);
+    out.csr("geo/prolongation", boundaryProlongation.coarseBoundaryFineBoundaryProlongation);
+    out.f64("geo/cell_samples", cl, 16);
+    std::vector<int> li;
+    for (const auto& l : lines) li.insert(li.end(), {l.prevLineIndex, l.nextLineIndex, l.length});
+    out.i32("geo/cell_lines", li, 3);
+    out.i32("geo/source", {src, (int)lines.size(), (int)nCellSamples, (int)hexSamples.size(), nf});
+    out.f64("geo/weights", {stiffnessWeight, 1e-6});
+    out.f64("geo/u", u);
+    out.f64("geo/fine_boundary_u", fbv);
+    out.f64("geo/rhs_interior", interiorRhs);
+    out.f64("geo/fine_boundary_rhs", fbr);
+    out.f64("geo/rhs", grhs);
+    out.f64("geo/dist", d);
+  }
+#endif
 
   // ---------------- output --------------------------------------------------------------
   out.i32("meta/size", {width, height, levels, (int)atlasCharts.size(), omp_get_max_threads()});

@@ -35,6 +35,27 @@ CASES = {
 }
 # tangent fields (reference .vf files) of the anisotropic cases
 FIELDS = {"genus2lic512": lambda mesh: meshgen.gaussian_bump_field(mesh, bumps=8, seed=0)}
+# heat-method geodesics (the Geodesics app's pipeline): mesh, levels, smoothing weight t, source texel
+GEODESIC = {"geo256": (lambda: meshgen.icosphere_atlas(256, 256, subdiv=5), 4, 1e-3, 12345)}
+
+
+def make_geodesic(name: str) -> None:
+    factory, levels, t, src = GEODESIC[name]
+    mesh = factory()
+    exe = os.path.join(ROOT, "oracle", "_ref", "gdtp_ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        gdm, out = os.path.join(tmp, "m.gdm"), os.path.join(tmp, "o.gdd")
+        meshgen.write_gdm(gdm, mesh)
+        subprocess.run([exe, gdm, out, str(levels), str(t), "0", "1", "geodesic", "1e-6", "", str(src)], check=True,
+                       capture_output=True)
+        d = read_dump(out)
+    keep = {"mesh/vertices": mesh["vertices"], "mesh/triangles": mesh["triangles"], "mesh/uv": mesh["uv"],
+            "mesh/texture": mesh["texture"][..., :1], "meta/size": d["meta/size"], "L0/counts": d["L0/counts"]}
+    for k in d:
+        if k.startswith("geo/"):
+            keep[k] = d[k]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k.replace("/", "__"): v for k, v in keep.items()})
+    print(name, sum(v.nbytes for v in keep.values()) / 1e6, "MB raw")
 INDEX_KEYS = ["counts", "nodeinfo", "boundaryGlobalIndex", "deepGlobalIndex", "boundaryAndDeepIndex", "rasterLines",
               "restrictionLines", "deepLines", "prolongationLines", "charts_i", "charts_d"]
 
@@ -84,5 +105,8 @@ def make(name: str) -> None:
 
 
 if __name__ == "__main__":
-    for name in (sys.argv[1:] or CASES):
-        make(name)
+    for name in (sys.argv[1:] or list(CASES) + list(GEODESIC)):
+        if name in GEODESIC:
+            make_geodesic(name)
+        else:
+            make(name)

@@ -1,0 +1,94 @@
+"""Heat-method geodesics against the compiled reference (tests/golden/geo256:
+icosphere 256^2, t = 1e-3, one source; the reference integrates in FP64 with
+exact solves).  Tolerances:
+
+* integrated right-hand side from the reference's own smoothed impulse: 5e-6 of
+  its largest entry (interior samples and integration in FP32 as in the app's
+  build, boundary elements in FP64; measured 4.9e-7);
+* distances from our mixed-precision pipeline (both solves to 1e-6): 1e-3 of
+  the largest distance;
+* k sources batched as right-hand sides give the single-source results.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_mesh, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def geo(built_lib):
+    from gradientdomaintextureprocessing_b200.geodesics import Geodesics
+    from gradientdomaintextureprocessing_b200.hierarchy import InitializeHierarchy
+    g = load_golden("geo256")
+    h = InitializeHierarchy(golden_mesh(g), levels=int(g["meta/size"][2]))
+    return g, Geodesics(h, smoothing=float(g["geo/weights"][0]), epsilon=float(g["geo/weights"][1]))
+
+
+def test_sample_counts_cover_reference(geo):
+    g, G = geo
+    c = G.counts()
+    # slots are (cell, triangle) / (element, triangle) pairs; the reference keeps the non-empty ones
+    assert c["cell_samples"] >= int(g["geo/source"][2])
+    assert c["boundary_samples"] >= int(g["geo/source"][3])
+
+
+def test_rhs_matches_reference(geo):
+    g, G = geo
+    rhs = G.rhs(g["geo/u"])
+    ref = g["geo/rhs"]
+    err = np.abs(rhs - ref).max() / np.abs(ref).max()
+    assert err < 5e-6, err
+
+
+def test_rhs_is_batched(geo):
+    g, G = geo
+    u = g["geo/u"]
+    U = np.stack([u, 2.0 * u, u[::-1].copy()], 1)
+    R = G.rhs(U)
+    for c in range(3):
+        np.testing.assert_array_equal(R[:, c], G.rhs(U[:, c]))
+    # the normalised field does not depend on the potential's scale
+    np.testing.assert_allclose(R[:, 1], R[:, 0], rtol=0, atol=1e-6 * np.abs(R[:, 0]).max())
+
+
+def test_distance_matches_reference(geo):
+    g, G = geo
+    src = int(g["geo/source"][0])
+    d, rep = G.distance([src])
+    ref = g["geo/dist"]
+    assert rep["rel_residual_max"] <= 1e-6
+    assert d[src, 0] == 0.0
+    err = np.abs(d[:, 0] - ref).max() / np.abs(ref).max()
+    assert err < 1e-3, err
+
+
+def test_multi_source_batch_matches_single(geo):
+    g, G = geo
+    n = G.n
+    srcs = [int(g["geo/source"][0]), n // 7, (5 * n) // 9]
+    D, _ = G.distance(srcs)
+    for c, s in enumerate(srcs):
+        d, _ = G.distance([s])
+        assert np.abs(D[:, c] - d[:, 0]).max() <= 1e-4 * np.abs(d).max()
+
+
+def test_geodesics_64_sources_1024(built_lib):
+    """The heat-method workload at 1024^2: icosphere(6) atlas, t = mean texel
+    area, 64 seeded sources as 64 right-hand sides of one batched pipeline."""
+    from gradientdomaintextureprocessing_b200 import meshgen
+    from gradientdomaintextureprocessing_b200.geodesics import Geodesics
+    from gradientdomaintextureprocessing_b200.hierarchy import InitializeHierarchy
+    mesh = meshgen.icosphere_atlas(1024, 1024, subdiv=6, seed=0)
+    h = InitializeHierarchy(mesh, levels=4)
+    G = Geodesics(h)
+    rng = np.random.default_rng(0)
+    srcs = rng.choice(G.n, size=64, replace=False)
+    D, rep = G.distance(srcs, tol=1e-6)
+    assert rep["rel_residual_max"] <= 1e-6
+    assert np.all(D[srcs, np.arange(64)] == 0.0)
+    assert D.min() > -1e-2 * D.max()
+    for c in (0, 37):
+        d, _ = G.distance([srcs[c]], tol=1e-6)
+        assert np.abs(D[:, c] - d[:, 0]).max() <= 1e-4 * np.abs(d).max()
