@@ -20,16 +20,25 @@ from .hierarchy import Hierarchy
 from .system import System
 
 
+# the Geodesics app's --stiffness default (Geodesics/Geodesics.cpp:19)
+DEFAULT_SMOOTHING = 1e-3
+
+
 def mean_texel_area(hierarchy: Hierarchy) -> float:
-    """Mean texel area of the finest level in the area-normalised metric (total area 1)."""
+    """Mean texel area of the finest level in the area-normalised metric (total area 1).
+
+    As a smoothing time it makes the impulse response decay like exp(-d / h):
+    beyond a few tens of texels it falls below what any solve to a relative
+    residual of 1e-6 resolves, and the normalised field there is noise.  The
+    app's default (``DEFAULT_SMOOTHING``) keeps the response resolved."""
     return 1.0 / hierarchy.counts(0)["numTexels"]
 
 
 class Geodesics:
-    def __init__(self, hierarchy: Hierarchy, smoothing: float | None = None, epsilon: float = 1e-6, device: int = 0,
+    def __init__(self, hierarchy: Hierarchy, smoothing: float = DEFAULT_SMOOTHING, epsilon: float = 1e-6, device: int = 0,
                  parameter_metric: np.ndarray | None = None):
         self.hierarchy = hierarchy
-        self.t = mean_texel_area(hierarchy) if smoothing is None else float(smoothing)
+        self.t = float(smoothing)
         self.smooth = System(hierarchy, device=device, parameter_metric=parameter_metric)
         self.smooth.update(self.t, 1.0)
         self.dist = System(hierarchy, device=device, parameter_metric=parameter_metric)

@@ -36,7 +36,9 @@ CASES = {
 # tangent fields (reference .vf files) of the anisotropic cases
 FIELDS = {"genus2lic512": lambda mesh: meshgen.gaussian_bump_field(mesh, bumps=8, seed=0)}
 # heat-method geodesics (the Geodesics app's pipeline): mesh, levels, smoothing weight t, source texel
-GEODESIC = {"geo256": (lambda: meshgen.icosphere_atlas(256, 256, subdiv=5), 4, 1e-3, 12345)}
+GEODESIC = {"geo256": (lambda: meshgen.icosphere_atlas(256, 256, subdiv=5), 4, 1e-3, 12345),
+            # the heat-method configuration at full size: only the source and the distances are kept (FP32)
+            "geo1024": (lambda: meshgen.icosphere_atlas(1024, 1024, subdiv=6, seed=0), 4, 1e-3, 100000)}
 
 
 def make_geodesic(name: str) -> None:
@@ -49,6 +51,12 @@ def make_geodesic(name: str) -> None:
         subprocess.run([exe, gdm, out, str(levels), str(t), "0", "1", "geodesic", "1e-6", "", str(src)], check=True,
                        capture_output=True)
         d = read_dump(out)
+    if name == "geo1024":  # the mesh is regenerated from its seed by the test
+        keep = {"meta/size": d["meta/size"], "L0/counts": d["L0/counts"], "geo/source": d["geo/source"],
+                "geo/weights": d["geo/weights"], "geo/dist": d["geo/dist"].astype(np.float32)}
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k.replace("/", "__"): v for k, v in keep.items()})
+        print(name, sum(v.nbytes for v in keep.values()) / 1e6, "MB raw")
+        return
     keep = {"mesh/vertices": mesh["vertices"], "mesh/triangles": mesh["triangles"], "mesh/uv": mesh["uv"],
             "mesh/texture": mesh["texture"][..., :1], "meta/size": d["meta/size"], "L0/counts": d["L0/counts"]}
     for k in d:

@@ -5,8 +5,8 @@ exact solves).  Tolerances:
 * integrated right-hand side from the reference's own smoothed impulse: 5e-6 of
   its largest entry (interior samples and integration in FP32 as in the app's
   build, boundary elements in FP64; measured 4.9e-7);
-* distances from our mixed-precision pipeline (both solves to 1e-6): 1e-3 of
-  the largest distance;
+* distances from our mixed-precision pipeline (both solves to 1e-6): 2e-4 of
+  the largest distance (measured 3e-5);
 * k sources batched as right-hand sides give the single-source results.
 """
 import numpy as np
@@ -61,7 +61,7 @@ def test_distance_matches_reference(geo):
     assert rep["rel_residual_max"] <= 1e-6
     assert d[src, 0] == 0.0
     err = np.abs(d[:, 0] - ref).max() / np.abs(ref).max()
-    assert err < 1e-3, err
+    assert err < 2e-4, err
 
 
 def test_multi_source_batch_matches_single(geo):
@@ -74,21 +74,45 @@ def test_multi_source_batch_matches_single(geo):
         assert np.abs(D[:, c] - d[:, 0]).max() <= 1e-4 * np.abs(d).max()
 
 
-def test_geodesics_64_sources_1024(built_lib):
-    """The heat-method workload at 1024^2: icosphere(6) atlas, t = mean texel
-    area, 64 seeded sources as 64 right-hand sides of one batched pipeline."""
+@pytest.fixture(scope="module")
+def geo1024(built_lib):
     from gradientdomaintextureprocessing_b200 import meshgen
     from gradientdomaintextureprocessing_b200.geodesics import Geodesics
     from gradientdomaintextureprocessing_b200.hierarchy import InitializeHierarchy
-    mesh = meshgen.icosphere_atlas(1024, 1024, subdiv=6, seed=0)
-    h = InitializeHierarchy(mesh, levels=4)
-    G = Geodesics(h)
+    g = load_golden("geo1024")
+    h = InitializeHierarchy(meshgen.icosphere_atlas(1024, 1024, subdiv=6, seed=0), levels=4)
+    assert list(h.counts(0).values())[:7] == list(g["L0/counts"])
+    return g, h, Geodesics(h, smoothing=float(g["geo/weights"][0]), epsilon=float(g["geo/weights"][1]))
+
+
+def test_distance_matches_reference_1024(geo1024):
+    """Full-size heat-method configuration (icosphere(6), 1024^2, 356,581 texels)
+    against the reference's exact FP64 pipeline."""
+    g, _, G = geo1024
+    src = int(g["geo/source"][0])
+    d, rep = G.distance([src])
+    ref = g["geo/dist"].astype(np.float64)
+    assert rep["rel_residual_max"] <= 1e-6 and d[src, 0] == 0.0
+    err = np.abs(d[:, 0] - ref).max() / ref.max()
+    assert err < 2e-4, err
+
+
+def test_geodesics_64_sources_1024(geo1024):
+    """64 seeded deep-texel sources as 64 right-hand sides of one batched
+    pipeline: every column converges, is 0 at its source, is not below -sqrt(t)
+    (the smoothed distance's minimum sits within the smoothing length of the
+    source, so values down to that scale are the method's, not the solver's)
+    and is bounded by half the great circle of the unit-area sphere
+    (pi r, r = 1 / sqrt(4 pi)); batched columns equal single-source runs."""
+    g, h, G = geo1024
+    deep = h.array("deepGlobal")
     rng = np.random.default_rng(0)
-    srcs = rng.choice(G.n, size=64, replace=False)
+    srcs = rng.choice(deep, size=64, replace=False)
     D, rep = G.distance(srcs, tol=1e-6)
     assert rep["rel_residual_max"] <= 1e-6
     assert np.all(D[srcs, np.arange(64)] == 0.0)
-    assert D.min() > -1e-2 * D.max()
+    assert D.min() > -np.sqrt(G.t)
+    assert D.max() < 1.1 * np.pi / np.sqrt(4 * np.pi)
     for c in (0, 37):
         d, _ = G.distance([srcs[c]], tol=1e-6)
         assert np.abs(D[:, c] - d[:, 0]).max() <= 1e-4 * np.abs(d).max()
