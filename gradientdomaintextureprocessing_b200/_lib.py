@@ -59,6 +59,17 @@ _SIGS = {
     "gdtp_system_autotune": (C.c_int, [_P, _P, C.c_int, C.c_double, _P]),
     "gdtp_residual_static": (C.c_int, [_P, _P, _P, _P, C.c_int, _P, _P]),
     "gdtp_system_device_bytes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "gdtp_server_create": (C.c_int, [C.c_int, C.c_int64, C.c_int, C.POINTER(_P)]),
+    "gdtp_server_free": (None, [_P]),
+    "gdtp_server_add_model": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                        C.c_double, _P, C.POINTER(C.c_int)]),
+    "gdtp_server_model_texels": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int64)]),
+    "gdtp_server_model_bytes": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int64)]),
+    "gdtp_server_warm": (C.c_int, [_P, C.c_int]),
+    "gdtp_server_submit": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int64)]),
+    "gdtp_server_poll": (C.c_int, [_P, C.c_int64, C.POINTER(C.c_int)]),
+    "gdtp_server_wait": (C.c_int, [_P, C.c_int64, _P, C.POINTER(Report), _P]),
+    "gdtp_server_stats": (C.c_int, [_P, _P]),
     "gdtp_geodesics_create": (C.c_int, [_P, C.POINTER(_P)]),
     "gdtp_geodesics_free": (None, [_P]),
     "gdtp_geodesics_counts": (C.c_int, [_P, _P]),

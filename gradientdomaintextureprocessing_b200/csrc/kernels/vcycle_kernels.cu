@@ -349,16 +349,18 @@ __global__ void k_pack_rhs(const double* __restrict__ r, T* __restrict__ rhs, lo
   rhs[t] = c < K ? T(r[i * K + c]) : T(0);
 }
 // x64 += e (padded FP32/FP64 correction); e is cleared for the next V-cycle
-// (its padding lanes stay zero through the V-cycle)
+// (its padding lanes stay zero through the V-cycle).  Columns with frozen[c]
+// set keep their x: a right-hand side that has converged stops changing, so
+// its result does not depend on what it was solved together with.
 template <typename T>
-__global__ void k_add_correction(double* __restrict__ x, T* __restrict__ e, long long n, int K, int KP) {
+__global__ void k_add_correction(double* __restrict__ x, T* __restrict__ e, long long n, int K, int KP, const int* __restrict__ frozen) {
   grid_dependency_wait();
   grid_launch_dependents();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * K) return;
   const long long i = t / K;
   const int c = int(t - i * K);
-  x[t] += double(e[i * KP + c]);
+  if (!frozen || !frozen[c]) x[t] += double(e[i * KP + c]);
   e[i * KP + c] = T(0);
 }
 
@@ -466,8 +468,8 @@ void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaSt
   launch(k_pack_rhs<T>, dim3(nblk(n * KP)), s, r, rhs, n, K, KP);
 }
 template <typename T>
-void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s) {
-  launch(k_add_correction<T>, dim3(nblk(n * K)), s, x, e, n, K, KP);
+void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s, const int* frozen) {
+  launch(k_add_correction<T>, dim3(nblk(n * K)), s, x, e, n, K, KP, frozen);
 }
 
 #define GDTP_INSTANTIATE(T, W)                                                                                             \
@@ -485,8 +487,8 @@ GDTP_INSTANTIATE(double, 1)
 GDTP_INSTANTIATE(double, 4)
 template void launch_pack_rhs<float>(const double*, float*, long long, int, int, cudaStream_t);
 template void launch_pack_rhs<double>(const double*, double*, long long, int, int, cudaStream_t);
-template void launch_add_correction<float>(double*, float*, long long, int, int, cudaStream_t);
-template void launch_add_correction<double>(double*, double*, long long, int, int, cudaStream_t);
+template void launch_add_correction<float>(double*, float*, long long, int, int, cudaStream_t, const int*);
+template void launch_add_correction<double>(double*, double*, long long, int, int, cudaStream_t, const int*);
 
 }  // namespace dev
 }  // namespace gdtp

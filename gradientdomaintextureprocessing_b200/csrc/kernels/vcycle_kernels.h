@@ -92,9 +92,9 @@ void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coe
                              float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s);
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s);
-// x += e, then e = 0
+// x += e (columns c with frozen[c] != 0 unchanged; frozen may be null), then e = 0
 template <typename T>
-void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s);
+void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s, const int* frozen = nullptr);
 // Coarse levels l0 .. L-1 in one thread-block cluster (coarse_cycle.cu).
 // leg 0: down leg of levels l0..L-2 (pre-smoothing, residual, restriction);
 // leg 1: up leg (prolongation, boundary solve, post-smoothing); leg 2: both with

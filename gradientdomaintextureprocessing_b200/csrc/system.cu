@@ -525,6 +525,8 @@ bool DeviceSystem::ensure_work(int k) {
   r64_ = workArena_.zeros<double>(n * k);
   const int blocks = dev::raw_operator_blocks(rawM_.nRuns, h_.levels[0].numBoundary, k);
   partials_ = workArena_.zeros<double>(size_t(blocks) * 2 * k);
+  frozen_ = workArena_.zeros<int>(size_t(k));
+  frozenHost_.assign(k, 0);
   sums_ = workArena_.zeros<double>(2 * size_t(k));
   if (sumsHost_) cudaFreeHost(sumsHost_);
   if (!check(cudaMallocHost(&sumsHost_, 2 * size_t(k) * sizeof(double)), "cudaMallocHost")) return false;
@@ -654,7 +656,7 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     // and by the correction update of every step
     LevelDev<float>& D0 = mg.levels[0];
     if (mg.KP == 1) vcycle<float, 1>(mg, s); else vcycle<float, 4>(mg, s);
-    dev::launch_add_correction<float>(X, D0.x, (long long)n, k, mg.KP, s);
+    dev::launch_add_correction<float>(X, D0.x, (long long)n, k, mg.KP, s, frozen_);
     // r = b - A x, written straight into the FP32 right-hand side of the next V-cycle
     dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
                                  rawA_.bGlobal, rawA_.nB, B, X, D0.b, k, mg.KP, partials_, sums_, s);
@@ -697,6 +699,17 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
   };
   double rm = rel_max();
   int it = 0;
+  // right-hand sides at tolerance are frozen (their x no longer changes)
+  auto update_frozen = [&]() {
+    bool changed = false;
+    for (int c = 0; c < k; c++) {
+      const int f = rep.rel[c] <= tol ? 1 : 0;
+      if (f != frozenHost_[c]) { frozenHost_[c] = f; changed = true; }
+    }
+    return !changed || check(cudaMemcpyAsync(frozen_, frozenHost_.data(), k * sizeof(int), cudaMemcpyHostToDevice, s), "frozen flags");
+  };
+  for (int c = 0; c < k; c++) frozenHost_[c] = 2;  // not a flag value: forces the first upload
+  if (!update_frozen()) return false;
   while (rm > tol && it < maxIters) {
     if (!check(cudaGraphLaunch(iterGraph_, s), "graph launch") ||
         !check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
@@ -704,6 +717,7 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
       return false;
     it++;
     rm = rel_max();
+    if (rm > tol && !update_frozen()) return false;
     if (knobs.traceLevels && traceEv_.size() == size_t(2 * mg.levels.size())) {
       const int L = (int)mg.levels.size();
       std::vector<float> t(2 * L, 0.f);

@@ -89,15 +89,18 @@ struct RawOperator {
   int nB = 0;
 };
 
+// Defaults are the autotuner's choice on the 2048^2 icosphere filtering workload
+// (3 + 3 deep sweeps on level 0, none before and 3 after the coarse correction on
+// the coarser levels).
 struct SolverKnobs {
-  int preSweeps = 2, postSweeps = 2;
+  int preSweeps = 3, postSweeps = 3;
   int preBoundary = 0, postBoundary = 1;  // exact boundary solve before the pre / post sweeps
   int maxBlock = 384;                   // boundary subdomain size
   int maxCoarse = 2600;                 // coarsest level size limit (texels)
   int traceLevels = 0;                  // time every level's down / up leg (events in the graph)
   int clusterTexels = 0;                // levels up to this size run in one thread-block cluster (0: off)
-  int coarsePreSweeps = -1, coarsePostSweeps = -1;  // sweeps on levels >= coarseFrom (-1: as level 0)
-  int coarseFrom = 2;
+  int coarsePreSweeps = 0, coarsePostSweeps = 3;  // sweeps on levels >= coarseFrom (-1: as level 0)
+  int coarseFrom = 1;
 };
 
 struct SolveReport {
@@ -195,6 +198,8 @@ class DeviceSystem {
   std::unique_ptr<Multigrid<double>> mg64_;
 
   // solve work (tight n x k FP64)
+  int* frozen_ = nullptr;              // per right-hand side: converged, x kept (device)
+  std::vector<int> frozenHost_;
   DeviceArena workArena_;
   int workK_ = 0;
   double *b64_ = nullptr, *x64_ = nullptr, *r64_ = nullptr, *partials_ = nullptr, *sums_ = nullptr;

@@ -164,9 +164,9 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
                          void* stream);
 
 /* Solver knobs (value as double): "pre_sweeps", "post_sweeps" (deep colour sweeps
- * per smoothing, default 2/2), "coarse_pre_sweeps", "coarse_post_sweeps" (the
- * same on levels >= "coarse_from", default -1 = as the finer levels; coarse_from
- * default 2), "pre_boundary", "post_boundary" (exact boundary solve before the
+ * per smoothing, default 3/3), "coarse_pre_sweeps", "coarse_post_sweeps" (the
+ * same on levels >= "coarse_from", -1 = as the finer levels; defaults 0/3 from
+ * level 1), "pre_boundary", "post_boundary" (exact boundary solve before the
  * pre / post sweeps, default 0/1), "max_block" (boundary subdomain size, 16..384,
  * next update), "max_coarse" (coarsest level size, next update),
  * "programmatic_launch" (0/1, default 1: V-cycle kernels overlap their launch
@@ -215,6 +215,47 @@ int gdtp_geodesic_rhs(gdtp_geodesics* g, const double* potential, double* rhs, i
 int gdtp_geodesic_rhs_device(gdtp_geodesics* g, const double* potential_dev, double* rhs_dev, int k, void* stream);
 int gdtp_geodesic_distance(gdtp_geodesics* g, gdtp_system* smooth, gdtp_system* distance, const int32_t* sources, int k, double tol,
                            int max_iters, double* distance_out, gdtp_report* report);
+
+/* ---------------------------------------------------------------------------
+ * Solve server (device).  Holds many meshes / resolutions, admits them to the
+ * device under an HBM budget (idle models evicted least recently used first;
+ * GDTP_ERR_BUDGET when a model cannot fit) and runs requests with `slots`
+ * worker threads: queued requests of one model (same tol and max_iters, up to 64
+ * right-hand sides) are solved as one batch on that model's stream while other
+ * models' batches run on theirs.  Converged right-hand sides are frozen inside a
+ * batch, so each result is the one the request gets alone.  Kinds:
+ *   GDTP_KIND_FILTER   M + weight S, request signal f (n x k) -> solve of
+ *                      M f + weight * second * S f   (TextureFiltering.cpp:693-700)
+ *   GDTP_KIND_GEODESIC smoothing weight t = weight, eps = second; request = k source
+ *                      texels -> distances (n x k)   (Geodesics.cpp)
+ *   GDTP_KIND_LIC      parameter_metric (nt*4) required, M + weight S, request
+ *                      signal f (n x 1..k) -> solve of M f  (LineIntegralConvolution.cpp:698-706)
+ * The hierarchy is built by gdtp_server_add_model (host); gdtp_server_warm makes
+ * a model resident now.  gdtp_server_wait blocks, copies the result (n x k) and
+ * forgets the request; timing (optional, 3): {latency ms, queued ms, batch size}.
+ * stats[14]: completed, failed, p50 ms, p99 ms, mean ms, texel x RHS per second,
+ * batches, requests in batches, evictions, builds, resident bytes, peak bytes,
+ * budget, 0.  Not a counterpart of a reference interface: the reference apps
+ * solve one mesh at a time.
+ * ------------------------------------------------------------------------- */
+#define GDTP_KIND_FILTER 0
+#define GDTP_KIND_GEODESIC 1
+#define GDTP_KIND_LIC 2
+typedef struct gdtp_server gdtp_server;
+int gdtp_server_create(int device, int64_t hbm_budget_bytes, int slots, gdtp_server** out);
+void gdtp_server_free(gdtp_server* s);
+int gdtp_server_add_model(gdtp_server* s, const double* vertices, int64_t nv, const int32_t* triangles, int64_t nt, const double* uv,
+                          int width, int height, int levels, int kind, double weight, double second, const double* parameter_metric,
+                          int* model_out);
+int gdtp_server_model_texels(gdtp_server* s, int model, int64_t* texels);
+/* measured device bytes of a resident model, else the admission estimate */
+int gdtp_server_model_bytes(gdtp_server* s, int model, int64_t* bytes);
+int gdtp_server_warm(gdtp_server* s, int model);
+int gdtp_server_submit(gdtp_server* s, int model, const double* signal, const int32_t* sources, int k, double tol, int max_iters,
+                       int64_t* request_out);
+int gdtp_server_poll(gdtp_server* s, int64_t request, int* done);
+int gdtp_server_wait(gdtp_server* s, int64_t request, double* out, gdtp_report* report, double* timing);
+int gdtp_server_stats(gdtp_server* s, double* stats);
 
 /* Device bytes held by the system (coefficients, vectors, coarse factor). */
 int gdtp_system_device_bytes(const gdtp_system* s, int64_t* bytes);
