@@ -162,6 +162,60 @@ def run_reference(args, rank: int) -> dict:
             "e2e": {"value": value, "unit": "Mtexels/s (texels x RHS)", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def serve(args):
+    """Serving stream: requests on torus / icosphere / genus-2 models at sizes
+    log-uniform in [256, max size] (sqrt(2) ladder, multiples of 8), kinds 60 %
+    filtering (k = 3), 30 % geodesic (k = 1), 10 % line-integral convolution
+    (k = 1, anisotropy 1e3), Poisson arrivals, HBM admission budget.  Models are
+    added and made resident before the stream (setup time reported apart)."""
+    import torch
+    torch.cuda.set_device(0)
+    from gradientdomaintextureprocessing_b200 import build as _build
+    _build.build()
+    from gradientdomaintextureprocessing_b200 import serving
+    stream = serving.request_stream(args.serve_requests, rate_per_s=1.0, max_size=args.serve_max_size, seed=0)
+    server = serving.Server(budget_bytes=int(args.serve_budget_gb * (1 << 30)), slots=4)
+    t0 = time.time()
+    models = serving.build_models(server, stream)
+    setup_s = time.time() - t0
+    # rate: saturate the device -> arrivals faster than the measured service rate
+    rate = args.serve_rate
+    if rate <= 0:
+        # one request at a time: mean service time, then arrivals 1.5x faster than that
+        probe = [(0.0,) + tuple(p[1:]) for p in stream[:16]]
+        t = []
+        for p in probe:
+            res, _, wall = serving.run_stream(server, [p], models)
+            if res[0][1]["ok"]:
+                t.append(wall)
+        rate = 1.5 / float(np.mean(t))
+    arrivals = serving.request_stream(args.serve_requests, rate_per_s=rate, max_size=args.serve_max_size, seed=0)
+    server2 = server  # models stay resident
+    before = server2.stats()
+    results, st, wall = serving.run_stream(server2, arrivals, models)
+    failed = [r for _, r in results if not r["ok"]]
+    kind_of = {v: k for k, v in serving.KIND_NAMES.items()}
+    results = [(x, r) for x, r in results if r["ok"]]
+    lat = np.array([r["latency_ms"] for _, r in results])
+    texel_rhs = sum(server2.texels[models[(r["mesh"], r["size"], kind_of[r["kind"]])][0]] * (3 if r["kind"] == "filtering" else 1)
+                    for _, r in results)
+    kinds = {serving.KIND_NAMES[k]: sum(1 for *_, kk in arrivals if kk == k) for k in serving.KIND_NAMES}
+    out = {"metric": "serving: latency p50/p99 and aggregate Mtexels solved/s at 1e-6 rel. residual", "impl": "ours",
+           "value": texel_rhs / wall / 1e6, "unit": "Mtexels/s (texels x RHS, whole stream)",
+           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+           "requests": len(arrivals), "failed": len(failed),
+           "failures": [{k: r[k] for k in ("mesh", "size", "kind", "error")} for r in failed[:5]],
+           "arrival_rate_per_s": rate, "wall_s": wall,
+           "max_rel_residual": float(max(r["rel_residual_max"] for _, r in results)),
+           "batches": st["batches"] - before["batches"], "requests_in_batches": st["batched_requests"] - before["batched_requests"],
+           "evictions": st["evictions"], "resident_gb": st["resident_bytes"] / 2**30, "peak_gb": st["peak_bytes"] / 2**30,
+           "budget_gb": args.serve_budget_gb, "models": len(models), "setup_s": round(setup_s, 1), "kinds": kinds,
+           "config": {"workload": f"torus / icosphere6 / genus-2, 256^2-{args.serve_max_size}^2 log-uniform, "
+                                  "60 % filtering k=3, 30 % geodesic k=1, 10 % LIC k=1, Poisson arrivals", "slots": 4},
+           "data": "synthetic"}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -172,7 +226,16 @@ def main():
     ap.add_argument("--profile-solves", type=int, default=0,
                     help="profiling run: build the workload, run this many solves and exit (for ncu launch lists)")
     ap.add_argument("--width", type=int, default=WIDTH, help="texture resolution (profiling of smaller cases)")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving workload instead: Poisson request stream over resident models (one JSON line)")
+    ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--serve-max-size", type=int, default=1024,
+                    help="largest texture size of the stream (4096 is the full range; host set-up then takes several minutes)")
+    ap.add_argument("--serve-rate", type=float, default=0.0, help="arrivals per second (0: calibrated to saturate)")
+    ap.add_argument("--serve-budget-gb", type=float, default=80.0)
     args = ap.parse_args()
+    if args.serve:
+        return serve(args)
 
     rank, world, local, dist = dist_setup(args.gpus)
     if args.impl == "reference":

@@ -138,7 +138,7 @@ def build_models(server: Server, stream, lic_ratio: float = 1e3, warm: bool = Tr
     return models
 
 
-def run_stream(server: Server, stream, models: dict, tol: float = 1e-6, seed: int = 1):
+def run_stream(server: Server, stream, models: dict, tol: float = 1e-6, seed: int = 1, max_iters: int = 500):
     """Submits every request at its arrival time (wall clock), waits for all;
     returns per-request results and the server's statistics."""
     rng = np.random.default_rng(seed)
@@ -158,8 +158,17 @@ def run_stream(server: Server, stream, models: dict, tol: float = 1e-6, seed: in
         if delay > 0:
             time.sleep(delay)
         mid = models[(name, size, kind)][0]
-        rid = server.submit(mid, sources=data, tol=tol) if what == "sources" else server.submit(mid, signal=data, tol=tol)
+        rid = (server.submit(mid, sources=data, tol=tol, max_iters=max_iters) if what == "sources"
+               else server.submit(mid, signal=data, tol=tol, max_iters=max_iters))
         ids.append((rid, mid, k))
-    results = [server.wait(rid, server.texels[mid], k) for rid, mid, k in ids]
+    results = []
+    for (rid, mid, k), (_, name, size, kind) in zip(ids, stream):
+        try:
+            x, rep = server.wait(rid, server.texels[mid], k)
+            rep["ok"] = True
+        except _lib.GDTPError as e:  # reported, not fatal: a request that misses its tolerance
+            x, rep = None, {"ok": False, "error": str(e), "latency_ms": float("nan"), "rel_residual_max": float("nan")}
+        rep.update({"mesh": name, "size": size, "kind": KIND_NAMES[kind]})
+        results.append((x, rep))
     wall = time.perf_counter() - t0
     return results, server.stats(), wall
