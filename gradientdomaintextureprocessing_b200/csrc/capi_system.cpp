@@ -86,9 +86,10 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
     if (name.rfind("coef.bb.", 0) == 0) return emit_csr(co[level].bb, part("coef.bb."), out, count);
     if (name.rfind("coef.bd.", 0) == 0) return emit_csr(co[level].bd, part("coef.bd."), out, count);
   }
-  if (name == "profile") {  // {timed groups, total ms, deep texels per group, kernels per refinement graph}
-    double v[4] = {s->sys->profCount, s->sys->profMs, s->sys->profTexels, double(s->sys->graphKernels)};
-    if (count) *count = 4;
+  if (name == "profile") {  // {timed groups, total ms, deep texels per group, kernels per step graph, kernels launched}
+    double v[5] = {s->sys->profCount, s->sys->profMs, s->sys->profTexels, double(s->sys->graphKernels),
+                   double(s->sys->kernelLaunches)};
+    if (count) *count = 5;
     if (out) std::memcpy(out, v, sizeof(v));
     return GDTP_OK;
   }
@@ -110,6 +111,7 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
     DeviceSystem* d = const_cast<DeviceSystem*>(s->sys.get());
     d->profCount = 0;
     d->profMs = 0;
+    d->kernelLaunches = 0;
     d->traceCount = 0;
     d->traceCoarseMs = 0;
     d->traceDownMs.clear();
@@ -209,6 +211,7 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
   else if (k == "coarse_pre_sweeps" && v >= -1 && v <= 16) kn.coarsePreSweeps = v;
   else if (k == "coarse_post_sweeps" && v >= -1 && v <= 16) kn.coarsePostSweeps = v;
   else if (k == "coarse_from" && v >= 1 && v <= 16) kn.coarseFrom = v;
+  else if (k == "krylov" && (v == 0 || v == 1)) kn.krylov = v;
   else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
   s->sys->invalidate_graph();
   return GDTP_OK;
@@ -230,6 +233,7 @@ extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* v
   else if (k == "coarse_pre_sweeps") *value = kn.coarsePreSweeps;
   else if (k == "coarse_post_sweeps") *value = kn.coarsePostSweeps;
   else if (k == "coarse_from") *value = kn.coarseFrom;
+  else if (k == "krylov") *value = kn.krylov;
   else return fail(GDTP_ERR_INVALID, "gdtp_system_get: unknown knob " + k);
   return GDTP_OK;
 }

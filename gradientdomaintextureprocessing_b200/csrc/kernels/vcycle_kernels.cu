@@ -225,8 +225,34 @@ __global__ void __launch_bounds__(256) k_coarse_solve(int n, const double* __res
   coarse_row<T, W, LoadDefault>(n, ainv, scale, rhs, x, KP, G, warp, lane);
 }
 
+// Per-block sums of two per-channel accumulators into partials[block][0..K) and
+// [K..2K): lanes l and l^s (s >= G) hold the same channel group, then the warps
+// are added in a fixed order (deterministic).  All threads of the block call it.
+__device__ __forceinline__ void block_partials(double (&ra)[4], double (&rb)[4], int G, int K, double* partials) {
+  __shared__ double red[8][2][64];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int ch = 0; ch < 4; ch++)
+    for (int s = 16; s >= G; s >>= 1) {
+      ra[ch] += __shfl_xor_sync(0xffffffffu, ra[ch], s);
+      rb[ch] += __shfl_xor_sync(0xffffffffu, rb[ch], s);
+    }
+  if (lane < G)
+#pragma unroll
+    for (int ch = 0; ch < 4; ch++)
+      if (4 * lane + ch < K) { red[warp][0][4 * lane + ch] = ra[ch]; red[warp][1][4 * lane + ch] = rb[ch]; }
+  __syncthreads();
+  if ((int)threadIdx.x < K) {
+    double a = 0, c = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a += red[w][0][threadIdx.x]; c += red[w][1][threadIdx.x]; }
+    partials[(long long)blockIdx.x * 2 * K + threadIdx.x] = a;
+    partials[(long long)blockIdx.x * 2 * K + K + threadIdx.x] = c;
+  }
+}
+
 // ----------------------------------------------------------------------------
-// FP64 raw operator: res = b - A x (mode 0) or y = A x (mode 1) on tight
+// FP64 raw operator: res = b - A x (mode 0), y = A x (mode 1) or y = A x with
+// the partial sums of x . y instead of y . y (mode 2) on tight
 // n x K vectors.  Deep rows use 9 raw coefficients per run texel, boundary rows
 // the merged BD/BB CSR.  A thread handles one texel and up to 4 channels
 // (group q of G = KP/4 groups, or G = 1 for K = 1).  Per-block sums of res^2
@@ -288,7 +314,7 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
         const double v = mode == 0 ? bv - acc[ch] : acc[ch];
         if (out32) out32[(long long)g * KP + c] = float(v);
         else out[(long long)g * K + c] = v;
-        rr[ch] += v * v;
+        rr[ch] += mode == 2 ? x[(long long)g * K + c] * v : v * v;  // mode 2: x . A x
         bb[ch] += bv * bv;
       }
       if (out32)  // zero the padding channels of this group
@@ -296,26 +322,7 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
     }
   }
   if (!partials) return;
-  // lanes l and l^s with s >= G share the group q: reduce across them
-  __shared__ double red[8][2][64];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-  for (int ch = 0; ch < 4; ch++)
-    for (int s = 16; s >= G; s >>= 1) {
-      rr[ch] += __shfl_xor_sync(0xffffffffu, rr[ch], s);
-      bb[ch] += __shfl_xor_sync(0xffffffffu, bb[ch], s);
-    }
-  if (lane < G)
-#pragma unroll
-    for (int ch = 0; ch < 4; ch++)
-      if (4 * lane + ch < K) { red[warp][0][4 * lane + ch] = rr[ch]; red[warp][1][4 * lane + ch] = bb[ch]; }
-  __syncthreads();
-  if ((int)threadIdx.x < K) {
-    double a = 0, c = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a += red[w][0][threadIdx.x]; c += red[w][1][threadIdx.x]; }
-    partials[(long long)blockIdx.x * 2 * K + threadIdx.x] = a;
-    partials[(long long)blockIdx.x * 2 * K + K + threadIdx.x] = c;
-  }
+  block_partials(rr, bb, G, K, partials);
 }
 
 // Sum of per-block partials in a fixed order (one block): sums[2K]
@@ -335,6 +342,97 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int nBlocks,
     if (threadIdx.x == 0) sums[c] = sh[0];
     __syncthreads();
   }
+}
+
+// ----------------------------------------------------------------------------
+// Flexible preconditioned conjugate gradients around the FP32 V-cycle (FP64
+// vectors, tight n x K; per right-hand side scalars in `sc`: alpha [0,K),
+// beta [K,2K), rho [2K,3K), previous rho [3K,4K)).  Items are texels x channel
+// groups of 4 over a fixed grid, so the partial sums have a fixed order.
+// ----------------------------------------------------------------------------
+// z = e (V-cycle output, FP32 padded), e cleared; partials: z . r and z . q
+__global__ void __launch_bounds__(256) k_fcg_precond(long long n, int K, int KP, int G, float* __restrict__ e,
+                                                     const double* __restrict__ r, const double* __restrict__ q,
+                                                     double* __restrict__ z, double* __restrict__ partials) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  const long long stride = (long long)gridDim.x * blockDim.x, t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int qg = int(t0 % G);
+  double a[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
+  for (long long t = t0; t < n * G; t += stride) {
+    const long long i = t / G;
+#pragma unroll
+    for (int ch = 0; ch < 4; ch++) {
+      const int c = 4 * qg + ch;
+      if (c >= K) continue;
+      const double v = double(e[i * KP + c]);
+      e[i * KP + c] = 0.f;
+      z[i * K + c] = v;
+      a[ch] += v * r[i * K + c];
+      b[ch] += v * q[i * K + c];
+    }
+  }
+  block_partials(a, b, G, K, partials);
+}
+
+// beta = -alpha_old (z . q_old) / rho_old (0 on a (re)start, rho_old = 0); rho = z . r
+__global__ void k_fcg_beta(int K, const double* __restrict__ sums, double* __restrict__ sc) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  const int c = threadIdx.x;
+  if (c >= K) return;
+  const double rho = sums[c], gamma = sums[K + c], rhoOld = sc[3 * K + c];
+  sc[K + c] = rhoOld != 0.0 ? -sc[c] * gamma / rhoOld : 0.0;
+  sc[2 * K + c] = rho;
+  sc[3 * K + c] = rho;
+}
+
+// p = z + beta p
+__global__ void __launch_bounds__(256) k_fcg_direction(long long n, int K, const double* __restrict__ z, const double* __restrict__ sc,
+                                                       double* __restrict__ p) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * K) return;
+  const int c = int(t % K);
+  p[t] = z[t] + sc[K + c] * p[t];
+}
+
+// alpha = rho / (p . A p), 0 for frozen right-hand sides
+__global__ void k_fcg_alpha(int K, const double* __restrict__ sums, const int* __restrict__ frozen, double* __restrict__ sc) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  const int c = threadIdx.x;
+  if (c >= K) return;
+  const double pq = sums[c];
+  sc[c] = (frozen && frozen[c]) || !(pq > 0) ? 0.0 : sc[2 * K + c] / pq;
+}
+
+// x += alpha p, r -= alpha q, r packed into the next V-cycle's FP32 right-hand
+// side; partials: r . r and 0
+__global__ void __launch_bounds__(256) k_fcg_update(long long n, int K, int KP, int G, const double* __restrict__ sc,
+                                                    const double* __restrict__ p, const double* __restrict__ q, double* __restrict__ x,
+                                                    double* __restrict__ r, float* __restrict__ rhs32, double* __restrict__ partials) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  const long long stride = (long long)gridDim.x * blockDim.x, t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int qg = int(t0 % G);
+  double a[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
+  for (long long t = t0; t < n * G; t += stride) {
+    const long long i = t / G;
+#pragma unroll
+    for (int ch = 0; ch < 4; ch++) {
+      const int c = 4 * qg + ch;
+      if (c >= K) continue;
+      const double al = sc[c];
+      x[i * K + c] += al * p[i * K + c];
+      const double rv = r[i * K + c] - al * q[i * K + c];
+      r[i * K + c] = rv;
+      rhs32[i * KP + c] = float(rv);
+      a[ch] += rv * rv;
+    }
+  }
+  block_partials(a, b, G, K, partials);
 }
 
 // FP64 residual (n*K, tight) -> FP32 right-hand side (n*KP, padded)
@@ -461,6 +559,39 @@ void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coe
   launch(k_raw_operator, dim3(blocks), s, runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, (double*)nullptr, K,
          G, 0, partials, rhs32, KP);
   if (partials && sums) launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
+}
+
+// ---- flexible CG steps (fixed grids: partial sums in a fixed order)
+static inline int fcg_blocks(long long n, int G) { return int(std::min<long long>(kRawBlocks, nblk(n * G))); }
+void launch_fcg_precond(long long n, int K, int KP, float* e, const double* r, const double* q, double* z, double* partials,
+                        double* sums, double* sc, cudaStream_t s) {
+  const int G = raw_groups(K), blocks = fcg_blocks(n, G);
+  launch(k_fcg_precond, dim3(blocks), s, n, K, KP, G, e, r, q, z, partials);
+  launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
+  launch(k_fcg_beta, dim3(1), s, K, (const double*)sums, sc);
+}
+void launch_fcg_direction(long long n, int K, const double* z, const double* sc, double* p, cudaStream_t s) {
+  launch(k_fcg_direction, dim3(nblk(n * K)), s, n, K, z, sc, p);
+}
+void launch_fcg_alpha(int K, const double* sums, const int* frozen, double* sc, cudaStream_t s) {
+  launch(k_fcg_alpha, dim3(1), s, K, sums, frozen, sc);
+}
+void launch_fcg_update(long long n, int K, int KP, const double* sc, const double* p, const double* q, double* x, double* r, float* rhs32,
+                       double* partials, double* sums, cudaStream_t s) {
+  const int G = raw_groups(K), blocks = fcg_blocks(n, G);
+  launch(k_fcg_update, dim3(blocks), s, n, K, KP, G, sc, p, q, x, r, rhs32, partials);
+  launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
+}
+void launch_raw_apply_dot(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr, const int* bCol,
+                          const double* bVal, const int* bGlobal, int nB, const double* x, double* out, int K, double* partials,
+                          double* sums, cudaStream_t s) {
+  const int G = raw_groups(K);
+  const long long items = (long long)nRuns * 32 * G + (long long)nB * G;
+  if (items == 0) return;
+  const int blocks = int(std::min<long long>(kRawBlocks, nblk(items)));
+  launch(k_raw_operator, dim3(blocks), s, runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, (const double*)nullptr, x,
+         out, K, G, 2, partials, (float*)nullptr, 0);
+  launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
 }
 
 template <typename T>

@@ -92,6 +92,22 @@ void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coe
                              float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s);
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s);
+// Flexible preconditioned CG around the FP32 V-cycle (vcycle_kernels.cu).  sc: 4K
+// per-RHS scalars {alpha, beta, rho, rho_old}; sums: 2K.
+//   precond:   z = e (e cleared), rho = z.r, beta = -alpha_old (z.q_old) / rho_old
+//   direction: p = z + beta p
+//   apply_dot: q = A p, sums[0..K) = p.q
+//   alpha:     alpha = rho / p.q (0 where frozen)
+//   update:    x += alpha p, r -= alpha q, rhs32 = r, sums[0..K) = r.r
+void launch_fcg_precond(long long n, int K, int KP, float* e, const double* r, const double* q, double* z, double* partials,
+                        double* sums, double* sc, cudaStream_t s);
+void launch_fcg_direction(long long n, int K, const double* z, const double* sc, double* p, cudaStream_t s);
+void launch_raw_apply_dot(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr, const int* bCol,
+                          const double* bVal, const int* bGlobal, int nB, const double* x, double* out, int K, double* partials,
+                          double* sums, cudaStream_t s);
+void launch_fcg_alpha(int K, const double* sums, const int* frozen, double* sc, cudaStream_t s);
+void launch_fcg_update(long long n, int K, int KP, const double* sc, const double* p, const double* q, double* x, double* r, float* rhs32,
+                       double* partials, double* sums, cudaStream_t s);
 // x += e (columns c with frozen[c] != 0 unchanged; frozen may be null), then e = 0
 template <typename T>
 void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s, const int* frozen = nullptr);

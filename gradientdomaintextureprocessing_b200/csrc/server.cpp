@@ -86,6 +86,8 @@ bool Server::build_device(Model& m, std::string& err) {
     if (!m.g->ok()) { err = m.g->error(); return false; }
   } else if (!make(m.a, m.w, 1.0)) {
     return false;
+  } else if (m.kind == kKindLic) {
+    m.a->knobs.krylov = 1;  // the anisotropic V-cycle contracts slowly: CG around it
   }
   return true;
 }

@@ -69,6 +69,7 @@ DeviceSystem::DeviceSystem(const Hierarchy& h, const BoundaryElements& be, int d
 DeviceSystem::~DeviceSystem() {
   cudaSetDevice(device_);
   if (iterGraph_) cudaGraphExecDestroy(iterGraph_);
+  if (krylovGraph_) cudaGraphExecDestroy(krylovGraph_);
   if (profEv_[0]) { cudaEventDestroy(profEv_[0]); cudaEventDestroy(profEv_[1]); }
   for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
   if (sumsHost_) cudaFreeHost(sumsHost_);
@@ -82,6 +83,9 @@ void DeviceSystem::invalidate_graph() {
   if (iterGraph_) cudaGraphExecDestroy(iterGraph_);
   iterGraph_ = nullptr;
   iterGraphK_ = -1;
+  if (krylovGraph_) cudaGraphExecDestroy(krylovGraph_);
+  krylovGraph_ = nullptr;
+  krylovGraphK_ = -1;
 }
 
 bool DeviceSystem::check(cudaError_t e, const char* what) {
@@ -248,7 +252,7 @@ bool DeviceSystem::update(double stiffness, double screen) {
   }
   mg32_.reset();
   mg64_.reset();
-  if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; iterGraphK_ = -1; }
+  invalidate_graph();
   updated_ = true;
   return true;
 }
@@ -532,7 +536,7 @@ bool DeviceSystem::ensure_work(int k) {
   if (!check(cudaMallocHost(&sumsHost_, 2 * size_t(k) * sizeof(double)), "cudaMallocHost")) return false;
   if (!check(workArena_.last, "work allocation")) return false;
   workK_ = k;
-  if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; iterGraphK_ = -1; }
+  invalidate_graph();
   return true;
 }
 
@@ -613,7 +617,7 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
   if (!mg32_ || mg32_->KP < KP) {
     mg32_.reset(new Multigrid<float>());
     if (!build_multigrid(*mg32_, KP)) return false;
-    if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; iterGraphK_ = -1; }
+    invalidate_graph();
   }
   if (!ensure_work(k)) return false;
   Multigrid<float>& mg = *mg32_;
@@ -632,115 +636,75 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
   if (b_host && !check(cudaMemcpyAsync(b64_, b_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d b")) return false;
   if (x_host && !zeroGuess && !check(cudaMemcpyAsync(x64_, x_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d x")) return false;
   if (zeroGuess && !check(cudaMemsetAsync(X, 0, n * k * 8, s), "zero x")) return false;
-  // refinement step graph: rhs <- r, e <- V(rhs), x += e, r <- b - A x (+ norms)
-  if (!iterGraph_ || iterGraphK_ != k || iterGraphB_ != B || iterGraphX_ != X) {
-    if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; }
-    cudaGraph_t g;
-    if (!profEv_[0]) {
-      cudaEventCreate(&profEv_[0]);
-      cudaEventCreate(&profEv_[1]);
-    }
-    if (knobs.traceLevels && !timeline_) {
-      timeline_ = static_cast<unsigned long long*>(rawArena_.alloc(1024 * sizeof(unsigned long long)));
-      if (!check(rawArena_.last, "timeline") || !check(cudaMemset(timeline_, 0, 1024 * sizeof(unsigned long long)), "timeline"))
-        return false;
-    }
-    profiling_ = true;
-    if (knobs.traceLevels && traceEv_.size() != size_t(2 * mg.levels.size())) {
-      for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
-      traceEv_.assign(2 * mg.levels.size(), nullptr);
-      for (cudaEvent_t& e : traceEv_) cudaEventCreate(&e);
-    }
-    if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
-    // D0.x (the correction) is zero on entry: cleared before the first step
-    // and by the correction update of every step
-    LevelDev<float>& D0 = mg.levels[0];
-    if (mg.KP == 1) vcycle<float, 1>(mg, s); else vcycle<float, 4>(mg, s);
-    dev::launch_add_correction<float>(X, D0.x, (long long)n, k, mg.KP, s, frozen_);
-    // r = b - A x, written straight into the FP32 right-hand side of the next V-cycle
-    dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
-                                 rawA_.bGlobal, rawA_.nB, B, X, D0.b, k, mg.KP, partials_, sums_, s);
-    profiling_ = false;
-    if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
-    {
-      size_t nn = 0;
-      cudaGraphGetNodes(g, nullptr, &nn);
-      std::vector<cudaGraphNode_t> nodes(nn);
-      cudaGraphGetNodes(g, nodes.data(), &nn);
-      graphKernels = 0;
-      for (auto nd : nodes) {
-        cudaGraphNodeType t;
-        cudaGraphNodeGetType(nd, &t);
-        if (t == cudaGraphNodeTypeKernel) graphKernels++;
-      }
-    }
-    if (!check(cudaGraphInstantiate(&iterGraph_, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
-    cudaGraphDestroy(g);
-    iterGraphK_ = k;
-    iterGraphB_ = B;
-    iterGraphX_ = X;
-  }
-  // zero correction, initial residual straight into the FP32 right-hand side
-  if (!check(cudaMemsetAsync(mg.levels[0].x, 0, n * mg.KP * sizeof(float), s), "zero correction")) return false;
-  dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
-                               rawA_.bGlobal, rawA_.nB, B, X, mg.levels[0].b, k, mg.KP, partials_, sums_, s);
-  if (!check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
-      !check(cudaStreamSynchronize(s), "initial residual"))
-    return false;
-  rep = SolveReport();
-  rep.rel.assign(k, 0.0);
-  auto rel_max = [&]() {
-    double m = 0;
-    for (int c = 0; c < k; c++) {
-      rep.rel[c] = std::sqrt(sumsHost_[c] / std::max(sumsHost_[k + c], 1e-300));
-      m = std::max(m, rep.rel[c]);
-    }
-    return m;
-  };
-  double rm = rel_max();
   int it = 0;
-  // right-hand sides at tolerance are frozen (their x no longer changes)
-  auto update_frozen = [&]() {
-    bool changed = false;
-    for (int c = 0; c < k; c++) {
-      const int f = rep.rel[c] <= tol ? 1 : 0;
-      if (f != frozenHost_[c]) { frozenHost_[c] = f; changed = true; }
+  double rm = 0;
+  if (knobs.krylov) {
+    if (!krylov_solve(mg, B, X, k, tol, maxIters, s, rep, it, rm)) return false;
+  } else {
+    // refinement step graph: rhs <- r, e <- V(rhs), x += e, r <- b - A x (+ norms)
+    if (!iterGraph_ || iterGraphK_ != k || iterGraphB_ != B || iterGraphX_ != X) {
+      if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; }
+      cudaGraph_t g;
+      if (!prepare_timing(mg)) return false;
+      profiling_ = true;
+      if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
+      // D0.x (the correction) is zero on entry: cleared before the first step
+      // and by the correction update of every step
+      LevelDev<float>& D0 = mg.levels[0];
+      if (mg.KP == 1) vcycle<float, 1>(mg, s); else vcycle<float, 4>(mg, s);
+      dev::launch_add_correction<float>(X, D0.x, (long long)n, k, mg.KP, s, frozen_);
+      // r = b - A x, written straight into the FP32 right-hand side of the next V-cycle
+      dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
+                                   rawA_.bGlobal, rawA_.nB, B, X, D0.b, k, mg.KP, partials_, sums_, s);
+      profiling_ = false;
+      if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
+      graphKernels = kernel_nodes(g);
+      if (!check(cudaGraphInstantiate(&iterGraph_, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
+      cudaGraphDestroy(g);
+      iterGraphK_ = k;
+      iterGraphB_ = B;
+      iterGraphX_ = X;
     }
-    return !changed || check(cudaMemcpyAsync(frozen_, frozenHost_.data(), k * sizeof(int), cudaMemcpyHostToDevice, s), "frozen flags");
-  };
-  for (int c = 0; c < k; c++) frozenHost_[c] = 2;  // not a flag value: forces the first upload
-  if (!update_frozen()) return false;
-  while (rm > tol && it < maxIters) {
-    if (!check(cudaGraphLaunch(iterGraph_, s), "graph launch") ||
-        !check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
-        !check(cudaStreamSynchronize(s), "refinement step"))
+    // zero correction, initial residual straight into the FP32 right-hand side
+    if (!check(cudaMemsetAsync(mg.levels[0].x, 0, n * mg.KP * sizeof(float), s), "zero correction")) return false;
+    kernelLaunches += 2;  // operator + norm reduction
+    dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
+                                 rawA_.bGlobal, rawA_.nB, B, X, mg.levels[0].b, k, mg.KP, partials_, sums_, s);
+    if (!check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
+        !check(cudaStreamSynchronize(s), "initial residual"))
       return false;
-    it++;
-    rm = rel_max();
-    if (rm > tol && !update_frozen()) return false;
-    if (knobs.traceLevels && traceEv_.size() == size_t(2 * mg.levels.size())) {
-      const int L = (int)mg.levels.size();
-      std::vector<float> t(2 * L, 0.f);
-      bool okT = true;
-      for (int i = 1; i < 2 * L; i++) okT = okT && cudaEventElapsedTime(&t[i], traceEv_[i - 1], traceEv_[i]) == cudaSuccess;
-      if (okT) {
-        traceDownMs.resize(L - 1, 0.0);
-        traceUpMs.resize(L - 1, 0.0);
-        for (int l = 0; l + 1 < L; l++) traceDownMs[l] += t[l + 1];
-        traceCoarseMs += t[L];
-        for (int l = L - 2; l >= 0; l--) traceUpMs[l] += t[L + 1 + (L - 2 - l)];
-        traceCount += 1;
-      } else {
-        cudaGetLastError();
+    rep = SolveReport();
+    rep.rel.assign(k, 0.0);
+    auto rel_max = [&]() {
+      double m = 0;
+      for (int c = 0; c < k; c++) {
+        rep.rel[c] = std::sqrt(sumsHost_[c] / std::max(sumsHost_[k + c], 1e-300));
+        m = std::max(m, rep.rel[c]);
       }
-    }
-    float pm = 0;
-    if (cudaEventElapsedTime(&pm, profEv_[0], profEv_[1]) == cudaSuccess) {
-      profCount += 1;
-      profMs += pm;
-      profTexels = mg.levels[0].nDeep;
-    } else {
-      cudaGetLastError();  // timing unavailable: do not leave the error for the next caller
+      return m;
+    };
+    rm = rel_max();
+    // right-hand sides at tolerance are frozen (their x no longer changes)
+    auto update_frozen = [&]() {
+      bool changed = false;
+      for (int c = 0; c < k; c++) {
+        const int f = rep.rel[c] <= tol ? 1 : 0;
+        if (f != frozenHost_[c]) { frozenHost_[c] = f; changed = true; }
+      }
+      return !changed || check(cudaMemcpyAsync(frozen_, frozenHost_.data(), k * sizeof(int), cudaMemcpyHostToDevice, s), "frozen flags");
+    };
+    for (int c = 0; c < k; c++) frozenHost_[c] = 2;  // not a flag value: forces the first upload
+    if (!update_frozen()) return false;
+    while (rm > tol && it < maxIters) {
+      kernelLaunches += graphKernels;
+      if (!check(cudaGraphLaunch(iterGraph_, s), "graph launch") ||
+          !check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
+          !check(cudaStreamSynchronize(s), "refinement step"))
+        return false;
+      it++;
+      rm = rel_max();
+      if (rm > tol && !update_frozen()) return false;
+      collect_timing(mg);
     }
   }
   if (x_host && !check(cudaMemcpyAsync(x_host, x64_, n * k * 8, cudaMemcpyDeviceToHost, s), "d2h x")) return false;
@@ -758,6 +722,170 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
   return true;
 }
 
+// events for the level-0 sweep timing (and the per-level trace), created
+// outside any capture
+bool DeviceSystem::prepare_timing(const Multigrid<float>& mg) {
+  if (!profEv_[0]) {
+    cudaEventCreate(&profEv_[0]);
+    cudaEventCreate(&profEv_[1]);
+  }
+  if (knobs.traceLevels && !timeline_) {
+    timeline_ = static_cast<unsigned long long*>(rawArena_.alloc(1024 * sizeof(unsigned long long)));
+    if (!check(rawArena_.last, "timeline") || !check(cudaMemset(timeline_, 0, 1024 * sizeof(unsigned long long)), "timeline"))
+      return false;
+  }
+  if (knobs.traceLevels && traceEv_.size() != size_t(2 * mg.levels.size())) {
+    for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
+    traceEv_.assign(2 * mg.levels.size(), nullptr);
+    for (cudaEvent_t& e : traceEv_) cudaEventCreate(&e);
+  }
+  return true;
+}
+
+int DeviceSystem::kernel_nodes(cudaGraph_t g) {
+  size_t nn = 0;
+  cudaGraphGetNodes(g, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn);
+  cudaGraphGetNodes(g, nodes.data(), &nn);
+  int c = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    cudaGraphNodeGetType(nd, &t);
+    if (t == cudaGraphNodeTypeKernel) c++;
+  }
+  return c;
+}
+
+// after a completed step: accumulate the events recorded inside its graph
+void DeviceSystem::collect_timing(const Multigrid<float>& mg) {
+  if (knobs.traceLevels && traceEv_.size() == size_t(2 * mg.levels.size())) {
+    const int L = (int)mg.levels.size();
+    std::vector<float> t(2 * L, 0.f);
+    bool okT = true;
+    for (int i = 1; i < 2 * L; i++) okT = okT && cudaEventElapsedTime(&t[i], traceEv_[i - 1], traceEv_[i]) == cudaSuccess;
+    if (okT) {
+      traceDownMs.resize(L - 1, 0.0);
+      traceUpMs.resize(L - 1, 0.0);
+      for (int l = 0; l + 1 < L; l++) traceDownMs[l] += t[l + 1];
+      traceCoarseMs += t[L];
+      for (int l = L - 2; l >= 0; l--) traceUpMs[l] += t[L + 1 + (L - 2 - l)];
+      traceCount += 1;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  float pm = 0;
+  if (cudaEventElapsedTime(&pm, profEv_[0], profEv_[1]) == cudaSuccess) {
+    profCount += 1;
+    profMs += pm;
+    profTexels = mg.levels[0].nDeep;
+  } else {
+    cudaGetLastError();  // timing unavailable: do not leave the error for the next caller
+  }
+}
+
+bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X, int k, double tol, int maxIters, cudaStream_t s,
+                                SolveReport& rep, int& it, double& rm) {
+  const size_t n = h_.levels[0].numTexels;
+  if (k > krylovK_) {
+    krylovArena_ = DeviceArena();
+    z_ = static_cast<double*>(krylovArena_.alloc(n * k * sizeof(double)));
+    p_ = static_cast<double*>(krylovArena_.alloc(n * k * sizeof(double)));
+    q_ = static_cast<double*>(krylovArena_.alloc(n * k * sizeof(double)));
+    sc_ = static_cast<double*>(krylovArena_.alloc(4 * size_t(k) * sizeof(double)));
+    if (!check(krylovArena_.last, "krylov vectors")) return false;
+    krylovK_ = k;
+    if (krylovGraph_) { cudaGraphExecDestroy(krylovGraph_); krylovGraph_ = nullptr; }
+  }
+  LevelDev<float>& D0 = mg.levels[0];
+  const int KP = mg.KP;
+  rep = SolveReport();
+  rep.rel.assign(k, 0.0);
+  std::vector<double> bb(k, 0.0);
+  auto rel_from = [&](bool setB) {
+    double m = 0;
+    for (int c = 0; c < k; c++) {
+      if (setB) bb[c] = sumsHost_[k + c];
+      rep.rel[c] = std::sqrt(sumsHost_[c] / std::max(bb[c], 1e-300));
+      m = std::max(m, rep.rel[c]);
+    }
+    return m;
+  };
+  auto fetch = [&](const char* what) {
+    return check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") &&
+           check(cudaStreamSynchronize(s), what);
+  };
+  // r = b - A x with the FP64 operator
+  auto true_residual = [&]() {
+    kernelLaunches += 2;  // operator + norm reduction
+    dev::launch_raw_operator(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal, rawA_.bGlobal,
+                             rawA_.nB, B, X, r64_, k, 0, partials_, sums_, s);
+    return fetch("residual");
+  };
+  // (re)start: p = q = 0, rho_old = 0, the V-cycle's right-hand side = r, e = 0
+  auto restart = [&]() {
+    if (!check(cudaMemsetAsync(p_, 0, n * k * sizeof(double), s), "krylov restart") ||
+        !check(cudaMemsetAsync(q_, 0, n * k * sizeof(double), s), "krylov restart") ||
+        !check(cudaMemsetAsync(sc_, 0, 4 * size_t(k) * sizeof(double), s), "krylov restart"))
+      return false;
+    kernelLaunches += 1;
+    dev::launch_pack_rhs<float>(r64_, D0.b, (long long)n, k, KP, s);
+    return check(cudaMemsetAsync(D0.x, 0, n * KP * sizeof(float), s), "krylov restart");
+  };
+  auto update_frozen = [&]() {
+    bool changed = false;
+    for (int c = 0; c < k; c++) {
+      const int f = rep.rel[c] <= tol ? 1 : 0;
+      if (f != frozenHost_[c]) { frozenHost_[c] = f; changed = true; }
+    }
+    return !changed || check(cudaMemcpyAsync(frozen_, frozenHost_.data(), k * sizeof(int), cudaMemcpyHostToDevice, s), "frozen flags");
+  };
+  if (!krylovGraph_ || krylovGraphX_ != X || krylovGraphK_ != k) {
+    if (krylovGraph_) { cudaGraphExecDestroy(krylovGraph_); krylovGraph_ = nullptr; }
+    cudaGraph_t g;
+    if (!prepare_timing(mg)) return false;
+    profiling_ = true;
+    if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
+    if (KP == 1) vcycle<float, 1>(mg, s); else vcycle<float, 4>(mg, s);
+    profiling_ = false;
+    dev::launch_fcg_precond((long long)n, k, KP, D0.x, r64_, q_, z_, partials_, sums_, sc_, s);
+    dev::launch_fcg_direction((long long)n, k, z_, sc_, p_, s);
+    dev::launch_raw_apply_dot(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal, rawA_.bGlobal,
+                              rawA_.nB, p_, q_, k, partials_, sums_, s);
+    dev::launch_fcg_alpha(k, sums_, frozen_, sc_, s);
+    dev::launch_fcg_update((long long)n, k, KP, sc_, p_, q_, X, r64_, D0.b, partials_, sums_, s);
+    if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
+    graphKernels = kernel_nodes(g);
+    if (!check(cudaGraphInstantiate(&krylovGraph_, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
+    cudaGraphDestroy(g);
+    krylovGraphX_ = X;
+    krylovGraphK_ = k;
+  }
+  if (!true_residual()) return false;
+  rm = rel_from(true);
+  for (int c = 0; c < k; c++) frozenHost_[c] = 2;  // not a flag value: forces the first upload
+  if (!update_frozen()) return false;
+  it = 0;
+  if (rm <= tol) return true;
+  if (!restart()) return false;
+  while (it < maxIters) {
+    kernelLaunches += graphKernels;
+    if (!check(cudaGraphLaunch(krylovGraph_, s), "graph launch") || !fetch("krylov step")) return false;
+    it++;
+    collect_timing(mg);
+    rm = rel_from(false);  // recursively updated residual
+    if (rm <= tol) {
+      if (!true_residual()) return false;  // confirm with b - A x
+      rm = rel_from(false);
+      if (rm <= tol) break;
+      if (!update_frozen() || !restart()) return false;  // drift: restart from the true residual
+      continue;
+    }
+    if (!update_frozen()) return false;
+  }
+  return true;
+}
+
 bool DeviceSystem::autotune(const double* b, int k, double tol, SolverKnobs& best, double& bestSeconds) {
   if (!err_.empty()) return false;
   cudaSetDevice(device_);
@@ -772,13 +900,16 @@ bool DeviceSystem::autotune(const double* b, int k, double tol, SolverKnobs& bes
   best = base;
   // candidates: deep sweeps before / after the coarse correction on the finer
   // levels, and on the levels from `coarseFrom` on (-1: same as the finer
-  // ones); the exact boundary solve follows the coarse correction
+  // ones); the exact boundary solve follows the coarse correction; the outer
+  // iteration is plain refinement or flexible CG
   const int fine[][2] = {{1, 1}, {2, 2}, {2, 3}, {3, 3}, {3, 4}, {4, 4}};
   const int coarse[][3] = {{-1, -1, 2}, {0, 1, 2}, {0, 2, 2}, {0, 3, 2}, {1, 1, 2}, {1, 2, 2},
                            {0, 2, 1}, {0, 3, 1}, {1, 2, 1}, {0, 2, 3}};
+  for (int kr = 0; kr < 2; kr++)
   for (const auto& f : fine)
     for (const auto& c : coarse) {
       knobs = base;
+      knobs.krylov = kr;
       knobs.preSweeps = f[0];
       knobs.postSweeps = f[1];
       knobs.preBoundary = 0;

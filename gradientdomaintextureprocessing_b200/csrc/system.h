@@ -101,6 +101,7 @@ struct SolverKnobs {
   int clusterTexels = 0;                // levels up to this size run in one thread-block cluster (0: off)
   int coarsePreSweeps = 0, coarsePostSweeps = 3;  // sweeps on levels >= coarseFrom (-1: as level 0)
   int coarseFrom = 1;
+  int krylov = 0;                       // 1: flexible CG around the V-cycle instead of plain refinement
 };
 
 struct SolveReport {
@@ -166,6 +167,7 @@ class DeviceSystem {
   bool is_updated() const { return updated_; }
   int num_texels() const { return h_.levels[0].numTexels; }
   int graphKernels = 0;         // kernel nodes in the refinement-step graph
+  int64_t kernelLaunches = 0;   // kernels launched by solve_mixed since the last profile reset
 
  private:
   template <typename T>
@@ -173,6 +175,11 @@ class DeviceSystem {
   template <typename T, int W>
   void vcycle(Multigrid<T>& mg, cudaStream_t s);
   bool ensure_work(int k);
+  bool prepare_timing(const Multigrid<float>& mg);
+  void collect_timing(const Multigrid<float>& mg);
+  static int kernel_nodes(cudaGraph_t g);
+  bool krylov_solve(Multigrid<float>& mg, const double* B, double* X, int k, double tol, int maxIters, cudaStream_t s,
+                    SolveReport& rep, int& it, double& rm);
   bool raw_apply_dev(const RawOperator& op, const double* b, const double* x, double* out, int k, int mode, cudaStream_t s,
                      double* sumsHost);
   bool check(cudaError_t e, const char* what);
@@ -199,6 +206,11 @@ class DeviceSystem {
 
   // solve work (tight n x k FP64)
   int* frozen_ = nullptr;              // per right-hand side: converged, x kept (device)
+  DeviceArena krylovArena_;            // flexible CG: z, p, q (n x k FP64), scalars
+  double *z_ = nullptr, *p_ = nullptr, *q_ = nullptr, *sc_ = nullptr;
+  int krylovK_ = 0, krylovGraphK_ = -1;
+  cudaGraphExec_t krylovGraph_ = nullptr;
+  const double* krylovGraphX_ = nullptr;
   std::vector<int> frozenHost_;
   DeviceArena workArena_;
   int workK_ = 0;

@@ -67,7 +67,7 @@ class System:
         out = np.zeros(5)
         _lib.check(_lib.lib().gdtp_system_autotune(self._s, _lib.ptr(b), k, float(tol), _lib.ptr(out)))
         knobs = {name: int(self.get(name)) for name in ("pre_sweeps", "post_sweeps", "pre_boundary", "post_boundary",
-                                                         "coarse_pre_sweeps", "coarse_post_sweeps", "coarse_from")}
+                                                         "coarse_pre_sweeps", "coarse_post_sweeps", "coarse_from", "krylov")}
         knobs["seconds"] = float(out[4])
         return knobs
 

@@ -105,7 +105,9 @@ void gdtp_system_free(gdtp_system* s);
 /* Named host copies of the assembled FP64 system (level 0 unless noted):
  *   "deepMass" "deepStiffness" (10 per deep texel)
  *   "bbMass.ptr/.col/.val" "bbStiffness.*" "bdMass.*" "bdStiffness.*"
- *   after gdtp_system_update: "coef.deep"(level l, raw, 10 per deep texel), "coef.bb.*", "coef.bd.*" */
+ *   after gdtp_system_update: "coef.deep"(level l, raw, 10 per deep texel), "coef.bb.*", "coef.bd.*"
+ *   "profile": {timed level-0 sweep groups, their total ms, deep texels per group,
+ *   kernels per step graph, kernels launched by solves}; "profile.reset" clears the counts */
 int gdtp_system_array(const gdtp_system* s, const char* name, int level, void* out, int64_t* count);
 
 /* Combine and coarsen: A = screen*M + stiffness*S, Galerkin hierarchy, coarse
@@ -173,7 +175,10 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * with the previous kernel's tail; process-wide), "cluster_texels" (levels up to
  * this many texels run in one thread-block cluster; default 0 = off),
  * "trace_levels" (0/1: time every level's legs, arrays "profile.levels" and
- * "profile.cluster"). */
+ * "profile.cluster"), "krylov" (0/1, default 0: flexible preconditioned
+ * conjugate gradients in FP64 around the FP32 V-cycle instead of plain
+ * iterative refinement; for slowly contracting V-cycles, e.g. strongly
+ * anisotropic metrics). */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
 int gdtp_system_get(const gdtp_system* s, const char* knob, double* value);
 /* Autotuner: times complete solves of b (host float64 numTexels*k, uploaded

@@ -179,3 +179,29 @@ def test_cluster_coarse_levels_match_launch_path(setup):
     np.testing.assert_array_equal(got, ref)
     assert rg["iterations"] == rr["iterations"]
     np.testing.assert_array_equal(xg, xr)
+
+
+@pytest.mark.parametrize("tol", [1e-6, 1e-8])
+def test_krylov_solve_matches_reference_solution(setup, tol):
+    """Flexible CG around the FP32 V-cycle: same residual bound and energy-norm
+    error as plain refinement, deterministic, and batch-independent (converged
+    columns are frozen)."""
+    import port
+    g, _, s = setup
+    b = g["solve/rhs"]
+    s.set("krylov", 1)
+    try:
+        x, rep = s.solve(b, tol=tol, max_iters=MAX_ITERS)
+        x2, rep2 = s.solve(b, tol=tol, max_iters=MAX_ITERS)
+        xc, _ = s.solve(b[:, 0], tol=tol, max_iters=MAX_ITERS)
+    finally:
+        s.set("krylov", 0)
+    _, plain = s.solve(b, tol=tol, max_iters=MAX_ITERS)
+    assert rep["converged"] and rep["rel_residual_max"] <= tol
+    assert s.residual(b, x).max() <= tol
+    assert port.energy_error(ref_full(g), x, g["solve/exact"]).max() < 1e-5
+    assert rep2["iterations"] == rep["iterations"]
+    np.testing.assert_array_equal(x, x2)
+    assert np.abs(xc[:, 0] - x[:, 0]).max() < 1e-5 * np.abs(x).max()
+    # CG never needs more V-cycles than refinement (+1 for the residual check)
+    assert rep["iterations"] <= plain["iterations"] + 1
