@@ -51,7 +51,10 @@ class Geodesics:
     def __del__(self):
         g, self._g = getattr(self, "_g", None), None
         if g:
-            _lib.lib().gdtp_geodesics_free(g)
+            try:
+                _lib.lib().gdtp_geodesics_free(g)
+            except (TypeError, AttributeError):  # interpreter exit: module globals already cleared
+                pass
 
     def counts(self) -> dict:
         c = np.zeros(2, dtype=np.int64)

@@ -29,7 +29,10 @@ class Hierarchy:
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None
         if h:
-            _lib.lib().gdtp_hierarchy_free(h)
+            try:
+                _lib.lib().gdtp_hierarchy_free(h)
+            except (TypeError, AttributeError):  # interpreter exit: module globals already cleared
+                pass
 
     @property
     def handle(self):

@@ -35,7 +35,10 @@ class Server:
     def __del__(self):
         s, self._s = getattr(self, "_s", None), None
         if s:
-            _lib.lib().gdtp_server_free(s)
+            try:
+                _lib.lib().gdtp_server_free(s)
+            except (TypeError, AttributeError):  # interpreter exit: module globals already cleared
+                pass
 
     def add_model(self, mesh: dict, kind: int, weight: float, second: float = 0.0, levels: int = 4,
                   parameter_metric: np.ndarray | None = None) -> int:

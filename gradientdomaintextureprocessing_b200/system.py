@@ -43,7 +43,10 @@ class System:
     def __del__(self):
         s, self._s = getattr(self, "_s", None), None
         if s:
-            _lib.lib().gdtp_system_free(s)
+            try:
+                _lib.lib().gdtp_system_free(s)
+            except (TypeError, AttributeError):  # interpreter exit: module globals already cleared
+                pass
 
     @property
     def handle(self):
