@@ -3,7 +3,7 @@
 #include <memory>
 #include <vector>
 
-#include "../../include/gdtp.h"
+#include "gdtp.h"
 #include "capi_internal.h"
 #include "geodesics.h"
 

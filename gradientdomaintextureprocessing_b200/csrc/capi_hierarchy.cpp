@@ -3,7 +3,7 @@
 #include <memory>
 #include <string>
 
-#include "../../include/gdtp.h"
+#include "gdtp.h"
 #include "capi_internal.h"
 
 namespace gdtp {

@@ -1,7 +1,7 @@
 // C ABI: per-triangle parameter metrics for gdtp_system_create (host only).
 #include <vector>
 
-#include "../../include/gdtp.h"
+#include "gdtp.h"
 #include "capi_internal.h"
 
 using namespace gdtp;

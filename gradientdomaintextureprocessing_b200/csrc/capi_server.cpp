@@ -2,7 +2,7 @@
 #include <cstring>
 #include <memory>
 
-#include "../../include/gdtp.h"
+#include "gdtp.h"
 #include "capi_internal.h"
 #include "server.h"
 

@@ -3,7 +3,7 @@
 #include <memory>
 #include <string>
 
-#include "../../include/gdtp.h"
+#include "gdtp.h"
 #include "capi_internal.h"
 #include "system.h"
 
@@ -119,6 +119,7 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
     if (count) *count = 0;
     return GDTP_OK;
   }
+  if (name == "levelStats") return vec(s->sys->level_stats());  // 9 per level, see DeviceSystem::level_stats
   if (name == "levelsUsed") {
     if (count) *count = 1;
     if (out) *static_cast<int32_t*>(out) = s->sys->levelsUsed();
@@ -208,6 +209,8 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
   else if (k == "programmatic_launch" && (v == 0 || v == 1)) dev::set_programmatic_launch(v != 0);
   else if (k == "trace_levels" && (v == 0 || v == 1)) kn.traceLevels = v;
   else if (k == "cluster_texels" && v >= 0) kn.clusterTexels = v;
+  else if (k == "grid_texels" && v >= 0) kn.gridTexels = v;
+  else if (k == "chart_texels" && v >= 0) kn.chartTexels = v;
   else if (k == "coarse_pre_sweeps" && v >= -1 && v <= 16) kn.coarsePreSweeps = v;
   else if (k == "coarse_post_sweeps" && v >= -1 && v <= 16) kn.coarsePostSweeps = v;
   else if (k == "coarse_from" && v >= 1 && v <= 16) kn.coarseFrom = v;
@@ -234,6 +237,8 @@ extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* v
   else if (k == "coarse_post_sweeps") *value = kn.coarsePostSweeps;
   else if (k == "coarse_from") *value = kn.coarseFrom;
   else if (k == "krylov") *value = kn.krylov;
+  else if (k == "grid_texels") *value = kn.gridTexels;
+  else if (k == "chart_texels") *value = kn.chartTexels;
   else return fail(GDTP_ERR_INVALID, "gdtp_system_get: unknown knob " + k);
   return GDTP_OK;
 }

@@ -14,6 +14,14 @@
 // (row groups of 128, j chunks of the same length, 8 interleaved warps per
 // chunk, chunk sums in chunk order), so a V-cycle gives the same bits on
 // either path.
+//
+// The same kernel also runs persistently on the whole GPU (one cooperative
+// launch, every CTA resident) with a software grid barrier between phases:
+// one barrier (an atomic arrival and a poll of a generation word in L2) costs
+// far less than a dependent launch, and the phases get all SMs instead of one
+// cluster's.  The barrier's polls are bounded: a block that waits too long
+// records an error and every block abandons the remaining phases, so a lost
+// block cannot hang the GPU; the host reads the error word after the solve.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -116,13 +124,53 @@ __device__ void cluster_bs_dense(const BoundaryDev<T>& B, int mode, const T* rhs
 struct CoarseCycleArgs {
   int l0, L;            // levels l0 .. L-1 of the V-cycle, L-1 the coarsest
   int leg;              // 0: down leg (ends with the restriction into L-1), 1: up leg, 2: both + coarse solve
-  int preSweeps, postSweeps, preBoundary, postBoundary;
+  CoarseSweeps sw;
   int KP;
   int coarseN;
   const double* coarseInv;
   const double* coarseScale;
   unsigned long long* timeline;  // optional: {phase code, globaltimer ns} after every phase (CTA 0)
+  GridBarrierState* barrier;     // persistent whole-GPU variant only
 };
+
+// Polls of the barrier's generation word before a block gives up (about a
+// second at most); a phase of the coarse levels takes microseconds.
+constexpr long long kBarrierPolls = 1ll << 20;
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier: every block's writes before it are visible to every block
+// after it.  The last block to arrive resets the count and advances the
+// generation; the others poll the generation (bounded).  Returns false, in
+// every thread of the block, once any block has recorded a timeout.
+__device__ bool grid_barrier(GridBarrierState* gb, unsigned int& gen) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // release this block's writes
+    const unsigned int g = gen;
+    if (atomicAdd(&gb->count, 1u) == gridDim.x - 1) {
+      atomicExch(&gb->count, 0u);
+      __threadfence();
+      atomicExch(&gb->gen, g + 1);
+    } else {
+      long long polls = 0;
+      while (ld_acquire_gpu(&gb->gen) == g) {
+        if (++polls > kBarrierPolls) { atomicExch(&gb->error, 1u); break; }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();  // acquire the other blocks' writes
+    gen = g + 1;
+    ok = ld_acquire_gpu(&gb->error) == 0;
+  }
+  __syncthreads();
+  return ok != 0;
+}
 
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -130,21 +178,32 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-template <typename T, int W>
+// kGrid false: one thread-block cluster (cluster barriers); true: every SM,
+// cooperative launch, grid barriers.
+template <typename T, int W, bool kGrid>
 __global__ void __launch_bounds__(kClusterBlock, 1) k_coarse_cycle(const LevelDev<T>* __restrict__ lv, CoarseCycleArgs a) {
   grid_dependency_wait();
-  grid_launch_dependents();
+  // the persistent variant lets the next kernel launch only when it is done
+  // (early dependents would only take SM slots from nothing)
+  if constexpr (!kGrid) grid_launch_dependents();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* red = reinterpret_cast<T*>(smem_raw);
   Vec<T, W>* vin = reinterpret_cast<Vec<T, W>*>(red + 32 * 32 * 4 * W);
-  cg::cluster_group cluster = cg::this_cluster();
   const int KP = a.KP, G = KP / W;
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nth = (long long)gridDim.x * blockDim.x;
   int phase = a.leg == 1 ? 255 : 0;  // the up leg stamps the second half
-  // barrier between phases; with a timeline, CTA 0 stamps the phase's end
+  unsigned int gen = 0;
+  if (kGrid) gen = ld_acquire_gpu(&a.barrier->gen);  // nobody advances it before every block has arrived once
+  bool alive = true;
+  // barrier between phases; with a timeline, CTA 0 stamps the phase's end.
+  // After a barrier timeout (grid variant) the remaining phases are skipped.
   auto sync = [&](int code) {
-    cluster.sync();
+    if constexpr (kGrid) {
+      if (alive) alive = grid_barrier(a.barrier, gen);
+    } else {
+      cg::this_cluster().sync();
+    }
     if (a.timeline && blockIdx.x == 0 && threadIdx.x == 0 && phase < 510) {
       a.timeline[2 * phase] = (unsigned long long)code;
       a.timeline[2 * phase + 1] = global_ns();
@@ -154,7 +213,7 @@ __global__ void __launch_bounds__(kClusterBlock, 1) k_coarse_cycle(const LevelDe
   if (a.timeline && blockIdx.x == 0 && threadIdx.x == 0) a.timeline[a.leg == 1 ? 1020 : 1022] = global_ns();  // start
   auto boundary_solve = [&](const LevelDev<T>& D, int code) {
     const BoundaryDev<T>& B = D.B;
-    if (B.nb == 0) return;
+    if (B.nb == 0 || !alive) return;
     if (B.nSubTasks > 0) { cluster_bs_dense<T, W>(B, 0, D.b, D.x, KP, G, red, vin); sync(code + 1); }
     if (B.nS > 0) { cluster_bs_dense<T, W>(B, 1, D.b, D.x, KP, G, red, vin); sync(code + 2); }
     if (B.nI > 0) {
@@ -163,19 +222,19 @@ __global__ void __launch_bounds__(kClusterBlock, 1) k_coarse_cycle(const LevelDe
     }
   };
   auto colour_pass = [&](const LevelDev<T>& D, int c, int code) {
-    const int nr = D.runStart[c + 1] - D.runStart[c];
+    const int nr = alive ? D.runStart[c + 1] - D.runStart[c] : 0;
     for (long long t = tid; t < (long long)nr * 32 * G; t += nth)
       gs_item<T, W, LoadL2>(D.runs + D.runStart[c], nr, D.coef, D.planeStride, D.b, D.x, KP, G, t);
     sync(code + c);
   };
   if (a.leg != 1) {
-    for (int l = a.l0; l + 1 < a.L; l++) {
+    for (int l = a.l0; l + 1 < a.L && alive; l++) {
       const LevelDev<T>& D = lv[l];
       const LevelDev<T>& C = lv[l + 1];
-      if (a.preBoundary) boundary_solve(D, 1000 * l);
-      for (int sw = 0; sw < a.preSweeps; sw++)
+      if (a.sw.preBoundary) boundary_solve(D, 1000 * l);
+      for (int sw = 0; sw < a.sw.pre(l); sw++)
         for (int c = 0; c < 4; c++) colour_pass(D, c, 1000 * l + 10);
-      for (long long t = tid; t < (long long)D.nRuns * 32 * G; t += nth)
+      for (long long t = alive ? tid : (long long)D.nRuns * 32 * G; t < (long long)D.nRuns * 32 * G; t += nth)
         residual_deep_item<T, W, LoadL2>(D.runs, D.nRuns, D.coef, D.planeStride, D.b, D.x, D.r, KP, G, t);
       for (long long t = tid; t < (long long)D.nB * G; t += nth)
         residual_boundary_item<T, W, LoadL2>(D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, G, t);
@@ -188,7 +247,7 @@ __global__ void __launch_bounds__(kClusterBlock, 1) k_coarse_cycle(const LevelDe
       sync(1000 * l + 21);
     }
   }
-  if (a.leg == 2) {
+  if (a.leg == 2 && alive) {
     const LevelDev<T>& C = lv[a.L - 1];
     const int lane = threadIdx.x & 31;
     for (long long w = tid >> 5; w < a.coarseN; w += nth >> 5)
@@ -196,14 +255,14 @@ __global__ void __launch_bounds__(kClusterBlock, 1) k_coarse_cycle(const LevelDe
     sync(1000 * (a.L - 1) + 30);
   }
   if (a.leg != 0) {
-    for (int l = a.L - 2; l >= a.l0; l--) {
+    for (int l = a.L - 2; l >= a.l0 && alive; l--) {
       const LevelDev<T>& D = lv[l];
       const LevelDev<T>& C = lv[l + 1];
       for (long long t = tid; t < (long long)D.nPRuns * 32 * G; t += nth)
         prolong_item<T, W, LoadL2>(D.pruns, D.nPRuns, C.x, D.x, KP, G, t);
       sync(1000 * l + 40);
-      if (a.postBoundary) boundary_solve(D, 1000 * l + 40);
-      for (int sw = 0; sw < a.postSweeps; sw++)
+      if (a.sw.postBoundary) boundary_solve(D, 1000 * l + 40);
+      for (int sw = 0; sw < a.sw.post(l); sw++)
         for (int c = 3; c >= 0; c--) colour_pass(D, c, 1000 * l + 50);
     }
   }
@@ -213,7 +272,7 @@ template <typename T, int W>
 int coarse_cycle_cluster_size() {
   static int cached = -1;
   if (cached >= 0) return cached;
-  auto k = k_coarse_cycle<T, W>;
+  auto k = k_coarse_cycle<T, W, false>;
   const size_t smem = cluster_smem_bytes<T, W>();
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
       cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
@@ -247,38 +306,72 @@ int coarse_cycle_cluster_size() {
   return cached = 0;
 }
 
+// Every SM x the CTAs of this kernel that fit on one (all resident at once, as
+// a cooperative launch requires).
 template <typename T, int W>
-bool launch_coarse_cycle(const LevelDev<T>* lvDev, int l0, int L, int leg, int preSweeps, int postSweeps, int preBoundary,
-                         int postBoundary, int KP, int coarseN, const double* coarseInv, const double* coarseScale,
-                         unsigned long long* timeline, cudaStream_t s) {
-  const int cs = coarse_cycle_cluster_size<T, W>();
-  if (cs == 0) return false;
-  CoarseCycleArgs a{l0, L, leg, preSweeps, postSweeps, preBoundary, postBoundary, KP, coarseN, coarseInv, coarseScale, timeline};
+int coarse_cycle_grid_size() {
+  static int cached = -1;
+  if (cached >= 0) return cached;
+  auto k = k_coarse_cycle<T, W, true>;
+  const size_t smem = cluster_smem_bytes<T, W>();
+  int dev = 0, sms = 0, coop = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kClusterBlock, smem) != cudaSuccess || per < 1) {
+    cudaGetLastError();
+    return cached = 0;
+  }
+  return cached = sms * per;
+}
+
+template <typename T, int W>
+bool launch_coarse_cycle(const LevelDev<T>* lvDev, int l0, int L, int leg, const CoarseSweeps& sw, int KP, int coarseN,
+                         const double* coarseInv, const double* coarseScale, unsigned long long* timeline,
+                         GridBarrierState* barrier, cudaStream_t s) {
+  CoarseCycleArgs a{l0, L, leg, sw, KP, coarseN, coarseInv, coarseScale, timeline, barrier};
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(cs);
   cfg.blockDim = dim3(kClusterBlock);
   cfg.dynamicSmemBytes = cluster_smem_bytes<T, W>();
   cfg.stream = s;
   cudaLaunchAttribute attr[2];
+  cfg.attrs = attr;
+  if (barrier) {
+    // every CTA resident: cooperative launch (no programmatic overlap with the
+    // previous kernel, whose CTAs would hold SMs the barrier needs)
+    const int ctas = coarse_cycle_grid_size<T, W>();
+    if (ctas == 0) return false;
+    cfg.gridDim = dim3(ctas);
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, W, true>, lvDev, a) == cudaSuccess;
+  }
+  const int cs = coarse_cycle_cluster_size<T, W>();
+  if (cs == 0) return false;
+  cfg.gridDim = dim3(cs);
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = cs;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[1].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
   cfg.numAttrs = programmatic_launch() ? 2 : 1;
-  return cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, W>, lvDev, a) == cudaSuccess;
+  return cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, W, false>, lvDev, a) == cudaSuccess;
 }
 
 int coarse_cycle_cluster_ctas(bool fp64, int W) {
   if (fp64) return W == 4 ? coarse_cycle_cluster_size<double, 4>() : coarse_cycle_cluster_size<double, 1>();
   return W == 4 ? coarse_cycle_cluster_size<float, 4>() : coarse_cycle_cluster_size<float, 1>();
 }
+int coarse_cycle_grid_ctas(bool fp64, int W) {
+  if (fp64) return W == 4 ? coarse_cycle_grid_size<double, 4>() : coarse_cycle_grid_size<double, 1>();
+  return W == 4 ? coarse_cycle_grid_size<float, 4>() : coarse_cycle_grid_size<float, 1>();
+}
 
-#define GDTP_COARSE_CYCLE(T, W)                                                                                           \
-  template bool launch_coarse_cycle<T, W>(const LevelDev<T>*, int, int, int, int, int, int, int, int, int, const double*, \
-                                          const double*, unsigned long long*, cudaStream_t);
+#define GDTP_COARSE_CYCLE(T, W)                                                                                         \
+  template bool launch_coarse_cycle<T, W>(const LevelDev<T>*, int, int, int, const CoarseSweeps&, int, int, const double*, \
+                                          const double*, unsigned long long*, GridBarrierState*, cudaStream_t);
 GDTP_COARSE_CYCLE(float, 1)
 GDTP_COARSE_CYCLE(float, 4)
 GDTP_COARSE_CYCLE(double, 1)

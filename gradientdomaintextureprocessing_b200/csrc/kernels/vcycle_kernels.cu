@@ -28,6 +28,77 @@ __global__ void __launch_bounds__(256) k_gs_colour(const ColourRun* __restrict__
   gs_item<T, W, LoadDefault>(runs, nRuns, coef, planeStride, rhs, x, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// Every sweep of one smoothing step on one chart per block: the colour passes
+// of a chart only read texels of that chart (deep) or boundary texels, which
+// the sweeps do not change, so block barriers order the passes.  The chart's
+// texel span of x is staged in shared memory for all passes (the smoothing of
+// a small level is a chain of dependent memory latencies, and shared memory
+// has the shortest); the updated deep texels are written back at the end.  The
+// arithmetic is gs_item's, so the result is the launch path's, bit for bit.
+constexpr int kGroupBlockMax = 1024;
+template <typename T, int W>
+__global__ void __launch_bounds__(kGroupBlockMax, 1) k_gs_groups(const ColourRun* __restrict__ runs, const int* __restrict__ groups,
+                                                               const T* __restrict__ coef, int planeStride, const T* __restrict__ rhs,
+                                                               T* __restrict__ x, int KP, int G, int sweeps, int reverse) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* xs = reinterpret_cast<T*>(smem_raw);
+  const int* g = groups + 10 * blockIdx.x;
+  const int lo = g[8], span = g[9];
+  const int nt = blockDim.x;
+  for (long long i = threadIdx.x; i < (long long)span * KP; i += nt) xs[i] = x[(long long)lo * KP + i];
+  __syncthreads();
+  for (int sw = 0; sw < sweeps; sw++)
+    for (int cc = 0; cc < 4; cc++) {
+      const int c = reverse ? 3 - cc : cc;
+      const int nr = g[4 + c];
+      const ColourRun* rc = runs + g[c];
+      for (long long t = threadIdx.x; t < (long long)nr * 32 * G; t += nt) {
+        const int per = 32 * G;
+        const int r = int(t / per), rem = int(t - (long long)r * per);
+        const int m = rem / G, q = rem - m * G;
+        const ColourRun R = rc[r];
+        if (m >= R.len) continue;
+        // gs_item with positions relative to the span
+        const int pos = R.pos0 + 2 * m - lo, pp = R.prev0 + 2 * m - lo, pn = R.next0 + 2 * m - lo;
+        const T* cf = coef + R.coef0 + m;
+        const int off = q * W;
+        Vec<T, W> acc;
+#pragma unroll
+        for (int k = 0; k < W; k++) acc.v[k] = 0;
+        axpy(acc, cf[0 * planeStride], vload<T, W>(xs + (pp - 1) * KP + off));
+        axpy(acc, cf[1 * planeStride], vload<T, W>(xs + (pp)*KP + off));
+        axpy(acc, cf[2 * planeStride], vload<T, W>(xs + (pp + 1) * KP + off));
+        axpy(acc, cf[3 * planeStride], vload<T, W>(xs + (pos - 1) * KP + off));
+        axpy(acc, cf[5 * planeStride], vload<T, W>(xs + (pos + 1) * KP + off));
+        axpy(acc, cf[6 * planeStride], vload<T, W>(xs + (pn - 1) * KP + off));
+        axpy(acc, cf[7 * planeStride], vload<T, W>(xs + (pn)*KP + off));
+        axpy(acc, cf[8 * planeStride], vload<T, W>(xs + (pn + 1) * KP + off));
+        const T c4 = cf[4 * planeStride];
+        const Vec<T, W> bv = vload<T, W>(rhs + (long long)(pos + lo) * KP + off);
+        Vec<T, W> out;
+#pragma unroll
+        for (int k = 0; k < W; k++) out.v[k] = bv.v[k] * c4 - acc.v[k];
+        vstore<T, W>(xs + pos * KP + off, out);
+      }
+      __syncthreads();
+    }
+  // write back the chart's deep texels (the rest of the span is unchanged and
+  // may not be written: boundary texels belong to the boundary solve's order)
+  for (int c = 0; c < 4; c++) {
+    const int nr = g[4 + c];
+    const ColourRun* rc = runs + g[c];
+    for (long long t = threadIdx.x; t < (long long)nr * 32; t += nt) {
+      const int r = int(t >> 5), m = int(t & 31);
+      const ColourRun R = rc[r];
+      if (m >= R.len) continue;
+      const int pos = R.pos0 + 2 * m;
+      for (int k = 0; k < KP; k++) x[(long long)pos * KP + k] = xs[(pos - lo) * KP + k];
+    }
+  }
+}
+
 // ----------------------------------------------------------------------------
 // Residual: deep rows by runs (all colours), boundary rows by CSR (global cols).
 // Blocks [0, deepBlocks) handle deep texels, the rest boundary rows.
@@ -186,6 +257,7 @@ __global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode,
     Vec<T, W> sum;
 #pragma unroll
     for (int c = 0; c < W; c++) sum.v[c] = 0;
+#pragma unroll 4
     for (int ch = 0; ch < nch; ch++) {
       const T* src = part + (((long long)blockIdx.x * nch + ch) * 128 + rt) * KP + off;
 #pragma unroll
@@ -498,6 +570,38 @@ void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int plane
   launch(k_gs_colour<T, W>, dim3(nblk((long long)nRuns * 32 * G)), s, runs, nRuns, coef, planeStride, rhs, x, KP, G);
 }
 template <typename T, int W>
+size_t gs_groups_smem(const LevelDev<T>& D, int KP) {
+  return size_t(D.maxGroupSpan) * KP * sizeof(T);
+}
+template <typename T, int W>
+bool launch_gs_groups(const LevelDev<T>& D, int sweeps, bool reverse, int KP, cudaStream_t s) {
+  if (D.nGroups == 0 || sweeps <= 0) return true;
+  const size_t smem = gs_groups_smem<T, W>(D, KP);
+  if (smem > kGroupSmemMax) return false;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_gs_groups<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGroupSmemMax)) != cudaSuccess)
+      return false;
+    attr = true;
+  }
+  const int G = KP / W;
+  // threads: the largest colour pass of a chart, in warps, at most 1024
+  const int items = 32 * G * std::max(1, (D.maxGroupDeep / 4 + 31) / 32 + 1);
+  const int nt = std::min(kGroupBlockMax, std::max(128, (items + 31) / 32 * 32));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(D.nGroups);
+  cfg.blockDim = dim3(nt);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = g_programmatic ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k_gs_groups<T, W>, D.runs, D.groups, (const T*)D.coef, D.planeStride, (const T*)D.b, D.x, KP, G,
+                            sweeps, reverse ? 1 : 0) == cudaSuccess;
+}
+template <typename T, int W>
 void launch_residual(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const int* bPtr, const int* bCol,
                      const T* bVal, const int* bGlobal, int nB, const T* rhs, const T* x, T* res, int KP, cudaStream_t s) {
   const int G = KP / W;
@@ -605,6 +709,7 @@ void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStre
 
 #define GDTP_INSTANTIATE(T, W)                                                                                             \
   template void launch_gs_colour<T, W>(const ColourRun*, int, const T*, int, const T*, T*, int, cudaStream_t);           \
+  template bool launch_gs_groups<T, W>(const LevelDev<T>&, int, bool, int, cudaStream_t);                                \
   template void launch_residual<T, W>(const ColourRun*, int, const T*, int, const int*, const int*, const T*, const int*, \
                                       int, const T*, const T*, T*, int, cudaStream_t);                                   \
   template void launch_restrict<T, W>(const RestrictRun*, int, const int*, const int*, const T*, const int*, int,        \

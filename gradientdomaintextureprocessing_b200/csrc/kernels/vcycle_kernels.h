@@ -64,10 +64,19 @@ struct LevelDev {
   const ProlongRun* pruns = nullptr;   // from the next level
   int nPRuns = 0;
   T *x = nullptr, *b = nullptr, *r = nullptr;
+  const int* groups = nullptr;  // per chart: first run of each colour [4], run counts [4], texel span [2]
+  int nGroups = 0, maxGroupDeep = 0, maxGroupSpan = 0;
 };
 
 template <typename T, int W>
 void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP, cudaStream_t s);
+// `sweeps` 4-colour Gauss-Seidel sweeps (colours 0..3, or 3..0 when reverse)
+// in one launch, one block per chart group with the chart's x in shared memory:
+// the same updates in the same order as launch_gs_colour per colour.  False
+// (nothing launched) when a chart's span does not fit kGroupSmemMax.
+constexpr size_t kGroupSmemMax = 200 * 1024;
+template <typename T, int W>
+bool launch_gs_groups(const LevelDev<T>& D, int sweeps, bool reverse, int KP, cudaStream_t s);
 template <typename T, int W>
 void launch_residual(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const int* bPtr, const int* bCol,
                      const T* bVal, const int* bGlobal, int nB, const T* rhs, const T* x, T* res, int KP, cudaStream_t s);
@@ -111,18 +120,37 @@ void launch_fcg_update(long long n, int K, int KP, const double* sc, const doubl
 // x += e (columns c with frozen[c] != 0 unchanged; frozen may be null), then e = 0
 template <typename T>
 void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s, const int* frozen = nullptr);
-// Coarse levels l0 .. L-1 in one thread-block cluster (coarse_cycle.cu).
+// Sweeps per level inside the coarse-level kernel (the host's pre_sweeps /
+// post_sweeps rule: levels >= coarseFrom use the coarse counts when >= 0).
+struct CoarseSweeps {
+  int finePre, finePost, coarsePre, coarsePost, coarseFrom;
+  int preBoundary, postBoundary;
+  __host__ __device__ int pre(int l) const { return (l >= coarseFrom && coarsePre >= 0) ? coarsePre : finePre; }
+  __host__ __device__ int post(int l) const { return (l >= coarseFrom && coarsePost >= 0) ? coarsePost : finePost; }
+};
+// State of the persistent kernel's grid barrier (device memory, zeroed once;
+// error != 0 after a barrier timed out: zero it again before the next launch)
+struct GridBarrierState {
+  unsigned int count, gen, error, pad;
+};
+// Coarse levels l0 .. L-1 in one kernel (coarse_cycle.cu): one thread-block
+// cluster (barrier == nullptr) or every SM of the device in a cooperative launch
+// with grid barriers (barrier: its state).
 // leg 0: down leg of levels l0..L-2 (pre-smoothing, residual, restriction);
 // leg 1: up leg (prolongation, boundary solve, post-smoothing); leg 2: both with
 // the coarsest dense solve in between.  lvDev: device array of all levels.
 // timeline (optional, 1024 entries): {phase code, globaltimer ns} pairs after each
-// phase, start time in [1022].  Returns false when no cluster can run.
+// phase, start time in [1022].  Returns false when the launch is not possible.
 template <typename T, int W>
-bool launch_coarse_cycle(const LevelDev<T>* lvDev, int l0, int L, int leg, int preSweeps, int postSweeps, int preBoundary,
-                         int postBoundary, int KP, int coarseN, const double* coarseInv, const double* coarseScale,
-                         unsigned long long* timeline, cudaStream_t s);
+bool launch_coarse_cycle(const LevelDev<T>* lvDev, int l0, int L, int leg, const CoarseSweeps& sw, int KP, int coarseN,
+                         const double* coarseInv, const double* coarseScale, unsigned long long* timeline,
+                         GridBarrierState* barrier, cudaStream_t s);
 // CTAs of the coarse-level cluster on this device (0: clusters unavailable)
 int coarse_cycle_cluster_ctas(bool fp64, int W);
+// CTAs of the persistent whole-GPU variant (0: cooperative launch unavailable)
+int coarse_cycle_grid_ctas(bool fp64, int W);
+// largest coarsest level the coarse kernels solve inside (leg 2)
+constexpr int kCoarseInKernelMax(bool grid) { return grid ? 4096 : 1024; }
 // Programmatic dependent launch of the V-cycle kernels (process-wide, default on)
 void set_programmatic_launch(bool on);
 bool programmatic_launch();

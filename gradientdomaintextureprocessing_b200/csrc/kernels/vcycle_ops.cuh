@@ -227,8 +227,12 @@ __device__ __forceinline__ void bs_back_item(const BoundaryDev<T>& B, T* x, int 
   const int p = B.rowSub[i], b0 = B.subPtr[p], m = B.subPtr[p + 1] - b0, a = int(i) - b0;
   Vec<T, W> acc = LD::template ld<T, W>(B.y + i * KP + off);
   const T* Wp = B.wt + B.wOff[p] + a;
-  for (int e = B.touchPtr[p]; e < B.touchPtr[p + 1]; e++, Wp += m)
-    axpy(acc, -*Wp, LD::template ld<T, W>(B.xs + (long long)B.touch[e] * KP + off));
+  const int e0 = B.touchPtr[p], e1 = B.touchPtr[p + 1];
+  // unrolled: the loads of later terms issue before the earlier terms are
+  // added (the additions keep their order)
+#pragma unroll 8
+  for (int e = e0; e < e1; e++)
+    axpy(acc, -Wp[(long long)(e - e0) * m], LD::template ld<T, W>(B.xs + (long long)B.touch[e] * KP + off));
   const T sc = B.scale[i];
 #pragma unroll
   for (int c = 0; c < W; c++) acc.v[c] *= sc;
@@ -242,11 +246,13 @@ __device__ __forceinline__ Vec<T, W> bs_input(const BoundaryDev<T>& B, int mode,
                                               int off) {
   const int k = (mode == 0 ? r0 : B.nI) + j;  // solver position
   Vec<T, W> acc = LD::template ld<T, W>(rhs + (long long)B.posGlobal[k] * KP + off);
+#pragma unroll 4
   for (int e = B.bdPtr[k]; e < B.bdPtr[k + 1]; e++) axpy(acc, -B.bdVal[e], LD::template ld<T, W>(x + (long long)B.bdCol[e] * KP + off));
   const T sc = B.scale[k];
 #pragma unroll
   for (int c = 0; c < W; c++) acc.v[c] *= sc;
   if (mode == 1)
+#pragma unroll 4
     for (int e = B.asiPtr[j]; e < B.asiPtr[j + 1]; e++)
       axpy(acc, -B.asiVal[e], LD::template ld<T, W>(B.y + (long long)B.asiCol[e] * KP + off));
   return acc;

@@ -13,7 +13,7 @@
 #include <cmath>
 #include <string>
 
-#include "../../include/gdtp.h"
+#include "gdtp.h"
 #include "capi_internal.h"
 #include "system.h"
 

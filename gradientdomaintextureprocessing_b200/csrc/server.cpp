@@ -4,7 +4,7 @@
 #include <algorithm>
 #include <cmath>
 
-#include "../../include/gdtp.h"
+#include "gdtp.h"
 
 namespace gdtp {
 

@@ -12,6 +12,7 @@
 // again.  The sequence of launches of one refinement step is captured once into
 // a CUDA graph and replayed.
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -21,7 +22,6 @@
 namespace gdtp {
 
 // coarsest levels up to this size are solved inside the coarse-level cluster
-static const int kClusterCoarseMax = 1024;
 
 static inline int kp_for(int k) {
   if (k <= 1) return 1;
@@ -58,6 +58,56 @@ DeepRuns build_deep_runs(const GridLevel& L) {
   return R;
 }
 
+// Per chart and colour, the range of that colour's runs that lie in the chart:
+// grp[10 g + c] = first run, grp[10 g + 4 + c] = run count, then the chart's
+// texel span (first texel, count) that its updates touch.  Runs of a colour
+// follow the raster lines, chart by chart; false if a chart's runs of some
+// colour are not contiguous (the grouped smoother is then not used).
+static bool chart_groups(const GridLevel& L, const DeepRuns& R, std::vector<int>& grp, int& maxDeep, int& maxSpan) {
+  grp.clear();
+  maxDeep = 0;
+  maxSpan = 0;
+  const int nc = (int)L.charts.size();
+  if (nc == 0 || R.runs.empty()) return false;
+  std::vector<int> first(size_t(nc) * 4, -1), count(size_t(nc) * 4, 0), deep(nc, 0);
+  for (int c = 0; c < 4; c++) {
+    int last = -1;
+    for (int r = R.runStart[c]; r < R.runStart[c + 1]; r++) {
+      const int ch = L.nodes[R.runs[r].pos0].chart;
+      if (ch < 0 || ch >= nc) return false;
+      int& f = first[size_t(ch) * 4 + c];
+      if (f < 0) f = r;
+      else if (ch != last) return false;  // the chart's runs of this colour are split
+      count[size_t(ch) * 4 + c]++;
+      deep[ch] += R.runs[r].len;
+      last = ch;
+    }
+  }
+  // texel span [lo, hi] every update of the chart reads or writes; the span
+  // must hold texels of that chart only (charts are contiguous in texel order)
+  for (int ch = 0; ch < nc; ch++) {
+    if (deep[ch] == 0) continue;
+    int lo = INT_MAX, hi = INT_MIN;
+    for (int c = 0; c < 4; c++)
+      for (int r = first[size_t(ch) * 4 + c], e = r + count[size_t(ch) * 4 + c]; r >= 0 && r < e; r++) {
+        const dev::ColourRun& u = R.runs[r];
+        const int last = 2 * (u.len - 1);
+        lo = std::min({lo, u.pos0 - 1, u.prev0 - 1, u.next0 - 1});
+        hi = std::max({hi, u.pos0 + last + 1, u.prev0 + last + 1, u.next0 + last + 1});
+      }
+    if (lo < 0 || hi >= L.numTexels) return false;
+    for (int i = lo; i <= hi; i++)
+      if (L.nodes[i].chart != ch) return false;
+    for (int c = 0; c < 4; c++) grp.push_back(std::max(0, first[size_t(ch) * 4 + c]));
+    for (int c = 0; c < 4; c++) grp.push_back(count[size_t(ch) * 4 + c]);
+    grp.push_back(lo);
+    grp.push_back(hi - lo + 1);
+    maxDeep = std::max(maxDeep, deep[ch]);
+    maxSpan = std::max(maxSpan, hi - lo + 1);
+  }
+  return !grp.empty();
+}
+
 DeviceSystem::DeviceSystem(const Hierarchy& h, const BoundaryElements& be, int device) : h_(h), be_(be), device_(device) {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { err_ = "no CUDA device"; return; }
@@ -73,6 +123,7 @@ DeviceSystem::~DeviceSystem() {
   if (profEv_[0]) { cudaEventDestroy(profEv_[0]); cudaEventDestroy(profEv_[1]); }
   for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
   if (sumsHost_) cudaFreeHost(sumsHost_);
+  if (barrierErrHost_) cudaFreeHost(barrierErrHost_);
   mg32_.reset();
   mg64_.reset();
   if (stream_) cudaStreamDestroy(stream_);
@@ -304,6 +355,19 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     std::copy(R.runStart, R.runStart + 5, D.runStart);
     D.coef = A.upload(planes);
     D.planeStride = R.count;
+    // chart groups of the runs (grouped smoother): deep texels of different
+    // charts never neighbour each other, so during Gauss-Seidel sweeps (which
+    // leave boundary texels alone) every chart is independent
+    {
+      std::vector<int> grp;
+      int maxDeep = 0, maxSpan = 0;
+      if (chart_groups(G, R, grp, maxDeep, maxSpan)) {
+        D.groups = A.upload(grp);
+        D.nGroups = (int)grp.size() / 10;
+        D.maxGroupDeep = maxDeep;
+        D.maxGroupSpan = maxSpan;
+      }
+    }
     // boundary rows (merged BD + BB, global columns)
     {
       std::vector<int> ptr(1, 0), col;
@@ -427,10 +491,13 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     }
   }
   if (!check(A.last, "multigrid upload")) return false;
-  // whether this device can run the coarse-level cluster (queried outside any capture)
+  // whether this device can run the coarse-level kernels (queried outside any capture)
   mg.clusterOK = dev::coarse_cycle_cluster_ctas(sizeof(T) == 8, (KP % 4 == 0) ? 4 : 1) > 0;
+  mg.gridOK = dev::coarse_cycle_grid_ctas(sizeof(T) == 8, (KP % 4 == 0) ? 4 : 1) > 0;
   mg.levelsDev = A.upload(mg.levels);
-  return check(A.last, "multigrid upload");
+  mg.barrier = static_cast<dev::GridBarrierState*>(A.alloc(sizeof(dev::GridBarrierState)));
+  if (!check(A.last, "multigrid upload")) return false;
+  return check(cudaMemset(mg.barrier, 0, sizeof(dev::GridBarrierState)), "grid barrier");
 }
 
 template bool DeviceSystem::build_multigrid<float>(Multigrid<float>&, int);
@@ -439,6 +506,19 @@ template bool DeviceSystem::build_multigrid<double>(Multigrid<double>&, int);
 // ----------------------------------------------------------------------------
 // V-cycle
 // ----------------------------------------------------------------------------
+std::vector<double> DeviceSystem::level_stats() const {
+  std::vector<double> v;
+  if (!mg32_) return v;
+  for (const LevelDev<float>& D : mg32_->levels) {
+    const dev::BoundaryDev<float>& B = D.B;
+    const double row[] = {double(D.n), double(D.nDeep), double(D.nB), double(B.nI), double(B.nS),
+                          double(B.nSubTasks) * B.subChunks, double(B.nSchurTasks) * B.schurChunks, double(D.nGroups),
+                          double(D.maxGroupDeep)};
+    v.insert(v.end(), row, row + 9);
+  }
+  return v;
+}
+
 bool DeviceSystem::cluster_timeline(std::vector<unsigned long long>& out) {
   out.clear();
   if (!timeline_) return true;
@@ -456,6 +536,27 @@ void DeviceSystem::trace_mark(int i, cudaStream_t s) {
   cudaEventRecordWithFlags(traceEv_[i], s, cudaEventRecordExternal);
 }
 
+// The persistent coarse-level kernel records a grid-barrier timeout in its
+// barrier state; after a solve that used it, the word is copied back with the
+// results and checked once the stream is done.
+template <typename T>
+void DeviceSystem::queue_barrier_check(Multigrid<T>& mg, cudaStream_t s) {
+  if (!usedGridBarrier_ || !mg.barrier) return;
+  if (!barrierErrHost_ && cudaMallocHost(&barrierErrHost_, sizeof(unsigned int)) != cudaSuccess) {
+    barrierErrHost_ = nullptr;
+    return;
+  }
+  *barrierErrHost_ = 0;
+  cudaMemcpyAsync(barrierErrHost_, &mg.barrier->error, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
+}
+template <typename T>
+bool DeviceSystem::barrier_ok(Multigrid<T>& mg) {
+  if (!usedGridBarrier_ || !mg.barrier || !barrierErrHost_ || *barrierErrHost_ == 0) return true;
+  cudaMemset(mg.barrier, 0, sizeof(dev::GridBarrierState));  // usable again for the next solve
+  err_ = "coarse-level kernel: a grid barrier timed out (results discarded)";
+  return false;
+}
+
 template <typename T, int W>
 void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
   const int L = (int)mg.levels.size();
@@ -463,39 +564,54 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
   // levels [lc, L) run in the coarse-level cluster when it is enabled: from the
   // first level below the finest with at most clusterTexels texels
   int lc = L - 1;
-  if (knobs.clusterTexels > 0 && mg.clusterOK)
+  bool grid = false;
+  if (knobs.gridTexels > 0 && mg.gridOK) {
+    for (int l = 1; l + 1 < L; l++)
+      if (mg.levels[l].n <= knobs.gridTexels) { lc = l; grid = true; break; }
+  } else if (knobs.clusterTexels > 0 && mg.clusterOK) {
     for (int l = 1; l + 1 < L; l++)
       if (mg.levels[l].n <= knobs.clusterTexels) { lc = l; break; }
+  }
+  const dev::CoarseSweeps sw{knobs.preSweeps, knobs.postSweeps, knobs.coarsePreSweeps, knobs.coarsePostSweeps, knobs.coarseFrom,
+                             knobs.preBoundary, knobs.postBoundary};
+  dev::GridBarrierState* barrier = grid ? mg.barrier : nullptr;
   trace_mark(0, s);
   for (int l = 0; l < lc; l++) {
     LevelDev<T>& D = mg.levels[l];
     LevelDev<T>& C = mg.levels[l + 1];
     // D.x of levels > 0 was cleared by the restriction into this level
     if (knobs.preBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
-    for (int sw = 0; sw < pre_sweeps(l); sw++) {
-      const bool prof = profiling_ && l == 0 && sw == 0;
-      if (prof) cudaEventRecordWithFlags(profEv_[0], s, cudaEventRecordExternal);
-      for (int c = 0; c < 4; c++)
-        dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
-      if (prof) cudaEventRecordWithFlags(profEv_[1], s, cudaEventRecordExternal);
+    if (grouped(D, KP) && pre_sweeps(l) > 0) {
+      dev::launch_gs_groups<T, W>(D, pre_sweeps(l), false, KP, s);
+    } else {
+      for (int sw = 0; sw < pre_sweeps(l); sw++) {
+        const bool prof = profiling_ && l == 0 && sw == 0;
+        if (prof) cudaEventRecordWithFlags(profEv_[0], s, cudaEventRecordExternal);
+        for (int c = 0; c < 4; c++)
+          dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP,
+                                      s);
+        if (prof) cudaEventRecordWithFlags(profEv_[1], s, cudaEventRecordExternal);
+      }
     }
     dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
     dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, D.r, C.b, C.x, C.n, KP, s);
     trace_mark(l + 1, s);
   }
   if (lc < L - 1) {
-    // coarse levels in one cluster; a large coarsest level is solved by the whole GPU in between
-    const bool whole = mg.coarseN <= kClusterCoarseMax;
+    // coarse levels in one kernel (one cluster, or every SM with grid barriers);
+    // a large coarsest level is solved by an ordinary launch in between
+    const bool whole = mg.coarseN <= dev::kCoarseInKernelMax(grid);
     if (whole) {
-      dev::launch_coarse_cycle<T, W>(mg.levelsDev, lc, L, 2, pre_sweeps(lc), post_sweeps(lc), knobs.preBoundary,
-                                     knobs.postBoundary, KP, mg.coarseN, mg.coarseInv, mg.coarseScale, clusterTimeline(), s);
+      dev::launch_coarse_cycle<T, W>(mg.levelsDev, lc, L, 2, sw, KP, mg.coarseN, mg.coarseInv, mg.coarseScale, clusterTimeline(),
+                                     barrier, s);
     } else {
-      dev::launch_coarse_cycle<T, W>(mg.levelsDev, lc, L, 0, pre_sweeps(lc), post_sweeps(lc), knobs.preBoundary,
-                                     knobs.postBoundary, KP, mg.coarseN, mg.coarseInv, mg.coarseScale, clusterTimeline(), s);
+      dev::launch_coarse_cycle<T, W>(mg.levelsDev, lc, L, 0, sw, KP, mg.coarseN, mg.coarseInv, mg.coarseScale, clusterTimeline(),
+                                     barrier, s);
       dev::launch_coarse_solve<T, W>(mg.coarseN, mg.coarseInv, mg.coarseScale, mg.levels[L - 1].b, mg.levels[L - 1].x, KP, s);
-      dev::launch_coarse_cycle<T, W>(mg.levelsDev, lc, L, 1, pre_sweeps(lc), post_sweeps(lc), knobs.preBoundary,
-                                     knobs.postBoundary, KP, mg.coarseN, mg.coarseInv, mg.coarseScale, clusterTimeline(), s);
+      dev::launch_coarse_cycle<T, W>(mg.levelsDev, lc, L, 1, sw, KP, mg.coarseN, mg.coarseInv, mg.coarseScale, clusterTimeline(),
+                                     barrier, s);
     }
+    usedGridBarrier_ = usedGridBarrier_ || grid;
     for (int i = lc + 1; i <= L + 1 + (L - 2 - lc); i++) trace_mark(i, s);  // the cluster's levels count as one segment
   } else {
     dev::launch_coarse_solve<T, W>(mg.coarseN, mg.coarseInv, mg.coarseScale, mg.levels[L - 1].b, mg.levels[L - 1].x, KP, s);
@@ -505,9 +621,14 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
     LevelDev<T>& D = mg.levels[l];
     dev::launch_prolong_add<T, W>(D.pruns, D.nPRuns, mg.levels[l + 1].x, D.x, KP, s);
     if (knobs.postBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
-    for (int sw = 0; sw < post_sweeps(l); sw++)
-      for (int c = 3; c >= 0; c--)
-        dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
+    if (grouped(D, KP) && post_sweeps(l) > 0) {
+      dev::launch_gs_groups<T, W>(D, post_sweeps(l), true, KP, s);
+    } else {
+      for (int sw = 0; sw < post_sweeps(l); sw++)
+        for (int c = 3; c >= 0; c--)
+          dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP,
+                                      s);
+    }
     trace_mark(L + 1 + (L - 2 - l), s);
   }
 }
@@ -598,9 +719,10 @@ bool DeviceSystem::vcycle_host(float* x, const float* rhs, int k) {
       !check(cudaMemcpyAsync(D0.b, pb.data(), pb.size() * 4, cudaMemcpyHostToDevice, stream_), "h2d"))
     return false;
   if (mg.KP == 1) vcycle<float, 1>(mg, stream_); else vcycle<float, 4>(mg, stream_);
+  queue_barrier_check(mg, stream_);
   if (!check(cudaGetLastError(), "vcycle") ||
       !check(cudaMemcpyAsync(px.data(), D0.x, px.size() * 4, cudaMemcpyDeviceToHost, stream_), "d2h") ||
-      !check(cudaStreamSynchronize(stream_), "vcycle"))
+      !check(cudaStreamSynchronize(stream_), "vcycle") || !barrier_ok(mg))
     return false;
   for (size_t i = 0; i < n; i++)
     for (int c = 0; c < k; c++) x[i * k + c] = px[i * mg.KP + c];
@@ -708,9 +830,10 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     }
   }
   if (x_host && !check(cudaMemcpyAsync(x_host, x64_, n * k * 8, cudaMemcpyDeviceToHost, s), "d2h x")) return false;
+  queue_barrier_check(mg, s);
   cudaEventRecord(e1, s);
   if (userStream) cudaStreamWaitEvent(userStream, e1, 0);
-  if (!check(cudaEventSynchronize(e1), "solve")) return false;
+  if (!check(cudaEventSynchronize(e1), "solve") || !barrier_ok(mg)) return false;
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
@@ -977,8 +1100,9 @@ bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, int k, doubl
     rm = rel_max();
   }
   if (!check(cudaMemcpyAsync(x_host, x64_, n * k * 8, cudaMemcpyDeviceToHost, s), "d2h x")) return false;
+  queue_barrier_check(mg, s);
   cudaEventRecord(e1, s);
-  if (!check(cudaEventSynchronize(e1), "solve")) return false;
+  if (!check(cudaEventSynchronize(e1), "solve") || !barrier_ok(mg)) return false;
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);

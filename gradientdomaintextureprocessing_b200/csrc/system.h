@@ -75,6 +75,8 @@ struct Multigrid {
   int KP = 0;                           // channel stride the vectors were sized for
   const dev::LevelDev<T>* levelsDev = nullptr;  // copy of `levels` in device memory (cluster kernel)
   bool clusterOK = false;               // the device can run the coarse-level cluster
+  bool gridOK = false;                  // the device can run the persistent coarse-level kernel
+  dev::GridBarrierState* barrier = nullptr;  // its grid barrier
   DeviceArena arena;
 };
 
@@ -99,6 +101,9 @@ struct SolverKnobs {
   int maxCoarse = 2600;                 // coarsest level size limit (texels)
   int traceLevels = 0;                  // time every level's down / up leg (events in the graph)
   int clusterTexels = 0;                // levels up to this size run in one thread-block cluster (0: off)
+  int gridTexels = 0;                   // levels up to this size run in one persistent whole-GPU kernel (0: off)
+  int chartTexels = 0;                  // levels whose largest chart has at most this many deep texels
+                                        // smooth all sweeps in one launch, a block per chart (0: off)
   int coarsePreSweeps = 0, coarsePostSweeps = 3;  // sweeps on levels >= coarseFrom (-1: as level 0)
   int coarseFrom = 1;
   int krylov = 0;                       // 1: flexible CG around the V-cycle instead of plain refinement
@@ -144,6 +149,11 @@ class DeviceSystem {
   bool residual_host(const double* b, const double* x, int k, double* rel);
 
   SolverKnobs knobs;
+  template <typename T>
+  bool grouped(const dev::LevelDev<T>& D, int KP) const {
+    return knobs.chartTexels > 0 && D.nGroups > 0 && D.maxGroupDeep <= knobs.chartTexels &&
+           size_t(D.maxGroupSpan) * KP * sizeof(T) <= dev::kGroupSmemMax;
+  }
   int pre_sweeps(int level) const {
     return (level >= knobs.coarseFrom && knobs.coarsePreSweeps >= 0) ? knobs.coarsePreSweeps : knobs.preSweeps;
   }
@@ -166,6 +176,10 @@ class DeviceSystem {
   const RawOperator& raw_system_operator() const { return rawA_; }
   bool is_updated() const { return updated_; }
   int num_texels() const { return h_.levels[0].numTexels; }
+  // per level of the FP32 multigrid (after a solve): texels, deep texels, boundary
+  // texels, subdomain rows, separator rows, subdomain tasks x chunks, Schur tasks
+  // x chunks, chart groups, largest chart (deep texels)
+  std::vector<double> level_stats() const;
   int graphKernels = 0;         // kernel nodes in the refinement-step graph
   int64_t kernelLaunches = 0;   // kernels launched by solve_mixed since the last profile reset
 
@@ -221,6 +235,12 @@ class DeviceSystem {
   std::vector<cudaEvent_t> traceEv_;   // 2 L markers of the captured V-cycle (traceLevels)
   void trace_mark(int i, cudaStream_t s);
   unsigned long long* timeline_ = nullptr;  // cluster phase timeline (traceLevels)
+  bool usedGridBarrier_ = false;        // a captured V-cycle runs the persistent coarse-level kernel
+  unsigned int* barrierErrHost_ = nullptr;  // pinned copy of its barrier's error word
+  template <typename T>
+  void queue_barrier_check(Multigrid<T>& mg, cudaStream_t s);
+  template <typename T>
+  bool barrier_ok(Multigrid<T>& mg);
   unsigned long long* clusterTimeline();
  public:
   // last cluster timeline: {code, ns} pairs (empty when not traced)

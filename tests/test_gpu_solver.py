@@ -161,21 +161,30 @@ def test_solve_is_deterministic(setup):
     np.testing.assert_array_equal(x1, x2)
 
 
-def test_cluster_coarse_levels_match_launch_path(setup):
-    """The coarse levels run in one thread-block cluster give the same bits as
-    one launch per phase (same per-item arithmetic and summation order)."""
+FUSED_KNOBS = ["cluster_texels", "grid_texels", "chart_texels"]
+
+
+@pytest.mark.parametrize("knob", FUSED_KNOBS)
+def test_fused_kernels_match_launch_path(setup, knob):
+    """The coarse levels run in one kernel (one thread-block cluster, or every SM
+    with grid barriers), and the smoothing sweeps run chart by chart in one
+    launch, give the same bits as one launch per phase (same per-item
+    arithmetic and summation order)."""
     g, _, s = setup
     b = g["solve/rhs"]
     x0 = np.zeros_like(b, dtype=np.float32)
-    s.set("cluster_texels", 0)
+    before = {k: s.get(k) for k in FUSED_KNOBS}
+    for k in FUSED_KNOBS:
+        s.set(k, 0)
     try:
         ref = s.vcycle(x0, b.astype(np.float32))
         xr, rr = s.solve(b, tol=1e-6, max_iters=MAX_ITERS)
+        s.set(knob, 1 << 30)
+        got = s.vcycle(x0, b.astype(np.float32))
+        xg, rg = s.solve(b, tol=1e-6, max_iters=MAX_ITERS)
     finally:
-        s.set("cluster_texels", 1 << 30)
-    got = s.vcycle(x0, b.astype(np.float32))
-    xg, rg = s.solve(b, tol=1e-6, max_iters=MAX_ITERS)
-    s.set("cluster_texels", 131072)
+        for k in FUSED_KNOBS:
+            s.set(k, before[k])
     np.testing.assert_array_equal(got, ref)
     assert rg["iterations"] == rr["iterations"]
     np.testing.assert_array_equal(xg, xr)
