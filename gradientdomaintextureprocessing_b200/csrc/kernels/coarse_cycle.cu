@@ -68,8 +68,17 @@ __device__ void cluster_bs_dense(const BoundaryDev<T>& B, int mode, const T* rhs
         // inputs of the (up to) kChunkGroups chunks
         for (int g = 0; g < kChunkGroups && c0 + g < nch; g++) {
           const int j0 = min(m, (c0 + g) * clen), j1 = min(m, j0 + clen);
-          for (int j = j0 + (int)threadIdx.x; j < j1; j += kClusterBlock)
-            vin[g * kBoundaryChunkMax + (j - j0)] = bs_input<T, W, LoadL2>(B, mode, r0, j, rhs, x, KP, off);
+          if (mode == 0) {
+            for (int j = j0 + (int)threadIdx.x; j < j1; j += kClusterBlock)
+              vin[g * kBoundaryChunkMax + (j - j0)] = LoadL2::ld<T, W>(B.rhat + (long long)(r0 + j) * KP + off);
+          } else {
+            const int lane8 = threadIdx.x & 7;
+            for (int jb = j0; jb < j1; jb += kClusterBlock / 8) {
+              const int j = jb + (int)(threadIdx.x >> 3);
+              const Vec<T, W> v = bs_schur_input_group<T, W, LoadL2>(B, j, j < j1, KP, off, lane8);
+              if (j < j1 && lane8 == 0) vin[g * kBoundaryChunkMax + (j - j0)] = v;
+            }
+          }
         }
         __syncthreads();
         T acc[4][W];
@@ -214,10 +223,17 @@ __global__ void __launch_bounds__(kClusterBlock, 1) k_coarse_cycle(const LevelDe
   auto boundary_solve = [&](const LevelDev<T>& D, int code) {
     const BoundaryDev<T>& B = D.B;
     if (B.nb == 0 || !alive) return;
+    // 8-lane group items, 4 per warp, warp-uniform loops
+    const long long w0 = tid >> 5, nw = nth >> 5;
+    const int lane = threadIdx.x & 31;
+    for (long long gb = w0 * 4; gb < (long long)B.nb * G; gb += nw * 4)
+      bs_prep_group<T, W, LoadL2>(B, D.b, D.x, KP, G, gb + (lane >> 3), lane & 7);
+    sync(code + 4);
     if (B.nSubTasks > 0) { cluster_bs_dense<T, W>(B, 0, D.b, D.x, KP, G, red, vin); sync(code + 1); }
     if (B.nS > 0) { cluster_bs_dense<T, W>(B, 1, D.b, D.x, KP, G, red, vin); sync(code + 2); }
     if (B.nI > 0) {
-      for (long long t = tid; t < (long long)B.nI * G; t += nth) bs_back_item<T, W, LoadL2>(B, D.x, KP, G, t);
+      for (long long gb = w0 * 4; gb < (long long)B.nI * G; gb += nw * 4)
+        bs_back_group<T, W, LoadL2>(B, D.x, KP, G, gb + (lane >> 3), lane & 7);
       sync(code + 3);
     }
   };

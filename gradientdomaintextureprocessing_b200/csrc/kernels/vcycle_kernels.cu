@@ -153,11 +153,13 @@ __global__ void __launch_bounds__(256) k_prolong_add(const ProlongRun* __restric
 
 // ----------------------------------------------------------------------------
 // Exact boundary-block solve  x_B = BB^-1 (rhs_B - BD x) over the subdomain /
-// separator split (scaled by s = BB_ii^-1/2), three launches per level:
-//   k_bs_dense mode 0:  y  = Inv_p r^_I,  r^ = s (rhs - BD x) built in the prologue
+// separator split (scaled by s = BB_ii^-1/2), four launches per level:
+//   k_bs_prep:          r^ = s (rhs - BD x) for every boundary position
+//   k_bs_dense mode 0:  y  = Inv_p r^_I
 //   k_bs_dense mode 1:  xs = Sinv t,      t  = r^_S - A_SI y built in the prologue;
 //                       x_S = s xs
 //   k_bs_back:          x_I = s (y - W_p xs),  W_p = Inv_p A_{I_p,S} (m x t_p)
+// The sparse row sums run on 8 lanes per row (group8_sum in vcycle_ops.cuh).
 // The dense products are memory-bound streams of the symmetric inverses,
 // stored row-major with rows padded to a multiple of 4: lane l of a warp reads
 // rows 4l..4l+3 of matrix row j with one vector load, so a warp reads
@@ -187,8 +189,19 @@ __global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode,
   T* part = mode == 0 ? B.subPart : B.schurPart;
   for (int q = 0; q < G; q++) {
     const int off = q * W;
-    // prologue: the chunk's input vector (scaled boundary right-hand side)
-    for (int j = j0 + (int)threadIdx.x; j < j1; j += blockDim.x) vin[j - j0] = bs_input<T, W, LoadDefault>(B, mode, r0, j, rhs, x, KP, off);
+    // prologue: the chunk's input vector (mode 0: the scaled right-hand side
+    // from k_bs_prep; mode 1: minus the coupling to the interior solution)
+    if (mode == 0) {
+      for (int j = j0 + (int)threadIdx.x; j < j1; j += blockDim.x)
+        vin[j - j0] = vload<T, W>(B.rhat + (long long)(r0 + j) * KP + off);
+    } else {
+      const int lane8 = threadIdx.x & 7, grp = threadIdx.x >> 3;
+      for (int jb = j0; jb < j1; jb += 32) {  // 32 groups of 8 lanes
+        const int j = jb + grp;
+        const Vec<T, W> v = bs_schur_input_group<T, W, LoadDefault>(B, j, j < j1, KP, off, lane8);
+        if (j < j1 && lane8 == 0) vin[j - j0] = v;
+      }
+    }
     __syncthreads();
     T acc[4][W];
 #pragma unroll
@@ -281,7 +294,17 @@ template <typename T, int W>
 __global__ void __launch_bounds__(256) k_bs_back(BoundaryDev<T> B, T* __restrict__ x, int KP, int G) {
   grid_dependency_wait();
   grid_launch_dependents();
-  bs_back_item<T, W, LoadDefault>(B, x, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bs_back_group<T, W, LoadDefault>(B, x, KP, G, t >> 3, int(t & 7));
+}
+
+// rhat = s (rhs - BD x) for every boundary position, 8 lanes per position
+template <typename T, int W>
+__global__ void __launch_bounds__(256) k_bs_prep(BoundaryDev<T> B, const T* __restrict__ rhs, const T* __restrict__ x, int KP, int G) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bs_prep_group<T, W, LoadDefault>(B, rhs, x, KP, G, t >> 3, int(t & 7));
 }
 
 // ----------------------------------------------------------------------------
@@ -628,9 +651,10 @@ template <typename T, int W>
 void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s) {
   if (B.nb == 0) return;
   const int G = KP / W;
+  launch(k_bs_prep<T, W>, dim3(nblk((long long)B.nb * G * 8)), s, B, rhs, x, KP, G);
   if (B.nSubTasks > 0) launch(k_bs_dense<T, W>, dim3(B.nSubTasks, B.subChunks), s, B, 0, rhs, x, KP, G);
   if (B.nS > 0) launch(k_bs_dense<T, W>, dim3(B.nSchurTasks, B.schurChunks), s, B, 1, rhs, x, KP, G);
-  if (B.nI > 0) launch(k_bs_back<T, W>, dim3(nblk((long long)B.nI * G)), s, B, x, KP, G);
+  if (B.nI > 0) launch(k_bs_back<T, W>, dim3(nblk((long long)B.nI * G * 8)), s, B, x, KP, G);
 }
 template <typename T, int W>
 void launch_coarse_solve(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, cudaStream_t s) {

@@ -41,6 +41,7 @@ struct BoundaryDev {
   const long long* wOff = nullptr;
   const T* wt = nullptr;                // Inv_p A_{I_p,touch}, column-major m x t_p
   T *y = nullptr, *xs = nullptr, *subPart = nullptr, *schurPart = nullptr;  // work
+  T* rhat = nullptr;                    // scaled right-hand side s (rhs - BD x) per position (work)
   int *subCount = nullptr, *schurCount = nullptr;                            // chunk arrival counters (zero between launches)
 };
 

@@ -218,44 +218,94 @@ __device__ __forceinline__ void prolong_item(const ProlongRun* runs, int nRuns, 
   vstore<T, W>(dst, acc);
 }
 
-// Boundary back substitution x_I = s (y - W_p xs[touch_p]).  Items: interior positions x G.
-template <typename T, int W, typename LD>
-__device__ __forceinline__ void bs_back_item(const BoundaryDev<T>& B, T* x, int KP, int G, long long tid) {
-  const long long i = tid / G;
-  if (i >= B.nI) return;
-  const int q = int(tid - i * G), off = q * W;
-  const int p = B.rowSub[i], b0 = B.subPtr[p], m = B.subPtr[p + 1] - b0, a = int(i) - b0;
-  Vec<T, W> acc = LD::template ld<T, W>(B.y + i * KP + off);
-  const T* Wp = B.wt + B.wOff[p] + a;
-  const int e0 = B.touchPtr[p], e1 = B.touchPtr[p + 1];
-  // unrolled: the loads of later terms issue before the earlier terms are
-  // added (the additions keep their order)
-#pragma unroll 8
-  for (int e = e0; e < e1; e++)
-    axpy(acc, -Wp[(long long)(e - e0) * m], LD::template ld<T, W>(B.xs + (long long)B.touch[e] * KP + off));
-  const T sc = B.scale[i];
+// ---- exact boundary solve, short-latency form.  Every sparse row sum of the
+// boundary solve (BD x, A_SI y, W_p xs) is split over an aligned group of 8
+// lanes (lane l takes terms l, l+8, ...) and added by a fixed shuffle tree
+// ((v0+v4)+(v2+v6))+((v1+v5)+(v3+v7)), so a row costs a couple of dependent
+// loads instead of a chain as long as the row, and the result does not depend
+// on which kernel or thread ran it.  Callers run whole warps (every lane
+// reaches the shuffles; items past the end contribute zeros).
+template <typename T, int W>
+__device__ __forceinline__ Vec<T, W> group8_sum(Vec<T, W> v) {
 #pragma unroll
-  for (int c = 0; c < W; c++) acc.v[c] *= sc;
-  vstore<T, W>(x + (long long)B.posGlobal[i] * KP + off, acc);
+  for (int s = 4; s >= 1; s >>= 1)
+#pragma unroll
+    for (int c = 0; c < W; c++) v.v[c] += __shfl_down_sync(0xffffffffu, v.v[c], s);
+  return v;  // valid in lane 0 of the group
 }
 
-// Input of a boundary dense product at position j of a subdomain (mode 0,
-// r^ = s (rhs - BD x)) or of the separator (mode 1, t = r^_S - A_SI y).
+// rhat_k = s_k (rhs_k - sum_e BD_ke x_e) for position k; group item gi = (k, q)
 template <typename T, int W, typename LD>
-__device__ __forceinline__ Vec<T, W> bs_input(const BoundaryDev<T>& B, int mode, int r0, int j, const T* rhs, const T* x, int KP,
-                                              int off) {
-  const int k = (mode == 0 ? r0 : B.nI) + j;  // solver position
-  Vec<T, W> acc = LD::template ld<T, W>(rhs + (long long)B.posGlobal[k] * KP + off);
-#pragma unroll 4
-  for (int e = B.bdPtr[k]; e < B.bdPtr[k + 1]; e++) axpy(acc, -B.bdVal[e], LD::template ld<T, W>(x + (long long)B.bdCol[e] * KP + off));
-  const T sc = B.scale[k];
+__device__ __forceinline__ void bs_prep_group(const BoundaryDev<T>& B, const T* rhs, const T* x, int KP, int G, long long gi,
+                                              int lane8) {
+  const long long k = gi / G;
+  const int q = int(gi - k * G), off = q * W;
+  const bool valid = k < B.nb;
+  Vec<T, W> acc;
 #pragma unroll
-  for (int c = 0; c < W; c++) acc.v[c] *= sc;
-  if (mode == 1)
-#pragma unroll 4
-    for (int e = B.asiPtr[j]; e < B.asiPtr[j + 1]; e++)
-      axpy(acc, -B.asiVal[e], LD::template ld<T, W>(B.y + (long long)B.asiCol[e] * KP + off));
-  return acc;
+  for (int c = 0; c < W; c++) acc.v[c] = 0;
+  if (valid)
+    for (int e = B.bdPtr[k] + lane8; e < B.bdPtr[k + 1]; e += 8)
+      axpy(acc, B.bdVal[e], LD::template ld<T, W>(x + (long long)B.bdCol[e] * KP + off));
+  acc = group8_sum(acc);
+  if (valid && lane8 == 0) {
+    Vec<T, W> r = LD::template ld<T, W>(rhs + (long long)B.posGlobal[k] * KP + off);
+    const T sc = B.scale[k];
+#pragma unroll
+    for (int c = 0; c < W; c++) r.v[c] = (r.v[c] - acc.v[c]) * sc;
+    vstore<T, W>(B.rhat + k * KP + off, r);
+  }
+}
+
+// Separator input t_j = rhat_{nI+j} - sum_e A_SI,je y_e (valid in lane8 0)
+template <typename T, int W, typename LD>
+__device__ __forceinline__ Vec<T, W> bs_schur_input_group(const BoundaryDev<T>& B, int j, bool valid, int KP, int off, int lane8) {
+  Vec<T, W> acc;
+#pragma unroll
+  for (int c = 0; c < W; c++) acc.v[c] = 0;
+  if (valid)
+    for (int e = B.asiPtr[j] + lane8; e < B.asiPtr[j + 1]; e += 8)
+      axpy(acc, B.asiVal[e], LD::template ld<T, W>(B.y + (long long)B.asiCol[e] * KP + off));
+  acc = group8_sum(acc);
+  Vec<T, W> r;
+#pragma unroll
+  for (int c = 0; c < W; c++) r.v[c] = 0;
+  if (valid && lane8 == 0) {
+    r = LD::template ld<T, W>(B.rhat + (long long)(B.nI + j) * KP + off);
+#pragma unroll
+    for (int c = 0; c < W; c++) r.v[c] -= acc.v[c];
+  }
+  return r;
+}
+
+// Back substitution x_I = s (y - W_p xs) for interior position i; group item gi = (i, q)
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void bs_back_group(const BoundaryDev<T>& B, T* x, int KP, int G, long long gi, int lane8) {
+  const long long i = gi / G;
+  const int q = int(gi - i * G), off = q * W;
+  const bool valid = i < B.nI;
+  Vec<T, W> acc;
+#pragma unroll
+  for (int c = 0; c < W; c++) acc.v[c] = 0;
+  int p = 0, m = 0, a = 0;
+  if (valid) {
+    p = B.rowSub[i];
+    const int b0 = B.subPtr[p];
+    m = B.subPtr[p + 1] - b0;
+    a = int(i) - b0;
+    const T* Wp = B.wt + B.wOff[p] + a;
+    const int e0 = B.touchPtr[p], e1 = B.touchPtr[p + 1];
+    for (int e = e0 + lane8; e < e1; e += 8)
+      axpy(acc, Wp[(long long)(e - e0) * m], LD::template ld<T, W>(B.xs + (long long)B.touch[e] * KP + off));
+  }
+  acc = group8_sum(acc);
+  if (valid && lane8 == 0) {
+    Vec<T, W> r = LD::template ld<T, W>(B.y + i * KP + off);
+    const T sc = B.scale[i];
+#pragma unroll
+    for (int c = 0; c < W; c++) r.v[c] = (r.v[c] - acc.v[c]) * sc;
+    vstore<T, W>(x + (long long)B.posGlobal[i] * KP + off, r);
+  }
 }
 
 // Coarsest level, one row per warp: x = D Ainv^ D rhs (FP64 accumulation).

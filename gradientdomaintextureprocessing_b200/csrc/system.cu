@@ -464,6 +464,7 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       B.asiVal = upT(bs.ASI.val);
       B.y = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nI)) * KP * sizeof(T)));
       B.xs = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * KP * sizeof(T)));
+      B.rhat = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nb)) * KP * sizeof(T)));
     }
     // transfers to / from level l+1
     {

@@ -176,7 +176,10 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * this many texels run in one thread-block cluster; default 0 = off),
  * "grid_texels" (levels up to this many texels run in one persistent kernel on
  * every SM, phases separated by grid barriers; same results as the launch
- * path; takes precedence over "cluster_texels"; 0 = off),
+ * path; takes precedence over "cluster_texels"; 0 = off), "chart_texels"
+ * (levels whose largest chart has at most this many deep texels run all sweeps
+ * of a smoothing step in one launch, one block per chart with the chart's
+ * texels in shared memory; same results; default 2000, 0 = off),
  * "trace_levels" (0/1: time every level's legs, arrays "profile.levels" and
  * "profile.cluster"), "krylov" (0/1, default 0: flexible preconditioned
  * conjugate gradients in FP64 around the FP32 V-cycle instead of plain
