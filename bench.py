@@ -205,6 +205,12 @@ def serve(args):
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
            "requests": len(arrivals), "failed": len(failed),
            "failures": [{k: r[k] for k in ("mesh", "size", "kind", "error")} for r in failed[:5]],
+           "by_kind": {kn: {"p50_ms": float(np.percentile([r["latency_ms"] for _, r in results if r["kind"] == kn], 50)),
+                            "p99_ms": float(np.percentile([r["latency_ms"] for _, r in results if r["kind"] == kn], 99)),
+                            "max_iterations": int(max(r.get("iterations", 0) for _, r in results if r["kind"] == kn))}
+                       for kn in sorted({r["kind"] for _, r in results})},
+           "slowest": sorted(({k: r.get(k) for k in ("mesh", "size", "kind", "latency_ms", "iterations", "batch")}
+                              for _, r in results), key=lambda d: -d["latency_ms"])[:5],
            "arrival_rate_per_s": rate, "wall_s": wall,
            "max_rel_residual": float(max(r["rel_residual_max"] for _, r in results)),
            "batches": st["batches"] - before["batches"], "requests_in_batches": st["batched_requests"] - before["batched_requests"],
@@ -213,6 +219,110 @@ def serve(args):
            "config": {"workload": f"torus / icosphere6 / genus-2, 256^2-{args.serve_max_size}^2 log-uniform, "
                                   "60 % filtering k=3, 30 % geodesic k=1, 10 % LIC k=1, Poisson arrivals", "slots": 4},
            "data": "synthetic"}
+    print(json.dumps(out), flush=True)
+
+
+def timed_config(args):
+    """Extra measurement lines for the geodesic and line-integral-convolution
+    configurations (one JSON line each; the default run measures the filtering
+    solve).  geodesics: icosphere(6) 1024^2, 64 seeded deep-texel sources as 64
+    right-hand sides through the whole heat-method pipeline (host API, sources
+    in, distances out).  lic: genus-2 4096^2 (32 charts), anisotropic metric of
+    ratio 1e3 along a seeded tangent field, M + 1e-4 S, right-hand side M f of a
+    uniform-noise texture, flexible CG around the FP32 V-cycle to 1e-6 (device
+    buffers, and the host API for e2e)."""
+    import torch
+    import ctypes as C
+    from gradientdomaintextureprocessing_b200 import build as _build
+    _build.build()
+    from gradientdomaintextureprocessing_b200 import _lib, meshgen
+    from gradientdomaintextureprocessing_b200.hierarchy import InitializeHierarchy
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    if args.config == "geodesics":
+        from gradientdomaintextureprocessing_b200.geodesics import Geodesics
+        mesh = meshgen.icosphere_atlas(1024, 1024, subdiv=6, seed=0)
+        h = InitializeHierarchy(mesh, levels=4)
+        G = Geodesics(h)
+        srcs = np.random.default_rng(0).choice(h.array("deepGlobal"), size=64, replace=False)
+        setup_s = time.time() - t0
+        for _ in range(args.warmup):
+            G.distance(srcs, tol=TOL)
+        times, reps = [], []
+        with ClockSampler(0) as clocks:
+            th = time.time()
+            for _ in range(args.steps):
+                t1 = time.perf_counter()
+                D, rep = G.distance(srcs, tol=TOL)
+                times.append(time.perf_counter() - t1)
+                reps.append(rep)
+            clocks.mark(th, time.time())
+        n = G.n
+        t = float(np.median(times))
+        out = {"metric": "heat-method geodesics: Mtexels x sources /s at 1e-6 rel. residual (both solves)", "impl": "ours",
+               "value": n * 64 / t / 1e6, "unit": "Mtexels/s (texels x RHS)", "ms_per_step": t * 1e3,
+               "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32 V-cycle + f64 refinement",
+               "data": "synthetic", "api": "gdtp_geodesic_distance (host sources in, host distances out, wall clock)",
+               "config": {"workload": "icosphere6 1024x1024, 16 charts, 64 sources, t = 1e-3, eps = 1e-6", "texels": n,
+                          "rhs": 64, "setup_s": round(setup_s, 1)},
+               "rel_residual_max": float(max(r["rel_residual_max"] for r in reps)),
+               "iterations": int(reps[-1]["iterations"]), "clocks": clocks.summary()}
+    else:
+        from gradientdomaintextureprocessing_b200.metric import InitializeAnisotropicMetric, across_for_ratio
+        from gradientdomaintextureprocessing_b200.system import MASS, System, texel_signal
+        mesh = meshgen.genus2_atlas(4096, 4096)
+        vf = meshgen.gaussian_bump_field(mesh, bumps=8, seed=0)
+        pm = InitializeAnisotropicMetric(mesh, vf, across=across_for_ratio(1e3))
+        h = InitializeHierarchy(mesh, levels=4)
+        s = System(h, parameter_metric=pm)
+        s.update(1e-4, 1.0)
+        s.set("krylov", 1)
+        f = texel_signal(h, mesh["texture"])
+        b = np.ascontiguousarray(s.apply(f, which=MASS).reshape(s.n, -1))
+        setup_s = time.time() - t0
+        L = _lib.lib()
+        b_dev = torch.from_numpy(b).cuda()
+        x_dev = torch.zeros_like(b_dev)
+        k = b.shape[1]
+        st = torch.cuda.current_stream()
+        rep = _lib.Report()
+
+        def step():
+            x_dev.zero_()
+            _lib.check(L.gdtp_solve_device(s.handle, C.c_void_p(b_dev.data_ptr()), C.c_void_p(x_dev.data_ptr()), k, TOL, 500,
+                                           C.c_void_p(st.cuda_stream), C.byref(rep)))
+            return rep.iterations, rep.rel_residual_max
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        with ClockSampler(0) as clocks:
+            th = time.time()
+            ev[0].record(st)
+            res = [step() for _ in range(args.steps)]
+            ev[1].record(st)
+            torch.cuda.synchronize()
+            clocks.mark(th, time.time())
+        t = ev[0].elapsed_time(ev[1]) / args.steps * 1e-3
+        b_pin = torch.from_numpy(b).pin_memory().numpy()
+        x_pin = torch.zeros(b.shape, dtype=torch.float64).pin_memory().numpy()
+        t1 = time.perf_counter()
+        for _ in range(args.steps):
+            _lib.check(L.gdtp_solve_ex(s.handle, b_pin.ctypes.data_as(C.c_void_p), x_pin.ctypes.data_as(C.c_void_p), k, TOL, 500, 1,
+                                       C.byref(rep)))
+        te = (time.perf_counter() - t1) / args.steps
+        n = s.n
+        out = {"metric": "line-integral convolution: Mtexels solved/s at 1e-6 rel. residual", "impl": "ours",
+               "value": n * k / t / 1e6, "unit": "Mtexels/s (texels x RHS)", "ms_per_step": t * 1e3,
+               "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+               "dtype": "f32 V-cycle + f64 flexible CG", "data": "synthetic",
+               "config": {"workload": "genus-2 4096x4096, 32 charts, anisotropic ratio 1e3, M + 1e-4 S, 1 RHS, tol 1e-6",
+                          "texels": n, "rhs": k, "levels_used": s.levels_used, "setup_s": round(setup_s, 1)},
+               "iterations": int(max(r[0] for r in res)), "rel_residual_max": float(max(r[1] for r in res)),
+               "e2e": {"value": n * k / te / 1e6, "unit": "Mtexels/s (texels x RHS)", "h2d_bytes_per_step": int(b.nbytes),
+                       "d2h_bytes_per_step": int(b.nbytes), "api": "gdtp_solve_ex, wall clock"},
+               "clocks": clocks.summary()}
     print(json.dumps(out), flush=True)
 
 
@@ -233,9 +343,13 @@ def main():
                     help="largest texture size of the stream (4096 is the full range; host set-up then takes several minutes)")
     ap.add_argument("--serve-rate", type=float, default=0.0, help="arrivals per second (0: calibrated to saturate)")
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
+    ap.add_argument("--config", choices=["filtering", "geodesics", "lic"], default="filtering",
+                    help="geodesics / lic: extra measurement lines for those workloads (1 GPU)")
     args = ap.parse_args()
     if args.serve:
         return serve(args)
+    if args.config != "filtering":
+        return timed_config(args)
 
     rank, world, local, dist = dist_setup(args.gpus)
     if args.impl == "reference":

@@ -155,8 +155,16 @@ bool GeodesicIntegrator::download(const std::string& name, std::vector<double>& 
   return false;
 }
 
-bool GeodesicIntegrator::ensure_k(int k) {
-  if (k <= G_.kMax) return true;
+// buffer capacity for k right-hand sides: the next power of two (at most 64)
+static int k_capacity(int k) {
+  int c = 1;
+  while (c < k) c *= 2;
+  return std::min(c, 64);
+}
+
+bool GeodesicIntegrator::ensure_k(int kk) {
+  if (kk <= G_.kMax) return true;
+  const int k = k_capacity(kk);
   work_ = DeviceArena();
   G_.fineU = static_cast<double*>(work_.alloc(size_t(std::max(1, G_.nFine)) * k * sizeof(double)));
   G_.fineRhs = static_cast<double*>(work_.alloc(size_t(std::max(1, G_.nFine)) * k * sizeof(double)));
@@ -197,18 +205,22 @@ bool GeodesicIntegrator::distance(DeviceSystem& smooth, DeviceSystem& dist, cons
     if (sources[c] < 0 || sources[c] >= G_.n) { err_ = "source texel out of range"; return false; }
   cudaSetDevice(sys_.device());
   cudaStream_t s = sys_.stream();
-  const size_t nk = size_t(G_.n) * k;
-  if (k != dK_) {
+  // the buffers only grow (to a power of two): varying batch sizes keep them,
+  // and with them the solves' captured graphs
+  if (k > dK_) {
+    const int kc = k_capacity(k);
+    const size_t nk = size_t(G_.n) * kc;
     dwork_ = DeviceArena();
     b_ = static_cast<double*>(dwork_.alloc(nk * sizeof(double)));
     u_ = static_cast<double*>(dwork_.alloc(nk * sizeof(double)));
     r_ = static_cast<double*>(dwork_.alloc(nk * sizeof(double)));
     d_ = static_cast<double*>(dwork_.alloc(nk * sizeof(double)));
-    sv_ = static_cast<double*>(dwork_.alloc(k * sizeof(double)));
-    src_ = static_cast<int*>(dwork_.alloc(k * sizeof(int)));
+    sv_ = static_cast<double*>(dwork_.alloc(kc * sizeof(double)));
+    src_ = static_cast<int*>(dwork_.alloc(kc * sizeof(int)));
     if (!check(dwork_.last, "geodesic buffers")) { dK_ = 0; return false; }
-    dK_ = k;
+    dK_ = kc;
   }
+  const size_t nk = size_t(G_.n) * k;
   double *b = b_, *u = u_, *r = r_, *d = d_, *sv = sv_;
   int* src = src_;
   if (!check(cudaMemcpyAsync(src, sources, k * sizeof(int), cudaMemcpyHostToDevice, s), "h2d sources")) return false;

@@ -186,12 +186,14 @@ void Server::worker() {
       return false;
     });
     if (stop_) return;
-    // batch: queued requests of the same model, tolerance and iteration limit, up to 64 right-hand sides
+    // batch: queued requests of the same model, tolerance and iteration limit,
+    // up to kMaxBatchRhs right-hand sides (a wider batch costs the same per
+    // right-hand side, but holds wider vectors and delays its first request)
     std::vector<ServerRequest*> batch;
     int K = 0;
     for (auto it = queue_.begin(); it != queue_.end();) {
       ServerRequest* r = requests_[*it].get();
-      if (r->model == m->id && r->tol == first->tol && r->maxIters == first->maxIters && K + r->k <= 64) {
+      if (r->model == m->id && r->tol == first->tol && r->maxIters == first->maxIters && K + r->k <= kMaxBatchRhs) {
         batch.push_back(r);
         K += r->k;
         it = queue_.erase(it);

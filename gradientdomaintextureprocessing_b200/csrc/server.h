@@ -7,7 +7,7 @@
 //   geodesic   (M + w S, s M + S) + integration samples; request = k source texels (Geodesics.cpp)
 //   lic        metric given per triangle (anisotropic), M + w S; rhs M f   (LineIntegralConvolution.cpp:698-706)
 // `slots` worker threads take requests in arrival order.  A worker claims an idle
-// model, drains every queued request of that model (up to 64 right-hand sides)
+// model, drains every queued request of that model (up to 16 right-hand sides)
 // into one batched solve, and runs it on the model's own CUDA stream, so work of
 // different models overlaps on the device while requests keep arriving.
 // Converged right-hand sides are frozen inside a batch, so a request's result is
@@ -31,6 +31,7 @@
 namespace gdtp {
 
 enum ModelKind { kKindFilter = 0, kKindGeodesic = 1, kKindLic = 2 };
+constexpr int kMaxBatchRhs = 16;  // right-hand sides per batched solve
 
 struct ServerRequest {
   int64_t id = 0;

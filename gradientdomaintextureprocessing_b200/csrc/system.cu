@@ -118,25 +118,50 @@ DeviceSystem::DeviceSystem(const Hierarchy& h, const BoundaryElements& be, int d
 
 DeviceSystem::~DeviceSystem() {
   cudaSetDevice(device_);
-  if (iterGraph_) cudaGraphExecDestroy(iterGraph_);
-  if (krylovGraph_) cudaGraphExecDestroy(krylovGraph_);
+  for (StepGraph& g : stepGraphs_) cudaGraphExecDestroy(g.exec);
   if (profEv_[0]) { cudaEventDestroy(profEv_[0]); cudaEventDestroy(profEv_[1]); }
   for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
   if (sumsHost_) cudaFreeHost(sumsHost_);
   if (barrierErrHost_) cudaFreeHost(barrierErrHost_);
-  mg32_.reset();
+  mg32_.clear();
   mg64_.reset();
   if (stream_) cudaStreamDestroy(stream_);
 }
 
 void DeviceSystem::invalidate_graph() {
   cudaSetDevice(device_);
-  if (iterGraph_) cudaGraphExecDestroy(iterGraph_);
-  iterGraph_ = nullptr;
-  iterGraphK_ = -1;
-  if (krylovGraph_) cudaGraphExecDestroy(krylovGraph_);
-  krylovGraph_ = nullptr;
-  krylovGraphK_ = -1;
+  for (StepGraph& g : stepGraphs_) cudaGraphExecDestroy(g.exec);
+  stepGraphs_.clear();
+}
+
+cudaGraphExec_t DeviceSystem::find_graph(bool krylov, int k, const double* b, const double* x) {
+  for (size_t i = 0; i < stepGraphs_.size(); i++) {
+    const StepGraph g = stepGraphs_[i];
+    if (g.krylov == krylov && g.k == k && g.b == b && g.x == x) {
+      stepGraphs_.erase(stepGraphs_.begin() + i);
+      stepGraphs_.push_back(g);
+      graphKernels = g.kernels;
+      return g.exec;
+    }
+  }
+  return nullptr;
+}
+
+void DeviceSystem::add_graph(const StepGraph& g) {
+  if (stepGraphs_.size() >= kMaxStepGraphs) {
+    cudaGraphExecDestroy(stepGraphs_.front().exec);
+    stepGraphs_.erase(stepGraphs_.begin());
+  }
+  stepGraphs_.push_back(g);
+  graphKernels = g.kernels;
+}
+
+// capacity for k right-hand sides: the next power of two (at most 64), so a
+// stream of varying batch sizes reallocates (and re-captures) rarely
+static int k_capacity(int k) {
+  int c = 1;
+  while (c < k) c *= 2;
+  return std::min(c, 64);
 }
 
 bool DeviceSystem::check(cudaError_t e, const char* what) {
@@ -147,7 +172,7 @@ bool DeviceSystem::check(cudaError_t e, const char* what) {
 
 size_t DeviceSystem::deviceBytes() const {
   size_t b = rawArena_.total + workArena_.total;
-  if (mg32_) b += mg32_->arena.total;
+  for (const auto& m : mg32_) b += m->arena.total;
   if (mg64_) b += mg64_->arena.total;
   return b;
 }
@@ -301,7 +326,7 @@ bool DeviceSystem::update(double stiffness, double screen) {
     rawA_.nB = L0.numBoundary;
     if (!check(rawArena_.last, "operator upload")) return false;
   }
-  mg32_.reset();
+  mg32_.clear();
   mg64_.reset();
   invalidate_graph();
   updated_ = true;
@@ -504,13 +529,58 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
 template bool DeviceSystem::build_multigrid<float>(Multigrid<float>&, int);
 template bool DeviceSystem::build_multigrid<double>(Multigrid<double>&, int);
 
+// Another channel stride on the same levels: the structure is base's (shared,
+// base outlives it), the vectors and the boundary solve's work are new.
+template <typename T>
+bool DeviceSystem::derive_multigrid(const Multigrid<T>& base, Multigrid<T>& mg, int KP) {
+  DeviceArena& A = mg.arena;
+  mg.levels = base.levels;
+  mg.KP = KP;
+  mg.coarseN = base.coarseN;
+  mg.coarseInv = base.coarseInv;
+  mg.coarseScale = base.coarseScale;
+  for (LevelDev<T>& D : mg.levels) {
+    D.x = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
+    D.b = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
+    D.r = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
+    dev::BoundaryDev<T>& B = D.B;
+    if (B.nb == 0) continue;
+    B.subPart = static_cast<T*>(A.alloc(size_t(std::max(1, B.nSubTasks)) * B.subChunks * 128 * KP * sizeof(T)));
+    B.subCount = A.zeros<int>(std::max(1, B.nSubTasks));
+    if (B.nS > 0) {
+      B.schurPart = static_cast<T*>(A.alloc(size_t(B.nSchurTasks) * B.schurChunks * 128 * KP * sizeof(T)));
+      B.schurCount = A.zeros<int>(B.nSchurTasks);
+    }
+    B.y = static_cast<T*>(A.alloc(size_t(std::max(1, B.nI)) * KP * sizeof(T)));
+    B.xs = static_cast<T*>(A.alloc(size_t(std::max(1, B.nS)) * KP * sizeof(T)));
+    B.rhat = static_cast<T*>(A.alloc(size_t(std::max(1, B.nb)) * KP * sizeof(T)));
+  }
+  if (!check(A.last, "multigrid vectors")) return false;
+  mg.clusterOK = dev::coarse_cycle_cluster_ctas(sizeof(T) == 8, (KP % 4 == 0) ? 4 : 1) > 0;
+  mg.gridOK = dev::coarse_cycle_grid_ctas(sizeof(T) == 8, (KP % 4 == 0) ? 4 : 1) > 0;
+  mg.levelsDev = A.upload(mg.levels);
+  mg.barrier = static_cast<dev::GridBarrierState*>(A.alloc(sizeof(dev::GridBarrierState)));
+  if (!check(A.last, "multigrid vectors")) return false;
+  return check(cudaMemset(mg.barrier, 0, sizeof(dev::GridBarrierState)), "grid barrier");
+}
+
+Multigrid<float>* DeviceSystem::mg32_for(int KP) {
+  for (auto& m : mg32_)
+    if (m->KP == KP) return m.get();
+  std::unique_ptr<Multigrid<float>> m(new Multigrid<float>());
+  const bool ok = mg32_.empty() ? build_multigrid(*m, KP) : derive_multigrid(*mg32_.front(), *m, KP);
+  if (!ok) return nullptr;
+  mg32_.push_back(std::move(m));
+  return mg32_.back().get();
+}
+
 // ----------------------------------------------------------------------------
 // V-cycle
 // ----------------------------------------------------------------------------
 std::vector<double> DeviceSystem::level_stats() const {
   std::vector<double> v;
-  if (!mg32_) return v;
-  for (const LevelDev<float>& D : mg32_->levels) {
+  if (mg32_.empty()) return v;
+  for (const LevelDev<float>& D : mg32_.front()->levels) {
     const dev::BoundaryDev<float>& B = D.B;
     const double row[] = {double(D.n), double(D.nDeep), double(D.nB), double(B.nI), double(B.nS),
                           double(B.nSubTasks) * B.subChunks, double(B.nSchurTasks) * B.schurChunks, double(D.nGroups),
@@ -642,8 +712,9 @@ template void DeviceSystem::vcycle<double, 4>(Multigrid<double>&, cudaStream_t);
 // ----------------------------------------------------------------------------
 // solve work and drivers
 // ----------------------------------------------------------------------------
-bool DeviceSystem::ensure_work(int k) {
-  if (k <= workK_) return true;
+bool DeviceSystem::ensure_work(int kk) {
+  if (kk <= workK_) return true;
+  const int k = k_capacity(kk);
   workArena_ = DeviceArena();
   const size_t n = h_.levels[0].numTexels;
   b64_ = workArena_.zeros<double>(n * k);
@@ -705,12 +776,9 @@ bool DeviceSystem::vcycle_host(float* x, const float* rhs, int k) {
   cudaSetDevice(device_);
   if (!updated_) { err_ = "vcycle before update"; return false; }
   if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
-  const int KP = kp_for(k);
-  if (!mg32_ || mg32_->KP < KP) {
-    mg32_.reset(new Multigrid<float>());
-    if (!build_multigrid(*mg32_, KP)) return false;
-  }
-  Multigrid<float>& mg = *mg32_;
+  Multigrid<float>* mgp = mg32_for(kp_for(k));
+  if (!mgp) return false;
+  Multigrid<float>& mg = *mgp;
   const size_t n = h_.levels[0].numTexels;
   std::vector<float> px(n * mg.KP, 0.f), pb(n * mg.KP, 0.f);
   for (size_t i = 0; i < n; i++)
@@ -736,14 +804,9 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
   cudaSetDevice(device_);
   if (!updated_) { err_ = "solve before update"; return false; }
   if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
-  const int KP = kp_for(k);
-  if (!mg32_ || mg32_->KP < KP) {
-    mg32_.reset(new Multigrid<float>());
-    if (!build_multigrid(*mg32_, KP)) return false;
-    invalidate_graph();
-  }
-  if (!ensure_work(k)) return false;
-  Multigrid<float>& mg = *mg32_;
+  Multigrid<float>* mgp = mg32_for(kp_for(k));
+  if (!mgp || !ensure_work(k)) return false;
+  Multigrid<float>& mg = *mgp;
   const size_t n = h_.levels[0].numTexels;
   cudaStream_t s = stream_;
   cudaEvent_t e0, e1;
@@ -765,8 +828,8 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     if (!krylov_solve(mg, B, X, k, tol, maxIters, s, rep, it, rm)) return false;
   } else {
     // refinement step graph: rhs <- r, e <- V(rhs), x += e, r <- b - A x (+ norms)
-    if (!iterGraph_ || iterGraphK_ != k || iterGraphB_ != B || iterGraphX_ != X) {
-      if (iterGraph_) { cudaGraphExecDestroy(iterGraph_); iterGraph_ = nullptr; }
+    cudaGraphExec_t iterGraph = find_graph(false, k, B, X);
+    if (!iterGraph) {
       cudaGraph_t g;
       if (!prepare_timing(mg)) return false;
       profiling_ = true;
@@ -781,12 +844,15 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
                                    rawA_.bGlobal, rawA_.nB, B, X, D0.b, k, mg.KP, partials_, sums_, s);
       profiling_ = false;
       if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
-      graphKernels = kernel_nodes(g);
-      if (!check(cudaGraphInstantiate(&iterGraph_, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
+      StepGraph sg;
+      sg.k = k;
+      sg.b = B;
+      sg.x = X;
+      sg.kernels = kernel_nodes(g);
+      if (!check(cudaGraphInstantiate(&sg.exec, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
       cudaGraphDestroy(g);
-      iterGraphK_ = k;
-      iterGraphB_ = B;
-      iterGraphX_ = X;
+      add_graph(sg);
+      iterGraph = sg.exec;
     }
     // zero correction, initial residual straight into the FP32 right-hand side
     if (!check(cudaMemsetAsync(mg.levels[0].x, 0, n * mg.KP * sizeof(float), s), "zero correction")) return false;
@@ -820,7 +886,7 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     if (!update_frozen()) return false;
     while (rm > tol && it < maxIters) {
       kernelLaunches += graphKernels;
-      if (!check(cudaGraphLaunch(iterGraph_, s), "graph launch") ||
+      if (!check(cudaGraphLaunch(iterGraph, s), "graph launch") ||
           !check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
           !check(cudaStreamSynchronize(s), "refinement step"))
         return false;
@@ -912,14 +978,15 @@ bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X
                                 SolveReport& rep, int& it, double& rm) {
   const size_t n = h_.levels[0].numTexels;
   if (k > krylovK_) {
+    const int cap = k_capacity(k);
     krylovArena_ = DeviceArena();
-    z_ = static_cast<double*>(krylovArena_.alloc(n * k * sizeof(double)));
-    p_ = static_cast<double*>(krylovArena_.alloc(n * k * sizeof(double)));
-    q_ = static_cast<double*>(krylovArena_.alloc(n * k * sizeof(double)));
-    sc_ = static_cast<double*>(krylovArena_.alloc(4 * size_t(k) * sizeof(double)));
+    z_ = static_cast<double*>(krylovArena_.alloc(n * cap * sizeof(double)));
+    p_ = static_cast<double*>(krylovArena_.alloc(n * cap * sizeof(double)));
+    q_ = static_cast<double*>(krylovArena_.alloc(n * cap * sizeof(double)));
+    sc_ = static_cast<double*>(krylovArena_.alloc(4 * size_t(cap) * sizeof(double)));
     if (!check(krylovArena_.last, "krylov vectors")) return false;
-    krylovK_ = k;
-    if (krylovGraph_) { cudaGraphExecDestroy(krylovGraph_); krylovGraph_ = nullptr; }
+    krylovK_ = cap;
+    invalidate_graph();  // the captured steps use the old vectors
   }
   LevelDev<float>& D0 = mg.levels[0];
   const int KP = mg.KP;
@@ -964,8 +1031,8 @@ bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X
     }
     return !changed || check(cudaMemcpyAsync(frozen_, frozenHost_.data(), k * sizeof(int), cudaMemcpyHostToDevice, s), "frozen flags");
   };
-  if (!krylovGraph_ || krylovGraphX_ != X || krylovGraphK_ != k) {
-    if (krylovGraph_) { cudaGraphExecDestroy(krylovGraph_); krylovGraph_ = nullptr; }
+  cudaGraphExec_t krylovGraph = find_graph(true, k, nullptr, X);
+  if (!krylovGraph) {
     cudaGraph_t g;
     if (!prepare_timing(mg)) return false;
     profiling_ = true;
@@ -979,11 +1046,15 @@ bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X
     dev::launch_fcg_alpha(k, sums_, frozen_, sc_, s);
     dev::launch_fcg_update((long long)n, k, KP, sc_, p_, q_, X, r64_, D0.b, partials_, sums_, s);
     if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
-    graphKernels = kernel_nodes(g);
-    if (!check(cudaGraphInstantiate(&krylovGraph_, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
+    StepGraph sg;
+    sg.krylov = true;
+    sg.k = k;
+    sg.x = X;
+    sg.kernels = kernel_nodes(g);
+    if (!check(cudaGraphInstantiate(&sg.exec, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
     cudaGraphDestroy(g);
-    krylovGraphX_ = X;
-    krylovGraphK_ = k;
+    add_graph(sg);
+    krylovGraph = sg.exec;
   }
   if (!true_residual()) return false;
   rm = rel_from(true);
@@ -994,7 +1065,7 @@ bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X
   if (!restart()) return false;
   while (it < maxIters) {
     kernelLaunches += graphKernels;
-    if (!check(cudaGraphLaunch(krylovGraph_, s), "graph launch") || !fetch("krylov step")) return false;
+    if (!check(cudaGraphLaunch(krylovGraph, s), "graph launch") || !fetch("krylov step")) return false;
     it++;
     collect_timing(mg);
     rm = rel_from(false);  // recursively updated residual

@@ -215,22 +215,40 @@ class DeviceSystem {
   RawOperator rawM_, rawS_, rawA_;
   DeepRuns runs0_;
 
-  std::unique_ptr<Multigrid<float>> mg32_;
+  // FP32 multigrids, one per channel stride KP in use: the first holds the
+  // level structure (coefficients, runs, boundary inverses), the others share
+  // it and own only their KP-wide vectors, so small solves stay narrow after
+  // a wide batch and a new width costs no rebuild
+  std::vector<std::unique_ptr<Multigrid<float>>> mg32_;
+  Multigrid<float>* mg32_for(int KP);
+  template <typename T>
+  bool derive_multigrid(const Multigrid<T>& base, Multigrid<T>& mg, int KP);
   std::unique_ptr<Multigrid<double>> mg64_;
 
   // solve work (tight n x k FP64)
   int* frozen_ = nullptr;              // per right-hand side: converged, x kept (device)
   DeviceArena krylovArena_;            // flexible CG: z, p, q (n x k FP64), scalars
   double *z_ = nullptr, *p_ = nullptr, *q_ = nullptr, *sc_ = nullptr;
-  int krylovK_ = 0, krylovGraphK_ = -1;
-  cudaGraphExec_t krylovGraph_ = nullptr;
-  const double* krylovGraphX_ = nullptr;
+  int krylovK_ = 0;
   std::vector<int> frozenHost_;
   DeviceArena workArena_;
   int workK_ = 0;
   double *b64_ = nullptr, *x64_ = nullptr, *r64_ = nullptr, *partials_ = nullptr, *sums_ = nullptr;
   double* sumsHost_ = nullptr;  // pinned
-  cudaGraphExec_t iterGraph_ = nullptr;
+  // captured step graphs (refinement or flexible-CG step), one per right-hand
+  // side count and buffers, most recently used last: a server batching
+  // requests of varying sizes reuses them instead of capturing again
+  struct StepGraph {
+    bool krylov = false;
+    int k = 0, kernels = 0;
+    const double *b = nullptr, *x = nullptr;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<StepGraph> stepGraphs_;
+  static constexpr size_t kMaxStepGraphs = 16;
+  // the cached graph for this step (moved to the back), or null
+  cudaGraphExec_t find_graph(bool krylov, int k, const double* b, const double* x);
+  void add_graph(const StepGraph& g);
   cudaEvent_t profEv_[2] = {nullptr, nullptr};
   std::vector<cudaEvent_t> traceEv_;   // 2 L markers of the captured V-cycle (traceLevels)
   void trace_mark(int i, cudaStream_t s);
@@ -245,9 +263,6 @@ class DeviceSystem {
  public:
   // last cluster timeline: {code, ns} pairs (empty when not traced)
   bool cluster_timeline(std::vector<unsigned long long>& out);
- private:
-  int iterGraphK_ = -1;
-  const double *iterGraphB_ = nullptr, *iterGraphX_ = nullptr;
 };
 
 }  // namespace gdtp

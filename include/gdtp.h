@@ -231,7 +231,7 @@ int gdtp_geodesic_distance(gdtp_geodesics* g, gdtp_system* smooth, gdtp_system* 
  * Solve server (device).  Holds many meshes / resolutions, admits them to the
  * device under an HBM budget (idle models evicted least recently used first;
  * GDTP_ERR_BUDGET when a model cannot fit) and runs requests with `slots`
- * worker threads: queued requests of one model (same tol and max_iters, up to 64
+ * worker threads: queued requests of one model (same tol and max_iters, up to 16
  * right-hand sides) are solved as one batch on that model's stream while other
  * models' batches run on theirs.  Converged right-hand sides are frozen inside a
  * batch, so each result is the one the request gets alone.  Kinds:
