@@ -315,9 +315,28 @@ __global__ void __launch_bounds__(256) k_coarse_solve(int n, const double* __res
                                                       const T* __restrict__ rhs, T* __restrict__ x, int KP, int G) {
   grid_dependency_wait();
   grid_launch_dependents();
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  coarse_row<T, W, LoadDefault>(n, ainv, scale, rhs, x, KP, G, warp, lane);
+  // 2 rows per block, a warp per part of a row, parts added in order
+  __shared__ double part[2][kCoarseParts][4 * W];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rl = warp / kCoarseParts, p = warp % kCoarseParts, row = blockIdx.x * 2 + rl;
+  for (int q = 0; q < G; q++) {
+    const int off = q * W;
+    double acc[W];
+    if (row < n) coarse_part<T, W, LoadDefault>(n, ainv, scale, rhs, KP, off, row, p, lane, acc);
+    if (row < n && lane == 0)
+#pragma unroll
+      for (int c = 0; c < W; c++) part[rl][p][c] = acc[c];
+    __syncthreads();
+    if (threadIdx.x < 2 * W) {
+      const int r2 = threadIdx.x / W, c = threadIdx.x % W, rr = blockIdx.x * 2 + r2;
+      if (rr < n) {
+        double sum = 0;
+        for (int pp = 0; pp < kCoarseParts; pp++) sum += part[r2][pp][c];
+        x[(long long)rr * KP + off + c] = T(sum * scale[rr]);
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // Per-block sums of two per-channel accumulators into partials[block][0..K) and
@@ -659,7 +678,7 @@ void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, 
 template <typename T, int W>
 void launch_coarse_solve(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, cudaStream_t s) {
   if (n == 0) return;
-  launch(k_coarse_solve<T, W>, dim3(nblk((long long)n * 32)), s, n, ainv, scale, rhs, x, KP, KP / W);
+  launch(k_coarse_solve<T, W>, dim3((n + 1) / 2), s, n, ainv, scale, rhs, x, KP, KP / W);
 }
 
 static inline int raw_groups(int K) { int G = 1; while (4 * G < K) G *= 2; return G; }

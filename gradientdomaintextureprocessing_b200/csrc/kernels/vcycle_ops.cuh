@@ -308,29 +308,49 @@ __device__ __forceinline__ void bs_back_group(const BoundaryDev<T>& B, T* x, int
   }
 }
 
-// Coarsest level, one row per warp: x = D Ainv^ D rhs (FP64 accumulation).
+// Coarsest level: x = D Ainv^ D rhs (FP64 accumulation).  A row's j range is
+// split into kCoarseParts contiguous parts; each part is summed by one warp
+// (lanes stride the part, xor-tree reduction) and the parts are added in part
+// order, so the launch kernel (a warp per part) and the coarse-level kernels
+// (a warp per row, parts in turn) give the same bits.
+constexpr int kCoarseParts = 4;
+template <typename T, int W, typename LD>
+__device__ __forceinline__ void coarse_part(int n, const double* ainv, const double* scale, const T* rhs, int KP, int off, int row,
+                                            int part, int lane, double (&acc)[W]) {
+  const int len = ((n + kCoarseParts - 1) / kCoarseParts + 31) & ~31;
+  const int j0 = part * len, j1 = min(n, j0 + len);
+  const double* arow = ainv + (long long)row * n;
+#pragma unroll
+  for (int c = 0; c < W; c++) acc[c] = 0;
+  for (int j = j0 + lane; j < j1; j += 32) {
+    const Vec<T, W> v = LD::template ld<T, W>(rhs + (long long)j * KP + off);
+    const double w = arow[j] * scale[j];
+#pragma unroll
+    for (int c = 0; c < W; c++) acc[c] += w * double(v.v[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < W; c++)
+    for (int s = 16; s > 0; s >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], s);
+}
+
+// One row by one warp (coarse-level kernels): the parts in turn
 template <typename T, int W, typename LD>
 __device__ __forceinline__ void coarse_row(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, int G, int row,
                                            int lane) {
-  const double* arow = ainv + (long long)row * n;
   for (int q = 0; q < G; q++) {
     const int off = q * W;
-    double acc[W];
+    double sum[W], acc[W];
 #pragma unroll
-    for (int c = 0; c < W; c++) acc[c] = 0;
-    for (int j = lane; j < n; j += 32) {
-      const Vec<T, W> v = LD::template ld<T, W>(rhs + (long long)j * KP + off);
-      const double w = arow[j] * scale[j];
+    for (int c = 0; c < W; c++) sum[c] = 0;
+    for (int p = 0; p < kCoarseParts; p++) {
+      coarse_part<T, W, LD>(n, ainv, scale, rhs, KP, off, row, p, lane, acc);
 #pragma unroll
-      for (int c = 0; c < W; c++) acc[c] += w * double(v.v[c]);
+      for (int c = 0; c < W; c++) sum[c] += acc[c];
     }
-#pragma unroll
-    for (int c = 0; c < W; c++)
-      for (int s = 16; s > 0; s >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], s);
     if (lane == 0) {
       Vec<T, W> out;
 #pragma unroll
-      for (int c = 0; c < W; c++) out.v[c] = T(acc[c] * scale[row]);
+      for (int c = 0; c < W; c++) out.v[c] = T(sum[c] * scale[row]);
       vstore<T, W>(x + (long long)row * KP + off, out);
     }
   }
