@@ -113,6 +113,21 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(f)}
 
 
+def max_over_ranks(ms: float, dist, device: str = "cuda") -> float:
+    """The slowest rank's time: every rank's replica must finish for the job to finish."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, units_per_rank: float, ms: float) -> float:
+    """Whole-job throughput in millions of units per second: all ranks' units over the slowest time."""
+    return world * units_per_rank / (ms * 1e-3) / 1e6
+
+
 def dist_setup(n_gpus: int):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -422,14 +437,11 @@ def main():
     for i in range(args.steps):
         lat.append(ev[i].elapsed_time(ev[i + 1]))
     total_ms = ev[0].elapsed_time(ev[-1])
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist)
     prof = np.zeros(5)
     cnt = C.c_int64()
     L.gdtp_system_array(s.handle, b"profile", 0, prof.ctypes.data_as(C.c_void_p), C.byref(cnt))
-    value = world * n0 * K * args.steps / (total_ms * 1e-3) / 1e6
+    value = job_rate(world, n0 * K * args.steps, total_ms)
 
     # end to end through the host API with pinned buffers
     b_pin = torch.from_numpy(b_host).pin_memory().numpy()
@@ -453,11 +465,8 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * n0 * K * args.steps / (e2e_ms * 1e-3) / 1e6
+    e2e_ms = max_over_ranks(e2e_ms, dist)
+    e2e_value = job_rate(world, n0 * K * args.steps, e2e_ms)
     rel_final = float(s.residual(b_host, x_pin).max())
 
     # plain FP64 GPU V-cycle on the same problem (the comparator path), one solve
