@@ -119,6 +119,7 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
     if (count) *count = 0;
     return GDTP_OK;
   }
+  if (name == "profile.setup") return vec(std::vector<double>(s->sys->setupMs, s->sys->setupMs + 4));
   if (name == "levelStats") return vec(s->sys->level_stats());  // 9 per level, see DeviceSystem::level_stats
   if (name == "levelsUsed") {
     if (count) *count = 1;

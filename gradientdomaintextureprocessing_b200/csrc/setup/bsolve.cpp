@@ -42,26 +42,33 @@ bool dense_spd_inverse(double* A, int n, bool parallel) {
       A[size_t(i) * n + k] = s * inv;
     }
   }
-  // W = L^-1 (lower), column by column
-  std::vector<double> W(size_t(n) * n, 0.0);
+  // W = L^-1 (lower), column by column, stored transposed (Wt[j][i] = W[i][j])
+  // so that every inner product below runs over contiguous rows
+  std::vector<double> Wt(size_t(n) * n, 0.0);
 #pragma omp parallel for schedule(dynamic, 8) if (parallel)
   for (int j = 0; j < n; j++) {
-    W[size_t(j) * n + j] = 1.0 / A[size_t(j) * n + j];
+    double* wj = &Wt[size_t(j) * n];
+    wj[j] = 1.0 / A[size_t(j) * n + j];
     for (int i = j + 1; i < n; i++) {
       double s = 0;
       const double* ri = &A[size_t(i) * n];
-      for (int p = j; p < i; p++) s -= ri[p] * W[size_t(p) * n + j];
-      W[size_t(i) * n + j] = s / A[size_t(i) * n + i];
+      for (int p = j; p < i; p++) s -= ri[p] * wj[p];
+      wj[i] = s / A[size_t(i) * n + i];
     }
   }
-  // A^-1 = W^T W
+  // A^-1 = W^T W: (i, j) = sum_{p >= max(i, j)} W[p][i] W[p][j]
 #pragma omp parallel for schedule(dynamic, 8) if (parallel)
-  for (int i = 0; i < n; i++)
+  for (int i = 0; i < n; i++) {
+    const double* wi = &Wt[size_t(i) * n];
     for (int j = 0; j <= i; j++) {
+      const double* wj = &Wt[size_t(j) * n];
       double s = 0;
-      for (int p = i; p < n; p++) s += W[size_t(p) * n + i] * W[size_t(p) * n + j];
-      A[size_t(i) * n + j] = A[size_t(j) * n + i] = s;
+      for (int p = i; p < n; p++) s += wi[p] * wj[p];
+      A[size_t(i) * n + j] = s;
     }
+  }
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < i; j++) A[size_t(j) * n + i] = A[size_t(i) * n + j];
   return true;
 }
 

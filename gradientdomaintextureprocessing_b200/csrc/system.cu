@@ -280,8 +280,13 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
 // ----------------------------------------------------------------------------
 // coefficient hierarchy + device multigrid
 // ----------------------------------------------------------------------------
+static double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 bool DeviceSystem::update(double stiffness, double screen) {
   if (!err_.empty()) return false;
+  const double tUpdate = now_ms();
   if (fine_.deepMass.empty() && h_.levels[0].numDeep > 0) { err_ = "update before assembly"; return false; }
   cudaSetDevice(device_);
   const GridLevel& L0 = h_.levels[0];
@@ -330,11 +335,14 @@ bool DeviceSystem::update(double stiffness, double screen) {
   mg64_.reset();
   invalidate_graph();
   updated_ = true;
+  setupMs[0] = now_ms() - tUpdate;
   return true;
 }
 
 template <typename T>
 bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
+  const double tBuild = now_ms();
+  double tBoundary = 0, tCoarse = 0;
   const int L = levelsUsed_;
   DeviceArena& A = mg.arena;
   mg.levels.assign(L, LevelDev<T>());
@@ -360,7 +368,9 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
           if (full.col[k] == i) scale[i] = 1.0 / std::sqrt(full.val[k]);
       for (int i = 0; i < n; i++)
         for (int k = full.ptr[i]; k < full.ptr[i + 1]; k++) dense[size_t(i) * n + full.col[k]] = full.val[k] * scale[i] * scale[full.col[k]];
+      const double t0 = now_ms();
       if (!dense_spd_inverse(dense.data(), n, true)) { err_ = "coarsest operator is not positive definite"; return false; }
+      tCoarse += now_ms() - t0;
       mg.coarseN = n;
       mg.coarseInv = A.upload(dense);
       mg.coarseScale = A.upload(scale);
@@ -410,7 +420,9 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     // exact boundary solver
     {
       BoundarySolverSetup bs;
+      const double t0 = now_ms();
       if (!build_boundary_solver(C.bb, C.bd, knobs.maxBlock, bs, err_)) { err_ = "level " + std::to_string(l) + ": " + err_; return false; }
+      tBoundary += now_ms() - t0;
       dev::BoundaryDev<T>& B = D.B;
       B.nb = bs.nb;
       B.nSub = bs.nSub;
@@ -523,6 +535,9 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
   mg.levelsDev = A.upload(mg.levels);
   mg.barrier = static_cast<dev::GridBarrierState*>(A.alloc(sizeof(dev::GridBarrierState)));
   if (!check(A.last, "multigrid upload")) return false;
+  setupMs[1] = tBoundary;
+  setupMs[2] = tCoarse;
+  setupMs[3] = now_ms() - tBuild - tBoundary - tCoarse;
   return check(cudaMemset(mg.barrier, 0, sizeof(dev::GridBarrierState)), "grid barrier");
 }
 

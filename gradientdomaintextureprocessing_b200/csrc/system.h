@@ -180,6 +180,10 @@ class DeviceSystem {
   // texels, subdomain rows, separator rows, subdomain tasks x chunks, Schur tasks
   // x chunks, chart groups, largest chart (deep texels)
   std::vector<double> level_stats() const;
+  // last set-up, ms: update (weights, Galerkin coarsening, FP64 operators),
+  // boundary solver factorisations, coarsest inverse, other multigrid set-up
+  // (device layouts, uploads); the last three when the multigrid is built
+  double setupMs[4] = {0, 0, 0, 0};
   int graphKernels = 0;         // kernel nodes in the refinement-step graph
   int64_t kernelLaunches = 0;   // kernels launched by solve_mixed since the last profile reset
 

@@ -107,7 +107,10 @@ void gdtp_system_free(gdtp_system* s);
  *   "bbMass.ptr/.col/.val" "bbStiffness.*" "bdMass.*" "bdStiffness.*"
  *   after gdtp_system_update: "coef.deep"(level l, raw, 10 per deep texel), "coef.bb.*", "coef.bd.*"
  *   "profile": {timed level-0 sweep groups, their total ms, deep texels per group,
- *   kernels per step graph, kernels launched by solves}; "profile.reset" clears the counts */
+ *   kernels per step graph, kernels launched by solves}; "profile.reset" clears the counts
+ *   "profile.setup": ms of the last set-up {update, boundary solver factorisations,
+ *   coarsest inverse, other multigrid set-up}; the last three are spent by the
+ *   first solve after an update (or after a new right-hand-side width) */
 int gdtp_system_array(const gdtp_system* s, const char* name, int level, void* out, int64_t* count);
 
 /* Combine and coarsen: A = screen*M + stiffness*S, Galerkin hierarchy, coarse
