@@ -214,3 +214,26 @@ def test_krylov_solve_matches_reference_solution(setup, tol):
     assert np.abs(xc[:, 0] - x[:, 0]).max() < 1e-5 * np.abs(x).max()
     # CG never needs more V-cycles than refinement (+1 for the residual check)
     assert rep["iterations"] <= plain["iterations"] + 1
+
+
+def test_widths_in_any_order(setup):
+    """Right-hand-side counts that need different channel widths (1, 5 -> 8,
+    16) solved one after another on one system: every column matches its
+    single-column solve, and a narrow solve after wide ones gives the same bits
+    as before them (each width has its own vectors and captured graphs)."""
+    g, _, s = setup
+    b = g["solve/rhs"]
+    rng = np.random.default_rng(0)
+    B = np.stack([b[:, c % b.shape[1]] * rng.uniform(0.5, 2.0) for c in range(16)], axis=1)
+    x1_before, _ = s.solve(B[:, 0], tol=1e-8, max_iters=MAX_ITERS)
+    x16, r16 = s.solve(B, tol=1e-8, max_iters=MAX_ITERS)
+    x5, r5 = s.solve(B[:, :5], tol=1e-8, max_iters=MAX_ITERS)
+    x1_after, _ = s.solve(B[:, 0], tol=1e-8, max_iters=MAX_ITERS)
+    np.testing.assert_array_equal(x1_after, x1_before)
+    assert r16["rel_residual_max"] <= 1e-8 and r5["rel_residual_max"] <= 1e-8
+    scale = np.abs(x16).max()
+    for c in (0, 3, 4, 15):
+        xc, _ = s.solve(B[:, c], tol=1e-8, max_iters=MAX_ITERS)
+        assert np.abs(x16[:, c] - xc[:, 0]).max() <= 1e-5 * scale
+        if c < 5:
+            assert np.abs(x5[:, c] - xc[:, 0]).max() <= 1e-5 * scale
