@@ -207,6 +207,7 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
   else if (k == "post_boundary" && (v == 0 || v == 1)) kn.postBoundary = v;
   else if (k == "max_block" && v >= 16 && v <= dev::kBoundaryChunkMax) kn.maxBlock = v;
   else if (k == "max_coarse" && v >= 16 && v <= 12000) kn.maxCoarse = v;
+  else if (k == "bs_blocks_per_sm" && v >= 1 && v <= 16) kn.bsBlocksPerSm = v;
   else if (k == "programmatic_launch" && (v == 0 || v == 1)) dev::set_programmatic_launch(v != 0);
   else if (k == "trace_levels" && (v == 0 || v == 1)) kn.traceLevels = v;
   else if (k == "cluster_texels" && v >= 0) kn.clusterTexels = v;
@@ -231,6 +232,7 @@ extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* v
   else if (k == "post_boundary") *value = kn.postBoundary;
   else if (k == "max_block") *value = kn.maxBlock;
   else if (k == "max_coarse") *value = kn.maxCoarse;
+  else if (k == "bs_blocks_per_sm") *value = kn.bsBlocksPerSm;
   else if (k == "programmatic_launch") *value = dev::programmatic_launch() ? 1 : 0;
   else if (k == "trace_levels") *value = kn.traceLevels;
   else if (k == "cluster_texels") *value = kn.clusterTexels;

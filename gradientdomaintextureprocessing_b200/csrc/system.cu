@@ -446,10 +446,11 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
         for (int j = 0; j < m; j++)
           for (int a = 0; a < m; a++) inv[size_t(off[p]) + size_t(j) * mp + a] = T(src[size_t(j) * m + a]);
       }
-      // blocks per row group: enough chunks for one wave of 3 resident blocks
-      // on each of the 148 SMs, each warp still taking >= 4 j steps
-      auto chunks_for = [](int tasks, int m, int minChunks) {
-        int c = (3 * 148 + std::max(1, tasks) - 1) / std::max(1, tasks);
+      // blocks per row group: enough chunks for one wave of bsBlocksPerSm
+      // resident blocks on each of the 148 SMs, each warp still taking >= 4 j steps
+      const int target = knobs.bsBlocksPerSm * 148;
+      auto chunks_for = [target](int tasks, int m, int minChunks) {
+        int c = (target + std::max(1, tasks) - 1) / std::max(1, tasks);
         c = std::min(c, std::max(1, m / 32));
         return std::max(c, std::max(1, minChunks));
       };

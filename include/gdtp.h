@@ -174,6 +174,8 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * level 1), "pre_boundary", "post_boundary" (exact boundary solve before the
  * pre / post sweeps, default 0/1), "max_block" (boundary subdomain size, 16..384,
  * next update), "max_coarse" (coarsest level size, next update),
+ * "bs_blocks_per_sm" (boundary products chunked for this many blocks per SM,
+ * 1..16, default 2, next update),
  * "programmatic_launch" (0/1, default 1: V-cycle kernels overlap their launch
  * with the previous kernel's tail; process-wide), "cluster_texels" (levels up to
  * this many texels run in one thread-block cluster; default 0 = off),
