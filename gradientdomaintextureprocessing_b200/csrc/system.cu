@@ -300,9 +300,31 @@ bool DeviceSystem::update(double stiffness, double screen) {
   for (int l = 0; l < (int)h_.levels.size(); l++)
     if (h_.levels[l].numTexels <= knobs.maxCoarse) { L = l + 1; break; }
   if (h_.levels[L - 1].numTexels > 12000) { err_ = "coarsest level too large for the dense direct solve; build more levels"; return false; }
-  std::vector<LevelCoefficients> co;
-  if (!galerkin_hierarchy(h_, L, deep, bb, bd, co, err_)) return false;
+  // Galerkin coarsening is linear in the weights: the mass and stiffness
+  // hierarchies are coarsened once (per level count) and every update
+  // combines them, so a re-weighting costs one pass over the coefficients
+  if (coLevels_ != L) {
+    Csr bdM = fine_.bdMass, bdS = fine_.bdStiffness;
+    bdM.cols = bdS.cols = L0.numTexels;
+    if (!galerkin_hierarchy(h_, L, fine_.deepMass, fine_.bbMass, bdM, coMass_, err_) ||
+        !galerkin_hierarchy(h_, L, fine_.deepStiffness, fine_.bbStiffness, bdS, coStiff_, err_))
+      return false;
+    coLevels_ = L;
+  }
+  std::vector<LevelCoefficients> co(L);
+  co[0].deep = std::move(deep);
+  co[0].bb = bb;
+  co[0].bd = bd;
+  for (int l = 1; l < L; l++) {
+    const LevelCoefficients &m = coMass_[l], &k = coStiff_[l];
+    co[l].deep.resize(m.deep.size());
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)m.deep.size(); i++) co[l].deep[i] = screen * m.deep[i] + stiffness * k.deep[i];
+    co[l].bb = csr_axpby(screen, m.bb, stiffness, k.bb);
+    co[l].bd = csr_axpby(screen, m.bd, stiffness, k.bd);
+  }
   coeffs_ = std::move(co);
+  const std::vector<double>& deep0 = coeffs_[0].deep;
   levelsUsed_ = L;
   stiffness_ = stiffness;
   screen_ = screen;
@@ -311,7 +333,7 @@ bool DeviceSystem::update(double stiffness, double screen) {
     const int cnt = runs0_.count;
     std::vector<double> planes(size_t(9) * cnt);
     for (int i = 0; i < cnt; i++)
-      for (int k = 0; k < 9; k++) planes[size_t(k) * cnt + i] = deep[10 * size_t(runs0_.texel[i]) + k];
+      for (int k = 0; k < 9; k++) planes[size_t(k) * cnt + i] = deep0[10 * size_t(runs0_.texel[i]) + k];
     std::vector<int> ptr(1, 0), col;
     std::vector<double> val;
     for (int b = 0; b < L0.numBoundary; b++) {

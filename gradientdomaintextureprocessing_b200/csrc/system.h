@@ -211,6 +211,8 @@ class DeviceSystem {
   FineSystem fine_;
   ChartMetrics metric_;
   std::vector<LevelCoefficients> coeffs_;
+  std::vector<LevelCoefficients> coMass_, coStiff_;  // Galerkin hierarchies of M and S (levels coLevels_)
+  int coLevels_ = 0;
   int levelsUsed_ = 0;
   double stiffness_ = 0, screen_ = 0;
   bool updated_ = false;
