@@ -285,15 +285,25 @@ __global__ void __launch_bounds__(kClusterBlock, 1) k_coarse_cycle(const LevelDe
 }
 
 template <typename T, int W>
+int coarse_cycle_cluster_size_uncached();
+template <typename T, int W>
 int coarse_cycle_cluster_size() {
-  static int cached = -1;
-  if (cached >= 0) return cached;
+  static std::atomic<int> cached[kMaxDevices];
+  static const bool init = [] {
+    for (auto& a : cached) a.store(kUnset);
+    return true;
+  }();
+  (void)init;
+  return per_device_once(cached, [] { return coarse_cycle_cluster_size_uncached<T, W>(); });
+}
+template <typename T, int W>
+int coarse_cycle_cluster_size_uncached() {
   auto k = k_coarse_cycle<T, W, false>;
   const size_t smem = cluster_smem_bytes<T, W>();
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
       cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
     cudaGetLastError();
-    return cached = 0;
+    return 0;
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(16);
@@ -316,18 +326,28 @@ int coarse_cycle_cluster_size() {
     attr[0].val.clusterDim.x = c;
     cfg.gridDim = dim3(c);
     int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, k, &cfg) == cudaSuccess && clusters >= 1) return cached = c;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k, &cfg) == cudaSuccess && clusters >= 1) return c;
     cudaGetLastError();
   }
-  return cached = 0;
+  return 0;
 }
 
 // Every SM x the CTAs of this kernel that fit on one (all resident at once, as
 // a cooperative launch requires).
 template <typename T, int W>
+int coarse_cycle_grid_size_uncached();
+template <typename T, int W>
 int coarse_cycle_grid_size() {
-  static int cached = -1;
-  if (cached >= 0) return cached;
+  static std::atomic<int> cached[kMaxDevices];
+  static const bool init = [] {
+    for (auto& a : cached) a.store(kUnset);
+    return true;
+  }();
+  (void)init;
+  return per_device_once(cached, [] { return coarse_cycle_grid_size_uncached<T, W>(); });
+}
+template <typename T, int W>
+int coarse_cycle_grid_size_uncached() {
   auto k = k_coarse_cycle<T, W, true>;
   const size_t smem = cluster_smem_bytes<T, W>();
   int dev = 0, sms = 0, coop = 0, per = 0;
@@ -336,9 +356,9 @@ int coarse_cycle_grid_size() {
       cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kClusterBlock, smem) != cudaSuccess || per < 1) {
     cudaGetLastError();
-    return cached = 0;
+    return 0;
   }
-  return cached = sms * per;
+  return sms * per;
 }
 
 template <typename T, int W>

@@ -620,12 +620,17 @@ bool launch_gs_groups(const LevelDev<T>& D, int sweeps, bool reverse, int KP, cu
   if (D.nGroups == 0 || sweeps <= 0) return true;
   const size_t smem = gs_groups_smem<T, W>(D, KP);
   if (smem > kGroupSmemMax) return false;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_gs_groups<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGroupSmemMax)) != cudaSuccess)
-      return false;
-    attr = true;
-  }
+  static std::atomic<int> attr[kMaxDevices];
+  static const bool init = [] {
+    for (auto& a : attr) a.store(kUnset);
+    return true;
+  }();
+  (void)init;
+  const int ok = per_device_once(attr, [] {
+    return cudaFuncSetAttribute(k_gs_groups<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGroupSmemMax)) == cudaSuccess ? 1
+                                                                                                                              : 0;
+  });
+  if (!ok) return false;
   const int G = KP / W;
   // threads: the largest colour pass of a chart, in warps, at most 1024
   const int items = 32 * G * std::max(1, (D.maxGroupDeep / 4 + 31) / 32 + 1);

@@ -1,9 +1,14 @@
 // Host-callable launchers of the V-cycle kernels (vcycle_kernels.cu).
 #pragma once
+#include <atomic>
 #include <cuda_runtime.h>
 
 namespace gdtp {
 namespace dev {
+
+constexpr int kMaxDevices = 64;
+constexpr int kUnset = -2;
+
 
 struct ColourRun;
 struct RestrictRun;
@@ -152,6 +157,20 @@ int coarse_cycle_cluster_ctas(bool fp64, int W);
 int coarse_cycle_grid_ctas(bool fp64, int W);
 // largest coarsest level the coarse kernels solve inside (leg 2)
 constexpr int kCoarseInKernelMax(bool grid) { return grid ? 4096 : 1024; }
+// Per-device cache of a value a kernel's launch set-up computes once (an
+// attribute set, an occupancy figure): `compute` runs once per device, calls
+// from several threads are safe (the server's workers launch concurrently).
+template <typename F>
+int per_device_once(std::atomic<int> (&slots)[kMaxDevices], F compute) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return compute();
+  int v = slots[dev].load(std::memory_order_acquire);
+  if (v == kUnset) {
+    v = compute();  // a racing thread computes the same value
+    slots[dev].store(v, std::memory_order_release);
+  }
+  return v;
+}
 // Programmatic dependent launch of the V-cycle kernels (process-wide, default on)
 void set_programmatic_launch(bool on);
 bool programmatic_launch();
