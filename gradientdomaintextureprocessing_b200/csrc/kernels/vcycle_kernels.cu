@@ -367,7 +367,8 @@ __device__ __forceinline__ void block_partials(double (&ra)[4], double (&rb)[4],
 // ----------------------------------------------------------------------------
 // FP64 raw operator: res = b - A x (mode 0), y = A x (mode 1) or y = A x with
 // the partial sums of x . y instead of y . y (mode 2) on tight
-// n x K vectors.  Deep rows use 9 raw coefficients per run texel, boundary rows
+// n x K vectors.  Deep rows use 9 raw coefficients per run texel (line runs:
+// up to 32 consecutive deep texels of a raster line), boundary rows
 // the merged BD/BB CSR.  A thread handles one texel and up to 4 channels
 // (group q of G = KP/4 groups, or G = 1 for K = 1).  Per-block sums of res^2
 // and b^2 per channel go to `partials` for a deterministic norm reduction.
@@ -394,8 +395,8 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
       const long long r = t / (32 * G);
       const int m = int(t - r * 32 * G) / G;
       const ColourRun R = runs[r];
-      if (m < R.len) {
-        const int pos = R.pos0 + 2 * m, pp = R.prev0 + 2 * m, pn = R.next0 + 2 * m;
+      if (m < R.len) {  // line runs: consecutive texels
+        const int pos = R.pos0 + m, pp = R.prev0 + m, pn = R.next0 + m;
         const double* c = coef + R.coef0 + m;
         const int nb[9] = {pp - 1, pp, pp + 1, pos - 1, pos, pos + 1, pn - 1, pn, pn + 1};
 #pragma unroll

@@ -30,6 +30,30 @@ static inline int kp_for(int k) {
   return kp;
 }
 
+// Line runs for the FP64 operator (no colouring needed): up to 32 consecutive
+// deep texels of a raster line, so a warp's loads of a neighbour row are
+// contiguous.  texel[i] = deep index of plane position i.
+DeepRuns build_line_runs(const GridLevel& L) {
+  DeepRuns R;
+  R.texel.reserve(L.numDeep);
+  for (const Line& l : L.rasterLines) {
+    const int len = l.end - l.start + 1;
+    for (int p = 0; p < len; p += 32) {
+      dev::ColourRun r;
+      r.pos0 = l.start + p;
+      r.prev0 = l.prev + p;
+      r.next0 = l.next + p;
+      r.coef0 = R.count;
+      r.len = std::min(32, len - p);
+      for (int m = 0; m < r.len; m++) R.texel.push_back(l.coeff + p + m);
+      R.count += r.len;
+      R.runs.push_back(r);
+    }
+  }
+  R.runStart[4] = (int)R.runs.size();
+  return R;
+}
+
 DeepRuns build_deep_runs(const GridLevel& L) {
   DeepRuns R;
   R.texel.reserve(L.numDeep);
@@ -247,8 +271,8 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
   if (!ok) return false;
   if (!assemble_boundary_blocks(h_, be_, w, ham, has, hbm, hbs, fine_, err_)) return false;
 
-  // raw FP64 operators of M and S on level 0 (deep planes in colour-run order)
-  runs0_ = build_deep_runs(h_.levels[0]);
+  // raw FP64 operators of M and S on level 0 (deep planes in line-run order)
+  runs0_ = build_line_runs(h_.levels[0]);
   const GridLevel& L0 = h_.levels[0];
   auto make_raw = [&](const std::vector<double>& deep, const Csr& bb, const Csr& bd, RawOperator& op) {
     const int cnt = runs0_.count;

@@ -62,6 +62,7 @@ struct DeepRuns {
   int count = 0;                // run texels = deep texels
 };
 DeepRuns build_deep_runs(const GridLevel& L);
+DeepRuns build_line_runs(const GridLevel& L);
 
 template <typename T>
 using LevelDev = dev::LevelDev<T>;
