@@ -22,49 +22,103 @@
 
 namespace gdtp {
 
+// Dot products of contiguous rows.  The simd reductions sum in vector lanes
+// (a fixed order for a given build, so results repeat run to run).
+static inline double dot(const double* a, const double* b, int n) {
+  double s = 0;
+#pragma omp simd reduction(+ : s)
+  for (int p = 0; p < n; p++) s += a[p] * b[p];
+  return s;
+}
+// four rows against one: each element of b is loaded once for four products
+static inline void dot4(const double* a0, const double* a1, const double* a2, const double* a3, const double* b, int n, double* out) {
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma omp simd reduction(+ : s0, s1, s2, s3)
+  for (int p = 0; p < n; p++) {
+    const double v = b[p];
+    s0 += a0[p] * v;
+    s1 += a1[p] * v;
+    s2 += a2[p] * v;
+    s3 += a3[p] * v;
+  }
+  out[0] = s0;
+  out[1] = s1;
+  out[2] = s2;
+  out[3] = s3;
+}
+
 // In-place inverse of a dense SPD matrix (row-major, n x n) via Cholesky.
-// Returns false if not positive definite.
+// Returns false if not positive definite.  Every phase works on 4 rows or
+// columns at a time, so that a streamed row serves 4 inner products (the
+// matrices of the coarsest level do not fit in cache).  Built for the baseline
+// x86-64 ISA and for AVX2 + FMA, picked at load time by the CPU that runs it.
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__CUDACC__)
+__attribute__((target_clones("default", "arch=haswell")))
+#endif
 bool dense_spd_inverse(double* A, int n, bool parallel) {
-  // Cholesky, lower triangle: A = L L^T
-  for (int k = 0; k < n; k++) {
-    double d = A[size_t(k) * n + k];
-    for (int p = 0; p < k; p++) d -= A[size_t(k) * n + p] * A[size_t(k) * n + p];
-    if (!(d > 0)) return false;
-    d = std::sqrt(d);
-    A[size_t(k) * n + k] = d;
-    const double inv = 1.0 / d;
-#pragma omp parallel for schedule(static) if (parallel && n - k > 256)
-    for (int i = k + 1; i < n; i++) {
-      double s = A[size_t(i) * n + k];
-      const double* ri = &A[size_t(i) * n];
-      const double* rk = &A[size_t(k) * n];
-      for (int p = 0; p < k; p++) s -= ri[p] * rk[p];
-      A[size_t(i) * n + k] = s * inv;
+  auto row = [&](int i) { return &A[size_t(i) * n]; };
+  // ---- Cholesky A = L L^T (lower triangle), columns in blocks of 4
+  for (int k0 = 0; k0 < n; k0 += 4) {
+    const int kb = std::min(4, n - k0);
+    // the block's own rows: columns k0 .. k0 + kb - 1, one after another
+    for (int k = k0; k < k0 + kb; k++) {
+      double* rk = row(k);
+      const double d2 = rk[k] - dot(rk, rk, k);
+      if (!(d2 > 0)) return false;
+      rk[k] = std::sqrt(d2);
+      for (int i = k + 1; i < k0 + kb; i++) {
+        double* ri = row(i);
+        ri[k] = (ri[k] - dot(ri, rk, k)) / rk[k];
+      }
+    }
+    // rows below: the block's 4 columns share the prefix [0, k0)
+#pragma omp parallel for schedule(static) if (parallel && n - k0 > 256)
+    for (int i = k0 + kb; i < n; i++) {
+      double* ri = row(i);
+      double pre[4] = {0, 0, 0, 0};
+      if (kb == 4) dot4(row(k0), row(k0 + 1), row(k0 + 2), row(k0 + 3), ri, k0, pre);
+      else
+        for (int c = 0; c < kb; c++) pre[c] = dot(row(k0 + c), ri, k0);
+      for (int c = 0; c < kb; c++) {
+        const int k = k0 + c;
+        const double* rk = row(k);
+        double s = ri[k] - pre[c];
+        for (int p = k0; p < k; p++) s -= ri[p] * rk[p];
+        ri[k] = s / rk[k];
+      }
     }
   }
-  // W = L^-1 (lower), column by column, stored transposed (Wt[j][i] = W[i][j])
-  // so that every inner product below runs over contiguous rows
+  // ---- W = L^-1 (lower), stored transposed (Wt[j][i] = W[i][j], zero for i < j),
+  // columns in blocks of 4: row i of L is streamed once for the 4 columns
   std::vector<double> Wt(size_t(n) * n, 0.0);
-#pragma omp parallel for schedule(dynamic, 8) if (parallel)
-  for (int j = 0; j < n; j++) {
-    double* wj = &Wt[size_t(j) * n];
-    wj[j] = 1.0 / A[size_t(j) * n + j];
-    for (int i = j + 1; i < n; i++) {
-      double s = 0;
-      const double* ri = &A[size_t(i) * n];
-      for (int p = j; p < i; p++) s -= ri[p] * wj[p];
-      wj[i] = s / A[size_t(i) * n + i];
+  const int nb4 = (n + 3) / 4;
+#pragma omp parallel for schedule(dynamic, 2) if (parallel)
+  for (int jb = 0; jb < nb4; jb++) {
+    const int j0 = 4 * jb, cb = std::min(4, n - j0);
+    double* w[4];
+    for (int c = 0; c < 4; c++) w[c] = &Wt[size_t(j0 + std::min(c, cb - 1)) * n];
+    for (int c = 0; c < cb; c++) w[c][j0 + c] = 1.0 / A[size_t(j0 + c) * n + j0 + c];
+    for (int i = j0 + 1; i < n; i++) {
+      const double* ri = row(i);
+      double s[4];
+      // sum over p in [j0, i): the zeros of Wt below each column's start add nothing
+      dot4(w[0] + j0, w[1] + j0, w[2] + j0, w[3] + j0, ri + j0, i - j0, s);
+      for (int c = 0; c < cb; c++)
+        if (i > j0 + c) w[c][i] = -s[c] / ri[i];
     }
   }
-  // A^-1 = W^T W: (i, j) = sum_{p >= max(i, j)} W[p][i] W[p][j]
-#pragma omp parallel for schedule(dynamic, 8) if (parallel)
-  for (int i = 0; i < n; i++) {
-    const double* wi = &Wt[size_t(i) * n];
-    for (int j = 0; j <= i; j++) {
-      const double* wj = &Wt[size_t(j) * n];
-      double s = 0;
-      for (int p = i; p < n; p++) s += wi[p] * wj[p];
-      A[size_t(i) * n + j] = s;
+  // ---- A^-1 = W^T W: (i, j) = sum_p Wt[i][p] Wt[j][p], rows i in blocks of 4
+#pragma omp parallel for schedule(dynamic, 2) if (parallel)
+  for (int ib = 0; ib < nb4; ib++) {
+    const int i0 = 4 * ib, rb = std::min(4, n - i0);
+    const double* wi[4];
+    for (int c = 0; c < 4; c++) wi[c] = &Wt[size_t(i0 + std::min(c, rb - 1)) * n];
+    for (int j = 0; j < i0 + rb; j++) {
+      // p from i0: Wt[i][p] is zero for p < i, so the common start adds zeros only
+      double s[4];
+      dot4(wi[0] + i0, wi[1] + i0, wi[2] + i0, wi[3] + i0, &Wt[size_t(j) * n] + i0, n - i0, s);
+      for (int c = 0; c < rb; c++)
+        if (j <= i0 + c) A[size_t(i0 + c) * n + j] = s[c];
     }
   }
   for (int i = 0; i < n; i++)
