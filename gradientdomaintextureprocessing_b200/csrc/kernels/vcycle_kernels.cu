@@ -550,6 +550,13 @@ __global__ void __launch_bounds__(256) k_fcg_update(long long n, int K, int KP, 
   block_partials(a, b, G, K, partials);
 }
 
+// out = a x + b y (the system operator's planes from the mass and stiffness planes)
+__global__ void k_axpby(double* __restrict__ out, double a, const double* __restrict__ x, double b, const double* __restrict__ y,
+                        long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a * x[i] + b * y[i];
+}
+
 // FP64 residual (n*K, tight) -> FP32 right-hand side (n*KP, padded)
 template <typename T>
 __global__ void k_pack_rhs(const double* __restrict__ r, T* __restrict__ rhs, long long n, int K, int KP) {
@@ -747,6 +754,9 @@ void launch_raw_apply_dot(const ColourRun* runs, int nRuns, const double* coef, 
   launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
 }
 
+void launch_axpby(double* out, double a, const double* x, double b, const double* y, long long n, cudaStream_t s) {
+  if (n > 0) k_axpby<<<nblk(n), 256, 0, s>>>(out, a, x, b, y, n);
+}
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s) {
   launch(k_pack_rhs<T>, dim3(nblk(n * KP)), s, r, rhs, n, K, KP);

@@ -123,6 +123,8 @@ void launch_raw_apply_dot(const ColourRun* runs, int nRuns, const double* coef, 
 void launch_fcg_alpha(int K, const double* sums, const int* frozen, double* sc, cudaStream_t s);
 void launch_fcg_update(long long n, int K, int KP, const double* sc, const double* p, const double* q, double* x, double* r, float* rhs32,
                        double* partials, double* sums, cudaStream_t s);
+// out = a x + b y over n doubles
+void launch_axpby(double* out, double a, const double* x, double b, const double* y, long long n, cudaStream_t s);
 // x += e (columns c with frozen[c] != 0 unchanged; frozen may be null), then e = 0
 template <typename T>
 void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s, const int* frozen = nullptr);

@@ -158,10 +158,10 @@ void DeviceSystem::invalidate_graph() {
   stepGraphs_.clear();
 }
 
-cudaGraphExec_t DeviceSystem::find_graph(bool krylov, int k, const double* b, const double* x) {
+cudaGraphExec_t DeviceSystem::find_graph(int kind, int k, const double* b, const double* x) {
   for (size_t i = 0; i < stepGraphs_.size(); i++) {
     const StepGraph g = stepGraphs_[i];
-    if (g.krylov == krylov && g.k == k && g.b == b && g.x == x) {
+    if (g.kind == kind && g.k == k && g.b == b && g.x == x) {
       stepGraphs_.erase(stepGraphs_.begin() + i);
       stepGraphs_.push_back(g);
       graphKernels = g.kernels;
@@ -195,7 +195,7 @@ bool DeviceSystem::check(cudaError_t e, const char* what) {
 }
 
 size_t DeviceSystem::deviceBytes() const {
-  size_t b = rawArena_.total + workArena_.total;
+  size_t b = rawArena_.total + rawAArena_.total + workArena_.total;
   for (const auto& m : mg32_) b += m->arena.total;
   if (mg64_) b += mg64_->arena.total;
   return b;
@@ -348,16 +348,17 @@ bool DeviceSystem::update(double stiffness, double screen) {
     co[l].bd = csr_axpby(screen, m.bd, stiffness, k.bd);
   }
   coeffs_ = std::move(co);
-  const std::vector<double>& deep0 = coeffs_[0].deep;
   levelsUsed_ = L;
   stiffness_ = stiffness;
   screen_ = screen;
-  // raw FP64 A on level 0
+  // raw FP64 A on level 0: its own arena, released on every update (the
+  // deep planes are screen M + stiffness S of the resident M and S planes)
   {
     const int cnt = runs0_.count;
-    std::vector<double> planes(size_t(9) * cnt);
-    for (int i = 0; i < cnt; i++)
-      for (int k = 0; k < 9; k++) planes[size_t(k) * cnt + i] = deep0[10 * size_t(runs0_.texel[i]) + k];
+    rawAArena_ = DeviceArena();
+    double* planes = static_cast<double*>(rawAArena_.alloc(size_t(9) * std::max(1, cnt) * sizeof(double)));
+    if (!check(rawAArena_.last, "operator planes")) return false;
+    dev::launch_axpby(planes, screen, rawM_.coef, stiffness, rawS_.coef, (long long)9 * cnt, stream_);
     std::vector<int> ptr(1, 0), col;
     std::vector<double> val;
     for (int b = 0; b < L0.numBoundary; b++) {
@@ -368,14 +369,14 @@ bool DeviceSystem::update(double stiffness, double screen) {
     rawA_ = RawOperator();
     rawA_.runs = rawM_.runs;
     rawA_.nRuns = rawM_.nRuns;
-    rawA_.coef = rawArena_.upload(planes);
+    rawA_.coef = planes;
     rawA_.planeStride = cnt;
-    rawA_.bPtr = rawArena_.upload(ptr);
-    rawA_.bCol = rawArena_.upload(col);
-    rawA_.bVal = rawArena_.upload(val);
+    rawA_.bPtr = rawAArena_.upload(ptr);
+    rawA_.bCol = rawAArena_.upload(col);
+    rawA_.bVal = rawAArena_.upload(val);
     rawA_.bGlobal = rawM_.bGlobal;
     rawA_.nB = L0.numBoundary;
-    if (!check(rawArena_.last, "operator upload")) return false;
+    if (!check(rawAArena_.last, "operator upload") || !check(cudaStreamSynchronize(stream_), "operator planes")) return false;
   }
   mg32_.clear();
   mg64_.reset();
@@ -425,6 +426,7 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     // deep runs + reciprocal coefficient planes
     DeepRuns R = build_deep_runs(G);
     std::vector<T> planes(size_t(10) * std::max(1, R.count));
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < R.count; i++) {
       const double* c = &C.deep[10 * size_t(R.texel[i])];
       const double c4 = c[4], inv = 1.0 / c4;
@@ -486,6 +488,7 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       }
       if (maxM > dev::kBoundaryChunkMax) { err_ = "boundary subdomain larger than the device chunk limit"; return false; }
       std::vector<T> inv(size_t(off[bs.nSub]), T(0));
+#pragma omp parallel for schedule(dynamic, 4)
       for (int p = 0; p < bs.nSub; p++) {
         const int m = bs.subPtr[p + 1] - bs.subPtr[p], mp = (m + 3) & ~3;
         const double* src = &bs.inv[size_t(bs.invOff[p])];
@@ -890,7 +893,7 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     if (!krylov_solve(mg, B, X, k, tol, maxIters, s, rep, it, rm)) return false;
   } else {
     // refinement step graph: rhs <- r, e <- V(rhs), x += e, r <- b - A x (+ norms)
-    cudaGraphExec_t iterGraph = find_graph(false, k, B, X);
+    cudaGraphExec_t iterGraph = find_graph(0, k, B, X);
     if (!iterGraph) {
       cudaGraph_t g;
       if (!prepare_timing(mg)) return false;
@@ -1093,7 +1096,7 @@ bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X
     }
     return !changed || check(cudaMemcpyAsync(frozen_, frozenHost_.data(), k * sizeof(int), cudaMemcpyHostToDevice, s), "frozen flags");
   };
-  cudaGraphExec_t krylovGraph = find_graph(true, k, nullptr, X);
+  cudaGraphExec_t krylovGraph = find_graph(1, k, nullptr, X);
   if (!krylovGraph) {
     cudaGraph_t g;
     if (!prepare_timing(mg)) return false;
@@ -1109,7 +1112,7 @@ bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X
     dev::launch_fcg_update((long long)n, k, KP, sc_, p_, q_, X, r64_, D0.b, partials_, sums_, s);
     if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
     StepGraph sg;
-    sg.krylov = true;
+    sg.kind = 1;
     sg.k = k;
     sg.x = X;
     sg.kernels = kernel_nodes(g);
@@ -1196,6 +1199,7 @@ bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, int k, doubl
   if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
   const int KP = kp_for(k);
   if (!mg64_ || mg64_->KP < KP) {
+    invalidate_graph();  // captured FP64 steps use the multigrid being replaced
     mg64_.reset(new Multigrid<double>());
     if (!build_multigrid(*mg64_, KP)) return false;
   }
@@ -1224,12 +1228,34 @@ bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, int k, doubl
   double rm = rel_max();
   int it = 0;
   LevelDev<double>& D0 = mg.levels[0];
-  while (rm > tol && it < maxIters) {
+  // one refinement step (rhs <- r, V-cycle, x += e, r <- b - A x and norms)
+  // as a captured graph, like the mixed-precision path
+  cudaGraphExec_t step = find_graph(2, k, b64_, x64_);
+  if (!step) {
+    cudaGraph_t g;
+    if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
     dev::launch_pack_rhs<double>(r64_, D0.b, (long long)n, k, mg.KP, s);
     cudaMemsetAsync(D0.x, 0, n * mg.KP * sizeof(double), s);
     if (mg.KP == 1) vcycle<double, 1>(mg, s); else vcycle<double, 4>(mg, s);
     dev::launch_add_correction<double>(x64_, D0.x, (long long)n, k, mg.KP, s);
-    if (!raw_apply_dev(rawA_, b64_, x64_, r64_, k, 0, s, sumsHost_)) return false;
+    raw_apply_dev(rawA_, b64_, x64_, r64_, k, 0, s, nullptr);
+    if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
+    StepGraph sg;
+    sg.kind = 2;
+    sg.k = k;
+    sg.b = b64_;
+    sg.x = x64_;
+    sg.kernels = kernel_nodes(g);
+    if (!check(cudaGraphInstantiate(&sg.exec, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
+    cudaGraphDestroy(g);
+    add_graph(sg);
+    step = sg.exec;
+  }
+  while (rm > tol && it < maxIters) {
+    if (!check(cudaGraphLaunch(step, s), "graph launch") ||
+        !check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
+        !check(cudaStreamSynchronize(s), "refinement step"))
+      return false;
     it++;
     rm = rel_max();
   }

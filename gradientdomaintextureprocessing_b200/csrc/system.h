@@ -219,7 +219,8 @@ class DeviceSystem {
   bool updated_ = false;
   bool profiling_ = false;
 
-  DeviceArena rawArena_;
+  DeviceArena rawArena_;                // M and S operators (assembly)
+  DeviceArena rawAArena_;               // A = screen M + stiffness S (replaced by every update)
   RawOperator rawM_, rawS_, rawA_;
   DeepRuns runs0_;
 
@@ -247,7 +248,7 @@ class DeviceSystem {
   // side count and buffers, most recently used last: a server batching
   // requests of varying sizes reuses them instead of capturing again
   struct StepGraph {
-    bool krylov = false;
+    int kind = 0;  // 0 refinement (FP32 V-cycle), 1 flexible CG, 2 FP64 V-cycle
     int k = 0, kernels = 0;
     const double *b = nullptr, *x = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -255,7 +256,7 @@ class DeviceSystem {
   std::vector<StepGraph> stepGraphs_;
   static constexpr size_t kMaxStepGraphs = 16;
   // the cached graph for this step (moved to the back), or null
-  cudaGraphExec_t find_graph(bool krylov, int k, const double* b, const double* x);
+  cudaGraphExec_t find_graph(int kind, int k, const double* b, const double* x);
   void add_graph(const StepGraph& g);
   cudaEvent_t profEv_[2] = {nullptr, nullptr};
   std::vector<cudaEvent_t> traceEv_;   // 2 L markers of the captured V-cycle (traceLevels)
