@@ -358,6 +358,8 @@ def main():
                     help="largest texture size of the stream (4096 is the full range; host set-up then takes several minutes)")
     ap.add_argument("--serve-rate", type=float, default=0.0, help="arrivals per second (0: calibrated to saturate)")
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
+    ap.add_argument("--trace-levels", action="store_true",
+                    help="per-level timing of the V-cycle (events inside the captured steps), one JSON line")
     ap.add_argument("--config", choices=["filtering", "geodesics", "lic"], default="filtering",
                     help="geodesics / lic: extra measurement lines for those workloads (1 GPU)")
     args = ap.parse_args()
@@ -391,6 +393,28 @@ def main():
     f = texel_signal(h, mesh["texture"])
     b_host = texture_filtering_rhs(s, f, LAMBDA, SHARP)
     setup_s = time.time() - t0
+    if args.trace_levels:
+        s.set("trace_levels", 1)
+        for _ in range(3):
+            s.solve(b_host, tol=TOL)
+        L = _lib.lib()
+        cnt = C.c_int64()
+        L.gdtp_system_array(s.handle, b"profile.reset", 0, None, C.byref(cnt))
+        for _ in range(10):
+            s.solve(b_host, tol=TOL)
+        L.gdtp_system_array(s.handle, b"profile.levels", 0, None, C.byref(cnt))
+        lv = np.zeros(cnt.value)
+        L.gdtp_system_array(s.handle, b"profile.levels", 0, lv.ctypes.data_as(C.c_void_p), C.byref(cnt))
+        n, nl = int(lv[0]), int(lv[1])
+        stats = np.zeros(9 * nl)
+        L.gdtp_system_array(s.handle, b"levelStats", 0, stats.ctypes.data_as(C.c_void_p), C.byref(cnt))
+        print(json.dumps({"v_cycles_timed": n, "levels": nl,
+                          "texels": [int(v) for v in stats.reshape(-1, 9)[:, 0]],
+                          "boundary_texels": [int(v) for v in stats.reshape(-1, 9)[:, 2]],
+                          "down_us": [round(1e3 * v / n, 1) for v in lv[2:2 + nl - 1]],
+                          "coarsest_us": round(1e3 * lv[1 + nl] / n, 1),
+                          "up_us": [round(1e3 * v / n, 1) for v in lv[2 + nl:2 * nl + 1]]}), flush=True)
+        return
     if args.profile_solves:  # default smoother settings, no autotuner trials in the launch list
         for _ in range(args.profile_solves):
             x, r = s.solve(b_host, tol=TOL)
