@@ -208,6 +208,7 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
   else if (k == "max_block" && v >= 16 && v <= dev::kBoundaryChunkMax) kn.maxBlock = v;
   else if (k == "max_coarse" && v >= 16 && v <= 12000) kn.maxCoarse = v;
   else if (k == "bs_blocks_per_sm" && v >= 1 && v <= 16) kn.bsBlocksPerSm = v;
+  else if (k == "dense_boundary_max" && v >= 0 && v <= 8192) kn.denseBoundaryMax = v;
   else if (k == "programmatic_launch" && (v == 0 || v == 1)) dev::set_programmatic_launch(v != 0);
   else if (k == "trace_levels" && (v == 0 || v == 1)) kn.traceLevels = v;
   else if (k == "cluster_texels" && v >= 0) kn.clusterTexels = v;
@@ -233,6 +234,7 @@ extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* v
   else if (k == "max_block") *value = kn.maxBlock;
   else if (k == "max_coarse") *value = kn.maxCoarse;
   else if (k == "bs_blocks_per_sm") *value = kn.bsBlocksPerSm;
+  else if (k == "dense_boundary_max") *value = kn.denseBoundaryMax;
   else if (k == "programmatic_launch") *value = dev::programmatic_launch() ? 1 : 0;
   else if (k == "trace_levels") *value = kn.traceLevels;
   else if (k == "cluster_texels") *value = kn.clusterTexels;

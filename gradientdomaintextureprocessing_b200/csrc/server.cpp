@@ -49,7 +49,11 @@ int Server::add_model(const Mesh& mesh, int width, int height, int levels, int k
   // (subdomains of up to 384), fixed allocations; the geodesic kind holds two
   // systems and its integration samples.  Fitted to measured sizes (torus,
   // icosphere, genus-2 from 256^2 to 2048^2) with 5-30 % headroom.
-  const double sys = 450.0 * m->h->levels[0].numTexels + 4000.0 * m->h->levels[0].numBoundary + double(24 << 20);
+  double sys = 450.0 * m->h->levels[0].numTexels + 4000.0 * m->h->levels[0].numBoundary + double(24 << 20);
+  // boundary blocks small enough to be inverted whole hold a dense FP32 inverse
+  const int denseMax = SolverKnobs().denseBoundaryMax;
+  for (const GridLevel& g : m->h->levels)
+    if (g.numBoundary <= denseMax) sys += 4.0 * double(g.numBoundary) * g.numBoundary;
   m->estimate = int64_t(kind == kKindGeodesic ? 1.8 * sys : sys);
   std::lock_guard<std::mutex> lk(mu_);
   const int id = (int)models_.size();

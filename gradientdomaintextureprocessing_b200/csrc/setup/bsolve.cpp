@@ -126,7 +126,7 @@ bool dense_spd_inverse(double* A, int n, bool parallel) {
   return true;
 }
 
-bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, BoundarySolverSetup& bs, std::string& err) {
+bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySolverSetup& bs, std::string& err) {
   const int nb = BB.rows;
   bs = BoundarySolverSetup();
   bs.nb = nb;
@@ -169,6 +169,10 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, BoundaryS
       int v = BB.col[k];
       if (part[u] != part[v]) sep[part[u] > part[v] ? u : v] = 1;
     }
+  // a small block is inverted whole: every row in the "separator", whose Schur
+  // complement is then the scaled block itself (one dense product per solve
+  // instead of four dependent steps)
+  if (nb <= denseMax) std::fill(sep.begin(), sep.end(), 1);
   // order: interiors grouped by subdomain, then separators
   std::vector<std::vector<int>> members(nSub);
   for (int u = 0; u < nb; u++)

@@ -277,7 +277,8 @@ struct BoundarySolverSetup {
   std::vector<double> Sinv;             // scaled nS x nS inverse Schur complement
   Csr BD;                               // positions x global texels (unscaled boundary-deep rows)
 };
-bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, BoundarySolverSetup& bs, std::string& err);
+// denseMax: blocks of at most this many rows are inverted whole (no subdomains)
+bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySolverSetup& bs, std::string& err);
 bool dense_spd_inverse(double* A, int n, bool parallel);
 
 }  // namespace gdtp

@@ -469,7 +469,10 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     {
       BoundarySolverSetup bs;
       const double t0 = now_ms();
-      if (!build_boundary_solver(C.bb, C.bd, knobs.maxBlock, bs, err_)) { err_ = "level " + std::to_string(l) + ": " + err_; return false; }
+      if (!build_boundary_solver(C.bb, C.bd, knobs.maxBlock, knobs.denseBoundaryMax, bs, err_)) {
+        err_ = "level " + std::to_string(l) + ": " + err_;
+        return false;
+      }
       tBoundary += now_ms() - t0;
       dev::BoundaryDev<T>& B = D.B;
       B.nb = bs.nb;

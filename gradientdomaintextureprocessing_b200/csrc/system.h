@@ -99,6 +99,7 @@ struct SolverKnobs {
   int preSweeps = 3, postSweeps = 3;
   int preBoundary = 0, postBoundary = 1;  // exact boundary solve before the pre / post sweeps
   int maxBlock = 384;                   // boundary subdomain size
+  int denseBoundaryMax = 0;             // boundary blocks up to this size are inverted whole (0: off)
   int bsBlocksPerSm = 2;                // boundary products: chunk so that a wave has this many blocks per SM
   int maxCoarse = 2600;                 // coarsest level size limit (texels)
   int traceLevels = 0;                  // time every level's down / up leg (events in the graph)

@@ -175,7 +175,9 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * pre / post sweeps, default 0/1), "max_block" (boundary subdomain size, 16..384,
  * next update), "max_coarse" (coarsest level size, next update),
  * "bs_blocks_per_sm" (boundary products chunked for this many blocks per SM,
- * 1..16, default 2, next update),
+ * 1..16, default 2, next update), "dense_boundary_max" (boundary blocks of at most this many
+ * texels are inverted whole instead of by subdomains, 0..8192, default 0 = off,
+ * next update),
  * "programmatic_launch" (0/1, default 1: V-cycle kernels overlap their launch
  * with the previous kernel's tail; process-wide), "cluster_texels" (levels up to
  * this many texels run in one thread-block cluster; default 0 = off),

@@ -110,7 +110,8 @@ int main(int argc, char** argv) {
   for (size_t l = 0; l < lc.size(); l++) {
     BoundarySolverSetup bs;
     int maxBlock = argc > 5 ? atoi(argv[5]) : 384;
-    if (!build_boundary_solver(lc[l].bb, lc[l].bd, maxBlock, bs, err)) { fprintf(stderr, "bsolve: %s\n", err.c_str()); return 3; }
+    int denseMax = argc > 6 ? atoi(argv[6]) : 0;
+    if (!build_boundary_solver(lc[l].bb, lc[l].bd, maxBlock, denseMax, bs, err)) { fprintf(stderr, "bsolve: %s\n", err.c_str()); return 3; }
     const Csr& BB = lc[l].bb;
     std::vector<double> xt(bs.nb), r(bs.nb, 0.0), x(bs.nb, 0.0);
     for (int i = 0; i < bs.nb; i++) xt[i] = std::sin(0.37 * i) + 0.1 * std::cos(1.3 * i);
