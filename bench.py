@@ -497,7 +497,9 @@ def main():
     x64, rep64 = s.solve(b_host, tol=TOL, precision="fp64")
     t64 = rep64["seconds"]
     # dominant kernel: level-0 colour Gauss-Seidel sweep (4 colour passes), timed
-    # by events recorded inside the captured refinement graph
+    # by events recorded inside the captured refinement graph: the average of
+    # the full sweeps of each V-cycle (the pre-smoothing after its zero-start
+    # sweep, and the post-smoothing)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))

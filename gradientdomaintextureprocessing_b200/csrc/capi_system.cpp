@@ -218,6 +218,7 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
   else if (k == "coarse_post_sweeps" && v >= -1 && v <= 16) kn.coarsePostSweeps = v;
   else if (k == "coarse_from" && v >= 1 && v <= 16) kn.coarseFrom = v;
   else if (k == "krylov" && (v == 0 || v == 1)) kn.krylov = v;
+  else if (k == "zero_start_skip" && (v == 0 || v == 1)) kn.zeroStartSkip = v;
   else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
   s->sys->invalidate_graph();
   return GDTP_OK;
@@ -242,6 +243,7 @@ extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* v
   else if (k == "coarse_post_sweeps") *value = kn.coarsePostSweeps;
   else if (k == "coarse_from") *value = kn.coarseFrom;
   else if (k == "krylov") *value = kn.krylov;
+  else if (k == "zero_start_skip") *value = kn.zeroStartSkip;
   else if (k == "grid_texels") *value = kn.gridTexels;
   else if (k == "chart_texels") *value = kn.chartTexels;
   else return fail(GDTP_ERR_INVALID, "gdtp_system_get: unknown knob " + k);

@@ -22,10 +22,11 @@ namespace dev {
 // ----------------------------------------------------------------------------
 template <typename T, int W>
 __global__ void __launch_bounds__(256) k_gs_colour(const ColourRun* __restrict__ runs, int nRuns, const T* __restrict__ coef,
-                                                   int planeStride, const T* __restrict__ rhs, T* __restrict__ x, int KP, int G) {
+                                                   int planeStride, const T* __restrict__ rhs, T* __restrict__ x, int KP, int G,
+                                                   int skip) {
   grid_dependency_wait();
   grid_launch_dependents();
-  gs_item<T, W, LoadDefault>(runs, nRuns, coef, planeStride, rhs, x, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  gs_item<T, W, LoadDefault>(runs, nRuns, coef, planeStride, rhs, x, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x, skip);
 }
 
 // Every sweep of one smoothing step on one chart per block: the colour passes
@@ -614,10 +615,10 @@ static void launch(void (*kernel)(P...), dim3 grid, cudaStream_t s, A... args) {
 
 template <typename T, int W>
 void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP,
-                      cudaStream_t s) {
+                      cudaStream_t s, int skip) {
   if (nRuns == 0) return;
   const int G = KP / W;
-  launch(k_gs_colour<T, W>, dim3(nblk((long long)nRuns * 32 * G)), s, runs, nRuns, coef, planeStride, rhs, x, KP, G);
+  launch(k_gs_colour<T, W>, dim3(nblk((long long)nRuns * 32 * G)), s, runs, nRuns, coef, planeStride, rhs, x, KP, G, skip);
 }
 template <typename T, int W>
 size_t gs_groups_smem(const LevelDev<T>& D, int KP) {
@@ -767,7 +768,7 @@ void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStre
 }
 
 #define GDTP_INSTANTIATE(T, W)                                                                                             \
-  template void launch_gs_colour<T, W>(const ColourRun*, int, const T*, int, const T*, T*, int, cudaStream_t);           \
+  template void launch_gs_colour<T, W>(const ColourRun*, int, const T*, int, const T*, T*, int, cudaStream_t, int);      \
   template bool launch_gs_groups<T, W>(const LevelDev<T>&, int, bool, int, cudaStream_t);                                \
   template void launch_residual<T, W>(const ColourRun*, int, const T*, int, const int*, const int*, const T*, const int*, \
                                       int, const T*, const T*, T*, int, cudaStream_t);                                   \

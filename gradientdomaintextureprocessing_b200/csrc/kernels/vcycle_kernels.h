@@ -75,7 +75,9 @@ struct LevelDev {
 };
 
 template <typename T, int W>
-void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP, cudaStream_t s);
+// skip: bit k set = neighbour slot k (3 (dy + 1) + dx + 1) is known to be zero
+void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP, cudaStream_t s,
+                      int skip = 0);
 // `sweeps` 4-colour Gauss-Seidel sweeps (colours 0..3, or 3..0 when reverse)
 // in one launch, one block per chart group with the chart's x in shared memory:
 // the same updates in the same order as launch_gs_colour per colour.  False

@@ -73,7 +73,7 @@ __device__ __forceinline__ void axpy(Vec<T, W>& acc, T a, const Vec<T, W>& v) {
 // (IterativeSolvers.inl:449-463).  Items: runs x 32 x G.
 template <typename T, int W, typename LD>
 __device__ __forceinline__ void gs_item(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x,
-                                        int KP, int G, long long t) {
+                                        int KP, int G, long long t, int skip = 0) {
   const int per = 32 * G;
   const long long r = t / per;
   if (r >= nRuns) return;
@@ -87,14 +87,15 @@ __device__ __forceinline__ void gs_item(const ColourRun* runs, int nRuns, const 
   Vec<T, W> acc;
 #pragma unroll
   for (int k = 0; k < W; k++) acc.v[k] = 0;
-  axpy(acc, c[0 * planeStride], LD::template ld<T, W>(x + (long long)(pp - 1) * KP + off));
-  axpy(acc, c[1 * planeStride], LD::template ld<T, W>(x + (long long)(pp)*KP + off));
-  axpy(acc, c[2 * planeStride], LD::template ld<T, W>(x + (long long)(pp + 1) * KP + off));
-  axpy(acc, c[3 * planeStride], LD::template ld<T, W>(x + (long long)(pos - 1) * KP + off));
-  axpy(acc, c[5 * planeStride], LD::template ld<T, W>(x + (long long)(pos + 1) * KP + off));
-  axpy(acc, c[6 * planeStride], LD::template ld<T, W>(x + (long long)(pn - 1) * KP + off));
-  axpy(acc, c[7 * planeStride], LD::template ld<T, W>(x + (long long)(pn)*KP + off));
-  axpy(acc, c[8 * planeStride], LD::template ld<T, W>(x + (long long)(pn + 1) * KP + off));
+  // skip: neighbour slots known to hold exact zeros (their terms add nothing)
+  if (!(skip & 1)) axpy(acc, c[0 * planeStride], LD::template ld<T, W>(x + (long long)(pp - 1) * KP + off));
+  if (!(skip & 2)) axpy(acc, c[1 * planeStride], LD::template ld<T, W>(x + (long long)(pp)*KP + off));
+  if (!(skip & 4)) axpy(acc, c[2 * planeStride], LD::template ld<T, W>(x + (long long)(pp + 1) * KP + off));
+  if (!(skip & 8)) axpy(acc, c[3 * planeStride], LD::template ld<T, W>(x + (long long)(pos - 1) * KP + off));
+  if (!(skip & 32)) axpy(acc, c[5 * planeStride], LD::template ld<T, W>(x + (long long)(pos + 1) * KP + off));
+  if (!(skip & 64)) axpy(acc, c[6 * planeStride], LD::template ld<T, W>(x + (long long)(pn - 1) * KP + off));
+  if (!(skip & 128)) axpy(acc, c[7 * planeStride], LD::template ld<T, W>(x + (long long)(pn)*KP + off));
+  if (!(skip & 256)) axpy(acc, c[8 * planeStride], LD::template ld<T, W>(x + (long long)(pn + 1) * KP + off));
   const T c4 = c[4 * planeStride];
   const Vec<T, W> b = LD::template ld<T, W>(rhs + (long long)pos * KP + off);
   Vec<T, W> out;

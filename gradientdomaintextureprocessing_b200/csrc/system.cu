@@ -143,7 +143,8 @@ DeviceSystem::DeviceSystem(const Hierarchy& h, const BoundaryElements& be, int d
 DeviceSystem::~DeviceSystem() {
   cudaSetDevice(device_);
   for (StepGraph& g : stepGraphs_) cudaGraphExecDestroy(g.exec);
-  if (profEv_[0]) { cudaEventDestroy(profEv_[0]); cudaEventDestroy(profEv_[1]); }
+  for (cudaEvent_t e : profEv_)
+    if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
   if (sumsHost_) cudaFreeHost(sumsHost_);
   if (barrierErrHost_) cudaFreeHost(barrierErrHost_);
@@ -696,8 +697,23 @@ bool DeviceSystem::barrier_ok(Multigrid<T>& mg) {
   return false;
 }
 
+// Neighbour slots (k = 3 (dy + 1) + dx + 1, centre 4 excluded) that a colour
+// pass of the first sweep from a zero iterate may skip: a neighbour is read
+// only when its colour comes earlier in the sweep (updated) -- later colours
+// and boundary texels still hold exact zeros, whose terms add nothing.
+static int zero_start_skip(int c) {
+  int skip = 0;
+  for (int k = 0; k < 9; k++) {
+    if (k == 4) continue;
+    const int dx = k % 3 - 1, dy = k / 3 - 1;
+    const int nc = c ^ ((dx != 0 ? 1 : 0) | (dy != 0 ? 2 : 0));
+    if (nc > c) skip |= 1 << k;
+  }
+  return skip;
+}
+
 template <typename T, int W>
-void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
+void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
   const int L = (int)mg.levels.size();
   const int KP = mg.KP;
   // levels [lc, L) run in the coarse-level cluster when it is enabled: from the
@@ -723,13 +739,22 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
     if (grouped(D, KP) && pre_sweeps(l) > 0) {
       dev::launch_gs_groups<T, W>(D, pre_sweeps(l), false, KP, s);
     } else {
+      // timed on level 0: every full sweep (all but a first sweep that skips
+      // zeros), here and in the post-smoothing; the sweep average is reported
+      const bool fromZero0 = zeroStart && knobs.zeroStartSkip && l == 0;
+      const int firstFull = fromZero0 ? 1 : 0;
+      if (profiling_ && l == 0) profSweeps_ = 0;
       for (int sw = 0; sw < pre_sweeps(l); sw++) {
-        const bool prof = profiling_ && l == 0 && sw == 0;
-        if (prof) cudaEventRecordWithFlags(profEv_[0], s, cudaEventRecordExternal);
+        const bool prof = profiling_ && l == 0;
+        if (prof && sw == firstFull) cudaEventRecordWithFlags(profEv_[0], s, cudaEventRecordExternal);
+        const bool fromZero = fromZero0 && sw == 0;
         for (int c = 0; c < 4; c++)
           dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP,
-                                      s);
-        if (prof) cudaEventRecordWithFlags(profEv_[1], s, cudaEventRecordExternal);
+                                      s, fromZero ? zero_start_skip(c) : 0);
+        if (prof && sw == pre_sweeps(l) - 1 && sw >= firstFull) {
+          cudaEventRecordWithFlags(profEv_[1], s, cudaEventRecordExternal);
+          profSweeps_ = pre_sweeps(l) - firstFull;
+        }
       }
     }
     dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
@@ -763,19 +788,26 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s) {
     if (grouped(D, KP) && post_sweeps(l) > 0) {
       dev::launch_gs_groups<T, W>(D, post_sweeps(l), true, KP, s);
     } else {
+      const bool prof = profiling_ && l == 0 && post_sweeps(l) > 0;
+      if (profiling_ && l == 0) profPostSweeps_ = 0;
+      if (prof) cudaEventRecordWithFlags(profEv_[2], s, cudaEventRecordExternal);
       for (int sw = 0; sw < post_sweeps(l); sw++)
         for (int c = 3; c >= 0; c--)
           dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP,
                                       s);
+      if (prof) {
+        cudaEventRecordWithFlags(profEv_[3], s, cudaEventRecordExternal);
+        profPostSweeps_ = post_sweeps(l);
+      }
     }
     trace_mark(L + 1 + (L - 2 - l), s);
   }
 }
 
-template void DeviceSystem::vcycle<float, 1>(Multigrid<float>&, cudaStream_t);
-template void DeviceSystem::vcycle<float, 4>(Multigrid<float>&, cudaStream_t);
-template void DeviceSystem::vcycle<double, 1>(Multigrid<double>&, cudaStream_t);
-template void DeviceSystem::vcycle<double, 4>(Multigrid<double>&, cudaStream_t);
+template void DeviceSystem::vcycle<float, 1>(Multigrid<float>&, cudaStream_t, bool);
+template void DeviceSystem::vcycle<float, 4>(Multigrid<float>&, cudaStream_t, bool);
+template void DeviceSystem::vcycle<double, 1>(Multigrid<double>&, cudaStream_t, bool);
+template void DeviceSystem::vcycle<double, 4>(Multigrid<double>&, cudaStream_t, bool);
 
 // ----------------------------------------------------------------------------
 // solve work and drivers
@@ -905,7 +937,7 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
       // D0.x (the correction) is zero on entry: cleared before the first step
       // and by the correction update of every step
       LevelDev<float>& D0 = mg.levels[0];
-      if (mg.KP == 1) vcycle<float, 1>(mg, s); else vcycle<float, 4>(mg, s);
+      if (mg.KP == 1) vcycle<float, 1>(mg, s, true); else vcycle<float, 4>(mg, s, true);
       dev::launch_add_correction<float>(X, D0.x, (long long)n, k, mg.KP, s, frozen_);
       // r = b - A x, written straight into the FP32 right-hand side of the next V-cycle
       dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
@@ -984,8 +1016,7 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
 // outside any capture
 bool DeviceSystem::prepare_timing(const Multigrid<float>& mg) {
   if (!profEv_[0]) {
-    cudaEventCreate(&profEv_[0]);
-    cudaEventCreate(&profEv_[1]);
+    for (cudaEvent_t& e : profEv_) cudaEventCreate(&e);
   }
   if (knobs.traceLevels && !timeline_) {
     timeline_ = static_cast<unsigned long long*>(rawArena_.alloc(1024 * sizeof(unsigned long long)));
@@ -1032,14 +1063,17 @@ void DeviceSystem::collect_timing(const Multigrid<float>& mg) {
       cudaGetLastError();
     }
   }
-  float pm = 0;
-  if (cudaEventElapsedTime(&pm, profEv_[0], profEv_[1]) == cudaSuccess) {
+  // average full level-0 sweep of this V-cycle (pre-smoothing and post-smoothing)
+  float pre = 0, post = 0;
+  const bool okPre = profSweeps_ > 0 && cudaEventElapsedTime(&pre, profEv_[0], profEv_[1]) == cudaSuccess;
+  const bool okPost = profPostSweeps_ > 0 && cudaEventElapsedTime(&post, profEv_[2], profEv_[3]) == cudaSuccess;
+  const int sweeps = (okPre ? profSweeps_ : 0) + (okPost ? profPostSweeps_ : 0);
+  if (sweeps > 0) {
     profCount += 1;
-    profMs += pm;
+    profMs += ((okPre ? pre : 0.f) + (okPost ? post : 0.f)) / sweeps;
     profTexels = mg.levels[0].nDeep;
-  } else {
-    cudaGetLastError();  // timing unavailable: do not leave the error for the next caller
   }
+  cudaGetLastError();  // a missing timing leaves no error for the next caller
 }
 
 bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X, int k, double tol, int maxIters, cudaStream_t s,
@@ -1105,7 +1139,7 @@ bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X
     if (!prepare_timing(mg)) return false;
     profiling_ = true;
     if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
-    if (KP == 1) vcycle<float, 1>(mg, s); else vcycle<float, 4>(mg, s);
+    if (KP == 1) vcycle<float, 1>(mg, s, true); else vcycle<float, 4>(mg, s, true);
     profiling_ = false;
     dev::launch_fcg_precond((long long)n, k, KP, D0.x, r64_, q_, z_, partials_, sums_, sc_, s);
     dev::launch_fcg_direction((long long)n, k, z_, sc_, p_, s);
@@ -1239,7 +1273,7 @@ bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, int k, doubl
     if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
     dev::launch_pack_rhs<double>(r64_, D0.b, (long long)n, k, mg.KP, s);
     cudaMemsetAsync(D0.x, 0, n * mg.KP * sizeof(double), s);
-    if (mg.KP == 1) vcycle<double, 1>(mg, s); else vcycle<double, 4>(mg, s);
+    if (mg.KP == 1) vcycle<double, 1>(mg, s, true); else vcycle<double, 4>(mg, s, true);
     dev::launch_add_correction<double>(x64_, D0.x, (long long)n, k, mg.KP, s);
     raw_apply_dev(rawA_, b64_, x64_, r64_, k, 0, s, nullptr);
     if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;

@@ -110,6 +110,7 @@ struct SolverKnobs {
   int coarsePreSweeps = 0, coarsePostSweeps = 3;  // sweeps on levels >= coarseFrom (-1: as level 0)
   int coarseFrom = 1;
   int krylov = 0;                       // 1: flexible CG around the V-cycle instead of plain refinement
+  int zeroStartSkip = 1;                // first sweep from a zero correction skips the zero neighbours
 };
 
 struct SolveReport {
@@ -166,8 +167,8 @@ class DeviceSystem {
   size_t deviceBytes() const;
   // knobs that change the launch sequence take effect on the next solve
   void invalidate_graph();
-  // live timing of the level-0 pre-smoothing colour passes inside the captured
-  // refinement graph: {launch groups timed, total ms, texels updated per group}
+  // live timing of the level-0 colour sweeps inside the captured step graphs:
+  // {V-cycles timed, sum of their average full-sweep ms, deep texels per sweep}
   double profCount = 0, profMs = 0, profTexels = 0;
   // level trace (knob traceLevels): refinement steps timed, then per level l the
   // summed ms of its down leg (smoothing, residual, restriction), the coarse
@@ -194,7 +195,9 @@ class DeviceSystem {
   template <typename T>
   bool build_multigrid(Multigrid<T>& mg, int KP);
   template <typename T, int W>
-  void vcycle(Multigrid<T>& mg, cudaStream_t s);
+  // zeroStart: the level-0 iterate is zero on entry (a correction), so the
+  // first sweep skips the neighbours it has not updated yet (exact zeros)
+  void vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart = false);
   bool ensure_work(int k);
   bool prepare_timing(const Multigrid<float>& mg);
   void collect_timing(const Multigrid<float>& mg);
@@ -259,7 +262,8 @@ class DeviceSystem {
   // the cached graph for this step (moved to the back), or null
   cudaGraphExec_t find_graph(int kind, int k, const double* b, const double* x);
   void add_graph(const StepGraph& g);
-  cudaEvent_t profEv_[2] = {nullptr, nullptr};
+  cudaEvent_t profEv_[4] = {nullptr, nullptr, nullptr, nullptr};  // level-0 full pre sweeps, post sweeps
+  int profSweeps_ = 0, profPostSweeps_ = 0;
   std::vector<cudaEvent_t> traceEv_;   // 2 L markers of the captured V-cycle (traceLevels)
   void trace_mark(int i, cudaStream_t s);
   unsigned long long* timeline_ = nullptr;  // cluster phase timeline (traceLevels)

@@ -191,7 +191,9 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * "profile.cluster"), "krylov" (0/1, default 0: flexible preconditioned
  * conjugate gradients in FP64 around the FP32 V-cycle instead of plain
  * iterative refinement; for slowly contracting V-cycles, e.g. strongly
- * anisotropic metrics). */
+ * anisotropic metrics), "zero_start_skip" (0/1, default 1: the first level-0
+ * sweep of a V-cycle on a zero correction reads only the neighbours it has
+ * already updated; same results). */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
 int gdtp_system_get(const gdtp_system* s, const char* knob, double* value);
 /* Autotuner: times complete solves of b (host float64 numTexels*k, uploaded

@@ -258,3 +258,19 @@ def test_reweighting_keeps_memory_and_results(setup):
     s.update(lam, 1.0)
     x1, _ = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
     np.testing.assert_array_equal(x1, x0)
+
+
+def test_zero_start_skip_is_exact(setup):
+    """The first level-0 sweep of each V-cycle starts from a zero correction and
+    skips the neighbours that still hold zeros: the solution is bitwise the one
+    of the full sweep."""
+    g, _, s = setup
+    b = g["solve/rhs"]
+    s.set("zero_start_skip", 0)
+    try:
+        x_full, r_full = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
+    finally:
+        s.set("zero_start_skip", 1)
+    x_skip, r_skip = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
+    assert r_skip["iterations"] == r_full["iterations"]
+    np.testing.assert_array_equal(x_skip, x_full)
