@@ -757,8 +757,13 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
         }
       }
     }
-    dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
-    dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, D.r, C.b, C.x, C.n, KP, s);
+    // a level entered with a zero iterate and left unsmoothed (no pre-sweeps, no
+    // boundary solve) has residual b - A 0 = b exactly: restrict b itself
+    const bool unsmoothed = knobs.zeroStartSkip && (l > 0 || zeroStart) && pre_sweeps(l) == 0 && !knobs.preBoundary;
+    if (!unsmoothed)
+      dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
+    dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, unsmoothed ? D.b : D.r, C.b, C.x, C.n, KP,
+                               s);
     trace_mark(l + 1, s);
   }
   if (lc < L - 1) {

@@ -193,7 +193,8 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * iterative refinement; for slowly contracting V-cycles, e.g. strongly
  * anisotropic metrics), "zero_start_skip" (0/1, default 1: the first level-0
  * sweep of a V-cycle on a zero correction reads only the neighbours it has
- * already updated; same results). */
+ * already updated, and a level entered with a zero iterate and no
+ * pre-smoothing restricts its right-hand side as its residual; same results). */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
 int gdtp_system_get(const gdtp_system* s, const char* knob, double* value);
 /* Autotuner: times complete solves of b (host float64 numTexels*k, uploaded

@@ -262,8 +262,9 @@ def test_reweighting_keeps_memory_and_results(setup):
 
 def test_zero_start_skip_is_exact(setup):
     """The first level-0 sweep of each V-cycle starts from a zero correction and
-    skips the neighbours that still hold zeros: the solution is bitwise the one
-    of the full sweep."""
+    skips the neighbours that still hold zeros, and the unsmoothed coarse levels
+    restrict their right-hand side as their residual: the solution is bitwise
+    the one of the full computation."""
     g, _, s = setup
     b = g["solve/rhs"]
     s.set("zero_start_skip", 0)
