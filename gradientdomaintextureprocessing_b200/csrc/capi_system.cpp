@@ -2,6 +2,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "gdtp.h"
 #include "capi_internal.h"
@@ -167,6 +168,23 @@ extern "C" int gdtp_solve_ex(gdtp_system* s, const double* b, double* x, int k, 
     return sys_fail(s, GDTP_ERR_CUDA);
   fill_report(report, rep);
   return rep.relMax <= tol ? GDTP_OK : fail(GDTP_ERR_NOT_CONVERGED, "relative residual above tolerance after max_iters");
+}
+
+extern "C" int gdtp_solve_stream(gdtp_system* s, const double* const* b, double* const* x, int count, int k, double tol, int max_iters,
+                                 gdtp_report* reports) {
+  GDTP_SYS_CHECK(s);
+  if (count < 0 || (count > 0 && (!b || !x)) || !(tol > 0) || max_iters < 0)
+    return fail(GDTP_ERR_INVALID, "gdtp_solve_stream: bad arguments");
+  for (int i = 0; i < count; i++)
+    if (!b[i] || !x[i]) return fail(GDTP_ERR_INVALID, "gdtp_solve_stream: null vector");
+  std::vector<SolveReport> reps(count);
+  if (!s->sys->solve_stream(b, x, count, k, tol, max_iters, reps.data())) return sys_fail(s, GDTP_ERR_CUDA);
+  bool converged = true;
+  for (int i = 0; i < count; i++) {
+    if (reports) fill_report(reports + i, reps[i]);
+    converged = converged && reps[i].relMax <= tol;
+  }
+  return converged ? GDTP_OK : fail(GDTP_ERR_NOT_CONVERGED, "relative residual above tolerance after max_iters");
 }
 
 extern "C" int gdtp_solve_device(gdtp_system* s, const double* b_dev, double* x_dev, int k, double tol, int max_iters, void* stream,

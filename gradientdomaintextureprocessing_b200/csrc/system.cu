@@ -148,6 +148,11 @@ DeviceSystem::~DeviceSystem() {
   for (cudaEvent_t e : traceEv_) cudaEventDestroy(e);
   if (sumsHost_) cudaFreeHost(sumsHost_);
   if (barrierErrHost_) cudaFreeHost(barrierErrHost_);
+  for (int j = 0; j < 2; j++)
+    for (cudaEvent_t e : {slotIn_[j], slotSolved_[j], slotOut_[j]})
+      if (e) cudaEventDestroy(e);
+  if (copyIn_) cudaStreamDestroy(copyIn_);
+  if (copyOut_) cudaStreamDestroy(copyOut_);
   mg32_.clear();
   mg64_.reset();
   if (stream_) cudaStreamDestroy(stream_);
@@ -196,7 +201,7 @@ bool DeviceSystem::check(cudaError_t e, const char* what) {
 }
 
 size_t DeviceSystem::deviceBytes() const {
-  size_t b = rawArena_.total + rawAArena_.total + workArena_.total;
+  size_t b = rawArena_.total + rawAArena_.total + workArena_.total + slotArena_.total;
   for (const auto& m : mg32_) b += m->arena.total;
   if (mg64_) b += mg64_->arena.total;
   return b;
@@ -1015,6 +1020,68 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
   rep.relMax = rm;
   rep.seconds = ms * 1e-3;
   return true;
+}
+
+// Problem i runs on slot i % 2.  Order of the work on the three streams:
+//   copyIn:  b[i] -> slot            after problem i-2 (same slot) has finished
+//   solve:   waits for b[i] and for the download of x[i-2] (same slot)
+//   copyOut: slot -> x[i]            after problem i has finished
+// so the upload of b[i+1] and the download of x[i-1] overlap solve i.  The
+// solves are those of solve_mixed on device buffers, unchanged.
+bool DeviceSystem::solve_stream(const double* const* b_host, double* const* x_host, int count, int k, double tol, int maxIters,
+                                SolveReport* reps) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (!updated_) { err_ = "solve before update"; return false; }
+  if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
+  if (count <= 0) return true;
+  if (!copyIn_) {
+    if (!check(cudaStreamCreateWithFlags(&copyIn_, cudaStreamNonBlocking), "copy stream") ||
+        !check(cudaStreamCreateWithFlags(&copyOut_, cudaStreamNonBlocking), "copy stream"))
+      return false;
+    for (int j = 0; j < 2; j++)
+      for (cudaEvent_t* e : {&slotIn_[j], &slotSolved_[j], &slotOut_[j]})
+        if (!check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "copy event")) return false;
+  }
+  const size_t n = h_.levels[0].numTexels, bytes = n * size_t(k) * sizeof(double);
+  if (k > slotK_) {
+    const int kc = k_capacity(k);
+    slotArena_ = DeviceArena();
+    slotK_ = 0;
+    for (int j = 0; j < 2; j++) {
+      slotB_[j] = static_cast<double*>(slotArena_.alloc(n * size_t(kc) * sizeof(double)));
+      if (!slotB_[j]) return check(slotArena_.last, "slot buffers");
+      slotX_[j] = static_cast<double*>(slotArena_.alloc(n * size_t(kc) * sizeof(double)));
+      if (!slotX_[j]) return check(slotArena_.last, "slot buffers");
+    }
+    slotK_ = kc;
+    invalidate_graph();  // graphs of freed slots must not match new ones at the same address
+  }
+  // every copy issued here has finished when this returns, on success or not
+  auto drain = [&]() {
+    cudaStreamSynchronize(copyIn_);
+    cudaStreamSynchronize(copyOut_);
+  };
+  auto upload = [&](int i) {
+    const int sl = i & 1;
+    if (i >= 2 && !check(cudaStreamWaitEvent(copyIn_, slotSolved_[sl], 0), "copy order")) return false;
+    return check(cudaMemcpyAsync(slotB_[sl], b_host[i], bytes, cudaMemcpyHostToDevice, copyIn_), "h2d b") &&
+           check(cudaEventRecord(slotIn_[sl], copyIn_), "copy event");
+  };
+  for (int i = 0; i < std::min(count, 2); i++)
+    if (!upload(i)) { drain(); return false; }
+  for (int i = 0; i < count; i++) {
+    const int sl = i & 1;
+    bool ok = check(cudaStreamWaitEvent(stream_, slotIn_[sl], 0), "copy order") &&
+              (i < 2 || check(cudaStreamWaitEvent(stream_, slotOut_[sl], 0), "copy order")) &&
+              solve_mixed(nullptr, nullptr, slotB_[sl], slotX_[sl], k, tol, maxIters, nullptr, reps[i], true) &&
+              check(cudaEventRecord(slotSolved_[sl], stream_), "copy event") &&
+              check(cudaStreamWaitEvent(copyOut_, slotSolved_[sl], 0), "copy order") &&
+              check(cudaMemcpyAsync(x_host[i], slotX_[sl], bytes, cudaMemcpyDeviceToHost, copyOut_), "d2h x") &&
+              check(cudaEventRecord(slotOut_[sl], copyOut_), "copy event") && (i + 2 >= count || upload(i + 2));
+    if (!ok) { drain(); return false; }
+  }
+  return check(cudaStreamSynchronize(copyOut_), "d2h x") && check(cudaStreamSynchronize(copyIn_), "h2d b");
 }
 
 // events for the level-0 sweep timing (and the per-level trace), created

@@ -146,6 +146,11 @@ class DeviceSystem {
   bool solve_mixed(const double* b_host, double* x_host, const double* b_dev, double* x_dev, int k, double tol, int maxIters,
                    cudaStream_t userStream, SolveReport& rep, bool zeroGuess = false);
   bool solve_fp64(const double* b_host, double* x_host, int k, double tol, int maxIters, SolveReport& rep);
+  // count independent problems from host buffers, each from a zero guess: the
+  // upload of b[i+1] and the download of x[i-1] run on two copy streams while
+  // problem i is solved; returns once every x[i] is written
+  bool solve_stream(const double* const* b_host, double* const* x_host, int count, int k, double tol, int maxIters,
+                    SolveReport* reps);
   bool vcycle_host(float* x, const float* rhs, int k);
   // times full solves of b (host, n x k) for a grid of smoother settings and
   // keeps the fastest that converges; returns the chosen knobs
@@ -248,6 +253,13 @@ class DeviceSystem {
   int workK_ = 0;
   double *b64_ = nullptr, *x64_ = nullptr, *r64_ = nullptr, *partials_ = nullptr, *sums_ = nullptr;
   double* sumsHost_ = nullptr;  // pinned
+  // solve_stream: two slots of device b / x (n x k FP64), alternating between
+  // problems, and the streams and events that order the copies around the solves
+  DeviceArena slotArena_;
+  int slotK_ = 0;
+  double *slotB_[2] = {nullptr, nullptr}, *slotX_[2] = {nullptr, nullptr};
+  cudaStream_t copyIn_ = nullptr, copyOut_ = nullptr;
+  cudaEvent_t slotIn_[2] = {}, slotSolved_[2] = {}, slotOut_[2] = {};
   // captured step graphs (refinement or flexible-CG step), one per right-hand
   // side count and buffers, most recently used last: a server batching
   // requests of varying sizes reuses them instead of capturing again

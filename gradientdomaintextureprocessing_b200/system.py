@@ -143,6 +143,33 @@ class System:
         return x, {"iterations": rep.iterations, "vcycles": rep.vcycles, "rel_residual_max": rep.rel_residual_max,
                    "seconds": rep.seconds, "converged": code == 0}
 
+    def solve_stream(self, bs, xs=None, tol: float = 1e-6, max_iters: int = 60, check: bool = True):
+        """Solve a sequence of problems (each from a zero guess) through
+        gdtp_solve_stream: the upload of the next right-hand side and the
+        download of the previous solution overlap each solve.  bs: arrays of
+        the same shape (numTexels[, k]); xs: optional output arrays of that
+        shape (pinned host memory, e.g. a pinned torch tensor's numpy view,
+        gives the overlap).  Returns (xs, reports)."""
+        vecs = [self._vec(b, np.float64) for b in bs]
+        if len({(v.shape, k) for v, k in vecs}) > 1:
+            raise ValueError("solve_stream: right-hand sides of different shapes")
+        k = vecs[0][1] if vecs else 1
+        if xs is None:
+            xs = [np.zeros_like(v) for v, _ in vecs]
+        if len(xs) != len(vecs) or any(x.size != v.size or x.dtype != np.float64 or not x.flags.c_contiguous
+                                       for x, (v, _) in zip(xs, vecs)):
+            raise ValueError("solve_stream: outputs must be C-contiguous float64 arrays sized as the right-hand sides")
+        n = len(vecs)
+        bp = (C.c_void_p * max(n, 1))(*[v.ctypes.data for v, _ in vecs])
+        xp = (C.c_void_p * max(n, 1))(*[x.ctypes.data for x in xs])
+        reps = (_lib.Report * max(n, 1))()
+        code = _lib.lib().gdtp_solve_stream(self._s, bp, xp, n, k, float(tol), int(max_iters), reps)
+        if code != 0 and (check or code != -4):
+            _lib.check(code)
+        out = [{"iterations": r.iterations, "vcycles": r.vcycles, "rel_residual_max": r.rel_residual_max, "seconds": r.seconds,
+                "converged": r.rel_residual_max <= tol} for r in reps[:n]]
+        return xs, out
+
 
 def InitializeMassAndStiffness(hierarchy: Hierarchy, device: int = 0, parameter_metric=None) -> System:
     return System(hierarchy, device=device, parameter_metric=parameter_metric)

@@ -144,6 +144,19 @@ int gdtp_solve(gdtp_system* s, const double* b, double* x, int k, double tol, in
  * output only (no host-to-device copy of x). */
 #define GDTP_ZERO_GUESS 1
 int gdtp_solve_ex(gdtp_system* s, const double* b, double* x, int k, double tol, int max_iters, int flags, gdtp_report* report);
+/* count independent problems, each solved as gdtp_solve_ex with GDTP_ZERO_GUESS:
+ * b[i] (input) and x[i] (output) host float64 numTexels*k, all k the same.
+ * The upload of b[i+1] and the download of x[i-1] run on two copy streams
+ * while problem i is solved, so a sequence of problems (frames of a filtering
+ * session, a queue of requests) costs about the solves alone.  Pinned host
+ * buffers (cudaMallocHost / cudaHostRegister) give the overlap; pageable ones
+ * give the same results with the copies serialised.  No x[i] may overlap a
+ * b[j].  reports: count entries, or NULL.  Returns after every x[i] is
+ * written; GDTP_ERR_NOT_CONVERGED if any problem stopped above tol (its x is
+ * still written).  No counterpart in the reference, which solves one problem
+ * per call (TextureFiltering.cpp:562-579). */
+int gdtp_solve_stream(gdtp_system* s, const double* const* b, double* const* x, int count, int k, double tol, int max_iters,
+                      gdtp_report* reports);
 /* Same on device float64 buffers (no host copies); stream = cudaStream_t or NULL. */
 int gdtp_solve_device(gdtp_system* s, const double* b_dev, double* x_dev, int k, double tol, int max_iters,
                       void* stream, gdtp_report* report);

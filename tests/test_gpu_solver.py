@@ -275,3 +275,26 @@ def test_zero_start_skip_is_exact(setup):
     x_skip, r_skip = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
     assert r_skip["iterations"] == r_full["iterations"]
     np.testing.assert_array_equal(x_skip, x_full)
+
+
+def test_solve_stream_matches_single_solves(setup):
+    """gdtp_solve_stream solves each problem of a sequence as gdtp_solve from a
+    zero guess (two device slots alternate, copies on their own streams):
+    bitwise the same solutions and reports.  One right-hand side first, then
+    three (the slots grow), an odd count so that both slots are reused."""
+    g, _, s = setup
+    b = g["solve/rhs"]
+    singles = [b[:, 0]]
+    xs, reps = s.solve_stream(singles, tol=1e-8, max_iters=MAX_ITERS)
+    x1, r1 = s.solve(b[:, 0], tol=1e-8, max_iters=MAX_ITERS)
+    np.testing.assert_array_equal(xs[0], x1)
+    assert reps[0]["iterations"] == r1["iterations"] and reps[0]["converged"]
+    problems = [b, 2.0 * b, np.ascontiguousarray(b[:, ::-1]), b - 0.5 * b[:, ::-1], b]
+    xs, reps = s.solve_stream(problems, tol=1e-8, max_iters=MAX_ITERS)
+    assert len(xs) == len(problems)
+    for p, x, r in zip(problems, xs, reps):
+        xr, rr = s.solve(p, tol=1e-8, max_iters=MAX_ITERS)
+        np.testing.assert_array_equal(x, xr)
+        assert r["iterations"] == rr["iterations"] and r["converged"]
+        assert r["rel_residual_max"] == rr["rel_residual_max"]
+    assert s.solve_stream([], tol=1e-8)[0] == []
