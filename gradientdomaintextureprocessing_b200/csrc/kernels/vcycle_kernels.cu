@@ -441,6 +441,22 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
   block_partials(rr, bb, G, K, partials);
 }
 
+// Small exchanges of the solve loops with the host, kept off the copy engines
+// (which a streaming solve keeps busy with whole vectors): the norms are
+// written into mapped pinned host memory, the per-right-hand-side flags come
+// in as a kernel argument.  One block each.
+__global__ void k_copy_f64(double* __restrict__ dst, const double* __restrict__ src, int n) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+__global__ void k_set_flags(int* __restrict__ flags, unsigned long long mask, int k) {
+  grid_dependency_wait();
+  grid_launch_dependents();
+  const int c = threadIdx.x;
+  if (c < k) flags[c] = int((mask >> c) & 1ull);
+}
+
 // Sum of per-block partials in a fixed order (one block): sums[2K]
 __global__ void k_sum_partials(const double* __restrict__ partials, int nBlocks, int K, double* __restrict__ sums) {
   grid_dependency_wait();
@@ -761,6 +777,10 @@ void launch_axpby(double* out, double a, const double* x, double b, const double
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s) {
   launch(k_pack_rhs<T>, dim3(nblk(n * KP)), s, r, rhs, n, K, KP);
+}
+void launch_copy_f64(double* dst, const double* src, int n, cudaStream_t s) { launch(k_copy_f64, dim3(1), s, dst, src, n); }
+void launch_set_flags(int* flags, unsigned long long mask, int k, cudaStream_t s) {
+  launch(k_set_flags, dim3(1), s, flags, mask, k);
 }
 template <typename T>
 void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStream_t s, const int* frozen) {

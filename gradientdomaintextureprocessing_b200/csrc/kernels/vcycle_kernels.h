@@ -109,6 +109,10 @@ void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coe
                              float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s);
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s);
+// n doubles (n <= a few hundred) by one block, e.g. into mapped pinned host memory
+void launch_copy_f64(double* dst, const double* src, int n, cudaStream_t s);
+// flags[c] = bit c of mask, c < k <= 64
+void launch_set_flags(int* flags, unsigned long long mask, int k, cudaStream_t s);
 // Flexible preconditioned CG around the FP32 V-cycle (vcycle_kernels.cu).  sc: 4K
 // per-RHS scalars {alpha, beta, rho, rho_old}; sums: 2K.
 //   precond:   z = e (e cleared), rho = z.r, beta = -alpha_old (z.q_old) / rho_old

@@ -836,11 +836,36 @@ bool DeviceSystem::ensure_work(int kk) {
   frozenHost_.assign(k, 0);
   sums_ = workArena_.zeros<double>(2 * size_t(k));
   if (sumsHost_) cudaFreeHost(sumsHost_);
-  if (!check(cudaMallocHost(&sumsHost_, 2 * size_t(k) * sizeof(double)), "cudaMallocHost")) return false;
+  sumsMapped_ = nullptr;
+  if (!check(cudaHostAlloc(&sumsHost_, 2 * size_t(k) * sizeof(double), cudaHostAllocMapped), "cudaHostAlloc")) return false;
+  if (cudaHostGetDevicePointer(&sumsMapped_, sumsHost_, 0) != cudaSuccess) {
+    sumsMapped_ = nullptr;
+    cudaGetLastError();  // not mappable here: the norms come back by copy
+  }
   if (!check(workArena_.last, "work allocation")) return false;
   workK_ = k;
   invalidate_graph();
   return true;
+}
+
+bool DeviceSystem::read_norms(int k, cudaStream_t s, const char* what) {
+  if (sumsMapped_) {
+    kernelLaunches += 1;
+    dev::launch_copy_f64(sumsMapped_, sums_, 2 * k, s);
+    if (!check(cudaGetLastError(), "norms to host")) return false;
+  } else if (!check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms")) {
+    return false;
+  }
+  return check(cudaStreamSynchronize(s), what);
+}
+
+bool DeviceSystem::upload_flags(int k, cudaStream_t s) {
+  unsigned long long mask = 0;
+  for (int c = 0; c < k; c++)
+    if (frozenHost_[c] == 1) mask |= 1ull << c;
+  kernelLaunches += 1;
+  dev::launch_set_flags(frozen_, mask, k, s);
+  return check(cudaGetLastError(), "frozen flags");
 }
 
 bool DeviceSystem::raw_apply_dev(const RawOperator& op, const double* b, const double* x, double* out, int k, int mode,
@@ -969,9 +994,7 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
     kernelLaunches += 2;  // operator + norm reduction
     dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
                                  rawA_.bGlobal, rawA_.nB, B, X, mg.levels[0].b, k, mg.KP, partials_, sums_, s);
-    if (!check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
-        !check(cudaStreamSynchronize(s), "initial residual"))
-      return false;
+    if (!read_norms(k, s, "initial residual")) return false;
     rep = SolveReport();
     rep.rel.assign(k, 0.0);
     auto rel_max = [&]() {
@@ -990,16 +1013,13 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
         const int f = rep.rel[c] <= tol ? 1 : 0;
         if (f != frozenHost_[c]) { frozenHost_[c] = f; changed = true; }
       }
-      return !changed || check(cudaMemcpyAsync(frozen_, frozenHost_.data(), k * sizeof(int), cudaMemcpyHostToDevice, s), "frozen flags");
+      return !changed || upload_flags(k, s);
     };
     for (int c = 0; c < k; c++) frozenHost_[c] = 2;  // not a flag value: forces the first upload
     if (!update_frozen()) return false;
     while (rm > tol && it < maxIters) {
       kernelLaunches += graphKernels;
-      if (!check(cudaGraphLaunch(iterGraph, s), "graph launch") ||
-          !check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
-          !check(cudaStreamSynchronize(s), "refinement step"))
-        return false;
+      if (!check(cudaGraphLaunch(iterGraph, s), "graph launch") || !read_norms(k, s, "refinement step")) return false;
       it++;
       rm = rel_max();
       if (rm > tol && !update_frozen()) return false;
@@ -1176,10 +1196,7 @@ bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X
     }
     return m;
   };
-  auto fetch = [&](const char* what) {
-    return check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") &&
-           check(cudaStreamSynchronize(s), what);
-  };
+  auto fetch = [&](const char* what) { return read_norms(k, s, what); };
   // r = b - A x with the FP64 operator
   auto true_residual = [&]() {
     kernelLaunches += 2;  // operator + norm reduction
@@ -1203,7 +1220,7 @@ bool DeviceSystem::krylov_solve(Multigrid<float>& mg, const double* B, double* X
       const int f = rep.rel[c] <= tol ? 1 : 0;
       if (f != frozenHost_[c]) { frozenHost_[c] = f; changed = true; }
     }
-    return !changed || check(cudaMemcpyAsync(frozen_, frozenHost_.data(), k * sizeof(int), cudaMemcpyHostToDevice, s), "frozen flags");
+    return !changed || upload_flags(k, s);
   };
   cudaGraphExec_t krylovGraph = find_graph(1, k, nullptr, X);
   if (!krylovGraph) {

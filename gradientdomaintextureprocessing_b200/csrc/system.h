@@ -252,7 +252,12 @@ class DeviceSystem {
   DeviceArena workArena_;
   int workK_ = 0;
   double *b64_ = nullptr, *x64_ = nullptr, *r64_ = nullptr, *partials_ = nullptr, *sums_ = nullptr;
-  double* sumsHost_ = nullptr;  // pinned
+  double* sumsHost_ = nullptr;    // pinned, mapped
+  double* sumsMapped_ = nullptr;  // its device address (null: norms come back by copy)
+  // the solve loops' small host exchanges, by kernel: norms sums_ -> sumsHost_
+  // (then waits for the stream), flags frozenHost_ -> frozen_
+  bool read_norms(int k, cudaStream_t s, const char* what);
+  bool upload_flags(int k, cudaStream_t s);
   // solve_stream: two slots of device b / x (n x k FP64), alternating between
   // problems, and the streams and events that order the copies around the solves
   DeviceArena slotArena_;
