@@ -11,8 +11,10 @@ One step = one solve of all 3 right-hand sides from x = 0 to relative residual
 
   value  Mtexels/s = texels x RHS / solve time / 1e6, inputs resident in HBM
          (device API gdtp_solve_device), device-timed with CUDA events.
-  e2e    same through the host API gdtp_solve with pinned host buffers
-         (H2D of b and x0, D2H of x inside every step).
+  e2e    same through the host API with pinned host buffers: gdtp_solve_stream
+         over the timed steps (H2D of b and D2H of x inside every step, on
+         copy streams that overlap the neighbouring steps' solves);
+         e2e.single_call is one gdtp_solve_ex per step, copies in series.
   --impl reference: the reference's own CPU solver (oracle/_ref/gdtp_ref: the
          reference headers compiled unmodified) on the host cores, same mesh,
          texture, operator and tolerance; its V-cycles are timed.
