@@ -31,3 +31,19 @@ def test_errors_are_reported_not_raised(built_lib):
     h = C.c_void_p()
     code = L.gdtp_hierarchy_build(None, 0, None, 0, None, 0, 0, 0, None, C.byref(h))
     assert code == -1 and b"invalid" in L.gdtp_last_error()
+
+
+def test_solve_entry_points_reject_a_null_system(built_lib):
+    """Every solve entry point checks its handle before touching the device (no GPU needed)."""
+    import ctypes as C
+    from gradientdomaintextureprocessing_b200 import _lib
+    L = _lib.lib()
+    rep = _lib.Report()
+    b = (C.c_double * 4)()
+    x = (C.c_double * 4)()
+    bp = (C.c_void_p * 1)(C.cast(b, C.c_void_p))
+    xp = (C.c_void_p * 1)(C.cast(x, C.c_void_p))
+    assert L.gdtp_solve(None, b, x, 1, 1e-6, 10, C.byref(rep)) == -1
+    assert L.gdtp_solve_ex(None, b, x, 1, 1e-6, 10, 1, C.byref(rep)) == -1
+    assert L.gdtp_solve_stream(None, bp, xp, 1, 1, 1e-6, 10, None) == -1
+    assert b"null system handle" in L.gdtp_last_error()
