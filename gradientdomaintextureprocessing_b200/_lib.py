@@ -60,6 +60,16 @@ _SIGS = {
     "gdtp_system_autotune": (C.c_int, [_P, _P, C.c_int, C.c_double, _P]),
     "gdtp_residual_static": (C.c_int, [_P, _P, _P, _P, C.c_int, _P, _P]),
     "gdtp_system_device_bytes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "gdtp_read_textured_mesh": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), _P, _P, _P]),
+    "gdtp_textured_mesh_texture_file": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int64)]),
+    "gdtp_write_textured_mesh": (C.c_int, [C.c_char_p, _P, C.c_int64, _P, C.c_int64, _P, C.c_char_p]),
+    "gdtp_read_image": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _P]),
+    "gdtp_write_image": (C.c_int, [C.c_char_p, _P, C.c_int, C.c_int]),
+    "gdtp_read_vector": (C.c_int, [C.c_char_p, C.c_int64, C.POINTER(C.c_int64), _P]),
+    "gdtp_write_vector": (C.c_int, [C.c_char_p, C.c_int64, C.c_int64, _P]),
+    "gdtp_compute_padding": (C.c_int, [C.c_int, C.c_int, _P, C.c_int64, _P]),
+    "gdtp_pad_texture_coordinates": (C.c_int, [_P, C.c_int, C.c_int, _P, C.c_int64, C.c_int]),
+    "gdtp_pad_image": (C.c_int, [_P, _P, C.c_int, C.c_int, _P, C.c_int]),
     "gdtp_server_create": (C.c_int, [C.c_int, C.c_int64, C.c_int, C.POINTER(_P)]),
     "gdtp_server_free": (None, [_P]),
     "gdtp_server_add_model": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
@@ -107,7 +117,7 @@ def lib():
 
 def check(code: int) -> None:
     if code != GDTP_OK:
-        raise GDTPError(code, lib().gdtp_last_error().decode())
+        raise GDTPError(code, lib().gdtp_last_error().decode(errors="replace"))
 
 
 def ptr(a: np.ndarray | None):

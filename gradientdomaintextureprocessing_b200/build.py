@@ -22,7 +22,7 @@ BUILD = os.path.join(ROOT, "_build")
 
 SOURCES = [
     "setup/atlas.cpp", "setup/grid.cpp", "setup/csr.cpp", "setup/boundary.cpp", "setup/assembly.cpp",
-    "setup/galerkin.cpp", "setup/bsolve.cpp", "setup/metric.cpp",
+    "setup/galerkin.cpp", "setup/bsolve.cpp", "setup/metric.cpp", "io/png.cpp", "io/ply.cpp", "io/texture_io.cpp", "capi_io.cpp",
     "capi_hierarchy.cpp", "capi_system.cpp", "capi_metric.cpp", "capi_geodesics.cpp", "geodesics.cu", "capi_server.cpp", "server.cpp", "system.cu", "noalloc.cu",
     "kernels/vcycle_kernels.cu", "kernels/coarse_cycle.cu", "kernels/geodesic_kernels.cu", "kernels/assembly_kernels.cu",
 ]
@@ -64,7 +64,7 @@ def build(verbose: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(_compile, SOURCES))
     if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(o) for o in objs):
-        cmd = [_nvcc(), "-shared", "-ccbin", _host_cxx()] + ARCH + ["-o", OUT] + objs + ["-lgomp", "-lcudart"]
+        cmd = [_nvcc(), "-shared", "-ccbin", _host_cxx()] + ARCH + ["-o", OUT] + objs + ["-lgomp", "-lcudart", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

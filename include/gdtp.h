@@ -294,6 +294,66 @@ int gdtp_server_stats(gdtp_server* s, double* stats);
 /* Device bytes held by the system (coefficients, vectors, coarse factor). */
 int gdtp_system_device_bytes(const gdtp_system* s, int64_t* bytes);
 
+/* ---------------------------------------------------------------------------
+ * Texture I/O (host; no device needed).  The apps' inputs and outputs: a
+ * textured mesh (PLY), a colour or normal texture, a tangent field, and the
+ * atlas padding applied before the texel grid is built
+ * (TextureFiltering.cpp:807-837, LineIntegralConvolution.cpp:579-586).
+ * Errors (unreadable or malformed files) return GDTP_ERR_INVALID with the
+ * reason in gdtp_last_error(); the reference exits or reads garbage instead.
+ * ------------------------------------------------------------------------- */
+/* ReadTexturedMesh without a texture (include/Src/SimpleMesh.h:118-146): the
+ * "vertex" element's x, y, z and the "face" element's vertex_indices and
+ * texcoord lists, ASCII or binary (either endianness), items converted as the
+ * reference's PLY library does (include/Misha/PlyFile.inl:2342-2480).  Faces
+ * keep their first three corners.  With all outputs NULL only *nv and *nt are
+ * written; otherwise *nv, *nt give the capacities of vertices (nv*3),
+ * triangles (nt*3) and uv (nt*3*2, per corner) and receive the counts. */
+int gdtp_read_textured_mesh(const char* path, int64_t* nv, int64_t* nt, double* vertices, int32_t* triangles, double* uv);
+/* The name of a "comment TextureFile <name>" header line ("" if none), as
+ * WriteTexturedMesh records the atlas; name NULL: *size = bytes needed. */
+int gdtp_textured_mesh_texture_file(const char* path, char* name, int64_t* size);
+/* WriteTexturedMesh (SimpleMesh.h:93-116): ASCII PLY with double vertices and
+ * texcoords, written with 17 significant digits so that they read back
+ * bit-exact (the reference prints fewer); texture_file (or NULL) goes into the
+ * TextureFile comment. */
+int gdtp_write_textured_mesh(const char* path, const double* vertices, int64_t nv, const int32_t* triangles, int64_t nt,
+                             const double* uv, const char* texture_file);
+/* Image<Point3D<float>>::read (include/Misha/Image.h:90-110) by extension:
+ * ".png" through the reference's PNGReadColor transforms (PNG.inl:10-72:
+ * 16-bit samples keep their high byte, 1/2/4-bit samples are unpacked without
+ * rescaling, palette indices are looked up, alpha is dropped; grey is copied to
+ * all three channels), each byte / 255; ".normap" as ReadBinaryImage
+ * (include/Src/VectorIO.h:47-58: int32 width, int32 height, float RGB).  rgb:
+ * width*height*3 floats, row 0 first (the first PNG row), pixel (i, j) at
+ * 3*(j*width + i).  rgb NULL: only *width, *height; otherwise they must match
+ * the file. */
+int gdtp_read_image(const char* path, int* width, int* height, float* rgb);
+/* Image<Point3D<float>>::write (Image.h:152-163): ".png" 8-bit RGB with each
+ * value v stored as min(255, max(0, (int)(v*255 + 0.5))) in float arithmetic
+ * (values beyond the int range, undefined in the reference, saturate);
+ * ".normap" as WriteBinaryImage (VectorIO.h:34-45). */
+int gdtp_write_image(const char* path, const float* rgb, int width, int height);
+/* ReadVector / WriteVector (VectorIO.h:9-32): int32 count, then count raw
+ * elements of elem_bytes each (16 for the Point2D<double> tangent fields of
+ * ".vf" files).  data NULL: *count = the file's count; otherwise *count is the
+ * capacity and receives the count. */
+int gdtp_read_vector(const char* path, int64_t elem_bytes, int64_t* count, void* data);
+int gdtp_write_vector(const char* path, int64_t elem_bytes, int64_t count, const void* data);
+/* ComputePadding (include/Src/Padding.h:16-46) over n_uv (u, v) pairs:
+ * padding = {left, bottom, right, top}; texture coordinates closer than half a
+ * texel to the image edge grow the grid, which is then rounded up to multiples
+ * of 8 by growing left and bottom (a no-op padding is all zeros). */
+int gdtp_compute_padding(int width, int height, const double* uv, int64_t n_uv, int32_t* padding);
+/* PaddTextureCoordinates / UnpaddTextureCoordinates (Padding.h:76-94) in
+ * place; width, height: the unpadded image size. */
+int gdtp_pad_texture_coordinates(const int32_t* padding, int width, int height, double* uv, int64_t n_uv, int unpad);
+/* PaddImage (Padding.h:48-60, edge texels repeated) into out of
+ * (width+left+right) x (height+bottom+top), or with unpad UnpaddImage
+ * (:62-73, a crop) into out of (width-left-right) x (height-bottom-top);
+ * width, height: the size of `in`. */
+int gdtp_pad_image(const int32_t* padding, const float* in, int width, int height, float* out, int unpad);
+
 #ifdef __cplusplus
 }
 #endif
