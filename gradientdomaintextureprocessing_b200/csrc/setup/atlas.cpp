@@ -191,6 +191,11 @@ bool build_atlas(const Mesh& mesh, int width, int height, Atlas& A, std::string&
     }
     C.triangles.push_back(tri);
   }
+  // grid origin as the reference's release build computes it: its Makefile
+  // builds with -ffast-math, which turns the loop-invariant divisions by width
+  // and height into multiplies by their reciprocals (exact for powers of two,
+  // the last bit may differ otherwise)
+  const double invW = 1.0 / double(width), invH = 1.0 / double(height);
   for (auto& C : A.charts) {
     V2 mid = (C.minCorner + C.maxCorner) / 2.0;
     mid.x *= double(width);
@@ -200,8 +205,8 @@ bool build_atlas(const Mesh& mesh, int width, int height, Atlas& A, std::string&
     C.originCoords[0] = int(std::round(mid.x));
     C.originCoords[1] = int(std::round(mid.y));
     mid = mid + V2(0.5, 0.5);
-    mid.x /= double(width);
-    mid.y /= double(height);
+    mid.x *= invW;
+    mid.y *= invH;
     C.gridOrigin = mid;
     for (size_t t = 0; t < C.meshTriangleIndices.size(); t++)
       for (int k = 0; k < 3; k++)

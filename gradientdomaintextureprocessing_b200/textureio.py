@@ -30,7 +30,7 @@ from . import _lib
 
 __all__ = ["ReadTexturedMesh", "WriteTexturedMesh", "read_image", "write_image", "ReadVector", "WriteVector", "Padding",
            "ComputePadding", "PaddTextureCoordinates", "UnpaddTextureCoordinates", "PaddImage", "UnpaddImage",
-           "load_filtering_input", "texture_from_texels"]
+           "prepare_filtering_mesh", "load_filtering_input", "texture_from_texels"]
 
 
 def _path(p) -> bytes:
@@ -168,24 +168,38 @@ def UnpaddImage(padding: Padding, img: np.ndarray) -> np.ndarray:
     return _pad_img(padding, img, 1)
 
 
+def prepare_filtering_mesh(mesh: dict, width: int, height: int) -> tuple[dict, Padding, int, int]:
+    """The filtering app's mesh preprocessing (TextureFiltering.cpp:814-837) for
+    a texture of width x height: vertices centred and scaled to unit radius, v
+    flipped, and texture coordinates (and the texture, if the mesh has one)
+    padded when the atlas reaches within half a texel of the image edge or the
+    size is not a multiple of 8.  The reference's optional random jitter
+    (--jitter, unseeded) is not applied.  Returns the new mesh, the padding and
+    the padded size."""
+    m = dict(mesh)
+    v = np.asarray(m["vertices"], np.float64)
+    centroid = v.sum(axis=0) / v.shape[0]
+    d = v - centroid
+    radius = float(np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2]).max())) if v.shape[0] else 1.0
+    m["vertices"] = d / radius
+    uv = np.array(m["uv"], np.float64)
+    uv[..., 1] = 1.0 - uv[..., 1]
+    padding = ComputePadding(width, height, uv)
+    if padding.nonTrivial:
+        uv = PaddTextureCoordinates(padding, width, height, uv)
+        if m.get("texture") is not None:
+            m["texture"] = PaddImage(padding, m["texture"])
+    m["uv"] = uv
+    return m, padding, width + padding.left + padding.right, height + padding.bottom + padding.top
+
+
 def load_filtering_input(mesh_path, texture_path) -> tuple[dict, Padding]:
     """The filtering app's input steps (TextureFiltering.cpp:807-837): read the
-    mesh and texture, centre the vertices and scale them to unit radius, flip
-    the v coordinate, then pad coordinates and texture when the atlas reaches
-    within half a texel of the image edge (or the size is not a multiple of 8).
-    The reference's optional random jitter (--jitter, unseeded) is not applied.
-    Returns the mesh (texture padded) and the padding to undo on export."""
+    mesh and its texture, then prepare_filtering_mesh.  Returns the mesh
+    (texture padded) and the padding to undo on export."""
     mesh = ReadTexturedMesh(mesh_path, texture_path)
-    v = mesh["vertices"]
-    centroid = v.sum(axis=0) / v.shape[0]
-    radius = max(float(np.sqrt(((p - centroid) ** 2).sum())) for p in v) if v.shape[0] else 1.0
-    mesh["vertices"] = (v - centroid) / radius
-    mesh["uv"][..., 1] = 1.0 - mesh["uv"][..., 1]
     h, w = mesh["texture"].shape[:2]
-    padding = ComputePadding(w, h, mesh["uv"])
-    if padding.nonTrivial:
-        mesh["uv"] = PaddTextureCoordinates(padding, w, h, mesh["uv"])
-        mesh["texture"] = PaddImage(padding, mesh["texture"])
+    mesh, padding, _, _ = prepare_filtering_mesh(mesh, w, h)
     return mesh, padding
 
 
