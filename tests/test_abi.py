@@ -47,3 +47,35 @@ def test_solve_entry_points_reject_a_null_system(built_lib):
     assert L.gdtp_solve_ex(None, b, x, 1, 1e-6, 10, 1, C.byref(rep)) == -1
     assert L.gdtp_solve_stream(None, bp, xp, 1, 1, 1e-6, 10, None) == -1
     assert b"null system handle" in L.gdtp_last_error()
+
+
+_NULL_CALLS = r'''
+import ctypes as C, sys
+sys.path.insert(0, sys.argv[1])
+from gradientdomaintextureprocessing_b200 import _lib
+L = _lib.lib()
+for name, (res, args) in _lib._SIGS.items():
+    if name in ("gdtp_last_error", "gdtp_version"):
+        continue
+    vals = [0 if a in (C.c_int, C.c_int64) else 1e-6 if a is C.c_double else None for a in args]
+    print(name, flush=True)
+    r = getattr(L, name)(*vals)
+    print("=", r, flush=True)
+'''
+
+
+def test_every_entry_point_rejects_null_and_zero_arguments(built_lib):
+    """Each entry point, called with null pointers and zero sizes, returns an
+    error (or, for the free / count functions, does nothing) instead of
+    crashing; run in a child process so that a crash names the entry point."""
+    import subprocess
+    import sys
+    from conftest import ROOT
+    p = subprocess.run([sys.executable, "-c", _NULL_CALLS, ROOT], capture_output=True, text=True, timeout=300)
+    lines = p.stdout.split("\n")
+    assert p.returncode == 0, f"crashed after: {lines[-3:]} {p.stderr[-300:]}"
+    results = dict(zip(lines[0::2], lines[1::2]))
+    assert len(results) >= 40
+    for name, r in results.items():
+        ok = {"= None", "= 0"} if name.endswith(("_free", "_levels", "_charts")) else {"= -1"}
+        assert r in ok, (name, r)
