@@ -13,6 +13,8 @@ Reference names and behaviour (fabianprada/GradientDomainTextureProcessing):
   app, ``TextureFiltering/TextureFiltering.cpp:807-837``
 * ``texture_from_texels``                       -- ``UpdateFilteredTexture``,
   ``TextureFiltering.cpp:296-302``
+* ``export_texture``                            -- ``ExportTextureCallBack``,
+  ``TextureFiltering.cpp:479-499``
 
 A mesh is the dict that :mod:`meshgen` produces and ``InitializeHierarchy``
 takes: ``vertices`` (nv, 3) float64, ``triangles`` (nt, 3) int32, ``uv``
@@ -30,7 +32,7 @@ from . import _lib
 
 __all__ = ["ReadTexturedMesh", "WriteTexturedMesh", "read_image", "write_image", "ReadVector", "WriteVector", "Padding",
            "ComputePadding", "PaddTextureCoordinates", "UnpaddTextureCoordinates", "PaddImage", "UnpaddImage",
-           "prepare_filtering_mesh", "load_filtering_input", "texture_from_texels"]
+           "prepare_filtering_mesh", "load_filtering_input", "texture_from_texels", "export_texture"]
 
 
 def _path(p) -> bytes:
@@ -216,3 +218,23 @@ def texture_from_texels(hierarchy, x: np.ndarray, width: int, height: int, backg
     if padding is not None and padding.nonTrivial:
         img = UnpaddImage(padding, img)
     return img
+
+
+def export_texture(path, img: np.ndarray, padding: Padding | None = None, normal: bool = False) -> None:
+    """ExportTextureCallBack (TextureFiltering.cpp:479-499): crop the padding
+    back, then ".png" gets the 8-bit colour write; for a normal texture each
+    pixel is first normalised and mapped to v * 0.5 + 0.5 (float32).  Any other
+    extension gets the raw layout of WriteBinaryImage (int32 width, int32
+    height, float RGB), whatever the name."""
+    out = np.ascontiguousarray(img, np.float32)
+    if padding is not None and padding.nonTrivial:
+        out = UnpaddImage(padding, out)
+    if str(path).lower().endswith(".png"):
+        if normal:
+            length = np.sqrt(out[..., 0] * out[..., 0] + out[..., 1] * out[..., 1] + out[..., 2] * out[..., 2])
+            out = (out / length[..., None]) * np.float32(0.5) + np.float32(0.5)
+        write_image(path, out)
+        return
+    h, w = out.shape[:2]
+    with open(path, "wb") as fh:
+        fh.write(np.array([w, h], "<i4").tobytes() + out.astype("<f4").tobytes())

@@ -311,3 +311,24 @@ def test_filtering_input_and_export(tio, tmp_path):
     full = tio.texture_from_texels(h, x, W, H)
     np.testing.assert_array_equal(full[tn[:, 1], tn[:, 0]], x.astype(np.float32))
     np.testing.assert_array_equal(out, full[pad.bottom:pad.bottom + 60, pad.left:pad.left + 100])
+
+
+def test_export_texture(tio, tmp_path):
+    """ExportTextureCallBack: colour PNG as written; normal maps normalised and
+    mapped to [0, 1] first; other extensions in the raw normap layout."""
+    import png_port
+    rng = np.random.default_rng(4)
+    img = rng.normal(size=(12, 20, 3)).astype(np.float32)
+    pad = tio.Padding(left=3, bottom=2, right=1, top=0)
+    tio.export_texture(tmp_path / "c.png", img, padding=pad)
+    crop = img[2:12, 3:19]
+    np.testing.assert_array_equal(tio.read_image(tmp_path / "c.png"), png_port.to_byte(crop).astype(np.float32) / np.float32(255))
+    tio.export_texture(tmp_path / "n.png", img, normal=True)
+    n = img / np.sqrt((img * img).sum(axis=2, keepdims=True))
+    want = png_port.to_byte((n * np.float32(0.5) + np.float32(0.5)).astype(np.float32))
+    got = np.rint(tio.read_image(tmp_path / "n.png") * 255).astype(np.int32)
+    assert np.abs(got - want.astype(np.int32)).max() <= 1  # the norm's last bit may round a byte the other way
+    tio.export_texture(tmp_path / "raw.bin", img, padding=pad)
+    raw = (tmp_path / "raw.bin").read_bytes()
+    assert struct.unpack("<ii", raw[:8]) == (16, 10)
+    np.testing.assert_array_equal(np.frombuffer(raw[8:], np.float32).reshape(10, 16, 3), crop)
