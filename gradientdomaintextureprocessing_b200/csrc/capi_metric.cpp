@@ -27,25 +27,29 @@ static void emit(const std::vector<M2>& P, double* out) {
 
 extern "C" int gdtp_surface_metric(const double* vertices, int64_t nv, const int32_t* triangles, int64_t nt, const double* uv,
                                    int mode, double* metric_out) {
-  Mesh m;
-  if (!metric_out || (mode != 0 && mode != 1) || !make_mesh(vertices, nv, triangles, nt, uv, m))
-    return fail(GDTP_ERR_INVALID, "gdtp_surface_metric: invalid arguments");
-  std::vector<M2> G, P;
-  if (!surface_metric(m, mode, true, G)) return fail(GDTP_ERR_SETUP, "gdtp_surface_metric: zero total area");
-  if (!parameter_metric(m, G, P)) return fail(GDTP_ERR_SETUP, "gdtp_surface_metric: degenerate texture triangle");
-  emit(P, metric_out);
-  return GDTP_OK;
+  return guarded("gdtp_surface_metric", [&]() -> int {
+    Mesh m;
+    if (!metric_out || (mode != 0 && mode != 1) || !make_mesh(vertices, nv, triangles, nt, uv, m))
+      return fail(GDTP_ERR_INVALID, "gdtp_surface_metric: invalid arguments");
+    std::vector<M2> G, P;
+    if (!surface_metric(m, mode, true, G)) return fail(GDTP_ERR_SETUP, "gdtp_surface_metric: zero total area");
+    if (!parameter_metric(m, G, P)) return fail(GDTP_ERR_SETUP, "gdtp_surface_metric: degenerate texture triangle");
+    emit(P, metric_out);
+    return GDTP_OK;
+  });
 }
 
 extern "C" int gdtp_anisotropic_metric(const double* vertices, int64_t nv, const int32_t* triangles, int64_t nt, const double* uv,
                                        const double* vf, double across, double isotropic, double* metric_out) {
-  Mesh m;
-  if (!metric_out || !vf || !(across >= 0) || !(isotropic > 0) || !make_mesh(vertices, nv, triangles, nt, uv, m))
-    return fail(GDTP_ERR_INVALID, "gdtp_anisotropic_metric: invalid arguments");
-  std::vector<M2> G, U, P;
-  if (!surface_metric(m, 0, true, G)) return fail(GDTP_ERR_SETUP, "gdtp_anisotropic_metric: zero total area");
-  if (!vector_field_metric(G, vf, across, isotropic, true, U)) return fail(GDTP_ERR_SETUP, "gdtp_anisotropic_metric: zero metric area");
-  if (!parameter_metric(m, U, P)) return fail(GDTP_ERR_SETUP, "gdtp_anisotropic_metric: degenerate texture triangle");
-  emit(P, metric_out);
-  return GDTP_OK;
+  return guarded("gdtp_anisotropic_metric", [&]() -> int {
+    Mesh m;
+    if (!metric_out || !vf || !(across >= 0) || !(isotropic > 0) || !make_mesh(vertices, nv, triangles, nt, uv, m))
+      return fail(GDTP_ERR_INVALID, "gdtp_anisotropic_metric: invalid arguments");
+    std::vector<M2> G, U, P;
+    if (!surface_metric(m, 0, true, G)) return fail(GDTP_ERR_SETUP, "gdtp_anisotropic_metric: zero total area");
+    if (!vector_field_metric(G, vf, across, isotropic, true, U)) return fail(GDTP_ERR_SETUP, "gdtp_anisotropic_metric: zero metric area");
+    if (!parameter_metric(m, U, P)) return fail(GDTP_ERR_SETUP, "gdtp_anisotropic_metric: degenerate texture triangle");
+    emit(P, metric_out);
+    return GDTP_OK;
+  });
 }

@@ -188,6 +188,18 @@ bool read_ply_textured_mesh(const std::string& path, TexturedMesh& m, std::strin
     }
   }
   if (!ended || format < 0) { err = path + ": incomplete PLY header"; return false; }
+  // every instance takes at least its scalars and list counts (binary) or one
+  // character and a separator per item (ASCII): counts the file cannot hold are
+  // rejected before anything is allocated for them
+  {
+    long double need = 0;
+    for (const Element& e : elems) {
+      long double per = 0;
+      for (const Property& p : e.props) per += format == 0 ? 2 : type_size(p.countType != kNone ? p.countType : p.type);
+      need += per * (long double)e.count;
+    }
+    if (need > (long double)(buf.size() - pos)) { err = path + ": PLY element counts exceed the file size"; return false; }
+  }
 
   Reader r(buf, pos, format);
   Item it;

@@ -79,3 +79,20 @@ def test_every_entry_point_rejects_null_and_zero_arguments(built_lib):
     for name, r in results.items():
         ok = {"= None", "= 0"} if name.endswith(("_free", "_levels", "_charts")) else {"= -1"}
         assert r in ok, (name, r)
+
+
+def test_entry_point_exceptions_become_error_codes(built_lib):
+    """guarded() (the wrapper of every C entry point's body) turns host
+    allocation failures and other C++ exceptions into error codes."""
+    import os
+    import subprocess
+    import tempfile
+    from conftest import ROOT
+    pkg = os.path.join(ROOT, "gradientdomaintextureprocessing_b200")
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = os.path.join(tmp, "guard_check")
+        subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(pkg, "csrc"), "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "native", "guard_check.cpp"), "-L", pkg, "-lgdtp", "-Wl,-rpath," + pkg,
+                        "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+        assert out.returncode == 0 and out.stdout.strip() == "ok", out.stdout + out.stderr

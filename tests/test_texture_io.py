@@ -332,3 +332,16 @@ def test_export_texture(tio, tmp_path):
     raw = (tmp_path / "raw.bin").read_bytes()
     assert struct.unpack("<ii", raw[:8]) == (16, 10)
     np.testing.assert_array_equal(np.frombuffer(raw[8:], np.float32).reshape(10, 16, 3), crop)
+
+
+def test_ply_counts_beyond_the_file_are_rejected(tio, tmp_path):
+    """A header that declares more data than the file holds is an error, not an
+    allocation of the declared size."""
+    from gradientdomaintextureprocessing_b200._lib import GDTPError
+    p = tmp_path / "huge.ply"
+    p.write_bytes(b"ply\nformat binary_little_endian 1.0\nelement vertex 4000000000000\nproperty float x\n"
+                  b"property float y\nproperty float z\nelement face 1\nproperty list uchar int vertex_indices\n"
+                  b"property list uchar float texcoord\nend_header\n" + b"\0" * 64)
+    with pytest.raises(GDTPError, match="exceed the file size"):
+        tio.ReadTexturedMesh(p)
+
