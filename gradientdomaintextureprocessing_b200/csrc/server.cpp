@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <exception>
+#include <new>
 
 #include "gdtp.h"
 
@@ -94,6 +96,22 @@ bool Server::build_device(Model& m, std::string& err) {
     m.a->knobs.krylov = 1;  // the anisotropic V-cycle contracts slowly: CG around it
   }
   return true;
+}
+
+// Runs a step of the worker that may allocate; a C++ exception becomes false
+// and a message, so that it fails the batch instead of ending the process.
+template <class F>
+static bool without_exceptions(F&& f, std::string& err) {
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    err = "out of host memory";
+  } catch (const std::exception& e) {
+    err = e.what();
+  } catch (...) {
+    err = "unexpected exception";
+  }
+  return false;
 }
 
 void Server::free_device(Model& m) {
@@ -212,7 +230,7 @@ void Server::worker() {
       ok = admit(*m, lk, err);
       if (ok) {
         lk.unlock();
-        ok = build_device(*m, err);
+        ok = without_exceptions([&] { return build_device(*m, err); }, err);
         lk.lock();
         builds_++;
         if (!ok) {
@@ -226,7 +244,12 @@ void Server::worker() {
     if (ok) {
       for (auto* r : batch) r->tStart = now();
       lk.unlock();
-      run_batch(*m, batch);
+      std::string batchErr;
+      if (!without_exceptions([&] { run_batch(*m, batch); return true; }, batchErr))
+        for (auto* r : batch) {
+          r->status = GDTP_ERR_SETUP;
+          r->error = batchErr;
+        }
       lk.lock();
       m->bytes = int64_t(m->a ? m->a->deviceBytes() : 0) + int64_t(m->b ? m->b->deviceBytes() : 0);
       m->estimate = std::max(m->estimate, m->bytes);
