@@ -171,8 +171,9 @@ def UnpaddImage(padding: Padding, img: np.ndarray) -> np.ndarray:
 
 
 def prepare_filtering_mesh(mesh: dict, width: int, height: int) -> tuple[dict, Padding, int, int]:
-    """The filtering app's mesh preprocessing (TextureFiltering.cpp:814-837) for
-    a texture of width x height: vertices centred and scaled to unit radius, v
+    """The apps' mesh preprocessing for a texture of width x height, the same in
+    all three (TextureFiltering.cpp:814-837, Geodesics.cpp:788-809,
+    LineIntegralConvolution.cpp:785-806): vertices centred and scaled to unit radius, v
     flipped, and texture coordinates (and the texture, if the mesh has one)
     padded when the atlas reaches within half a texel of the image edge or the
     size is not a multiple of 8.  The reference's optional random jitter
