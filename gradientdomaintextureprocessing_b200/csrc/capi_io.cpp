@@ -118,8 +118,10 @@ static io::Padding padding_of(const int32_t* p) {
 
 extern "C" int gdtp_compute_padding(int width, int height, const double* uv, int64_t n_uv, int32_t* padding) {
   return guarded("gdtp_compute_padding", [&]() -> int {
-    if (width <= 0 || height <= 0 || n_uv < 0 || (n_uv && !uv) || !padding) return fail(GDTP_ERR_INVALID, "gdtp_compute_padding: bad arguments");
-    const io::Padding p = io::compute_padding(width, height, uv, size_t(n_uv));
+    if (width <= 0 || height <= 0 || width > (1 << 24) || height > (1 << 24) || n_uv < 0 || (n_uv && !uv) || !padding) return fail(GDTP_ERR_INVALID, "gdtp_compute_padding: bad arguments");
+    io::Padding p;
+    std::string err;
+    if (!io::compute_padding(width, height, uv, size_t(n_uv), p, err)) return fail(GDTP_ERR_INVALID, "gdtp_compute_padding: " + err);
     padding[0] = p.left, padding[1] = p.bottom, padding[2] = p.right, padding[3] = p.top;
     return GDTP_OK;
   });
@@ -127,7 +129,7 @@ extern "C" int gdtp_compute_padding(int width, int height, const double* uv, int
 
 extern "C" int gdtp_pad_texture_coordinates(const int32_t* padding, int width, int height, double* uv, int64_t n_uv, int unpad) {
   return guarded("gdtp_pad_texture_coordinates", [&]() -> int {
-    if (!padding || width <= 0 || height <= 0 || n_uv < 0 || (n_uv && !uv)) return fail(GDTP_ERR_INVALID, "gdtp_pad_texture_coordinates: bad arguments");
+    if (!padding || width <= 0 || height <= 0 || width > (1 << 24) || height > (1 << 24) || n_uv < 0 || (n_uv && !uv)) return fail(GDTP_ERR_INVALID, "gdtp_pad_texture_coordinates: bad arguments");
     io::pad_texture_coordinates(padding_of(padding), width, height, uv, size_t(n_uv), unpad != 0);
     return GDTP_OK;
   });

@@ -110,7 +110,7 @@ bool read_vector(const std::string& path, size_t elemBytes, std::vector<unsigned
   int32_t n = 0;
   if (buf.size() < 4) { err = path + ": truncated vector file"; return false; }
   std::memcpy(&n, buf.data(), 4);
-  if (n < 0 || buf.size() - 4 < size_t(n) * elemBytes) { err = path + ": vector file shorter than its count"; return false; }
+  if (n < 0 || size_t(n) > (buf.size() - 4) / elemBytes) { err = path + ": vector file shorter than its count"; return false; }
   data.assign(buf.begin() + 4, buf.begin() + 4 + size_t(n) * elemBytes);
   return true;
 }
@@ -127,23 +127,28 @@ bool write_vector(const std::string& path, size_t elemBytes, const void* data, s
 // Padding.h:16-46: the texel grid must hold every texture coordinate at least
 // half a texel inside; the padded size is then rounded up to multiples of 8 by
 // growing left / bottom
-Padding compute_padding(int width, int height, const double* uv, size_t nUv) {
-  Padding p;
-  if (nUv == 0) return p;
+bool compute_padding(int width, int height, const double* uv, size_t nUv, Padding& p, std::string& err) {
+  p = Padding();
+  if (nUv == 0) return true;
+  for (size_t i = 0; i < 2 * nUv; i++)
+    if (!(std::fabs(uv[i]) <= 1e6)) { err = "texture coordinate not finite or beyond 1e6"; return false; }
   const double pixMin[2] = {0.5 / double(width), 0.5 / double(height)};
   const double pixMax[2] = {(double(width) - 0.5) / double(width), (double(height) - 0.5) / double(height)};
   double tMin[2] = {uv[0], uv[1]}, tMax[2] = {uv[0], uv[1]};
   for (size_t i = 0; i < nUv; i++)
     for (int c = 0; c < 2; c++) tMin[c] = std::min(tMin[c], uv[2 * i + c]), tMax[c] = std::max(tMax[c], uv[2 * i + c]);
-  p.left = tMin[0] < pixMin[0] ? int(std::ceil((pixMin[0] - tMin[0]) * double(width))) : 0;
-  p.bottom = tMin[1] < pixMin[1] ? int(std::ceil((pixMin[1] - tMin[1]) * double(height))) : 0;
-  p.right = tMax[0] > pixMax[0] ? int(std::ceil((tMax[0] - pixMax[0]) * double(width))) : 0;
-  p.top = tMax[1] > pixMax[1] ? int(std::ceil((tMax[1] - pixMax[1]) * double(height))) : 0;
+  const double pad[4] = {tMin[0] < pixMin[0] ? std::ceil((pixMin[0] - tMin[0]) * double(width)) : 0.0,
+                         tMin[1] < pixMin[1] ? std::ceil((pixMin[1] - tMin[1]) * double(height)) : 0.0,
+                         tMax[0] > pixMax[0] ? std::ceil((tMax[0] - pixMax[0]) * double(width)) : 0.0,
+                         tMax[1] > pixMax[1] ? std::ceil((tMax[1] - pixMax[1]) * double(height)) : 0.0};
+  for (double d : pad)
+    if (d > 16777216.0) { err = "padding beyond 2^24 texels"; return false; }
+  p.left = int(pad[0]), p.bottom = int(pad[1]), p.right = int(pad[2]), p.top = int(pad[3]);
   const int newW = width + p.left + p.right, newH = height + p.bottom + p.top;
   p.left += 8 * ((newW - 1) / 8 + 1) - newW;
   p.bottom += 8 * ((newH - 1) / 8 + 1) - newH;
   p.nonTrivial = p.left || p.right || p.bottom || p.top;
-  return p;
+  return true;
 }
 
 // Padding.h:76-94.  The loop-invariant divisions are multiplies by the
@@ -152,7 +157,7 @@ Padding compute_padding(int width, int height, const double* uv, size_t nUv) {
 // x * (1 / c)); the plain quotient differs in the last bit for ~10-20 % of
 // coordinates.
 void pad_texture_coordinates(const Padding& p, int width, int height, double* uv, size_t nUv, bool unpad) {
-  const double newW = double(width + p.left + p.right), newH = double(height + p.bottom + p.top);
+  const double newW = double(width) + p.left + p.right, newH = double(height) + p.bottom + p.top;
   const double rx = unpad ? 1.0 / double(width) : 1.0 / newW, ry = unpad ? 1.0 / double(height) : 1.0 / newH;
   for (size_t i = 0; i < nUv; i++) {
     double& u = uv[2 * i];
@@ -171,7 +176,9 @@ void pad_texture_coordinates(const Padding& p, int width, int height, double* uv
 bool pad_image(const Padding& p, const float* in, int width, int height, std::vector<float>& out, bool unpad, std::string& err) {
   if (!in || width <= 0 || height <= 0 || p.left < 0 || p.right < 0 || p.bottom < 0 || p.top < 0) { err = "bad image or padding"; return false; }
   if (!unpad) {
-    const int w = width + p.left + p.right, h = height + p.bottom + p.top;
+    const long long wl = (long long)width + p.left + p.right, hl = (long long)height + p.bottom + p.top;
+    if (wl > (1 << 24) || hl > (1 << 24)) { err = "padded image larger than 2^24 texels on a side"; return false; }
+    const int w = int(wl), h = int(hl);
     out.resize(size_t(w) * h * 3);
     for (int j = 0; j < h; j++) {
       const int sj = std::min(std::max(0, j - p.bottom), height - 1);
@@ -182,8 +189,9 @@ bool pad_image(const Padding& p, const float* in, int width, int height, std::ve
     }
     return true;
   }
-  const int w = width - p.left - p.right, h = height - p.bottom - p.top;
-  if (w <= 0 || h <= 0) { err = "padding larger than the image"; return false; }
+  const long long wl = (long long)width - p.left - p.right, hl = (long long)height - p.bottom - p.top;
+  if (wl <= 0 || hl <= 0) { err = "padding larger than the image"; return false; }
+  const int w = int(wl), h = int(hl);
   out.resize(size_t(w) * h * 3);
   for (int j = 0; j < h; j++)
     std::memcpy(&out[3 * size_t(j) * w], &in[3 * (size_t(p.bottom + j) * width + p.left)], 3 * size_t(w) * sizeof(float));

@@ -69,7 +69,8 @@ struct Padding {
   int left = 0, bottom = 0, right = 0, top = 0;
   bool nonTrivial = false;
 };
-Padding compute_padding(int width, int height, const double* uv, size_t nUv);
+// false (with err) for texture coordinates that are not finite or beyond 1e6
+bool compute_padding(int width, int height, const double* uv, size_t nUv, Padding& p, std::string& err);
 // uv: nUv (u, v) pairs in place; unpad reverses
 void pad_texture_coordinates(const Padding& p, int width, int height, double* uv, size_t nUv, bool unpad);
 // pad: out is (width + left + right) x (height + bottom + top), edge texels

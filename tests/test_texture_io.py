@@ -345,3 +345,25 @@ def test_ply_counts_beyond_the_file_are_rejected(tio, tmp_path):
     with pytest.raises(GDTPError, match="exceed the file size"):
         tio.ReadTexturedMesh(p)
 
+
+
+def test_sizes_that_would_overflow_are_errors(tio, tmp_path, golden):
+    """Element sizes, texture coordinates and paddings whose products overflow
+    are rejected (the padding of valid inputs is unchanged)."""
+    import ctypes as C
+    from gradientdomaintextureprocessing_b200 import _lib
+    from gradientdomaintextureprocessing_b200._lib import GDTPError
+    L = _lib.lib()
+    n = C.c_int64(0)
+    assert L.gdtp_read_vector(os.path.join(IO, "field.vf").encode(), 1 << 60, C.byref(n), None) == -1
+    with pytest.raises(GDTPError, match="not finite or beyond"):
+        tio.ComputePadding(256, 256, np.array([[0.5, 0.5], [np.inf, 0.5]]))
+    with pytest.raises(GDTPError, match="beyond 2"):
+        tio.ComputePadding(1 << 24, 256, np.array([[0.5, 0.5], [1e5, 0.5]]))
+    pad = np.array([1 << 30, 0, 1 << 30, 0], np.int32)
+    img = np.zeros((4, 4, 3), np.float32)
+    out = np.zeros(3, np.float32)
+    assert L.gdtp_pad_image(_lib.ptr(pad), _lib.ptr(img), 4, 4, _lib.ptr(out), 0) == -1
+    assert "2^24" in L.gdtp_last_error().decode()
+    w, h = map(int, golden["pad1/size"])
+    assert list(tio.ComputePadding(w, h, golden["pad1/uv"])) == list(golden["pad1/padding"].ravel()[:4])
