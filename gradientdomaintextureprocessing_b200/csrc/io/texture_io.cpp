@@ -66,7 +66,7 @@ bool read_image(const std::string& path, std::vector<float>* rgb, int& width, in
     int32_t wh[2];
     if (buf.size() < 8) { err = path + ": truncated normap"; return false; }
     std::memcpy(wh, buf.data(), 8);
-    if (wh[0] <= 0 || wh[1] <= 0 || buf.size() - 8 < size_t(wh[0]) * size_t(wh[1]) * 12) {
+    if (wh[0] <= 0 || wh[1] <= 0 || size_t(wh[0]) > (buf.size() - 8) / 12 / size_t(wh[1])) {
       err = path + ": bad or truncated normap";
       return false;
     }

@@ -367,3 +367,11 @@ def test_sizes_that_would_overflow_are_errors(tio, tmp_path, golden):
     assert "2^24" in L.gdtp_last_error().decode()
     w, h = map(int, golden["pad1/size"])
     assert list(tio.ComputePadding(w, h, golden["pad1/uv"])) == list(golden["pad1/padding"].ravel()[:4])
+
+
+def test_normap_header_larger_than_the_file(tio, tmp_path):
+    from gradientdomaintextureprocessing_b200._lib import GDTPError
+    p = tmp_path / "big.normap"
+    p.write_bytes(struct.pack("<ii", 2_000_000_000, 2_000_000_000) + b"\0" * 48)
+    with pytest.raises(GDTPError, match="truncated"):
+        tio.read_image(p)
