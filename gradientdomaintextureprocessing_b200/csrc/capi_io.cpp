@@ -47,7 +47,7 @@ extern "C" int gdtp_textured_mesh_texture_file(const char* path, char* name, int
 extern "C" int gdtp_write_textured_mesh(const char* path, const double* vertices, int64_t nv, const int32_t* triangles, int64_t nt,
                                         const double* uv, const char* texture_file) {
   return guarded("gdtp_write_textured_mesh", [&]() -> int {
-    if (!path || nv < 0 || nt < 0 || (nv && !vertices) || (nt && (!triangles || !uv)))
+    if (!path || nv < 0 || nt < 0 || nv > INT32_MAX || nt > INT32_MAX || (nv && !vertices) || (nt && (!triangles || !uv)))
       return fail(GDTP_ERR_INVALID, "gdtp_write_textured_mesh: bad arguments");
     io::TexturedMesh m;
     m.vertices.assign(vertices, vertices + nv * 3);

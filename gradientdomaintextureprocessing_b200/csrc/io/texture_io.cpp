@@ -117,6 +117,7 @@ bool read_vector(const std::string& path, size_t elemBytes, std::vector<unsigned
 
 bool write_vector(const std::string& path, size_t elemBytes, const void* data, size_t count, std::string& err) {
   if (count > size_t(INT32_MAX)) { err = "vector too long for an int32 count"; return false; }
+  if (elemBytes == 0 || (count && elemBytes > (SIZE_MAX - 4) / count)) { err = "bad element size"; return false; }
   std::vector<unsigned char> out(4 + count * elemBytes);
   const int32_t n = int32_t(count);
   std::memcpy(out.data(), &n, 4);
