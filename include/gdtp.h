@@ -343,7 +343,9 @@ int gdtp_write_vector(const char* path, int64_t elem_bytes, int64_t count, const
 /* ComputePadding (include/Src/Padding.h:16-46) over n_uv (u, v) pairs:
  * padding = {left, bottom, right, top}; texture coordinates closer than half a
  * texel to the image edge grow the grid, which is then rounded up to multiples
- * of 8 by growing left and bottom (a no-op padding is all zeros). */
+ * of 8 by growing left and bottom (a no-op padding is all zeros).
+ * GDTP_ERR_INVALID for width or height above 2^24, coordinates that are not
+ * finite or beyond 1e6, or a padding beyond 2^24 texels. */
 int gdtp_compute_padding(int width, int height, const double* uv, int64_t n_uv, int32_t* padding);
 /* PaddTextureCoordinates / UnpaddTextureCoordinates (Padding.h:76-94) in
  * place; width, height: the unpadded image size. */
