@@ -113,8 +113,9 @@ void gdtp_system_free(gdtp_system* s);
  *   first solve after an update (or after a new right-hand-side width) */
 int gdtp_system_array(const gdtp_system* s, const char* name, int level, void* out, int64_t* count);
 
-/* Combine and coarsen: A = screen*M + stiffness*S, Galerkin hierarchy, coarse
- * Cholesky.  Replaces UpdateLinearSystem (include/Src/UpdateCoefficients.inl:463-513),
+/* Combine and coarsen: A = screen*M + stiffness*S and its Galerkin hierarchy;
+ * the boundary-block and coarsest-level inverses are rebuilt by the next solve.
+ * Replaces UpdateLinearSystem (include/Src/UpdateCoefficients.inl:463-513),
  * UpdateMultigridCoefficients (:285-399) and UpdateMultigridSolvers (:402-439). */
 int gdtp_system_update(gdtp_system* s, double stiffness_weight, double screen_weight);
 
