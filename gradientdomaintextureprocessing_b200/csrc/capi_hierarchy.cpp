@@ -139,10 +139,10 @@ extern "C" int gdtp_hierarchy_array(const gdtp_hierarchy* h, const char* cname, 
         double a[4] = {c.corner.x, c.corner.y, c.cellSizeW, c.cellSizeH};
         return a[i % 4];
       });
-    if (name == "nodeType" || name == "cellType") {
+    if (name == "nodeType" || name == "cellType" || name == "cellCorners") {
       std::vector<int> all;
       for (const GridChart& c : L.charts) {
-        const std::vector<int>& v = name == "nodeType" ? c.nodeType : c.cellType;
+        const std::vector<int>& v = name == "nodeType" ? c.nodeType : name == "cellType" ? c.cellType : c.cellCorners;
         all.insert(all.end(), v.begin(), v.end());
       }
       return emit_vec(out, count, all);

@@ -63,6 +63,8 @@ int gdtp_hierarchy_counts(const gdtp_hierarchy* h, int level, int64_t* counts);
  *   "prolongationLines"(6)                                         Hierarchy.h:242
  *   "charts"(12) chart grid ints, "chartsd"(4, float64) corner+cell size   Hierarchy.h:146-161
  *   "nodeType" "cellType" concatenated per-chart images
+ *   "cellCorners"(4) global texels of every active cell, chart by chart in raster
+ *   order: the global cell index (InitializeCellNodes, HierarchyConstruction.inl:557-566)
  *   "textureNodes"(5: ci,cj,chart,tId,isInterior) level 0 only     Basis.h:4-28
  *   "textureBary"(2, float64) level 0 only
  *   "boundaryRestriction.ptr/.col/.val(float64)"  HierarchicalSystem::boundaryRestriction

@@ -426,6 +426,11 @@ int main(int argc, char** argv) {
     out.f64(p + "charts_d", cd, 4);
     out.i32(p + "cellType", ctype);
     out.i32(p + "nodeType", ntype);
+    std::vector<int> cc;  // every active cell's corners, in global cell order
+    for (auto& c : g.gridCharts)
+      for (const CellIndex& q : c.cellIndices)
+        for (int k = 0; k < 4; k++) cc.push_back(int(q[k]));
+    out.i32(p + "cellIndices", cc, 4);
     // multigrid coefficients (reciprocal form for l < levels-1)
     std::vector<double> dc(coeffs[l].deepCoefficients.begin(), coeffs[l].deepCoefficients.end());
     out.f64(p + "coef/deep", dc, 10);

@@ -42,7 +42,8 @@ SIZE, LEVELS, SAMPLE = 256, 4, 3000
 INDEX_ARRAYS = {"nodeinfo": "nodeinfo", "boundaryGlobalIndex": "boundaryGlobal", "deepGlobalIndex": "deepGlobal",
                 "boundaryAndDeepIndex": "boundaryAndDeep", "rasterLines": "rasterLines",
                 "restrictionLines": "restrictionLines", "deepLines": "deepLines",
-                "prolongationLines": "prolongationLines", "charts_i": "charts"}
+                "prolongationLines": "prolongationLines", "charts_i": "charts", "cellType": "cellType",
+                "nodeType": "nodeType", "cellIndices": "cellCorners"}
 
 
 def digest(a) -> str:

@@ -2,7 +2,8 @@
 256 x 256 after the filtering app's preprocessing) against the UNMODIFIED
 reference hierarchy on the same input (tests/golden/make_real_golden.py).
 
-* counts, every index array, the boundary restriction, chart corners and cell
+* counts, every index array, cell and node types, every active cell's corners
+  (the global cell order), the boundary restriction, chart corners and cell
   sizes, texture node positions / charts / interior flags, boundary nodes:
   bit-exact;
 * texture node triangle ids: equal except for at most two exterior texels per
