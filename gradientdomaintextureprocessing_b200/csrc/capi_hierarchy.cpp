@@ -114,6 +114,21 @@ extern "C" int gdtp_hierarchy_array(const gdtp_hierarchy* h, const char* cname, 
     };
     if (name == "rasterLines") return lines5(L.rasterLines);
     if (name == "restrictionLines") return lines5(L.restrictionLines);
+    if (name == "interiorTexelToCellLines") {
+      // InitializeInteriorTexelToCellLines (InteriorTexelToCellLines.inl:3-29): per
+      // raster line its texels, coefficient offset, and the global index of the
+      // first cell of the row above (cells (ci-1, cj-1)...) and below ((ci-1, cj)...)
+      if (level != 0) return fail(GDTP_ERR_INVALID, "interiorTexelToCellLines exist on level 0 only");
+      return emit<int32_t>(out, count, 5 * (int64_t)L.rasterLines.size(), [&](int64_t i) {
+        const Line& r = L.rasterLines[i / 5];
+        const NodeInfo& n = L.nodes[r.start];
+        const GridChart& c = L.charts[n.chart];
+        const int prev = c.localCell[(n.cj - 1) * (c.width - 1) + (n.ci - 1)] + c.cellOffset;
+        const int next = c.localCell[n.cj * (c.width - 1) + (n.ci - 1)] + c.cellOffset;
+        const int a[5] = {r.start, r.end, r.coeff, prev, next};
+        return a[i % 5];
+      });
+    }
     if (name == "deepLines")
       return emit<int32_t>(out, count, 5 * (int64_t)L.deepLines.size(), [&](int64_t i) {
         const DeepLine& l = L.deepLines[i / 5];

@@ -14,7 +14,7 @@ import numpy as np
 
 from . import _lib
 
-_I32 = {"cellCorners": 4, "nodeinfo": 4, "boundaryAndDeep": 1, "boundaryGlobal": 1, "deepGlobal": 1, "rasterLines": 5,
+_I32 = {"cellCorners": 4, "interiorTexelToCellLines": 5, "nodeinfo": 4, "boundaryAndDeep": 1, "boundaryGlobal": 1, "deepGlobal": 1, "rasterLines": 5,
         "restrictionLines": 5, "deepLines": 5, "prolongationLines": 6, "charts": 12, "nodeType": 1, "cellType": 1,
         "textureNodes": 5, "boundaryNodes": 1}
 _F64 = {"chartsd": 4, "textureBary": 2}

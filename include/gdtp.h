@@ -63,6 +63,9 @@ int gdtp_hierarchy_counts(const gdtp_hierarchy* h, int level, int64_t* counts);
  *   "prolongationLines"(6)                                         Hierarchy.h:242
  *   "charts"(12) chart grid ints, "chartsd"(4, float64) corner+cell size   Hierarchy.h:146-161
  *   "nodeType" "cellType" concatenated per-chart images
+ *   "interiorTexelToCellLines"(5: texel start, texel end, coefficient offset, first
+ *   cell of the row above, of the row below) per raster line, level 0 only
+ *   (InitializeInteriorTexelToCellLines, InteriorTexelToCellLines.inl:3-29)
  *   "cellCorners"(4) global texels of every active cell, chart by chart in raster
  *   order: the global cell index (InitializeCellNodes, HierarchyConstruction.inl:557-566)
  *   "textureNodes"(5: ci,cj,chart,tId,isInterior) level 0 only     Basis.h:4-28

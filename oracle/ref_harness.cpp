@@ -42,6 +42,7 @@ unsigned char* PNGReadColor(const char*, int&, int&) { return nullptr; }
 #include <Src/MassAndStiffness.h>
 #include <Src/VectorIO.h>
 #include <Src/VectorFieldIntergration.inl>
+#include <Src/InteriorTexelToCellLines.inl>
 #include <algorithm>
 
 #include <chrono>
@@ -431,6 +432,14 @@ int main(int argc, char** argv) {
       for (const CellIndex& q : c.cellIndices)
         for (int k = 0; k < 4; k++) cc.push_back(int(q[k]));
     out.i32(p + "cellIndices", cc, 4);
+    if (l == 0) {  // InitializeInteriorTexelToCellLines (InteriorTexelToCellLines.inl:3-29)
+      std::vector<InteriorTexelToCellLine> tl;
+      InitializeInteriorTexelToCellLines(tl, g);
+      std::vector<int> t5;
+      for (const auto& t : tl)
+        t5.insert(t5.end(), {t.texelStartIndex, t.texelEndIndex, t.coeffOffset, t.previousCellStartIndex, t.nextCellStartIndex});
+      out.i32(p + "interiorTexelToCellLines", t5, 5);
+    }
     // multigrid coefficients (reciprocal form for l < levels-1)
     std::vector<double> dc(coeffs[l].deepCoefficients.begin(), coeffs[l].deepCoefficients.end());
     out.f64(p + "coef/deep", dc, 10);

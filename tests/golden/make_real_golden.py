@@ -43,7 +43,8 @@ INDEX_ARRAYS = {"nodeinfo": "nodeinfo", "boundaryGlobalIndex": "boundaryGlobal",
                 "boundaryAndDeepIndex": "boundaryAndDeep", "rasterLines": "rasterLines",
                 "restrictionLines": "restrictionLines", "deepLines": "deepLines",
                 "prolongationLines": "prolongationLines", "charts_i": "charts", "cellType": "cellType",
-                "nodeType": "nodeType", "cellIndices": "cellCorners"}
+                "nodeType": "nodeType", "cellIndices": "cellCorners",
+                "interiorTexelToCellLines": "interiorTexelToCellLines"}
 
 
 def digest(a) -> str:
