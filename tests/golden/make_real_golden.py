@@ -12,7 +12,8 @@ mode).  Stored, per mesh (tests/golden/real/):
   index array, of the canonical boundary restriction (sorted CSR) and of the
   texture nodes' (ci, cj, chart, interior) columns;
 * <mesh>.npz: per-level chart corners and cell sizes, every texture node's
-  triangle id, and the barycentric coordinates of a seeded sample of nodes.
+  triangle id, the barycentric coordinates of a seeded sample of nodes, and the
+  embedding metric (InitializeMetric) of a seeded sample of triangles.
 
 The meshes themselves are not copied: the test reads them from the reference's
 data directory when it is present.
@@ -96,6 +97,11 @@ def main(ref_tree: str) -> None:
         arrays["interior"] = tn[:, 4]
         arrays["bary_rows"] = rows.astype(np.int32)
         arrays["bary"] = g["fine/textureBary"][rows]
+        pm = g["metric/parameter"]  # the reference's embedding metric, per mesh triangle
+        mrows = np.sort(np.random.default_rng(100 + len(table)).choice(len(pm), size=min(SAMPLE, len(pm)), replace=False))
+        arrays["metric_rows"] = mrows.astype(np.int32)
+        arrays["metric"] = pm[mrows]
+        arrays["metric_scale"] = np.array([np.abs(pm).max()])
         key = os.path.splitext(os.path.basename(name))[0]
         np.savez_compressed(os.path.join(OUT, f"{key}.npz"), **arrays)
         table[name] = entry

@@ -10,7 +10,9 @@ reference hierarchy on the same input (tests/golden/make_real_golden.py).
   mesh, whose nearest-triangle test is a near-tie (the reference's release
   build computes with -ffast-math, so its roundings differ in the last bit);
 * texture node barycentric coordinates (seeded sample): within 1e-13, for the
-  same reason.
+  same reason;
+* the embedding parameter metric (seeded sample of triangles): within 1e-12 of
+  its largest entry.
 
 Needs the reference's data directory (skipped otherwise); no GPU.
 """
@@ -87,3 +89,14 @@ def test_texture_and_boundary_nodes(case):
     same = np.isin(rows, differ, invert=True)
     bary = h.array("textureBary")[rows]
     np.testing.assert_allclose(bary[same], arrays["bary"][same], rtol=0, atol=1e-13)
+
+
+def test_embedding_metric(case):
+    entry, h, arrays, mk = case
+    from gradientdomaintextureprocessing_b200 import textureio
+    from gradientdomaintextureprocessing_b200.metric import InitializeMetric
+    name = next(n for n, e in TABLE.items() if e is entry)
+    mesh = textureio.ReadTexturedMesh(os.path.join(REFERENCE_DATA, name))
+    mesh, _, _, _ = textureio.prepare_filtering_mesh(mesh, mk.SIZE, mk.SIZE)
+    P = InitializeMetric(mesh).reshape(-1, 4)[arrays["metric_rows"]]
+    assert np.abs(P - arrays["metric"]).max() <= 1e-12 * arrays["metric_scale"][0]
