@@ -497,8 +497,9 @@ def main():
     # the same steps as one stream of problems (gdtp_solve_stream): every step
     # still uploads its b and downloads its x, on copy streams that overlap the
     # neighbouring steps' solves; one pinned output buffer per step
-    x_pins = [torch.zeros(b_host.shape, dtype=torch.float64).pin_memory().numpy() for _ in range(args.steps)]
-    s.solve_stream([b_pin] * 2, x_pins[:2], tol=TOL)  # slot buffers and their step graphs
+    x_pins = [torch.zeros(b_host.shape, dtype=torch.float64).pin_memory().numpy() for _ in range(max(args.steps, 2))]
+    s.solve_stream([b_pin] * 2, x_pins[:2], tol=TOL)  # slot buffers and the graphs of both slots
+    x_pins = x_pins[:args.steps]
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
