@@ -1,10 +1,17 @@
-"""Galerkin coarsening (csrc/setup/galerkin.cpp) on the reference's own meshes:
+"""Host set-up on the reference's own meshes, from the reference's own operator.
+
+Galerkin coarsening (csrc/setup/galerkin.cpp):
 the reference's fine operator M + 1e-3 S of Julius and Bunny (256 x 256 after the
 filtering app's preprocessing), from the unmodified reference (oracle/_ref/
 gdtp_ref), is coarsened by the library's code (tests/native/galerkin_check.cpp)
 and every level's deep stencils, BB and BD blocks are compared with the
 reference's UpdateLinearSystem hierarchy (UpdateCoefficients.inl:285-399) to
 1e-12 of each block's largest entry (measured ~1e-15).
+
+Exact boundary-block solve (csrc/setup/bsolve.cpp): built from the reference's
+boundary block of every level below the coarsest and applied on the host in the
+kernels' sequence (tests/native/bsolve_check.cpp); the solution agrees with a
+direct sparse solve to 1e-10 (measured 1e-16 to 1e-13).
 
 Needs the reference's data directory and the built oracle (skipped otherwise);
 no GPU.
@@ -59,19 +66,34 @@ def _rel(a, b):
     return abs(a - b).max() / max(abs(b).max(), 1e-300)
 
 
-@pytest.mark.parametrize("name", ["Julius/julius.ply", "Bunny/bunny.ply"])
-def test_galerkin_hierarchy_matches_reference(built_lib, tmp_path, name):
+def _native(tmp_path, name):
+    pkg = os.path.join(ROOT, "gradientdomaintextureprocessing_b200")
+    exe = str(tmp_path / name)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(pkg, "csrc"), "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "native", name + ".cpp"), "-L", pkg, "-lgdtp", "-Wl,-rpath," + pkg, "-o", exe],
+                   check=True)
+    return exe
+
+
+@pytest.fixture(scope="module", params=["Julius/julius.ply", "Bunny/bunny.ply"])
+def reference_case(request, built_lib, tmp_path_factory):
+    """The mesh after the app's preprocessing and the reference's dump of it."""
     import gdd
-    import port
     sys.path.insert(0, GOLDEN)
     import make_real_golden as mk
     from gradientdomaintextureprocessing_b200 import meshgen
-    mesh, _, w, h = mk.prepared(os.path.dirname(REFERENCE_DATA), name)
+    mesh, _, w, h = mk.prepared(os.path.dirname(REFERENCE_DATA), request.param)
     mesh["texture"] = np.zeros((h, w, 3), np.float32)
-    gdm, dump = str(tmp_path / "m.gdm"), str(tmp_path / "m.gdd")
+    tmp = tmp_path_factory.mktemp("ref")
+    gdm, dump = str(tmp / "m.gdm"), str(tmp / "m.gdd")
     meshgen.write_gdm(gdm, mesh)
     subprocess.run([REF, gdm, dump, str(LEVELS), str(LAMBDA), "2.0", "2", "dump"], check=True, capture_output=True, timeout=600)
-    g = gdd.read_dump(dump)
+    return gdm, gdd.read_dump(dump)
+
+
+def test_galerkin_hierarchy_matches_reference(reference_case, tmp_path):
+    import port
+    gdm, g = reference_case
     nt, nb = int(g["L0/counts"][0]), int(g["L0/counts"][2])
     deep0 = g["fine/deepMass"].ravel() + LAMBDA * g["fine/deepStiffness"].ravel()
     fine = tmp_path / "fine.bin"
@@ -79,11 +101,7 @@ def test_galerkin_hierarchy_matches_reference(built_lib, tmp_path, name):
         f.write(struct.pack("<q", len(deep0)) + deep0.astype("<f8").tobytes())
         _write_csr(f, _csr(g, "fine/BBmass") + LAMBDA * _csr(g, "fine/BBstiffness"), nb)
         _write_csr(f, _csr(g, "fine/BDmass") + LAMBDA * _csr(g, "fine/BDstiffness"), nt)
-    pkg = os.path.join(ROOT, "gradientdomaintextureprocessing_b200")
-    exe = str(tmp_path / "galerkin_check")
-    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(pkg, "csrc"), "-I", os.path.join(ROOT, "include"),
-                    os.path.join(ROOT, "tests", "native", "galerkin_check.cpp"), "-L", pkg, "-lgdtp", "-Wl,-rpath," + pkg,
-                    "-o", exe], check=True)
+    exe = _native(tmp_path, "galerkin_check")
     out = tmp_path / "out.bin"
     r = subprocess.run([exe, gdm, str(LEVELS), str(fine), str(out)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
@@ -100,3 +118,23 @@ def test_galerkin_hierarchy_matches_reference(built_lib, tmp_path, name):
         assert np.abs(mine[:, :cols] - ref[:, :cols]).max() <= 1e-12 * np.abs(ref[:, :cols]).max(), l
         assert _rel(bb, _csr(g, f"L{l}/coef/BB")) <= 1e-12, l
         assert _rel(bd, _csr(g, f"L{l}/coef/BD")) <= 1e-12, l
+
+
+def test_boundary_solve_on_reference_blocks(reference_case, tmp_path):
+    from scipy.sparse.linalg import spsolve
+    _, g = reference_case
+    exe = _native(tmp_path, "bsolve_check")
+    for l in range(LEVELS - 1):
+        BB = _csr(g, f"L{l}/coef/BB").tocsr()
+        BB.sort_indices()
+        n = BB.shape[0]
+        r = np.random.default_rng(l).normal(size=n)
+        inp, out = tmp_path / "in.bin", tmp_path / "out.bin"
+        with open(inp, "wb") as f:
+            _write_csr(f, BB, n)
+            f.write(struct.pack("<q", n) + r.astype("<f8").tobytes())
+        p = subprocess.run([exe, str(inp), str(out)], capture_output=True, text=True, timeout=600)
+        assert p.returncode == 0, p.stdout + p.stderr
+        x = np.fromfile(out, "<f8")
+        xd = spsolve(BB.tocsc(), r)
+        assert np.linalg.norm(x - xd) <= 1e-10 * np.linalg.norm(xd), (l, p.stdout)
