@@ -138,3 +138,35 @@ def test_boundary_solve_on_reference_blocks(reference_case, tmp_path):
         x = np.fromfile(out, "<f8")
         xd = spsolve(BB.tocsc(), r)
         assert np.linalg.norm(x - xd) <= 1e-10 * np.linalg.norm(xd), (l, p.stdout)
+
+
+def test_coarsest_level_operator_and_inverse(reference_case, tmp_path):
+    """The coarsest level: the full operator that full_matrix assembles from the
+    reference's coarsest coefficients equals the oracle port's assembly of them
+    (oracle/port.py full_matrix), and its Jacobi-scaled dense inverse solves it
+    to 1e-10 of a direct sparse solve."""
+    import port
+    from scipy.sparse.linalg import spsolve
+    gdm, g = reference_case
+    exe = _native(tmp_path, "coarse_check")
+    l = LEVELS - 1
+    deep = np.ascontiguousarray(g[f"L{l}/coef/deep"], np.float64)
+    nb, nt = int(g[f"L{l}/counts"][2]), int(g[f"L{l}/counts"][0])
+    BB, BD = _csr(g, f"L{l}/coef/BB"), _csr(g, f"L{l}/coef/BD")
+    r = np.random.default_rng(5).normal(size=nt)
+    inp, out = tmp_path / "in.bin", tmp_path / "out.bin"
+    with open(inp, "wb") as f:
+        f.write(struct.pack("<q", deep.size) + deep.astype("<f8").tobytes())
+        _write_csr(f, BB, nb)
+        _write_csr(f, BD, nt)
+        f.write(struct.pack("<q", nt) + r.astype("<f8").tobytes())
+    p = subprocess.run([exe, gdm, str(LEVELS), str(inp), str(out)], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout + p.stderr
+    b = out.read_bytes()
+    full, o = _read_csr(b, 0)
+    x = np.frombuffer(b, "<f8", nt, o)
+    ref = port.full_matrix(g[f"L{l}/nodeinfo"], g[f"L{l}/deepGlobalIndex"], g[f"L{l}/boundaryGlobalIndex"], deep,
+                           _csr(g, f"L{l}/coef/BB"), _csr(g, f"L{l}/coef/BD"))
+    assert _rel(full, ref.tocsr()) <= 1e-15
+    xd = spsolve(ref.tocsc(), r)
+    assert np.linalg.norm(x - xd) <= 1e-10 * np.linalg.norm(xd)
