@@ -43,7 +43,7 @@ METRIC = "Mtexels solved/s at 1e-6 rel. residual, mixed vs FP64; p50/p99 latency
 WIDTH = 2048
 LAMBDA, SHARP, TOL, K = 1e-3, 2.0, 1e-6, 3
 # DRAM bytes (read + write) per deep texel of one level-0 4-colour sweep, from an
-# ncu capture of k_gs_colour on this workload (cold L2; profiles/gs_colour_icosphere2048.md)
+# ncu capture of k_gs_colour on this workload (cold L2)
 NCU_SWEEP_BYTES_PER_DEEP_TEXEL = 4 * 48.68e6 / 1432006
 
 

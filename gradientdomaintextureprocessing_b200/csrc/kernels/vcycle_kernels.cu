@@ -713,33 +713,50 @@ void launch_coarse_solve(int n, const double* ainv, const double* scale, const T
 
 static inline int raw_groups(int K) { int G = 1; while (4 * G < K) G *= 2; return G; }
 // fixed grid (grid-stride): bounded number of partial sums, launch-shape-independent order
-static const int kRawBlocks = 148 * 8;
+// Fixed grid of the FP64 operator and its reductions: 8 blocks per SM of the
+// device (its partial sums are added in block order, so one device always gives
+// the same bits), at most kRawMaxBlocks.
+static int raw_blocks() {
+  static std::atomic<int> slots[kMaxDevices];
+  static const bool init = [] {
+    for (auto& a : slots) a.store(kUnset);
+    return true;
+  }();
+  (void)init;
+  return per_device_once(slots, [] {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        sms <= 0)
+      return kRawMaxBlocks;
+    return std::min(kRawMaxBlocks, 8 * sms);
+  });
+}
 void launch_raw_operator(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr, const int* bCol,
                          const double* bVal, const int* bGlobal, int nB, const double* b, const double* x, double* out, int K,
                          int mode, double* partials, double* sums, cudaStream_t s) {
   const int G = raw_groups(K);
   const long long items = (long long)nRuns * 32 * G + (long long)nB * G;
   if (items == 0) return;
-  const int blocks = int(std::min<long long>(kRawBlocks, nblk(items)));
+  const int blocks = int(std::min<long long>(raw_blocks(), nblk(items)));
   launch(k_raw_operator, dim3(blocks), s, runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, out, K, G, mode,
          partials, (float*)nullptr, 0);
   if (partials && sums) launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
 }
-int raw_operator_blocks(int nRuns, int nB, int K) { return kRawBlocks; }
+int raw_operator_blocks(int nRuns, int nB, int K) { return raw_blocks(); }
 void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr,
                              const int* bCol, const double* bVal, const int* bGlobal, int nB, const double* b, const double* x,
                              float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s) {
   const int G = raw_groups(K);
   const long long items = (long long)nRuns * 32 * G + (long long)nB * G;
   if (items == 0) return;
-  const int blocks = int(std::min<long long>(kRawBlocks, nblk(items)));
+  const int blocks = int(std::min<long long>(raw_blocks(), nblk(items)));
   launch(k_raw_operator, dim3(blocks), s, runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, (double*)nullptr, K,
          G, 0, partials, rhs32, KP);
   if (partials && sums) launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
 }
 
 // ---- flexible CG steps (fixed grids: partial sums in a fixed order)
-static inline int fcg_blocks(long long n, int G) { return int(std::min<long long>(kRawBlocks, nblk(n * G))); }
+static inline int fcg_blocks(long long n, int G) { return int(std::min<long long>(raw_blocks(), nblk(n * G))); }
 void launch_fcg_precond(long long n, int K, int KP, float* e, const double* r, const double* q, double* z, double* partials,
                         double* sums, double* sc, cudaStream_t s) {
   const int G = raw_groups(K), blocks = fcg_blocks(n, G);
@@ -765,7 +782,7 @@ void launch_raw_apply_dot(const ColourRun* runs, int nRuns, const double* coef, 
   const int G = raw_groups(K);
   const long long items = (long long)nRuns * 32 * G + (long long)nB * G;
   if (items == 0) return;
-  const int blocks = int(std::min<long long>(kRawBlocks, nblk(items)));
+  const int blocks = int(std::min<long long>(raw_blocks(), nblk(items)));
   launch(k_raw_operator, dim3(blocks), s, runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, (const double*)nullptr, x,
          out, K, G, 2, partials, (float*)nullptr, 0);
   launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);

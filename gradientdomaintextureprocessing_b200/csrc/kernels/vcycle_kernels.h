@@ -102,6 +102,9 @@ void launch_coarse_solve(int n, const double* ainv, const double* scale, const T
 void launch_raw_operator(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr, const int* bCol,
                          const double* bVal, const int* bGlobal, int nB, const double* b, const double* x, double* out, int K,
                          int mode, double* partials, double* sums, cudaStream_t s);
+// Blocks of the FP64 operator's fixed grid on the current device (8 per SM, at
+// most kRawMaxBlocks): the partial-sum buffers hold this many blocks x 2K.
+constexpr int kRawMaxBlocks = 2048;
 int raw_operator_blocks(int nRuns, int nB, int K);
 // r = b - A x written as the padded FP32 right-hand side (n x KP), plus norms
 void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr,

@@ -10,28 +10,44 @@
 // of in memory allocated by the library.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <string>
 
 #include "gdtp.h"
 #include "capi_internal.h"
+#include "kernels/vcycle_kernels.h"
 #include "system.h"
 
 namespace {
 
 // Upper bounds of the static scratch: the operator kernel runs a fixed grid of
-// at most kStaticBlocks blocks, each writing 2*k partial sums, plus 2*k totals.
+// at most kRawMaxBlocks blocks, each writing 2*k partial sums, plus 2*k totals.
 constexpr int kStaticMaxRhs = 64;
-constexpr int kStaticBlocks = 148 * 8;
-constexpr size_t kStaticScratch = size_t(kStaticBlocks) * 2 * kStaticMaxRhs + 2 * kStaticMaxRhs;  // doubles (~1.2 MB)
+constexpr int kStaticBlocks = gdtp::dev::kRawMaxBlocks;
+constexpr size_t kStaticScratch = size_t(kStaticBlocks) * 2 * kStaticMaxRhs + 2 * kStaticMaxRhs;  // doubles (~2.1 MB)
 
 // Held by every device that loads the library until the process exits.  In
 // host code this name is only a stand-in for the symbol: its device address is
 // looked up once per device with cudaGetSymbolAddress.
 __device__ __align__(256) double g_residual_scratch[kStaticScratch];
 
+// Device address of the array per device ordinal, published atomically: the
+// server's workers may make their first call on one device at the same time
+// (both resolve and store the same address).
 constexpr int kMaxDevices = 64;
-double* g_scratch_address[kMaxDevices] = {nullptr};
+std::atomic<double*> g_scratch_address[kMaxDevices];
+
+// Puts the caller's current device back on every return path.
+struct DeviceRestore {
+  int saved = -1;
+  DeviceRestore() {
+    if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+  }
+  ~DeviceRestore() {
+    if (saved >= 0) cudaSetDevice(saved);
+  }
+};
 
 }  // namespace
 
@@ -52,19 +68,25 @@ extern "C" int gdtp_residual_static(gdtp_system* s, const double* b_dev, const d
   if (!sys.is_updated()) return fail(GDTP_ERR_STATE, "gdtp_residual_static: system not updated");
   const int dev = sys.device();
   if (dev < 0 || dev >= kMaxDevices) return fail(GDTP_ERR_INVALID, "gdtp_residual_static: device ordinal out of range");
+  DeviceRestore restore;
   cudaError_t e = cudaSetDevice(dev);
   if (e != cudaSuccess) return fail(GDTP_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  const RawOperator& op = sys.raw_system_operator();
+  if (op.nRuns == 0 && op.nB == 0) {  // no rows: nothing to write, and no norm to report
+    for (int c = 0; c < k; c++) rel_host[c] = 0.0;
+    return GDTP_OK;
+  }
   // first call on this device: resolve the static array's device address (must
   // happen outside stream capture; later calls only launch kernels and copy)
-  if (!g_scratch_address[dev]) {
+  double* partials = g_scratch_address[dev].load(std::memory_order_acquire);
+  if (!partials) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_residual_scratch);
     if (e != cudaSuccess) return fail(GDTP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_scratch_address[dev] = static_cast<double*>(p);
+    partials = static_cast<double*>(p);
+    g_scratch_address[dev].store(partials, std::memory_order_release);
   }
-  double* partials = g_scratch_address[dev];
   double* sums = partials + size_t(kStaticBlocks) * 2 * kStaticMaxRhs;
-  const RawOperator& op = sys.raw_system_operator();
   if (dev::raw_operator_blocks(op.nRuns, op.nB, k) > kStaticBlocks)
     return fail(GDTP_ERR_INVALID, "gdtp_residual_static: operator grid exceeds the static scratch");
   cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -292,23 +292,29 @@ bool Server::warm(int model, std::string& err) {
   bool ok = admit(m, lk, err);
   if (ok) {
     lk.unlock();
-    ok = build_device(m, err);
-    // settle the multigrid and work buffers with one zero-right-hand-side solve per system
-    if (ok) {
-      const size_t n = m.h->levels[0].numTexels;
-      const int k = m.kind == kKindFilter ? 3 : 1;
-      std::vector<double> b(n * k, 0.0), x(n * k, 0.0);
-      SolveReport r;
-      if (m.kind == kKindGeodesic) {
-        std::vector<int> src(1, int(n / 2));
-        std::vector<double> d(n);
-        SolveReport r2;
-        ok = m.g->distance(*m.a, *m.b, src.data(), 1, 1e-6, 60, d.data(), r, r2);
-      } else {
-        ok = m.a->solve_mixed(b.data(), x.data(), nullptr, nullptr, k, 1e-6, 60, nullptr, r, true);
-      }
-      if (!ok) err = m.g ? m.g->error() : m.a->error();
-    }
+    // an exception here (a host allocation, say) must still clear busy and the
+    // admission below, or every later warm / submit of this model waits forever
+    ok = without_exceptions(
+        [&] {
+          if (!build_device(m, err)) return false;
+          // settle the multigrid and work buffers with one zero-right-hand-side solve per system
+          const size_t n = m.h->levels[0].numTexels;
+          const int k = m.kind == kKindFilter ? 3 : 1;
+          std::vector<double> b(n * k, 0.0), x(n * k, 0.0);
+          SolveReport r;
+          bool solved;
+          if (m.kind == kKindGeodesic) {
+            std::vector<int> src(1, int(n / 2));
+            std::vector<double> d(n);
+            SolveReport r2;
+            solved = m.g->distance(*m.a, *m.b, src.data(), 1, 1e-6, 60, d.data(), r, r2);
+          } else {
+            solved = m.a->solve_mixed(b.data(), x.data(), nullptr, nullptr, k, 1e-6, 60, nullptr, r, true);
+          }
+          if (!solved) err = m.g ? m.g->error() : m.a->error();
+          return solved;
+        },
+        err);
     lk.lock();
     builds_++;
     if (ok) {

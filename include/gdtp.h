@@ -178,12 +178,12 @@ int gdtp_residual(gdtp_system* s, const double* b, const double* x, int k, doubl
  * their own work).  No counterpart in the reference.  Device buffers b_dev,
  * x_dev (inputs) and r_dev (output residual b - A x), float64 numTexels*k;
  * rel_host receives ||b - A x|| / ||b|| per right-hand side.  k <= 64: the
- * norm reduction's scratch is a fixed ~1.2 MB static device array that every
+ * norm reduction's scratch is a fixed ~2.1 MB static device array that every
  * device loading the library holds until exit.  The first call on a device
  * resolves that array's address (cudaGetSymbolAddress) and must come before any
  * stream capture.  All calls share the array: calls that overlap on the GPU
- * race; the call waits on `stream` before returning.  Calls no cudaMalloc or
- * cudaFree. */
+ * race; the call waits on `stream` before returning.  The caller's current
+ * device is left as it was.  Calls no cudaMalloc or cudaFree. */
 int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_dev, double* r_dev, int k, double* rel_host,
                          void* stream);
 

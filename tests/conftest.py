@@ -10,6 +10,27 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
+def reference_checkout():
+    """The reference checkout: $GDTP_REFERENCE, else the one oracle/Makefile
+    compiled the oracle from (recorded in oracle/_ref/REFERENCE); None when
+    neither names an existing directory (tests that read its data then skip)."""
+    path = os.environ.get("GDTP_REFERENCE")
+    if not path:
+        try:
+            with open(os.path.join(ROOT, "oracle", "_ref", "REFERENCE")) as fh:
+                path = fh.read().strip()
+        except OSError:
+            return None
+    return path if path and os.path.isdir(path) else None
+
+
+def reference_data():
+    """The reference's Data/ directory (its shipped meshes and fields), or a path
+    that does not exist."""
+    ref = reference_checkout()
+    return os.path.join(ref, "Data") if ref else os.path.join(ROOT, "oracle", "_ref", "no-reference-checkout")
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
 

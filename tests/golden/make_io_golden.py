@@ -1,7 +1,7 @@
 """Generates the texture I/O fixtures under tests/golden/io/ (run in a checkout
 that has the reference tree and oracle/_ref/gdtp_ref_io built by oracle/Makefile):
 
-    python tests/golden/make_io_golden.py [/root/reference]
+    python tests/golden/make_io_golden.py <reference checkout>
 
 * PLY files in several encodings (ASCII with float and with double columns,
   binary little and big endian, a quad face, extra properties and elements),
@@ -181,4 +181,6 @@ def main(ref_tree: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <reference checkout>")
+    main(sys.argv[1])

@@ -1,7 +1,7 @@
 """Hierarchy fixtures on the reference's own meshes (Data/{Julius,Hand,Bunny,David}),
 run in a checkout that has the reference tree and oracle/_ref built:
 
-    python tests/golden/make_real_golden.py [/root/reference]
+    python tests/golden/make_real_golden.py <reference checkout>
 
 Each mesh goes through the filtering app's preprocessing (textureio.
 prepare_filtering_mesh: unit radius, v flipped, padding) for a 256 x 256 texture,
@@ -111,4 +111,6 @@ def main(ref_tree: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <reference checkout>")
+    main(sys.argv[1])

@@ -25,9 +25,9 @@ import numpy as np
 import pytest
 import scipy.sparse as sp
 
-from conftest import GOLDEN, ROOT
+from conftest import GOLDEN, ROOT, reference_data
 
-REFERENCE_DATA = os.environ.get("GDTP_REFERENCE_DATA", "/root/reference/Data")
+REFERENCE_DATA = reference_data()
 REF = os.path.join(ROOT, "oracle", "_ref", "gdtp_ref")
 LEVELS, LAMBDA = 4, 1e-3
 

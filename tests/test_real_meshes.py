@@ -23,10 +23,10 @@ import sys
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, reference_data
 
 REAL = os.path.join(GOLDEN, "real")
-REFERENCE_DATA = os.environ.get("GDTP_REFERENCE_DATA", "/root/reference/Data")
+REFERENCE_DATA = reference_data()
 with open(os.path.join(REAL, "real_meshes.json")) as fh:
     TABLE = json.load(fh)
 sys.path.insert(0, GOLDEN)  # make_real_golden: the digests and array names the fixtures use

@@ -21,10 +21,10 @@ import zlib
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, reference_data
 
 IO = os.path.join(GOLDEN, "io")
-REFERENCE_DATA = os.environ.get("GDTP_REFERENCE_DATA", "/root/reference/Data")
+REFERENCE_DATA = reference_data()
 
 
 @pytest.fixture(scope="module")

@@ -35,6 +35,7 @@ def test_static_residual_matches_allocating_residual(built_lib):
     r_dev = torch.empty_like(b_dev)
     stream = torch.cuda.current_stream()
     torch.cuda.synchronize()
+    device_before = torch.cuda.current_device()
     for _ in range(2):
         r_dev.fill_(float("nan"))
         rel = np.zeros(k)
@@ -42,6 +43,7 @@ def test_static_residual_matches_allocating_residual(built_lib):
                                                C.c_void_p(r_dev.data_ptr()), k, rel.ctypes.data_as(C.c_void_p),
                                                C.c_void_p(stream.cuda_stream))
         _lib.check(code)
+        assert torch.cuda.current_device() == device_before  # the caller's device is left as it was
         np.testing.assert_allclose(rel, ref, rtol=1e-12)
         r = r_dev.cpu().numpy()
         assert np.abs(r - r_ref).max() <= 1e-12 * np.abs(r_ref).max()
