@@ -15,9 +15,15 @@ One step = one solve of all 3 right-hand sides from x = 0 to relative residual
          over the timed steps (H2D of b and D2H of x inside every step, on
          copy streams that overlap the neighbouring steps' solves);
          e2e.single_call is one gdtp_solve_ex per step, copies in series.
-  --impl reference: the reference's own CPU solver (oracle/_ref/gdtp_ref: the
-         reference headers compiled unmodified) on the host cores, same mesh,
-         texture, operator and tolerance; its V-cycles are timed.
+  fp64_vcycle  the plain FP64 GPU V-cycle (gdtp_solve_fp64_device) on the same
+         device-resident problem, timed like value; mixed_over_fp64 = the ratio.
+  cpu_baseline / oracle_error: the reference's own CPU solver (oracle/_ref/
+         gdtp_ref: the reference headers compiled unmodified) run once on the
+         host cores after the timed regions, FP64 V-cycles to 1e-12: its
+         V-cycles to 1e-6 give the CPU rate, its converged iterate the FP64
+         ground truth the device solutions are measured against.
+  --impl reference: the same reference solver timed as its own arm (V-cycles
+         to 1e-6), same mesh, texture, operator and tolerance.
 
 Multi-GPU (torchrun): every rank solves its own copy (replicas, no collective on
 the solve path); value = total texels x RHS of all ranks / max-over-ranks time.
@@ -42,9 +48,6 @@ sys.path.insert(0, ROOT)
 METRIC = "Mtexels solved/s at 1e-6 rel. residual, mixed vs FP64; p50/p99 latency"
 WIDTH = 2048
 LAMBDA, SHARP, TOL, K = 1e-3, 2.0, 1e-6, 3
-# DRAM bytes (read + write) per deep texel of one level-0 4-colour sweep, from an
-# ncu capture of k_gs_colour on this workload (cold L2)
-NCU_SWEEP_BYTES_PER_DEEP_TEXEL = 4 * 48.68e6 / 1432006
 
 
 def workload(width: int = WIDTH):
@@ -177,6 +180,47 @@ def run_reference(args, rank: int) -> dict:
             "cpu_baseline": {"value": value, "unit": "Mtexels/s (texels x RHS)", "cores": cores, "kind": "reference",
                              "sample": "full workload: the reference V-cycles to 1e-6, set-up excluded"},
             "e2e": {"value": value, "unit": "Mtexels/s (texels x RHS)", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def reference_leg(mesh, s, b_dev, x_dev, x_own, stream) -> dict:
+    """The reference's CPU solver on this workload, run once (rank 0, N=1, after
+    the timed regions): the compiled reference (oracle/_ref/gdtp_ref) builds the
+    same hierarchy and operator and iterates its FP64 V-cycle to 1e-12.
+    cpu_baseline: its V-cycles up to the first at <= 1e-6, timed by the reference
+    run itself (set-up excluded).  oracle_error: energy-norm errors, in the
+    reference's FP64 operator, of the device solve of the reference's right-hand
+    side (solver error) and of this workload's own host-path solve (solver plus
+    assembly and right-hand-side differences) against the reference's solution."""
+    import ctypes as C
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference_solution as rs
+    from gradientdomaintextureprocessing_b200 import _lib
+    if not rs.available():
+        return {"cpu_baseline": {"unavailable": "oracle/_ref/gdtp_ref not built (needs the reference sources at build time)"}}
+    ref = rs.reference_solution(mesh, 4, LAMBDA, SHARP, tol=1e-12, max_vcycles=60)
+    hist, times = ref["history"], ref["vcycle_times"]
+    cycles = next((i for i in range(1, len(hist)) if hist[i] <= TOL), len(hist) - 1)
+    t_cpu = float(np.sum(times[:cycles]))
+    n0 = int(ref["counts"][0])
+    cpu = {"value": n0 * K / t_cpu / 1e6, "unit": "Mtexels/s (texels x RHS)", "cores": ref["threads"], "kind": "reference",
+           "sample": "full workload: the reference FP64 V-cycles (Vec4d, OpenMP) to 1e-6, set-up excluded",
+           "vcycles": cycles, "rel_residual": float(hist[cycles])}
+    b_ref = torch.from_numpy(np.ascontiguousarray(ref["rhs"])).to(b_dev.device)
+    x_dev.zero_()
+    rep = _lib.Report()
+    _lib.check(_lib.lib().gdtp_solve_device(s.handle, C.c_void_p(b_ref.data_ptr()), C.c_void_p(x_dev.data_ptr()), K, TOL, 60,
+                                            C.c_void_p(stream.cuda_stream), C.byref(rep)))
+    torch.cuda.synchronize()
+    x_mine = x_dev.cpu().numpy()
+    err = rs.energy_error(ref["A"], x_mine, ref["x"])
+    err_own = rs.energy_error(ref["A"], x_own, ref["x"])
+    return {"cpu_baseline": cpu,
+            "oracle_error": {"energy_norm_max": float(err.max()), "energy_norm_max_own_rhs": float(err_own.max()),
+                             "rel_residual_reference_operator": float(rs.relative_residual(ref["A"], ref["rhs"], x_mine).max()),
+                             "reference_rel_residual": float(hist[-1]),
+                             "reference": "the reference's FP64 V-cycle iterated to its residual floor on the same mesh, "
+                                          "texture and operator (oracle/_ref/gdtp_ref vsolve)"}}
 
 
 def serve(args):
@@ -464,7 +508,7 @@ def main():
         lat.append(ev[i].elapsed_time(ev[i + 1]))
     total_ms = ev[0].elapsed_time(ev[-1])
     total_ms = max_over_ranks(total_ms, dist)
-    prof = np.zeros(5)
+    prof = np.zeros(6)
     cnt = C.c_int64()
     L.gdtp_system_array(s.handle, b"profile", 0, prof.ctypes.data_as(C.c_void_p), C.byref(cnt))
     value = job_rate(world, n0 * K * args.steps, total_ms)
@@ -511,9 +555,27 @@ def main():
     e2e_value = job_rate(world, n0 * K * args.steps, e2e_ms)
     rel_stream = max(float(s.residual(b_host, x).max()) for x in (x_pins[0], x_pins[-1]))
 
-    # plain FP64 GPU V-cycle on the same problem (the comparator path), one solve
-    x64, rep64 = s.solve(b_host, tol=TOL, precision="fp64")
-    t64 = rep64["seconds"]
+    # plain FP64 GPU V-cycle on the same problem (the comparator path), timed
+    # like value: device-resident b and x, warm-up, then K solves between events
+    def fp64_step():
+        x_dev.zero_()
+        code = L.gdtp_solve_fp64_device(s.handle, C.c_void_p(b_dev.data_ptr()), C.c_void_p(x_dev.data_ptr()), K, TOL, 60,
+                                        C.c_void_p(stream.cuda_stream), C.byref(rep))
+        if code != 0:
+            _lib.check(code)
+        return rep.vcycles, rep.rel_residual_max
+
+    for _ in range(args.warmup):
+        fp64_step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    res64 = [fp64_step() for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fp64_ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    fp64_value = job_rate(world, n0 * K * args.steps, fp64_ms)
     # dominant kernel: level-0 colour Gauss-Seidel sweep (4 colour passes), timed
     # by events recorded inside the captured refinement graph: the average of
     # the full sweeps of each V-cycle (the pre-smoothing after its zero-start
@@ -526,11 +588,26 @@ def main():
     peak = float(peaks.get("hbm_gbs", 6650.0))
     sweep_ms = prof[1] / max(prof[0], 1)
     texels = prof[2]
-    # algorithmic bytes of one 4-colour sweep on level 0 (FP32, 4 channels): per
-    # deep texel 10 coefficients (40 B) + rhs (16 B) + x written once (16 B) +
-    # x read once per colour pass for the 3 other colours' values (3 x 16 B)
-    sweep_bytes = texels * (40 + 16 + 16 + 48)
+    tiled = bool(prof[5])
+    # algorithmic bytes per deep texel of one timed group (a colour sweep, or a
+    # round of the fused tile smoother): 10 FP32 coefficients (40 B) + rhs
+    # read, x read and x written once, k = 3 channels of 4 B (3 x 12 B) = 76 B
+    sweep_bytes = texels * (40 + 3 * K * 4)
+    if tiled:
+        kernel = "level-0 fused tile-smoother round (k_tile_smooth, one launch: every sweep of the round in 32x32 tiles)"
+        # moved with the padded 4-lane vectors and the one-texel ring of a tile
+        model_bytes = texels * (40 + 16 + 16 * 34 * 34 / 1024 + 16)
+    else:
+        kernel = "level-0 4-colour Gauss-Seidel sweep (k_gs_colour x4)"
+        # the 4-launch colour decomposition with padded 4-lane vectors:
+        # coefficients, rhs, x written, and the x of the three other colours
+        # read by each colour pass (40 + 16 + 16 + 3 x 16 = 120 B)
+        model_bytes = texels * (40 + 16 + 16 + 48)
     achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9 if sweep_ms > 0 else None
+    try:  # DRAM bytes per deep texel per timed group, from ncu captures of this workload
+        traffic_per_texel = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["tile" if tiled else "colour"]
+    except (OSError, ValueError, KeyError):
+        traffic_per_texel = None
     launches = int(prof[4])  # counted by the solver: graph kernel nodes x graph launches + direct launches
 
     out = {"metric": METRIC, "value": value, "unit": "Mtexels/s (texels x RHS)", "n_gpus": world, "steps": args.steps,
@@ -543,8 +620,10 @@ def main():
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
            "refinement_steps": {"mean": float(np.mean(iters)), "max": int(max(iters))},
            "rel_residual": {"device_path_max": float(max(resid)), "host_path_final": rel_final},
-           "fp64_vcycle": {"value": n0 * K / t64 / 1e6, "unit": "Mtexels/s (texels x RHS)", "vcycles": rep64["vcycles"],
-                           "rel_residual": rep64["rel_residual_max"]},
+           "fp64_vcycle": {"value": fp64_value, "unit": "Mtexels/s (texels x RHS)", "ms_per_step": fp64_ms / args.steps,
+                           "vcycles": int(max(r[0] for r in res64)), "rel_residual": float(max(r[1] for r in res64)),
+                           "api": "gdtp_solve_fp64_device (device-resident, same warm-up, steps and events as value)"},
+           "mixed_over_fp64": value / fp64_value,
            "e2e": {"value": e2e_value, "unit": "Mtexels/s (texels x RHS)", "h2d_bytes_per_step": int(b_host.nbytes),
                    "d2h_bytes_per_step": int(b_host.nbytes), "ms_per_step": e2e_ms / args.steps,
                    "api": "gdtp_solve_stream (zero initial guess, pinned host buffers, copies overlapped with the "
@@ -552,20 +631,18 @@ def main():
                    "rel_residual_max": rel_stream,
                    "single_call": {"value": single_value, "ms_per_step": single_ms / args.steps,
                                    "api": "gdtp_solve_ex per step (copies in series with the solve)"}},
-           "roofline": {"bound": "hbm", "kernel": "level-0 4-colour Gauss-Seidel sweep (k_gs_colour x4)",
+           "roofline": {"bound": "hbm", "kernel": kernel,
                         "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": (achieved / peak) if achieved else None,
-                        "traffic": texels * NCU_SWEEP_BYTES_PER_DEEP_TEXEL if texels else None,
-                        "traffic_source": "ncu dram__bytes_read+write per deep texel x deep texels (cold L2)",
+                        "traffic": texels * traffic_per_texel["bytes_per_deep_texel"] if traffic_per_texel and texels else None,
+                        "traffic_source": traffic_per_texel["source"] if traffic_per_texel else "no ncu capture recorded",
                         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                        "bytes_per_launch": sweep_bytes, "ms_per_launch": sweep_ms},
+                        "bytes_per_launch": sweep_bytes, "bytes_per_deep_texel": 40 + 3 * K * 4,
+                        "bytes_moved_model": model_bytes, "ms_per_launch": sweep_ms},
            "gpu_launches": launches,
            "clocks": clocks.summary()}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        ref = run_reference(argparse.Namespace(gpus=1, steps=1, warmup=0), 0)
-        out["cpu_baseline"] = ref.get("cpu_baseline", {"unavailable": ref.get("unavailable")})
-        if "config" in ref:
-            out["cpu_baseline"]["vcycles"] = ref["config"]["vcycles"]
+        out.update(reference_leg(mesh, s, b_dev, x_dev, x_pin, stream))
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:

@@ -49,11 +49,13 @@ _SIGS = {
     "gdtp_system_update": (C.c_int, [_P, C.c_double, C.c_double]),
     "gdtp_apply": (C.c_int, [_P, C.c_int, _P, _P, C.c_int]),
     "gdtp_vcycle": (C.c_int, [_P, _P, _P, C.c_int]),
+    "gdtp_relax": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int]),
     "gdtp_solve": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.POINTER(Report)]),
     "gdtp_solve_ex": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(Report)]),
     "gdtp_solve_stream": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_double, C.c_int, _P]),
     "gdtp_solve_device": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, _P, C.POINTER(Report)]),
     "gdtp_solve_fp64": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.POINTER(Report)]),
+    "gdtp_solve_fp64_device": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, _P, C.POINTER(Report)]),
     "gdtp_residual": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "gdtp_system_set": (C.c_int, [_P, C.c_char_p, C.c_double]),
     "gdtp_system_get": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_double)]),

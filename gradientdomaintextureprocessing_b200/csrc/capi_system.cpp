@@ -92,10 +92,11 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
       if (name.rfind("coef.bb.", 0) == 0) return emit_csr(co[level].bb, part("coef.bb."), out, count);
       if (name.rfind("coef.bd.", 0) == 0) return emit_csr(co[level].bd, part("coef.bd."), out, count);
     }
-    if (name == "profile") {  // {timed groups, total ms, deep texels per group, kernels per step graph, kernels launched}
-      double v[5] = {s->sys->profCount, s->sys->profMs, s->sys->profTexels, double(s->sys->graphKernels),
-                     double(s->sys->kernelLaunches)};
-      if (count) *count = 5;
+    if (name == "profile") {  // {timed groups, total ms, deep texels per group, kernels per step graph, kernels launched,
+                              //  1 if the timed group is one fused tile-smoother launch, else 0 (colour sweeps)}
+      double v[6] = {s->sys->profCount, s->sys->profMs, s->sys->profTexels, double(s->sys->graphKernels),
+                     double(s->sys->kernelLaunches), s->sys->profTiled() ? 1.0 : 0.0};
+      if (count) *count = 6;
       if (out) std::memcpy(out, v, sizeof(v));
       return GDTP_OK;
     }
@@ -149,6 +150,14 @@ extern "C" int gdtp_vcycle(gdtp_system* s, float* x, const float* rhs, int k) {
     GDTP_SYS_CHECK(s);
     if (!x || !rhs) return fail(GDTP_ERR_INVALID, "gdtp_vcycle: null vector");
     return s->sys->vcycle_host(x, rhs, k) ? GDTP_OK : sys_fail(s, GDTP_ERR_CUDA);
+  });
+}
+
+extern "C" int gdtp_relax(gdtp_system* s, float* x, const float* rhs, int k, int sweeps, int reverse) {
+  return guarded("gdtp_relax", [&]() -> int {
+    GDTP_SYS_CHECK(s);
+    if (!x || !rhs || sweeps < 0 || sweeps > 64) return fail(GDTP_ERR_INVALID, "gdtp_relax: bad arguments");
+    return s->sys->relax_host(x, rhs, k, sweeps, reverse != 0) ? GDTP_OK : sys_fail(s, GDTP_ERR_CUDA);
   });
 }
 
@@ -221,7 +230,20 @@ extern "C" int gdtp_solve_fp64(gdtp_system* s, const double* b, double* x, int k
     GDTP_SYS_CHECK(s);
     if (!b || !x || !(tol > 0) || max_iters < 0) return fail(GDTP_ERR_INVALID, "gdtp_solve_fp64: bad arguments");
     SolveReport rep;
-    if (!s->sys->solve_fp64(b, x, k, tol, max_iters, rep)) return sys_fail(s, GDTP_ERR_CUDA);
+    if (!s->sys->solve_fp64(b, x, nullptr, nullptr, k, tol, max_iters, nullptr, rep)) return sys_fail(s, GDTP_ERR_CUDA);
+    fill_report(report, rep);
+    return rep.relMax <= tol ? GDTP_OK : fail(GDTP_ERR_NOT_CONVERGED, "relative residual above tolerance after max_iters");
+  });
+}
+
+extern "C" int gdtp_solve_fp64_device(gdtp_system* s, const double* b_dev, double* x_dev, int k, double tol, int max_iters,
+                                      void* stream, gdtp_report* report) {
+  return guarded("gdtp_solve_fp64_device", [&]() -> int {
+    GDTP_SYS_CHECK(s);
+    if (!b_dev || !x_dev || !(tol > 0) || max_iters < 0) return fail(GDTP_ERR_INVALID, "gdtp_solve_fp64_device: bad arguments");
+    SolveReport rep;
+    if (!s->sys->solve_fp64(nullptr, nullptr, b_dev, x_dev, k, tol, max_iters, static_cast<cudaStream_t>(stream), rep))
+      return sys_fail(s, GDTP_ERR_CUDA);
     fill_report(report, rep);
     return rep.relMax <= tol ? GDTP_OK : fail(GDTP_ERR_NOT_CONVERGED, "relative residual above tolerance after max_iters");
   });
@@ -255,6 +277,9 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
     else if (k == "cluster_texels" && v >= 0) kn.clusterTexels = v;
     else if (k == "grid_texels" && v >= 0) kn.gridTexels = v;
     else if (k == "chart_texels" && v >= 0) kn.chartTexels = v;
+    else if (k == "tile_texels" && v >= 0) kn.tileTexels = v;
+    else if (k == "tile_rounds" && v >= 1 && v <= 16) kn.tileRounds = v;
+    else if (k == "tile_finish" && (v == 0 || v == 1)) kn.tileFinish = v;
     else if (k == "coarse_pre_sweeps" && v >= -1 && v <= 16) kn.coarsePreSweeps = v;
     else if (k == "coarse_post_sweeps" && v >= -1 && v <= 16) kn.coarsePostSweeps = v;
     else if (k == "coarse_from" && v >= 1 && v <= 16) kn.coarseFrom = v;
@@ -289,6 +314,9 @@ extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* v
     else if (k == "zero_start_skip") *value = kn.zeroStartSkip;
     else if (k == "grid_texels") *value = kn.gridTexels;
     else if (k == "chart_texels") *value = kn.chartTexels;
+    else if (k == "tile_texels") *value = kn.tileTexels;
+    else if (k == "tile_rounds") *value = kn.tileRounds;
+    else if (k == "tile_finish") *value = kn.tileFinish;
     else return fail(GDTP_ERR_INVALID, "gdtp_system_get: unknown knob " + k);
     return GDTP_OK;
   });

@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(kGroupBlockMax, 1) k_gs_groups(const ColourRun
 // Residual: deep rows by runs (all colours), boundary rows by CSR (global cols).
 // Blocks [0, deepBlocks) handle deep texels, the rest boundary rows.
 // ----------------------------------------------------------------------------
-template <typename T, int W>
+template <typename T, int W, typename LD = LoadDefault>
 __global__ void __launch_bounds__(256) k_residual(const ColourRun* __restrict__ runs, int nRuns, const T* __restrict__ coef,
                                                   int planeStride, int deepBlocks, const int* __restrict__ bPtr,
                                                   const int* __restrict__ bCol, const T* __restrict__ bVal,
@@ -113,8 +113,7 @@ __global__ void __launch_bounds__(256) k_residual(const ColourRun* __restrict__ 
   grid_dependency_wait();
   grid_launch_dependents();
   if ((int)blockIdx.x < deepBlocks)
-    residual_deep_item<T, W, LoadDefault>(runs, nRuns, coef, planeStride, rhs, x, res, KP, G,
-                                          (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    residual_deep_item<T, W, LD>(runs, nRuns, coef, planeStride, rhs, x, res, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
   else
     residual_boundary_item<T, W, LoadDefault>(bPtr, bCol, bVal, bGlobal, nB, rhs, x, res, KP, G,
                                               (long long)(blockIdx.x - deepBlocks) * blockDim.x + threadIdx.x);

@@ -72,6 +72,15 @@ struct LevelDev {
   T *x = nullptr, *b = nullptr, *r = nullptr;
   const int* groups = nullptr;  // per chart: first run of each colour [4], run counts [4], texel span [2]
   int nGroups = 0, maxGroupDeep = 0, maxGroupSpan = 0;
+  // fused tile smoother (launch_tile_smooth): tiles ordered by tile colour
+  // (tiles of colour c are [tileStart[c], tileStart[c + 1])), segments, FP32
+  // coefficient blocks
+  const int4* tiles = nullptr;
+  int nTiles = 0, tileStart[5] = {0, 0, 0, 0, 0};
+  const int4* tileSegs = nullptr;
+  const int* tileNbrs = nullptr;
+  const float* tileCoef = nullptr;
+  int* tileSync = nullptr;      // per multigrid (its rounds run in its stream order)
 };
 
 template <typename T, int W>
@@ -85,6 +94,36 @@ void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int plane
 constexpr size_t kGroupSmemMax = 200 * 1024;
 template <typename T, int W>
 bool launch_gs_groups(const LevelDev<T>& D, int sweeps, bool reverse, int KP, cudaStream_t s);
+// Fused smoothing round (tile_smoother.cu): tiles of kTileW x kTileH texels of
+// one chart, a CTA each, `sweeps` 4-colour sweeps in shared memory, x updated
+// in place.  Tiles are ordered by tile colour (tile column parity | tile row
+// parity << 1): colour c is [tileStart[c], tileStart[c + 1]).  A tile starts
+// once its neighbours of earlier colours (colours 0..3, or 3..0 in reverse)
+// are done.  tiles[t] = {first coefficient of the tile, first segment, segment
+// count (<= kTileMaxSegs), element count}; coefficients: 10 planes of
+// kTileSlots per tile, slot = colour * kTileSlots / 4 + (j / 2) * kTileW / 2 +
+// i / 2 for tile-local (i, j) of colour (i & 1) | (j & 1) << 1, zeros where
+// the texel is not deep; segs[s] = {global texel of the first element, row r |
+// first column u0 << 6 | length << 12, first element of the segment in the
+// tile, 0}: runs of consecutive global texels on one row of the tile with its
+// one-texel ring (r, u0 in 0 .. size + 1), in row order; nbrs: 8 neighbour
+// tiles per tile (-1: none); sync: 2 + nTiles ints, zero (the kernel leaves
+// them zero); err: set to 2 when a wait for a neighbour timed out.
+// zeroStart: x = 0 on entry.  KP = 1 or 4; false if not launched.
+constexpr int kTileW = 32, kTileH = 32, kTileSlots = kTileW * kTileH;
+constexpr int kTileMaxSegs = (kTileH + 2) * (kTileW / 2 + 1);  // every other ring texel active
+struct TileRound {
+  const int4* tiles;
+  const int4* segs;
+  const int* nbrs;
+  const float* coef;
+  const float* rhs;
+  int* sync;
+  unsigned int* err;
+  int nTiles, tileStart[5];
+  int sweeps, reverse, zeroStart;
+};
+bool launch_tile_smooth(const TileRound& round, float* x, int KP, cudaStream_t s);
 template <typename T, int W>
 void launch_residual(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const int* bPtr, const int* bCol,
                      const T* bVal, const int* bGlobal, int nB, const T* rhs, const T* x, T* res, int KP, cudaStream_t s);

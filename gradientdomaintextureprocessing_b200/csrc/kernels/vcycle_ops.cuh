@@ -18,11 +18,19 @@ namespace dev {
 struct LoadDefault {
   template <typename T, int W>
   static __device__ __forceinline__ Vec<T, W> ld(const T* p) { return vload<T, W>(p); }
+  template <typename T>
+  static __device__ __forceinline__ T coef(const T* p) { return *p; }
+  template <typename T, int W>
+  static __device__ __forceinline__ void st(T* p, const Vec<T, W>& v) { vstore<T, W>(p, v); }
 };
 
 struct LoadL2 {
   template <typename T, int W>
   static __device__ __forceinline__ Vec<T, W> ld(const T* p);
+  template <typename T>
+  static __device__ __forceinline__ T coef(const T* p) { return *p; }
+  template <typename T, int W>
+  static __device__ __forceinline__ void st(T* p, const Vec<T, W>& v) { vstore<T, W>(p, v); }
 };
 template <>
 __device__ __forceinline__ Vec<float, 4> LoadL2::ld<float, 4>(const float* p) {
@@ -88,20 +96,20 @@ __device__ __forceinline__ void gs_item(const ColourRun* runs, int nRuns, const 
 #pragma unroll
   for (int k = 0; k < W; k++) acc.v[k] = 0;
   // skip: neighbour slots known to hold exact zeros (their terms add nothing)
-  if (!(skip & 1)) axpy(acc, c[0 * planeStride], LD::template ld<T, W>(x + (long long)(pp - 1) * KP + off));
-  if (!(skip & 2)) axpy(acc, c[1 * planeStride], LD::template ld<T, W>(x + (long long)(pp)*KP + off));
-  if (!(skip & 4)) axpy(acc, c[2 * planeStride], LD::template ld<T, W>(x + (long long)(pp + 1) * KP + off));
-  if (!(skip & 8)) axpy(acc, c[3 * planeStride], LD::template ld<T, W>(x + (long long)(pos - 1) * KP + off));
-  if (!(skip & 32)) axpy(acc, c[5 * planeStride], LD::template ld<T, W>(x + (long long)(pos + 1) * KP + off));
-  if (!(skip & 64)) axpy(acc, c[6 * planeStride], LD::template ld<T, W>(x + (long long)(pn - 1) * KP + off));
-  if (!(skip & 128)) axpy(acc, c[7 * planeStride], LD::template ld<T, W>(x + (long long)(pn)*KP + off));
-  if (!(skip & 256)) axpy(acc, c[8 * planeStride], LD::template ld<T, W>(x + (long long)(pn + 1) * KP + off));
-  const T c4 = c[4 * planeStride];
+  if (!(skip & 1)) axpy(acc, LD::coef(c + 0 * planeStride), LD::template ld<T, W>(x + (long long)(pp - 1) * KP + off));
+  if (!(skip & 2)) axpy(acc, LD::coef(c + 1 * planeStride), LD::template ld<T, W>(x + (long long)(pp)*KP + off));
+  if (!(skip & 4)) axpy(acc, LD::coef(c + 2 * planeStride), LD::template ld<T, W>(x + (long long)(pp + 1) * KP + off));
+  if (!(skip & 8)) axpy(acc, LD::coef(c + 3 * planeStride), LD::template ld<T, W>(x + (long long)(pos - 1) * KP + off));
+  if (!(skip & 32)) axpy(acc, LD::coef(c + 5 * planeStride), LD::template ld<T, W>(x + (long long)(pos + 1) * KP + off));
+  if (!(skip & 64)) axpy(acc, LD::coef(c + 6 * planeStride), LD::template ld<T, W>(x + (long long)(pn - 1) * KP + off));
+  if (!(skip & 128)) axpy(acc, LD::coef(c + 7 * planeStride), LD::template ld<T, W>(x + (long long)(pn)*KP + off));
+  if (!(skip & 256)) axpy(acc, LD::coef(c + 8 * planeStride), LD::template ld<T, W>(x + (long long)(pn + 1) * KP + off));
+  const T c4 = LD::coef(c + 4 * planeStride);
   const Vec<T, W> b = LD::template ld<T, W>(rhs + (long long)pos * KP + off);
   Vec<T, W> out;
 #pragma unroll
   for (int k = 0; k < W; k++) out.v[k] = b.v[k] * c4 - acc.v[k];
-  vstore<T, W>(x + (long long)pos * KP + off, out);
+  LD::template st<T, W>(x + (long long)pos * KP + off, out);
 }
 
 // Deep residual r = rhs - (sum_{k!=4} c_k x_k + x) * c9 (IterativeSolvers.inl:479-493).
@@ -120,15 +128,15 @@ __device__ __forceinline__ void residual_deep_item(const ColourRun* runs, int nR
   const T* c = coef + R.coef0 + m;
   const int off = q * W;
   Vec<T, W> acc = LD::template ld<T, W>(x + (long long)pos * KP + off);
-  axpy(acc, c[0 * planeStride], LD::template ld<T, W>(x + (long long)(pp - 1) * KP + off));
-  axpy(acc, c[1 * planeStride], LD::template ld<T, W>(x + (long long)(pp)*KP + off));
-  axpy(acc, c[2 * planeStride], LD::template ld<T, W>(x + (long long)(pp + 1) * KP + off));
-  axpy(acc, c[3 * planeStride], LD::template ld<T, W>(x + (long long)(pos - 1) * KP + off));
-  axpy(acc, c[5 * planeStride], LD::template ld<T, W>(x + (long long)(pos + 1) * KP + off));
-  axpy(acc, c[6 * planeStride], LD::template ld<T, W>(x + (long long)(pn - 1) * KP + off));
-  axpy(acc, c[7 * planeStride], LD::template ld<T, W>(x + (long long)(pn)*KP + off));
-  axpy(acc, c[8 * planeStride], LD::template ld<T, W>(x + (long long)(pn + 1) * KP + off));
-  const T c9 = c[9 * planeStride];
+  axpy(acc, LD::coef(c + 0 * planeStride), LD::template ld<T, W>(x + (long long)(pp - 1) * KP + off));
+  axpy(acc, LD::coef(c + 1 * planeStride), LD::template ld<T, W>(x + (long long)(pp)*KP + off));
+  axpy(acc, LD::coef(c + 2 * planeStride), LD::template ld<T, W>(x + (long long)(pp + 1) * KP + off));
+  axpy(acc, LD::coef(c + 3 * planeStride), LD::template ld<T, W>(x + (long long)(pos - 1) * KP + off));
+  axpy(acc, LD::coef(c + 5 * planeStride), LD::template ld<T, W>(x + (long long)(pos + 1) * KP + off));
+  axpy(acc, LD::coef(c + 6 * planeStride), LD::template ld<T, W>(x + (long long)(pn - 1) * KP + off));
+  axpy(acc, LD::coef(c + 7 * planeStride), LD::template ld<T, W>(x + (long long)(pn)*KP + off));
+  axpy(acc, LD::coef(c + 8 * planeStride), LD::template ld<T, W>(x + (long long)(pn + 1) * KP + off));
+  const T c9 = LD::coef(c + 9 * planeStride);
   const Vec<T, W> b = LD::template ld<T, W>(rhs + (long long)pos * KP + off);
   Vec<T, W> out;
 #pragma unroll

@@ -17,6 +17,10 @@
 #include <cmath>
 #include <cstring>
 
+#include <map>
+#include <stdexcept>
+#include <tuple>
+
 #include "system.h"
 
 namespace gdtp {
@@ -130,6 +134,103 @@ static bool chart_groups(const GridLevel& L, const DeepRuns& R, std::vector<int>
     maxSpan = std::max(maxSpan, hi - lo + 1);
   }
   return !grp.empty();
+}
+
+// Levels with at least this many deep texels get tiles for the fused smoother
+// (the tile_texels knob then chooses where they are used).
+static constexpr int kTileBuildMin = 4096;
+
+// Tiles of the fused smoother over one level: kTileW x kTileH texels of a
+// chart's grid with origins at multiples of the tile size, every tile holding
+// at least one active texel.  Per tile the reciprocal-form coefficients of its
+// deep texels (the colour-run planes' arithmetic: c_k / c_4, 1 / c_4, c_4; zeros
+// elsewhere) and the runs of consecutive global texels on each row of the tile
+// with its one-texel ring (the layout launch_tile_smooth documents).
+struct TileLayout {
+  std::vector<int4> tiles;              // ordered by tile colour
+  int tileStart[5] = {0, 0, 0, 0, 0};
+  std::vector<int4> segs;
+  std::vector<int> nbrs;                // 8 per tile: the tiles around it (-1: none)
+  std::vector<float> coef;
+};
+static void build_tiles(const GridLevel& G, const LevelCoefficients& C, TileLayout& T) {
+  using dev::kTileH;
+  using dev::kTileSlots;
+  using dev::kTileW;
+  constexpr int perColour = kTileSlots / 4, halfW = kTileW / 2;
+  std::vector<int4> byColour[4];
+  std::vector<int3> where[4];           // chart, tile column, tile row of each tile
+  for (int ch = 0; ch < (int)G.charts.size(); ch++) {
+    const GridChart& gc = G.charts[ch];
+    const int w = gc.width, h = gc.height;
+    auto texel = [&](int i, int j) { return (i < 0 || j < 0 || i >= w || j >= h) ? -1 : gc.texel[gc.at(i, j)]; };
+    for (int j0 = 0; j0 < h; j0 += kTileH)
+      for (int i0 = 0; i0 < w; i0 += kTileW) {
+        bool any = false;
+        for (int j = j0; j < std::min(h, j0 + kTileH) && !any; j++)
+          for (int i = i0; i < std::min(w, i0 + kTileW) && !any; i++) any = texel(i, j) >= 0;
+        if (!any) continue;
+        int4 tile;
+        tile.x = (int)T.coef.size();
+        tile.y = (int)T.segs.size();
+        T.coef.resize(T.coef.size() + size_t(10) * kTileSlots, 0.f);
+        float* block = T.coef.data() + tile.x;
+        for (int cc = 0; cc < 4; cc++)
+          for (int q = 0; q < kTileH / 2; q++)
+            for (int p = 0; p < halfW; p++) {
+              const int i = i0 + 2 * p + (cc & 1), j = j0 + 2 * q + (cc >> 1);
+              if (i >= w || j >= h) continue;
+              const int d = gc.deepTexel[gc.at(i, j)];
+              if (d < 0) continue;
+              const double* c = &C.deep[10 * size_t(d)];
+              const double c4 = c[4], inv = 1.0 / c4;
+              const int slot = cc * perColour + q * halfW + p;
+              for (int k = 0; k < 9; k++) block[size_t(k) * kTileSlots + slot] = float(k == 4 ? inv : c[k] * inv);
+              block[size_t(9) * kTileSlots + slot] = float(c4);
+            }
+        int elems = 0;
+        for (int r = 0; r <= kTileH + 1; r++) {
+          const int j = j0 - 1 + r;
+          for (int u = 0; u <= kTileW + 1;) {
+            const int g0 = texel(i0 - 1 + u, j);
+            if (g0 < 0) { u++; continue; }
+            int len = 1;
+            while (u + len <= kTileW + 1 && texel(i0 - 1 + u + len, j) == g0 + len) len++;
+            T.segs.push_back(make_int4(g0, r | (u << 6) | (len << 12), elems, 0));
+            elems += len;
+            u += len;
+          }
+        }
+        tile.z = (int)T.segs.size() - tile.y;
+        tile.w = elems;
+        // a ring row holds at most every other texel as its own segment
+        if (tile.z > dev::kTileMaxSegs) throw std::logic_error("tile segment bound exceeded");
+        const int colour = ((i0 / kTileW) & 1) | (((j0 / kTileH) & 1) << 1);
+        byColour[colour].push_back(tile);
+        where[colour].push_back(make_int3(ch, i0 / kTileW, j0 / kTileH));
+      }
+  }
+  std::map<std::tuple<int, int, int>, int> index;
+  std::vector<int3> at;
+  for (int c = 0; c < 4; c++) {
+    T.tileStart[c] = (int)T.tiles.size();
+    for (size_t k = 0; k < byColour[c].size(); k++) {
+      index[std::make_tuple(where[c][k].x, where[c][k].y, where[c][k].z)] = (int)T.tiles.size();
+      T.tiles.push_back(byColour[c][k]);
+      at.push_back(where[c][k]);
+    }
+  }
+  T.tileStart[4] = (int)T.tiles.size();
+  T.nbrs.assign(size_t(8) * T.tiles.size(), -1);
+  for (size_t t = 0; t < T.tiles.size(); t++) {
+    int k = 0;
+    for (int dj = -1; dj <= 1; dj++)
+      for (int di = -1; di <= 1; di++) {
+        if (!di && !dj) continue;
+        auto it = index.find(std::make_tuple(at[t].x, at[t].y + di, at[t].z + dj));
+        T.nbrs[8 * t + k++] = it == index.end() ? -1 : it->second;
+      }
+  }
 }
 
 DeviceSystem::DeviceSystem(const Hierarchy& h, const BoundaryElements& be, int device) : h_(h), be_(be), device_(device) {
@@ -444,6 +545,18 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     std::copy(R.runStart, R.runStart + 5, D.runStart);
     D.coef = A.upload(planes);
     D.planeStride = R.count;
+    // tiles of the fused smoother (FP32 levels with enough deep texels)
+    if (sizeof(T) == 4 && G.numDeep >= kTileBuildMin) {
+      TileLayout TL;
+      build_tiles(G, C, TL);
+      D.tiles = A.upload(TL.tiles);
+      D.nTiles = (int)TL.tiles.size();
+      D.tileSegs = A.upload(TL.segs);
+      D.tileCoef = A.upload(TL.coef);
+      D.tileNbrs = A.upload(TL.nbrs);
+      D.tileSync = A.zeros<int>(2 + TL.tiles.size());
+      std::copy(TL.tileStart, TL.tileStart + 5, D.tileStart);
+    }
     // chart groups of the runs (grouped smoother): deep texels of different
     // charts never neighbour each other, so during Gauss-Seidel sweeps (which
     // leave boundary texels alone) every chart is independent
@@ -617,6 +730,7 @@ bool DeviceSystem::derive_multigrid(const Multigrid<T>& base, Multigrid<T>& mg, 
     D.x = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
     D.b = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
     D.r = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
+    if (D.nTiles > 0) D.tileSync = A.zeros<int>(2 + size_t(D.nTiles));
     dev::BoundaryDev<T>& B = D.B;
     if (B.nb == 0) continue;
     B.subPart = static_cast<T*>(A.alloc(size_t(std::max(1, B.nSubTasks)) * B.subChunks * 128 * KP * sizeof(T)));
@@ -686,7 +800,7 @@ void DeviceSystem::trace_mark(int i, cudaStream_t s) {
 // results and checked once the stream is done.
 template <typename T>
 void DeviceSystem::queue_barrier_check(Multigrid<T>& mg, cudaStream_t s) {
-  if (!usedGridBarrier_ || !mg.barrier) return;
+  if (!(usedGridBarrier_ || usedTileWait_) || !mg.barrier) return;
   if (!barrierErrHost_ && cudaMallocHost(&barrierErrHost_, sizeof(unsigned int)) != cudaSuccess) {
     barrierErrHost_ = nullptr;
     return;
@@ -696,9 +810,11 @@ void DeviceSystem::queue_barrier_check(Multigrid<T>& mg, cudaStream_t s) {
 }
 template <typename T>
 bool DeviceSystem::barrier_ok(Multigrid<T>& mg) {
-  if (!usedGridBarrier_ || !mg.barrier || !barrierErrHost_ || *barrierErrHost_ == 0) return true;
+  if (!(usedGridBarrier_ || usedTileWait_) || !mg.barrier || !barrierErrHost_ || *barrierErrHost_ == 0) return true;
+  const unsigned int code = *barrierErrHost_;
   cudaMemset(mg.barrier, 0, sizeof(dev::GridBarrierState));  // usable again for the next solve
-  err_ = "coarse-level kernel: a grid barrier timed out (results discarded)";
+  err_ = code == 2 ? "tile smoother: a wait for a neighbouring tile timed out (results discarded)"
+                   : "coarse-level kernel: a grid barrier timed out (results discarded)";
   return false;
 }
 
@@ -715,6 +831,52 @@ static int zero_start_skip(int c) {
     if (nc > c) skip |= 1 << k;
   }
   return skip;
+}
+
+// One smoothing step of `sweeps` sweeps with the fused tile smoother, in
+// place: `tileRounds` rounds (one launch each) over the tiles in tile-colour
+// order (3..0 with reverse), the sweeps split between the rounds; only the
+// first round may start from a zero iterate.  With tileFinish, one global
+// colour sweep follows.
+template <typename T>
+void DeviceSystem::tile_smooth(Multigrid<T>& mg, LevelDev<T>& D, int sweeps, bool reverse, bool zeroStart, cudaStream_t s,
+                               bool prof) {
+  const int KP = mg.KP;
+  const int rounds = std::max(1, std::min(knobs.tileRounds, sweeps));
+  dev::TileRound a;
+  a.tiles = D.tiles;
+  a.segs = D.tileSegs;
+  a.nbrs = D.tileNbrs;
+  a.coef = D.tileCoef;
+  a.rhs = reinterpret_cast<const float*>(D.b);
+  a.sync = D.tileSync;
+  a.err = &mg.barrier->error;
+  a.nTiles = D.nTiles;
+  std::copy(D.tileStart, D.tileStart + 5, a.tileStart);
+  a.reverse = reverse ? 1 : 0;
+  // profiling: the rounds are timed as `rounds` launch groups (the closing
+  // colour sweep is not part of them)
+  if (prof) cudaEventRecordWithFlags(profEv_[2], s, cudaEventRecordExternal);
+  for (int r = 0; r < rounds; r++) {
+    a.sweeps = sweeps / rounds + (r < sweeps % rounds ? 1 : 0);
+    a.zeroStart = zeroStart && r == 0 ? 1 : 0;
+    dev::launch_tile_smooth(a, reinterpret_cast<float*>(D.x), KP, s);
+  }
+  if (prof) {
+    cudaEventRecordWithFlags(profEv_[3], s, cudaEventRecordExternal);
+    profPostSweeps_ = rounds;
+    profTiled_ = true;
+  }
+  usedTileWait_ = true;
+  if (knobs.tileFinish) {
+    for (int p = 0; p < 4; p++) {
+      const int c = reverse ? 3 - p : p;
+      if (KP % 4 == 0)
+        dev::launch_gs_colour<T, 4>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
+      else
+        dev::launch_gs_colour<T, 1>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
+    }
+  }
 }
 
 template <typename T, int W>
@@ -736,19 +898,23 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
                              knobs.preBoundary, knobs.postBoundary};
   dev::GridBarrierState* barrier = grid ? mg.barrier : nullptr;
   trace_mark(0, s);
+  if (profiling_) profSweeps_ = profPostSweeps_ = 0;
   for (int l = 0; l < lc; l++) {
     LevelDev<T>& D = mg.levels[l];
     LevelDev<T>& C = mg.levels[l + 1];
     // D.x of levels > 0 was cleared by the restriction into this level
     if (knobs.preBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
-    if (grouped(D, KP) && pre_sweeps(l) > 0) {
+    if (tiled(D, KP) && pre_sweeps(l) > 0) {
+      // x = 0 on entry (a refinement step's correction, or a level entered
+      // through the restriction) unless a boundary solve ran first
+      tile_smooth(mg, D, pre_sweeps(l), false, (l > 0 || zeroStart) && !knobs.preBoundary, s, false);
+    } else if (grouped(D, KP) && pre_sweeps(l) > 0) {
       dev::launch_gs_groups<T, W>(D, pre_sweeps(l), false, KP, s);
     } else {
       // timed on level 0: every full sweep (all but a first sweep that skips
       // zeros), here and in the post-smoothing; the sweep average is reported
-      const bool fromZero0 = zeroStart && knobs.zeroStartSkip && l == 0;
+      const bool fromZero0 = zeroStart && knobs.zeroStartSkip && l == 0 && !knobs.preBoundary;
       const int firstFull = fromZero0 ? 1 : 0;
-      if (profiling_ && l == 0) profSweeps_ = 0;
       for (int sw = 0; sw < pre_sweeps(l); sw++) {
         const bool prof = profiling_ && l == 0;
         if (prof && sw == firstFull) cudaEventRecordWithFlags(profEv_[0], s, cudaEventRecordExternal);
@@ -795,11 +961,14 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
     LevelDev<T>& D = mg.levels[l];
     dev::launch_prolong_add<T, W>(D.pruns, D.nPRuns, mg.levels[l + 1].x, D.x, KP, s);
     if (knobs.postBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
-    if (grouped(D, KP) && post_sweeps(l) > 0) {
+    if (tiled(D, KP) && post_sweeps(l) > 0) {
+      // timed on level 0: the post-smoothing rounds (coefficients, rhs, x read
+      // and written once each per round)
+      tile_smooth(mg, D, post_sweeps(l), true, false, s, profiling_ && l == 0);
+    } else if (grouped(D, KP) && post_sweeps(l) > 0) {
       dev::launch_gs_groups<T, W>(D, post_sweeps(l), true, KP, s);
     } else {
       const bool prof = profiling_ && l == 0 && post_sweeps(l) > 0;
-      if (profiling_ && l == 0) profPostSweeps_ = 0;
       if (prof) cudaEventRecordWithFlags(profEv_[2], s, cudaEventRecordExternal);
       for (int sw = 0; sw < post_sweeps(l); sw++)
         for (int c = 3; c >= 0; c--)
@@ -808,6 +977,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
       if (prof) {
         cudaEventRecordWithFlags(profEv_[3], s, cudaEventRecordExternal);
         profPostSweeps_ = post_sweeps(l);
+        profTiled_ = false;
       }
     }
     trace_mark(L + 1 + (L - 2 - l), s);
@@ -903,6 +1073,47 @@ bool DeviceSystem::residual_host(const double* b, const double* x, int k, double
       !raw_apply_dev(rawA_, b64_, x64_, r64_, k, 0, stream_, sumsHost_))
     return false;
   for (int c = 0; c < k; c++) rel[c] = std::sqrt(sumsHost_[c] / std::max(sumsHost_[k + c], 1e-300));
+  return true;
+}
+
+bool DeviceSystem::relax_host(float* x, const float* rhs, int k, int sweeps, bool reverse) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (!updated_) { err_ = "relax before update"; return false; }
+  if (k < 1 || k > 64 || sweeps < 0 || sweeps > 64) { err_ = "k must be in [1, 64] and sweeps in [0, 64]"; return false; }
+  Multigrid<float>* mgp = mg32_for(kp_for(k));
+  if (!mgp) return false;
+  Multigrid<float>& mg = *mgp;
+  const size_t n = h_.levels[0].numTexels;
+  std::vector<float> px(n * mg.KP, 0.f), pb(n * mg.KP, 0.f);
+  for (size_t i = 0; i < n; i++)
+    for (int c = 0; c < k; c++) { px[i * mg.KP + c] = x[i * k + c]; pb[i * mg.KP + c] = rhs[i * k + c]; }
+  LevelDev<float>& D0 = mg.levels[0];
+  if (!check(cudaMemcpyAsync(D0.x, px.data(), px.size() * 4, cudaMemcpyHostToDevice, stream_), "h2d") ||
+      !check(cudaMemcpyAsync(D0.b, pb.data(), pb.size() * 4, cudaMemcpyHostToDevice, stream_), "h2d"))
+    return false;
+  if (tiled(D0, mg.KP)) {
+    if (sweeps > 0) tile_smooth(mg, D0, sweeps, reverse, false, stream_, false);
+  } else {
+    const int W = (mg.KP % 4 == 0) ? 4 : 1;
+    for (int sw = 0; sw < sweeps; sw++)
+      for (int p = 0; p < 4; p++) {
+        const int c = reverse ? 3 - p : p;
+        if (W == 4)
+          dev::launch_gs_colour<float, 4>(D0.runs + D0.runStart[c], D0.runStart[c + 1] - D0.runStart[c], D0.coef, D0.planeStride, D0.b,
+                                          D0.x, mg.KP, stream_);
+        else
+          dev::launch_gs_colour<float, 1>(D0.runs + D0.runStart[c], D0.runStart[c + 1] - D0.runStart[c], D0.coef, D0.planeStride, D0.b,
+                                          D0.x, mg.KP, stream_);
+      }
+  }
+  queue_barrier_check(mg, stream_);
+  if (!check(cudaGetLastError(), "relax") ||
+      !check(cudaMemcpyAsync(px.data(), D0.x, px.size() * 4, cudaMemcpyDeviceToHost, stream_), "d2h") ||
+      !check(cudaStreamSynchronize(stream_), "relax") || !barrier_ok(mg))
+    return false;
+  for (size_t i = 0; i < n; i++)
+    for (int c = 0; c < k; c++) x[i * k + c] = px[i * mg.KP + c];
   return true;
 }
 
@@ -1313,12 +1524,39 @@ bool DeviceSystem::autotune(const double* b, int k, double tol, SolverKnobs& bes
       }
       if (t < bestSeconds) { bestSeconds = t; best = knobs; }
     }
+  // then, on the best setting, the fused tile smoother on the finest level (or
+  // the two finest): one round with a closing global colour sweep, or two rounds
+  const SolverKnobs colourBest = best;
+  std::vector<int> tileLevels;
+  for (int l = 0; l < 2 && l + 1 < levelsUsed_; l++)
+    if (h_.levels[l].numDeep >= kTileBuildMin) tileLevels.push_back(h_.levels[l].numDeep);
+  const int tileSweeps[][2] = {{2, 2}, {2, 3}, {3, 3}};
+  for (int threshold : tileLevels)
+    for (int variant = 0; variant < 2; variant++)
+      for (const auto& f : tileSweeps) {
+        knobs = colourBest;
+        knobs.tileTexels = threshold;
+        knobs.tileRounds = variant == 0 ? 1 : 2;
+        knobs.tileFinish = variant == 0 ? 1 : 0;
+        knobs.preSweeps = f[0];
+        knobs.postSweeps = f[1];
+        invalidate_graph();
+        double t = 1e300;
+        for (int rep = 0; rep < 3; rep++) {
+          SolveReport r;
+          if (!solve_mixed(nullptr, nullptr, bDev, xDev, k, tol, 60, nullptr, r, true)) return false;
+          if (r.relMax > tol) { t = 1e300; break; }
+          if (rep > 0) t = std::min(t, r.seconds);
+        }
+        if (t < bestSeconds) { bestSeconds = t; best = knobs; }
+      }
   knobs = best;
   invalidate_graph();
   return true;
 }
 
-bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, int k, double tol, int maxIters, SolveReport& rep) {
+bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, const double* b_dev, double* x_dev, int k, double tol,
+                              int maxIters, cudaStream_t userStream, SolveReport& rep) {
   if (!err_.empty()) return false;
   cudaSetDevice(device_);
   if (!updated_) { err_ = "solve before update"; return false; }
@@ -1336,11 +1574,19 @@ bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, int k, doubl
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  if (userStream) {
+    cudaEventRecord(e0, userStream);
+    cudaStreamWaitEvent(s, e0, 0);
+  }
   cudaEventRecord(e0, s);
-  if (!check(cudaMemcpyAsync(b64_, b_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d b") ||
-      !check(cudaMemcpyAsync(x64_, x_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d x") ||
-      !raw_apply_dev(rawA_, b64_, x64_, r64_, k, 0, s, sumsHost_))
-    return false;
+  // caller's device buffers (x holds the initial guess), or the work vectors
+  // filled from the host
+  const double* B = b_dev ? b_dev : b64_;
+  double* X = x_dev ? x_dev : x64_;
+  if (b_host && !check(cudaMemcpyAsync(b64_, b_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d b")) return false;
+  if (x_host && !check(cudaMemcpyAsync(x64_, x_host, n * k * 8, cudaMemcpyHostToDevice, s), "h2d x")) return false;
+  kernelLaunches += 2;  // operator + norm reduction
+  if (!raw_apply_dev(rawA_, B, X, r64_, k, 0, s, nullptr) || !read_norms(k, s, "initial residual")) return false;
   rep = SolveReport();
   rep.rel.assign(k, 0.0);
   auto rel_max = [&]() {
@@ -1356,21 +1602,21 @@ bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, int k, doubl
   LevelDev<double>& D0 = mg.levels[0];
   // one refinement step (rhs <- r, V-cycle, x += e, r <- b - A x and norms)
   // as a captured graph, like the mixed-precision path
-  cudaGraphExec_t step = find_graph(2, k, b64_, x64_);
+  cudaGraphExec_t step = find_graph(2, k, B, X);
   if (!step) {
     cudaGraph_t g;
     if (!check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture")) return false;
     dev::launch_pack_rhs<double>(r64_, D0.b, (long long)n, k, mg.KP, s);
     cudaMemsetAsync(D0.x, 0, n * mg.KP * sizeof(double), s);
     if (mg.KP == 1) vcycle<double, 1>(mg, s, true); else vcycle<double, 4>(mg, s, true);
-    dev::launch_add_correction<double>(x64_, D0.x, (long long)n, k, mg.KP, s);
-    raw_apply_dev(rawA_, b64_, x64_, r64_, k, 0, s, nullptr);
+    dev::launch_add_correction<double>(X, D0.x, (long long)n, k, mg.KP, s);
+    raw_apply_dev(rawA_, B, X, r64_, k, 0, s, nullptr);
     if (!check(cudaStreamEndCapture(s, &g), "capture end")) return false;
     StepGraph sg;
     sg.kind = 2;
     sg.k = k;
-    sg.b = b64_;
-    sg.x = x64_;
+    sg.b = B;
+    sg.x = X;
     sg.kernels = kernel_nodes(g);
     if (!check(cudaGraphInstantiate(&sg.exec, g, 0), "graph instantiate")) { cudaGraphDestroy(g); return false; }
     cudaGraphDestroy(g);
@@ -1378,16 +1624,15 @@ bool DeviceSystem::solve_fp64(const double* b_host, double* x_host, int k, doubl
     step = sg.exec;
   }
   while (rm > tol && it < maxIters) {
-    if (!check(cudaGraphLaunch(step, s), "graph launch") ||
-        !check(cudaMemcpyAsync(sumsHost_, sums_, 2 * size_t(k) * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h norms") ||
-        !check(cudaStreamSynchronize(s), "refinement step"))
-      return false;
+    kernelLaunches += graphKernels;
+    if (!check(cudaGraphLaunch(step, s), "graph launch") || !read_norms(k, s, "refinement step")) return false;
     it++;
     rm = rel_max();
   }
-  if (!check(cudaMemcpyAsync(x_host, x64_, n * k * 8, cudaMemcpyDeviceToHost, s), "d2h x")) return false;
+  if (x_host && !check(cudaMemcpyAsync(x_host, x64_, n * k * 8, cudaMemcpyDeviceToHost, s), "d2h x")) return false;
   queue_barrier_check(mg, s);
   cudaEventRecord(e1, s);
+  if (userStream) cudaStreamWaitEvent(userStream, e1, 0);
   if (!check(cudaEventSynchronize(e1), "solve") || !barrier_ok(mg)) return false;
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);

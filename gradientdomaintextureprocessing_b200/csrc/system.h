@@ -111,6 +111,11 @@ struct SolverKnobs {
   int coarseFrom = 1;
   int krylov = 0;                       // 1: flexible CG around the V-cycle instead of plain refinement
   int zeroStartSkip = 1;                // first sweep from a zero correction skips the zero neighbours
+  int tileTexels = 0;                   // levels with at least this many deep texels run each smoothing
+                                        // step with the fused tile smoother (0: off)
+  int tileRounds = 1;                   // passes over the four tile colours per smoothing step (the
+                                        // step's sweeps split between them)
+  int tileFinish = 0;                   // 1: one global colour sweep after each tiled smoothing step
 };
 
 struct SolveReport {
@@ -145,23 +150,37 @@ class DeviceSystem {
   bool apply(int which, const double* x, double* y, int k);
   bool solve_mixed(const double* b_host, double* x_host, const double* b_dev, double* x_dev, int k, double tol, int maxIters,
                    cudaStream_t userStream, SolveReport& rep, bool zeroGuess = false);
-  bool solve_fp64(const double* b_host, double* x_host, int k, double tol, int maxIters, SolveReport& rep);
+  // plain FP64 V-cycles: host buffers (b_host, x_host) or the caller's device
+  // buffers (b_dev, x_dev, ordered after userStream when given)
+  bool solve_fp64(const double* b_host, double* x_host, const double* b_dev, double* x_dev, int k, double tol, int maxIters,
+                  cudaStream_t userStream, SolveReport& rep);
   // count independent problems from host buffers, each from a zero guess: the
   // upload of b[i+1] and the download of x[i-1] run on two copy streams while
   // problem i is solved; returns once every x[i] is written
   bool solve_stream(const double* const* b_host, double* const* x_host, int count, int k, double tol, int maxIters,
                     SolveReport* reps);
   bool vcycle_host(float* x, const float* rhs, int k);
+  // `sweeps` level-0 smoothing sweeps (host FP32 vectors, x in place) with the
+  // level-0 smoother the V-cycle uses (colour passes or the fused tile smoother)
+  bool relax_host(float* x, const float* rhs, int k, int sweeps, bool reverse);
   // times full solves of b (host, n x k) for a grid of smoother settings and
   // keeps the fastest that converges; returns the chosen knobs
   bool autotune(const double* b, int k, double tol, SolverKnobs& best, double& bestSeconds);
   bool residual_host(const double* b, const double* x, int k, double* rel);
 
   SolverKnobs knobs;
+  bool profTiled() const { return profTiled_; }
+  template <typename T>
+  void tile_smooth(Multigrid<T>& mg, dev::LevelDev<T>& D, int sweeps, bool reverse, bool zeroStart, cudaStream_t s, bool prof);
   template <typename T>
   bool grouped(const dev::LevelDev<T>& D, int KP) const {
     return knobs.chartTexels > 0 && D.nGroups > 0 && D.maxGroupDeep <= knobs.chartTexels &&
            size_t(D.maxGroupSpan) * KP * sizeof(T) <= dev::kGroupSmemMax;
+  }
+  // the fused tile smoother runs this level (FP32 vectors of 1 or 4 channels)
+  template <typename T>
+  bool tiled(const dev::LevelDev<T>& D, int KP) const {
+    return sizeof(T) == 4 && knobs.tileTexels > 0 && D.nTiles > 0 && D.nDeep >= knobs.tileTexels && (KP == 1 || KP == 4);
   }
   int pre_sweeps(int level) const {
     return (level >= knobs.coarseFrom && knobs.coarsePreSweeps >= 0) ? knobs.coarsePreSweeps : knobs.preSweeps;
@@ -281,10 +300,12 @@ class DeviceSystem {
   void add_graph(const StepGraph& g);
   cudaEvent_t profEv_[4] = {nullptr, nullptr, nullptr, nullptr};  // level-0 full pre sweeps, post sweeps
   int profSweeps_ = 0, profPostSweeps_ = 0;
+  bool profTiled_ = false;              // the timed level-0 group is one fused tile-smoother launch
   std::vector<cudaEvent_t> traceEv_;   // 2 L markers of the captured V-cycle (traceLevels)
   void trace_mark(int i, cudaStream_t s);
   unsigned long long* timeline_ = nullptr;  // cluster phase timeline (traceLevels)
   bool usedGridBarrier_ = false;        // a captured V-cycle runs the persistent coarse-level kernel
+  bool usedTileWait_ = false;           // ... or the tile smoother (bounded waits on neighbouring tiles)
   unsigned int* barrierErrHost_ = nullptr;  // pinned copy of its barrier's error word
   template <typename T>
   void queue_barrier_check(Multigrid<T>& mg, cudaStream_t s);

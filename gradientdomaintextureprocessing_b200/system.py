@@ -70,7 +70,8 @@ class System:
         out = np.zeros(5)
         _lib.check(_lib.lib().gdtp_system_autotune(self._s, _lib.ptr(b), k, float(tol), _lib.ptr(out)))
         knobs = {name: int(self.get(name)) for name in ("pre_sweeps", "post_sweeps", "pre_boundary", "post_boundary",
-                                                         "coarse_pre_sweeps", "coarse_post_sweeps", "coarse_from", "krylov")}
+                                                         "coarse_pre_sweeps", "coarse_post_sweeps", "coarse_from", "krylov",
+                                                         "tile_texels", "tile_rounds", "tile_finish")}
         knobs["seconds"] = float(out[4])
         return knobs
 
@@ -122,6 +123,15 @@ class System:
         x = x.copy()
         rhs, _ = self._vec(rhs, np.float32)
         _lib.check(_lib.lib().gdtp_vcycle(self._s, _lib.ptr(x), _lib.ptr(rhs), k))
+        return x
+
+    def relax(self, x: np.ndarray, rhs: np.ndarray, sweeps: int = 1, reverse: bool = False) -> np.ndarray:
+        """``Relaxation`` (IterativeSolvers.inl:174-395): level-0 Gauss-Seidel
+        sweeps with the V-cycle's level-0 smoother; returns the new x."""
+        x, k = self._vec(x, np.float32)
+        x = x.copy()
+        rhs, _ = self._vec(rhs, np.float32)
+        _lib.check(_lib.lib().gdtp_relax(self._s, _lib.ptr(x), _lib.ptr(rhs), k, int(sweeps), int(bool(reverse))))
         return x
 
     def residual(self, b: np.ndarray, x: np.ndarray) -> np.ndarray:

@@ -112,7 +112,8 @@ void gdtp_system_free(gdtp_system* s);
  *   "bbMass.ptr/.col/.val" "bbStiffness.*" "bdMass.*" "bdStiffness.*"
  *   after gdtp_system_update: "coef.deep"(level l, raw, 10 per deep texel), "coef.bb.*", "coef.bd.*"
  *   "profile": {timed level-0 sweep groups, their total ms, deep texels per group,
- *   kernels per step graph, kernels launched by solves}; "profile.reset" clears the counts
+ *   kernels per step graph, kernels launched by solves, 1 if a timed group is one
+ *   fused tile-smoother launch (else colour sweeps)}; "profile.reset" clears the counts
  *   "profile.setup": ms of the last set-up {update, boundary solver factorisations,
  *   coarsest inverse, other multigrid set-up}; the last three are spent by the
  *   first solve after an update (or after a new right-hand-side width) */
@@ -132,6 +133,15 @@ int gdtp_apply(gdtp_system* s, int which, const double* x, double* y, int k);
 /* One FP32 V-cycle on level-0 vectors (host float32, numTexels*k), x updated in
  * place.  Replaces VCycle (include/Src/IterativeSolvers.inl:1211-1333). */
 int gdtp_vcycle(gdtp_system* s, float* x, const float* rhs, int k);
+
+/* `sweeps` Gauss-Seidel sweeps over the level-0 deep texels (host float32,
+ * numTexels*k, x updated in place; boundary texels unchanged), colours in
+ * order 0..3 (reverse: 3..0), with the smoother the V-cycle uses on level 0:
+ * one launch per colour pass, or, when the "tile_texels" knob selects level 0,
+ * the fused tile smoother (Gauss-Seidel inside 32 x 32 tiles of a chart,
+ * Jacobi across tile borders).  Replaces Relaxation
+ * (include/Src/IterativeSolvers.inl:174-395). */
+int gdtp_relax(gdtp_system* s, float* x, const float* rhs, int k, int sweeps, int reverse);
 
 typedef struct gdtp_report {
   int iterations;          /* outer FP64 refinement steps (or V-cycles for the plain FP64 path) */
@@ -166,8 +176,15 @@ int gdtp_solve_stream(gdtp_system* s, const double* const* b, double* const* x, 
 /* Same on device float64 buffers (no host copies); stream = cudaStream_t or NULL. */
 int gdtp_solve_device(gdtp_system* s, const double* b_dev, double* x_dev, int k, double tol, int max_iters,
                       void* stream, gdtp_report* report);
-/* Plain FP64 V-cycles (no mixed precision) until tol: the comparator path. */
+/* Plain FP64 V-cycles (no mixed precision) until tol: the comparator path, the
+ * app loop of VCycle calls in the reference's FP64 build (USE_FLOAT 0,
+ * TextureFiltering.cpp:562-579 with IterativeSolvers.inl:1211-1333) on the
+ * device.  Host float64 numTexels*k; x holds the initial guess. */
 int gdtp_solve_fp64(gdtp_system* s, const double* b, double* x, int k, double tol, int max_iters, gdtp_report* report);
+/* Same on device float64 buffers (x_dev holds the initial guess; no host
+ * copies), ordered after `stream` (cudaStream_t or NULL) like gdtp_solve_device. */
+int gdtp_solve_fp64_device(gdtp_system* s, const double* b_dev, double* x_dev, int k, double tol, int max_iters, void* stream,
+                           gdtp_report* report);
 
 /* Relative residuals ||b - A x|| / ||b|| per RHS (FP64 operator), host buffers. */
 int gdtp_residual(gdtp_system* s, const double* b, const double* x, int k, double* rel);
@@ -213,7 +230,15 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * anisotropic metrics), "zero_start_skip" (0/1, default 1: the first level-0
  * sweep of a V-cycle on a zero correction reads only the neighbours it has
  * already updated, and a level entered with a zero iterate and no
- * pre-smoothing restricts its right-hand side as its residual; same results). */
+ * pre-smoothing restricts its right-hand side as its residual; same results),
+ * "tile_texels" (levels with at least this many deep texels smooth with the
+ * fused tile smoother: 32 x 32 texel tiles of a chart, each running all sweeps
+ * of a step in shared memory, tiles in four tile colours so that every tile
+ * sees its neighbours' newest values; 0 = off, the default), "tile_rounds"
+ * (passes over the tiles per smoothing step, the sweeps split between them,
+ * default 1), "tile_finish" (0/1: one global colour sweep closes each tiled
+ * smoothing step).  The autotuner tries the tile smoother on the finest one
+ * or two levels. */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
 int gdtp_system_get(const gdtp_system* s, const char* knob, double* value);
 /* Autotuner: times complete solves of b (host float64 numTexels*k, uploaded

@@ -11,6 +11,9 @@ Every function restates one reference operator on the reference's data layout
 * ``multiply_no_reciprocals`` MultiplyBySystemMatrix_NoReciprocals include/Src/IterativeSolvers.inl:881-950
 * ``prolongation``            InitializeProlongationMatrix include/Src/ProlongationAndRestriction.inl:218-263
 * ``reciprocal_form``         UpdateMultigridCoefficients include/Src/UpdateCoefficients.inl:374-397
+* ``relax``                   Relaxation's per-texel update include/Src/IterativeSolvers.inl:449-463, in the
+                              device's 4-colour order (one colour per chart-local parity), optionally tile
+                              by tile (32 x 32 blocks of a chart, four block colours in turn)
 * ``direct_solve``            the --useDirectSolver FP64 solve (TextureFiltering.cpp:651-655, 704-707;
                               Eigen SimplicialLDLT in include/Src/Solver.h:144-203, here scipy's LU)
 * ``embedding_metric``        InitializeEmbeddingMetric include/Src/Metric.inl:248-275
@@ -88,6 +91,43 @@ def reciprocal_form(deep: np.ndarray) -> np.ndarray:
     out[:, :9] = deep[:, :9] / c4[:, None]
     out[:, 4] = 1.0 / c4
     out[:, 9] = c4
+    return out
+
+
+def relax(nodeinfo: np.ndarray, deep_global: np.ndarray, recip: np.ndarray, x: np.ndarray, rhs: np.ndarray, sweeps: int,
+          reverse: bool = False, tile: int = 0) -> np.ndarray:
+    """Gauss-Seidel sweeps over the deep texels in FP32: x_i = rhs_i c4 - sum_{k != 4} c_k x_k
+    with the reciprocal-form coefficients ``recip`` (n_deep x 10, stencil slot 3 (dj + 1) + di + 1),
+    colour (ci & 1) | (cj & 1) << 1 of the chart-local coordinates, colours 0..3 (3..0 if reverse).
+    tile > 0: texels are grouped in tile x tile blocks of their chart's grid, coloured by block parity
+    (bi & 1) | (bj & 1) << 1; the blocks of one colour run all sweeps in turn (colours of blocks
+    0..3, 3..0 if reverse), each seeing the current values of every neighbour.
+    x, rhs: n x k; returns the new x (float32)."""
+    ni = np.asarray(nodeinfo)
+    chart, ci, cj = ni[:, 0], ni[:, 1], ni[:, 2]
+    w, h = ci.max() + 3, cj.max() + 3
+    look = -np.ones((chart.max() + 1, w, h), dtype=np.int64)
+    look[chart, ci + 1, cj + 1] = np.arange(len(ni))
+    g = np.asarray(deep_global, dtype=np.int64)
+    gc, gi, gj = chart[g], ci[g], cj[g]
+    nb = np.empty((len(g), 9), dtype=np.int64)
+    for k in range(9):
+        di, dj = k % 3 - 1, k // 3 - 1
+        nb[:, k] = look[gc, gi + di + 1, gj + dj + 1]
+    assert (nb >= 0).all(), "a deep texel has an inactive neighbour"
+    c = np.asarray(recip, dtype=np.float32)
+    out = np.asarray(x, dtype=np.float32).reshape(len(ni), -1).copy()
+    b = np.asarray(rhs, dtype=np.float32).reshape(len(ni), -1)
+    colour = (gi & 1) | ((gj & 1) << 1)
+    block = ((gi // tile) & 1) | (((gj // tile) & 1) << 1) if tile else np.zeros_like(gi)
+    order = [3, 2, 1, 0] if reverse else [0, 1, 2, 3]
+    for blk in (order if tile else [0]):
+        for _ in range(sweeps):
+            for col in order:
+                sel = np.nonzero((colour == col) & (block == blk))[0]
+                t = [c[sel, k][:, None] * out[nb[sel, k]] for k in range(9)]
+                acc = ((t[0] + t[1] + t[2]) + (t[6] + t[7] + t[8])) + (t[3] + t[5])
+                out[g[sel]] = b[g[sel]] * c[sel, 4][:, None] - acc
     return out
 
 

@@ -21,7 +21,11 @@
 //   restriction, (1e-6 M + S) d = rhs with exact solves, d shifted to 0 at the source.
 //
 // Usage: gdtp_ref <mesh.gdm> <out.gdd> [levels] [stiffness] [sharpness] [vcycles] [mode] [tol] [field.vf] [source]
-//   mode "dump": everything (small meshes); "solve": counts + rhs + exact solution + V-cycle timing.
+//   mode "dump": everything (small meshes); "solve": counts + rhs + exact solution + V-cycle timing;
+//   "time": V-cycles to tol only (no dumps, no direct solve); "vsolve": V-cycles to tol (the FP64
+//   reference solution where a direct solve is too large) plus the FP64 operator fine/A.
+//   field.vf may instead be a ".pm" file: the parameter metric itself (nt x 4 float64,
+//   g(0,0) g(0,1) g(1,0) g(1,1) per mesh triangle), which InitializeMassAndStiffness then uses.
 //   The RHS is  M f + stiffness*sharpness * S f  and the operator  M + stiffness*S.
 //   With field.vf (the reference's vector file: int32 count + per-triangle Point2D<double> in the
 //   triangle's edge basis, read by its own ReadVector) M and S use the anisotropic metric instead.
@@ -157,7 +161,8 @@ int main(int argc, char** argv) {
   const int vcycles = argc > 6 ? atoi(argv[6]) : 12;
   const std::string mode = argc > 7 ? argv[7] : "dump";
   const bool full = (mode == "dump");
-  const bool timeOnly = (mode == "time");  // V-cycles to `tol` (argv[8]) only: no dumps, no direct solve
+  // V-cycles to `tol` (argv[8]) only: no dumps, no direct solve ("vsolve" also dumps fine/A)
+  const bool timeOnly = (mode == "time" || mode == "vsolve");
   const double tol = argc > 8 ? atof(argv[8]) : 1e-6;
 
   TexturedMesh mesh;
@@ -186,7 +191,23 @@ int main(int argc, char** argv) {
   if (!InitializeBoundaryProlongationData(hierarchy.gridAtlases[0], boundaryProlongation)) return 3;
   std::vector<std::vector<SquareMatrix<double, 2>>> parameterMetric;
   const char* vfPath = argc > 9 ? argv[9] : nullptr;
-  if (vfPath && *vfPath) {
+  const std::string vfName = vfPath ? vfPath : "";
+  if (vfName.size() > 3 && vfName.compare(vfName.size() - 3, 3, ".pm") == 0) {
+    std::vector<double> pm(4 * mesh.triangles.size());
+    FILE* fp = fopen(vfPath, "rb");
+    const bool okRead = fp && fread(pm.data(), sizeof(double), pm.size(), fp) == pm.size();
+    if (fp) fclose(fp);
+    if (!okRead) { fprintf(stderr, "bad parameter metric %s\n", vfPath); return 2; }
+    parameterMetric.resize(atlasCharts.size());
+    for (size_t c = 0; c < atlasCharts.size(); c++) {
+      parameterMetric[c].resize(atlasCharts[c].meshTriangleIndices.size());
+      for (size_t k = 0; k < atlasCharts[c].meshTriangleIndices.size(); k++) {
+        const int t = atlasCharts[c].meshTriangleIndices[k];
+        SquareMatrix<double, 2>& g = parameterMetric[c][k];
+        g(0, 0) = pm[4 * t]; g(0, 1) = pm[4 * t + 1]; g(1, 0) = pm[4 * t + 2]; g(1, 1) = pm[4 * t + 3];
+      }
+    }
+  } else if (vfPath && *vfPath) {
     std::vector<Point2D<double>> vf;
     if (!ReadVector(vf, vfPath) || vf.size() != mesh.triangles.size()) { fprintf(stderr, "bad vector field %s\n", vfPath); return 2; }
     if (!InitializeAnisotropicMetric(mesh, atlasCharts, parameterMetric, vf, false)) return 3;
@@ -386,6 +407,7 @@ int main(int argc, char** argv) {
   out.f64("solve/rhs", vec3(rhs), 3);
   out.f64("solve/exact", vec3(exact), 3);
   out.f64("solve/vcycle_x", vec3(vars[0].x), 3);
+  if (mode == "vsolve") out.csr("fine/A", A);
   if (full) out.f64("solve/vcycle_x1", firstIterate, 3);
 
   for (int l = 0; l < levels; l++) {

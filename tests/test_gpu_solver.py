@@ -298,3 +298,77 @@ def test_solve_stream_matches_single_solves(setup):
         assert r["iterations"] == rr["iterations"] and r["converged"]
         assert r["rel_residual_max"] == rr["rel_residual_max"]
     assert s.solve_stream([], tol=1e-8)[0] == []
+
+
+def test_fp64_device_entry_point_matches_host_path(setup):
+    """gdtp_solve_fp64_device (the caller's device buffers, timed like the
+    mixed path's device entry point) runs the same captured FP64 steps as
+    gdtp_solve_fp64 on host buffers: the same bits and report."""
+    import ctypes as C
+    import torch
+    from gradientdomaintextureprocessing_b200 import _lib
+    g, _, s = setup
+    b = np.ascontiguousarray(g["solve/rhs"])
+    xh, rh = s.solve(b, tol=1e-8, precision="fp64", max_iters=MAX_ITERS)
+    b_dev = torch.from_numpy(b).cuda()
+    x_dev = torch.zeros_like(b_dev)
+    rep = _lib.Report()
+    st = torch.cuda.current_stream()
+    code = _lib.lib().gdtp_solve_fp64_device(s.handle, C.c_void_p(b_dev.data_ptr()), C.c_void_p(x_dev.data_ptr()), b.shape[1],
+                                             1e-8, MAX_ITERS, C.c_void_p(st.cuda_stream), C.byref(rep))
+    _lib.check(code)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(x_dev.cpu().numpy(), xh)
+    assert rep.iterations == rh["iterations"] and rep.rel_residual_max == rh["rel_residual_max"]
+
+
+@pytest.mark.parametrize("tile", [0, 1])
+@pytest.mark.parametrize("reverse", [False, True])
+def test_relax_matches_port(setup, tile, reverse):
+    """gdtp_relax runs the V-cycle's level-0 smoother: one launch per colour
+    pass (tile_texels 0) or the fused tile smoother (every level with tiles),
+    against the FP32 restatement in the oracle port (the same colour order; in
+    32 x 32 tiles whose neighbours keep their values from before the step)."""
+    import port
+    g, h, s = setup
+    rng = np.random.default_rng(7)
+    n = h.counts(0)["numTexels"]
+    k = g["solve/rhs"].shape[1]
+    x0 = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    rhs = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    recip = port.reciprocal_form(s.array("coef.deep", 0))
+    before = s.get("tile_texels")
+    s.set("tile_texels", 1 if tile else 0)
+    try:
+        got = s.relax(x0, rhs, sweeps=3, reverse=reverse)
+    finally:
+        s.set("tile_texels", before)
+    ref = port.relax(h.array("nodeinfo"), h.array("deepGlobal"), recip, x0, rhs, 3, reverse=reverse, tile=32 if tile else 0)
+    assert np.abs(got - ref).max() <= 2e-5 * np.abs(ref).max()
+    boundary = h.array("boundaryGlobal")
+    np.testing.assert_array_equal(got[boundary], x0[boundary])
+
+
+def test_tile_smoother_solves_to_reference(setup):
+    """The V-cycle with the fused tile smoother on every level that has tiles:
+    same residual bound and energy-norm error against the reference's FP64
+    solution, deterministic, and no more refinement steps than one more than
+    the colour-pass smoother."""
+    import port
+    g, _, s = setup
+    b = g["solve/rhs"]
+    before = s.get("tile_texels")
+    s.set("tile_texels", 0)
+    try:
+        _, plain = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
+        s.set("tile_texels", 1)
+        x, rep = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
+        x2, rep2 = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
+    finally:
+        s.set("tile_texels", before)
+    assert rep["converged"] and rep["rel_residual_max"] <= 1e-8
+    assert s.residual(b, x).max() <= 1e-8
+    assert port.energy_error(ref_full(g), x, g["solve/exact"]).max() < 1e-5
+    np.testing.assert_array_equal(x, x2)
+    assert rep2["iterations"] == rep["iterations"]
+    assert rep["iterations"] <= plain["iterations"] + 1, (rep["iterations"], plain["iterations"])
