@@ -133,6 +133,24 @@ def job_rate(world: int, units_per_rank: float, ms: float) -> float:
     return world * units_per_rank / (ms * 1e-3) / 1e6
 
 
+def gpu_local_cpus(device: int):
+    """CPUs of the NUMA node the GPU hangs off (from sysfs), or None.  Pinned
+    host buffers first touched from these CPUs sit in that node's memory, so
+    host<->device copies do not cross the socket link."""
+    try:
+        import torch
+        bus = torch.cuda.get_device_properties(device).pci_bus_id.lower()
+        dom, rest = bus.split(":", 1)
+        with open(f"/sys/bus/pci/devices/{int(dom, 16):04x}:{rest}/local_cpulist") as fh:
+            cpus = set()
+            for part in fh.read().strip().split(","):
+                a, _, b = part.partition("-")
+                cpus.update(range(int(a), int(b or a) + 1))
+        return cpus & os.sched_getaffinity(0) or None
+    except (OSError, ValueError, AttributeError, RuntimeError):
+        return None
+
+
 def dist_setup(n_gpus: int):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -406,6 +424,8 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
     ap.add_argument("--trace-levels", action="store_true",
                     help="per-level timing of the V-cycle (events inside the captured steps), one JSON line")
+    ap.add_argument("--knob", action="append", default=[], metavar="NAME=VALUE",
+                    help="solver knob for --profile-solves / --trace-levels runs (e.g. tile_texels=1000000)")
     ap.add_argument("--config", choices=["filtering", "geodesics", "lic"], default="filtering",
                     help="geodesics / lic: extra measurement lines for those workloads (1 GPU)")
     args = ap.parse_args()
@@ -439,6 +459,11 @@ def main():
     f = texel_signal(h, mesh["texture"])
     b_host = texture_filtering_rhs(s, f, LAMBDA, SHARP)
     setup_s = time.time() - t0
+    if args.knob and not (args.trace_levels or args.profile_solves):
+        sys.exit("--knob applies to --profile-solves and --trace-levels runs only")
+    for kv in args.knob:
+        name, value = kv.split("=", 1)
+        s.set(name, float(value))
     if args.trace_levels:
         s.set("trace_levels", 1)
         for _ in range(3):
@@ -513,7 +538,12 @@ def main():
     L.gdtp_system_array(s.handle, b"profile", 0, prof.ctypes.data_as(C.c_void_p), C.byref(cnt))
     value = job_rate(world, n0 * K * args.steps, total_ms)
 
-    # end to end through the host API with pinned buffers
+    # end to end through the host API with pinned buffers, allocated and used
+    # from the CPUs next to the GPU (their NUMA node's memory)
+    all_cpus = os.sched_getaffinity(0)
+    near_cpus = gpu_local_cpus(local)
+    if near_cpus:
+        os.sched_setaffinity(0, near_cpus)
     b_pin = torch.from_numpy(b_host).pin_memory().numpy()
     x_pin = torch.zeros(b_host.shape, dtype=torch.float64).pin_memory().numpy()
 
@@ -554,6 +584,7 @@ def main():
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist)
     e2e_value = job_rate(world, n0 * K * args.steps, e2e_ms)
     rel_stream = max(float(s.residual(b_host, x).max()) for x in (x_pins[0], x_pins[-1]))
+    os.sched_setaffinity(0, all_cpus)  # the reference's CPU leg below uses every core
 
     # plain FP64 GPU V-cycle on the same problem (the comparator path), timed
     # like value: device-resident b and x, warm-up, then K solves between events

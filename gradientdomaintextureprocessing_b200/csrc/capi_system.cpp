@@ -279,6 +279,8 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
     else if (k == "chart_texels" && v >= 0) kn.chartTexels = v;
     else if (k == "tile_texels" && v >= 0) kn.tileTexels = v;
     else if (k == "tile_rounds" && v >= 1 && v <= 16) kn.tileRounds = v;
+    else if (k == "tile_pre_sweeps" && v >= 0 && v <= 16) kn.tilePreSweeps = v;
+    else if (k == "tile_post_sweeps" && v >= 0 && v <= 16) kn.tilePostSweeps = v;
     else if (k == "tile_finish" && (v == 0 || v == 1)) kn.tileFinish = v;
     else if (k == "coarse_pre_sweeps" && v >= -1 && v <= 16) kn.coarsePreSweeps = v;
     else if (k == "coarse_post_sweeps" && v >= -1 && v <= 16) kn.coarsePostSweeps = v;
@@ -316,6 +318,8 @@ extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* v
     else if (k == "chart_texels") *value = kn.chartTexels;
     else if (k == "tile_texels") *value = kn.tileTexels;
     else if (k == "tile_rounds") *value = kn.tileRounds;
+    else if (k == "tile_pre_sweeps") *value = kn.tilePreSweeps;
+    else if (k == "tile_post_sweeps") *value = kn.tilePostSweeps;
     else if (k == "tile_finish") *value = kn.tileFinish;
     else return fail(GDTP_ERR_INVALID, "gdtp_system_get: unknown knob " + k);
     return GDTP_OK;

@@ -904,10 +904,10 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
     LevelDev<T>& C = mg.levels[l + 1];
     // D.x of levels > 0 was cleared by the restriction into this level
     if (knobs.preBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
-    if (tiled(D, KP) && pre_sweeps(l) > 0) {
+    if (tiled(D, KP) && knobs.tilePreSweeps > 0) {
       // x = 0 on entry (a refinement step's correction, or a level entered
       // through the restriction) unless a boundary solve ran first
-      tile_smooth(mg, D, pre_sweeps(l), false, (l > 0 || zeroStart) && !knobs.preBoundary, s, false);
+      tile_smooth(mg, D, knobs.tilePreSweeps, false, (l > 0 || zeroStart) && !knobs.preBoundary, s, false);
     } else if (grouped(D, KP) && pre_sweeps(l) > 0) {
       dev::launch_gs_groups<T, W>(D, pre_sweeps(l), false, KP, s);
     } else {
@@ -930,7 +930,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
     }
     // a level entered with a zero iterate and left unsmoothed (no pre-sweeps, no
     // boundary solve) has residual b - A 0 = b exactly: restrict b itself
-    const bool unsmoothed = knobs.zeroStartSkip && (l > 0 || zeroStart) && pre_sweeps(l) == 0 && !knobs.preBoundary;
+    const bool unsmoothed = knobs.zeroStartSkip && (l > 0 || zeroStart) && pre_sweeps(l, D, KP) == 0 && !knobs.preBoundary;
     if (!unsmoothed)
       dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
     dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, unsmoothed ? D.b : D.r, C.b, C.x, C.n, KP,
@@ -961,10 +961,10 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
     LevelDev<T>& D = mg.levels[l];
     dev::launch_prolong_add<T, W>(D.pruns, D.nPRuns, mg.levels[l + 1].x, D.x, KP, s);
     if (knobs.postBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
-    if (tiled(D, KP) && post_sweeps(l) > 0) {
+    if (tiled(D, KP) && knobs.tilePostSweeps > 0) {
       // timed on level 0: the post-smoothing rounds (coefficients, rhs, x read
       // and written once each per round)
-      tile_smooth(mg, D, post_sweeps(l), true, false, s, profiling_ && l == 0);
+      tile_smooth(mg, D, knobs.tilePostSweeps, true, false, s, profiling_ && l == 0);
     } else if (grouped(D, KP) && post_sweeps(l) > 0) {
       dev::launch_gs_groups<T, W>(D, post_sweeps(l), true, KP, s);
     } else {
@@ -1538,8 +1538,8 @@ bool DeviceSystem::autotune(const double* b, int k, double tol, SolverKnobs& bes
         knobs.tileTexels = threshold;
         knobs.tileRounds = variant == 0 ? 1 : 2;
         knobs.tileFinish = variant == 0 ? 1 : 0;
-        knobs.preSweeps = f[0];
-        knobs.postSweeps = f[1];
+        knobs.tilePreSweeps = f[0];
+        knobs.tilePostSweeps = f[1];
         invalidate_graph();
         double t = 1e300;
         for (int rep = 0; rep < 3; rep++) {

@@ -113,6 +113,7 @@ struct SolverKnobs {
   int zeroStartSkip = 1;                // first sweep from a zero correction skips the zero neighbours
   int tileTexels = 0;                   // levels with at least this many deep texels run each smoothing
                                         // step with the fused tile smoother (0: off)
+  int tilePreSweeps = 2, tilePostSweeps = 2;  // sweeps per smoothing step on tiled levels
   int tileRounds = 1;                   // passes over the four tile colours per smoothing step (the
                                         // step's sweeps split between them)
   int tileFinish = 0;                   // 1: one global colour sweep after each tiled smoothing step
@@ -181,6 +182,15 @@ class DeviceSystem {
   template <typename T>
   bool tiled(const dev::LevelDev<T>& D, int KP) const {
     return sizeof(T) == 4 && knobs.tileTexels > 0 && D.nTiles > 0 && D.nDeep >= knobs.tileTexels && (KP == 1 || KP == 4);
+  }
+  // sweeps of a smoothing step on a level: tiled levels have their own counts
+  template <typename T>
+  int pre_sweeps(int level, const dev::LevelDev<T>& D, int KP) const {
+    return tiled(D, KP) ? knobs.tilePreSweeps : pre_sweeps(level);
+  }
+  template <typename T>
+  int post_sweeps(int level, const dev::LevelDev<T>& D, int KP) const {
+    return tiled(D, KP) ? knobs.tilePostSweeps : post_sweeps(level);
   }
   int pre_sweeps(int level) const {
     return (level >= knobs.coarseFrom && knobs.coarsePreSweeps >= 0) ? knobs.coarsePreSweeps : knobs.preSweeps;

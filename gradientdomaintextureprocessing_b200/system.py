@@ -71,7 +71,8 @@ class System:
         _lib.check(_lib.lib().gdtp_system_autotune(self._s, _lib.ptr(b), k, float(tol), _lib.ptr(out)))
         knobs = {name: int(self.get(name)) for name in ("pre_sweeps", "post_sweeps", "pre_boundary", "post_boundary",
                                                          "coarse_pre_sweeps", "coarse_post_sweeps", "coarse_from", "krylov",
-                                                         "tile_texels", "tile_rounds", "tile_finish")}
+                                                         "tile_texels", "tile_pre_sweeps", "tile_post_sweeps", "tile_rounds",
+                                                         "tile_finish")}
         knobs["seconds"] = float(out[4])
         return knobs
 

@@ -234,7 +234,9 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * "tile_texels" (levels with at least this many deep texels smooth with the
  * fused tile smoother: 32 x 32 texel tiles of a chart, each running all sweeps
  * of a step in shared memory, tiles in four tile colours so that every tile
- * sees its neighbours' newest values; 0 = off, the default), "tile_rounds"
+ * sees its neighbours' newest values; 0 = off, the default),
+ * "tile_pre_sweeps", "tile_post_sweeps" (sweeps per smoothing step on tiled
+ * levels, default 2/2), "tile_rounds"
  * (passes over the tiles per smoothing step, the sweeps split between them,
  * default 1), "tile_finish" (0/1: one global colour sweep closes each tiled
  * smoothing step).  The autotuner tries the tile smoother on the finest one
