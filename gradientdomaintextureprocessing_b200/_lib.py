@@ -49,6 +49,7 @@ _SIGS = {
     "gdtp_system_update": (C.c_int, [_P, C.c_double, C.c_double]),
     "gdtp_apply": (C.c_int, [_P, C.c_int, _P, _P, C.c_int]),
     "gdtp_vcycle": (C.c_int, [_P, _P, _P, C.c_int]),
+    "gdtp_vcycle64": (C.c_int, [_P, _P, _P, C.c_int]),
     "gdtp_relax": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int]),
     "gdtp_solve": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.POINTER(Report)]),
     "gdtp_solve_ex": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(Report)]),

@@ -153,6 +153,14 @@ extern "C" int gdtp_vcycle(gdtp_system* s, float* x, const float* rhs, int k) {
   });
 }
 
+extern "C" int gdtp_vcycle64(gdtp_system* s, double* x, const double* rhs, int k) {
+  return guarded("gdtp_vcycle64", [&]() -> int {
+    GDTP_SYS_CHECK(s);
+    if (!x || !rhs) return fail(GDTP_ERR_INVALID, "gdtp_vcycle64: null vector");
+    return s->sys->vcycle_host64(x, rhs, k) ? GDTP_OK : sys_fail(s, GDTP_ERR_CUDA);
+  });
+}
+
 extern "C" int gdtp_relax(gdtp_system* s, float* x, const float* rhs, int k, int sweeps, int reverse) {
   return guarded("gdtp_relax", [&]() -> int {
     GDTP_SYS_CHECK(s);

@@ -1076,6 +1076,37 @@ bool DeviceSystem::residual_host(const double* b, const double* x, int k, double
   return true;
 }
 
+bool DeviceSystem::vcycle_host64(double* x, const double* rhs, int k) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (!updated_) { err_ = "vcycle before update"; return false; }
+  if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
+  const int KP = kp_for(k);
+  if (!mg64_ || mg64_->KP < KP) {
+    invalidate_graph();  // captured FP64 steps use the multigrid being replaced
+    mg64_.reset(new Multigrid<double>());
+    if (!build_multigrid(*mg64_, KP)) return false;
+  }
+  Multigrid<double>& mg = *mg64_;
+  const size_t n = h_.levels[0].numTexels;
+  std::vector<double> px(n * mg.KP, 0.0), pb(n * mg.KP, 0.0);
+  for (size_t i = 0; i < n; i++)
+    for (int c = 0; c < k; c++) { px[i * mg.KP + c] = x[i * k + c]; pb[i * mg.KP + c] = rhs[i * k + c]; }
+  LevelDev<double>& D0 = mg.levels[0];
+  if (!check(cudaMemcpyAsync(D0.x, px.data(), px.size() * 8, cudaMemcpyHostToDevice, stream_), "h2d") ||
+      !check(cudaMemcpyAsync(D0.b, pb.data(), pb.size() * 8, cudaMemcpyHostToDevice, stream_), "h2d"))
+    return false;
+  if (mg.KP == 1) vcycle<double, 1>(mg, stream_); else vcycle<double, 4>(mg, stream_);
+  queue_barrier_check(mg, stream_);
+  if (!check(cudaGetLastError(), "vcycle") ||
+      !check(cudaMemcpyAsync(px.data(), D0.x, px.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") ||
+      !check(cudaStreamSynchronize(stream_), "vcycle") || !barrier_ok(mg))
+    return false;
+  for (size_t i = 0; i < n; i++)
+    for (int c = 0; c < k; c++) x[i * k + c] = px[i * mg.KP + c];
+  return true;
+}
+
 bool DeviceSystem::relax_host(float* x, const float* rhs, int k, int sweeps, bool reverse) {
   if (!err_.empty()) return false;
   cudaSetDevice(device_);

@@ -161,6 +161,8 @@ class DeviceSystem {
   bool solve_stream(const double* const* b_host, double* const* x_host, int count, int k, double tol, int maxIters,
                     SolveReport* reps);
   bool vcycle_host(float* x, const float* rhs, int k);
+  // one plain FP64 V-cycle on level-0 host vectors (the FP64 multigrid)
+  bool vcycle_host64(double* x, const double* rhs, int k);
   // `sweeps` level-0 smoothing sweeps (host FP32 vectors, x in place) with the
   // level-0 smoother the V-cycle uses (colour passes or the fused tile smoother)
   bool relax_host(float* x, const float* rhs, int k, int sweeps, bool reverse);

@@ -133,6 +133,9 @@ int gdtp_apply(gdtp_system* s, int which, const double* x, double* y, int k);
 /* One FP32 V-cycle on level-0 vectors (host float32, numTexels*k), x updated in
  * place.  Replaces VCycle (include/Src/IterativeSolvers.inl:1211-1333). */
 int gdtp_vcycle(gdtp_system* s, float* x, const float* rhs, int k);
+/* The same V-cycle in FP64 (host float64 numTexels*k): VCycle of the
+ * reference's FP64 build (USE_FLOAT 0, IterativeSolvers.inl:1211-1333). */
+int gdtp_vcycle64(gdtp_system* s, double* x, const double* rhs, int k);
 
 /* `sweeps` Gauss-Seidel sweeps over the level-0 deep texels (host float32,
  * numTexels*k, x updated in place; boundary texels unchanged), colours in
