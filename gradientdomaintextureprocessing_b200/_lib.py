@@ -50,6 +50,10 @@ _SIGS = {
     "gdtp_apply": (C.c_int, [_P, C.c_int, _P, _P, C.c_int]),
     "gdtp_vcycle": (C.c_int, [_P, _P, _P, C.c_int]),
     "gdtp_vcycle64": (C.c_int, [_P, _P, _P, C.c_int]),
+    "gdtp_brush_create": (C.c_int, [_P, _P, C.c_int, C.POINTER(_P)]),
+    "gdtp_brush_free": (None, [_P]),
+    "gdtp_brush_apply": (C.c_int, [_P, _P, _P]),
+    "gdtp_brush_apply_device": (C.c_int, [_P, _P, _P, _P]),
     "gdtp_relax": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int]),
     "gdtp_solve": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.POINTER(Report)]),
     "gdtp_solve_ex": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(Report)]),

@@ -182,6 +182,38 @@ class System:
         return xs, out
 
 
+class Brush:
+    """The sharpening brush's cell-based stiffness of a signal f (numTexels x k):
+    ``apply(mask)`` = sum over cells of mask[cell] S_cell f, the reference's
+    CellStiffnessToTexelStiffness (IterativeSolvers.inl:1170-1208) on the
+    device.  The mask has one value per cell (the hierarchy's global cell order)."""
+
+    def __init__(self, system: System, signal: np.ndarray):
+        self.system = system  # the brush reads the system's device data
+        f, self.k = system._vec(signal, np.float64)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().gdtp_brush_create(system.handle, _lib.ptr(f), self.k, C.byref(h)))
+        self._b = h
+
+    def __del__(self):
+        b, self._b = getattr(self, "_b", None), None
+        if b:
+            try:
+                _lib.lib().gdtp_brush_free(b)
+            except (TypeError, AttributeError):  # interpreter exit
+                pass
+
+    def apply(self, mask: np.ndarray) -> np.ndarray:
+        m = np.ascontiguousarray(mask, dtype=np.float64)
+        out = np.empty((self.system.n, self.k))
+        _lib.check(_lib.lib().gdtp_brush_apply(self._b, _lib.ptr(m), _lib.ptr(out)))
+        return out
+
+
+def CellStiffnessToTexelStiffness(brush: Brush, cell_mask: np.ndarray) -> np.ndarray:
+    return brush.apply(cell_mask)
+
+
 def InitializeMassAndStiffness(hierarchy: Hierarchy, device: int = 0, parameter_metric=None) -> System:
     return System(hierarchy, device=device, parameter_metric=parameter_metric)
 

@@ -253,6 +253,28 @@ int gdtp_system_get(const gdtp_system* s, const char* knob, double* value);
  * sweeps, pre boundary, post boundary, best solve seconds. */
 int gdtp_system_autotune(gdtp_system* s, const double* b, int k, double tol, double* knobs_out);
 /* ---------------------------------------------------------------------------
+ * Sharpening brush (device): the filtering app's right-hand side
+ * M f + lambda sum_cells m_c S_c f for a per-cell mask m (TextureFiltering.cpp:
+ * 562-570).  gdtp_brush_create keeps, for the signal f (host float64
+ * numTexels*k, 1 <= k <= 4), every cell's stiffness applied to f: the four
+ * cells around each deep texel, and for the boundary texels a boundary x cells
+ * matrix per channel (the fine boundary rows restricted to the boundary
+ * texels) -- what InitializeMassAndStiffness computes with
+ * computeCellBasedStiffness (MassAndStiffness.h:490-546).
+ * gdtp_brush_apply: out (numTexels*k) = sum_cells mask[cell] S_cell f, the
+ * modulated stiffness; replaces CellStiffnessToTexelStiffness
+ * (IterativeSolvers.inl:1170-1208).  mask: one float64 per cell in the global
+ * cell order (the hierarchy's "cellCorners" rows; counts[3] cells); host
+ * buffers, or device buffers ordered on `stream` for _device.  The system must
+ * outlive the brush.
+ * ------------------------------------------------------------------------- */
+typedef struct gdtp_brush gdtp_brush;
+int gdtp_brush_create(gdtp_system* s, const double* signal, int k, gdtp_brush** out);
+void gdtp_brush_free(gdtp_brush* b);
+int gdtp_brush_apply(gdtp_brush* b, const double* cell_mask, double* out);
+int gdtp_brush_apply_device(gdtp_brush* b, const double* mask_dev, double* out_dev, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Heat-method geodesics (device).  gdtp_geodesics_create builds, for the
  * system's mesh, atlas and metric, the integration samples of the Geodesics
  * app: replaces InitializeGridAtladInteriorCellLines and

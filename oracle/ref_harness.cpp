@@ -23,7 +23,8 @@
 // Usage: gdtp_ref <mesh.gdm> <out.gdd> [levels] [stiffness] [sharpness] [vcycles] [mode] [tol] [field.vf] [source]
 //   mode "dump": everything (small meshes); "solve": counts + rhs + exact solution + V-cycle timing;
 //   "time": V-cycles to tol only (no dumps, no direct solve); "vsolve": V-cycles to tol (the FP64
-//   reference solution where a direct solve is too large) plus the FP64 operator fine/A.
+//   reference solution where a direct solve is too large) plus the FP64 operator fine/A;
+//   "brush": the sharpening brush's modulated stiffness for a seeded cell mask (brush/mask, brush/out).
 //   field.vf may instead be a ".pm" file: the parameter metric itself (nt x 4 float64,
 //   g(0,0) g(0,1) g(1,0) g(1,1) per mesh triangle), which InitializeMassAndStiffness then uses.
 //   The RHS is  M f + stiffness*sharpness * S f  and the operator  M + stiffness*S.
@@ -236,12 +237,55 @@ int main(int argc, char** argv) {
 
   std::vector<double> deepMass, deepStiffness, texelToCell;
   SparseMatrix<double, int> bbM, bbS, bdM, bdS, cellRHS[3];
+  const bool brush = (mode == "brush");  // the sharpening brush's cell-based stiffness (TextureFiltering.cpp:569)
   if (!InitializeMassAndStiffness(deepMass, deepStiffness, bbM, bbS, bdM, bdS, hierarchy, parameterMetric, atlasCharts,
-                                  boundaryProlongation, false, inputSignal, texelToCell, cellRHS)) {
+                                  boundaryProlongation, brush, inputSignal, texelToCell, cellRHS)) {
     fprintf(stderr, "InitializeMassAndStiffness failed\n");
     return 3;
   }
   double tAssembly = secs(T1);
+  if (brush) {
+    // CellStiffnessToTexelStiffness (IterativeSolvers.inl:1170-1208) for a seeded
+    // cell mask m_c = ((c * 2654435761) mod 2^32 mod 1000) / 1000, in FP64 (Vec4d),
+    // the texel-to-cell coefficients converted as the app does (TextureFiltering.cpp:641-642)
+    std::vector<InteriorTexelToCellLine> lines;
+    InitializeInteriorTexelToCellLines(lines, fine);
+    std::vector<Vec> coeffs(4 * size_t(fine.numDeepTexels));
+    for (size_t i = 0; i < coeffs.size(); i++) coeffs[i] = SetData(texelToCell[3 * i], texelToCell[3 * i + 1], texelToCell[3 * i + 2]);
+    std::vector<Real> mask(fine.numCells), boundaryValues[3];
+    for (int c = 0; c < fine.numCells; c++) mask[c] = Real(double((uint32_t(c) * 2654435761u) % 1000u) / 1000.0);
+    for (int c = 0; c < 3; c++) boundaryValues[c].resize(fine.boundaryGlobalIndex.size());
+    std::vector<Vec> modulated(fine.numTexels, ZeroData());
+    auto flat = [&] {
+      std::vector<double> o(3 * size_t(fine.numTexels));
+      for (size_t i = 0; i < modulated.size(); i++)
+        for (int c = 0; c < 3; c++) o[3 * i + c] = double(modulated[i][c]);
+      return o;
+    };
+    CellStiffnessToTexelStiffness(mask, lines, coeffs, cellRHS, boundaryValues, fine.boundaryGlobalIndex, modulated);
+    out.f64("brush/mask", std::vector<double>(mask.begin(), mask.end()));
+    out.f64("brush/out", flat(), 3);
+    std::vector<Real> ones(fine.numCells, Real(1));  // a uniform brush: the stiffness applied to the signal
+    CellStiffnessToTexelStiffness(ones, lines, coeffs, cellRHS, boundaryValues, fine.boundaryGlobalIndex, modulated);
+    out.f64("brush/out_ones", flat(), 3);
+    std::vector<Vec> sf(fine.numTexels);
+    MultiplyBySystemMatrix_NoReciprocals(deepStiffness, bdS, bbS, fine.boundaryGlobalIndex, fine.rasterLines, f0, sf);
+    out.f64("brush/stiffness_f", [&] {
+      std::vector<double> o(3 * sf.size());
+      for (size_t i = 0; i < sf.size(); i++)
+        for (int c = 0; c < 3; c++) o[3 * i + c] = double(sf[i][c]);
+      return o;
+    }(), 3);
+    out.f64("solve/f", [&] {
+      std::vector<double> f(3 * inputSignal.size());
+      for (size_t i = 0; i < inputSignal.size(); i++)
+        for (int c = 0; c < 3; c++) f[3 * i + c] = inputSignal[i][c];
+      return f;
+    }(), 3);
+    out.i32("L0/counts", {fine.numTexels, fine.numDeepTexels, (int)fine.boundaryGlobalIndex.size(), fine.numCells});
+    fprintf(stderr, "ok: brush, %d texels, %d cells\n", fine.numTexels, fine.numCells);
+    return 0;
+  }
 
   // ---------------- system ---------------------------------------------------------------
   auto T2 = std::chrono::steady_clock::now();
