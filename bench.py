@@ -241,26 +241,20 @@ def reference_leg(mesh, s, b_dev, x_dev, x_own, stream) -> dict:
                                           "texture and operator (oracle/_ref/gdtp_ref vsolve)"}}
 
 
-def serve(args):
+def serving_stream(n_requests: int, max_size: int, budget_gb: float, rate: float = 0.0) -> dict:
     """Serving stream: requests on torus / icosphere / genus-2 models at sizes
-    log-uniform in [256, max size] (sqrt(2) ladder, multiples of 8), kinds 60 %
+    log-uniform in [256, max_size] (sqrt(2) ladder, multiples of 8), kinds 60 %
     filtering (k = 3), 30 % geodesic (k = 1), 10 % line-integral convolution
     (k = 1, anisotropy 1e3), Poisson arrivals, HBM admission budget.  Models are
-    added and made resident before the stream (setup time reported apart)."""
-    import torch
-    torch.cuda.set_device(0)
-    from gradientdomaintextureprocessing_b200 import build as _build
-    _build.build()
+    added and made resident before the stream (set-up time reported apart);
+    rate 0: arrivals 1.5x faster than the measured one-at-a-time service rate."""
     from gradientdomaintextureprocessing_b200 import serving
-    stream = serving.request_stream(args.serve_requests, rate_per_s=1.0, max_size=args.serve_max_size, seed=0)
-    server = serving.Server(budget_bytes=int(args.serve_budget_gb * (1 << 30)), slots=4)
+    stream = serving.request_stream(n_requests, rate_per_s=1.0, max_size=max_size, seed=0)
+    server = serving.Server(budget_bytes=int(budget_gb * (1 << 30)), slots=4)
     t0 = time.time()
     models = serving.build_models(server, stream)
     setup_s = time.time() - t0
-    # rate: saturate the device -> arrivals faster than the measured service rate
-    rate = args.serve_rate
     if rate <= 0:
-        # one request at a time: mean service time, then arrivals 1.5x faster than that
         probe = [(0.0,) + tuple(p[1:]) for p in stream[:16]]
         t = []
         for p in probe:
@@ -268,36 +262,44 @@ def serve(args):
             if res[0][1]["ok"]:
                 t.append(wall)
         rate = 1.5 / float(np.mean(t))
-    arrivals = serving.request_stream(args.serve_requests, rate_per_s=rate, max_size=args.serve_max_size, seed=0)
-    server2 = server  # models stay resident
-    before = server2.stats()
-    results, st, wall = serving.run_stream(server2, arrivals, models)
+    arrivals = serving.request_stream(n_requests, rate_per_s=rate, max_size=max_size, seed=0)
+    before = server.stats()
+    results, st, wall = serving.run_stream(server, arrivals, models)
     failed = [r for _, r in results if not r["ok"]]
     kind_of = {v: k for k, v in serving.KIND_NAMES.items()}
     results = [(x, r) for x, r in results if r["ok"]]
     lat = np.array([r["latency_ms"] for _, r in results])
-    texel_rhs = sum(server2.texels[models[(r["mesh"], r["size"], kind_of[r["kind"]])][0]] * (3 if r["kind"] == "filtering" else 1)
+    texel_rhs = sum(server.texels[models[(r["mesh"], r["size"], kind_of[r["kind"]])][0]] * (3 if r["kind"] == "filtering" else 1)
                     for _, r in results)
     kinds = {serving.KIND_NAMES[k]: sum(1 for *_, kk in arrivals if kk == k) for k in serving.KIND_NAMES}
-    out = {"metric": "serving: latency p50/p99 and aggregate Mtexels solved/s at 1e-6 rel. residual", "impl": "ours",
-           "value": texel_rhs / wall / 1e6, "unit": "Mtexels/s (texels x RHS, whole stream)",
-           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
-           "requests": len(arrivals), "failed": len(failed),
-           "failures": [{k: r[k] for k in ("mesh", "size", "kind", "error")} for r in failed[:5]],
-           "by_kind": {kn: {"p50_ms": float(np.percentile([r["latency_ms"] for _, r in results if r["kind"] == kn], 50)),
-                            "p99_ms": float(np.percentile([r["latency_ms"] for _, r in results if r["kind"] == kn], 99)),
-                            "max_iterations": int(max(r.get("iterations", 0) for _, r in results if r["kind"] == kn))}
-                       for kn in sorted({r["kind"] for _, r in results})},
-           "slowest": sorted(({k: r.get(k) for k in ("mesh", "size", "kind", "latency_ms", "iterations", "batch")}
-                              for _, r in results), key=lambda d: -d["latency_ms"])[:5],
-           "arrival_rate_per_s": rate, "wall_s": wall,
-           "max_rel_residual": float(max(r["rel_residual_max"] for _, r in results)),
-           "batches": st["batches"] - before["batches"], "requests_in_batches": st["batched_requests"] - before["batched_requests"],
-           "evictions": st["evictions"], "resident_gb": st["resident_bytes"] / 2**30, "peak_gb": st["peak_bytes"] / 2**30,
-           "budget_gb": args.serve_budget_gb, "models": len(models), "setup_s": round(setup_s, 1), "kinds": kinds,
-           "config": {"workload": f"torus / icosphere6 / genus-2, 256^2-{args.serve_max_size}^2 log-uniform, "
-                                  "60 % filtering k=3, 30 % geodesic k=1, 10 % LIC k=1, Poisson arrivals", "slots": 4},
-           "data": "synthetic"}
+    return {"value": texel_rhs / wall / 1e6, "unit": "Mtexels/s (texels x RHS, whole stream)",
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "requests": len(arrivals), "failed": len(failed),
+            "failures": [{k: r[k] for k in ("mesh", "size", "kind", "error")} for r in failed[:5]],
+            "by_kind": {kn: {"p50_ms": float(np.percentile([r["latency_ms"] for _, r in results if r["kind"] == kn], 50)),
+                             "p99_ms": float(np.percentile([r["latency_ms"] for _, r in results if r["kind"] == kn], 99)),
+                             "max_iterations": int(max(r.get("iterations", 0) for _, r in results if r["kind"] == kn))}
+                        for kn in sorted({r["kind"] for _, r in results})},
+            "slowest": sorted(({k: r.get(k) for k in ("mesh", "size", "kind", "latency_ms", "iterations", "batch")}
+                               for _, r in results), key=lambda d: -d["latency_ms"])[:5],
+            "arrival_rate_per_s": rate, "wall_s": wall,
+            "max_rel_residual": float(max(r["rel_residual_max"] for _, r in results)),
+            "batches": st["batches"] - before["batches"], "requests_in_batches": st["batched_requests"] - before["batched_requests"],
+            "evictions": st["evictions"], "resident_gb": st["resident_bytes"] / 2**30, "peak_gb": st["peak_bytes"] / 2**30,
+            "budget_gb": budget_gb, "models": len(models), "setup_s": round(setup_s, 1), "kinds": kinds,
+            "config": {"workload": f"torus / icosphere6 / genus-2, 256^2-{max_size}^2 log-uniform, "
+                                   "60 % filtering k=3, 30 % geodesic k=1, 10 % LIC k=1, Poisson arrivals", "slots": 4}}
+
+
+def serve(args):
+    """The serving stream as its own measurement line (--serve)."""
+    import torch
+    torch.cuda.set_device(0)
+    from gradientdomaintextureprocessing_b200 import build as _build
+    _build.build()
+    out = {"metric": "serving: latency p50/p99 and aggregate Mtexels solved/s at 1e-6 rel. residual", "impl": "ours"}
+    out.update(serving_stream(args.serve_requests, args.serve_max_size, args.serve_budget_gb, args.serve_rate))
+    out["data"] = "synthetic"
     print(json.dumps(out), flush=True)
 
 
@@ -422,6 +424,8 @@ def main():
                     help="largest texture size of the stream (4096 is the full range; host set-up then takes several minutes)")
     ap.add_argument("--serve-rate", type=float, default=0.0, help="arrivals per second (0: calibrated to saturate)")
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
+    ap.add_argument("--serve-requests-in-line", type=int, default=64,
+                    help="requests of the compact serving stream (256^2-512^2) reported in the main line (0: none)")
     ap.add_argument("--trace-levels", action="store_true",
                     help="per-level timing of the V-cycle (events inside the captured steps), one JSON line")
     ap.add_argument("--knob", action="append", default=[], metavar="NAME=VALUE",
@@ -674,6 +678,13 @@ def main():
            "clocks": clocks.summary()}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         out.update(reference_leg(mesh, s, b_dev, x_dev, x_pin, stream))
+    if rank == 0 and world == 1 and args.serve_requests_in_line > 0:
+        # a compact serving stream after the timed regions (continuous batching,
+        # admission, mixed kinds), so that every run reports serving latency
+        blk = serving_stream(args.serve_requests_in_line, 512, args.serve_budget_gb)
+        out["serving"] = {k: blk[k] for k in ("value", "unit", "latency_ms", "requests", "failed", "arrival_rate_per_s",
+                                               "max_rel_residual", "batches", "requests_in_batches", "models", "setup_s",
+                                               "by_kind", "config")}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:

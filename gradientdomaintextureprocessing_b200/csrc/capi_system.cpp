@@ -296,6 +296,7 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
     else if (k == "krylov" && (v == 0 || v == 1)) kn.krylov = v;
     else if (k == "zero_start_skip" && (v == 0 || v == 1)) kn.zeroStartSkip = v;
     else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
+    if (k == "tile_texels") s->sys->invalidate_multigrids();  // tiles are built for the levels the knob selects
     s->sys->invalidate_graph();
     return GDTP_OK;
   });

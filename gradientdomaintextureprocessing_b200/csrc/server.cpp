@@ -162,20 +162,15 @@ void Server::run_batch(Model& m, std::vector<ServerRequest*>& batch) {
     rep.relMax = std::max(rep.relMax, rep2.relMax);
     rep.seconds += rep2.seconds;
   } else {
-    std::vector<double> f(size_t(n) * K), mf(f.size()), sf;
+    std::vector<double> f(size_t(n) * K);
     int c0 = 0;
     for (auto* r : batch) {
       for (int64_t i = 0; i < n; i++)
         for (int c = 0; c < r->k; c++) f[size_t(i) * K + c0 + c] = r->signal[size_t(i) * r->k + c];
       c0 += r->k;
     }
-    ok = m.a->apply(1, f.data(), mf.data(), K);
-    if (ok && m.kind == kKindFilter && m.s != 0) {
-      sf.resize(f.size());
-      ok = m.a->apply(2, f.data(), sf.data(), K);
-      for (size_t i = 0; ok && i < mf.size(); i++) mf[i] += m.w * m.s * sf[i];
-    }
-    ok = ok && m.a->solve_mixed(mf.data(), x.data(), nullptr, nullptr, K, batch[0]->tol, batch[0]->maxIters, nullptr, rep, true);
+    // M f + w s S f (filtering) or M f (LIC), formed on the device from one upload of f
+    ok = m.a->solve_filtering(f.data(), x.data(), K, m.kind == kKindFilter ? m.w * m.s : 0.0, batch[0]->tol, batch[0]->maxIters, rep);
     if (!ok) err = m.a->error();
   }
   int c0 = 0;

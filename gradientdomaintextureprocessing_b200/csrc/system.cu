@@ -259,6 +259,12 @@ DeviceSystem::~DeviceSystem() {
   if (stream_) cudaStreamDestroy(stream_);
 }
 
+void DeviceSystem::invalidate_multigrids() {
+  invalidate_graph();
+  mg32_.clear();
+  mg64_.reset();
+}
+
 void DeviceSystem::invalidate_graph() {
   cudaSetDevice(device_);
   for (StepGraph& g : stepGraphs_) cudaGraphExecDestroy(g.exec);
@@ -545,8 +551,9 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     std::copy(R.runStart, R.runStart + 5, D.runStart);
     D.coef = A.upload(planes);
     D.planeStride = R.count;
-    // tiles of the fused smoother (FP32 levels with enough deep texels)
-    if (sizeof(T) == 4 && G.numDeep >= kTileBuildMin) {
+    // tiles of the fused smoother (FP32 levels it runs on; the tile_texels knob
+    // drops the multigrids when it changes)
+    if (sizeof(T) == 4 && G.numDeep >= kTileBuildMin && knobs.tileTexels > 0 && G.numDeep >= knobs.tileTexels) {
       TileLayout TL;
       build_tiles(G, C, TL);
       D.tiles = A.upload(TL.tiles);
@@ -1076,6 +1083,34 @@ bool DeviceSystem::residual_host(const double* b, const double* x, int k, double
   return true;
 }
 
+bool DeviceSystem::solve_filtering(const double* f_host, double* x_host, int k, double coefS, double tol, int maxIters,
+                                   SolveReport& rep) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (!updated_) { err_ = "solve before update"; return false; }
+  if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
+  if (!ensure_work(k)) return false;
+  const size_t n = h_.levels[0].numTexels;
+  if (filterK_ < workK_) {  // signal and S f work vectors, grown with the other work buffers
+    filterArena_ = DeviceArena();
+    fDev_ = static_cast<double*>(filterArena_.alloc(n * workK_ * sizeof(double)));
+    sfDev_ = static_cast<double*>(filterArena_.alloc(n * workK_ * sizeof(double)));
+    if (!check(filterArena_.last, "filtering buffers")) return false;
+    filterK_ = workK_;
+  }
+  // b = M f (+ coefS S f) on the device from one upload of f
+  if (!check(cudaMemcpyAsync(fDev_, f_host, n * k * sizeof(double), cudaMemcpyHostToDevice, stream_), "h2d f") ||
+      !raw_apply_dev(rawM_, nullptr, fDev_, b64_, k, 1, stream_, nullptr))
+    return false;
+  kernelLaunches += 1;
+  if (coefS != 0.0) {
+    if (!raw_apply_dev(rawS_, nullptr, fDev_, sfDev_, k, 1, stream_, nullptr)) return false;
+    dev::launch_axpby(b64_, 1.0, b64_, coefS, sfDev_, (long long)(n * k), stream_);
+    kernelLaunches += 2;
+  }
+  return solve_mixed(nullptr, x_host, b64_, x64_, k, tol, maxIters, nullptr, rep, true);
+}
+
 bool DeviceSystem::vcycle_host64(double* x, const double* rhs, int k) {
   if (!err_.empty()) return false;
   cudaSetDevice(device_);
@@ -1555,32 +1590,6 @@ bool DeviceSystem::autotune(const double* b, int k, double tol, SolverKnobs& bes
       }
       if (t < bestSeconds) { bestSeconds = t; best = knobs; }
     }
-  // then, on the best setting, the fused tile smoother on the finest level (or
-  // the two finest): one round with a closing global colour sweep, or two rounds
-  const SolverKnobs colourBest = best;
-  std::vector<int> tileLevels;
-  for (int l = 0; l < 2 && l + 1 < levelsUsed_; l++)
-    if (h_.levels[l].numDeep >= kTileBuildMin) tileLevels.push_back(h_.levels[l].numDeep);
-  const int tileSweeps[][2] = {{2, 2}, {2, 3}, {3, 3}};
-  for (int threshold : tileLevels)
-    for (int variant = 0; variant < 2; variant++)
-      for (const auto& f : tileSweeps) {
-        knobs = colourBest;
-        knobs.tileTexels = threshold;
-        knobs.tileRounds = variant == 0 ? 1 : 2;
-        knobs.tileFinish = variant == 0 ? 1 : 0;
-        knobs.tilePreSweeps = f[0];
-        knobs.tilePostSweeps = f[1];
-        invalidate_graph();
-        double t = 1e300;
-        for (int rep = 0; rep < 3; rep++) {
-          SolveReport r;
-          if (!solve_mixed(nullptr, nullptr, bDev, xDev, k, tol, 60, nullptr, r, true)) return false;
-          if (r.relMax > tol) { t = 1e300; break; }
-          if (rep > 0) t = std::min(t, r.seconds);
-        }
-        if (t < bestSeconds) { bestSeconds = t; best = knobs; }
-      }
   knobs = best;
   invalidate_graph();
   return true;

@@ -161,6 +161,9 @@ class DeviceSystem {
   bool solve_stream(const double* const* b_host, double* const* x_host, int count, int k, double tol, int maxIters,
                     SolveReport* reps);
   bool vcycle_host(float* x, const float* rhs, int k);
+  // the filtering solve A x = M f + coefS S f from the host signal f (n x k):
+  // the right-hand side is formed on the device, x (host) receives the solution
+  bool solve_filtering(const double* f_host, double* x_host, int k, double coefS, double tol, int maxIters, SolveReport& rep);
   // one plain FP64 V-cycle on level-0 host vectors (the FP64 multigrid)
   bool vcycle_host64(double* x, const double* rhs, int k);
   // `sweeps` level-0 smoothing sweeps (host FP32 vectors, x in place) with the
@@ -202,6 +205,8 @@ class DeviceSystem {
   }
   size_t deviceBytes() const;
   // knobs that change the launch sequence take effect on the next solve
+  // drop the multigrids (rebuilt by the next solve), e.g. when a knob changes their layout
+  void invalidate_multigrids();
   void invalidate_graph();
   // live timing of the level-0 colour sweeps inside the captured step graphs:
   // {V-cycles timed, sum of their average full-sweep ms, deep texels per sweep}
@@ -283,6 +288,9 @@ class DeviceSystem {
   DeviceArena workArena_;
   int workK_ = 0;
   double *b64_ = nullptr, *x64_ = nullptr, *r64_ = nullptr, *partials_ = nullptr, *sums_ = nullptr;
+  DeviceArena filterArena_;                // signal and S f of solve_filtering
+  double *fDev_ = nullptr, *sfDev_ = nullptr;
+  int filterK_ = 0;
   double* sumsHost_ = nullptr;    // pinned, mapped
   double* sumsMapped_ = nullptr;  // its device address (null: norms come back by copy)
   // the solve loops' small host exchanges, by kernel: norms sums_ -> sumsHost_

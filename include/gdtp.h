@@ -242,8 +242,9 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * levels, default 2/2), "tile_rounds"
  * (passes over the tiles per smoothing step, the sweeps split between them,
  * default 1), "tile_finish" (0/1: one global colour sweep closes each tiled
- * smoothing step).  The autotuner tries the tile smoother on the finest one
- * or two levels. */
+ * smoothing step).  The autotuner leaves the tile smoother off: with host
+ * copies running beside the solve (gdtp_solve_stream) its rounds slow down
+ * more than the sweeps they replace. */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
 int gdtp_system_get(const gdtp_system* s, const char* knob, double* value);
 /* Autotuner: times complete solves of b (host float64 numTexels*k, uploaded
