@@ -126,7 +126,7 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
       if (count) *count = 0;
       return GDTP_OK;
     }
-    if (name == "profile.setup") return vec(std::vector<double>(s->sys->setupMs, s->sys->setupMs + 4));
+    if (name == "profile.setup") return vec(std::vector<double>(s->sys->setupMs, s->sys->setupMs + 8));
     if (name == "levelStats") return vec(s->sys->level_stats());  // 9 per level, see DeviceSystem::level_stats
     if (name == "levelsUsed") {
       if (count) *count = 1;
@@ -295,8 +295,10 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
     else if (k == "coarse_from" && v >= 1 && v <= 16) kn.coarseFrom = v;
     else if (k == "krylov" && (v == 0 || v == 1)) kn.krylov = v;
     else if (k == "zero_start_skip" && (v == 0 || v == 1)) kn.zeroStartSkip = v;
+    else if (k == "device_factor" && (v == 0 || v == 1)) kn.deviceFactor = v;
     else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
-    if (k == "tile_texels") s->sys->invalidate_multigrids();  // tiles are built for the levels the knob selects
+    if (k == "tile_texels" || k == "device_factor" || k == "max_block" || k == "dense_boundary_max" || k == "max_coarse")
+      s->sys->invalidate_multigrids();  // the multigrids are laid out and factorised by these knobs
     s->sys->invalidate_graph();
     return GDTP_OK;
   });
@@ -323,6 +325,7 @@ extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* v
     else if (k == "coarse_from") *value = kn.coarseFrom;
     else if (k == "krylov") *value = kn.krylov;
     else if (k == "zero_start_skip") *value = kn.zeroStartSkip;
+    else if (k == "device_factor") *value = kn.deviceFactor;
     else if (k == "grid_texels") *value = kn.gridTexels;
     else if (k == "chart_texels") *value = kn.chartTexels;
     else if (k == "tile_texels") *value = kn.tileTexels;

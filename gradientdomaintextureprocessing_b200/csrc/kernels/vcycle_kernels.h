@@ -1,6 +1,9 @@
 // Host-callable launchers of the V-cycle kernels (vcycle_kernels.cu).
 #pragma once
 #include <atomic>
+#include <cstdint>
+#include <string>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace gdtp {
@@ -234,6 +237,16 @@ void launch_deep_gather(int nDeep, const int* deepCells, const double* cellMass,
 void launch_boundary_triangles(int n, const int* btPtr, const int* btTri, const double* btPos, const double* triPos,
                                const double* triMetric, const double* triMetricInv, double* mass, double* stiff, cudaStream_t s);
 void launch_gather_cells(int n, const int* idx, const double* src, double* dst, cudaStream_t s);
+
+// Dense FP64 set-up products (kernels/dense_kernels.cu), synchronous on s.
+// In-place inverses of SPD matrices data[off[q] ..] (size[q] x size[q],
+// row-major) by Gauss-Jordan elimination, made exactly symmetric.
+bool gpu_spd_inverse_batched(double* data, const std::vector<int64_t>& offsets, const std::vector<int>& sizes, cudaStream_t s,
+                             std::string& err);
+// Per block p: G_p = Inv_p C_p (m_p x t_p) and local_p = C_p^T G_p (t_p x t_p).
+bool gpu_schur_products(const std::vector<double>& inv, const std::vector<int64_t>& invOff, const std::vector<int>& m,
+                        const std::vector<double>& C, const std::vector<int64_t>& cOff, const std::vector<int>& t, std::vector<double>& G,
+                        std::vector<double>& local, const std::vector<int64_t>& localOff, cudaStream_t s, std::string& err);
 
 }  // namespace dev
 }  // namespace gdtp

@@ -14,6 +14,7 @@
 // Jacobi-scaled block D^-1/2 BB D^-1/2 (unit diagonal), which keeps the FP32
 // copies well scaled; they are computed here in FP64.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <numeric>
 #include <queue>
@@ -126,7 +127,18 @@ bool dense_spd_inverse(double* A, int n, bool parallel) {
   return true;
 }
 
-bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySolverSetup& bs, std::string& err) {
+namespace {
+double wall_ms() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+}  // namespace
+
+bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySolverSetup& bs, std::string& err,
+                           DenseBackend* dense) {
+  double tMark = wall_ms();
+  auto lap = [&](int slot) {
+    const double t = wall_ms();
+    bs.ms[slot] += t - tMark;
+    tMark = t;
+  };
   const int nb = BB.rows;
   bs = BoundarySolverSetup();
   bs.nb = nb;
@@ -195,6 +207,7 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int dense
   auto scaled = [&](int i, int kk) { return BB.val[kk] * bs.scale[pos[i]] * bs.scale[pos[BB.col[kk]]]; };
 
   // ---- subdomain inverses (scaled), and the interior/separator couplings
+  lap(0);
   bs.invOff.assign(bs.nSub + 1, 0);
   for (int p = 0; p < bs.nSub; p++) {
     int64_t m = bs.subPtr[p + 1] - bs.subPtr[p];
@@ -202,9 +215,11 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int dense
   }
   bs.inv.assign(size_t(bs.invOff[bs.nSub]), 0.0);
   bool ok = true;
+  std::vector<int> subSize(bs.nSub);
 #pragma omp parallel for schedule(dynamic, 1) reduction(&& : ok)
   for (int p = 0; p < bs.nSub; p++) {
     const int b0 = bs.subPtr[p], m = bs.subPtr[p + 1] - b0;
+    subSize[p] = m;
     double* D = &bs.inv[size_t(bs.invOff[p])];
     for (int a = 0; a < m; a++) {
       int i = bs.order[b0 + a];
@@ -213,9 +228,14 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int dense
         if (c >= 0 && c < m) D[size_t(a) * m + c] = scaled(i, kk);
       }
     }
-    ok = dense_spd_inverse(D, m, false) && ok;
+    if (!dense) ok = dense_spd_inverse(D, m, false) && ok;
   }
-  if (!ok) { err = "boundary subdomain block is not positive definite"; return false; }
+  if (dense && bs.nSub > 0) {
+    std::vector<int64_t> off(bs.invOff.begin(), bs.invOff.end() - 1);
+    ok = dense->spd_inverse_batched(bs.inv.data(), off, subSize, err);
+  }
+  if (!ok) { err = "boundary subdomain block is not positive definite" + (err.empty() ? std::string() : ": " + err); return false; }
+  lap(1);
   std::vector<Triplet> tIS;
   for (int k = 0; k < bs.nI; k++) {
     int i = bs.order[k];
@@ -263,6 +283,40 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int dense
     // per-subdomain contributions, subtracted afterwards in subdomain order so
     // that the complement is bit-identical from run to run
     std::vector<std::vector<double>> contrib(bs.nSub);
+    if (dense) {
+      // C_p (m x t, row-major) for every subdomain, then G_p and C_p^T G_p on the device
+      std::vector<int64_t> cOff(bs.nSub, 0), lOff(bs.nSub, 0);
+      std::vector<int> tSize(bs.nSub);
+      int64_t cTotal = 0, lTotal = 0;
+      for (int p = 0; p < bs.nSub; p++) {
+        const int m = bs.subPtr[p + 1] - bs.subPtr[p];
+        tSize[p] = (int)touches[p].size();
+        cOff[p] = cTotal;
+        lOff[p] = lTotal;
+        cTotal += int64_t(m) * tSize[p];
+        lTotal += int64_t(tSize[p]) * tSize[p];
+      }
+      std::vector<double> C(size_t(cTotal), 0.0), G, local;
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int p = 0; p < bs.nSub; p++) {
+        const int b0 = bs.subPtr[p], m = bs.subPtr[p + 1] - b0, t = tSize[p];
+        const std::vector<int>& touch = touches[p];
+        for (int a = 0; a < m; a++)
+          for (int kk = bs.AIS.ptr[b0 + a]; kk < bs.AIS.ptr[b0 + a + 1]; kk++) {
+            int c = int(std::lower_bound(touch.begin(), touch.end(), bs.AIS.col[kk]) - touch.begin());
+            C[size_t(cOff[p]) + size_t(a) * t + c] = bs.AIS.val[kk];
+          }
+      }
+      std::vector<int64_t> invOff(bs.invOff.begin(), bs.invOff.end() - 1);
+      if (!dense->schur_products(bs.inv, invOff, subSize, C, cOff, tSize, G, local, lOff, err)) return false;
+      for (int p = 0; p < bs.nSub; p++) {
+        const int m = bs.subPtr[p + 1] - bs.subPtr[p], t = tSize[p];
+        double* Wp = &bs.W[size_t(bs.wOff[p])];
+        for (int a = 0; a < m; a++)
+          for (int c = 0; c < t; c++) Wp[size_t(c) * m + a] = G[size_t(cOff[p]) + size_t(a) * t + c];
+        contrib[p].assign(local.begin() + lOff[p], local.begin() + lOff[p] + int64_t(t) * t);
+      }
+    } else
 #pragma omp parallel
     {
 #pragma omp for schedule(dynamic, 1)
@@ -307,12 +361,16 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int dense
         for (int c2 = 0; c2 < t; c2++) bs.Sinv[size_t(touch[c1]) * nS + touch[c2]] -= contrib[p][size_t(c1) * t + c2];
     }
     // symmetrise against rounding, then invert
+    lap(2);
     for (int a = 0; a < nS; a++)
       for (int c = 0; c < a; c++) {
         double v = 0.5 * (bs.Sinv[size_t(a) * nS + c] + bs.Sinv[size_t(c) * nS + a]);
         bs.Sinv[size_t(a) * nS + c] = bs.Sinv[size_t(c) * nS + a] = v;
       }
-    if (!dense_spd_inverse(bs.Sinv.data(), nS, true)) { err = "boundary Schur complement is not positive definite"; return false; }
+    const bool inverted = dense ? dense->spd_inverse_batched(bs.Sinv.data(), std::vector<int64_t>(1, 0), std::vector<int>(1, nS), err)
+                                : dense_spd_inverse(bs.Sinv.data(), nS, true);
+    if (!inverted) { err = "boundary Schur complement is not positive definite" + (err.empty() ? std::string() : ": " + err); return false; }
+    lap(3);
   }
   // ---- boundary-deep coupling rows in solver order (unscaled, global texel columns)
   std::vector<Triplet> tBD;
@@ -321,6 +379,7 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int dense
     for (int kk = BD.ptr[i]; kk < BD.ptr[i + 1]; kk++) tBD.push_back({k, BD.col[kk], BD.val[kk]});
   }
   bs.BD = csr_from_triplets(nb, BD.cols, tBD);
+  lap(0);
   return true;
 }
 

@@ -276,9 +276,26 @@ struct BoundarySolverSetup {
   std::vector<double> W;                // Inv_p A_{I_p,touch}, m x t column-major (scaled)
   std::vector<double> Sinv;             // scaled nS x nS inverse Schur complement
   Csr BD;                               // positions x global texels (unscaled boundary-deep rows)
+  // ms spent: partition and sparse assembly, subdomain inverses, Schur
+  // products and assembly, Schur complement inverse
+  double ms[4] = {0, 0, 0, 0};
+};
+// Where the dense FP64 products of the set-up run: the host (nullptr) or a
+// device backend (system.cu: kernels/dense_kernels.cu).
+struct DenseBackend {
+  virtual ~DenseBackend() = default;
+  // in-place inverses of SPD matrices data[off[q] ..], size[q] x size[q] row-major
+  virtual bool spd_inverse_batched(double* data, const std::vector<int64_t>& off, const std::vector<int>& size, std::string& err) = 0;
+  // per subdomain p: G_p = Inv_p C_p (m_p x t_p, C_p row-major at cOff[p]) and
+  // local_p = C_p^T G_p (t_p x t_p at localOff[p])
+  virtual bool schur_products(const std::vector<double>& inv, const std::vector<int64_t>& invOff, const std::vector<int>& m,
+                              const std::vector<double>& C, const std::vector<int64_t>& cOff, const std::vector<int>& t,
+                              std::vector<double>& G, std::vector<double>& local, const std::vector<int64_t>& localOff,
+                              std::string& err) = 0;
 };
 // denseMax: blocks of at most this many rows are inverted whole (no subdomains)
-bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySolverSetup& bs, std::string& err);
+bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySolverSetup& bs, std::string& err,
+                           DenseBackend* dense = nullptr);
 bool dense_spd_inverse(double* A, int n, bool parallel);
 
 }  // namespace gdtp

@@ -417,6 +417,22 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
 // ----------------------------------------------------------------------------
 // coefficient hierarchy + device multigrid
 // ----------------------------------------------------------------------------
+namespace {
+// the dense inverses and products of the set-up on the device (kernels/dense_kernels.cu)
+struct DeviceDense final : DenseBackend {
+  cudaStream_t s;
+  explicit DeviceDense(cudaStream_t stream) : s(stream) {}
+  bool spd_inverse_batched(double* data, const std::vector<int64_t>& off, const std::vector<int>& size, std::string& err) override {
+    return dev::gpu_spd_inverse_batched(data, off, size, s, err);
+  }
+  bool schur_products(const std::vector<double>& inv, const std::vector<int64_t>& invOff, const std::vector<int>& m,
+                      const std::vector<double>& C, const std::vector<int64_t>& cOff, const std::vector<int>& t, std::vector<double>& G,
+                      std::vector<double>& local, const std::vector<int64_t>& localOff, std::string& err) override {
+    return dev::gpu_schur_products(inv, invOff, m, C, cOff, t, G, local, localOff, s, err);
+  }
+};
+}  // namespace
+
 static double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -493,6 +509,7 @@ bool DeviceSystem::update(double stiffness, double screen) {
   }
   mg32_.clear();
   mg64_.reset();
+  bsCache_.clear();
   invalidate_graph();
   updated_ = true;
   setupMs[0] = now_ms() - tUpdate;
@@ -502,8 +519,15 @@ bool DeviceSystem::update(double stiffness, double screen) {
 template <typename T>
 bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
   const double tBuild = now_ms();
-  double tBoundary = 0, tCoarse = 0;
+  double tBoundary = 0, tCoarse = 0, tBs[4] = {0, 0, 0, 0};
   const int L = levelsUsed_;
+  DeviceDense deviceDense(stream_);
+  DenseBackend* dense = knobs.deviceFactor ? &deviceDense : nullptr;
+  const int bsKey[3] = {knobs.maxBlock, knobs.denseBoundaryMax, knobs.deviceFactor};
+  if (!std::equal(bsKey, bsKey + 3, bsCacheKey_) || (int)bsCache_.size() != L) {
+    bsCache_.assign(L, nullptr);
+    std::copy(bsKey, bsKey + 3, bsCacheKey_);
+  }
   DeviceArena& A = mg.arena;
   mg.levels.assign(L, LevelDev<T>());
   mg.KP = KP;
@@ -522,17 +546,20 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       Csr full;
       full_matrix(G, C, full);
       const int n = G.numTexels;
-      std::vector<double> dense(size_t(n) * n, 0.0), scale(n);
+      std::vector<double> denseA(size_t(n) * n, 0.0), scale(n);
       for (int i = 0; i < n; i++)
         for (int k = full.ptr[i]; k < full.ptr[i + 1]; k++)
           if (full.col[k] == i) scale[i] = 1.0 / std::sqrt(full.val[k]);
       for (int i = 0; i < n; i++)
-        for (int k = full.ptr[i]; k < full.ptr[i + 1]; k++) dense[size_t(i) * n + full.col[k]] = full.val[k] * scale[i] * scale[full.col[k]];
+        for (int k = full.ptr[i]; k < full.ptr[i + 1]; k++) denseA[size_t(i) * n + full.col[k]] = full.val[k] * scale[i] * scale[full.col[k]];
       const double t0 = now_ms();
-      if (!dense_spd_inverse(dense.data(), n, true)) { err_ = "coarsest operator is not positive definite"; return false; }
+      std::string e;
+      const bool inverted = dense ? dense->spd_inverse_batched(denseA.data(), std::vector<int64_t>(1, 0), std::vector<int>(1, n), e)
+                                  : dense_spd_inverse(denseA.data(), n, true);
+      if (!inverted) { err_ = "coarsest operator is not positive definite" + (e.empty() ? std::string() : ": " + e); return false; }
       tCoarse += now_ms() - t0;
       mg.coarseN = n;
-      mg.coarseInv = A.upload(dense);
+      mg.coarseInv = A.upload(denseA);
       mg.coarseScale = A.upload(scale);
       continue;
     }
@@ -591,15 +618,20 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       D.bVal = A.upload(val);
       D.bGlobal = A.upload(G.boundaryGlobal);
     }
-    // exact boundary solver
+    // exact boundary solver (set up once per update, for either multigrid)
     {
-      BoundarySolverSetup bs;
-      const double t0 = now_ms();
-      if (!build_boundary_solver(C.bb, C.bd, knobs.maxBlock, knobs.denseBoundaryMax, bs, err_)) {
-        err_ = "level " + std::to_string(l) + ": " + err_;
-        return false;
+      if (!bsCache_[l]) {
+        auto built = std::make_shared<BoundarySolverSetup>();
+        const double t0 = now_ms();
+        if (!build_boundary_solver(C.bb, C.bd, knobs.maxBlock, knobs.denseBoundaryMax, *built, err_, dense)) {
+          err_ = "level " + std::to_string(l) + ": " + err_;
+          return false;
+        }
+        tBoundary += now_ms() - t0;
+        for (int q = 0; q < 4; q++) tBs[q] += built->ms[q];
+        bsCache_[l] = built;
       }
-      tBoundary += now_ms() - t0;
+      const BoundarySolverSetup& bs = *bsCache_[l];
       dev::BoundaryDev<T>& B = D.B;
       B.nb = bs.nb;
       B.nSub = bs.nSub;
@@ -717,6 +749,7 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
   setupMs[1] = tBoundary;
   setupMs[2] = tCoarse;
   setupMs[3] = now_ms() - tBuild - tBoundary - tCoarse;
+  std::copy(tBs, tBs + 4, setupMs + 4);
   return check(cudaMemset(mg.barrier, 0, sizeof(dev::GridBarrierState)), "grid barrier");
 }
 

@@ -117,6 +117,7 @@ struct SolverKnobs {
   int tileRounds = 1;                   // passes over the four tile colours per smoothing step (the
                                         // step's sweeps split between them)
   int tileFinish = 0;                   // 1: one global colour sweep after each tiled smoothing step
+  int deviceFactor = 1;                 // dense set-up inverses and products on the device (0: host)
 };
 
 struct SolveReport {
@@ -227,8 +228,10 @@ class DeviceSystem {
   std::vector<double> level_stats() const;
   // last set-up, ms: update (weights, Galerkin coarsening, FP64 operators),
   // boundary solver factorisations, coarsest inverse, other multigrid set-up
-  // (device layouts, uploads); the last three when the multigrid is built
-  double setupMs[4] = {0, 0, 0, 0};
+  // (device layouts, uploads); the last three when the multigrid is built;
+  // then the boundary solver factorisations split into partition and sparse
+  // assembly, subdomain inverses, Schur products, Schur complement inverse
+  double setupMs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int graphKernels = 0;         // kernel nodes in the refinement-step graph
   int64_t kernelLaunches = 0;   // kernels launched by solve_mixed since the last profile reset
 
@@ -258,6 +261,10 @@ class DeviceSystem {
   ChartMetrics metric_;
   std::vector<LevelCoefficients> coeffs_;
   std::vector<LevelCoefficients> coMass_, coStiff_;  // Galerkin hierarchies of M and S (levels coLevels_)
+  // boundary solver set-ups per level, shared by the FP32 and FP64 multigrids of
+  // one update (cleared by update; keyed by the knobs that shape them)
+  std::vector<std::shared_ptr<BoundarySolverSetup>> bsCache_;
+  int bsCacheKey_[3] = {-1, -1, -1};
   int coLevels_ = 0;
   int levelsUsed_ = 0;
   double stiffness_ = 0, screen_ = 0;

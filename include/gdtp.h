@@ -115,8 +115,10 @@ void gdtp_system_free(gdtp_system* s);
  *   kernels per step graph, kernels launched by solves, 1 if a timed group is one
  *   fused tile-smoother launch (else colour sweeps)}; "profile.reset" clears the counts
  *   "profile.setup": ms of the last set-up {update, boundary solver factorisations,
- *   coarsest inverse, other multigrid set-up}; the last three are spent by the
- *   first solve after an update (or after a new right-hand-side width) */
+ *   coarsest inverse, other multigrid set-up, then the factorisations split into
+ *   partition and sparse assembly, subdomain inverses, Schur products, Schur
+ *   complement inverse}; all but the first are spent by the first solve after
+ *   an update (or after a new right-hand-side width) */
 int gdtp_system_array(const gdtp_system* s, const char* name, int level, void* out, int64_t* count);
 
 /* Combine and coarsen: A = screen*M + stiffness*S and its Galerkin hierarchy;
@@ -242,7 +244,12 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * levels, default 2/2), "tile_rounds"
  * (passes over the tiles per smoothing step, the sweeps split between them,
  * default 1), "tile_finish" (0/1: one global colour sweep closes each tiled
- * smoothing step).  The autotuner leaves the tile smoother off: with host
+ * smoothing step), "device_factor" (0/1, default 1: the dense FP64 inverses
+ * and products of the set-up -- boundary subdomain blocks, separator Schur
+ * complement, coarsest level -- run on the device by blocked Gauss-Jordan
+ * elimination; 0 = host Cholesky).  "max_block", "max_coarse",
+ * "dense_boundary_max", "device_factor" and "tile_texels" drop the built
+ * multigrids; the next solve builds them again.  The autotuner leaves the tile smoother off: with host
  * copies running beside the solve (gdtp_solve_stream) its rounds slow down
  * more than the sweeps they replace. */
 int gdtp_system_set(gdtp_system* s, const char* knob, double value);
