@@ -23,7 +23,7 @@ BUILD = os.path.join(ROOT, "_build")
 SOURCES = [
     "setup/atlas.cpp", "setup/grid.cpp", "setup/csr.cpp", "setup/boundary.cpp", "setup/assembly.cpp",
     "setup/galerkin.cpp", "setup/bsolve.cpp", "setup/metric.cpp", "io/png.cpp", "io/ply.cpp", "io/texture_io.cpp", "capi_io.cpp",
-    "capi_hierarchy.cpp", "capi_system.cpp", "capi_metric.cpp", "capi_geodesics.cpp", "geodesics.cu", "capi_server.cpp", "server.cpp", "system.cu", "brush.cu", "noalloc.cu",
+    "capi_hierarchy.cpp", "capi_system.cpp", "capi_metric.cpp", "capi_geodesics.cpp", "geodesics.cu", "capi_server.cpp", "server.cpp", "system.cu", "numeric.cu", "brush.cu", "noalloc.cu",
     "kernels/vcycle_kernels.cu", "kernels/tile_smoother.cu", "kernels/dense_kernels.cu", "kernels/coarse_cycle.cu", "kernels/geodesic_kernels.cu", "kernels/assembly_kernels.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -36,12 +36,6 @@ constexpr int kPB = 64;  // pivot block of the blocked Gauss-Jordan elimination
 // is A (M x K, leading dimension lda) or, with transA, the transpose of A
 // stored K x M.  64 x 64 tiles, 256 threads of 4 x 4 outputs each (rows ty +
 // 16 r, columns tx + 16 c), K in chunks of 16 through shared memory.
-struct GemmTask {
-  long long a, b, c;
-  int M, N, K, lda, ldb, ldc, transA, pad;
-  double alpha, beta;
-};
-
 __global__ void __launch_bounds__(256) k_gemm(const GemmTask* __restrict__ tasks, const double* __restrict__ A,
                                               const double* __restrict__ B, double* __restrict__ C) {
   const GemmTask T = tasks[blockIdx.z];
@@ -246,46 +240,47 @@ bool upload(Buf& b, const std::vector<T>& v, cudaStream_t s, std::string& err) {
 
 constexpr int kMaxGridZ = 65535;
 
-void gemm_launch(const GemmTask* dTasks, int nTasks, int maxM, int maxN, const double* A, const double* B, double* C, cudaStream_t s) {
+}  // namespace
+
+void launch_gemm_batch(const GemmTask* dTasks, int nTasks, int maxM, int maxN, const double* A, const double* B, double* C,
+                       cudaStream_t s) {
   for (int t0 = 0; t0 < nTasks; t0 += kMaxGridZ) {
     const dim3 grid(unsigned((maxN + 63) / 64), unsigned((maxM + 63) / 64), unsigned(std::min(kMaxGridZ, nTasks - t0)));
     k_gemm<<<grid, 256, 0, s>>>(dTasks + t0, A, B, C);
   }
 }
 
-}  // namespace
-
-bool gpu_spd_inverse_batched(double* data, const std::vector<int64_t>& offsets, const std::vector<int>& sizes, cudaStream_t s,
-                             std::string& err) {
-  const int nMat = (int)sizes.size();
-  if (nMat == 0) return true;
-  std::vector<int64_t> first(nMat), ws(nMat);
-  long long total = 0, elems = 0, wsTotal = 0;
-  int mMax = 0;
-  for (int q = 0; q < nMat; q++) {
-    first[q] = total;
-    ws[q] = wsTotal;
-    total += (long long)sizes[q] * sizes[q];
-    wsTotal += (long long)kPB * sizes[q];
-    elems = std::max<long long>(elems, offsets[q] + (long long)sizes[q] * sizes[q]);
-    mMax = std::max(mMax, sizes[q]);
-  }
-  if (mMax == 0) return true;
-  if (nMat > kMaxGridZ) {
+bool spd_inverse_layout(const std::vector<int64_t>& offsets, const std::vector<int>& sizes, SpdInverseLayout& L, std::string& err) {
+  L = SpdInverseLayout();
+  L.nMat = (int)sizes.size();
+  if (L.nMat > kMaxGridZ) {
     err = "more dense blocks than one launch holds";
     return false;
   }
-  const int steps = (mMax + kPB - 1) / kPB;
+  L.offsets = offsets;
+  L.sizes = sizes;
+  L.first.resize(L.nMat);
+  L.ws.resize(L.nMat);
+  int mMax = 0;
+  for (int q = 0; q < L.nMat; q++) {
+    L.first[q] = L.total;
+    L.ws[q] = L.wsTotal;
+    L.total += (long long)sizes[q] * sizes[q];
+    L.wsTotal += (long long)kPB * sizes[q];
+    L.elems = std::max<long long>(L.elems, offsets[q] + (long long)sizes[q] * sizes[q]);
+    mMax = std::max(mMax, sizes[q]);
+  }
+  L.steps = (mMax + kPB - 1) / kPB;
   // rank-64 update tasks of every step: A_q -= Cold_q R_q over the matrices still eliminating
-  std::vector<GemmTask> tasks;
-  std::vector<int> taskStart(steps + 1, 0), stepMax(steps, 0);
-  for (int k = 0; k < steps; k++) {
-    for (int q = 0; q < nMat; q++) {
+  L.taskStart.assign(L.steps + 1, 0);
+  L.stepMax.assign(L.steps, 0);
+  for (int k = 0; k < L.steps; k++) {
+    for (int q = 0; q < L.nMat; q++) {
       const int m = sizes[q], kb = k * kPB;
       if (kb >= m) continue;
       GemmTask T{};
-      T.a = ws[q];
-      T.b = ws[q];
+      T.a = L.ws[q];
+      T.b = L.ws[q];
       T.c = offsets[q];
       T.M = T.N = m;
       T.K = std::min(kPB, m - kb);
@@ -294,43 +289,76 @@ bool gpu_spd_inverse_batched(double* data, const std::vector<int64_t>& offsets, 
       T.ldc = m;
       T.alpha = -1.0;
       T.beta = 1.0;
-      tasks.push_back(T);
-      stepMax[k] = std::max(stepMax[k], m);
+      L.tasks.push_back(T);
+      L.stepMax[k] = std::max(L.stepMax[k], m);
     }
-    taskStart[k + 1] = (int)tasks.size();
+    L.taskStart[k + 1] = (int)L.tasks.size();
   }
-  Buf a, b, off, siz, fir, wso, bad, pinv, rw, cw, tk;
-  if (!upload(a, data, size_t(elems), s, err) || !alloc(b, size_t(elems) * sizeof(double), s, err) || !upload(off, offsets, s, err) ||
-      !upload(siz, sizes, s, err) || !upload(fir, first, s, err) || !upload(wso, ws, s, err) ||
-      !upload(bad, std::vector<int>(1, 0), s, err) || !alloc(pinv, size_t(nMat) * kPB * kPB * sizeof(double), s, err) ||
-      !alloc(rw, size_t(wsTotal) * sizeof(double), s, err) || !alloc(cw, size_t(wsTotal) * sizeof(double), s, err) ||
-      !upload(tk, tasks, s, err))
-    return false;
-  const int panelSmem = 2 * kPB * (kPB + 1) * sizeof(double);
-  if (!check(cudaFuncSetAttribute(k_bgj_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, panelSmem), "panel attribute", err))
-    return false;
-  const long long* dOff = off.as<long long>();
-  for (int k = 0; k < steps; k++) {
-    // a matrix of size m has ceil(m/64) column tiles; tiles past its own size return at once
-    k_bgj_diag<<<nMat, 256, 0, s>>>(k, dOff, siz.as<int>(), a.as<double>(), pinv.as<double>(), bad.as<int>());
-    const dim3 pg(unsigned((stepMax[k] + kPB - 1) / kPB), 2, unsigned(nMat));
-    k_bgj_panel<<<pg, 256, panelSmem, s>>>(k, dOff, siz.as<int>(), wso.as<long long>(), a.as<double>(), pinv.as<double>(),
-                                           rw.as<double>(), cw.as<double>());
-    gemm_launch(tk.as<GemmTask>() + taskStart[k], taskStart[k + 1] - taskStart[k], stepMax[k], stepMax[k], cw.as<double>(),
-                rw.as<double>(), a.as<double>(), s);
+  return true;
+}
+
+size_t spd_inverse_scratch_doubles(const SpdInverseLayout& L) { return size_t(L.nMat) * kPB * kPB + 2 * size_t(L.wsTotal); }
+
+bool launch_spd_inverse(const SpdInverseLayout& L, const SpdInverseDevice& D, double* A, double* out, double* scratch, int* bad,
+                        cudaStream_t s) {
+  if (L.nMat == 0 || L.steps == 0) return true;
+  static const int panelSmem = 2 * kPB * (kPB + 1) * sizeof(double);
+  if (cudaFuncSetAttribute(k_bgj_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, panelSmem) != cudaSuccess) return false;
+  double* pinv = scratch;
+  double* rw = pinv + size_t(L.nMat) * kPB * kPB;
+  double* cw = rw + L.wsTotal;
+  for (int k = 0; k < L.steps; k++) {
+    // matrices of size m <= 64k, and tiles past a matrix's own size, return at once
+    k_bgj_diag<<<L.nMat, 256, 0, s>>>(k, D.off, D.size, A, pinv, bad);
+    const dim3 pg(unsigned((L.stepMax[k] + kPB - 1) / kPB), 2, unsigned(L.nMat));
+    k_bgj_panel<<<pg, 256, panelSmem, s>>>(k, D.off, D.size, D.ws, A, pinv, rw, cw);
+    launch_gemm_batch(D.tasks + L.taskStart[k], L.taskStart[k + 1] - L.taskStart[k], L.stepMax[k], L.stepMax[k], cw, rw, A, s);
   }
-  const unsigned blocks = unsigned((total + 255) / 256);
-  k_symmetrise<<<blocks, 256, 0, s>>>(nMat, dOff, siz.as<int>(), fir.as<long long>(), total, a.as<double>(), b.as<double>());
+  const unsigned blocks = unsigned((L.total + 255) / 256);
+  k_symmetrise<<<blocks, 256, 0, s>>>(L.nMat, D.off, D.size, D.first, L.total, A, out);
+  return cudaGetLastError() == cudaSuccess;
+}
+
+namespace {
+
+// device copies of a layout's arrays in stream-ordered scratch
+struct LayoutUpload {
+  Buf off, size, first, ws, tasks;
+  SpdInverseDevice dev;
+  bool run(const SpdInverseLayout& L, cudaStream_t s, std::string& err) {
+    if (!upload(off, L.offsets, s, err) || !upload(size, L.sizes, s, err) || !upload(first, L.first, s, err) ||
+        !upload(ws, L.ws, s, err) || !upload(tasks, L.tasks, s, err))
+      return false;
+    dev = {off.as<long long>(), size.as<int>(), first.as<long long>(), ws.as<long long>(), tasks.as<GemmTask>()};
+    return true;
+  }
+};
+
+}  // namespace
+
+bool gpu_spd_inverse_batched(double* data, const std::vector<int64_t>& offsets, const std::vector<int>& sizes, cudaStream_t s,
+                             std::string& err) {
+  SpdInverseLayout L;
+  if (!spd_inverse_layout(offsets, sizes, L, err)) return false;
+  if (L.nMat == 0 || L.steps == 0) return true;
+  LayoutUpload U;
+  Buf a, b, bad, scratch;
+  if (!U.run(L, s, err) || !upload(a, data, size_t(L.elems), s, err) || !alloc(b, size_t(L.elems) * sizeof(double), s, err) ||
+      !upload(bad, std::vector<int>(1, 0), s, err) || !alloc(scratch, spd_inverse_scratch_doubles(L) * sizeof(double), s, err))
+    return false;
+  if (!launch_spd_inverse(L, U.dev, a.as<double>(), b.as<double>(), scratch.as<double>(), bad.as<int>(), s)) {
+    err = std::string("Gauss-Jordan: ") + cudaGetErrorString(cudaGetLastError());
+    return false;
+  }
   int badHost = 0;
-  if (!check(cudaGetLastError(), "Gauss-Jordan", err) ||
-      !check(cudaMemcpyAsync(&badHost, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s), "d2h", err) ||
+  if (!check(cudaMemcpyAsync(&badHost, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s), "d2h", err) ||
       !check(cudaStreamSynchronize(s), "Gauss-Jordan", err))
     return false;
   if (badHost) {
     err = "dense block is not positive definite";
     return false;
   }
-  for (int q = 0; q < nMat; q++) {
+  for (int q = 0; q < L.nMat; q++) {
     const size_t bytes = size_t(sizes[q]) * sizes[q] * sizeof(double);
     if (bytes && !check(cudaMemcpyAsync(data + offsets[q], b.as<double>() + offsets[q], bytes, cudaMemcpyDeviceToHost, s), "d2h", err))
       return false;
@@ -338,17 +366,13 @@ bool gpu_spd_inverse_batched(double* data, const std::vector<int64_t>& offsets, 
   return check(cudaStreamSynchronize(s), "Gauss-Jordan", err);
 }
 
-bool gpu_schur_products(const std::vector<double>& inv, const std::vector<int64_t>& invOff, const std::vector<int>& m,
-                        const std::vector<double>& C, const std::vector<int64_t>& cOff, const std::vector<int>& t, std::vector<double>& G,
-                        std::vector<double>& local, const std::vector<int64_t>& localOff, cudaStream_t s, std::string& err) {
-  const int nSub = (int)m.size();
-  G.assign(C.size(), 0.0);
-  long long localTotal = 0;
-  for (int p = 0; p < nSub; p++) localTotal = std::max<long long>(localTotal, localOff[p] + (long long)t[p] * t[p]);
-  local.assign(size_t(localTotal), 0.0);
-  std::vector<GemmTask> gTasks, lTasks;
-  int maxM = 1, maxT = 1;
-  for (int p = 0; p < nSub; p++) {
+void schur_product_tasks(const std::vector<int64_t>& invOff, const std::vector<int>& m, const std::vector<int64_t>& cOff,
+                         const std::vector<int>& t, const std::vector<int64_t>& localOff, std::vector<GemmTask>& gTasks,
+                         std::vector<GemmTask>& lTasks, int& maxM, int& maxT) {
+  gTasks.clear();
+  lTasks.clear();
+  maxM = maxT = 1;
+  for (size_t p = 0; p < m.size(); p++) {
     if (t[p] == 0 || m[p] == 0) continue;
     GemmTask g{};  // G = Inv C   (m x t)
     g.a = invOff[p];
@@ -378,13 +402,26 @@ bool gpu_schur_products(const std::vector<double>& inv, const std::vector<int64_
     maxM = std::max(maxM, m[p]);
     maxT = std::max(maxT, t[p]);
   }
+}
+
+bool gpu_schur_products(const std::vector<double>& inv, const std::vector<int64_t>& invOff, const std::vector<int>& m,
+                        const std::vector<double>& C, const std::vector<int64_t>& cOff, const std::vector<int>& t, std::vector<double>& G,
+                        std::vector<double>& local, const std::vector<int64_t>& localOff, cudaStream_t s, std::string& err) {
+  const int nSub = (int)m.size();
+  G.assign(C.size(), 0.0);
+  long long localTotal = 0;
+  for (int p = 0; p < nSub; p++) localTotal = std::max<long long>(localTotal, localOff[p] + (long long)t[p] * t[p]);
+  local.assign(size_t(localTotal), 0.0);
+  std::vector<GemmTask> gTasks, lTasks;
+  int maxM = 1, maxT = 1;
+  schur_product_tasks(invOff, m, cOff, t, localOff, gTasks, lTasks, maxM, maxT);
   if (gTasks.empty()) return true;
   Buf dInv, dC, dG, dL, dgt, dlt;
   if (!upload(dInv, inv, s, err) || !upload(dC, C, s, err) || !alloc(dG, C.size() * sizeof(double), s, err) ||
       !alloc(dL, size_t(localTotal) * sizeof(double), s, err) || !upload(dgt, gTasks, s, err) || !upload(dlt, lTasks, s, err))
     return false;
-  gemm_launch(dgt.as<GemmTask>(), (int)gTasks.size(), maxM, maxT, dInv.as<double>(), dC.as<double>(), dG.as<double>(), s);
-  gemm_launch(dlt.as<GemmTask>(), (int)lTasks.size(), maxT, maxT, dC.as<double>(), dG.as<double>(), dL.as<double>(), s);
+  launch_gemm_batch(dgt.as<GemmTask>(), (int)gTasks.size(), maxM, maxT, dInv.as<double>(), dC.as<double>(), dG.as<double>(), s);
+  launch_gemm_batch(dlt.as<GemmTask>(), (int)lTasks.size(), maxT, maxT, dC.as<double>(), dG.as<double>(), dL.as<double>(), s);
   if (!check(cudaGetLastError(), "products", err) ||
       !check(cudaMemcpyAsync(G.data(), dG.p, G.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h", err) ||
       !check(cudaMemcpyAsync(local.data(), dL.p, local.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "d2h", err) ||

@@ -238,8 +238,46 @@ void launch_boundary_triangles(int n, const int* btPtr, const int* btTri, const 
                                const double* triMetric, const double* triMetricInv, double* mass, double* stiff, cudaStream_t s);
 void launch_gather_cells(int n, const int* idx, const double* src, double* dst, cudaStream_t s);
 
-// Dense FP64 set-up products (kernels/dense_kernels.cu), synchronous on s.
-// In-place inverses of SPD matrices data[off[q] ..] (size[q] x size[q],
+// Dense FP64 set-up products (kernels/dense_kernels.cu).
+// One task of a batched C = alpha op(A) B + beta C (row-major, offsets in
+// doubles into the A, B and C buffers of the launch; op(A) = A (M x K) or,
+// transA, the transpose of A stored K x M).
+struct GemmTask {
+  long long a, b, c;
+  int M, N, K, lda, ldb, ldc, transA, pad;
+  double alpha, beta;
+};
+void launch_gemm_batch(const GemmTask* dTasks, int nTasks, int maxM, int maxN, const double* A, const double* B, double* C,
+                       cudaStream_t s);
+// Batched inverse of SPD blocks by blocked Gauss-Jordan elimination: the
+// layout (host) of blocks q at offsets[q], sizes[q] x sizes[q] row-major, and
+// its device arrays (uploaded by the caller from the layout's vectors).
+struct SpdInverseLayout {
+  int nMat = 0, steps = 0;
+  long long total = 0, elems = 0, wsTotal = 0;
+  std::vector<int64_t> offsets, first, ws;
+  std::vector<int> sizes, taskStart, stepMax;
+  std::vector<GemmTask> tasks;
+};
+struct SpdInverseDevice {
+  const long long* off;
+  const int* size;
+  const long long* first;
+  const long long* ws;
+  const GemmTask* tasks;
+};
+bool spd_inverse_layout(const std::vector<int64_t>& offsets, const std::vector<int>& sizes, SpdInverseLayout& L, std::string& err);
+// scratch doubles one launch_spd_inverse needs
+size_t spd_inverse_scratch_doubles(const SpdInverseLayout& L);
+// A (elems doubles, destroyed) -> out = the exactly symmetric inverses at the
+// same offsets; *bad set to 1 on a non-positive pivot (caller zeroes it)
+bool launch_spd_inverse(const SpdInverseLayout& L, const SpdInverseDevice& D, double* A, double* out, double* scratch, int* bad,
+                        cudaStream_t s);
+// per block p: G_p = Inv_p C_p (m x t at cOff[p]) and local_p = C_p^T G_p (t x t at localOff[p])
+void schur_product_tasks(const std::vector<int64_t>& invOff, const std::vector<int>& m, const std::vector<int64_t>& cOff,
+                         const std::vector<int>& t, const std::vector<int64_t>& localOff, std::vector<GemmTask>& gTasks,
+                         std::vector<GemmTask>& lTasks, int& maxM, int& maxT);
+// Host-vector forms, synchronous on s: in-place inverses of SPD matrices data[off[q] ..] (size[q] x size[q],
 // row-major) by Gauss-Jordan elimination, made exactly symmetric.
 bool gpu_spd_inverse_batched(double* data, const std::vector<int64_t>& offsets, const std::vector<int>& sizes, cudaStream_t s,
                              std::string& err);

@@ -127,29 +127,12 @@ bool dense_spd_inverse(double* A, int n, bool parallel) {
   return true;
 }
 
-namespace {
-double wall_ms() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
-}  // namespace
-
-bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySolverSetup& bs, std::string& err,
-                           DenseBackend* dense) {
-  double tMark = wall_ms();
-  auto lap = [&](int slot) {
-    const double t = wall_ms();
-    bs.ms[slot] += t - tMark;
-    tMark = t;
-  };
+void partition_boundary(const Csr& BB, int maxBlock, int denseMax, std::vector<int>& order, std::vector<int>& subPtr, int& nI) {
   const int nb = BB.rows;
-  bs = BoundarySolverSetup();
-  bs.nb = nb;
-  if (nb == 0) return true;
-  std::vector<double> diag(nb, 0.0);
-  for (int i = 0; i < nb; i++)
-    for (int k = BB.ptr[i]; k < BB.ptr[i + 1]; k++)
-      if (BB.col[k] == i) diag[i] = BB.val[k];
-  for (int i = 0; i < nb; i++)
-    if (!(diag[i] > 0)) { err = "boundary block has a non-positive diagonal"; return false; }
-
+  order.clear();
+  subPtr.assign(1, 0);
+  nI = 0;
+  if (nb == 0) return;
   // ---- subdomains: breadth-first growth from the lowest unassigned row
   std::vector<int> part(nb, -1);
   int nSub = 0;
@@ -189,16 +172,43 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int dense
   std::vector<std::vector<int>> members(nSub);
   for (int u = 0; u < nb; u++)
     if (!sep[u]) members[part[u]].push_back(u);
-  bs.subPtr.assign(1, 0);
+  subPtr.assign(1, 0);
   for (int p = 0; p < nSub; p++) {
     if (members[p].empty()) continue;
-    bs.order.insert(bs.order.end(), members[p].begin(), members[p].end());
-    bs.subPtr.push_back((int)bs.order.size());
+    order.insert(order.end(), members[p].begin(), members[p].end());
+    subPtr.push_back((int)order.size());
   }
-  bs.nSub = (int)bs.subPtr.size() - 1;
-  bs.nI = (int)bs.order.size();
+  nI = (int)order.size();
   for (int u = 0; u < nb; u++)
-    if (sep[u]) bs.order.push_back(u);
+    if (sep[u]) order.push_back(u);
+}
+
+namespace {
+double wall_ms() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+}  // namespace
+
+bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySolverSetup& bs, std::string& err,
+                           DenseBackend* dense) {
+  double tMark = wall_ms();
+  auto lap = [&](int slot) {
+    const double t = wall_ms();
+    bs.ms[slot] += t - tMark;
+    tMark = t;
+  };
+  const int nb = BB.rows;
+  bs = BoundarySolverSetup();
+  bs.nb = nb;
+  if (nb == 0) return true;
+  std::vector<double> diag(nb, 0.0);
+  for (int i = 0; i < nb; i++)
+    for (int k = BB.ptr[i]; k < BB.ptr[i + 1]; k++)
+      if (BB.col[k] == i) diag[i] = BB.val[k];
+  for (int i = 0; i < nb; i++)
+    if (!(diag[i] > 0)) { err = "boundary block has a non-positive diagonal"; return false; }
+
+  // ---- subdomains and separator; order: interiors grouped by subdomain, then separators
+  partition_boundary(BB, maxBlock, denseMax, bs.order, bs.subPtr, bs.nI);
+  bs.nSub = (int)bs.subPtr.size() - 1;
   bs.nS = nb - bs.nI;
   std::vector<int> pos(nb);
   for (int k = 0; k < nb; k++) pos[bs.order[k]] = k;
@@ -380,6 +390,95 @@ bool build_boundary_solver(const Csr& BB, const Csr& BD, int maxBlock, int dense
   }
   bs.BD = csr_from_triplets(nb, BD.cols, tBD);
   lap(0);
+  return true;
+}
+
+bool build_boundary_symbolic(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySymbolic& sym, std::string& err) {
+  const int nb = BB.rows;
+  sym = BoundarySymbolic();
+  sym.nb = nb;
+  if (nb == 0) return true;
+  sym.bbRow.resize(BB.col.size());
+  sym.diagEntry.assign(nb, -1);
+  for (int i = 0; i < nb; i++)
+    for (int k = BB.ptr[i]; k < BB.ptr[i + 1]; k++) {
+      sym.bbRow[k] = i;
+      if (BB.col[k] == i) sym.diagEntry[i] = k;
+    }
+  for (int i = 0; i < nb; i++)
+    if (sym.diagEntry[i] < 0) { err = "boundary block has no diagonal entry"; return false; }
+  partition_boundary(BB, maxBlock, denseMax, sym.order, sym.subPtr, sym.nI);
+  sym.nSub = (int)sym.subPtr.size() - 1;
+  sym.nS = nb - sym.nI;
+  sym.pos.resize(nb);
+  for (int k = 0; k < nb; k++) sym.pos[sym.order[k]] = k;
+  std::vector<int> subOf(nb, -1);
+  for (int p = 0; p < sym.nSub; p++)
+    for (int k = sym.subPtr[p]; k < sym.subPtr[p + 1]; k++) subOf[k] = p;
+  // subdomain blocks (row-major m x m per subdomain) and the separator block
+  sym.invOff.assign(sym.nSub + 1, 0);
+  for (int p = 0; p < sym.nSub; p++) {
+    const int64_t m = sym.subPtr[p + 1] - sym.subPtr[p];
+    sym.invOff[p + 1] = sym.invOff[p] + m * m;
+  }
+  // entries between interior and separator rows: AIS (interior rows), with the
+  // BB entry in place of the value
+  std::vector<Triplet> tIS;
+  for (int i = 0; i < nb; i++)
+    for (int k = BB.ptr[i]; k < BB.ptr[i + 1]; k++) {
+      const int a = sym.pos[i], c = sym.pos[BB.col[k]];
+      if (a < sym.nI && c < sym.nI) {
+        const int p = subOf[a];
+        if (subOf[c] != p) continue;  // no coupling between different subdomains' interiors
+        const int b0 = sym.subPtr[p], m = sym.subPtr[p + 1] - b0;
+        sym.fillEntry.push_back(k);
+        sym.fillDest.push_back(sym.invOff[p] + int64_t(a - b0) * m + (c - b0));
+      } else if (a < sym.nI) {
+        tIS.push_back({a, c - sym.nI, double(k)});
+      } else if (c >= sym.nI) {
+        sym.ssEntry.push_back(k);
+        sym.ssDest.push_back(int64_t(a - sym.nI) * sym.nS + (c - sym.nI));
+      }
+    }
+  sym.AIS = csr_from_triplets(sym.nI, sym.nS, tIS);
+  sym.ASI = csr_transpose(sym.AIS);
+  // separator columns per subdomain, and the m x t blocks of C_p = A_{I_p,touch}
+  sym.touchPtr.assign(sym.nSub + 1, 0);
+  std::vector<std::vector<int>> touches(sym.nSub);
+  for (int p = 0; p < sym.nSub; p++) {
+    std::vector<int>& touch = touches[p];
+    for (int a = sym.subPtr[p]; a < sym.subPtr[p + 1]; a++)
+      for (int kk = sym.AIS.ptr[a]; kk < sym.AIS.ptr[a + 1]; kk++) touch.push_back(sym.AIS.col[kk]);
+    std::sort(touch.begin(), touch.end());
+    touch.erase(std::unique(touch.begin(), touch.end()), touch.end());
+    sym.touchPtr[p + 1] = sym.touchPtr[p] + (int)touch.size();
+  }
+  sym.wOff.assign(sym.nSub + 1, 0);
+  sym.lOff.assign(sym.nSub + 1, 0);
+  for (int p = 0; p < sym.nSub; p++) {
+    const int64_t m = sym.subPtr[p + 1] - sym.subPtr[p], t = (int64_t)touches[p].size();
+    sym.wOff[p + 1] = sym.wOff[p] + m * t;
+    sym.lOff[p + 1] = sym.lOff[p] + t * t;
+    sym.touch.insert(sym.touch.end(), touches[p].begin(), touches[p].end());
+  }
+  sym.aisDest.resize(sym.AIS.col.size());
+  for (int p = 0; p < sym.nSub; p++) {
+    const int b0 = sym.subPtr[p];
+    const std::vector<int>& touch = touches[p];
+    const int t = (int)touch.size();
+    for (int a = b0; a < sym.subPtr[p + 1]; a++)
+      for (int kk = sym.AIS.ptr[a]; kk < sym.AIS.ptr[a + 1]; kk++) {
+        const int c = int(std::lower_bound(touch.begin(), touch.end(), sym.AIS.col[kk]) - touch.begin());
+        sym.aisDest[kk] = sym.wOff[p] + int64_t(a - b0) * t + c;
+      }
+  }
+  // boundary-deep rows in solver order, with the BD entry in place of the value
+  std::vector<Triplet> tBD;
+  for (int k = 0; k < nb; k++) {
+    const int i = sym.order[k];
+    for (int kk = BD.ptr[i]; kk < BD.ptr[i + 1]; kk++) tBD.push_back({k, BD.col[kk], double(kk)});
+  }
+  sym.BD = csr_from_triplets(nb, BD.cols, tBD);
   return true;
 }
 

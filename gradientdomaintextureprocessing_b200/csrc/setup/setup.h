@@ -280,6 +280,33 @@ struct BoundarySolverSetup {
   // products and assembly, Schur complement inverse
   double ms[4] = {0, 0, 0, 0};
 };
+// Subdomains and separator of a boundary block from its pattern alone:
+// order (position -> row; interiors grouped by subdomain, then the separator),
+// subPtr (subdomain -> position range), nI (interior positions).
+void partition_boundary(const Csr& BB, int maxBlock, int denseMax, std::vector<int>& order, std::vector<int>& subPtr, int& nI);
+
+// The weight-independent structure of the boundary solver: the partition, and
+// for each of its values the boundary-block entry it is made from, so that the
+// values can be recomputed on the device for new weights.  A BB entry k of rows
+// i, j gives the scaled value BB_k s_pos(i) s_pos(j), s = 1 / sqrt(diag).
+struct BoundarySymbolic {
+  int nb = 0, nSub = 0, nI = 0, nS = 0;
+  std::vector<int> order, pos, subPtr;
+  std::vector<int> bbRow;                   // BB entry -> its row
+  std::vector<int> diagEntry;               // row -> its diagonal BB entry
+  std::vector<int64_t> invOff;              // subdomain -> offset of its m x m block (nSub + 1)
+  std::vector<int> fillEntry;               // BB entries inside a subdomain block ...
+  std::vector<int64_t> fillDest;            // ... and their position in the blocks
+  std::vector<int> ssEntry;                 // BB entries between separator rows ...
+  std::vector<int64_t> ssDest;              // ... and their position in the nS x nS Schur block
+  Csr AIS, ASI;                             // interior x separator coupling and transpose; val = BB entry
+  std::vector<int64_t> aisDest;             // AIS entry -> position in the C_p blocks (m x t row-major at wOff[p])
+  std::vector<int> touchPtr, touch;         // per subdomain: the separator columns its rows couple to
+  std::vector<int64_t> wOff, lOff;          // per subdomain: m x t block offset, t x t block offset (nSub + 1)
+  Csr BD;                                   // boundary-deep rows in solver order; val = BD entry
+};
+bool build_boundary_symbolic(const Csr& BB, const Csr& BD, int maxBlock, int denseMax, BoundarySymbolic& sym, std::string& err);
+
 // Where the dense FP64 products of the set-up run: the host (nullptr) or a
 // device backend (system.cu: kernels/dense_kernels.cu).
 struct DenseBackend {

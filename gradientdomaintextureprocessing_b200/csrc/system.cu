@@ -311,6 +311,7 @@ size_t DeviceSystem::deviceBytes() const {
   size_t b = rawArena_.total + rawAArena_.total + workArena_.total + slotArena_.total;
   for (const auto& m : mg32_) b += m->arena.total;
   if (mg64_) b += mg64_->arena.total;
+  if (plan_) b += plan_->deviceBytes();
   return b;
 }
 
@@ -418,6 +419,9 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
 // coefficient hierarchy + device multigrid
 // ----------------------------------------------------------------------------
 namespace {
+bool fill_one(NumericPlan& p, int l, LevelValues<float>& v, cudaStream_t s, std::string& e) { return p.fill_level(l, &v, nullptr, s, e); }
+bool fill_one(NumericPlan& p, int l, LevelValues<double>& v, cudaStream_t s, std::string& e) { return p.fill_level(l, nullptr, &v, s, e); }
+
 // the dense inverses and products of the set-up on the device (kernels/dense_kernels.cu)
 struct DeviceDense final : DenseBackend {
   cudaStream_t s;
@@ -443,11 +447,6 @@ bool DeviceSystem::update(double stiffness, double screen) {
   if (fine_.deepMass.empty() && h_.levels[0].numDeep > 0) { err_ = "update before assembly"; return false; }
   cudaSetDevice(device_);
   const GridLevel& L0 = h_.levels[0];
-  std::vector<double> deep(fine_.deepMass.size());
-  for (size_t i = 0; i < deep.size(); i++) deep[i] = screen * fine_.deepMass[i] + stiffness * fine_.deepStiffness[i];
-  Csr bb = csr_axpby(screen, fine_.bbMass, stiffness, fine_.bbStiffness);
-  Csr bd = csr_axpby(screen, fine_.bdMass, stiffness, fine_.bdStiffness);
-  bd.cols = L0.numTexels;
   // levels used: stop once the coarsest fits the dense direct solve
   int L = (int)h_.levels.size();
   for (int l = 0; l < (int)h_.levels.size(); l++)
@@ -464,35 +463,44 @@ bool DeviceSystem::update(double stiffness, double screen) {
       return false;
     coLevels_ = L;
   }
-  std::vector<LevelCoefficients> co(L);
-  co[0].deep = std::move(deep);
-  co[0].bb = bb;
-  co[0].bd = bd;
-  for (int l = 1; l < L; l++) {
-    const LevelCoefficients &m = coMass_[l], &k = coStiff_[l];
-    co[l].deep.resize(m.deep.size());
-#pragma omp parallel for schedule(static)
-    for (long long i = 0; i < (long long)m.deep.size(); i++) co[l].deep[i] = screen * m.deep[i] + stiffness * k.deep[i];
-    co[l].bb = csr_axpby(screen, m.bb, stiffness, k.bb);
-    co[l].bd = csr_axpby(screen, m.bd, stiffness, k.bd);
-  }
-  coeffs_ = std::move(co);
+  const bool sameLevels = (levelsUsed_ == L);
   levelsUsed_ = L;
   stiffness_ = stiffness;
   screen_ = screen;
-  // raw FP64 A on level 0: its own arena, released on every update (the
-  // deep planes are screen M + stiffness S of the resident M and S planes)
-  {
+  hostCoeffs_ = false;
+  bsCache_.clear();
+  if (use_numeric()) {
+    // values on the device from the resident M and S: the multigrids built by
+    // this path keep their layout and are refilled in place
+    if (!ensure_plan() || !plan_->combine(screen, stiffness, stream_, err_)) return false;
+    if (!refresh_raw_operator()) return false;
+    bool keep = sameLevels && (!mg32_.empty() || mg64_);
+    if (!mg32_.empty()) keep = keep && mg32_.front()->planGen == plan_->gen;
+    if (mg64_) keep = keep && mg64_->planGen == plan_->gen;
+    if (keep) {
+      if (!refresh_multigrids()) return false;
+      invalidate_graph();
+    } else {
+      mg32_.clear();
+      mg64_.reset();
+      invalidate_graph();
+    }
+  } else {
+    if (!ensure_host_coefficients()) return false;
+    // raw FP64 A on level 0: its own arena, released on every update (the
+    // deep planes are screen M + stiffness S of the resident M and S planes)
+    const LevelCoefficients& c0 = coeffs_[0];
     const int cnt = runs0_.count;
     rawAArena_ = DeviceArena();
+    rawFromPlan_ = false;
     double* planes = static_cast<double*>(rawAArena_.alloc(size_t(9) * std::max(1, cnt) * sizeof(double)));
     if (!check(rawAArena_.last, "operator planes")) return false;
     dev::launch_axpby(planes, screen, rawM_.coef, stiffness, rawS_.coef, (long long)9 * cnt, stream_);
     std::vector<int> ptr(1, 0), col;
     std::vector<double> val;
     for (int b = 0; b < L0.numBoundary; b++) {
-      for (int k = bd.ptr[b]; k < bd.ptr[b + 1]; k++) { col.push_back(bd.col[k]); val.push_back(bd.val[k]); }
-      for (int k = bb.ptr[b]; k < bb.ptr[b + 1]; k++) { col.push_back(L0.boundaryGlobal[bb.col[k]]); val.push_back(bb.val[k]); }
+      for (int k = c0.bd.ptr[b]; k < c0.bd.ptr[b + 1]; k++) { col.push_back(c0.bd.col[k]); val.push_back(c0.bd.val[k]); }
+      for (int k = c0.bb.ptr[b]; k < c0.bb.ptr[b + 1]; k++) { col.push_back(L0.boundaryGlobal[c0.bb.col[k]]); val.push_back(c0.bb.val[k]); }
       ptr.push_back((int)col.size());
     }
     rawA_ = RawOperator();
@@ -506,13 +514,172 @@ bool DeviceSystem::update(double stiffness, double screen) {
     rawA_.bGlobal = rawM_.bGlobal;
     rawA_.nB = L0.numBoundary;
     if (!check(rawAArena_.last, "operator upload") || !check(cudaStreamSynchronize(stream_), "operator planes")) return false;
+    mg32_.clear();
+    mg64_.reset();
+    invalidate_graph();
   }
-  mg32_.clear();
-  mg64_.reset();
-  bsCache_.clear();
-  invalidate_graph();
   updated_ = true;
   setupMs[0] = now_ms() - tUpdate;
+  return true;
+}
+
+bool DeviceSystem::use_numeric() const { return knobs.deviceFactor != 0 && knobs.tileTexels == 0; }
+
+// host combination of the coefficient hierarchy for the current weights (the
+// host-built multigrid, the tile layout and the coefficient export read it)
+bool DeviceSystem::ensure_host_coefficients() {
+  if (hostCoeffs_) return true;
+  const int L = levelsUsed_;
+  const GridLevel& L0 = h_.levels[0];
+  std::vector<LevelCoefficients> co(L);
+  co[0].deep.resize(fine_.deepMass.size());
+  for (size_t i = 0; i < co[0].deep.size(); i++) co[0].deep[i] = screen_ * fine_.deepMass[i] + stiffness_ * fine_.deepStiffness[i];
+  co[0].bb = csr_axpby(screen_, fine_.bbMass, stiffness_, fine_.bbStiffness);
+  co[0].bd = csr_axpby(screen_, fine_.bdMass, stiffness_, fine_.bdStiffness);
+  co[0].bd.cols = L0.numTexels;
+  for (int l = 1; l < L; l++) {
+    const LevelCoefficients &m = coMass_[l], &k = coStiff_[l];
+    co[l].deep.resize(m.deep.size());
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)m.deep.size(); i++) co[l].deep[i] = screen_ * m.deep[i] + stiffness_ * k.deep[i];
+    co[l].bb = csr_axpby(screen_, m.bb, stiffness_, k.bb);
+    co[l].bd = csr_axpby(screen_, m.bd, stiffness_, k.bd);
+  }
+  coeffs_ = std::move(co);
+  hostCoeffs_ = true;
+  return true;
+}
+
+const std::vector<LevelCoefficients>& DeviceSystem::coefficients() {
+  if (updated_ && !ensure_host_coefficients()) coeffs_.clear();
+  return coeffs_;
+}
+
+bool DeviceSystem::ensure_plan() {
+  const int L = levelsUsed_;
+  if (plan_ && plan_->L == L && plan_->maxBlock == knobs.maxBlock && plan_->denseMax == knobs.denseBoundaryMax) return true;
+  // multigrids laid out for an earlier plan keep their own buffers; an update
+  // rebuilds them (their generation differs)
+  plan_.reset(new NumericPlan());
+  plan_->gen = ++planCount_;
+  const double t0 = now_ms();
+  if (!plan_->build(h_, L, fine_, coMass_, coStiff_, knobs.maxBlock, knobs.denseBoundaryMax, stream_, err_)) {
+    plan_.reset();
+    return false;
+  }
+  planMs_ = now_ms() - t0;
+  rawFromPlan_ = false;
+  return true;
+}
+
+// level-0 FP64 operator: structure once per plan, values from the combined M and S
+bool DeviceSystem::refresh_raw_operator() {
+  const GridLevel& L0 = h_.levels[0];
+  const int cnt = runs0_.count;
+  if (!rawFromPlan_) {
+    const NumericLevel& N = plan_->levels[0];
+    rawAArena_ = DeviceArena();
+    rawA_ = RawOperator();
+    rawA_.runs = rawM_.runs;
+    rawA_.nRuns = rawM_.nRuns;
+    rawA_.coef = static_cast<double*>(rawAArena_.alloc(size_t(9) * std::max(1, cnt) * sizeof(double)));
+    rawA_.planeStride = cnt;
+    if (N.coarsest) {  // a single-level system: the boundary rows of the union patterns
+      std::vector<int> ptr(1, 0), col;
+      for (int b = 0; b < L0.numBoundary; b++) {
+        for (int k = N.bd.ptr[b]; k < N.bd.ptr[b + 1]; k++) col.push_back(N.bd.col[k]);
+        for (int k = N.bb.ptr[b]; k < N.bb.ptr[b + 1]; k++) col.push_back(L0.boundaryGlobal[N.bb.col[k]]);
+        ptr.push_back((int)col.size());
+      }
+      rawA_.bPtr = rawAArena_.upload(ptr);
+      rawA_.bCol = rawAArena_.upload(col);
+      rawA_.bVal = static_cast<double*>(rawAArena_.alloc(std::max<size_t>(1, col.size()) * sizeof(double)));
+    } else {
+      rawA_.bPtr = rawAArena_.upload(N.bPtr);
+      rawA_.bCol = rawAArena_.upload(N.bCol);
+      rawA_.bVal = static_cast<double*>(rawAArena_.alloc(std::max<size_t>(1, N.bCol.size()) * sizeof(double)));
+    }
+    rawA_.bGlobal = rawM_.bGlobal;
+    rawA_.nB = L0.numBoundary;
+    if (!check(rawAArena_.last, "operator upload")) return false;
+    rawFromPlan_ = true;
+  }
+  dev::launch_axpby(const_cast<double*>(rawA_.coef), screen_, rawM_.coef, stiffness_, rawS_.coef, (long long)9 * cnt, stream_);
+  const NumericLevel& N = plan_->levels[0];
+  if (N.coarsest) {
+    // the operator's boundary rows in the union layout: bd entries, then bb entries
+    std::vector<int> src;
+    for (int b = 0; b < L0.numBoundary; b++) {
+      for (int k = N.bd.ptr[b]; k < N.bd.ptr[b + 1]; k++) src.push_back(k);
+      for (int k = N.bb.ptr[b]; k < N.bb.ptr[b + 1]; k++) src.push_back(-1 - k);
+    }
+    if (!src.empty()) {
+      std::vector<double> bd(N.nBD), bb(N.nBB), v(src.size());
+      if (!check(cudaMemcpyAsync(bd.data(), N.bdV, bd.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_), "operator rows") ||
+          !check(cudaMemcpyAsync(bb.data(), N.bbV, bb.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_), "operator rows") ||
+          !check(cudaStreamSynchronize(stream_), "operator rows"))
+        return false;
+      for (size_t i = 0; i < src.size(); i++) v[i] = src[i] >= 0 ? bd[src[i]] : bb[-1 - src[i]];
+      if (!check(cudaMemcpyAsync(const_cast<double*>(rawA_.bVal), v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
+                 "operator rows"))
+        return false;
+    }
+  } else if (!plan_->fill_raw_rows(const_cast<double*>(rawA_.bVal), stream_, err_)) {
+    return false;
+  }
+  return check(cudaStreamSynchronize(stream_), "operator values");
+}
+
+template <typename T>
+LevelValues<T> DeviceSystem::level_values(Multigrid<T>& mg, int l) {
+  LevelValues<T> v;
+  if (l == (int)mg.levels.size() - 1) {
+    v.coarseInv = const_cast<double*>(mg.coarseInv);
+    v.coarseScale = const_cast<double*>(mg.coarseScale);
+    return v;
+  }
+  LevelDev<T>& D = mg.levels[l];
+  v.planes = const_cast<T*>(D.coef);
+  v.planeStride = D.planeStride;
+  v.bVal = const_cast<T*>(D.bVal);
+  dev::BoundaryDev<T>& B = D.B;
+  v.inv = const_cast<T*>(B.inv);
+  v.sinv = const_cast<T*>(B.sinv);
+  v.scale = const_cast<T*>(B.scale);
+  v.bdVal = const_cast<T*>(B.bdVal);
+  v.asiVal = const_cast<T*>(B.asiVal);
+  v.wt = const_cast<T*>(B.wt);
+  v.nSp = (B.nS + 3) & ~3;
+  return v;
+}
+
+// values of the resident multigrids (the FP32 base, whose derived widths share
+// its buffers, and the FP64 one) for the current weights
+bool DeviceSystem::refresh_multigrids() {
+  Multigrid<float>* m32 = mg32_.empty() ? nullptr : mg32_.front().get();
+  Multigrid<double>* m64 = mg64_.get();
+  if (m32 && m32->planGen != plan_->gen) m32 = nullptr;
+  if (m64 && m64->planGen != plan_->gen) m64 = nullptr;
+  std::fill(plan_->ms, plan_->ms + 4, 0.0);
+  double t0 = now_ms();
+  for (int l = 0; l < levelsUsed_; l++) {
+    if (l == levelsUsed_ - 1) {
+      // boundary factorisations {values, subdomain inverses, Schur products, Schur inverse}
+      setupMs[1] = plan_->ms[0] + plan_->ms[1] + plan_->ms[2] + plan_->ms[3];
+      std::copy(plan_->ms, plan_->ms + 4, setupMs + 4);
+      t0 = now_ms();
+    }
+    LevelValues<float> v32;
+    LevelValues<double> v64;
+    if (m32) v32 = level_values(*m32, l);
+    if (m64) v64 = level_values(*m64, l);
+    if (!plan_->fill_level(l, m32 ? &v32 : nullptr, m64 ? &v64 : nullptr, stream_, err_)) {
+      err_ = "level " + std::to_string(l) + ": " + err_;
+      return false;
+    }
+  }
+  setupMs[2] = now_ms() - t0;
+  setupMs[3] = 0;
   return true;
 }
 
@@ -521,6 +688,10 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
   const double tBuild = now_ms();
   double tBoundary = 0, tCoarse = 0, tBs[4] = {0, 0, 0, 0};
   const int L = levelsUsed_;
+  // numeric: the layout here, every value by the device numeric set-up below;
+  // otherwise values from the host coefficients and host (or backend) factorisations
+  const bool numeric = use_numeric();
+  if (numeric ? !ensure_plan() : !ensure_host_coefficients()) return false;
   DeviceDense deviceDense(stream_);
   DenseBackend* dense = knobs.deviceFactor ? &deviceDense : nullptr;
   const int bsKey[3] = {knobs.maxBlock, knobs.denseBoundaryMax, knobs.deviceFactor};
@@ -533,7 +704,7 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
   mg.KP = KP;
   for (int l = 0; l < L; l++) {
     const GridLevel& G = h_.levels[l];
-    const LevelCoefficients& C = coeffs_[l];
+    const LevelCoefficients* C = numeric ? nullptr : &coeffs_[l];
     LevelDev<T>& D = mg.levels[l];
     D.n = G.numTexels;
     D.nDeep = G.numDeep;
@@ -542,10 +713,16 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     D.b = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
     D.r = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
     if (l == L - 1) {
+      const int n = G.numTexels;
+      mg.coarseN = n;
+      if (numeric) {
+        mg.coarseInv = static_cast<double*>(A.alloc(size_t(n) * n * sizeof(double)));
+        mg.coarseScale = static_cast<double*>(A.alloc(size_t(n) * sizeof(double)));
+        continue;
+      }
       // coarsest: scaled dense inverse (FP64)
       Csr full;
-      full_matrix(G, C, full);
-      const int n = G.numTexels;
+      full_matrix(G, *C, full);
       std::vector<double> denseA(size_t(n) * n, 0.0), scale(n);
       for (int i = 0; i < n; i++)
         for (int k = full.ptr[i]; k < full.ptr[i + 1]; k++)
@@ -558,31 +735,36 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
                                   : dense_spd_inverse(denseA.data(), n, true);
       if (!inverted) { err_ = "coarsest operator is not positive definite" + (e.empty() ? std::string() : ": " + e); return false; }
       tCoarse += now_ms() - t0;
-      mg.coarseN = n;
       mg.coarseInv = A.upload(denseA);
       mg.coarseScale = A.upload(scale);
       continue;
     }
     // deep runs + reciprocal coefficient planes
     DeepRuns R = build_deep_runs(G);
-    std::vector<T> planes(size_t(10) * std::max(1, R.count));
+    if (numeric) {
+      if ((int)R.texel.size() != R.count) { err_ = "deep runs: texel list and count differ"; return false; }
+      if (!plan_->set_run_order(l, R.texel, err_)) return false;
+      D.coef = static_cast<T*>(A.alloc(size_t(10) * std::max(1, R.count) * sizeof(T)));
+    } else {
+      std::vector<T> planes(size_t(10) * std::max(1, R.count));
 #pragma omp parallel for schedule(static)
-    for (int i = 0; i < R.count; i++) {
-      const double* c = &C.deep[10 * size_t(R.texel[i])];
-      const double c4 = c[4], inv = 1.0 / c4;
-      for (int k = 0; k < 9; k++) planes[size_t(k) * R.count + i] = T(k == 4 ? inv : c[k] * inv);
-      planes[size_t(9) * R.count + i] = T(c4);
+      for (int i = 0; i < R.count; i++) {
+        const double* c = &C->deep[10 * size_t(R.texel[i])];
+        const double c4 = c[4], inv = 1.0 / c4;
+        for (int k = 0; k < 9; k++) planes[size_t(k) * R.count + i] = T(k == 4 ? inv : c[k] * inv);
+        planes[size_t(9) * R.count + i] = T(c4);
+      }
+      D.coef = A.upload(planes);
     }
     D.runs = A.upload(R.runs);
     D.nRuns = (int)R.runs.size();
     std::copy(R.runStart, R.runStart + 5, D.runStart);
-    D.coef = A.upload(planes);
     D.planeStride = R.count;
     // tiles of the fused smoother (FP32 levels it runs on; the tile_texels knob
-    // drops the multigrids when it changes)
-    if (sizeof(T) == 4 && G.numDeep >= kTileBuildMin && knobs.tileTexels > 0 && G.numDeep >= knobs.tileTexels) {
+    // drops the multigrids when it changes; host-built values only)
+    if (!numeric && sizeof(T) == 4 && G.numDeep >= kTileBuildMin && knobs.tileTexels > 0 && G.numDeep >= knobs.tileTexels) {
       TileLayout TL;
-      build_tiles(G, C, TL);
+      build_tiles(G, *C, TL);
       D.tiles = A.upload(TL.tiles);
       D.nTiles = (int)TL.tiles.size();
       D.tileSegs = A.upload(TL.segs);
@@ -605,33 +787,27 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       }
     }
     // boundary rows (merged BD + BB, global columns)
-    {
+    if (numeric) {
+      const NumericLevel& N = plan_->levels[l];
+      D.bPtr = A.upload(N.bPtr);
+      D.bCol = A.upload(N.bCol);
+      D.bVal = static_cast<T*>(A.alloc(std::max<size_t>(1, N.bCol.size()) * sizeof(T)));
+    } else {
       std::vector<int> ptr(1, 0), col;
       std::vector<T> val;
       for (int b = 0; b < G.numBoundary; b++) {
-        for (int k = C.bd.ptr[b]; k < C.bd.ptr[b + 1]; k++) { col.push_back(C.bd.col[k]); val.push_back(T(C.bd.val[k])); }
-        for (int k = C.bb.ptr[b]; k < C.bb.ptr[b + 1]; k++) { col.push_back(G.boundaryGlobal[C.bb.col[k]]); val.push_back(T(C.bb.val[k])); }
+        for (int k = C->bd.ptr[b]; k < C->bd.ptr[b + 1]; k++) { col.push_back(C->bd.col[k]); val.push_back(T(C->bd.val[k])); }
+        for (int k = C->bb.ptr[b]; k < C->bb.ptr[b + 1]; k++) { col.push_back(G.boundaryGlobal[C->bb.col[k]]); val.push_back(T(C->bb.val[k])); }
         ptr.push_back((int)col.size());
       }
       D.bPtr = A.upload(ptr);
       D.bCol = A.upload(col);
       D.bVal = A.upload(val);
-      D.bGlobal = A.upload(G.boundaryGlobal);
     }
-    // exact boundary solver (set up once per update, for either multigrid)
-    {
-      if (!bsCache_[l]) {
-        auto built = std::make_shared<BoundarySolverSetup>();
-        const double t0 = now_ms();
-        if (!build_boundary_solver(C.bb, C.bd, knobs.maxBlock, knobs.denseBoundaryMax, *built, err_, dense)) {
-          err_ = "level " + std::to_string(l) + ": " + err_;
-          return false;
-        }
-        tBoundary += now_ms() - t0;
-        for (int q = 0; q < 4; q++) tBs[q] += built->ms[q];
-        bsCache_[l] = built;
-      }
-      const BoundarySolverSetup& bs = *bsCache_[l];
+    D.bGlobal = A.upload(G.boundaryGlobal);
+    // exact boundary solver: the layout of its structure (a host set-up with
+    // values, or the numeric plan's structure with value buffers left to fill)
+    auto layout_boundary = [&](const auto& bs, const BoundarySolverSetup* vals) -> bool {
       dev::BoundaryDev<T>& B = D.B;
       B.nb = bs.nb;
       B.nSub = bs.nSub;
@@ -648,13 +824,18 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
         for (int rq = 0; rq < mp / 4; rq += 32) tasks.push_back(make_int4(p, rq, 0, m));
       }
       if (maxM > dev::kBoundaryChunkMax) { err_ = "boundary subdomain larger than the device chunk limit"; return false; }
-      std::vector<T> inv(size_t(off[bs.nSub]), T(0));
+      if (vals) {
+        std::vector<T> inv(size_t(off[bs.nSub]), T(0));
 #pragma omp parallel for schedule(dynamic, 4)
-      for (int p = 0; p < bs.nSub; p++) {
-        const int m = bs.subPtr[p + 1] - bs.subPtr[p], mp = (m + 3) & ~3;
-        const double* src = &bs.inv[size_t(bs.invOff[p])];
-        for (int j = 0; j < m; j++)
-          for (int a = 0; a < m; a++) inv[size_t(off[p]) + size_t(j) * mp + a] = T(src[size_t(j) * m + a]);
+        for (int p = 0; p < bs.nSub; p++) {
+          const int m = bs.subPtr[p + 1] - bs.subPtr[p], mp = (m + 3) & ~3;
+          const double* src = &vals->inv[size_t(vals->invOff[p])];
+          for (int j = 0; j < m; j++)
+            for (int a = 0; a < m; a++) inv[size_t(off[p]) + size_t(j) * mp + a] = T(src[size_t(j) * m + a]);
+        }
+        B.inv = A.upload(inv);
+      } else {
+        B.inv = static_cast<T*>(A.alloc(std::max<size_t>(1, size_t(off[bs.nSub])) * sizeof(T)));
       }
       // blocks per row group: enough chunks for one wave of bsBlocksPerSm
       // resident blocks on each of the 148 SMs, each warp still taking >= 4 j steps
@@ -670,7 +851,6 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       B.subPtr = A.upload(bs.subPtr);
       B.rowSub = A.upload(rowSub);
       B.invOff = A.upload(off);
-      B.inv = A.upload(inv);
       B.subTasks = A.upload(tasks);
       B.nSubTasks = (int)tasks.size();
       B.subChunks = chunks_for(B.nSubTasks, maxM, 1);
@@ -679,12 +859,16 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       // separator Schur complement inverse, same layout
       if (bs.nS > 0) {
         const int nS = bs.nS, nSp = (nS + 3) & ~3;
-        std::vector<T> sinv(size_t(nS) * nSp, T(0));
-        for (int j = 0; j < nS; j++)
-          for (int a = 0; a < nS; a++) sinv[size_t(j) * nSp + a] = T(bs.Sinv[size_t(j) * nS + a]);
+        if (vals) {
+          std::vector<T> sinv(size_t(nS) * nSp, T(0));
+          for (int j = 0; j < nS; j++)
+            for (int a = 0; a < nS; a++) sinv[size_t(j) * nSp + a] = T(vals->Sinv[size_t(j) * nS + a]);
+          B.sinv = A.upload(sinv);
+        } else {
+          B.sinv = static_cast<T*>(A.alloc(size_t(nS) * nSp * sizeof(T)));
+        }
         std::vector<int4> st;
         for (int rq = 0; rq < nSp / 4; rq += 32) st.push_back(make_int4(0, rq, 0, nS));
-        B.sinv = A.upload(sinv);
         B.schurTasks = A.upload(st);
         B.nSchurTasks = (int)st.size();
         B.schurChunks = chunks_for(B.nSchurTasks, nS, (nS + dev::kBoundaryChunkMax - 1) / dev::kBoundaryChunkMax);
@@ -693,26 +877,45 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
       }
       // back substitution: W_p column-major with its separator columns
       std::vector<long long> wOff(bs.wOff.begin(), bs.wOff.end());
-      std::vector<T> wt(bs.W.begin(), bs.W.end());
       B.touchPtr = A.upload(bs.touchPtr);
       B.touch = A.upload(bs.touch);
       B.wOff = A.upload(wOff);
-      B.wt = A.upload(wt);
-      std::vector<T> scale(bs.scale.begin(), bs.scale.end());
       std::vector<int> pg(bs.nb);
       for (int k = 0; k < bs.nb; k++) pg[k] = G.boundaryGlobal[bs.order[k]];
-      auto upT = [&](const std::vector<double>& v) { std::vector<T> t(v.begin(), v.end()); return (const T*)A.upload(t); };
       B.posGlobal = A.upload(pg);
-      B.scale = A.upload(scale);
       B.bdPtr = A.upload(bs.BD.ptr);
       B.bdCol = A.upload(bs.BD.col);
-      B.bdVal = upT(bs.BD.val);
       B.asiPtr = A.upload(bs.ASI.ptr);
       B.asiCol = A.upload(bs.ASI.col);
-      B.asiVal = upT(bs.ASI.val);
+      auto values = [&](const std::vector<double>& v, size_t n) -> const T* {
+        if (!vals) return static_cast<T*>(A.alloc(std::max<size_t>(1, n) * sizeof(T)));
+        std::vector<T> t(v.begin(), v.end());
+        return A.upload(t);
+      };
+      B.wt = values(vals ? vals->W : std::vector<double>(), size_t(bs.wOff.back()));
+      B.scale = values(vals ? vals->scale : std::vector<double>(), size_t(bs.nb));
+      B.bdVal = values(vals ? vals->BD.val : std::vector<double>(), bs.BD.col.size());
+      B.asiVal = values(vals ? vals->ASI.val : std::vector<double>(), bs.ASI.col.size());
       B.y = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nI)) * KP * sizeof(T)));
       B.xs = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nS)) * KP * sizeof(T)));
       B.rhat = static_cast<T*>(A.alloc(size_t(std::max(1, bs.nb)) * KP * sizeof(T)));
+      return true;
+    };
+    if (numeric) {
+      if (!layout_boundary(plan_->levels[l].sym, nullptr)) return false;
+    } else {
+      if (!bsCache_[l]) {
+        auto built = std::make_shared<BoundarySolverSetup>();
+        const double t0 = now_ms();
+        if (!build_boundary_solver(C->bb, C->bd, knobs.maxBlock, knobs.denseBoundaryMax, *built, err_, dense)) {
+          err_ = "level " + std::to_string(l) + ": " + err_;
+          return false;
+        }
+        tBoundary += now_ms() - t0;
+        for (int q = 0; q < 4; q++) tBs[q] += built->ms[q];
+        bsCache_[l] = built;
+      }
+      if (!layout_boundary(*bsCache_[l], bsCache_[l].get())) return false;
     }
     // transfers to / from level l+1
     {
@@ -746,10 +949,39 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
   mg.levelsDev = A.upload(mg.levels);
   mg.barrier = static_cast<dev::GridBarrierState*>(A.alloc(sizeof(dev::GridBarrierState)));
   if (!check(A.last, "multigrid upload")) return false;
-  setupMs[1] = tBoundary;
-  setupMs[2] = tCoarse;
-  setupMs[3] = now_ms() - tBuild - tBoundary - tCoarse;
-  std::copy(tBs, tBs + 4, setupMs + 4);
+  if (numeric) {
+    // every value of the layout above, on the device
+    const double tLayout = now_ms() - tBuild;
+    std::fill(plan_->ms, plan_->ms + 4, 0.0);
+    for (int l = 0; l + 1 < L; l++) {
+      LevelValues<T> v = level_values(mg, l);
+      if (!fill_one(*plan_, l, v, stream_, err_)) {
+        err_ = "level " + std::to_string(l) + ": " + err_;
+        return false;
+      }
+    }
+    std::copy(plan_->ms, plan_->ms + 4, tBs);
+    tBoundary = tBs[0] + tBs[1] + tBs[2] + tBs[3];
+    const double t0 = now_ms();
+    LevelValues<T> vc = level_values(mg, L - 1);
+    if (!fill_one(*plan_, L - 1, vc, stream_, err_)) {
+      err_ = "coarsest level: " + err_;
+      return false;
+    }
+    tCoarse = now_ms() - t0;
+    mg.planGen = plan_->gen;
+    setupMs[1] = tBoundary;
+    setupMs[2] = tCoarse;
+    setupMs[3] = tLayout + planMs_;
+    planMs_ = 0;
+    std::copy(tBs, tBs + 4, setupMs + 4);
+  } else {
+    mg.planGen = -1;
+    setupMs[1] = tBoundary;
+    setupMs[2] = tCoarse;
+    setupMs[3] = now_ms() - tBuild - tBoundary - tCoarse;
+    std::copy(tBs, tBs + 4, setupMs + 4);
+  }
   return check(cudaMemset(mg.barrier, 0, sizeof(dev::GridBarrierState)), "grid barrier");
 }
 
@@ -766,6 +998,7 @@ bool DeviceSystem::derive_multigrid(const Multigrid<T>& base, Multigrid<T>& mg, 
   mg.coarseN = base.coarseN;
   mg.coarseInv = base.coarseInv;
   mg.coarseScale = base.coarseScale;
+  mg.planGen = base.planGen;
   for (LevelDev<T>& D : mg.levels) {
     D.x = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));
     D.b = static_cast<T*>(A.alloc(size_t(D.n) * KP * sizeof(T)));

@@ -10,6 +10,7 @@
 
 #include "kernels/vcycle.cuh"
 #include "kernels/vcycle_kernels.h"
+#include "numeric.h"
 #include "setup/setup.h"
 
 namespace gdtp {
@@ -78,6 +79,7 @@ struct Multigrid {
   bool clusterOK = false;               // the device can run the coarse-level cluster
   bool gridOK = false;                  // the device can run the persistent coarse-level kernel
   dev::GridBarrierState* barrier = nullptr;  // its grid barrier
+  int planGen = -1;                     // the numeric plan its layout follows (-1: host-built values)
   DeviceArena arena;
 };
 
@@ -145,7 +147,8 @@ class DeviceSystem {
 
   // A = screen*M + stiffness*S, Galerkin hierarchy, boundary solvers, coarse inverse
   bool update(double stiffness, double screen);
-  const std::vector<LevelCoefficients>& coefficients() const { return coeffs_; }
+  // the coefficient hierarchy for the current weights (combined on the host on demand)
+  const std::vector<LevelCoefficients>& coefficients();
   int levelsUsed() const { return levelsUsed_; }
 
   // host in/out, k right-hand sides (tight n x k)
@@ -238,6 +241,15 @@ class DeviceSystem {
  private:
   template <typename T>
   bool build_multigrid(Multigrid<T>& mg, int KP);
+  // numeric set-up on the device (numeric.h): used unless device_factor is 0 or
+  // the tile smoother is on
+  bool use_numeric() const;
+  bool ensure_plan();
+  bool ensure_host_coefficients();
+  bool refresh_raw_operator();
+  bool refresh_multigrids();
+  template <typename T>
+  LevelValues<T> level_values(Multigrid<T>& mg, int l);
   template <typename T, int W>
   // zeroStart: the level-0 iterate is zero on entry (a correction), so the
   // first sweep skips the neighbours it has not updated yet (exact zeros)
@@ -265,6 +277,11 @@ class DeviceSystem {
   // one update (cleared by update; keyed by the knobs that shape them)
   std::vector<std::shared_ptr<BoundarySolverSetup>> bsCache_;
   int bsCacheKey_[3] = {-1, -1, -1};
+  bool hostCoeffs_ = false;             // coeffs_ holds the current weights' combination
+  std::unique_ptr<NumericPlan> plan_;
+  double planMs_ = 0;                   // host layout time of the plan, reported with the next build
+  int planCount_ = 0;                   // numeric plans built so far (their generation numbers)
+  bool rawFromPlan_ = false;            // rawA_ holds the plan's boundary-row layout
   int coLevels_ = 0;
   int levelsUsed_ = 0;
   double stiffness_ = 0, screen_ = 0;
