@@ -126,7 +126,7 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
       if (count) *count = 0;
       return GDTP_OK;
     }
-    if (name == "profile.setup") return vec(std::vector<double>(s->sys->setupMs, s->sys->setupMs + 8));
+    if (name == "profile.setup") return vec(std::vector<double>(s->sys->setupMs, s->sys->setupMs + 14));
     if (name == "levelStats") return vec(s->sys->level_stats());  // 9 per level, see DeviceSystem::level_stats
     if (name == "levelsUsed") {
       if (count) *count = 1;
@@ -142,6 +142,14 @@ extern "C" int gdtp_apply(gdtp_system* s, int which, const double* x, double* y,
     GDTP_SYS_CHECK(s);
     if (!x || !y || which < 0 || which > 2) return fail(GDTP_ERR_INVALID, "gdtp_apply: bad arguments");
     return s->sys->apply(which, x, y, k) ? GDTP_OK : sys_fail(s, GDTP_ERR_CUDA);
+  });
+}
+
+extern "C" int gdtp_apply_mass_stiffness(gdtp_system* s, double mass_weight, double stiffness_weight, const double* x, double* y, int k) {
+  return guarded("gdtp_apply_mass_stiffness", [&]() -> int {
+    GDTP_SYS_CHECK(s);
+    if (!x || !y) return fail(GDTP_ERR_INVALID, "gdtp_apply_mass_stiffness: bad arguments");
+    return s->sys->apply_combination(mass_weight, stiffness_weight, x, y, k) ? GDTP_OK : sys_fail(s, GDTP_ERR_CUDA);
   });
 }
 

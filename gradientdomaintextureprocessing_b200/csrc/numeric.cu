@@ -220,14 +220,38 @@ std::vector<int> as_int(const std::vector<T>& v) {
 
 std::vector<long long> as_ll(const std::vector<int64_t>& v) { return std::vector<long long>(v.begin(), v.end()); }
 
+__global__ void k_gather_planes(int count, const int* __restrict__ texel, const double* __restrict__ deep, double* __restrict__ planes) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const double* c = deep + 10LL * texel[i];
+#pragma unroll
+  for (int k = 0; k < 9; k++) planes[(long long)k * count + i] = c[k];
+}
+
 }  // namespace
+
+void launch_gather_planes(int count, const int* texel, const double* deep, double* planes, cudaStream_t s) {
+  k_gather_planes<<<blocks_for(count), kThreads, 0, s>>>(count, texel, deep, planes);
+}
 
 NumericPlan::~NumericPlan() { delete arena_; }
 
 size_t NumericPlan::deviceBytes() const { return arena_ ? arena_->total : 0; }
 
+namespace {
+// host side of one level's plan, built for all levels in parallel before the uploads
+struct LevelHost {
+  Csr bbS, bdS;                           // S aligned to the union patterns (N.bb, N.bd hold M)
+  std::vector<int> bsrc;
+  std::vector<long long> denseSrc, diagSrc;
+  std::vector<int> denseRow, denseCol, m, t;
+  std::string err;
+};
+}  // namespace
+
 bool NumericPlan::build(const Hierarchy& h, int L_, const FineSystem& fine, const std::vector<LevelCoefficients>& coM,
-                        const std::vector<LevelCoefficients>& coS, int maxBlock_, int denseMax_, cudaStream_t s, std::string& err) {
+                        const std::vector<LevelCoefficients>& coS, const double* deep0M, const double* deep0S, int maxBlock_,
+                        int denseMax_, cudaStream_t s, std::string& err) {
   (void)s;
   delete arena_;
   arena_ = new DeviceArena();
@@ -236,38 +260,32 @@ bool NumericPlan::build(const Hierarchy& h, int L_, const FineSystem& fine, cons
   maxBlock = maxBlock_;
   denseMax = denseMax_;
   levels.assign(L, NumericLevel());
+  std::vector<LevelHost> host(L);
+  // ---- structure of every level (host, levels in parallel)
+#pragma omp parallel for schedule(dynamic, 1)
   for (int l = 0; l < L; l++) {
     const GridLevel& G = h.levels[l];
     NumericLevel& N = levels[l];
+    LevelHost& H = host[l];
     N.n = G.numTexels;
     N.nDeep = G.numDeep;
     N.nB = G.numBoundary;
     N.coarsest = (l == L - 1);
-    const std::vector<double>& dM = l == 0 ? fine.deepMass : coM[l].deep;
-    const std::vector<double>& dS = l == 0 ? fine.deepStiffness : coS[l].deep;
-    Csr bbM = l == 0 ? fine.bbMass : coM[l].bb, bbS = l == 0 ? fine.bbStiffness : coS[l].bb;
+    const Csr& bbM = l == 0 ? fine.bbMass : coM[l].bb;
+    const Csr& bbS = l == 0 ? fine.bbStiffness : coS[l].bb;
     Csr bdM = l == 0 ? fine.bdMass : coM[l].bd, bdS = l == 0 ? fine.bdStiffness : coS[l].bd;
     bdM.cols = bdS.cols = G.numTexels;
     // union patterns, M and S aligned to them
-    const Csr bbMu = csr_axpby(1.0, bbM, 0.0, bbS), bbSu = csr_axpby(0.0, bbM, 1.0, bbS);
-    const Csr bdMu = csr_axpby(1.0, bdM, 0.0, bdS), bdSu = csr_axpby(0.0, bdM, 1.0, bdS);
-    N.bb = bbMu;
-    N.bd = bdMu;
-    N.nBB = (long long)bbMu.col.size();
-    N.nBD = (long long)bdMu.col.size();
-    N.deepM = A.upload(dM);
-    N.deepS = A.upload(dS);
-    N.bbM = A.upload(bbMu.val);
-    N.bbS = A.upload(bbSu.val);
-    N.bdM = A.upload(bdMu.val);
-    N.bdS = A.upload(bdSu.val);
-    N.bbV = static_cast<double*>(A.alloc(std::max<long long>(1, N.nBB) * sizeof(double)));
-    N.bdV = static_cast<double*>(A.alloc(std::max<long long>(1, N.nBD) * sizeof(double)));
+    N.bb = csr_axpby(1.0, bbM, 0.0, bbS);
+    H.bbS = csr_axpby(0.0, bbM, 1.0, bbS);
+    N.bd = csr_axpby(1.0, bdM, 0.0, bdS);
+    H.bdS = csr_axpby(0.0, bdM, 1.0, bdS);
+    N.nBB = (long long)N.bb.col.size();
+    N.nBD = (long long)N.bd.col.size();
     if (N.coarsest) {
       // dense entries: deep rows' 3x3 stencils, boundary rows' bd and bb entries
       // (the layout of full_matrix, galerkin.cpp)
-      std::vector<long long> src, diag(G.numTexels, -1);
-      std::vector<int> row, col;
+      H.diagSrc.assign(G.numTexels, -1);
       for (int d = 0; d < G.numDeep; d++) {
         const int r = G.deepGlobal[d];
         const NodeInfo& nd = G.nodes[r];
@@ -276,100 +294,121 @@ bool NumericPlan::build(const Hierarchy& h, int L_, const FineSystem& fine, cons
           for (int ox = -1; ox <= 1; ox++) {
             const int c = gc.texel[gc.at(nd.ci + ox, nd.cj + oy)];
             const long long sIdx = 10LL * d + (oy + 1) * 3 + (ox + 1);
-            row.push_back(r);
-            col.push_back(c);
-            src.push_back(sIdx);
-            if (c == r) diag[r] = sIdx;
+            H.denseRow.push_back(r);
+            H.denseCol.push_back(c);
+            H.denseSrc.push_back(sIdx);
+            if (c == r) H.diagSrc[r] = sIdx;
           }
       }
       for (int b = 0; b < G.numBoundary; b++) {
         const int r = G.boundaryGlobal[b];
-        for (int k = bdMu.ptr[b]; k < bdMu.ptr[b + 1]; k++) {
-          row.push_back(r);
-          col.push_back(bdMu.col[k]);
-          src.push_back((1LL << 40) | k);
-          if (bdMu.col[k] == r) diag[r] = (1LL << 40) | k;
+        for (int k = N.bd.ptr[b]; k < N.bd.ptr[b + 1]; k++) {
+          H.denseRow.push_back(r);
+          H.denseCol.push_back(N.bd.col[k]);
+          H.denseSrc.push_back((1LL << 40) | k);
+          if (N.bd.col[k] == r) H.diagSrc[r] = (1LL << 40) | k;
         }
-        for (int k = bbMu.ptr[b]; k < bbMu.ptr[b + 1]; k++) {
-          const int c = G.boundaryGlobal[bbMu.col[k]];
-          row.push_back(r);
-          col.push_back(c);
-          src.push_back((2LL << 40) | k);
-          if (c == r) diag[r] = (2LL << 40) | k;
+        for (int k = N.bb.ptr[b]; k < N.bb.ptr[b + 1]; k++) {
+          const int c = G.boundaryGlobal[N.bb.col[k]];
+          H.denseRow.push_back(r);
+          H.denseCol.push_back(c);
+          H.denseSrc.push_back((2LL << 40) | k);
+          if (c == r) H.diagSrc[r] = (2LL << 40) | k;
         }
       }
-      for (int i = 0; i < G.numTexels; i++)
-        if (diag[i] < 0) { err = "coarsest level: texel without a diagonal entry"; return false; }
-      for (int c : col)
-        if (c < 0 || c >= G.numTexels) { err = "coarsest level: stencil column outside the level"; return false; }
-      N.nDense = (long long)src.size();
-      N.denseSrc = A.upload(src);
-      N.diagSrc = A.upload(diag);
-      N.denseRow = A.upload(row);
-      N.denseCol = A.upload(col);
-      if (!dev::spd_inverse_layout(std::vector<int64_t>(1, 0), std::vector<int>(1, G.numTexels), N.coarseLayout, err)) return false;
-      N.coarseDev = {A.upload(as_ll(N.coarseLayout.offsets)), A.upload(N.coarseLayout.sizes), A.upload(as_ll(N.coarseLayout.first)),
-                     A.upload(as_ll(N.coarseLayout.ws)), A.upload(N.coarseLayout.tasks)};
+      for (int i = 0; i < G.numTexels && H.err.empty(); i++)
+        if (H.diagSrc[i] < 0) H.err = "coarsest level: texel without a diagonal entry";
+      for (int c : H.denseCol)
+        if (H.err.empty() && (c < 0 || c >= G.numTexels)) H.err = "coarsest level: stencil column outside the level";
+      if (H.err.empty())
+        dev::spd_inverse_layout(std::vector<int64_t>(1, 0), std::vector<int>(1, G.numTexels), N.coarseLayout, H.err);
       continue;
     }
     // boundary rows of the smoother
     N.bPtr.assign(1, 0);
-    std::vector<int> bsrc;
     for (int b = 0; b < G.numBoundary; b++) {
-      for (int k = bdMu.ptr[b]; k < bdMu.ptr[b + 1]; k++) { N.bCol.push_back(bdMu.col[k]); bsrc.push_back(k); }
-      for (int k = bbMu.ptr[b]; k < bbMu.ptr[b + 1]; k++) { N.bCol.push_back(G.boundaryGlobal[bbMu.col[k]]); bsrc.push_back(-1 - k); }
+      for (int k = N.bd.ptr[b]; k < N.bd.ptr[b + 1]; k++) { N.bCol.push_back(N.bd.col[k]); H.bsrc.push_back(k); }
+      for (int k = N.bb.ptr[b]; k < N.bb.ptr[b + 1]; k++) { N.bCol.push_back(G.boundaryGlobal[N.bb.col[k]]); H.bsrc.push_back(-1 - k); }
       N.bPtr.push_back((int)N.bCol.size());
     }
-    N.nBRow = (long long)bsrc.size();
-    N.bSrc = A.upload(bsrc);
+    N.nBRow = (long long)H.bsrc.size();
     // boundary solver structure
     BoundarySymbolic& sym = N.sym;
-    if (!build_boundary_symbolic(bbMu, bdMu, maxBlock, denseMax, sym, err)) {
-      err = "level " + std::to_string(l) + ": " + err;
+    if (!build_boundary_symbolic(N.bb, N.bd, maxBlock, denseMax, sym, H.err)) {
+      H.err = "level " + std::to_string(l) + ": " + H.err;
+      continue;
+    }
+    if (sym.nb == 0) continue;
+    N.invOffPadHost.assign(sym.nSub + 1, 0);
+    H.m.resize(sym.nSub);
+    H.t.resize(sym.nSub);
+    for (int p = 0; p < sym.nSub; p++) {
+      H.m[p] = sym.subPtr[p + 1] - sym.subPtr[p];
+      H.t[p] = sym.touchPtr[p + 1] - sym.touchPtr[p];
+      N.invOffPadHost[p + 1] = N.invOffPadHost[p] + (long long)H.m[p] * ((H.m[p] + 3) & ~3);
+    }
+    std::vector<int64_t> invOff(sym.invOff.begin(), sym.invOff.end() - 1);
+    if (!dev::spd_inverse_layout(invOff, H.m, N.subLayout, H.err)) continue;
+    if (sym.nS > 0 && !dev::spd_inverse_layout(std::vector<int64_t>(1, 0), std::vector<int>(1, sym.nS), N.schurLayout, H.err)) continue;
+    std::vector<int64_t> cOff(sym.wOff.begin(), sym.wOff.end() - 1), lOff(sym.lOff.begin(), sym.lOff.end() - 1);
+    dev::schur_product_tasks(invOff, H.m, cOff, H.t, lOff, N.gTasks, N.lTasks, N.maxM, N.maxT);
+  }
+  for (const LevelHost& H : host)
+    if (!H.err.empty()) {
+      err = H.err;
       return false;
     }
-    if (sym.nb > 0) {
-      N.pos = A.upload(sym.pos);
-      N.order = A.upload(sym.order);
-      N.bbRow = A.upload(sym.bbRow);
-      N.bbCol = A.upload(bbMu.col);
-      N.diagEntry = A.upload(sym.diagEntry);
-      N.fillEntry = A.upload(sym.fillEntry);
-      N.fillDest = A.upload(as_ll(sym.fillDest));
-      N.ssEntry = A.upload(sym.ssEntry);
-      N.ssDest = A.upload(as_ll(sym.ssDest));
-      N.aisEntry = A.upload(as_int(sym.AIS.val));
-      N.aisDest = A.upload(as_ll(sym.aisDest));
-      N.asiEntry = A.upload(as_int(sym.ASI.val));
-      N.bdEntry = A.upload(as_int(sym.BD.val));
-      N.subPtr = A.upload(sym.subPtr);
-      N.touchPtr = A.upload(sym.touchPtr);
-      N.touch = A.upload(sym.touch);
-      N.wOff = A.upload(as_ll(sym.wOff));
-      N.lOff = A.upload(as_ll(sym.lOff));
-      N.invOff = A.upload(as_ll(sym.invOff));
-      N.invOffPadHost.assign(sym.nSub + 1, 0);
-      std::vector<int> m(sym.nSub), t(sym.nSub);
-      for (int p = 0; p < sym.nSub; p++) {
-        m[p] = sym.subPtr[p + 1] - sym.subPtr[p];
-        t[p] = sym.touchPtr[p + 1] - sym.touchPtr[p];
-        N.invOffPadHost[p + 1] = N.invOffPadHost[p] + (long long)m[p] * ((m[p] + 3) & ~3);
-      }
-      N.invOffPad = A.upload(N.invOffPadHost);
-      std::vector<int64_t> invOff(sym.invOff.begin(), sym.invOff.end() - 1);
-      if (!dev::spd_inverse_layout(invOff, m, N.subLayout, err)) return false;
-      N.subDev = {A.upload(as_ll(N.subLayout.offsets)), A.upload(N.subLayout.sizes), A.upload(as_ll(N.subLayout.first)),
-                  A.upload(as_ll(N.subLayout.ws)), A.upload(N.subLayout.tasks)};
-      if (sym.nS > 0) {
-        if (!dev::spd_inverse_layout(std::vector<int64_t>(1, 0), std::vector<int>(1, sym.nS), N.schurLayout, err)) return false;
-        N.schurDev = {A.upload(as_ll(N.schurLayout.offsets)), A.upload(N.schurLayout.sizes), A.upload(as_ll(N.schurLayout.first)),
-                      A.upload(as_ll(N.schurLayout.ws)), A.upload(N.schurLayout.tasks)};
-      }
-      std::vector<int64_t> cOff(sym.wOff.begin(), sym.wOff.end() - 1), lOff(sym.lOff.begin(), sym.lOff.end() - 1);
-      dev::schur_product_tasks(invOff, m, cOff, t, lOff, N.gTasks, N.lTasks, N.maxM, N.maxT);
-      N.gTasksDev = A.upload(N.gTasks);
-      N.lTasksDev = A.upload(N.lTasks);
+  // ---- resident sources and structure arrays (device)
+  auto layout_dev = [&](const dev::SpdInverseLayout& Ly) -> dev::SpdInverseDevice {
+    return {A.upload(as_ll(Ly.offsets)), A.upload(Ly.sizes), A.upload(as_ll(Ly.first)), A.upload(as_ll(Ly.ws)), A.upload(Ly.tasks)};
+  };
+  for (int l = 0; l < L; l++) {
+    NumericLevel& N = levels[l];
+    const LevelHost& H = host[l];
+    N.deepM = (l == 0 && deep0M) ? deep0M : A.upload(l == 0 ? fine.deepMass : coM[l].deep);
+    N.deepS = (l == 0 && deep0S) ? deep0S : A.upload(l == 0 ? fine.deepStiffness : coS[l].deep);
+    N.bbM = A.upload(N.bb.val);
+    N.bbS = A.upload(H.bbS.val);
+    N.bdM = A.upload(N.bd.val);
+    N.bdS = A.upload(H.bdS.val);
+    N.bbV = static_cast<double*>(A.alloc(std::max<long long>(1, N.nBB) * sizeof(double)));
+    N.bdV = static_cast<double*>(A.alloc(std::max<long long>(1, N.nBD) * sizeof(double)));
+    if (N.coarsest) {
+      N.nDense = (long long)H.denseSrc.size();
+      N.denseSrc = A.upload(H.denseSrc);
+      N.diagSrc = A.upload(H.diagSrc);
+      N.denseRow = A.upload(H.denseRow);
+      N.denseCol = A.upload(H.denseCol);
+      N.coarseDev = layout_dev(N.coarseLayout);
+      continue;
     }
+    N.bSrc = A.upload(H.bsrc);
+    const BoundarySymbolic& sym = N.sym;
+    if (sym.nb == 0) continue;
+    N.pos = A.upload(sym.pos);
+    N.order = A.upload(sym.order);
+    N.bbRow = A.upload(sym.bbRow);
+    N.bbCol = A.upload(N.bb.col);
+    N.diagEntry = A.upload(sym.diagEntry);
+    N.fillEntry = A.upload(sym.fillEntry);
+    N.fillDest = A.upload(as_ll(sym.fillDest));
+    N.ssEntry = A.upload(sym.ssEntry);
+    N.ssDest = A.upload(as_ll(sym.ssDest));
+    N.aisEntry = A.upload(as_int(sym.AIS.val));
+    N.aisDest = A.upload(as_ll(sym.aisDest));
+    N.asiEntry = A.upload(as_int(sym.ASI.val));
+    N.bdEntry = A.upload(as_int(sym.BD.val));
+    N.subPtr = A.upload(sym.subPtr);
+    N.touchPtr = A.upload(sym.touchPtr);
+    N.touch = A.upload(sym.touch);
+    N.wOff = A.upload(as_ll(sym.wOff));
+    N.lOff = A.upload(as_ll(sym.lOff));
+    N.invOff = A.upload(as_ll(sym.invOff));
+    N.invOffPad = A.upload(N.invOffPadHost);
+    N.subDev = layout_dev(N.subLayout);
+    if (sym.nS > 0) N.schurDev = layout_dev(N.schurLayout);
+    N.gTasksDev = A.upload(N.gTasks);
+    N.lTasksDev = A.upload(N.lTasks);
   }
   if (A.last != cudaSuccess) {
     err = std::string("numeric plan upload: ") + cudaGetErrorString(A.last);

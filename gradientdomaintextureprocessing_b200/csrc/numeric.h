@@ -77,6 +77,9 @@ struct LevelValues {
   double *coarseInv = nullptr, *coarseScale = nullptr;
 };
 
+// planes[k][i] = deep[10 texel[i] + k], k < 9 (raw FP64 operator planes in run order)
+void launch_gather_planes(int count, const int* texel, const double* deep, double* planes, cudaStream_t s);
+
 class NumericPlan {
  public:
   NumericPlan() = default;
@@ -84,8 +87,10 @@ class NumericPlan {
   NumericPlan& operator=(const NumericPlan&) = delete;
   ~NumericPlan();
   // structure of levels [0, L) and their resident M / S sources
+  // (deep0M, deep0S: the level-0 deep coefficients already resident on the device)
   bool build(const Hierarchy& h, int L, const FineSystem& fine, const std::vector<LevelCoefficients>& coM,
-             const std::vector<LevelCoefficients>& coS, int maxBlock, int denseMax, cudaStream_t s, std::string& err);
+             const std::vector<LevelCoefficients>& coS, const double* deep0M, const double* deep0S, int maxBlock, int denseMax,
+             cudaStream_t s, std::string& err);
   // bbV, bdV of every level for screen M + stiffness S
   bool combine(double screen, double stiffness, cudaStream_t s, std::string& err);
   // run order of a level's smoother planes (the multigrid's deep runs)

@@ -174,50 +174,91 @@ bool assemble_boundary_blocks(const Hierarchy& h, const BoundaryElements& be, co
                               const std::vector<double>& btMass, const std::vector<double>& btStiffness, FineSystem& fs,
                               std::string& err) {
   const GridLevel& L = h.levels[0];
-  std::vector<Triplet> bbM, bbS, bdM, bdS;
-  for (size_t a = 0; a < w.boundaryAdjacentCells.size(); a++) {
-    int ic = w.boundaryAdjacentCells[a];
+  // entries in a fixed order (adjacent cells, then boundary triangles), each
+  // cell's and triangle's slots computed first so that they fill in parallel
+  const int nAdj = (int)w.boundaryAdjacentCells.size();
+  std::vector<int> bbCount(size_t(nAdj) + 1, 0), bdCount(size_t(nAdj) + 1, 0);
+  bool bad = false;
+#pragma omp parallel for schedule(static) reduction(||: bad)
+  for (int a = 0; a < nAdj; a++) {
+    const int ic = w.boundaryAdjacentCells[a];
     const GridChart& gc = L.charts[w.cellChart[ic]];
-    int i = w.cellIJ[2 * ic], j = w.cellIJ[2 * ic + 1];
-    int pos[4] = {gc.at(i, j), gc.at(i + 1, j), gc.at(i + 1, j + 1), gc.at(i, j + 1)};
-    const double* M = &adjCellMass[16 * a];
-    const double* S = &adjCellStiffness[16 * a];
+    const int i = w.cellIJ[2 * ic], j = w.cellIJ[2 * ic + 1];
+    const int pos[4] = {gc.at(i, j), gc.at(i + 1, j), gc.at(i + 1, j + 1), gc.at(i, j + 1)};
+    int nbb = 0, nbd = 0;
     for (int k = 0; k < 4; k++) {
-      int node = gc.texel[pos[k]];
-      int bd = L.boundaryAndDeep[node];
-      if (bd < 0) continue;  // deep rows come from the device gather
-      int b = bd - 1;
+      if (L.boundaryAndDeep[gc.texel[pos[k]]] < 0) continue;  // deep rows come from the device gather
       for (int l = 0; l < 4; l++) {
-        int nb = gc.texel[pos[l]];
+        if (L.boundaryAndDeep[gc.texel[pos[l]]] < 0) nbd++;
+        else {
+          nbb++;
+          if (be.fineBoundaryIndex[gc.interiorTexel[pos[k]]] < 0 || be.fineBoundaryIndex[gc.interiorTexel[pos[l]]] < 0) bad = true;
+        }
+      }
+    }
+    bbCount[a + 1] = nbb;
+    bdCount[a + 1] = nbd;
+  }
+  if (bad) { err = "interior cell corner without fine boundary index"; return false; }
+  for (int a = 0; a < nAdj; a++) {
+    bbCount[a + 1] += bbCount[a];
+    bdCount[a + 1] += bdCount[a];
+  }
+  const size_t nbbCells = size_t(bbCount[nAdj]), nbb = nbbCells + 36 * size_t(w.numBoundaryTriangles), nbd = size_t(bdCount[nAdj]);
+  std::vector<int> bbR(nbb), bbC(nbb), bdR(nbd), bdC(nbd);
+  std::vector<double> bbMv(nbb), bbSv(nbb), bdMv(nbd), bdSv(nbd);
+#pragma omp parallel for schedule(static)
+  for (int a = 0; a < nAdj; a++) {
+    const int ic = w.boundaryAdjacentCells[a];
+    const GridChart& gc = L.charts[w.cellChart[ic]];
+    const int i = w.cellIJ[2 * ic], j = w.cellIJ[2 * ic + 1];
+    const int pos[4] = {gc.at(i, j), gc.at(i + 1, j), gc.at(i + 1, j + 1), gc.at(i, j + 1)};
+    const double* M = &adjCellMass[16 * size_t(a)];
+    const double* S = &adjCellStiffness[16 * size_t(a)];
+    size_t ob = size_t(bbCount[a]), od = size_t(bdCount[a]);
+    for (int k = 0; k < 4; k++) {
+      const int node = gc.texel[pos[k]];
+      const int bdk = L.boundaryAndDeep[node];
+      if (bdk < 0) continue;
+      const int b = bdk - 1;
+      for (int l = 0; l < 4; l++) {
+        const int nb = gc.texel[pos[l]];
         if (L.boundaryAndDeep[nb] < 0) {
-          bdM.push_back({b, nb, M[4 * k + l]});
-          bdS.push_back({b, nb, S[4 * k + l]});
+          bdR[od] = b;
+          bdC[od] = nb;
+          bdMv[od] = M[4 * k + l];
+          bdSv[od++] = S[4 * k + l];
         } else {
-          int fk = be.fineBoundaryIndex[gc.interiorTexel[pos[k]]], fl = be.fineBoundaryIndex[gc.interiorTexel[pos[l]]];
-          if (fk < 0 || fl < 0) { err = "interior cell corner without fine boundary index"; return false; }
-          bbM.push_back({fk, fl, M[4 * k + l]});
-          bbS.push_back({fk, fl, S[4 * k + l]});
+          bbR[ob] = be.fineBoundaryIndex[gc.interiorTexel[pos[k]]];
+          bbC[ob] = be.fineBoundaryIndex[gc.interiorTexel[pos[l]]];
+          bbMv[ob] = M[4 * k + l];
+          bbSv[ob++] = S[4 * k + l];
         }
       }
     }
   }
+#pragma omp parallel for schedule(static)
   for (int b = 0; b < w.numBoundaryTriangles; b++) {
     const int* f = &w.btIdx[6 * size_t(b)];
     const double* M = &btMass[36 * size_t(b)];
     const double* S = &btStiffness[36 * size_t(b)];
+    size_t o = nbbCells + 36 * size_t(b);
     for (int k = 0; k < 6; k++)
-      for (int l = 0; l < 6; l++) {
-        bbM.push_back({f[k], f[l], M[6 * l + k]});
-        bbS.push_back({f[k], f[l], S[6 * l + k]});
+      for (int l = 0; l < 6; l++, o++) {
+        bbR[o] = f[k];
+        bbC[o] = f[l];
+        bbMv[o] = M[6 * l + k];
+        bbSv[o] = S[6 * l + k];
       }
   }
-  Csr fineBBM = csr_from_triplets(be.numFineBoundary, be.numFineBoundary, bbM);
-  Csr fineBBS = csr_from_triplets(be.numFineBoundary, be.numFineBoundary, bbS);
-  Csr R = csr_transpose(be.prolongation);
-  fs.bbMass = csr_multiply(R, csr_multiply(fineBBM, be.prolongation));
-  fs.bbStiffness = csr_multiply(R, csr_multiply(fineBBS, be.prolongation));
-  fs.bdMass = csr_from_triplets(L.numBoundary, L.numTexels, bdM);
-  fs.bdStiffness = csr_from_triplets(L.numBoundary, L.numTexels, bdS);
+  // fine boundary blocks, then the texel boundary blocks P^T BB P (one pattern for M and S)
+  Csr fineBBM, fineBBS;
+  csr_from_pairs(be.numFineBoundary, be.numFineBoundary, bbR, bbC, bbMv, bbSv, fineBBM, fineBBS);
+  const Csr R = csr_transpose(be.prolongation);
+  Csr bbPM, bbPS;
+  csr_multiply2(fineBBM, &fineBBS.val, be.prolongation, nullptr, bbPM, bbPS);
+  csr_multiply2(R, nullptr, bbPM, &bbPS.val, fs.bbMass, fs.bbStiffness);
+  csr_from_pairs(L.numBoundary, L.numTexels, bdR, bdC, bdMv, bdSv, fs.bdMass, fs.bdStiffness);
   return true;
 }
 

@@ -11,13 +11,41 @@
 #include <cmath>
 #include <cstring>
 #include <queue>
-#include <unordered_map>
+#include <vector>
 
 #include "setup.h"
 
 namespace gdtp {
 
-static inline uint64_t edge_key(uint32_t a, uint32_t b) { return (uint64_t(a) << 32) | uint64_t(b); }
+// Directed edges (a, b) of a triangle list, grouped by their first vertex:
+// edge lookups scan the few edges leaving a vertex instead of hashing.
+struct DirectedEdges {
+  std::vector<int> start;              // vertex -> first outgoing edge (nv + 1)
+  std::vector<int> to, halfEdge;       // per outgoing edge: end vertex, half-edge 3 t + k
+  // false on a repeated directed edge
+  bool build(const int* tri, int nt, int nv) {
+    start.assign(size_t(nv) + 1, 0);
+    for (int h = 0; h < 3 * nt; h++) start[size_t(tri[h]) + 1]++;
+    for (int v = 0; v < nv; v++) start[v + 1] += start[v];
+    to.resize(3 * size_t(nt));
+    halfEdge.resize(3 * size_t(nt));
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int t = 0; t < nt; t++)
+      for (int k = 0; k < 3; k++) {
+        const int a = tri[3 * t + k], b = tri[3 * t + (k + 1) % 3];
+        for (int e = start[a]; e < fill[a]; e++)
+          if (to[e] == b) return false;
+        to[fill[a]] = b;
+        halfEdge[fill[a]++] = 3 * t + k;
+      }
+    return true;
+  }
+  int find(int a, int b) const {
+    for (int e = start[a]; e < start[a + 1]; e++)
+      if (to[e] == b) return halfEdge[e];
+    return -1;
+  }
+};
 
 static bool same_uv(const V2& a, const V2& b) { return a.x == b.x && a.y == b.y; }
 
@@ -28,17 +56,9 @@ bool build_atlas(const Mesh& mesh, int width, int height, Atlas& A, std::string&
   const int* T = mesh.triangles.data();
 
   // directed half-edge table of the input mesh
-  std::unordered_map<uint64_t, int> half;
-  half.reserve(size_t(nt) * 4);
-  for (int t = 0; t < nt; t++)
-    for (int k = 0; k < 3; k++) {
-      uint64_t key = edge_key(T[3 * t + k], T[3 * t + (k + 1) % 3]);
-      if (!half.emplace(key, 3 * t + k).second) { err = "non-manifold mesh (repeated directed edge)"; return false; }
-    }
-  auto opposite = [&](int t, int k) -> int {
-    auto it = half.find(edge_key(T[3 * t + (k + 1) % 3], T[3 * t + k]));
-    return it == half.end() ? -1 : it->second;
-  };
+  DirectedEdges half;
+  if (!half.build(T, nt, mesh.nv())) { err = "non-manifold mesh (repeated directed edge)"; return false; }
+  auto opposite = [&](int t, int k) -> int { return half.find(T[3 * t + (k + 1) % 3], T[3 * t + k]); };
   // an edge is interior to a chart when its twin carries the same texture coordinates
   auto uv_continuous = [&](int t, int k, int o) {
     int s = o / 3, m = o % 3;
@@ -69,31 +89,28 @@ bool build_atlas(const Mesh& mesh, int width, int height, Atlas& A, std::string&
   }
   A.numCharts = comp + 1;
 
-  // ---- atlas vertices: one per distinct (texture coordinate, mesh vertex) pair, first-seen order
-  struct Key { uint64_t u, v; int m; bool operator==(const Key& o) const { return u == o.u && v == o.v && m == o.m; } };
-  struct KeyHash { size_t operator()(const Key& k) const { return std::hash<uint64_t>()(k.u * 0x9E3779B97F4A7C15ull ^ (k.v + 0x7F4A7C15ull * (uint64_t)k.m)); } };
-  std::unordered_map<Key, int, KeyHash> vmap;
-  vmap.reserve(size_t(nt) * 2);
+  // ---- atlas vertices: one per distinct (texture coordinate, mesh vertex) pair,
+  // first-seen order; the atlas vertices of a mesh vertex are chained
+  // (bitwise comparison of the coordinates)
   A.triangles.resize(nt);
-  for (int t = 0; t < nt; t++)
-    for (int k = 0; k < 3; k++) {
-      V2 p = mesh.corner(t, k);
-      Key key;
-      std::memcpy(&key.u, &p.x, 8);
-      std::memcpy(&key.v, &p.y, 8);
-      key.m = T[3 * t + k];
-      auto it = vmap.find(key);
-      int id;
-      if (it == vmap.end()) {
-        id = (int)A.vertices.size();
-        vmap.emplace(key, id);
-        A.vertices.push_back(p);
-        A.vertexMap.push_back(T[3 * t + k]);
-      } else {
-        id = it->second;
+  {
+    std::vector<int> firstOf(mesh.nv(), -1), nextOf;
+    for (int t = 0; t < nt; t++)
+      for (int k = 0; k < 3; k++) {
+        const V2 p = mesh.corner(t, k);
+        const int m = T[3 * t + k];
+        int id = firstOf[m];
+        while (id != -1 && std::memcmp(&A.vertices[id], &p, sizeof(V2)) != 0) id = nextOf[id];
+        if (id == -1) {
+          id = (int)A.vertices.size();
+          A.vertices.push_back(p);
+          A.vertexMap.push_back(m);
+          nextOf.push_back(firstOf[m]);
+          firstOf[m] = id;
+        }
+        A.triangles[t][k] = id;
       }
-      A.triangles[t][k] = id;
-    }
+  }
 
   // ---- vertices within 1e-6 texel of a texel-centre line are moved off it
   // (the reference does this with rand(); a deterministic offset keeps the atlas
@@ -113,22 +130,20 @@ bool build_atlas(const Mesh& mesh, int width, int height, Atlas& A, std::string&
     }
 
   // ---- atlas edge indices
-  std::unordered_map<uint64_t, int> ahalf;
-  ahalf.reserve(size_t(nt) * 4);
+  std::vector<int> atlasTri(3 * size_t(nt));
   for (int t = 0; t < nt; t++)
-    for (int k = 0; k < 3; k++) {
-      uint64_t key = edge_key(A.triangles[t][k], A.triangles[t][(k + 1) % 3]);
-      if (!ahalf.emplace(key, 3 * t + k).second) { err = "non-oriented-manifold atlas"; return false; }
-    }
+    for (int k = 0; k < 3; k++) atlasTri[3 * t + k] = A.triangles[t][k];
+  DirectedEdges ahalf;
+  if (!ahalf.build(atlasTri.data(), nt, (int)A.vertices.size())) { err = "non-oriented-manifold atlas"; return false; }
   const int res = std::max(width, height);
   int nextEdge = 2 * res * res * A.numCharts;
   A.halfEdgeToEdgeIndex.assign(3 * nt, -1);
   for (int t = 0; t < nt; t++)
     for (int k = 0; k < 3; k++) {
       int cur = 3 * t + k;
-      auto it = ahalf.find(edge_key(A.triangles[t][(k + 1) % 3], A.triangles[t][k]));
-      if (it != ahalf.end()) {
-        if (cur < it->second) A.halfEdgeToEdgeIndex[cur] = A.halfEdgeToEdgeIndex[it->second] = nextEdge++;
+      const int o = ahalf.find(A.triangles[t][(k + 1) % 3], A.triangles[t][k]);
+      if (o >= 0) {
+        if (cur < o) A.halfEdgeToEdgeIndex[cur] = A.halfEdgeToEdgeIndex[o] = nextEdge++;
       } else {
         A.halfEdgeToEdgeIndex[cur] = nextEdge++;
       }

@@ -315,7 +315,12 @@ bool build_boundary_elements(const Hierarchy& H, BoundaryElements& be, std::stri
     std::vector<int> idx, atlasVertex, atlasEdge, parentEdge;
   };
   std::vector<std::vector<std::vector<Poly>>> cellPolys(nCharts);
+  // charts in parallel: each writes its own polygons and auxiliary nodes; the
+  // seam-node coverage counts are summed atomically
+  std::vector<std::string> chartErr(nCharts);
+#pragma omp parallel for schedule(dynamic, 1)
   for (int c = 0; c < nCharts; c++) {
+    auto chart_polygons = [&](std::string& err) -> bool {
     const AtlasChart& ac = A.charts[c];
     const GridChart& g = L.charts[c];
     ChartBoundary& cb = be.charts[c];
@@ -433,6 +438,7 @@ bool build_boundary_elements(const Hierarchy& H, BoundaryElements& be, std::stri
           Q.parentEdge.push_back(parent);
           for (auto& in : ins) {
             if (in.second < A.numBoundaryVertices || in.second > be.numBoundaryNodes) { err = "seam node index out of range"; return false; }
+#pragma omp atomic
             oppositeCovered[in.second - A.numBoundaryVertices]++;
             V2 pos = P.v[j] * (1.0 - in.first) + P.v[(j + 1) % m] * in.first;
             cb.aux.push_back({pos, in.second + numInterior});
@@ -446,13 +452,37 @@ bool build_boundary_elements(const Hierarchy& H, BoundaryElements& be, std::stri
         cellPolys[c][cell].push_back(std::move(Q));
       }
     }
+        return true;
+    };
+    chart_polygons(chartErr[c]);
   }
+  for (const std::string& e : chartErr)
+    if (!e.empty()) { err = e; return false; }
   if (A.isClosed)
     for (size_t i = 0; i < oppositeCovered.size(); i++)
       if (oppositeCovered[i] != 1) { err = "seam node " + std::to_string(i) + " not matched on the opposite side"; return false; }
 
   // (3) quadratic elements: triangulate every cell polygon, add mid-edge nodes
   const int firstMid = be.numBoundaryNodes + numInterior;
+  // triangulations of every polygon (charts in parallel), then the mid-edge
+  // nodes numbered in chart, cell and polygon order
+  std::vector<std::vector<std::vector<std::vector<I3>>>> polyTris(nCharts);
+  std::vector<std::vector<std::vector<char>>> polyOk(nCharts);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < nCharts; c++) {
+    const int nCells = (int)cellPolys[c].size();
+    polyTris[c].resize(nCells);
+    polyOk[c].resize(nCells);
+    for (int cell = 0; cell < nCells; cell++) {
+      const std::vector<Poly>& polys = cellPolys[c][cell];
+      polyTris[c][cell].resize(polys.size());
+      polyOk[c][cell].resize(polys.size());
+      for (size_t q = 0; q < polys.size(); q++) {
+        std::vector<I3>& tris = polyTris[c][cell][q];
+        polyOk[c][cell][q] = triangulate_polygon(polys[q].v, tris) && tris.size() + 2 == polys[q].v.size();
+      }
+    }
+  }
   std::unordered_map<uint64_t, int> midOf;
   int nextMid = 0;
   for (int c = 0; c < nCharts; c++) {
@@ -460,10 +490,11 @@ bool build_boundary_elements(const Hierarchy& H, BoundaryElements& be, std::stri
     ChartBoundary& cb = be.charts[c];
     cb.cellTriangles.assign(g.numBoundaryCells, {});
     for (int cell = 0; cell < g.numBoundaryCells; cell++)
-      for (const Poly& P : cellPolys[c][cell]) {
-        std::vector<I3> tris;
+      for (size_t q = 0; q < cellPolys[c][cell].size(); q++) {
+        const Poly& P = cellPolys[c][cell][q];
+        const std::vector<I3>& tris = polyTris[c][cell][q];
         const int n = (int)P.v.size();
-        if (!triangulate_polygon(P.v, tris) || (int)tris.size() != n - 2) {
+        if (!polyOk[c][cell][q]) {
           be.degenerateTriangulations++;
           if (getenv("GDTP_DEBUG_POLY")) {
             fprintf(stderr, "degenerate polygon chart %d cell %d n=%d tris=%d\n", c, cell, n, (int)tris.size());

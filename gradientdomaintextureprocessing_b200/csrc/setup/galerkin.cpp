@@ -10,6 +10,7 @@
 // the reference by summation order.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <map>
 
 #include "setup.h"
@@ -87,45 +88,59 @@ bool galerkin_hierarchy(const Hierarchy& h, int L, const std::vector<double>& de
       for (int k = 0; k < 9; k++) B.deep[10 * size_t(d) + k] = acc[k];
     }
     if (bad) { err = "coarse deep texel over a non-deep fine neighbourhood"; return false; }
-    // ---- boundary rows: R_b (A P), one row at a time
+    // ---- boundary rows: R_b (A P), one row at a time (rows in parallel
+    // chunks, their triplets concatenated in row order)
     const Csr& Rb = F.boundaryRestriction;
     std::vector<Triplet> tbb, tbd;
-    std::vector<double> acc(C.numTexels, 0.0);
-    std::vector<int> mark(C.numTexels, -1), touched;
-    for (int b = 0; b < C.numBoundary; b++) {
-      touched.clear();
-      auto add = [&](int fineCol, double v) {
-        int cols[4];
-        double wts[4];
-        int m = prolong_row(F, C, fineCol, cols, wts);
-        if (m < 0) { bad = true; return; }
-        for (int k = 0; k < m; k++) {
-          int c = cols[k];
-          if (mark[c] != b) { mark[c] = b; acc[c] = 0.0; touched.push_back(c); }
-          acc[c] += v * wts[k];
-        }
-      };
-      for (int e = Rb.ptr[b]; e < Rb.ptr[b + 1]; e++) {
-        const int p = Rb.col[e];
-        const double wp = Rb.val[e];
-        const int bd = F.boundaryAndDeep[p];
-        if (bd < 0) {  // deep fine row: 9-point stencil
-          const NodeInfo& n = F.nodes[p];
-          const GridChart& fc = F.charts[n.chart];
-          const double* a = &A.deep[10 * size_t(-bd - 1)];
-          for (int oy = -1; oy <= 1; oy++)
-            for (int ox = -1; ox <= 1; ox++) add(fc.texel[fc.at(n.ci + ox, n.cj + oy)], wp * a[(oy + 1) * 3 + (ox + 1)]);
-        } else {
-          const int fb = bd - 1;
-          for (int k = A.bd.ptr[fb]; k < A.bd.ptr[fb + 1]; k++) add(A.bd.col[k], wp * A.bd.val[k]);
-          for (int k = A.bb.ptr[fb]; k < A.bb.ptr[fb + 1]; k++) add(F.boundaryGlobal[A.bb.col[k]], wp * A.bb.val[k]);
+    const int nChunks = std::max(1, std::min(256, C.numBoundary / 64));
+    std::vector<std::vector<Triplet>> cbb(nChunks), cbd(nChunks);
+#pragma omp parallel reduction(||: bad)
+    {
+      std::vector<double> acc(C.numTexels, 0.0);
+      std::vector<int> mark(C.numTexels, -1), touched;
+#pragma omp for schedule(dynamic, 1)
+      for (int q = 0; q < nChunks; q++) {
+        const int b0 = int(int64_t(C.numBoundary) * q / nChunks), b1 = int(int64_t(C.numBoundary) * (q + 1) / nChunks);
+        for (int b = b0; b < b1; b++) {
+          touched.clear();
+          auto add = [&](int fineCol, double v) {
+            int cols[4];
+            double wts[4];
+            int m = prolong_row(F, C, fineCol, cols, wts);
+            if (m < 0) { bad = true; return; }
+            for (int k = 0; k < m; k++) {
+              int c = cols[k];
+              if (mark[c] != b) { mark[c] = b; acc[c] = 0.0; touched.push_back(c); }
+              acc[c] += v * wts[k];
+            }
+          };
+          for (int e = Rb.ptr[b]; e < Rb.ptr[b + 1]; e++) {
+            const int p = Rb.col[e];
+            const double wp = Rb.val[e];
+            const int bd = F.boundaryAndDeep[p];
+            if (bd < 0) {  // deep fine row: 9-point stencil
+              const NodeInfo& n = F.nodes[p];
+              const GridChart& fc = F.charts[n.chart];
+              const double* a = &A.deep[10 * size_t(-bd - 1)];
+              for (int oy = -1; oy <= 1; oy++)
+                for (int ox = -1; ox <= 1; ox++) add(fc.texel[fc.at(n.ci + ox, n.cj + oy)], wp * a[(oy + 1) * 3 + (ox + 1)]);
+            } else {
+              const int fb = bd - 1;
+              for (int k = A.bd.ptr[fb]; k < A.bd.ptr[fb + 1]; k++) add(A.bd.col[k], wp * A.bd.val[k]);
+              for (int k = A.bb.ptr[fb]; k < A.bb.ptr[fb + 1]; k++) add(F.boundaryGlobal[A.bb.col[k]], wp * A.bb.val[k]);
+            }
+          }
+          for (int c : touched) {
+            int cb = C.boundaryAndDeep[c];
+            if (cb > 0) cbb[q].push_back({b, cb - 1, acc[c]});
+            else cbd[q].push_back({b, c, acc[c]});
+          }
         }
       }
-      for (int c : touched) {
-        int cb = C.boundaryAndDeep[c];
-        if (cb > 0) tbb.push_back({b, cb - 1, acc[c]});
-        else tbd.push_back({b, c, acc[c]});
-      }
+    }
+    for (int q = 0; q < nChunks; q++) {
+      tbb.insert(tbb.end(), cbb[q].begin(), cbb[q].end());
+      tbd.insert(tbd.end(), cbd[q].begin(), cbd[q].end());
     }
     if (bad) { err = "prolongation reads an inactive coarse texel"; return false; }
     B.bb = csr_from_triplets(C.numBoundary, C.numBoundary, tbb);

@@ -41,8 +41,8 @@ static M2 barycentric_map(const V2 t[3]) {
   return m.inverse();
 }
 
-static bool classify_chart(int chartId, const AtlasChart& ac, GridChart& g, GridLevel& L, int deepRadius,
-                           std::string& err) {
+// (1)-(3): node and cell types of one chart (chart-local; charts in parallel)
+static bool classify_chart(const AtlasChart& ac, GridChart& g, int deepRadius, std::string& err) {
   const int W = g.width, H = g.height;
   const double cw = g.cellSizeW, ch = g.cellSizeH;
   g.nodeType.assign(size_t(W) * H, -1);
@@ -147,7 +147,12 @@ static bool classify_chart(int chartId, const AtlasChart& ac, GridChart& g, Grid
           if (g.cellType[g.cat(i + di, j + dj)] != 1) { deep = false; break; }
       if (deep) g.nodeType[g.at(i, j)] = 2;
     }
+  return true;
+}
 
+// (4)-(5): global enumeration of one chart's texels and cells, in chart order
+static bool enumerate_chart(int chartId, GridChart& g, GridLevel& L, std::string& err) {
+  const int W = g.width, H = g.height;
   // (4) enumeration
   g.texelOffset = L.numTexels;
   g.interiorTexelOffset = L.numInteriorTexels;
@@ -216,7 +221,10 @@ static bool build_level(const Atlas& A, int level, int width, int height, const 
   const double cw = double(factor) / double(width);
   const double ch = double(factor) / double(height);
   L.charts.assign(A.charts.size(), GridChart());
-  for (size_t c = 0; c < A.charts.size(); c++) {
+  const int nCharts = (int)A.charts.size();
+  std::vector<std::string> chartErr(nCharts);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < nCharts; c++) {
     const AtlasChart& ac = A.charts[c];
     GridChart& g = L.charts[c];
     int half[2][2];
@@ -234,7 +242,11 @@ static bool build_level(const Atlas& A, int level, int width, int height, const 
     g.cellSizeH = ch;
     int approx = std::max(int(std::ceil(1.0 / cw)), int(std::ceil(1.0 / ch)));
     g.gridIndexOffset = 2 * approx * approx * int(c);
-    if (!classify_chart(int(c), ac, g, L, info.boundaryDilation + 1, err)) return false;
+    classify_chart(ac, g, info.boundaryDilation + 1, chartErr[c]);
+  }
+  for (int c = 0; c < nCharts; c++) {
+    if (!chartErr[c].empty()) { err = chartErr[c]; return false; }
+    if (!enumerate_chart(c, L.charts[c], L, err)) return false;
   }
   if (L.numTexels != L.numBoundary + L.numDeep) { err = "boundary and deep texels do not partition the texels"; return false; }
   L.boundaryAndDeep.assign(L.numTexels, 0);

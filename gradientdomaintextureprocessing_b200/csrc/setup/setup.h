@@ -143,6 +143,13 @@ struct Csr {                                                          // CSR, so
 };
 struct Triplet { int r, c; double v; };
 Csr csr_from_triplets(int rows, int cols, std::vector<Triplet>& t);    // sums duplicates
+// two value sets on one list of (row, column) entries: m1 from v1, m2 from v2,
+// each as csr_from_triplets would build it
+void csr_from_pairs(int rows, int cols, const std::vector<int>& r, const std::vector<int>& c, const std::vector<double>& v1,
+                    const std::vector<double>& v2, Csr& m1, Csr& m2);
+// c1 = a b and c2 = a' b' on one pattern, a' = a with values *a2 (or a's own
+// when null), b' likewise; each as csr_multiply would compute it
+void csr_multiply2(const Csr& a, const std::vector<double>* a2, const Csr& b, const std::vector<double>* b2, Csr& c1, Csr& c2);
 Csr csr_transpose(const Csr& a);
 Csr csr_multiply(const Csr& a, const Csr& b);
 Csr csr_axpby(double a, const Csr& A, double b, const Csr& B);

@@ -19,6 +19,7 @@
 
 #include <map>
 #include <stdexcept>
+#include <thread>
 #include <tuple>
 
 #include "system.h"
@@ -308,7 +309,7 @@ bool DeviceSystem::check(cudaError_t e, const char* what) {
 }
 
 size_t DeviceSystem::deviceBytes() const {
-  size_t b = rawArena_.total + rawAArena_.total + workArena_.total + slotArena_.total;
+  size_t b = rawArena_.total + rawAArena_.total + workArena_.total + slotArena_.total + deepArena_.total;
   for (const auto& m : mg32_) b += m->arena.total;
   if (mg64_) b += mg64_->arena.total;
   if (plan_) b += plan_->deviceBytes();
@@ -318,8 +319,22 @@ size_t DeviceSystem::deviceBytes() const {
 // ----------------------------------------------------------------------------
 // assembly
 // ----------------------------------------------------------------------------
+static double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
   if (!err_.empty()) return false;
+  const double tAssembly = now_ms();
+  // a new assembly replaces everything built from the previous one
+  mg32_.clear();
+  mg64_.reset();
+  invalidate_graph();
+  plan_.reset();
+  bsCache_.clear();
+  coLevels_ = 0;
+  hostCoeffs_ = false;
+  rawFromPlan_ = false;
   cudaSetDevice(device_);
   ChartMetrics g;
   if (parameterMetric) {
@@ -338,6 +353,7 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
   metric_ = g;
   AssemblyWork w;
   build_assembly_work(h_, be_, g, w);
+  setupMs[8] = now_ms() - tAssembly;
   DeviceArena A;
   int* cellPtr = A.upload(w.cellPtr);
   int* cellTri = A.upload(w.cellTri);
@@ -356,8 +372,14 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
   double* cm = A.zeros<double>(16 * size_t(w.numInteriorCells));
   double* cs = A.zeros<double>(16 * size_t(w.numInteriorCells));
   const int nd = h_.levels[0].numDeep;
-  double* dm = A.zeros<double>(10 * size_t(nd));
-  double* ds = A.zeros<double>(10 * size_t(nd));
+  // the level-0 deep coefficients stay resident: the operators' planes and the
+  // numeric set-up read them on the device
+  deepArena_ = DeviceArena();
+  double* dm = deepArena_.zeros<double>(10 * size_t(nd));
+  double* ds = deepArena_.zeros<double>(10 * size_t(nd));
+  deepMassDev_ = dm;
+  deepStiffDev_ = ds;
+  if (!check(deepArena_.last, "deep coefficients")) return false;
   const size_t na = w.boundaryAdjacentCells.size();
   double* am = A.zeros<double>(16 * na);
   double* as = A.zeros<double>(16 * na);
@@ -383,16 +405,19 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
             check(cudaMemcpyAsync(hbs.data(), bs, hbs.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
             check(cudaStreamSynchronize(stream_), "assembly");
   if (!ok) return false;
+  setupMs[9] = now_ms() - tAssembly - setupMs[8];
   if (!assemble_boundary_blocks(h_, be_, w, ham, has, hbm, hbs, fine_, err_)) return false;
+  setupMs[10] = now_ms() - tAssembly - setupMs[8] - setupMs[9];
 
   // raw FP64 operators of M and S on level 0 (deep planes in line-run order)
   runs0_ = build_line_runs(h_.levels[0]);
   const GridLevel& L0 = h_.levels[0];
-  auto make_raw = [&](const std::vector<double>& deep, const Csr& bb, const Csr& bd, RawOperator& op) {
+  rawArena_ = DeviceArena();
+  const int* runTexel = rawArena_.upload(runs0_.texel);
+  auto make_raw = [&](const double* deepDev, const Csr& bb, const Csr& bd, RawOperator& op) {
     const int cnt = runs0_.count;
-    std::vector<double> planes(size_t(9) * cnt);
-    for (int i = 0; i < cnt; i++)
-      for (int k = 0; k < 9; k++) planes[size_t(k) * cnt + i] = deep[10 * size_t(runs0_.texel[i]) + k];
+    double* planes = static_cast<double*>(rawArena_.alloc(size_t(9) * std::max(1, cnt) * sizeof(double)));
+    if (planes && cnt > 0) launch_gather_planes(cnt, runTexel, deepDev, planes, stream_);
     std::vector<int> ptr(1, 0), col;
     std::vector<double> val;
     for (int b = 0; b < L0.numBoundary; b++) {
@@ -402,7 +427,7 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
     }
     op.runs = rawArena_.upload(runs0_.runs);
     op.nRuns = (int)runs0_.runs.size();
-    op.coef = rawArena_.upload(planes);
+    op.coef = planes;
     op.planeStride = cnt;
     op.bPtr = rawArena_.upload(ptr);
     op.bCol = rawArena_.upload(col);
@@ -410,8 +435,10 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
     op.bGlobal = rawArena_.upload(L0.boundaryGlobal);
     op.nB = L0.numBoundary;
   };
-  make_raw(fine_.deepMass, fine_.bbMass, fine_.bdMass, rawM_);
-  make_raw(fine_.deepStiffness, fine_.bbStiffness, fine_.bdStiffness, rawS_);
+  make_raw(dm, fine_.bbMass, fine_.bdMass, rawM_);
+  make_raw(ds, fine_.bbStiffness, fine_.bdStiffness, rawS_);
+  if (!check(cudaStreamSynchronize(stream_), "operator planes")) return false;
+  setupMs[11] = now_ms() - tAssembly - setupMs[8] - setupMs[9] - setupMs[10];
   return check(rawArena_.last, "operator upload");
 }
 
@@ -437,9 +464,6 @@ struct DeviceDense final : DenseBackend {
 };
 }  // namespace
 
-static double now_ms() {
-  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
 
 bool DeviceSystem::update(double stiffness, double screen) {
   if (!err_.empty()) return false;
@@ -456,12 +480,22 @@ bool DeviceSystem::update(double stiffness, double screen) {
   // hierarchies are coarsened once (per level count) and every update
   // combines them, so a re-weighting costs one pass over the coefficients
   if (coLevels_ != L) {
+    const double t0 = now_ms();
     Csr bdM = fine_.bdMass, bdS = fine_.bdStiffness;
     bdM.cols = bdS.cols = L0.numTexels;
-    if (!galerkin_hierarchy(h_, L, fine_.deepMass, fine_.bbMass, bdM, coMass_, err_) ||
-        !galerkin_hierarchy(h_, L, fine_.deepStiffness, fine_.bbStiffness, bdS, coStiff_, err_))
+    // M and S coarsen side by side (each with its own parallel loops)
+    std::string errS;
+    bool okS = false;
+    std::thread stiff([&] { okS = galerkin_hierarchy(h_, L, fine_.deepStiffness, fine_.bbStiffness, bdS, coStiff_, errS); });
+    const bool okM = galerkin_hierarchy(h_, L, fine_.deepMass, fine_.bbMass, bdM, coMass_, err_);
+    stiff.join();
+    if (!okM) return false;
+    if (!okS) {
+      err_ = errS;
       return false;
+    }
     coLevels_ = L;
+    setupMs[12] = now_ms() - t0;
   }
   const bool sameLevels = (levelsUsed_ == L);
   levelsUsed_ = L;
@@ -563,11 +597,12 @@ bool DeviceSystem::ensure_plan() {
   plan_.reset(new NumericPlan());
   plan_->gen = ++planCount_;
   const double t0 = now_ms();
-  if (!plan_->build(h_, L, fine_, coMass_, coStiff_, knobs.maxBlock, knobs.denseBoundaryMax, stream_, err_)) {
+  if (!plan_->build(h_, L, fine_, coMass_, coStiff_, deepMassDev_, deepStiffDev_, knobs.maxBlock, knobs.denseBoundaryMax, stream_,
+                    err_)) {
     plan_.reset();
     return false;
   }
-  planMs_ = now_ms() - t0;
+  setupMs[13] = now_ms() - t0;
   rawFromPlan_ = false;
   return true;
 }
@@ -972,8 +1007,7 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     mg.planGen = plan_->gen;
     setupMs[1] = tBoundary;
     setupMs[2] = tCoarse;
-    setupMs[3] = tLayout + planMs_;
-    planMs_ = 0;
+    setupMs[3] = tLayout;
     std::copy(tBs, tBs + 4, setupMs + 4);
   } else {
     mg.planGen = -1;
@@ -1331,6 +1365,21 @@ bool DeviceSystem::apply(int which, const double* x, double* y, int k) {
   return check(cudaMemcpyAsync(x64_, x, n * k * 8, cudaMemcpyHostToDevice, stream_), "h2d") &&
          raw_apply_dev(*op, nullptr, x64_, r64_, k, 1, stream_, nullptr) &&
          check(cudaMemcpyAsync(y, r64_, n * k * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
+         check(cudaStreamSynchronize(stream_), "apply");
+}
+
+bool DeviceSystem::apply_combination(double a, double b, const double* x, double* y, int k) {
+  if (!err_.empty()) return false;
+  cudaSetDevice(device_);
+  if (k < 1 || k > 64) { err_ = "k must be in [1, 64]"; return false; }
+  if (!ensure_work(k)) return false;
+  const size_t n = h_.levels[0].numTexels;
+  if (!check(cudaMemcpyAsync(x64_, x, n * k * 8, cudaMemcpyHostToDevice, stream_), "h2d") ||
+      !raw_apply_dev(rawM_, nullptr, x64_, r64_, k, 1, stream_, nullptr) ||
+      !raw_apply_dev(rawS_, nullptr, x64_, b64_, k, 1, stream_, nullptr))
+    return false;
+  dev::launch_axpby(r64_, a, r64_, b, b64_, (long long)(n * k), stream_);
+  return check(cudaMemcpyAsync(y, r64_, n * k * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
          check(cudaStreamSynchronize(stream_), "apply");
 }
 

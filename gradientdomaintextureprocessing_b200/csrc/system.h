@@ -153,6 +153,8 @@ class DeviceSystem {
 
   // host in/out, k right-hand sides (tight n x k)
   bool apply(int which, const double* x, double* y, int k);
+  // y = a M x + b S x (one upload, one download)
+  bool apply_combination(double a, double b, const double* x, double* y, int k);
   bool solve_mixed(const double* b_host, double* x_host, const double* b_dev, double* x_dev, int k, double tol, int maxIters,
                    cudaStream_t userStream, SolveReport& rep, bool zeroGuess = false);
   // plain FP64 V-cycles: host buffers (b_host, x_host) or the caller's device
@@ -233,8 +235,12 @@ class DeviceSystem {
   // boundary solver factorisations, coarsest inverse, other multigrid set-up
   // (device layouts, uploads); the last three when the multigrid is built;
   // then the boundary solver factorisations split into partition and sparse
-  // assembly, subdomain inverses, Schur products, Schur complement inverse
-  double setupMs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // assembly, subdomain inverses, Schur products, Schur complement inverse;
+  // then the assembly {assembly work lists (host), device assembly with its
+  // transfers, boundary blocks (host), level-0 operator layouts}, the Galerkin
+  // coarsening of M and S (host, once per level count) and the numeric plan's
+  // layout (host, once per level count and boundary partition)
+  double setupMs[14] = {0};
   int graphKernels = 0;         // kernel nodes in the refinement-step graph
   int64_t kernelLaunches = 0;   // kernels launched by solve_mixed since the last profile reset
 
@@ -279,7 +285,6 @@ class DeviceSystem {
   int bsCacheKey_[3] = {-1, -1, -1};
   bool hostCoeffs_ = false;             // coeffs_ holds the current weights' combination
   std::unique_ptr<NumericPlan> plan_;
-  double planMs_ = 0;                   // host layout time of the plan, reported with the next build
   int planCount_ = 0;                   // numeric plans built so far (their generation numbers)
   bool rawFromPlan_ = false;            // rawA_ holds the plan's boundary-row layout
   int coLevels_ = 0;
@@ -289,6 +294,8 @@ class DeviceSystem {
   bool profiling_ = false;
 
   DeviceArena rawArena_;                // M and S operators (assembly)
+  DeviceArena deepArena_;               // level-0 deep M and S coefficients (assembly)
+  const double *deepMassDev_ = nullptr, *deepStiffDev_ = nullptr;
   DeviceArena rawAArena_;               // A = screen M + stiffness S (replaced by every update)
   RawOperator rawM_, rawS_, rawA_;
   DeepRuns runs0_;

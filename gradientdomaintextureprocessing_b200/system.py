@@ -231,8 +231,12 @@ def VCycle(system: System, x: np.ndarray, rhs: np.ndarray) -> np.ndarray:
 
 
 def texture_filtering_rhs(system: System, f: np.ndarray, stiffness: float, sharpness: float) -> np.ndarray:
-    """``M f + stiffness * sharpness * S f`` (TextureFiltering.cpp:693-700)."""
-    return system.apply(f, MASS) + stiffness * sharpness * system.apply(f, STIFFNESS)
+    """``M f + stiffness * sharpness * S f`` (TextureFiltering.cpp:693-700), formed
+    on the device from one upload of ``f``."""
+    x, k = system._vec(f, np.float64)
+    y = np.empty_like(x)
+    _lib.check(_lib.lib().gdtp_apply_mass_stiffness(system.handle, 1.0, float(stiffness) * float(sharpness), _lib.ptr(x), _lib.ptr(y), k))
+    return y
 
 
 def texel_signal(hierarchy: Hierarchy, texture: np.ndarray) -> np.ndarray:

@@ -117,12 +117,21 @@ void gdtp_system_free(gdtp_system* s);
  *   "profile.setup": ms of the last set-up {update, boundary solver factorisations,
  *   coarsest inverse, other multigrid set-up, then the factorisations split into
  *   partition and sparse assembly, subdomain inverses, Schur products, Schur
- *   complement inverse}; all but the first are spent by the first solve after
- *   an update (or after a new right-hand-side width) */
+ *   complement inverse; then the assembly {work lists, device assembly with its
+ *   transfers, boundary blocks, level-0 operators}, the Galerkin coarsening of M
+ *   and S and the numeric set-up's layout}: 14 values.  With the numeric set-up
+ *   (device_factor 1) an update of a built system refills its multigrid in
+ *   place and reports that in the first eight; otherwise the multigrid values
+ *   are spent by the first solve after an update (or after a new
+ *   right-hand-side width) */
 int gdtp_system_array(const gdtp_system* s, const char* name, int level, void* out, int64_t* count);
 
-/* Combine and coarsen: A = screen*M + stiffness*S and its Galerkin hierarchy;
- * the boundary-block and coarsest-level inverses are rebuilt by the next solve.
+/* Combine and coarsen: A = screen*M + stiffness*S and its Galerkin hierarchy
+ * (M and S are coarsened once per level count; an update combines them).  With
+ * device_factor 1 (the default) every weight-dependent value -- smoother planes,
+ * boundary rows, boundary-block and coarsest-level inverses -- is recomputed on
+ * the device, in place in a multigrid already built; otherwise the next solve
+ * rebuilds the multigrid from host-combined coefficients.
  * Replaces UpdateLinearSystem (include/Src/UpdateCoefficients.inl:463-513),
  * UpdateMultigridCoefficients (:285-399) and UpdateMultigridSolvers (:402-439). */
 int gdtp_system_update(gdtp_system* s, double stiffness_weight, double screen_weight);
@@ -131,6 +140,11 @@ int gdtp_system_update(gdtp_system* s, double stiffness_weight, double screen_we
  * MultiplyBySystemMatrix_NoReciprocals (include/Src/IterativeSolvers.inl:881-950).
  * Host float64 buffers of numTexels*k. */
 int gdtp_apply(gdtp_system* s, int which, const double* x, double* y, int k);
+/* y = mass_weight M x + stiffness_weight S x (host float64 numTexels*k, one
+ * upload and one download): the filtering right-hand side M f + w s S f of
+ * TextureFiltering.cpp:693-700, which the reference forms with two
+ * MultiplyBySystemMatrix_NoReciprocals calls (IterativeSolvers.inl:881-950). */
+int gdtp_apply_mass_stiffness(gdtp_system* s, double mass_weight, double stiffness_weight, const double* x, double* y, int k);
 
 /* One FP32 V-cycle on level-0 vectors (host float32, numTexels*k), x updated in
  * place.  Replaces VCycle (include/Src/IterativeSolvers.inl:1211-1333). */
