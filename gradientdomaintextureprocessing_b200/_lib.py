@@ -47,6 +47,7 @@ _SIGS = {
     "gdtp_system_free": (None, [_P]),
     "gdtp_system_array": (C.c_int, [_P, C.c_char_p, C.c_int, _P, C.POINTER(C.c_int64)]),
     "gdtp_apply_mass_stiffness": (C.c_int, [_P, C.c_double, C.c_double, _P, _P, C.c_int]),
+    "gdtp_texel_signal": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, _P]),
     "gdtp_system_update": (C.c_int, [_P, C.c_double, C.c_double]),
     "gdtp_apply": (C.c_int, [_P, C.c_int, _P, _P, C.c_int]),
     "gdtp_vcycle": (C.c_int, [_P, _P, _P, C.c_int]),

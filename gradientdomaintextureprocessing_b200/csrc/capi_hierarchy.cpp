@@ -188,3 +188,32 @@ extern "C" int gdtp_hierarchy_array(const gdtp_hierarchy* h, const char* cname, 
     return fail(GDTP_ERR_INVALID, "gdtp_hierarchy_array: unknown array " + name);
   });
 }
+
+extern "C" int gdtp_texel_signal(const gdtp_hierarchy* h, const void* texture, int width, int height, int channels, int bytes_per_value,
+                                 int64_t row_stride, int64_t pixel_stride, int64_t channel_stride, double* out) {
+  return guarded("gdtp_texel_signal", [&]() -> int {
+    if (!h || !texture || !out || width <= 0 || height <= 0 || channels <= 0 || (bytes_per_value != 4 && bytes_per_value != 8))
+      return fail(GDTP_ERR_INVALID, "gdtp_texel_signal: bad arguments");
+    const GridLevel& L = h->h.levels[0];
+    const int nCharts = (int)L.charts.size();
+    bool outside = false;
+#pragma omp parallel for schedule(dynamic, 1) reduction(||: outside)
+    for (int c = 0; c < nCharts; c++) {
+      const GridChart& g = L.charts[c];
+      for (int j = 0; j < g.height; j++)
+        for (int i = 0; i < g.width; i++) {
+          const int t = g.texel[g.at(i, j)];
+          if (t == -1) continue;
+          const int x = g.cornerCoords[0] + i, y = g.cornerCoords[1] + j;
+          if (x < 0 || y < 0 || x >= width || y >= height) { outside = true; continue; }
+          const char* px = static_cast<const char*>(texture) + int64_t(y) * row_stride + int64_t(x) * pixel_stride;
+          for (int q = 0; q < channels; q++) {
+            const char* v = px + int64_t(q) * channel_stride;
+            out[size_t(t) * channels + q] = bytes_per_value == 4 ? double(*reinterpret_cast<const float*>(v)) : *reinterpret_cast<const double*>(v);
+          }
+        }
+    }
+    if (outside) return fail(GDTP_ERR_INVALID, "gdtp_texel_signal: a texel lies outside the texture");
+    return GDTP_OK;
+  });
+}

@@ -2,7 +2,9 @@
 #include "numeric.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <cstdint>
 #include <cmath>
 
 #include "system.h"
@@ -470,7 +472,28 @@ void convert_boundary(const NumericLevel& N, const BoundarySymbolic& sym, const 
 
 }  // namespace
 
+// The numeric set-up's scratch comes from the device's default memory pool;
+// freed blocks stay in the pool (no release threshold), so that the next
+// update reuses them instead of mapping new memory.
+static void keep_pool_memory() {
+  static std::atomic<int> slots[dev::kMaxDevices];
+  static const bool init = [] {
+    for (auto& a : slots) a.store(dev::kUnset);
+    return true;
+  }();
+  (void)init;
+  dev::per_device_once(slots, [] {
+    int d = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&d) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, d) != cudaSuccess) return 1;
+    uint64_t keep = ~0ULL;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    return 1;
+  });
+}
+
 bool NumericPlan::fill_level(int l, LevelValues<float>* f32, LevelValues<double>* f64, cudaStream_t s, std::string& err) {
+  keep_pool_memory();
   const NumericLevel& N = levels[l];
   Scratch S(s);
   int* bad = S.get<int>(1);

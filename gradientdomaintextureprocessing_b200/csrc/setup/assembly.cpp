@@ -46,7 +46,9 @@ void build_assembly_work(const Hierarchy& h, const BoundaryElements& be, const C
   w.triMetric.resize(4 * size_t(w.numTriangles));
   w.triMetricInv.resize(4 * size_t(w.numTriangles));
   w.triScale.resize(w.numTriangles);
-  for (size_t c = 0; c < A.charts.size(); c++) {
+  const int nCharts = (int)A.charts.size();
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < nCharts; c++) {
     const AtlasChart& ac = A.charts[c];
     const GridChart& gc = L.charts[c];
     for (size_t t = 0; t < ac.triangles.size(); t++) {
@@ -70,7 +72,8 @@ void build_assembly_work(const Hierarchy& h, const BoundaryElements& be, const C
   w.numInteriorCells = icBase.back();
   w.cellIJ.resize(2 * size_t(w.numInteriorCells));
   w.cellChart.resize(w.numInteriorCells);
-  for (size_t c = 0; c < L.charts.size(); c++) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < nCharts; c++) {
     const GridChart& gc = L.charts[c];
     for (int j = 0; j < gc.height - 1; j++)
       for (int i = 0; i < gc.width - 1; i++) {
@@ -109,9 +112,13 @@ void build_assembly_work(const Hierarchy& h, const BoundaryElements& be, const C
     }
     cellFirstBt[c][be.charts[c].cellTriangles.size()] = b;
   }
-  // (cell or boundary triangle, chart triangle) pairs in chart-triangle order, bucketed
-  std::vector<std::pair<int, int>> icPairs, btPairs;
-  for (size_t c = 0; c < L.charts.size(); c++) {
+  // (cell or boundary triangle, chart triangle) pairs, bucketed by cell and
+  // boundary triangle in chart-triangle order.  A chart's pairs only touch its
+  // own cells and boundary triangles, so the charts count and fill in parallel:
+  // count, prefix sums, fill.
+  w.cellPtr.assign(size_t(w.numInteriorCells) + 1, 0);
+  w.btPtr.assign(size_t(w.numBoundaryTriangles) + 1, 0);
+  auto visit_pairs = [&](int c, auto&& onCell, auto&& onBt) {
     const AtlasChart& ac = A.charts[c];
     const GridChart& gc = L.charts[c];
     for (size_t t = 0; t < ac.triangles.size(); t++) {
@@ -119,31 +126,36 @@ void build_assembly_work(const Hierarchy& h, const BoundaryElements& be, const C
       for (int k = 0; k < 3; k++) p[k] = ac.vertices[ac.triangles[t][k]] - gc.corner;
       int mn[2], mx[2];
       bbox_cells(p, gc.cellSizeW, gc.cellSizeH, mn, mx);
+      const int tri = triBase[c] + (int)t;
       for (int j = mn[1]; j < mx[1]; j++)
         for (int i = mn[0]; i < mx[0]; i++) {
           int ic = gc.localInteriorCell[gc.cat(i, j)];
-          if (ic >= 0) { icPairs.push_back({icBase[c] + ic, triBase[c] + (int)t}); continue; }
+          if (ic >= 0) { onCell(icBase[c] + ic, tri); continue; }
           int bc = gc.localBoundaryCell[gc.cat(i, j)];
           if (bc >= 0)
-            for (int b = cellFirstBt[c][bc]; b < cellFirstBt[c][bc + 1]; b++) btPairs.push_back({b, triBase[c] + (int)t});
+            for (int b = cellFirstBt[c][bc]; b < cellFirstBt[c][bc + 1]; b++) onBt(b, tri);
         }
     }
-  }
-  auto bucket = [](int n, const std::vector<std::pair<int, int>>& pairs, std::vector<int>& ptr, std::vector<int>& idx) {
-    ptr.assign(n + 1, 0);
-    for (auto& p : pairs) ptr[p.first + 1]++;
-    for (int i = 0; i < n; i++) ptr[i + 1] += ptr[i];
-    idx.resize(pairs.size());
-    std::vector<int> fill(ptr.begin(), ptr.end() - 1);
-    for (auto& p : pairs) idx[fill[p.first]++] = p.second;  // stable: chart-triangle order kept
   };
-  bucket(w.numInteriorCells, icPairs, w.cellPtr, w.cellTri);
-  bucket(w.numBoundaryTriangles, btPairs, w.btPtr, w.btTri);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < nCharts; c++)
+    visit_pairs(c, [&](int cell, int) { w.cellPtr[size_t(cell) + 1]++; }, [&](int b, int) { w.btPtr[size_t(b) + 1]++; });
+  for (int i = 0; i < w.numInteriorCells; i++) w.cellPtr[i + 1] += w.cellPtr[i];
+  for (int i = 0; i < w.numBoundaryTriangles; i++) w.btPtr[i + 1] += w.btPtr[i];
+  w.cellTri.resize(w.cellPtr.back());
+  w.btTri.resize(w.btPtr.back());
+  {
+    std::vector<int> cellFill(w.cellPtr.begin(), w.cellPtr.end() - 1), btFill(w.btPtr.begin(), w.btPtr.end() - 1);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < nCharts; c++)
+      visit_pairs(c, [&](int cell, int tri) { w.cellTri[cellFill[cell]++] = tri; }, [&](int b, int tri) { w.btTri[btFill[b]++] = tri; });
+  }
 
   // deep texels: the four surrounding interior cells (raster order) and the
   // texel's corner slot in each
   w.deepCells.resize(4 * size_t(L.numDeep));
-  for (size_t c = 0; c < L.charts.size(); c++) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < nCharts; c++) {
     const GridChart& gc = L.charts[c];
     for (int j = 0; j < gc.height; j++)
       for (int i = 0; i < gc.width; i++) {
@@ -154,13 +166,17 @@ void build_assembly_work(const Hierarchy& h, const BoundaryElements& be, const C
       }
   }
   // interior cells touching a boundary texel (their boundary rows are built on the host)
+  std::vector<char> adjacent(w.numInteriorCells, 0);
+#pragma omp parallel for schedule(static)
   for (int ic = 0; ic < w.numInteriorCells; ic++) {
     const GridChart& gc = L.charts[w.cellChart[ic]];
     int i = w.cellIJ[2 * ic], j = w.cellIJ[2 * ic + 1];
     int q[4] = {gc.at(i, j), gc.at(i + 1, j), gc.at(i + 1, j + 1), gc.at(i, j + 1)};
     for (int k = 0; k < 4; k++)
-      if (gc.nodeType[q[k]] != 2) { w.boundaryAdjacentCells.push_back(ic); break; }
+      if (gc.nodeType[q[k]] != 2) { adjacent[ic] = 1; break; }
   }
+  for (int ic = 0; ic < w.numInteriorCells; ic++)
+    if (adjacent[ic]) w.boundaryAdjacentCells.push_back(ic);
 }
 
 // Deep coefficient of texel slot k (corner of a cell) toward neighbour slot l.

@@ -483,7 +483,8 @@ bool build_boundary_elements(const Hierarchy& H, BoundaryElements& be, std::stri
       }
     }
   }
-  std::unordered_map<uint64_t, int> midOf;
+  // mid-edge node of edge (a, b), a < b: chained per a, numbered in first-seen order
+  std::vector<int> midHead(size_t(firstMid), -1), midNext, midTo;
   int nextMid = 0;
   for (int c = 0; c < nCharts; c++) {
     const GridChart& g = L.charts[c];
@@ -517,10 +518,15 @@ bool build_boundary_elements(const Hierarchy& H, BoundaryElements& be, std::stri
           for (int v = 0; v < 3; v++) {
             int a = bt.idx[(v + 1) % 3], b = bt.idx[(v + 2) % 3];
             if (a > b) std::swap(a, b);
-            auto it = midOf.find(pair_key(uint32_t(a), uint32_t(b)));
-            int mid;
-            if (it == midOf.end()) { mid = nextMid++; midOf.emplace(pair_key(uint32_t(a), uint32_t(b)), mid); }
-            else mid = it->second;
+            if (a < 0 || a >= firstMid) { err = "boundary triangle vertex out of range"; return false; }
+            int mid = midHead[a];
+            while (mid != -1 && midTo[mid] != b) mid = midNext[mid];
+            if (mid == -1) {
+              mid = nextMid++;
+              midTo.push_back(b);
+              midNext.push_back(midHead[a]);
+              midHead[a] = mid;
+            }
             bt.idx[3 + v] = mid + firstMid;
             cb.aux.push_back({(bt.v[(v + 1) % 3] + bt.v[(v + 2) % 3]) / 2.0, mid + firstMid});
           }
@@ -549,8 +555,13 @@ bool build_boundary_elements(const Hierarchy& H, BoundaryElements& be, std::stri
   std::vector<int> degree(numAux, 0);
   for (const ChartBoundary& cb : be.charts)
     for (const AuxNode& a : cb.aux) degree[a.index - numInterior]++;
+  // auxiliary-node rows, charts in parallel, concatenated in chart order
+  std::vector<std::vector<Triplet>> auxTrip(nCharts);
+  std::vector<std::string> auxErr(nCharts);
+#pragma omp parallel for schedule(dynamic, 1)
   for (int c = 0; c < nCharts; c++) {
     const GridChart& g = L.charts[c];
+    auto aux_rows = [&](std::vector<Triplet>& trip, std::string& err) -> bool {
     for (const AuxNode& a : be.charts[c].aux) {
       int fid = be.fineBoundaryIndex[a.index];
       int deg = degree[a.index - numInterior];
@@ -574,6 +585,13 @@ bool build_boundary_elements(const Hierarchy& H, BoundaryElements& be, std::stri
         trip.push_back({fid, bidx, tw});
       }
     }
+      return true;
+    };
+    aux_rows(auxTrip[c], auxErr[c]);
+  }
+  for (int c = 0; c < nCharts; c++) {
+    if (!auxErr[c].empty()) { err = auxErr[c]; return false; }
+    trip.insert(trip.end(), auxTrip[c].begin(), auxTrip[c].end());
   }
   be.prolongation = csr_from_triplets(be.numFineBoundary, L.numBoundary, trip);
   return true;

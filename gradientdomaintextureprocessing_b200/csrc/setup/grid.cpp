@@ -150,15 +150,28 @@ static bool classify_chart(const AtlasChart& ac, GridChart& g, int deepRadius, s
   return true;
 }
 
-// (4)-(5): global enumeration of one chart's texels and cells, in chart order
-static bool enumerate_chart(int chartId, GridChart& g, GridLevel& L, std::string& err) {
+// Texel and cell counts of one chart (its nodeType / cellType images).
+struct ChartCounts { int texels = 0, interior = 0, boundary = 0, deep = 0, cells = 0; };
+static ChartCounts count_chart(const GridChart& g) {
+  ChartCounts k;
+  for (int t : g.nodeType) {
+    if (t != -1) k.texels++;
+    if (t >= 1) k.interior++;
+    if (t == 0 || t == 1) k.boundary++;
+    if (t == 2) k.deep++;
+  }
+  for (int c : g.cellType)
+    if (c != -1) k.cells++;
+  return k;
+}
+
+// (4)-(5): global enumeration of one chart's texels and cells from its offsets
+// (the counts of the charts before it): texels, cells, their nodes and raster
+// lines in raster order.  Charts enumerate in parallel; L.nodes is presized.
+static bool enumerate_chart(int chartId, GridChart& g, GridLevel& L, std::vector<Line>& lines, std::string& err) {
   const int W = g.width, H = g.height;
   // (4) enumeration
-  g.texelOffset = L.numTexels;
-  g.interiorTexelOffset = L.numInteriorTexels;
-  g.cellOffset = L.numCells;
-  g.deepOffset = L.numDeep;
-  g.boundaryOffset = L.numBoundary;
+  int nTex = g.texelOffset, nInt = g.interiorTexelOffset, nBnd = g.boundaryOffset, nDeep = g.deepOffset;
   g.texel.assign(size_t(W) * H, -1);
   g.interiorTexel.assign(size_t(W) * H, -1);
   g.deepTexel.assign(size_t(W) * H, -1);
@@ -166,10 +179,10 @@ static bool enumerate_chart(int chartId, GridChart& g, GridLevel& L, std::string
   for (int j = 0; j < H; j++)
     for (int i = 0; i < W; i++) {
       int n = g.at(i, j), t = g.nodeType[n];
-      if (t != -1) { g.texel[n] = L.numTexels++; L.nodes.push_back({chartId, i, j, t}); }
-      if (t >= 1) g.interiorTexel[n] = L.numInteriorTexels++;
-      if (t == 0 || t == 1) g.boundaryTexel[n] = L.numBoundary++;
-      if (t == 2) g.deepTexel[n] = L.numDeep++;
+      if (t != -1) { L.nodes[nTex] = {chartId, i, j, t}; g.texel[n] = nTex++; }
+      if (t >= 1) g.interiorTexel[n] = nInt++;
+      if (t == 0 || t == 1) g.boundaryTexel[n] = nBnd++;
+      if (t == 2) g.deepTexel[n] = nDeep++;
     }
   g.localCell.assign(size_t(W - 1) * (H - 1), -1);
   g.localInteriorCell.assign(size_t(W - 1) * (H - 1), -1);
@@ -192,9 +205,6 @@ static bool enumerate_chart(int chartId, GridChart& g, GridLevel& L, std::string
         g.interiorCellCorners.insert(g.interiorCellCorners.end(), q, q + 4);
       }
     }
-  L.numCells += nCell;
-  L.numBoundaryCells += g.numBoundaryCells;
-  L.numInteriorCells += g.numInteriorCells;
 
   // (5) raster lines: maximal runs of deep texels per row
   for (int j = 0; j < H; j++) {
@@ -207,7 +217,7 @@ static bool enumerate_chart(int chartId, GridChart& g, GridLevel& L, std::string
         Line l{g.texel[g.at(start, j)], g.texel[g.at(i - 1, j)], g.texel[g.at(start, j - 1)], g.texel[g.at(start, j + 1)],
                g.deepTexel[g.at(start, j)]};
         if (l.start < 0 || l.end < 0 || l.prev < 0 || l.next < 0) { err = "invalid raster line"; return false; }
-        L.rasterLines.push_back(l);
+        lines.push_back(l);
       }
       prevDeep = deep;
     }
@@ -244,9 +254,34 @@ static bool build_level(const Atlas& A, int level, int width, int height, const 
     g.gridIndexOffset = 2 * approx * approx * int(c);
     classify_chart(ac, g, info.boundaryDilation + 1, chartErr[c]);
   }
+  for (int c = 0; c < nCharts; c++)
+    if (!chartErr[c].empty()) { err = chartErr[c]; return false; }
+  // offsets of every chart from the counts of the charts before it
+  std::vector<ChartCounts> counts(nCharts);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < nCharts; c++) counts[c] = count_chart(L.charts[c]);
+  for (int c = 0; c < nCharts; c++) {
+    GridChart& g = L.charts[c];
+    g.texelOffset = L.numTexels;
+    g.interiorTexelOffset = L.numInteriorTexels;
+    g.cellOffset = L.numCells;
+    g.deepOffset = L.numDeep;
+    g.boundaryOffset = L.numBoundary;
+    L.numTexels += counts[c].texels;
+    L.numInteriorTexels += counts[c].interior;
+    L.numBoundary += counts[c].boundary;
+    L.numDeep += counts[c].deep;
+    L.numCells += counts[c].cells;
+  }
+  L.nodes.resize(L.numTexels);
+  std::vector<std::vector<Line>> lines(nCharts);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < nCharts; c++) enumerate_chart(c, L.charts[c], L, lines[c], chartErr[c]);
   for (int c = 0; c < nCharts; c++) {
     if (!chartErr[c].empty()) { err = chartErr[c]; return false; }
-    if (!enumerate_chart(c, L.charts[c], L, err)) return false;
+    L.numBoundaryCells += L.charts[c].numBoundaryCells;
+    L.numInteriorCells += L.charts[c].numInteriorCells;
+    L.rasterLines.insert(L.rasterLines.end(), lines[c].begin(), lines[c].end());
   }
   if (L.numTexels != L.numBoundary + L.numDeep) { err = "boundary and deep texels do not partition the texels"; return false; }
   L.boundaryAndDeep.assign(L.numTexels, 0);

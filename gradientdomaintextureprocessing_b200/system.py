@@ -241,5 +241,11 @@ def texture_filtering_rhs(system: System, f: np.ndarray, stiffness: float, sharp
 
 def texel_signal(hierarchy: Hierarchy, texture: np.ndarray) -> np.ndarray:
     """Texture value of every active texel, in texel order (TextureFiltering.cpp:603-608)."""
-    tn = hierarchy.array("textureNodes")
-    return np.ascontiguousarray(texture[tn[:, 1], tn[:, 0]], dtype=np.float64)
+    tex = texture if texture.dtype in (np.float32, np.float64) else texture.astype(np.float64)
+    height, width = tex.shape[:2]
+    channels = 1 if tex.ndim == 2 else int(tex.shape[2])
+    strides = (tex.strides[0], tex.strides[1], tex.strides[2] if tex.ndim == 3 else 0)
+    out = np.empty((hierarchy.counts(0)["numTexels"], channels), dtype=np.float64)
+    _lib.check(_lib.lib().gdtp_texel_signal(hierarchy.handle, C.c_void_p(tex.ctypes.data), int(width), int(height), channels,
+                                            tex.itemsize, *strides, _lib.ptr(out)))
+    return out if tex.ndim == 3 else out[:, 0]

@@ -74,6 +74,14 @@ int gdtp_hierarchy_counts(const gdtp_hierarchy* h, int level, int64_t* counts);
  *   "boundaryNodes"(4: boundaryNodes, midPoints, fineNodes, fineBoundaryNodes) level 0
  *   "boundaryProlongation.ptr/.col/.val(float64)" level 0 (coarseBoundaryFineBoundaryProlongation) */
 int gdtp_hierarchy_array(const gdtp_hierarchy* h, const char* name, int level, void* out, int64_t* count);
+/* The texture value of every level-0 texel, in texel order: out[t * channels
+ * + c] = the texture's channel c at the texel's pixel (x, y)
+ * (TextureFiltering.cpp:603-608).  texture: height x width x channels values,
+ * float32 (bytes_per_value 4) or float64 (8), at byte offset y * row_stride +
+ * x * pixel_stride + c * channel_stride (any layout, no copy); out: float64
+ * numTexels * channels.  GDTP_ERR_INVALID when a texel lies outside the image. */
+int gdtp_texel_signal(const gdtp_hierarchy* h, const void* texture, int width, int height, int channels, int bytes_per_value,
+                      int64_t row_stride, int64_t pixel_stride, int64_t channel_stride, double* out);
 
 /* ---------------------------------------------------------------------------
  * Metrics (host).  Per mesh triangle parameter metric (nt*4, the layout of

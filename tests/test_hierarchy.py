@@ -58,3 +58,26 @@ def test_texture_nodes_and_boundary_nodes(case):
 def test_extra_levels_reach_dense_coarse_size(case):
     _, h, levels = case
     assert h.counts(h.levels - 1)["numTexels"] <= 2600 or h.levels == 12
+
+
+def test_texel_signal_samples_every_layout(case):
+    """gdtp_texel_signal reads the texel's pixel (textureNodes' x, y) from any
+    strided float32 / float64 image, equal to the gather by the reference's
+    texture nodes (TextureFiltering.cpp:603-608)."""
+    from gradientdomaintextureprocessing_b200.system import texel_signal
+    g, h, _ = case
+    tn = g["fine/textureNodes"]
+    w = int(tn[:, 0].max()) + 2
+    hgt = int(tn[:, 1].max()) + 3
+    rng = np.random.default_rng(0)
+    img = rng.random((hgt, w, 3)).astype(np.float32)
+    want = img[tn[:, 1], tn[:, 0]].astype(np.float64)
+    np.testing.assert_array_equal(texel_signal(h, img), want)
+    np.testing.assert_array_equal(texel_signal(h, img.astype(np.float64)), want)
+    # channel-planar storage seen as height x width x channels, and a single channel
+    planar = np.ascontiguousarray(img.transpose(2, 0, 1)).transpose(1, 2, 0)
+    assert not planar.flags["C_CONTIGUOUS"]
+    np.testing.assert_array_equal(texel_signal(h, planar), want)
+    np.testing.assert_array_equal(texel_signal(h, img[:, :, 1]), want[:, 1])
+    with pytest.raises(Exception):
+        texel_signal(h, img[: int(tn[:, 1].max()), :, :])
