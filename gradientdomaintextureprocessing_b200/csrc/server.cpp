@@ -46,17 +46,18 @@ int Server::add_model(const Mesh& mesh, int width, int height, int levels, int k
   if (!build_hierarchy(m->mesh, width, height, levels, BlockInfo(), *m->h, 2600, 12)) { err = "hierarchy: " + m->h->error; return -1; }
   if (!build_boundary_elements(*m->h, *m->be, err)) { err = "boundary elements: " + err; return -1; }
   // device bytes before the first build, corrected by the measured size once
-  // built: FP64 operators, FP32 multigrid with up to 4 right-hand sides and
-  // coarse factor per texel, dense boundary-block inverses per boundary texel
-  // (subdomains of up to 384), fixed allocations; the geodesic kind holds two
-  // systems and its integration samples.  Fitted to measured sizes (torus,
-  // icosphere, genus-2 from 256^2 to 2048^2) with 5-30 % headroom.
-  double sys = 450.0 * m->h->levels[0].numTexels + 4000.0 * m->h->levels[0].numBoundary + double(24 << 20);
+  // built: FP64 operators, resident M and S of every level for the numeric
+  // set-up, FP32 multigrid with up to 4 right-hand sides and coarse factor per
+  // texel, dense boundary-block inverses and their value maps per boundary
+  // texel (subdomains of up to 384), fixed allocations; the geodesic kind holds
+  // two systems and its integration samples.  Fitted to measured sizes (torus,
+  // icosphere, genus-2 from 256^2 to 2048^2): 3-77 % headroom.
+  double sys = 700.0 * m->h->levels[0].numTexels + 5500.0 * m->h->levels[0].numBoundary + double(48 << 20);
   // boundary blocks small enough to be inverted whole hold a dense FP32 inverse
   const int denseMax = SolverKnobs().denseBoundaryMax;
   for (const GridLevel& g : m->h->levels)
     if (g.numBoundary <= denseMax) sys += 4.0 * double(g.numBoundary) * g.numBoundary;
-  m->estimate = int64_t(kind == kKindGeodesic ? 1.8 * sys : sys);
+  m->estimate = int64_t(kind == kKindGeodesic ? 1.75 * sys : sys);
   std::lock_guard<std::mutex> lk(mu_);
   const int id = (int)models_.size();
   m->id = id;
