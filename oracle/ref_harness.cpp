@@ -245,6 +245,10 @@ int main(int argc, char** argv) {
   }
   double tAssembly = secs(T1);
   if (brush) {
+#if USE_FLOAT  // the brush's cell matrices are FP64 (SparseMatrix<double>); the FP32 build has no brush mode
+    fprintf(stderr, "brush mode needs the FP64 build (gdtp_ref)\n");
+    return 2;
+#else
     // CellStiffnessToTexelStiffness (IterativeSolvers.inl:1170-1208) for a seeded
     // cell mask m_c = ((c * 2654435761) mod 2^32 mod 1000) / 1000, in FP64 (Vec4d),
     // the texel-to-cell coefficients converted as the app does (TextureFiltering.cpp:641-642)
@@ -285,6 +289,7 @@ int main(int argc, char** argv) {
     out.i32("L0/counts", {fine.numTexels, fine.numDeepTexels, (int)fine.boundaryGlobalIndex.size(), fine.numCells});
     fprintf(stderr, "ok: brush, %d texels, %d cells\n", fine.numTexels, fine.numCells);
     return 0;
+#endif
   }
 
   // ---------------- system ---------------------------------------------------------------

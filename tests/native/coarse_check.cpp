@@ -1,7 +1,10 @@
 // The coarsest level's direct solve set-up on given coefficients: the full
 // operator assembled by full_matrix (csrc/setup/galerkin.cpp) and its
-// Jacobi-scaled dense inverse (dense_spd_inverse, csrc/setup/bsolve.cpp), as the
-// solver builds them, applied to a right-hand side on the host.
+// Jacobi-scaled dense inverse (dense_spd_inverse, csrc/setup/bsolve.cpp),
+// applied to a right-hand side on the host.  The Jacobi scaling and the apply
+// loop are restated here (the solver's own versions run on the device: the
+// host build in system.cu, or the numeric set-up of numeric.cu, and
+// k_coarse_solve); what this check pins is full_matrix and the dense inverse.
 //
 //   coarse_check <mesh.gdm> <levels> <in.bin> <out.bin>
 //
