@@ -141,7 +141,7 @@ def build_models(server: Server, stream, lic_ratio: float = 1e3, warm: bool = Tr
     return models
 
 
-def run_stream(server: Server, stream, models: dict, tol: float = 1e-6, seed: int = 1, max_iters: int = 500):
+def run_stream(server: Server, stream, models: dict, tol: float = 1e-6, seed: int = 1, max_iters: int = 1000):
     """Submits every request at its arrival time (wall clock), waits for all;
     returns per-request results and the server's statistics."""
     rng = np.random.default_rng(seed)
