@@ -191,28 +191,6 @@ __global__ void k_coarse_fill(long long nD, int n, const long long* __restrict__
   dense[(long long)r * n + c] = __dmul_rn(__dmul_rn(v(src[e]), scale[r]), scale[c]);
 }
 
-// stream-ordered scratch
-struct Scratch {
-  std::vector<void*> ptrs;
-  cudaStream_t s;
-  cudaError_t last = cudaSuccess;
-  explicit Scratch(cudaStream_t stream) : s(stream) {}
-  ~Scratch() {
-    for (void* p : ptrs) cudaFreeAsync(p, s);
-  }
-  template <class T>
-  T* get(size_t n) {
-    void* p = nullptr;
-    cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(16, n * sizeof(T)), s);
-    if (e != cudaSuccess) {
-      last = e;
-      return nullptr;
-    }
-    ptrs.push_back(p);
-    return static_cast<T*>(p);
-  }
-};
-
 template <class T>
 std::vector<int> as_int(const std::vector<T>& v) {
   std::vector<int> out(v.size());
@@ -472,10 +450,7 @@ void convert_boundary(const NumericLevel& N, const BoundarySymbolic& sym, const 
 
 }  // namespace
 
-// The numeric set-up's scratch comes from the device's default memory pool;
-// freed blocks stay in the pool (no release threshold), so that the next
-// update reuses them instead of mapping new memory.
-static void keep_pool_memory() {
+void keep_pool_memory() {
   static std::atomic<int> slots[dev::kMaxDevices];
   static const bool init = [] {
     for (auto& a : slots) a.store(dev::kUnset);
@@ -493,9 +468,8 @@ static void keep_pool_memory() {
 }
 
 bool NumericPlan::fill_level(int l, LevelValues<float>* f32, LevelValues<double>* f64, cudaStream_t s, std::string& err) {
-  keep_pool_memory();
   const NumericLevel& N = levels[l];
-  Scratch S(s);
+  StreamScratch S(s);
   int* bad = S.get<int>(1);
   if (!bad) {
     err = std::string("numeric scratch: ") + cudaGetErrorString(S.last);

@@ -77,6 +77,48 @@ struct LevelValues {
   double *coarseInv = nullptr, *coarseScale = nullptr;
 };
 
+// Set-up scratch comes from the device's default memory pool, stream-ordered;
+// freed blocks stay in the pool (no release threshold), so that the next
+// set-up or update reuses them instead of mapping new memory.  Called once per
+// device before the first StreamScratch.
+void keep_pool_memory();
+
+// Stream-ordered scratch buffers of one set-up step, released (to the pool) on
+// destruction; `last` holds the first allocation or copy error.
+struct StreamScratch {
+  std::vector<void*> ptrs;
+  cudaStream_t s;
+  cudaError_t last = cudaSuccess;
+  explicit StreamScratch(cudaStream_t stream) : s(stream) { keep_pool_memory(); }
+  StreamScratch(const StreamScratch&) = delete;
+  StreamScratch& operator=(const StreamScratch&) = delete;
+  ~StreamScratch() {
+    for (void* p : ptrs) cudaFreeAsync(p, s);
+  }
+  template <class T>
+  T* get(size_t n) {
+    void* p = nullptr;
+    size_t bytes = (n ? n : 1) * sizeof(T);
+    if (bytes < 16) bytes = 16;
+    const cudaError_t e = cudaMallocAsync(&p, bytes, s);
+    if (e != cudaSuccess) {
+      if (last == cudaSuccess) last = e;
+      return nullptr;
+    }
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  template <class T>
+  T* upload(const std::vector<T>& v) {
+    T* p = get<T>(v.size());
+    if (p && !v.empty()) {
+      const cudaError_t e = cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess && last == cudaSuccess) last = e;
+    }
+    return p;
+  }
+};
+
 // planes[k][i] = deep[10 texel[i] + k], k < 9 (raw FP64 operator planes in run order)
 void launch_gather_planes(int count, const int* texel, const double* deep, double* planes, cudaStream_t s);
 

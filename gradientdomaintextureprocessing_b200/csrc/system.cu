@@ -354,7 +354,9 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
   AssemblyWork w;
   build_assembly_work(h_, be_, g, w);
   setupMs[8] = now_ms() - tAssembly;
-  DeviceArena A;
+  // temporaries from the stream-ordered pool (every output below is written in
+  // full by its kernel, so nothing is zeroed)
+  StreamScratch A(stream_);
   int* cellPtr = A.upload(w.cellPtr);
   int* cellTri = A.upload(w.cellTri);
   int* cellIJ = A.upload(w.cellIJ);
@@ -369,23 +371,23 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
   int* btPtr = A.upload(w.btPtr);
   int* btTri = A.upload(w.btTri);
   double* btPos = A.upload(w.btPos);
-  double* cm = A.zeros<double>(16 * size_t(w.numInteriorCells));
-  double* cs = A.zeros<double>(16 * size_t(w.numInteriorCells));
+  double* cm = A.get<double>(16 * size_t(w.numInteriorCells));
+  double* cs = A.get<double>(16 * size_t(w.numInteriorCells));
   const int nd = h_.levels[0].numDeep;
   // the level-0 deep coefficients stay resident: the operators' planes and the
   // numeric set-up read them on the device
   deepArena_ = DeviceArena();
-  double* dm = deepArena_.zeros<double>(10 * size_t(nd));
-  double* ds = deepArena_.zeros<double>(10 * size_t(nd));
+  double* dm = static_cast<double*>(deepArena_.alloc(10 * std::max<size_t>(1, size_t(nd)) * sizeof(double)));
+  double* ds = static_cast<double*>(deepArena_.alloc(10 * std::max<size_t>(1, size_t(nd)) * sizeof(double)));
   deepMassDev_ = dm;
   deepStiffDev_ = ds;
   if (!check(deepArena_.last, "deep coefficients")) return false;
   const size_t na = w.boundaryAdjacentCells.size();
-  double* am = A.zeros<double>(16 * na);
-  double* as = A.zeros<double>(16 * na);
-  double* bm = A.zeros<double>(36 * size_t(w.numBoundaryTriangles));
-  double* bs = A.zeros<double>(36 * size_t(w.numBoundaryTriangles));
-  if (!check(A.last, "assembly upload")) return false;
+  double* am = A.get<double>(16 * na);
+  double* as = A.get<double>(16 * na);
+  double* bm = A.get<double>(36 * size_t(w.numBoundaryTriangles));
+  double* bs = A.get<double>(36 * size_t(w.numBoundaryTriangles));
+  if (!check(A.last, "assembly buffers")) return false;
   dev::launch_interior_cells(w.numInteriorCells, cellPtr, cellTri, cellIJ, cellChart, cellSize, triPos, triInv, triScale, cm, cs,
                              stream_);
   dev::launch_deep_gather(nd, deepCells, cm, cs, dm, ds, stream_);
@@ -397,16 +399,27 @@ bool DeviceSystem::assemble(const Mesh& mesh, const double* parameterMetric) {
   fine_.deepMass.resize(10 * size_t(nd));
   fine_.deepStiffness.resize(10 * size_t(nd));
   std::vector<double> ham(16 * na), has(16 * na), hbm(36 * size_t(w.numBoundaryTriangles)), hbs(hbm.size());
-  bool ok = check(cudaMemcpyAsync(fine_.deepMass.data(), dm, fine_.deepMass.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
-            check(cudaMemcpyAsync(fine_.deepStiffness.data(), ds, fine_.deepStiffness.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
-            check(cudaMemcpyAsync(ham.data(), am, ham.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
+  bool ok = check(cudaMemcpyAsync(ham.data(), am, ham.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
             check(cudaMemcpyAsync(has.data(), as, has.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
             check(cudaMemcpyAsync(hbm.data(), bm, hbm.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
             check(cudaMemcpyAsync(hbs.data(), bs, hbs.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h") &&
             check(cudaStreamSynchronize(stream_), "assembly");
   if (!ok) return false;
   setupMs[9] = now_ms() - tAssembly - setupMs[8];
-  if (!assemble_boundary_blocks(h_, be_, w, ham, has, hbm, hbs, fine_, err_)) return false;
+  // the host copies of the deep coefficients (read by the Galerkin coarsening)
+  // come down on a helper thread while this one builds the boundary blocks
+  cudaError_t deepCopy = cudaSuccess;
+  std::thread deepDown([&] {
+    deepCopy = cudaSetDevice(device_);
+    if (deepCopy == cudaSuccess)
+      deepCopy = cudaMemcpyAsync(fine_.deepMass.data(), dm, fine_.deepMass.size() * 8, cudaMemcpyDeviceToHost, stream_);
+    if (deepCopy == cudaSuccess)
+      deepCopy = cudaMemcpyAsync(fine_.deepStiffness.data(), ds, fine_.deepStiffness.size() * 8, cudaMemcpyDeviceToHost, stream_);
+    if (deepCopy == cudaSuccess) deepCopy = cudaStreamSynchronize(stream_);
+  });
+  const bool blocks = assemble_boundary_blocks(h_, be_, w, ham, has, hbm, hbs, fine_, err_);
+  deepDown.join();
+  if (!blocks || !check(deepCopy, "deep coefficients d2h")) return false;
   setupMs[10] = now_ms() - tAssembly - setupMs[8] - setupMs[9];
 
   // raw FP64 operators of M and S on level 0 (deep planes in line-run order)
