@@ -2,12 +2,15 @@
 // host: x = BB^-1 r through the subdomain inverses, the separator's Schur
 // complement and the back substitution, the same sequence as the device
 // kernels (k_bs_prep, k_bs_dense, k_bs_back).  The test feeds it boundary blocks
-// of the reference's own operator and checks the residual BB x - r.
+// of the reference's own operator and checks the residual BB x - r.  It also
+// checks that build_boundary_symbolic (the device numeric set-up's layout)
+// gives the host set-up's partition, patterns and scaled couplings.
 //
 //   bsolve_check <in.bin> <out.bin>
 //
 // in.bin: CSR BB (int64 rows, cols, nnz + int32 ptr, int32 col, float64 val),
 // int64 n + n float64 right-hand side.  out.bin: n float64 solution.
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <fstream>
@@ -48,6 +51,23 @@ int main(int argc, char** argv) {
   BoundarySolverSetup bs;
   std::string err;
   if (!build_boundary_solver(BB, BD, 384, 0, bs, err)) { std::fprintf(stderr, "%s\n", err.c_str()); return 3; }
+  // the device numeric set-up lays the solver out from build_boundary_symbolic:
+  // the same partition and patterns, and values made from the recorded entries
+  // (scaled BB entry k of rows i, j: (BB_k s_pos(i)) s_pos(j)) equal to the
+  // host set-up's bit for bit
+  {
+    BoundarySymbolic sym;
+    if (!build_boundary_symbolic(BB, BD, 384, 0, sym, err)) { std::fprintf(stderr, "symbolic: %s\n", err.c_str()); return 3; }
+    auto scaled = [&](int e) { return BB.val[e] * bs.scale[sym.pos[sym.bbRow[e]]] * bs.scale[sym.pos[BB.col[e]]]; };
+    bool same = sym.nb == bs.nb && sym.nSub == bs.nSub && sym.nI == bs.nI && sym.nS == bs.nS && sym.order == bs.order &&
+                sym.subPtr == bs.subPtr && sym.touchPtr == bs.touchPtr && sym.touch == bs.touch && sym.wOff == bs.wOff &&
+                sym.invOff == bs.invOff && sym.AIS.ptr == bs.AIS.ptr && sym.AIS.col == bs.AIS.col && sym.ASI.ptr == bs.ASI.ptr &&
+                sym.ASI.col == bs.ASI.col && sym.BD.ptr == bs.BD.ptr && sym.BD.col == bs.BD.col;
+    for (size_t k = 0; same && k < sym.AIS.val.size(); k++) same = scaled(int(sym.AIS.val[k])) == bs.AIS.val[k];
+    for (size_t k = 0; same && k < sym.ASI.val.size(); k++) same = scaled(int(sym.ASI.val[k])) == bs.ASI.val[k];
+    for (int k = 0; same && k < bs.nb; k++) same = 1.0 / std::sqrt(BB.val[sym.diagEntry[bs.order[k]]]) == bs.scale[k];
+    if (!same) { std::fprintf(stderr, "symbolic layout differs from the host set-up\n"); return 4; }
+  }
   // scaled right-hand side by position
   std::vector<double> rhat(bs.nb), y(bs.nI, 0.0), xs(bs.nS, 0.0), x(static_cast<size_t>(n), 0.0);
   for (int k = 0; k < bs.nb; k++) rhat[k] = bs.scale[k] * r[bs.order[k]];
