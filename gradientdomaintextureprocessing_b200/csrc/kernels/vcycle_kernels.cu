@@ -23,10 +23,51 @@ namespace dev {
 template <typename T, int W>
 __global__ void __launch_bounds__(256) k_gs_colour(const ColourRun* __restrict__ runs, int nRuns, const T* __restrict__ coef,
                                                    int planeStride, const T* __restrict__ rhs, T* __restrict__ x, int KP, int G,
-                                                   int skip) {
+                                                   int skip, int rhsEarly) {
+  // What the previous launch cannot have written is loaded before waiting for
+  // it, so that these loads overlap its tail: the run and its coefficients
+  // (written at set-up), and the right-hand side when the previous launch is a
+  // colour pass of the same smoothing step (rhsEarly).  x is read after the
+  // wait.  The arithmetic is gs_item's, in the same order.
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int per = 32 * G;
+  const long long r = t / per;
+  const int rem = int(t - r * per);
+  const int m = rem / G, q = rem - m * G;
+  ColourRun R;
+  R.len = 0;
+  if (r < nRuns) R = runs[r];
+  const bool active = r < nRuns && m < R.len;
+  T w[10];
+  Vec<T, W> b;
+  int pos = 0, pp = 0, pn = 0;
+  const int off = q * W;
+  if (active) {
+    pos = R.pos0 + 2 * m, pp = R.prev0 + 2 * m, pn = R.next0 + 2 * m;
+    const T* c = coef + R.coef0 + m;
+#pragma unroll
+    for (int k = 0; k < 9; k++) w[k] = c[k * planeStride];
+    if (rhsEarly) b = vload<T, W>(rhs + (long long)pos * KP + off);
+  }
   grid_dependency_wait();
   grid_launch_dependents();
-  gs_item<T, W, LoadDefault>(runs, nRuns, coef, planeStride, rhs, x, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x, skip);
+  if (!active) return;
+  if (!rhsEarly) b = vload<T, W>(rhs + (long long)pos * KP + off);
+  Vec<T, W> acc;
+#pragma unroll
+  for (int k = 0; k < W; k++) acc.v[k] = 0;
+  if (!(skip & 1)) axpy(acc, w[0], vload<T, W>(x + (long long)(pp - 1) * KP + off));
+  if (!(skip & 2)) axpy(acc, w[1], vload<T, W>(x + (long long)(pp)*KP + off));
+  if (!(skip & 4)) axpy(acc, w[2], vload<T, W>(x + (long long)(pp + 1) * KP + off));
+  if (!(skip & 8)) axpy(acc, w[3], vload<T, W>(x + (long long)(pos - 1) * KP + off));
+  if (!(skip & 32)) axpy(acc, w[5], vload<T, W>(x + (long long)(pos + 1) * KP + off));
+  if (!(skip & 64)) axpy(acc, w[6], vload<T, W>(x + (long long)(pn - 1) * KP + off));
+  if (!(skip & 128)) axpy(acc, w[7], vload<T, W>(x + (long long)(pn)*KP + off));
+  if (!(skip & 256)) axpy(acc, w[8], vload<T, W>(x + (long long)(pn + 1) * KP + off));
+  Vec<T, W> out;
+#pragma unroll
+  for (int k = 0; k < W; k++) out.v[k] = b.v[k] * w[4] - acc.v[k];
+  vstore<T, W>(x + (long long)pos * KP + off, out);
 }
 
 // Every sweep of one smoothing step on one chart per block: the colour passes
@@ -104,19 +145,60 @@ __global__ void __launch_bounds__(kGroupBlockMax, 1) k_gs_groups(const ColourRun
 // Residual: deep rows by runs (all colours), boundary rows by CSR (global cols).
 // Blocks [0, deepBlocks) handle deep texels, the rest boundary rows.
 // ----------------------------------------------------------------------------
-template <typename T, int W, typename LD = LoadDefault>
+template <typename T, int W>
 __global__ void __launch_bounds__(256) k_residual(const ColourRun* __restrict__ runs, int nRuns, const T* __restrict__ coef,
                                                   int planeStride, int deepBlocks, const int* __restrict__ bPtr,
                                                   const int* __restrict__ bCol, const T* __restrict__ bVal,
                                                   const int* __restrict__ bGlobal, int nB, const T* __restrict__ rhs,
-                                                  const T* __restrict__ x, T* __restrict__ res, int KP, int G) {
-  grid_dependency_wait();
-  grid_launch_dependents();
-  if ((int)blockIdx.x < deepBlocks)
-    residual_deep_item<T, W, LD>(runs, nRuns, coef, planeStride, rhs, x, res, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
-  else
+                                                  const T* __restrict__ x, T* __restrict__ res, int KP, int G, int rhsEarly) {
+  if ((int)blockIdx.x >= deepBlocks) {
+    grid_dependency_wait();
+    grid_launch_dependents();
     residual_boundary_item<T, W, LoadDefault>(bPtr, bCol, bVal, bGlobal, nB, rhs, x, res, KP, G,
                                               (long long)(blockIdx.x - deepBlocks) * blockDim.x + threadIdx.x);
+    return;
+  }
+  // deep items (residual_deep_item's arithmetic, same order): the run and its
+  // coefficients (set-up data), and rhs when the previous launch does not
+  // write it (rhsEarly), are loaded before waiting for the previous launch
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int per = 32 * G;
+  const long long r = t / per;
+  const int rem = int(t - r * per);
+  const int m = rem / G, q = rem - m * G;
+  ColourRun R;
+  R.len = 0;
+  if (r < nRuns) R = runs[r];
+  const bool active = r < nRuns && m < R.len;
+  T w[10];
+  Vec<T, W> b;
+  int pos = 0, pp = 0, pn = 0;
+  const int off = q * W;
+  if (active) {
+    pos = R.pos0 + 2 * m, pp = R.prev0 + 2 * m, pn = R.next0 + 2 * m;
+    const T* c = coef + R.coef0 + m;
+#pragma unroll
+    for (int k = 0; k < 10; k++)
+      if (k != 4) w[k] = c[k * planeStride];
+    if (rhsEarly) b = vload<T, W>(rhs + (long long)pos * KP + off);
+  }
+  grid_dependency_wait();
+  grid_launch_dependents();
+  if (!active) return;
+  if (!rhsEarly) b = vload<T, W>(rhs + (long long)pos * KP + off);
+  Vec<T, W> acc = vload<T, W>(x + (long long)pos * KP + off);
+  axpy(acc, w[0], vload<T, W>(x + (long long)(pp - 1) * KP + off));
+  axpy(acc, w[1], vload<T, W>(x + (long long)(pp)*KP + off));
+  axpy(acc, w[2], vload<T, W>(x + (long long)(pp + 1) * KP + off));
+  axpy(acc, w[3], vload<T, W>(x + (long long)(pos - 1) * KP + off));
+  axpy(acc, w[5], vload<T, W>(x + (long long)(pos + 1) * KP + off));
+  axpy(acc, w[6], vload<T, W>(x + (long long)(pn - 1) * KP + off));
+  axpy(acc, w[7], vload<T, W>(x + (long long)(pn)*KP + off));
+  axpy(acc, w[8], vload<T, W>(x + (long long)(pn + 1) * KP + off));
+  Vec<T, W> out;
+#pragma unroll
+  for (int k = 0; k < W; k++) out.v[k] = b.v[k] - acc.v[k] * w[9];
+  vstore<T, W>(res + (long long)pos * KP + off, out);
 }
 
 // ----------------------------------------------------------------------------
@@ -630,10 +712,11 @@ static void launch(void (*kernel)(P...), dim3 grid, cudaStream_t s, A... args) {
 
 template <typename T, int W>
 void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP,
-                      cudaStream_t s, int skip) {
+                      cudaStream_t s, int skip, bool rhsEarly) {
   if (nRuns == 0) return;
   const int G = KP / W;
-  launch(k_gs_colour<T, W>, dim3(nblk((long long)nRuns * 32 * G)), s, runs, nRuns, coef, planeStride, rhs, x, KP, G, skip);
+  launch(k_gs_colour<T, W>, dim3(nblk((long long)nRuns * 32 * G)), s, runs, nRuns, coef, planeStride, rhs, x, KP, G, skip,
+         rhsEarly ? 1 : 0);
 }
 template <typename T, int W>
 size_t gs_groups_smem(const LevelDev<T>& D, int KP) {
@@ -674,11 +757,13 @@ bool launch_gs_groups(const LevelDev<T>& D, int sweeps, bool reverse, int KP, cu
 }
 template <typename T, int W>
 void launch_residual(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const int* bPtr, const int* bCol,
-                     const T* bVal, const int* bGlobal, int nB, const T* rhs, const T* x, T* res, int KP, cudaStream_t s) {
+                     const T* bVal, const int* bGlobal, int nB, const T* rhs, const T* x, T* res, int KP, cudaStream_t s,
+                     bool rhsEarly) {
   const int G = KP / W;
   const int db = nblk((long long)nRuns * 32 * G), bb = nblk((long long)nB * G);
   if (db + bb == 0) return;
-  launch(k_residual<T, W>, dim3(db + bb), s, runs, nRuns, coef, planeStride, db, bPtr, bCol, bVal, bGlobal, nB, rhs, x, res, KP, G);
+  launch(k_residual<T, W>, dim3(db + bb), s, runs, nRuns, coef, planeStride, db, bPtr, bCol, bVal, bGlobal, nB, rhs, x, res, KP, G,
+         rhsEarly ? 1 : 0);
 }
 template <typename T, int W>
 void launch_restrict(const RestrictRun* runs, int nRuns, const int* rPtr, const int* rCol, const T* rVal, const int* rOut,
@@ -804,10 +889,10 @@ void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStre
 }
 
 #define GDTP_INSTANTIATE(T, W)                                                                                             \
-  template void launch_gs_colour<T, W>(const ColourRun*, int, const T*, int, const T*, T*, int, cudaStream_t, int);      \
+  template void launch_gs_colour<T, W>(const ColourRun*, int, const T*, int, const T*, T*, int, cudaStream_t, int, bool); \
   template bool launch_gs_groups<T, W>(const LevelDev<T>&, int, bool, int, cudaStream_t);                                \
   template void launch_residual<T, W>(const ColourRun*, int, const T*, int, const int*, const int*, const T*, const int*, \
-                                      int, const T*, const T*, T*, int, cudaStream_t);                                   \
+                                      int, const T*, const T*, T*, int, cudaStream_t, bool);                             \
   template void launch_restrict<T, W>(const RestrictRun*, int, const int*, const int*, const T*, const int*, int,        \
                                       const T*, T*, T*, long long, int, cudaStream_t);                                   \
   template void launch_prolong_add<T, W>(const ProlongRun*, int, const T*, T*, int, cudaStream_t);                       \

@@ -87,9 +87,11 @@ struct LevelDev {
 };
 
 template <typename T, int W>
-// skip: bit k set = neighbour slot k (3 (dy + 1) + dx + 1) is known to be zero
+// skip: bit k set = neighbour slot k (3 (dy + 1) + dx + 1) is known to be zero;
+// rhsEarly: the previous launch in the stream does not write rhs (a colour pass
+// of the same smoothing step), so rhs is read before waiting for it
 void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP, cudaStream_t s,
-                      int skip = 0);
+                      int skip = 0, bool rhsEarly = false);
 // `sweeps` 4-colour Gauss-Seidel sweeps (colours 0..3, or 3..0 when reverse)
 // in one launch, one block per chart group with the chart's x in shared memory:
 // the same updates in the same order as launch_gs_colour per colour.  False
@@ -128,8 +130,11 @@ struct TileRound {
 };
 bool launch_tile_smooth(const TileRound& round, float* x, int KP, cudaStream_t s);
 template <typename T, int W>
+// rhsEarly: the previous launch in the stream does not write rhs (it only wrote
+// x: smoothing or a boundary solve), so rhs is read before waiting for it
 void launch_residual(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const int* bPtr, const int* bCol,
-                     const T* bVal, const int* bGlobal, int nB, const T* rhs, const T* x, T* res, int KP, cudaStream_t s);
+                     const T* bVal, const int* bGlobal, int nB, const T* rhs, const T* x, T* res, int KP, cudaStream_t s,
+                     bool rhsEarly = false);
 // also clears the coarse iterate coarseX (coarseTexels x KP values)
 template <typename T, int W>
 void launch_restrict(const RestrictRun* runs, int nRuns, const int* rPtr, const int* rCol, const T* rVal, const int* rOut,

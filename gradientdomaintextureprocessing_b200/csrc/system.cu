@@ -1192,9 +1192,11 @@ void DeviceSystem::tile_smooth(Multigrid<T>& mg, LevelDev<T>& D, int sweeps, boo
     for (int p = 0; p < 4; p++) {
       const int c = reverse ? 3 - p : p;
       if (KP % 4 == 0)
-        dev::launch_gs_colour<T, 4>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
+        dev::launch_gs_colour<T, 4>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s, 0,
+                                    p > 0);
       else
-        dev::launch_gs_colour<T, 1>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s);
+        dev::launch_gs_colour<T, 1>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s, 0,
+                                    p > 0);
     }
   }
 }
@@ -1241,7 +1243,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
         const bool fromZero = fromZero0 && sw == 0;
         for (int c = 0; c < 4; c++)
           dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP,
-                                      s, fromZero ? zero_start_skip(c) : 0);
+                                      s, fromZero ? zero_start_skip(c) : 0, sw > 0 || c > 0);
         if (prof && sw == pre_sweeps(l) - 1 && sw >= firstFull) {
           cudaEventRecordWithFlags(profEv_[1], s, cudaEventRecordExternal);
           profSweeps_ = pre_sweeps(l) - firstFull;
@@ -1251,8 +1253,11 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
     // a level entered with a zero iterate and left unsmoothed (no pre-sweeps, no
     // boundary solve) has residual b - A 0 = b exactly: restrict b itself
     const bool unsmoothed = knobs.zeroStartSkip && (l > 0 || zeroStart) && pre_sweeps(l, D, KP) == 0 && !knobs.preBoundary;
+    // after smoothing or a boundary solve (x written) the right-hand side of this
+    // level is not what the previous launch wrote
     if (!unsmoothed)
-      dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s);
+      dev::launch_residual<T, W>(D.runs, D.nRuns, D.coef, D.planeStride, D.bPtr, D.bCol, D.bVal, D.bGlobal, D.nB, D.b, D.x, D.r, KP, s,
+                                 pre_sweeps(l, D, KP) > 0 || knobs.preBoundary);
     dev::launch_restrict<T, W>(D.rruns, D.nRRuns, D.rbPtr, D.rbCol, D.rbVal, D.rbOut, D.nRB, unsmoothed ? D.b : D.r, C.b, C.x, C.n, KP,
                                s);
     trace_mark(l + 1, s);
@@ -1293,7 +1298,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
       for (int sw = 0; sw < post_sweeps(l); sw++)
         for (int c = 3; c >= 0; c--)
           dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP,
-                                      s);
+                                      s, 0, sw > 0 || c < 3);
       if (prof) {
         cudaEventRecordWithFlags(profEv_[3], s, cudaEventRecordExternal);
         profPostSweeps_ = post_sweeps(l);
@@ -1495,10 +1500,10 @@ bool DeviceSystem::relax_host(float* x, const float* rhs, int k, int sweeps, boo
         const int c = reverse ? 3 - p : p;
         if (W == 4)
           dev::launch_gs_colour<float, 4>(D0.runs + D0.runStart[c], D0.runStart[c + 1] - D0.runStart[c], D0.coef, D0.planeStride, D0.b,
-                                          D0.x, mg.KP, stream_);
+                                          D0.x, mg.KP, stream_, 0, sw > 0 || p > 0);
         else
           dev::launch_gs_colour<float, 1>(D0.runs + D0.runStart[c], D0.runStart[c + 1] - D0.runStart[c], D0.coef, D0.planeStride, D0.b,
-                                          D0.x, mg.KP, stream_);
+                                          D0.x, mg.KP, stream_, 0, sw > 0 || p > 0);
       }
   }
   queue_barrier_check(mg, stream_);
