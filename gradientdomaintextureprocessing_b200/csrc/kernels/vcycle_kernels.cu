@@ -210,11 +210,13 @@ __global__ void __launch_bounds__(256) k_restrict(const RestrictRun* __restrict_
                                                   const T* __restrict__ rVal, const int* __restrict__ rOut, int nB,
                                                   const T* __restrict__ res, T* __restrict__ coarseRhs, T* __restrict__ coarseX,
                                                   long long coarseVals, int KP, int G) {
-  grid_dependency_wait();
-  grid_launch_dependents();
-  // the coarse iterate starts from zero: cleared here (grid-stride)
+  // the coarse iterate starts from zero: cleared here (grid-stride), before
+  // waiting for the previous launch (the residual of this level, which does
+  // not touch the coarse level)
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < coarseVals; i += (long long)gridDim.x * blockDim.x)
     coarseX[i] = T(0);
+  grid_dependency_wait();
+  grid_launch_dependents();
   if ((int)blockIdx.x < deepBlocks)
     restrict_deep_item<T, W, LoadDefault>(runs, nRuns, res, coarseRhs, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
   else
@@ -228,9 +230,40 @@ __global__ void __launch_bounds__(256) k_restrict(const RestrictRun* __restrict_
 template <typename T, int W>
 __global__ void __launch_bounds__(256) k_prolong_add(const ProlongRun* __restrict__ runs, int nRuns, const T* __restrict__ coarse,
                                                      T* __restrict__ fine, int KP, int G) {
+  // prolong_item's arithmetic; the run and the fine value (this level's iterate,
+  // which the previous launch, on the coarse level, does not write) are loaded
+  // before waiting for it, the coarse values after
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int per = 32 * G;
+  const long long r = t / per;
+  const int rem = int(t - r * per);
+  const int m = rem / G, q = rem - m * G;
+  ProlongRun R{};
+  if (r < nRuns) R = runs[r];
+  const bool active = r < nRuns && m < R.len;
+  const int off = q * W;
+  T* dst = active ? fine + (long long)(R.f0 + m) * KP + off : nullptr;
+  Vec<T, W> acc;
+  if (active) acc = vload<T, W>(dst);
   grid_dependency_wait();
   grid_launch_dependents();
-  prolong_item<T, W, LoadDefault>(runs, nRuns, coarse, fine, KP, G, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  if (!active) return;
+  const int i = R.i0 + m, o = R.aligned ? 0 : 1;
+  const int p = (i + o) / 2, n = (i + o + 1) / 2;
+  if (R.center >= 0) {
+    const Vec<T, W> a = vload<T, W>(coarse + (long long)(R.center + p) * KP + off),
+                    b = vload<T, W>(coarse + (long long)(R.center + n) * KP + off);
+#pragma unroll
+    for (int k = 0; k < W; k++) acc.v[k] += (a.v[k] + b.v[k]) * T(0.5);
+  } else {
+    const Vec<T, W> a = vload<T, W>(coarse + (long long)(R.prev + p) * KP + off),
+                    b = vload<T, W>(coarse + (long long)(R.prev + n) * KP + off),
+                    c = vload<T, W>(coarse + (long long)(R.next + p) * KP + off),
+                    d = vload<T, W>(coarse + (long long)(R.next + n) * KP + off);
+#pragma unroll
+    for (int k = 0; k < W; k++) acc.v[k] += (a.v[k] + b.v[k] + c.v[k] + d.v[k]) * T(0.25);
+  }
+  vstore<T, W>(dst, acc);
 }
 
 // ----------------------------------------------------------------------------
@@ -373,20 +406,91 @@ __global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode,
 // x_I = s (y - W_p xs[touch_p]) for every interior position (W_p column-major,
 // so a warp reads consecutive rows of one column)
 template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bs_back(BoundaryDev<T> B, T* __restrict__ x, int KP, int G) {
+__global__ void __launch_bounds__(256) k_bs_back(BoundaryDev<T> B, T* __restrict__ x, int KP, int G, int yEarly) {
+  // bs_back_group's arithmetic.  Before waiting for the previous launch (the
+  // separator product, which writes xs): the row's subdomain, its W_p column
+  // range and scale (set-up data), and y when yEarly (then y comes from the
+  // subdomain product, which the previous launch itself waited for)
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gi = t >> 3;
+  const int lane8 = int(t & 7);
+  const long long i = gi / G;
+  const int q = int(gi - i * G), off = q * W;
+  const bool valid = i < B.nI;
+  int m = 0, e0 = 0, e1 = 0;
+  const T* Wp = nullptr;
+  Vec<T, W> yv;
+  T sc = T(0);
+  int g = 0;
+  if (valid) {
+    const int p = B.rowSub[i];
+    const int b0 = B.subPtr[p];
+    m = B.subPtr[p + 1] - b0;
+    Wp = B.wt + B.wOff[p] + (int(i) - b0);
+    e0 = B.touchPtr[p];
+    e1 = B.touchPtr[p + 1];
+    if (lane8 == 0) {
+      if (yEarly) yv = vload<T, W>(B.y + i * KP + off);
+      sc = B.scale[i];
+      g = B.posGlobal[i];
+    }
+  }
   grid_dependency_wait();
   grid_launch_dependents();
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bs_back_group<T, W, LoadDefault>(B, x, KP, G, t >> 3, int(t & 7));
+  if (valid && lane8 == 0 && !yEarly) yv = vload<T, W>(B.y + i * KP + off);
+  Vec<T, W> acc;
+#pragma unroll
+  for (int c = 0; c < W; c++) acc.v[c] = 0;
+  if (valid)
+    for (int e = e0 + lane8; e < e1; e += 8) axpy(acc, Wp[(long long)(e - e0) * m], vload<T, W>(B.xs + (long long)B.touch[e] * KP + off));
+  acc = group8_sum(acc);
+  if (valid && lane8 == 0) {
+#pragma unroll
+    for (int c = 0; c < W; c++) yv.v[c] = (yv.v[c] - acc.v[c]) * sc;
+    vstore<T, W>(x + (long long)g * KP + off, yv);
+  }
 }
 
 // rhat = s (rhs - BD x) for every boundary position, 8 lanes per position
 template <typename T, int W>
-__global__ void __launch_bounds__(256) k_bs_prep(BoundaryDev<T> B, const T* __restrict__ rhs, const T* __restrict__ x, int KP, int G) {
+__global__ void __launch_bounds__(256) k_bs_prep(BoundaryDev<T> B, const T* __restrict__ rhs, const T* __restrict__ x, int KP, int G,
+                                                 int rhsEarly) {
+  // bs_prep_group's arithmetic.  Before waiting for the previous launch: the
+  // row's BD range, position and scale (set-up data), and rhs when the previous
+  // launch does not write it (rhsEarly: the prolongation before a boundary solve
+  // after the coarse correction)
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gi = t >> 3;
+  const int lane8 = int(t & 7);
+  const long long k = gi / G;
+  const int q = int(gi - k * G), off = q * W;
+  const bool valid = k < B.nb;
+  int e0 = 0, e1 = 0, g = 0;
+  T sc = T(0);
+  Vec<T, W> r;
+  if (valid) {
+    e0 = B.bdPtr[k];
+    e1 = B.bdPtr[k + 1];
+    if (lane8 == 0) {
+      g = B.posGlobal[k];
+      sc = B.scale[k];
+      if (rhsEarly) r = vload<T, W>(rhs + (long long)g * KP + off);
+    }
+  }
   grid_dependency_wait();
   grid_launch_dependents();
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bs_prep_group<T, W, LoadDefault>(B, rhs, x, KP, G, t >> 3, int(t & 7));
+  Vec<T, W> acc;
+#pragma unroll
+  for (int c = 0; c < W; c++) acc.v[c] = 0;
+  if (valid)
+    for (int e = e0 + lane8; e < e1; e += 8) axpy(acc, B.bdVal[e], vload<T, W>(x + (long long)B.bdCol[e] * KP + off));
+  acc = group8_sum(acc);
+  if (valid && lane8 == 0) {
+    if (!rhsEarly) r = vload<T, W>(rhs + (long long)g * KP + off);
+#pragma unroll
+    for (int c = 0; c < W; c++) r.v[c] = (r.v[c] - acc.v[c]) * sc;
+    vstore<T, W>(B.rhat + k * KP + off, r);
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -781,13 +885,15 @@ void launch_prolong_add(const ProlongRun* runs, int nRuns, const T* coarse, T* f
   launch(k_prolong_add<T, W>, dim3(nblk((long long)nRuns * 32 * G)), s, runs, nRuns, coarse, fine, KP, G);
 }
 template <typename T, int W>
-void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s) {
+void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s, bool rhsEarly) {
   if (B.nb == 0) return;
   const int G = KP / W;
-  launch(k_bs_prep<T, W>, dim3(nblk((long long)B.nb * G * 8)), s, B, rhs, x, KP, G);
+  launch(k_bs_prep<T, W>, dim3(nblk((long long)B.nb * G * 8)), s, B, rhs, x, KP, G, rhsEarly ? 1 : 0);
   if (B.nSubTasks > 0) launch(k_bs_dense<T, W>, dim3(B.nSubTasks, B.subChunks), s, B, 0, rhs, x, KP, G);
   if (B.nS > 0) launch(k_bs_dense<T, W>, dim3(B.nSchurTasks, B.schurChunks), s, B, 1, rhs, x, KP, G);
-  if (B.nI > 0) launch(k_bs_back<T, W>, dim3(nblk((long long)B.nI * G * 8)), s, B, x, KP, G);
+  // y comes from the subdomain product: read early only when the separator
+  // product sits between the two launches
+  if (B.nI > 0) launch(k_bs_back<T, W>, dim3(nblk((long long)B.nI * G * 8)), s, B, x, KP, G, B.nS > 0 ? 1 : 0);
 }
 template <typename T, int W>
 void launch_coarse_solve(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, cudaStream_t s) {
@@ -896,7 +1002,7 @@ void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStre
   template void launch_restrict<T, W>(const RestrictRun*, int, const int*, const int*, const T*, const int*, int,        \
                                       const T*, T*, T*, long long, int, cudaStream_t);                                   \
   template void launch_prolong_add<T, W>(const ProlongRun*, int, const T*, T*, int, cudaStream_t);                       \
-  template void launch_boundary_solve<T, W>(const BoundaryDev<T>&, const T*, T*, int, cudaStream_t);                     \
+  template void launch_boundary_solve<T, W>(const BoundaryDev<T>&, const T*, T*, int, cudaStream_t, bool);               \
   template void launch_coarse_solve<T, W>(int, const double*, const double*, const T*, T*, int, cudaStream_t);
 GDTP_INSTANTIATE(float, 1)
 GDTP_INSTANTIATE(float, 4)

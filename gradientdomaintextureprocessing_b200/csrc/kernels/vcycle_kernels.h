@@ -142,7 +142,9 @@ void launch_restrict(const RestrictRun* runs, int nRuns, const int* rPtr, const 
 template <typename T, int W>
 void launch_prolong_add(const ProlongRun* runs, int nRuns, const T* coarse, T* fine, int KP, cudaStream_t s);
 template <typename T, int W>
-void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s);
+// rhsEarly: the previous launch in the stream does not write rhs (the
+// prolongation before the solve after the coarse correction)
+void launch_boundary_solve(const BoundaryDev<T>& B, const T* rhs, T* x, int KP, cudaStream_t s, bool rhsEarly = false);
 template <typename T, int W>
 void launch_coarse_solve(int n, const double* ainv, const double* scale, const T* rhs, T* x, int KP, cudaStream_t s);
 

@@ -1285,7 +1285,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
   for (int l = std::min(lc, L - 1) - 1; l >= 0; l--) {
     LevelDev<T>& D = mg.levels[l];
     dev::launch_prolong_add<T, W>(D.pruns, D.nPRuns, mg.levels[l + 1].x, D.x, KP, s);
-    if (knobs.postBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s);
+    if (knobs.postBoundary) dev::launch_boundary_solve<T, W>(D.B, D.b, D.x, KP, s, true);
     if (tiled(D, KP) && knobs.tilePostSweeps > 0) {
       // timed on level 0: the post-smoothing rounds (coefficients, rhs, x read
       // and written once each per round)
