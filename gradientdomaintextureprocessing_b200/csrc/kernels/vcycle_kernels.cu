@@ -288,11 +288,11 @@ __global__ void __launch_bounds__(256) k_prolong_add(const ProlongRun* __restric
 template <typename T, int W>
 __global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode, const T* __restrict__ rhs, T* __restrict__ x, int KP,
                                                   int G) {
-  grid_dependency_wait();
-  grid_launch_dependents();
   __shared__ T red[8][32][4 * W];
   __shared__ Vec<T, W> vin[kBoundaryChunkMax];
   __shared__ int lastFlag;
+  // the block's task, its matrix and its rows of it are set-up data: read (and
+  // the rows prefetched into L2) before waiting for the previous launch
   const int4 task = (mode == 0 ? B.subTasks : B.schurTasks)[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rq = task.y + lane;
   const int r0 = mode == 0 ? B.subPtr[task.x] : 0;
@@ -300,6 +300,15 @@ __global__ void __launch_bounds__(256, 3) k_bs_dense(BoundaryDev<T> B, int mode,
   const T* M = mode == 0 ? B.inv + B.invOff[task.x] : B.sinv;
   const int nch = gridDim.y, chunk = blockIdx.y;
   const int clen = (m + nch - 1) / nch, j0 = min(m, chunk * clen), j1 = min(m, j0 + clen);
+  {
+    // rows j0..j1 of columns 4 task.y .. 4 task.y + 127 (clipped to the padded row)
+    const int c0 = 4 * task.y, cols = max(0, min(mp - c0, 128));
+    if (cols > 0)
+      for (int j = j0 + warp; j < j1; j += 8)
+        if (lane * 32 < cols * (int)sizeof(T)) asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char*>(M + (long long)j * mp + c0) + lane * 32));
+  }
+  grid_dependency_wait();
+  grid_launch_dependents();
   const bool active = 4 * rq < m;
   T* part = mode == 0 ? B.subPart : B.schurPart;
   for (int q = 0; q < G; q++) {
@@ -493,12 +502,26 @@ __global__ void __launch_bounds__(256) k_bs_prep(BoundaryDev<T> B, const T* __re
   }
 }
 
+// L2 prefetch of [p, p + bytes) by the threads of a block (128-byte lines);
+// used for set-up matrices before a kernel waits for the previous launch
+__device__ __forceinline__ void prefetch_l2_block(const void* p, long long bytes) {
+  const char* c = static_cast<const char*>(p);
+  for (long long o = (long long)threadIdx.x * 128; o < bytes; o += (long long)blockDim.x * 128)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c + o));
+}
+
 // ----------------------------------------------------------------------------
 // Coarsest level: x = D Ainv^ D rhs with the scaled dense inverse (FP64).
 // ----------------------------------------------------------------------------
 template <typename T, int W>
 __global__ void __launch_bounds__(256) k_coarse_solve(int n, const double* __restrict__ ainv, const double* __restrict__ scale,
                                                       const T* __restrict__ rhs, T* __restrict__ x, int KP, int G) {
+  // this block's two rows of the inverse (set-up data) start moving into L2
+  // while the previous launch finishes
+  {
+    const int r0 = blockIdx.x * 2;
+    if (r0 < n) prefetch_l2_block(ainv + (long long)r0 * n, (long long)min(2, n - r0) * n * sizeof(double));
+  }
   grid_dependency_wait();
   grid_launch_dependents();
   // 2 rows per block, a warp per part of a row, parts added in order
