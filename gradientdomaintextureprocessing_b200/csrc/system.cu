@@ -519,7 +519,8 @@ bool DeviceSystem::update(double stiffness, double screen) {
   if (use_numeric()) {
     // values on the device from the resident M and S: the multigrids built by
     // this path keep their layout and are refilled in place
-    if (!ensure_plan() || !plan_->combine(screen, stiffness, stream_, err_)) return false;
+    bool built = false;
+    if (!ensure_plan(&built) || (!built && !plan_->combine(screen, stiffness, stream_, err_))) return false;
     if (!refresh_raw_operator()) return false;
     bool keep = sameLevels && (!mg32_.empty() || mg64_);
     if (!mg32_.empty()) keep = keep && mg32_.front()->planGen == plan_->gen;
@@ -602,8 +603,9 @@ const std::vector<LevelCoefficients>& DeviceSystem::coefficients() {
   return coeffs_;
 }
 
-bool DeviceSystem::ensure_plan() {
+bool DeviceSystem::ensure_plan(bool* built) {
   const int L = levelsUsed_;
+  if (built) *built = false;
   if (plan_ && plan_->L == L && plan_->maxBlock == knobs.maxBlock && plan_->denseMax == knobs.denseBoundaryMax) return true;
   // multigrids laid out for an earlier plan keep their own buffers; an update
   // rebuilds them (their generation differs)
@@ -617,6 +619,13 @@ bool DeviceSystem::ensure_plan() {
   }
   setupMs[13] = now_ms() - t0;
   rawFromPlan_ = false;
+  // a knob change rebuilds the plan after the update: its combined values come
+  // from the weights already in force
+  if (!plan_->combine(screen_, stiffness_, stream_, err_)) {
+    plan_.reset();
+    return false;
+  }
+  if (built) *built = true;
   return true;
 }
 

@@ -250,7 +250,9 @@ class DeviceSystem {
   // numeric set-up on the device (numeric.h): used unless device_factor is 0 or
   // the tile smoother is on
   bool use_numeric() const;
-  bool ensure_plan();
+  // the numeric plan for the current level count and boundary layout knobs; a
+  // plan built here is combined for the current weights (*built: it was)
+  bool ensure_plan(bool* built = nullptr);
   bool ensure_host_coefficients();
   bool refresh_raw_operator();
   bool refresh_multigrids();

@@ -432,3 +432,39 @@ def test_reweighting_refresh_equals_rebuild(setup):
         s.update(lam, 1.0)
     assert r1["iterations"] == r2["iterations"]
     np.testing.assert_array_equal(x_refresh, x_build)
+
+
+@pytest.mark.parametrize("knob,value,update", [("dense_boundary_max", 8192, False), ("max_block", 64, False),
+                                               ("max_coarse", 800, True)])
+def test_boundary_layouts_solve_to_reference(setup, knob, value, update):
+    """Other layouts of the exact boundary solve and the coarsest level, built by
+    the device numeric set-up: every boundary block inverted whole (no
+    subdomains, all rows in the separator), subdomains of at most 64 rows (a
+    large separator), and a smaller coarsest level (more levels).  Each solves
+    to the requested residual and to the reference's FP64 solution; the last two
+    agree with the host set-up's solutions to 1e-6 of the largest entry."""
+    import port
+    g, _, s = setup
+    b = g["solve/rhs"]
+    lam = float(g["meta/weights"][0])
+    before = s.get(knob)
+    try:
+        s.set(knob, value)
+        if update:
+            s.update(lam, 1.0)
+        x, rep = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
+        host = None
+        if knob != "dense_boundary_max":  # the host path would invert a block of thousands of rows on the CPU
+            s.set("device_factor", 0)
+            host, _ = s.solve(b, tol=1e-8, max_iters=MAX_ITERS)
+            s.set("device_factor", 1)
+    finally:
+        s.set("device_factor", 1)
+        s.set(knob, before)
+        if update:
+            s.update(lam, 1.0)
+    assert rep["converged"] and rep["rel_residual_max"] <= 1e-8
+    assert s.residual(b, x).max() <= 1e-8
+    assert port.energy_error(ref_full(g), x, g["solve/exact"]).max() < 1e-5
+    if host is not None:
+        assert np.abs(x - host).max() <= 1e-6 * np.abs(host).max()
