@@ -245,35 +245,57 @@ def serving_stream(n_requests: int, max_size: int, budget_gb: float, rate: float
     """Serving stream: requests on torus / icosphere / genus-2 models at sizes
     log-uniform in [256, max_size] (sqrt(2) ladder, multiples of 8), kinds 60 %
     filtering (k = 3), 30 % geodesic (k = 1), 10 % line-integral convolution
-    (k = 1, anisotropy 1e3), Poisson arrivals, HBM admission budget.  Models are
-    added and made resident before the stream (set-up time reported apart);
-    rate 0: arrivals 1.5x faster than the measured one-at-a-time service rate."""
+    (k = 1, anisotropy 1e3), HBM admission budget.  Models are added and made
+    resident before the stream (set-up time reported apart).  The same requests
+    run three ways:
+    * one at a time (each submitted after the previous one finished): the
+      single-model service rate at these sizes, `single_rate`;
+    * all queued at once: the server's capacity with batching and its worker
+      slots, `value` (aggregate Mtexels/s) and `value_over_single`;
+    * Poisson arrivals at the one-at-a-time capacity (rate 0) or at `rate` per
+      second: the latencies under an offered load (`latency_ms`, `open_loop`)."""
     from gradientdomaintextureprocessing_b200 import serving
     stream = serving.request_stream(n_requests, rate_per_s=1.0, max_size=max_size, seed=0)
     server = serving.Server(budget_bytes=int(budget_gb * (1 << 30)), slots=4)
     t0 = time.time()
     models = serving.build_models(server, stream)
     setup_s = time.time() - t0
-    if rate <= 0:
-        probe = [(0.0,) + tuple(p[1:]) for p in stream[:16]]
-        t = []
-        for p in probe:
-            res, _, wall = serving.run_stream(server, [p], models)
-            if res[0][1]["ok"]:
-                t.append(wall)
-        rate = 1.5 / float(np.mean(t))
-    arrivals = serving.request_stream(n_requests, rate_per_s=rate, max_size=max_size, seed=0)
-    before = server.stats()
-    results, st, wall = serving.run_stream(server, arrivals, models)
-    failed = [r for _, r in results if not r["ok"]]
     kind_of = {v: k for k, v in serving.KIND_NAMES.items()}
+
+    def work(r):  # texels x right-hand sides of a finished request
+        return server.texels[models[(r["mesh"], r["size"], kind_of[r["kind"]])][0]] * (3 if r["kind"] == "filtering" else 1)
+
+    queued = [(0.0,) + tuple(p[1:]) for p in stream]
+    # one at a time
+    t_alone, w_alone = [], []
+    for p in queued:
+        res, _, wall = serving.run_stream(server, [p], models)
+        if res[0][1]["ok"]:
+            t_alone.append(wall)
+            w_alone.append(work(res[0][1]))
+    single_rate = sum(w_alone) / sum(t_alone) / 1e6
+    # all queued at once
+    before = server.stats()
+    res_q, st_q, wall_q = serving.run_stream(server, queued, models)
+    ok_q = [r for _, r in res_q if r["ok"]]
+    capacity = sum(work(r) for r in ok_q) / wall_q / 1e6
+    batches = st_q["batches"] - before["batches"]
+    batched = st_q["batched_requests"] - before["batched_requests"]
+    # open loop
+    if rate <= 0:
+        rate = len(t_alone) / sum(t_alone)
+    arrivals = serving.request_stream(n_requests, rate_per_s=rate, max_size=max_size, seed=0)
+    results, st, wall = serving.run_stream(server, arrivals, models)
+    failed = [r for _, r in results if not r["ok"]] + [r for _, r in res_q if not r["ok"]]
     results = [(x, r) for x, r in results if r["ok"]]
     lat = np.array([r["latency_ms"] for _, r in results])
-    texel_rhs = sum(server.texels[models[(r["mesh"], r["size"], kind_of[r["kind"]])][0]] * (3 if r["kind"] == "filtering" else 1)
-                    for _, r in results)
     kinds = {serving.KIND_NAMES[k]: sum(1 for *_, kk in arrivals if kk == k) for k in serving.KIND_NAMES}
-    return {"value": texel_rhs / wall / 1e6, "unit": "Mtexels/s (texels x RHS, whole stream)",
+    return {"value": capacity, "unit": "Mtexels/s (texels x RHS, all requests queued at once)",
+            "single_rate": single_rate, "value_over_single": capacity / single_rate,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "open_loop": {"arrival_rate_per_s": rate, "value": sum(work(r) for _, r in results) / wall / 1e6,
+                          "note": "Poisson arrivals at the one-at-a-time capacity" if rate == len(t_alone) / sum(t_alone)
+                          else "Poisson arrivals at the given rate"},
             "requests": len(arrivals), "failed": len(failed),
             "failures": [{k: r[k] for k in ("mesh", "size", "kind", "error")} for r in failed[:5]],
             "by_kind": {kn: {"p50_ms": float(np.percentile([r["latency_ms"] for _, r in results if r["kind"] == kn], 50)),
@@ -284,11 +306,11 @@ def serving_stream(n_requests: int, max_size: int, budget_gb: float, rate: float
                                for _, r in results), key=lambda d: -d["latency_ms"])[:5],
             "arrival_rate_per_s": rate, "wall_s": wall,
             "max_rel_residual": float(max(r["rel_residual_max"] for _, r in results)),
-            "batches": st["batches"] - before["batches"], "requests_in_batches": st["batched_requests"] - before["batched_requests"],
+            "batches": batches, "requests_in_batches": batched,
             "evictions": st["evictions"], "resident_gb": st["resident_bytes"] / 2**30, "peak_gb": st["peak_bytes"] / 2**30,
             "budget_gb": budget_gb, "models": len(models), "setup_s": round(setup_s, 1), "kinds": kinds,
             "config": {"workload": f"torus / icosphere6 / genus-2, 256^2-{max_size}^2 log-uniform, "
-                                   "60 % filtering k=3, 30 % geodesic k=1, 10 % LIC k=1, Poisson arrivals", "slots": 4}}
+                                   "60 % filtering k=3, 30 % geodesic k=1, 10 % LIC k=1", "slots": 4}}
 
 
 def serve(args):
@@ -422,7 +444,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-max-size", type=int, default=1024,
                     help="largest texture size of the stream (4096 is the full range; host set-up then takes several minutes)")
-    ap.add_argument("--serve-rate", type=float, default=0.0, help="arrivals per second (0: calibrated to saturate)")
+    ap.add_argument("--serve-rate", type=float, default=0.0, help="open-loop arrivals per second (0: the one-at-a-time capacity)")
     ap.add_argument("--serve-budget-gb", type=float, default=80.0)
     ap.add_argument("--serve-requests-in-line", type=int, default=64,
                     help="requests of the compact serving stream (256^2-512^2) reported in the main line (0: none)")
@@ -661,15 +683,21 @@ def main():
     peak = float(peaks.get("hbm_gbs", 6650.0))
     sweep_ms = prof[1] / max(prof[0], 1)
     texels = prof[2]
-    tiled = bool(prof[5])
+    smoother = int(prof[5])  # 0 four colour passes per sweep, 1 fused tile-smoother round, 2 two row-smoother launches
     # algorithmic bytes per deep texel of one timed group (a colour sweep, or a
     # round of the fused tile smoother): 10 FP32 coefficients (40 B) + rhs
     # read, x read and x written once, k = 3 channels of 4 B (3 x 12 B) = 76 B
     sweep_bytes = texels * (40 + 3 * K * 4)
-    if tiled:
+    if smoother == 1:
         kernel = "level-0 fused tile-smoother round (k_tile_smooth, one launch: every sweep of the round in 32x32 tiles)"
         # moved with the padded 4-lane vectors and the one-texel ring of a tile
         model_bytes = texels * (40 + 16 + 16 * 34 * 34 / 1024 + 16)
+    elif smoother == 2:
+        kernel = "level-0 4-colour Gauss-Seidel sweep (k_gs_rows x2: both colours of a row parity per launch)"
+        # padded 4-lane vectors: coefficients, rhs, x written, and x of the
+        # line's own row and of the rows above and below, each staged once per
+        # launch (40 + 16 + 16 + 3 x 16 = 120 B)
+        model_bytes = texels * (40 + 16 + 16 + 48)
     else:
         kernel = "level-0 4-colour Gauss-Seidel sweep (k_gs_colour x4)"
         # the 4-launch colour decomposition with padded 4-lane vectors:
@@ -678,7 +706,8 @@ def main():
         model_bytes = texels * (40 + 16 + 16 + 48)
     achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9 if sweep_ms > 0 else None
     try:  # DRAM bytes per deep texel per timed group, from ncu captures of this workload
-        traffic_per_texel = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["tile" if tiled else "colour"]
+        traffic_per_texel = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))[
+            {0: "colour", 1: "tile", 2: "rows"}[smoother]]
     except (OSError, ValueError, KeyError):
         traffic_per_texel = None
     launches = int(prof[4])  # counted by the solver: graph kernel nodes x graph launches + direct launches
@@ -720,9 +749,9 @@ def main():
         # a compact serving stream after the timed regions (continuous batching,
         # admission, mixed kinds), so that every run reports serving latency
         blk = serving_stream(args.serve_requests_in_line, 512, args.serve_budget_gb)
-        out["serving"] = {k: blk[k] for k in ("value", "unit", "latency_ms", "requests", "failed", "arrival_rate_per_s",
-                                               "max_rel_residual", "batches", "requests_in_batches", "evictions", "models",
-                                               "setup_s", "by_kind", "slowest", "config")}
+        out["serving"] = {k: blk[k] for k in ("value", "unit", "single_rate", "value_over_single", "latency_ms", "open_loop",
+                                               "requests", "failed", "max_rel_residual", "batches", "requests_in_batches",
+                                               "evictions", "models", "setup_s", "by_kind", "slowest", "config")}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:

@@ -304,6 +304,7 @@ extern "C" int gdtp_system_set(gdtp_system* s, const char* knob, double value) {
     else if (k == "krylov" && (v == 0 || v == 1)) kn.krylov = v;
     else if (k == "zero_start_skip" && (v == 0 || v == 1)) kn.zeroStartSkip = v;
     else if (k == "device_factor" && (v == 0 || v == 1)) kn.deviceFactor = v;
+    else if (k == "row_sweeps" && (v == 0 || v == 1)) kn.rowSweeps = v;
     else return fail(GDTP_ERR_INVALID, "gdtp_system_set: unknown knob or value out of range: " + k);
     if (k == "tile_texels" || k == "device_factor" || k == "max_block" || k == "dense_boundary_max" || k == "max_coarse")
       s->sys->invalidate_multigrids();  // the multigrids are laid out and factorised by these knobs
@@ -334,6 +335,7 @@ extern "C" int gdtp_system_get(const gdtp_system* s, const char* knob, double* v
     else if (k == "krylov") *value = kn.krylov;
     else if (k == "zero_start_skip") *value = kn.zeroStartSkip;
     else if (k == "device_factor") *value = kn.deviceFactor;
+    else if (k == "row_sweeps") *value = kn.rowSweeps;
     else if (k == "grid_texels") *value = kn.gridTexels;
     else if (k == "chart_texels") *value = kn.chartTexels;
     else if (k == "tile_texels") *value = kn.tileTexels;

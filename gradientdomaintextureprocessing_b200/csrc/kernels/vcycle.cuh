@@ -23,6 +23,16 @@ namespace dev {
 struct ColourRun {       // texels pos0 + 2m, m < len
   int pos0, prev0, next0, coef0, len;
 };
+// One raster line of deep texels (row smoother): texels pos + i, i < len, the
+// rows above and below start at prev and next; coefficient index of its first
+// even- / odd-column texel (its texels of one colour are consecutive in the
+// colour-run planes); meta = first thread of the line in its block (bits 0-10)
+// | first shared-memory slot (bits 11-23, slot of texel -1) | 1 << 24 when its
+// first texel is in an odd column.
+struct __align__(16) RowLine {
+  int pos, prev, next, len;
+  int cEven, cOdd, meta, pad;
+};
 struct RestrictRun {     // coarse texel out0 + m reads fine f0 + 2m and rows fp0/fn0 + 2m
   int out0, f0, fp0, fn0, len;
 };

@@ -70,6 +70,148 @@ __global__ void __launch_bounds__(256) k_gs_colour(const ColourRun* __restrict__
   vstore<T, W>(x + (long long)pos * KP + off, out);
 }
 
+// Two colour passes of one row parity (launch_gs_rows).  Colours 0 and 1 hold
+// the even rows, 2 and 3 the odd rows, and the 9-point stencil of a row reaches
+// only its own row and the two rows of the other parity.  So the passes of one
+// row parity update each raster line independently: the first colour (A) from
+// the line's old values, then the second (B) from A's new values in the line.
+// A block holds whole lines; thread q of a line owns its texels 2q and 2q + 1
+// (A texel oA + 2q, B texel oB + 2q), which it stages with the rows above and
+// below into shared memory (slot 0 of a line: texel -1, slot len + 1: texel
+// len, the line's non-deep neighbours).  Coefficients and (rhsEarly) the
+// right-hand side are loaded before the dependency wait, as in k_gs_colour; A
+// texels of a line are consecutive in the colour-run planes, as are B texels.
+// Each update is gs_item's sum in gs_item's order.
+// blocks of BS threads per SM the row smoother is compiled for (registers)
+template <typename T>
+constexpr int rows_min_blocks(int bs) {
+  return (sizeof(T) == 4 ? 1280 : 768) / bs > 0 ? (sizeof(T) == 4 ? 1280 : 768) / bs : 1;
+}
+template <typename T, int W, int BS>
+__global__ void __launch_bounds__(BS) k_gs_rows(const RowLine* __restrict__ lines, const int* __restrict__ lineOf,
+                                                           const T* __restrict__ coef, int planeStride, const T* __restrict__ rhs,
+                                                           T* __restrict__ x, int KP, int slots, int oddFirst, int skip,
+                                                           int rhsEarly) {
+  extern __shared__ __align__(32) unsigned char smem_raw[];
+  Vec<T, W>* up = reinterpret_cast<Vec<T, W>*>(smem_raw);
+  Vec<T, W>* mid = up + slots;
+  Vec<T, W>* dn = mid + slots;
+  const int li = lineOf[(long long)blockIdx.x * BS + threadIdx.x];
+  const int off = blockIdx.y * W;
+  RowLine Ln;
+  Ln.len = 0;
+  int q = 0, a = 0, b = 0, s0 = 0, H = 0;
+  bool hasA = false, hasB = false;
+  T wA[9], wB[9];
+  Vec<T, W> bA, bB;
+  if (li >= 0) {
+    Ln = lines[li];
+    q = int(threadIdx.x) - (Ln.meta & 2047);
+    s0 = (Ln.meta >> 11) & 8191;
+    H = (Ln.len + 3) >> 1;
+    const int oA = ((Ln.meta >> 24) & 1) ^ oddFirst;
+    a = oA + 2 * q;
+    b = (oA ^ 1) + 2 * q;
+    hasA = a < Ln.len;
+    hasB = b < Ln.len;
+    const T* cA = coef + (oddFirst ? Ln.cOdd : Ln.cEven) + q;
+    const T* cB = coef + (oddFirst ? Ln.cEven : Ln.cOdd) + q;
+    if (hasA) {
+#pragma unroll
+      for (int k = 0; k < 9; k++) wA[k] = cA[k * planeStride];
+      if (rhsEarly) bA = vload<T, W>(rhs + (long long)(Ln.pos + a) * KP + off);
+    }
+    if (hasB) {
+#pragma unroll
+      for (int k = 0; k < 9; k++) wB[k] = cB[k * planeStride];
+      if (rhsEarly) bB = vload<T, W>(rhs + (long long)(Ln.pos + b) * KP + off);
+    }
+  }
+  // shared slot of line texel i (-1 .. len): texels of even and odd i + 1 in
+  // two halves, so that consecutive threads touch consecutive slots
+  auto slot = [&](int i) { return s0 + (((i + 1) & 1) ? H + ((i + 1) >> 1) : ((i + 1) >> 1)); };
+  grid_dependency_wait();
+  grid_launch_dependents();
+  const bool rowsA = !(skip & 1), rowsB = !(skip & 4);
+  if (li >= 0) {
+    const bool rows = rowsA || rowsB;
+    auto stage = [&](int i) {
+      const int sl = slot(i);
+      mid[sl] = vload<T, W>(x + (long long)(Ln.pos + i) * KP + off);
+      if (rows) {
+        up[sl] = vload<T, W>(x + (long long)(Ln.prev + i) * KP + off);
+        dn[sl] = vload<T, W>(x + (long long)(Ln.next + i) * KP + off);
+      }
+    };
+    // the pair of texels (2q, 2q + 1) of the three rows, and the line's ends:
+    // the first thread texel -1, the last thread texel len
+    stage(2 * q);
+    if (2 * q + 1 < Ln.len) stage(2 * q + 1);
+    if (q == 0) stage(-1);
+    if (2 * q + 2 >= Ln.len) stage(Ln.len);
+    if (!rhsEarly) {
+      if (hasA) bA = vload<T, W>(rhs + (long long)(Ln.pos + a) * KP + off);
+      if (hasB) bB = vload<T, W>(rhs + (long long)(Ln.pos + b) * KP + off);
+    }
+  }
+  __syncthreads();
+  Vec<T, W> xa, xb;
+  if (hasA) {
+    const int sm = slot(a - 1), sc = slot(a), sp = slot(a + 1);
+    Vec<T, W> acc;
+#pragma unroll
+    for (int k = 0; k < W; k++) acc.v[k] = 0;
+    if (rowsA) {
+      axpy(acc, wA[0], up[sm]);
+      axpy(acc, wA[1], up[sc]);
+      axpy(acc, wA[2], up[sp]);
+    }
+    if (!(skip & 2)) {
+      axpy(acc, wA[3], mid[sm]);
+      axpy(acc, wA[5], mid[sp]);
+    }
+    if (rowsA) {
+      axpy(acc, wA[6], dn[sm]);
+      axpy(acc, wA[7], dn[sc]);
+      axpy(acc, wA[8], dn[sp]);
+    }
+#pragma unroll
+    for (int k = 0; k < W; k++) xa.v[k] = bA.v[k] * wA[4] - acc.v[k];
+    mid[sc] = xa;  // A slots are read only by B updates, after the barrier
+  }
+  __syncthreads();
+  if (hasB) {
+    const int sm = slot(b - 1), sc = slot(b), sp = slot(b + 1);
+    Vec<T, W> acc;
+#pragma unroll
+    for (int k = 0; k < W; k++) acc.v[k] = 0;
+    if (rowsB) {
+      axpy(acc, wB[0], up[sm]);
+      axpy(acc, wB[1], up[sc]);
+      axpy(acc, wB[2], up[sp]);
+    }
+    if (!(skip & 8)) {
+      axpy(acc, wB[3], mid[sm]);
+      axpy(acc, wB[5], mid[sp]);
+    }
+    if (rowsB) {
+      axpy(acc, wB[6], dn[sm]);
+      axpy(acc, wB[7], dn[sc]);
+      axpy(acc, wB[8], dn[sp]);
+    }
+#pragma unroll
+    for (int k = 0; k < W; k++) xb.v[k] = bB.v[k] * wB[4] - acc.v[k];
+  }
+  // texels 2q and 2q + 1 of the line, in address order
+  if (a < b) {
+    if (hasA) vstore<T, W>(x + (long long)(Ln.pos + a) * KP + off, xa);
+    if (hasB) vstore<T, W>(x + (long long)(Ln.pos + b) * KP + off, xb);
+  } else {
+    if (hasB) vstore<T, W>(x + (long long)(Ln.pos + b) * KP + off, xb);
+    if (hasA) vstore<T, W>(x + (long long)(Ln.pos + a) * KP + off, xa);
+  }
+}
+
 // Every sweep of one smoothing step on one chart per block: the colour passes
 // of a chart only read texels of that chart (deep) or boundary texels, which
 // the sweeps do not change, so block barriers order the passes.  The chart's
@@ -846,6 +988,60 @@ void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int plane
          rhsEarly ? 1 : 0);
 }
 template <typename T, int W>
+size_t gs_rows_smem(const LevelDev<T>& D) {
+  return size_t(3) * D.rowSlots * sizeof(Vec<T, W>);  // three rows
+}
+// The row smoother's shared memory fits this device (its attribute set): 1, else 0.
+template <typename T, int W, int BS>
+static int gs_rows_ready() {
+  static std::atomic<int> slots[kMaxDevices];
+  static const bool init = [] {
+    for (auto& v : slots) v.store(kUnset);
+    return true;
+  }();
+  (void)init;
+  return per_device_once(slots, [] {
+    const int smem = int(3 * row_slot_cap(BS) * sizeof(Vec<T, W>));
+    if (cudaFuncSetAttribute(k_gs_rows<T, W, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    return 1;
+  });
+}
+template <typename T, int W, int BS>
+static bool launch_gs_rows_bs(const LevelDev<T>& D, int rows, bool oddFirst, int KP, cudaStream_t s, int skip, bool rhsEarly) {
+  if (gs_rows_ready<T, W, BS>() <= 0) return false;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(D.nRowBins[rows]), unsigned(KP / W));
+  cfg.blockDim = dim3(BS);
+  cfg.dynamicSmemBytes = gs_rows_smem<T, W>(D);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = g_programmatic ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k_gs_rows<T, W, BS>, D.rowLines[rows], D.rowLineOf[rows], D.coef, D.planeStride,
+                     static_cast<const T*>(D.b), D.x, KP, D.rowSlots, oddFirst ? 1 : 0, skip, rhsEarly ? 1 : 0);
+  return true;
+}
+template <typename T, int W>
+bool gs_rows_available(const LevelDev<T>& D) {
+  if (D.rowBlock == 256) return gs_rows_ready<T, W, 256>() > 0;
+  if (D.rowBlock == 512) return gs_rows_ready<T, W, 512>() > 0;
+  if (D.rowBlock == 1024) return gs_rows_ready<T, W, 1024>() > 0;
+  return false;
+}
+template <typename T, int W>
+bool launch_gs_rows(const LevelDev<T>& D, int rows, bool oddFirst, int KP, cudaStream_t s, int skip, bool rhsEarly) {
+  if (D.nRowBins[rows] == 0) return true;
+  if (D.rowBlock == 256) return launch_gs_rows_bs<T, W, 256>(D, rows, oddFirst, KP, s, skip, rhsEarly);
+  if (D.rowBlock == 512) return launch_gs_rows_bs<T, W, 512>(D, rows, oddFirst, KP, s, skip, rhsEarly);
+  if (D.rowBlock == 1024) return launch_gs_rows_bs<T, W, 1024>(D, rows, oddFirst, KP, s, skip, rhsEarly);
+  return false;
+}
+template <typename T, int W>
 size_t gs_groups_smem(const LevelDev<T>& D, int KP) {
   return size_t(D.maxGroupSpan) * KP * sizeof(T);
 }
@@ -1019,6 +1215,9 @@ void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStre
 
 #define GDTP_INSTANTIATE(T, W)                                                                                             \
   template void launch_gs_colour<T, W>(const ColourRun*, int, const T*, int, const T*, T*, int, cudaStream_t, int, bool); \
+  template bool launch_gs_rows<T, W>(const LevelDev<T>&, int, bool, int, cudaStream_t, int, bool);                       \
+  template bool gs_rows_available<T, W>(const LevelDev<T>&);                                                             \
+  template size_t gs_rows_smem<T, W>(const LevelDev<T>&);                                                                \
   template bool launch_gs_groups<T, W>(const LevelDev<T>&, int, bool, int, cudaStream_t);                                \
   template void launch_residual<T, W>(const ColourRun*, int, const T*, int, const int*, const int*, const T*, const int*, \
                                       int, const T*, const T*, T*, int, cudaStream_t, bool);                             \

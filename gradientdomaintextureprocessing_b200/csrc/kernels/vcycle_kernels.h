@@ -14,6 +14,7 @@ constexpr int kUnset = -2;
 
 
 struct ColourRun;
+struct RowLine;
 struct RestrictRun;
 struct ProlongRun;
 
@@ -84,6 +85,13 @@ struct LevelDev {
   const int* tileNbrs = nullptr;
   const float* tileCoef = nullptr;
   int* tileSync = nullptr;      // per multigrid (its rounds run in its stream order)
+  // row smoother (launch_gs_rows): the raster lines of even [0] and odd [1]
+  // rows packed into blocks of rowBlock threads; rowLineOf[block * rowBlock +
+  // thread] = its line (-1: idle)
+  const RowLine* rowLines[2] = {nullptr, nullptr};
+  const int* rowLineOf[2] = {nullptr, nullptr};
+  int nRowBins[2] = {0, 0};
+  int rowBlock = 0, rowSlots = 0;
 };
 
 template <typename T, int W>
@@ -92,6 +100,27 @@ template <typename T, int W>
 // of the same smoothing step), so rhs is read before waiting for it
 void launch_gs_colour(const ColourRun* runs, int nRuns, const T* coef, int planeStride, const T* rhs, T* x, int KP, cudaStream_t s,
                       int skip = 0, bool rhsEarly = false);
+// Two colour passes of one row parity in one launch (rows: 0 even rows, colours
+// 0 then 1 or, with oddFirst, 1 then 0; 1 odd rows, colours 2 / 3): a block
+// per group of whole raster lines, which stages the line's row and the rows
+// above and below in shared memory, updates the first colour, then the second
+// from the first's new values.  A row's update reads only the other parity's
+// rows and its own, so the lines are independent and the result is that of
+// the two launch_gs_colour passes, bit for bit.  skip: bit 0 / 1 = the first
+// colour's row (above and below) / own-row neighbours are known zeros, bits 2
+// / 3 the same for the second colour.
+constexpr int kRowBlockMax = 1024;
+// shared-memory slots per row-smoother block of bs threads (a line of len
+// texels takes len + 2; bs threads hold lines of at most 2 bs texels)
+constexpr int row_slot_cap(int bs) { return 2 * bs + 64; }
+// false: nothing launched (the level has no row blocks, or their shared memory
+// does not fit this device); gs_rows_available tells before any launch
+template <typename T, int W>
+bool launch_gs_rows(const LevelDev<T>& D, int rows, bool oddFirst, int KP, cudaStream_t s, int skip = 0, bool rhsEarly = false);
+template <typename T, int W>
+bool gs_rows_available(const LevelDev<T>& D);
+template <typename T, int W>
+size_t gs_rows_smem(const LevelDev<T>& D);
 // `sweeps` 4-colour Gauss-Seidel sweeps (colours 0..3, or 3..0 when reverse)
 // in one launch, one block per chart group with the chart's x in shared memory:
 // the same updates in the same order as launch_gs_colour per colour.  False

@@ -62,14 +62,17 @@ DeepRuns build_line_runs(const GridLevel& L) {
 DeepRuns build_deep_runs(const GridLevel& L) {
   DeepRuns R;
   R.texel.reserve(L.numDeep);
+  R.lineCoef.assign(L.rasterLines.size() * 2, -1);
   for (int c = 0; c < 4; c++) {
     R.runStart[c] = (int)R.runs.size();
     const int ci = c & 1, cj = c >> 1;
-    for (const Line& l : L.rasterLines) {
+    for (size_t li = 0; li < L.rasterLines.size(); li++) {
+      const Line& l = L.rasterLines[li];
       const NodeInfo& n = L.nodes[l.start];
       if ((n.cj & 1) != cj) continue;
       const int len = l.end - l.start + 1;
       const int o = (ci - (n.ci & 1)) & 1;
+      if (o < len) R.lineCoef[2 * li + ci] = R.count;
       for (int p = o; p < len; p += 64) {
         dev::ColourRun r;
         r.pos0 = l.start + p;
@@ -85,6 +88,57 @@ DeepRuns build_deep_runs(const GridLevel& L) {
   }
   R.runStart[4] = (int)R.runs.size();
   return R;
+}
+
+// Raster lines of each row parity packed, in raster order, into blocks of
+// `block` threads (a line of len texels takes (len + 1) / 2 threads and len + 2
+// shared-memory slots).  The block size is the smallest of 256, 512 and 1024
+// threads that holds the longest line; false (row smoother unused) when a line
+// is longer than 2 kRowBlockMax texels.
+bool build_row_bins(const GridLevel& L, const DeepRuns& R, RowBins& out) {
+  out = RowBins();
+  int maxThr = 0;
+  for (const Line& l : L.rasterLines) maxThr = std::max(maxThr, (l.end - l.start + 2) / 2);
+  int bs = 256;
+  while (bs < maxThr && bs < dev::kRowBlockMax) bs *= 2;
+  if (maxThr > bs || L.rasterLines.empty()) return false;
+  out.block = bs;
+  out.slots = dev::row_slot_cap(bs);
+  for (int rows = 0; rows < 2; rows++) {
+    std::vector<dev::RowLine>& lines = out.lines[rows];
+    std::vector<int>& lineOf = out.lineOf[rows];
+    int thr = bs, slot = out.slots;  // the current block is full: open one on the first line
+    for (size_t li = 0; li < L.rasterLines.size(); li++) {
+      const Line& l = L.rasterLines[li];
+      const NodeInfo& n = L.nodes[l.start];
+      if ((n.cj & 1) != rows) continue;
+      const int len = l.end - l.start + 1, nt = (len + 1) / 2;
+      if (thr + nt > bs || slot + len + 2 > out.slots) {
+        lineOf.resize(lineOf.size() + bs, -1);
+        out.bins[rows]++;
+        thr = slot = 0;
+      }
+      const int oddStart = n.ci & 1;
+      dev::RowLine r;
+      r.pos = l.start;
+      r.prev = l.prev;
+      r.next = l.next;
+      r.len = len;
+      // the line's first texel of even / odd column (colour-run coefficient index)
+      r.cEven = R.lineCoef[2 * li + 0];
+      r.cOdd = R.lineCoef[2 * li + 1];
+      r.meta = thr | (slot << 11) | (oddStart << 24);
+      r.pad = 0;
+      if ((r.cEven < 0 && len > oddStart) || (r.cOdd < 0 && len > 1 - oddStart)) return false;
+      const int idx = (int)lines.size();
+      lines.push_back(r);
+      const size_t base = lineOf.size() - bs;
+      for (int t = 0; t < nt; t++) lineOf[base + thr + t] = idx;
+      thr += nt;
+      slot += len + 2;
+    }
+  }
+  return true;
 }
 
 // Per chart and colour, the range of that colour's runs that lie in the chart:
@@ -817,6 +871,19 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
     D.nRuns = (int)R.runs.size();
     std::copy(R.runStart, R.runStart + 5, D.runStart);
     D.planeStride = R.count;
+    // raster lines in blocks for the row smoother (two colours per launch)
+    {
+      RowBins RB;
+      if (build_row_bins(G, R, RB)) {
+        for (int p = 0; p < 2; p++) {
+          D.rowLines[p] = A.upload(RB.lines[p]);
+          D.rowLineOf[p] = A.upload(RB.lineOf[p]);
+          D.nRowBins[p] = RB.bins[p];
+        }
+        D.rowBlock = RB.block;
+        D.rowSlots = RB.slots;
+      }
+    }
     // tiles of the fused smoother (FP32 levels it runs on; the tile_texels knob
     // drops the multigrids when it changes; host-built values only)
     if (!numeric && sizeof(T) == 4 && G.numDeep >= kTileBuildMin && knobs.tileTexels > 0 && G.numDeep >= knobs.tileTexels) {
@@ -1162,6 +1229,35 @@ static int zero_start_skip(int c) {
   return skip;
 }
 
+template <typename T, int W>
+void DeviceSystem::colour_sweep(const LevelDev<T>& D, int KP, bool reverse, bool fromZero, bool rhsEarly, cudaStream_t s) {
+  if (knobs.rowSweeps && D.rowBlock > 0 && dev::gs_rows_available<T, W>(D)) {
+    // a colour's zero-start skips cover its rows above and below, or its own
+    // row, whole: the row smoother skips them as groups
+    constexpr int kRows = 1 | 2 | 4 | 64 | 128 | 256, kOwn = 8 | 32;
+    for (int h = 0; h < 2; h++) {
+      const int rows = reverse ? 1 - h : h;
+      const int cA = 2 * rows + (reverse ? 1 : 0), cB = cA ^ 1;
+      int skip = 0;
+      if (fromZero) {
+        const int sa = zero_start_skip(cA), sb = zero_start_skip(cB);
+        skip = ((sa & kRows) ? 1 : 0) | ((sa & kOwn) ? 2 : 0) | ((sb & kRows) ? 4 : 0) | ((sb & kOwn) ? 8 : 0);
+      }
+      dev::launch_gs_rows<T, W>(D, rows, reverse, KP, s, skip, h > 0 || rhsEarly);
+    }
+    return;
+  }
+  for (int p = 0; p < 4; p++) {
+    const int c = reverse ? 3 - p : p;
+    dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s,
+                                fromZero ? zero_start_skip(c) : 0, p > 0 || rhsEarly);
+  }
+}
+template void DeviceSystem::colour_sweep<float, 1>(const LevelDev<float>&, int, bool, bool, bool, cudaStream_t);
+template void DeviceSystem::colour_sweep<float, 4>(const LevelDev<float>&, int, bool, bool, bool, cudaStream_t);
+template void DeviceSystem::colour_sweep<double, 1>(const LevelDev<double>&, int, bool, bool, bool, cudaStream_t);
+template void DeviceSystem::colour_sweep<double, 4>(const LevelDev<double>&, int, bool, bool, bool, cudaStream_t);
+
 // One smoothing step of `sweeps` sweeps with the fused tile smoother, in
 // place: `tileRounds` rounds (one launch each) over the tiles in tile-colour
 // order (3..0 with reverse), the sweeps split between the rounds; only the
@@ -1195,18 +1291,14 @@ void DeviceSystem::tile_smooth(Multigrid<T>& mg, LevelDev<T>& D, int sweeps, boo
     cudaEventRecordWithFlags(profEv_[3], s, cudaEventRecordExternal);
     profPostSweeps_ = rounds;
     profTiled_ = true;
+    profRows_ = false;
   }
   usedTileWait_ = true;
   if (knobs.tileFinish) {
-    for (int p = 0; p < 4; p++) {
-      const int c = reverse ? 3 - p : p;
-      if (KP % 4 == 0)
-        dev::launch_gs_colour<T, 4>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s, 0,
-                                    p > 0);
-      else
-        dev::launch_gs_colour<T, 1>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP, s, 0,
-                                    p > 0);
-    }
+    if (KP % 4 == 0)
+      colour_sweep<T, 4>(D, KP, reverse, false, false, s);
+    else
+      colour_sweep<T, 1>(D, KP, reverse, false, false, s);
   }
 }
 
@@ -1249,10 +1341,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
       for (int sw = 0; sw < pre_sweeps(l); sw++) {
         const bool prof = profiling_ && l == 0;
         if (prof && sw == firstFull) cudaEventRecordWithFlags(profEv_[0], s, cudaEventRecordExternal);
-        const bool fromZero = fromZero0 && sw == 0;
-        for (int c = 0; c < 4; c++)
-          dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP,
-                                      s, fromZero ? zero_start_skip(c) : 0, sw > 0 || c > 0);
+        colour_sweep<T, W>(D, KP, false, fromZero0 && sw == 0, sw > 0, s);
         if (prof && sw == pre_sweeps(l) - 1 && sw >= firstFull) {
           cudaEventRecordWithFlags(profEv_[1], s, cudaEventRecordExternal);
           profSweeps_ = pre_sweeps(l) - firstFull;
@@ -1304,14 +1393,12 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
     } else {
       const bool prof = profiling_ && l == 0 && post_sweeps(l) > 0;
       if (prof) cudaEventRecordWithFlags(profEv_[2], s, cudaEventRecordExternal);
-      for (int sw = 0; sw < post_sweeps(l); sw++)
-        for (int c = 3; c >= 0; c--)
-          dev::launch_gs_colour<T, W>(D.runs + D.runStart[c], D.runStart[c + 1] - D.runStart[c], D.coef, D.planeStride, D.b, D.x, KP,
-                                      s, 0, sw > 0 || c < 3);
+      for (int sw = 0; sw < post_sweeps(l); sw++) colour_sweep<T, W>(D, KP, true, false, sw > 0, s);
       if (prof) {
         cudaEventRecordWithFlags(profEv_[3], s, cudaEventRecordExternal);
         profPostSweeps_ = post_sweeps(l);
         profTiled_ = false;
+        profRows_ = knobs.rowSweeps && D.rowBlock > 0 && dev::gs_rows_available<T, W>(D);
       }
     }
     trace_mark(L + 1 + (L - 2 - l), s);
@@ -1503,17 +1590,12 @@ bool DeviceSystem::relax_host(float* x, const float* rhs, int k, int sweeps, boo
   if (tiled(D0, mg.KP)) {
     if (sweeps > 0) tile_smooth(mg, D0, sweeps, reverse, false, stream_, false);
   } else {
-    const int W = (mg.KP % 4 == 0) ? 4 : 1;
-    for (int sw = 0; sw < sweeps; sw++)
-      for (int p = 0; p < 4; p++) {
-        const int c = reverse ? 3 - p : p;
-        if (W == 4)
-          dev::launch_gs_colour<float, 4>(D0.runs + D0.runStart[c], D0.runStart[c + 1] - D0.runStart[c], D0.coef, D0.planeStride, D0.b,
-                                          D0.x, mg.KP, stream_, 0, sw > 0 || p > 0);
-        else
-          dev::launch_gs_colour<float, 1>(D0.runs + D0.runStart[c], D0.runStart[c + 1] - D0.runStart[c], D0.coef, D0.planeStride, D0.b,
-                                          D0.x, mg.KP, stream_, 0, sw > 0 || p > 0);
-      }
+    for (int sw = 0; sw < sweeps; sw++) {
+      if (mg.KP % 4 == 0)
+        colour_sweep<float, 4>(D0, mg.KP, reverse, false, sw > 0, stream_);
+      else
+        colour_sweep<float, 1>(D0, mg.KP, reverse, false, sw > 0, stream_);
+    }
   }
   queue_barrier_check(mg, stream_);
   if (!check(cudaGetLastError(), "relax") ||

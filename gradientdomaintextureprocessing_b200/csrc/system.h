@@ -61,9 +61,22 @@ struct DeepRuns {
   int runStart[5] = {0, 0, 0, 0, 0};
   std::vector<int> texel;       // run texel -> deep index (plane order)
   int count = 0;                // run texels = deep texels
+  // per raster line: plane index of its first even- [2 l] and odd-column [2 l + 1]
+  // texel (-1: none; deep runs only)
+  std::vector<int> lineCoef;
 };
 DeepRuns build_deep_runs(const GridLevel& L);
 DeepRuns build_line_runs(const GridLevel& L);
+
+// Raster lines of even [0] and odd [1] rows packed into blocks of the row
+// smoother (dev::launch_gs_rows)
+struct RowBins {
+  std::vector<dev::RowLine> lines[2];
+  std::vector<int> lineOf[2];   // block * block size + thread -> line (-1: idle)
+  int bins[2] = {0, 0};
+  int block = 0, slots = 0;
+};
+bool build_row_bins(const GridLevel& L, const DeepRuns& R, RowBins& out);
 
 template <typename T>
 using LevelDev = dev::LevelDev<T>;
@@ -120,6 +133,7 @@ struct SolverKnobs {
                                         // step's sweeps split between them)
   int tileFinish = 0;                   // 1: one global colour sweep after each tiled smoothing step
   int deviceFactor = 1;                 // dense set-up inverses and products on the device (0: host)
+  int rowSweeps = 1;                    // colour sweeps as two row-smoother launches (0: four colour passes)
 };
 
 struct SolveReport {
@@ -182,8 +196,16 @@ class DeviceSystem {
 
   SolverKnobs knobs;
   bool profTiled() const { return profTiled_; }
+  bool profRows() const { return profRows_; }
   template <typename T>
   void tile_smooth(Multigrid<T>& mg, dev::LevelDev<T>& D, int sweeps, bool reverse, bool zeroStart, cudaStream_t s, bool prof);
+  // one 4-colour Gauss-Seidel sweep (colours 0..3, or 3..0 when reverse): two
+  // row-smoother launches (knob row_sweeps, where the level has row blocks) or
+  // four colour passes, the same updates either way.  fromZero: the first sweep
+  // from a zero iterate (zero neighbours skipped); rhsEarly: the launch before
+  // the sweep does not write the right-hand side.
+  template <typename T, int W>
+  void colour_sweep(const dev::LevelDev<T>& D, int KP, bool reverse, bool fromZero, bool rhsEarly, cudaStream_t s);
   template <typename T>
   bool grouped(const dev::LevelDev<T>& D, int KP) const {
     return knobs.chartTexels > 0 && D.nGroups > 0 && D.maxGroupDeep <= knobs.chartTexels &&
@@ -354,6 +376,7 @@ class DeviceSystem {
   cudaEvent_t profEv_[4] = {nullptr, nullptr, nullptr, nullptr};  // level-0 full pre sweeps, post sweeps
   int profSweeps_ = 0, profPostSweeps_ = 0;
   bool profTiled_ = false;              // the timed level-0 group is one fused tile-smoother launch
+  bool profRows_ = false;               // the timed level-0 sweeps are row-smoother launches (two per sweep)
   std::vector<cudaEvent_t> traceEv_;   // 2 L markers of the captured V-cycle (traceLevels)
   void trace_mark(int i, cudaStream_t s);
   unsigned long long* timeline_ = nullptr;  // cluster phase timeline (traceLevels)

@@ -120,8 +120,9 @@ void gdtp_system_free(gdtp_system* s);
  *   "bbMass.ptr/.col/.val" "bbStiffness.*" "bdMass.*" "bdStiffness.*"
  *   after gdtp_system_update: "coef.deep"(level l, raw, 10 per deep texel), "coef.bb.*", "coef.bd.*"
  *   "profile": {timed level-0 sweep groups, their total ms, deep texels per group,
- *   kernels per step graph, kernels launched by solves, 1 if a timed group is one
- *   fused tile-smoother launch (else colour sweeps)}; "profile.reset" clears the counts
+ *   kernels per step graph, kernels launched by solves, the timed group's smoother:
+ *   1 one fused tile-smoother launch, 2 a sweep of two row-smoother launches, 0 a
+ *   sweep of four colour passes}; "profile.reset" clears the counts
  *   "profile.setup": ms of the last set-up {update, boundary solver factorisations,
  *   coarsest inverse, other multigrid set-up, then the factorisations split into
  *   partition and sparse assembly, subdomain inverses, Schur products, Schur
@@ -265,7 +266,10 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * "tile_pre_sweeps", "tile_post_sweeps" (sweeps per smoothing step on tiled
  * levels, default 2/2), "tile_rounds"
  * (passes over the tiles per smoothing step, the sweeps split between them,
- * default 1), "tile_finish" (0/1: one global colour sweep closes each tiled
+ * default 1), "row_sweeps" (0/1, default 1: each 4-colour sweep of a level
+ * whose raster lines fit a block runs as two launches, both colours of a row
+ * parity per launch, the same updates bit for bit), "tile_finish" (0/1: one
+ * global colour sweep closes each tiled
  * smoothing step), "device_factor" (0/1, default 1: the dense FP64 inverses
  * and products of the set-up -- boundary subdomain blocks, separator Schur
  * complement, coarsest level -- run on the device by blocked Gauss-Jordan

@@ -468,3 +468,35 @@ def test_boundary_layouts_solve_to_reference(setup, knob, value, update):
     assert port.energy_error(ref_full(g), x, g["solve/exact"]).max() < 1e-5
     if host is not None:
         assert np.abs(x - host).max() <= 1e-6 * np.abs(host).max()
+
+
+@pytest.mark.parametrize("k", [1, 3, 8])
+def test_row_smoother_matches_colour_passes(setup, k):
+    """A colour sweep as two row-smoother launches (row_sweeps 1: both colours of
+    a row parity per launch, lines staged in shared memory) gives the bits of
+    the four colour-pass launches: forward and reverse relaxation from random
+    data, a V-cycle (its first sweep from zero skips the same neighbours), the
+    mixed solve and the FP64 multigrid's solve.  k = 1, 3, 8: one channel, the
+    padded 4-lane vectors, two channel groups per texel."""
+    g, h, s = setup
+    rng = np.random.default_rng(11)
+    n = h.counts(0)["numTexels"]
+    x0 = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    rhs = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    b = np.repeat(g["solve/rhs"], (k + 2) // 3, axis=1)[:, :k]
+    before = s.get("row_sweeps")
+    out = {}
+    try:
+        for rows in (0, 1):
+            s.set("row_sweeps", rows)
+            out[rows] = (s.relax(x0, rhs, sweeps=2), s.relax(x0, rhs, sweeps=2, reverse=True),
+                         s.vcycle(np.zeros_like(x0), rhs), s.solve(b, tol=1e-6, max_iters=MAX_ITERS),
+                         s.solve(b, tol=1e-8, precision="fp64", max_iters=MAX_ITERS))
+    finally:
+        s.set("row_sweeps", before)
+    for i in range(3):
+        np.testing.assert_array_equal(out[1][i], out[0][i])
+    for i in (3, 4):
+        (x1, r1), (x0_, r0) = out[1][i], out[0][i]
+        assert r1["iterations"] == r0["iterations"]
+        np.testing.assert_array_equal(x1, x0_)
