@@ -93,9 +93,10 @@ extern "C" int gdtp_system_array(const gdtp_system* s, const char* cname, int le
       if (name.rfind("coef.bd.", 0) == 0) return emit_csr(co[level].bd, part("coef.bd."), out, count);
     }
     if (name == "profile") {  // {timed groups, total ms, deep texels per group, kernels per step graph, kernels launched,
-                              //  1 if the timed group is one fused tile-smoother launch, else 0 (colour sweeps)}
+                              //  smoother of the timed group: 1 one fused tile-smoother launch, 2 a sweep of two
+                              //  row-smoother launches, 0 a sweep of four colour passes}
       double v[6] = {s->sys->profCount, s->sys->profMs, s->sys->profTexels, double(s->sys->graphKernels),
-                     double(s->sys->kernelLaunches), s->sys->profTiled() ? 1.0 : 0.0};
+                     double(s->sys->kernelLaunches), s->sys->profTiled() ? 1.0 : (s->sys->profRows() ? 2.0 : 0.0)};
       if (count) *count = 6;
       if (out) std::memcpy(out, v, sizeof(v));
       return GDTP_OK;
