@@ -716,9 +716,10 @@ __device__ __forceinline__ void block_partials(double (&ra)[4], double (&rb)[4],
 }
 
 // ----------------------------------------------------------------------------
-// FP64 raw operator: res = b - A x (mode 0), y = A x (mode 1) or y = A x with
-// the partial sums of x . y instead of y . y (mode 2) on tight
-// n x K vectors.  Deep rows use 9 raw coefficients per run texel (line runs:
+// FP64 raw operator: res = b - A x (mode 0), y = A x (mode 1), y = A x with
+// the partial sums of x . y instead of y . y (mode 2), or res = b for x = 0
+// (mode 3: the stencil and x are not read; A 0 sums signed zeros to +0, so
+// mode 0 on x = 0 gives these bits) on tight n x K vectors.  Deep rows use 9 raw coefficients per run texel (line runs:
 // up to 32 consecutive deep texels of a raster line), boundary rows
 // the merged BD/BB CSR.  A thread handles one texel and up to 4 channels
 // (group q of G = KP/4 groups, or G = 1 for K = 1).  Per-block sums of res^2
@@ -746,7 +747,9 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
       const long long r = t / (32 * G);
       const int m = int(t - r * 32 * G) / G;
       const ColourRun R = runs[r];
-      if (m < R.len) {  // line runs: consecutive texels
+      if (m < R.len && mode == 3) {
+        g = R.pos0 + m;
+      } else if (m < R.len) {  // line runs: consecutive texels
         const int pos = R.pos0 + m, pp = R.prev0 + m, pn = R.next0 + m;
         const double* c = coef + R.coef0 + m;
         const int nb[9] = {pp - 1, pp, pp + 1, pos - 1, pos, pos + 1, pn - 1, pn, pn + 1};
@@ -762,7 +765,7 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
       }
     } else {
       const long long row = (t - nDeepItems) / G;
-      for (int k = bPtr[row]; k < bPtr[row + 1]; k++) {
+      for (int k = mode == 3 ? bPtr[row + 1] : bPtr[row]; k < bPtr[row + 1]; k++) {
         const double w = bVal[k];
         const double* xs = x + (long long)bCol[k] * K + 4 * q;
 #pragma unroll
@@ -777,7 +780,7 @@ __global__ void __launch_bounds__(256) k_raw_operator(const ColourRun* __restric
         const int c = 4 * q + ch;
         if (c >= K) continue;
         const double bv = b ? b[(long long)g * K + c] : 0.0;
-        const double v = mode == 0 ? bv - acc[ch] : acc[ch];
+        const double v = (mode == 0 || mode == 3) ? bv - acc[ch] : acc[ch];
         if (out32) out32[(long long)g * KP + c] = float(v);
         else out[(long long)g * K + c] = v;
         rr[ch] += mode == 2 ? x[(long long)g * K + c] * v : v * v;  // mode 2: x . A x
@@ -1154,13 +1157,13 @@ void launch_raw_operator(const ColourRun* runs, int nRuns, const double* coef, i
 int raw_operator_blocks(int nRuns, int nB, int K) { return raw_blocks(); }
 void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr,
                              const int* bCol, const double* bVal, const int* bGlobal, int nB, const double* b, const double* x,
-                             float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s) {
+                             float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s, bool xZero) {
   const int G = raw_groups(K);
   const long long items = (long long)nRuns * 32 * G + (long long)nB * G;
   if (items == 0) return;
   const int blocks = int(std::min<long long>(raw_blocks(), nblk(items)));
   launch(k_raw_operator, dim3(blocks), s, runs, nRuns, coef, planeStride, bPtr, bCol, bVal, bGlobal, nB, b, x, (double*)nullptr, K,
-         G, 0, partials, rhs32, KP);
+         G, xZero ? 3 : 0, partials, rhs32, KP);
   if (partials && sums) launch(k_sum_partials, dim3(1), s, partials, blocks, K, sums);
 }
 

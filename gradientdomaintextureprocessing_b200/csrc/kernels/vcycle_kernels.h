@@ -184,10 +184,12 @@ void launch_raw_operator(const ColourRun* runs, int nRuns, const double* coef, i
 // most kRawMaxBlocks): the partial-sum buffers hold this many blocks x 2K.
 constexpr int kRawMaxBlocks = 2048;
 int raw_operator_blocks(int nRuns, int nB, int K);
-// r = b - A x written as the padded FP32 right-hand side (n x KP), plus norms
+// r = b - A x written as the padded FP32 right-hand side (n x KP), plus norms;
+// xZero: x is known to be zero, r = b without reading x or the operator (the
+// same bits and norms)
 void launch_raw_residual_f32(const ColourRun* runs, int nRuns, const double* coef, int planeStride, const int* bPtr,
                              const int* bCol, const double* bVal, const int* bGlobal, int nB, const double* b, const double* x,
-                             float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s);
+                             float* rhs32, int K, int KP, double* partials, double* sums, cudaStream_t s, bool xZero = false);
 template <typename T>
 void launch_pack_rhs(const double* r, T* rhs, long long n, int K, int KP, cudaStream_t s);
 // n doubles (n <= a few hundred) by one block, e.g. into mapped pinned host memory

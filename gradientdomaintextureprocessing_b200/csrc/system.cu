@@ -1691,10 +1691,11 @@ bool DeviceSystem::solve_mixed(const double* b_host, double* x_host, const doubl
       iterGraph = sg.exec;
     }
     // zero correction, initial residual straight into the FP32 right-hand side
+    // (from a zero guess r = b: the operator is skipped, same bits)
     if (!check(cudaMemsetAsync(mg.levels[0].x, 0, n * mg.KP * sizeof(float), s), "zero correction")) return false;
     kernelLaunches += 2;  // operator + norm reduction
     dev::launch_raw_residual_f32(rawA_.runs, rawA_.nRuns, rawA_.coef, rawA_.planeStride, rawA_.bPtr, rawA_.bCol, rawA_.bVal,
-                                 rawA_.bGlobal, rawA_.nB, B, X, mg.levels[0].b, k, mg.KP, partials_, sums_, s);
+                                 rawA_.bGlobal, rawA_.nB, B, X, mg.levels[0].b, k, mg.KP, partials_, sums_, s, zeroGuess);
     if (!read_norms(k, s, "initial residual")) return false;
     rep = SolveReport();
     rep.rel.assign(k, 0.0);

@@ -280,8 +280,11 @@ def test_zero_start_skip_is_exact(setup):
 def test_solve_stream_matches_single_solves(setup):
     """gdtp_solve_stream solves each problem of a sequence as gdtp_solve from a
     zero guess (two device slots alternate, copies on their own streams):
-    bitwise the same solutions and reports.  One right-hand side first, then
-    three (the slots grow), an odd count so that both slots are reused."""
+    bitwise the same solutions and reports.  The stream's zero guess skips the
+    FP64 operator in the initial residual (r = b); gdtp_solve, given x = 0,
+    applies it, so the equality also pins that shortcut.  One right-hand side
+    first, then three (the slots grow), an odd count so that both slots are
+    reused."""
     g, _, s = setup
     b = g["solve/rhs"]
     singles = [b[:, 0]]
