@@ -133,7 +133,7 @@ struct SolverKnobs {
                                         // step's sweeps split between them)
   int tileFinish = 0;                   // 1: one global colour sweep after each tiled smoothing step
   int deviceFactor = 1;                 // dense set-up inverses and products on the device (0: host)
-  int rowSweeps = 1;                    // colour sweeps as two row-smoother launches (0: four colour passes)
+  int rowSweeps = 1;                    // FP32 colour sweeps as two row-smoother launches (0: four colour passes)
 };
 
 struct SolveReport {

@@ -478,9 +478,10 @@ def test_row_smoother_matches_colour_passes(setup, k):
     """A colour sweep as two row-smoother launches (row_sweeps 1: both colours of
     a row parity per launch, lines staged in shared memory) gives the bits of
     the four colour-pass launches: forward and reverse relaxation from random
-    data, a V-cycle (its first sweep from zero skips the same neighbours), the
-    mixed solve and the FP64 multigrid's solve.  k = 1, 3, 8: one channel, the
-    padded 4-lane vectors, two channel groups per texel."""
+    data, a V-cycle (its first sweep from zero skips the same neighbours) and
+    the mixed solve; the FP64 multigrid keeps the colour passes either way, so
+    its solve does not change.  k = 1, 3, 8: one channel, the padded 4-lane
+    vectors, two channel groups per texel."""
     g, h, s = setup
     rng = np.random.default_rng(11)
     n = h.counts(0)["numTexels"]
