@@ -97,46 +97,65 @@ __global__ void __launch_bounds__(256) k_gemm(const GemmTask* __restrict__ tasks
 }
 
 // P_q = A_q[K,K]^-1 for every matrix q with m_q > 64k (one CTA each):
-// unblocked Gauss-Jordan on the pivot block in shared memory.
+// unblocked Gauss-Jordan on the pivot block, held in registers.
 __global__ void __launch_bounds__(256) k_bgj_diag(int k, const long long* __restrict__ off, const int* __restrict__ size,
                                                   const double* __restrict__ A, double* __restrict__ Pinv, int* __restrict__ bad) {
   const int q = blockIdx.x, m = size[q], kb = k * kPB;
   if (kb >= m) return;
   const int bs = min(kPB, m - kb);
-  __shared__ double P[kPB][kPB + 1];
-  __shared__ double rowS[kPB], colS[kPB];
+  // thread (tr, tc) holds entries (tr + 16 a, tc + 16 b), a, b < 4, in
+  // registers; the pivot row and column of each step go through shared
+  // memory, double-buffered so that one barrier per step orders them
+  const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
+  __shared__ double rowS[2][kPB], colS[2][kPB];
   const double* Aq = A + off[q];
-  for (int e = threadIdx.x; e < kPB * kPB; e += 256) {
-    const int i = e / kPB, j = e % kPB;
-    P[i][j] = (i < bs && j < bs) ? Aq[(long long)(kb + i) * m + kb + j] : 0.0;
-  }
-  for (int s = 0; s < bs; s++) {
-    __syncthreads();
-    if (threadIdx.x < kPB) {
-      rowS[threadIdx.x] = P[s][threadIdx.x];
-      colS[threadIdx.x] = P[threadIdx.x][s];
+  double P[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int i = tr + 16 * a, j = tc + 16 * b;
+      P[a][b] = (i < bs && j < bs) ? Aq[(long long)(kb + i) * m + kb + j] : 0.0;
     }
+  for (int s = 0; s < bs; s++) {
+    const int buf = s & 1;
+    // the pivot row s and column s as they stand before step s
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+      if (tr + 16 * a == s)
+#pragma unroll
+        for (int b = 0; b < 4; b++) rowS[buf][tc + 16 * b] = P[a][b];
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+      if (tc + 16 * b == s)
+#pragma unroll
+        for (int a = 0; a < 4; a++) colS[buf][tr + 16 * a] = P[a][b];
     __syncthreads();
-    double p = rowS[s];
+    double p = rowS[buf][s];
     if (!(p > 0.0)) {
       if (threadIdx.x == 0) atomicExch(bad, 1);
       p = 1.0;
     }
     const double ip = 1.0 / p;
-    for (int e = threadIdx.x; e < bs * kPB; e += 256) {
-      const int i = e / kPB, j = e % kPB;
-      if (j >= bs) continue;
-      double v;
-      if (i == s && j == s) v = ip;
-      else if (i == s) v = rowS[j] * ip;
-      else if (j == s) v = -colS[i] * ip;
-      else v = P[i][j] - colS[i] * (rowS[j] * ip);
-      P[i][j] = v;
-    }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const int i = tr + 16 * a, j = tc + 16 * b;
+        if (i >= bs || j >= bs) continue;
+        double v;
+        if (i == s && j == s) v = ip;
+        else if (i == s) v = rowS[buf][j] * ip;
+        else if (j == s) v = -colS[buf][i] * ip;
+        else v = P[a][b] - colS[buf][i] * (rowS[buf][j] * ip);
+        P[a][b] = v;
+      }
   }
-  __syncthreads();
   double* Pq = Pinv + (long long)q * kPB * kPB;
-  for (int e = threadIdx.x; e < kPB * kPB; e += 256) Pq[e] = P[e / kPB][e % kPB];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) Pq[(tr + 16 * a) * kPB + tc + 16 * b] = P[a][b];
 }
 
 // blockIdx.y == 0: row tile t of R = P [A[K,:], A[K,K] -> I], written to R

@@ -504,3 +504,30 @@ def test_row_smoother_matches_colour_passes(setup, k):
         (x1, r1), (x0_, r0) = out[1][i], out[0][i]
         assert r1["iterations"] == r0["iterations"]
         np.testing.assert_array_equal(x1, x0_)
+
+
+@pytest.mark.parametrize("width,block,k", [(2048, 512, 3), (4096, 1024, 1)])
+def test_row_smoother_long_lines(built_lib, width, block, k):
+    """Raster lines longer than 512 texels run in row-smoother blocks of 512 or
+    1024 threads (one-chart-per-quadrant torus: level-0 lines of about 1000 and
+    2000 texels).  Relaxation sweeps both ways and a V-cycle give the bits of
+    the four colour passes."""
+    from gradientdomaintextureprocessing_b200 import meshgen
+    from gradientdomaintextureprocessing_b200.hierarchy import InitializeHierarchy
+    from gradientdomaintextureprocessing_b200.system import System
+    h = InitializeHierarchy(meshgen.torus_atlas(width, width), levels=4)
+    lines = h.array("rasterLines").reshape(-1, 5)
+    longest = int((lines[:, 1] - lines[:, 0] + 1).max())
+    assert block // 2 < (longest + 1) // 2 <= block  # the block size this level needs
+    s = System(h)
+    s.update(1e-3, 1.0)
+    rng = np.random.default_rng(5)
+    n = h.counts(0)["numTexels"]
+    x0 = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    rhs = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    out = {}
+    for rows in (0, 1):
+        s.set("row_sweeps", rows)
+        out[rows] = (s.relax(x0, rhs, sweeps=2), s.relax(x0, rhs, sweeps=2, reverse=True), s.vcycle(np.zeros_like(x0), rhs))
+    for a, c in zip(out[1], out[0]):
+        np.testing.assert_array_equal(a, c)
