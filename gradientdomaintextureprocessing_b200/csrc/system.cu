@@ -1231,10 +1231,12 @@ static int zero_start_skip(int c) {
 
 template <typename T, int W>
 void DeviceSystem::colour_sweep(const LevelDev<T>& D, int KP, bool reverse, bool fromZero, bool rhsEarly, cudaStream_t s) {
-  // FP32 multigrids only: with FP64 vectors (32 bytes per texel) the row
-  // smoother's blocks need twice the shared memory and more registers, and
-  // its sweeps are slower than the colour passes
-  if (knobs.rowSweeps && sizeof(T) == 4 && D.rowBlock > 0 && dev::gs_rows_available<T, W>(D)) {
+  // FP32 multigrids with one channel group only (k <= 4): with FP64 vectors
+  // the row smoother's blocks need twice the shared memory and more registers,
+  // and with several channel groups every group's block loads the
+  // coefficients again (a colour pass shares them across a warp); both were
+  // measured slower than the colour passes
+  if (row_sweeps_on(D, KP, sizeof(T), W)) {
     // a colour's zero-start skips cover its rows above and below, or its own
     // row, whole: the row smoother skips them as groups
     constexpr int kRows = 1 | 2 | 4 | 64 | 128 | 256, kOwn = 8 | 32;
@@ -1401,7 +1403,7 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
         cudaEventRecordWithFlags(profEv_[3], s, cudaEventRecordExternal);
         profPostSweeps_ = post_sweeps(l);
         profTiled_ = false;
-        profRows_ = knobs.rowSweeps && sizeof(T) == 4 && D.rowBlock > 0 && dev::gs_rows_available<T, W>(D);
+        profRows_ = row_sweeps_on(D, KP, sizeof(T), W);
       }
     }
     trace_mark(L + 1 + (L - 2 - l), s);

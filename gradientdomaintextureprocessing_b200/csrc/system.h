@@ -133,7 +133,8 @@ struct SolverKnobs {
                                         // step's sweeps split between them)
   int tileFinish = 0;                   // 1: one global colour sweep after each tiled smoothing step
   int deviceFactor = 1;                 // dense set-up inverses and products on the device (0: host)
-  int rowSweeps = 1;                    // FP32 colour sweeps as two row-smoother launches (0: four colour passes)
+  int rowSweeps = 1;                    // FP32 colour sweeps of k <= 4 channels as two row-smoother launches
+                                        // (0: four colour passes)
 };
 
 struct SolveReport {
@@ -206,6 +207,12 @@ class DeviceSystem {
   // the sweep does not write the right-hand side.
   template <typename T, int W>
   void colour_sweep(const dev::LevelDev<T>& D, int KP, bool reverse, bool fromZero, bool rhsEarly, cudaStream_t s);
+  // the row smoother runs this level's sweeps: FP32 vectors of one channel group
+  template <typename T>
+  bool row_sweeps_on(const dev::LevelDev<T>& D, int KP, size_t valueBytes, int W) const {
+    if (!knobs.rowSweeps || valueBytes != 4 || KP != W || D.rowBlock == 0) return false;
+    return W == 4 ? dev::gs_rows_available<T, 4>(D) : dev::gs_rows_available<T, 1>(D);
+  }
   template <typename T>
   bool grouped(const dev::LevelDev<T>& D, int KP) const {
     return knobs.chartTexels > 0 && D.nGroups > 0 && D.maxGroupDeep <= knobs.chartTexels &&

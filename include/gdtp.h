@@ -267,9 +267,10 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * levels, default 2/2), "tile_rounds"
  * (passes over the tiles per smoothing step, the sweeps split between them,
  * default 1), "row_sweeps" (0/1, default 1: each 4-colour sweep of an FP32
- * multigrid level whose raster lines fit a block runs as two launches, both
- * colours of a row parity per launch, the same updates bit for bit; FP64
- * multigrids keep the colour passes), "tile_finish" (0/1: one
+ * multigrid level of up to 4 channels whose raster lines fit a block runs as
+ * two launches, both colours of a row parity per launch, the same updates bit
+ * for bit; FP64 multigrids and wider batches keep the colour passes),
+ * "tile_finish" (0/1: one
  * global colour sweep closes each tiled
  * smoothing step), "device_factor" (0/1, default 1: the dense FP64 inverses
  * and products of the set-up -- boundary subdomain blocks, separator Schur

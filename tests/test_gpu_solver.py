@@ -480,8 +480,8 @@ def test_row_smoother_matches_colour_passes(setup, k):
     the four colour-pass launches: forward and reverse relaxation from random
     data, a V-cycle (its first sweep from zero skips the same neighbours) and
     the mixed solve; the FP64 multigrid keeps the colour passes either way, so
-    its solve does not change.  k = 1, 3, 8: one channel, the padded 4-lane
-    vectors, two channel groups per texel."""
+    its solve does not change.  k = 1, 3: one channel and the padded 4-lane
+    vectors; k = 8 (two channel groups per texel) keeps the colour passes."""
     g, h, s = setup
     rng = np.random.default_rng(11)
     n = h.counts(0)["numTexels"]
