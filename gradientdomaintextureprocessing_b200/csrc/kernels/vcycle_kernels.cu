@@ -9,6 +9,7 @@
 //   boundary residual IterativeSolvers.inl:549-555  r_B = rhs_B - BD x - BB x_B
 //   raw operator     IterativeSolvers.inl:881-950   y = A x (MultiplyBySystemMatrix_NoReciprocals)
 #include <algorithm>
+#include <type_traits>
 
 #include "vcycle.cuh"
 #include "vcycle_kernels.h"
@@ -281,6 +282,87 @@ __global__ void __launch_bounds__(kGroupBlockMax, 1) k_gs_groups(const ColourRun
       for (int k = 0; k < KP; k++) x[(long long)pos * KP + k] = xs[(pos - lo) * KP + k];
     }
   }
+}
+
+// The chart smoother for FP32 vectors of one channel group whose colour passes
+// fit kGroupRegBlock threads: thread t owns item t of every colour (run t / 32,
+// texel t % 32) and loads its run, coefficients and (rhsEarly) right-hand side
+// for all four colours before the dependency wait, with independent loads;
+// the passes then read x from shared memory only.  REV: colours 3..0.  Same
+// updates, same order, same bits as k_gs_groups.
+constexpr int kGroupRegBlock = 512;
+template <int W, bool REV>
+__global__ void __launch_bounds__(kGroupRegBlock, 1) k_gs_groups_reg(const ColourRun* __restrict__ runs,
+                                                                   const int* __restrict__ groups, const float* __restrict__ coef,
+                                                                   int planeStride, const float* __restrict__ rhs,
+                                                                   float* __restrict__ x, int sweeps, int rhsEarly) {
+  constexpr int KP = W;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* xs = reinterpret_cast<float*>(smem_raw);
+  const int* g = groups + 10 * blockIdx.x;
+  const int lo = g[8], span = g[9];
+  const int t = threadIdx.x, m = t & 31;
+  bool act[4];
+  int pos[4], pp[4], pn[4];
+  float w[4][9];
+  Vec<float, W> bv[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    act[c] = false;
+    pos[c] = pp[c] = pn[c] = 0;
+    if (t < g[4 + c] * 32) {
+      const ColourRun R = runs[g[c] + (t >> 5)];
+      if (m < R.len) {
+        act[c] = true;
+        pos[c] = R.pos0 + 2 * m - lo;
+        pp[c] = R.prev0 + 2 * m - lo;
+        pn[c] = R.next0 + 2 * m - lo;
+        const float* cf = coef + R.coef0 + m;
+#pragma unroll
+        for (int k = 0; k < 9; k++) w[c][k] = cf[k * planeStride];
+        if (rhsEarly) bv[c] = vload<float, W>(rhs + (long long)(pos[c] + lo) * KP);
+      }
+    }
+  }
+  grid_dependency_wait();
+  grid_launch_dependents();
+  for (int i = t; i < span * KP; i += blockDim.x) xs[i] = x[(long long)lo * KP + i];
+  if (!rhsEarly)
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+      if (act[c]) bv[c] = vload<float, W>(rhs + (long long)(pos[c] + lo) * KP);
+  __syncthreads();
+  // the pass loop stays rolled (the per-colour arrays then live in local
+  // memory, L1-resident): unrolled, the compiled passes did not reproduce the
+  // launch path's bits
+  for (int sw = 0; sw < sweeps; sw++) {
+#pragma unroll 1
+    for (int cc = 0; cc < 4; cc++) {
+      const int c = REV ? 3 - cc : cc;
+      if (act[c]) {
+        Vec<float, W> acc;
+#pragma unroll
+        for (int k = 0; k < W; k++) acc.v[k] = 0;
+        axpy(acc, w[c][0], vload<float, W>(xs + (pp[c] - 1) * KP));
+        axpy(acc, w[c][1], vload<float, W>(xs + (pp[c]) * KP));
+        axpy(acc, w[c][2], vload<float, W>(xs + (pp[c] + 1) * KP));
+        axpy(acc, w[c][3], vload<float, W>(xs + (pos[c] - 1) * KP));
+        axpy(acc, w[c][5], vload<float, W>(xs + (pos[c] + 1) * KP));
+        axpy(acc, w[c][6], vload<float, W>(xs + (pn[c] - 1) * KP));
+        axpy(acc, w[c][7], vload<float, W>(xs + (pn[c]) * KP));
+        axpy(acc, w[c][8], vload<float, W>(xs + (pn[c] + 1) * KP));
+        Vec<float, W> out;
+#pragma unroll
+        for (int k = 0; k < W; k++) out.v[k] = bv[c].v[k] * w[c][4] - acc.v[k];
+        vstore<float, W>(xs + pos[c] * KP, out);
+      }
+      __syncthreads();
+    }
+  }
+  // write back this thread's deep texels (boundary texels of the span stay)
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+    if (act[c]) vstore<float, W>(x + (long long)(pos[c] + lo) * KP, vload<float, W>(xs + pos[c] * KP));
 }
 
 // ----------------------------------------------------------------------------
@@ -1049,10 +1131,41 @@ size_t gs_groups_smem(const LevelDev<T>& D, int KP) {
   return size_t(D.maxGroupSpan) * KP * sizeof(T);
 }
 template <typename T, int W>
-bool launch_gs_groups(const LevelDev<T>& D, int sweeps, bool reverse, int KP, cudaStream_t s) {
+bool launch_gs_groups(const LevelDev<T>& D, int sweeps, bool reverse, int KP, cudaStream_t s, bool rhsEarly) {
   if (D.nGroups == 0 || sweeps <= 0) return true;
   const size_t smem = gs_groups_smem<T, W>(D, KP);
   if (smem > kGroupSmemMax) return false;
+  if constexpr (std::is_same<T, float>::value) {
+    // one channel group, every colour pass of a chart within one block: the
+    // register-staged variant
+    if (KP == W && D.maxGroupColourRuns > 0 && D.maxGroupColourRuns * 32 <= kGroupRegBlock) {
+      auto kern = reverse ? k_gs_groups_reg<W, true> : k_gs_groups_reg<W, false>;
+      static std::atomic<int> regAttr[2][kMaxDevices];
+      static const bool regInit = [] {
+        for (auto& r : regAttr)
+          for (auto& a : r) a.store(kUnset);
+        return true;
+      }();
+      (void)regInit;
+      const int okReg = per_device_once(regAttr[reverse ? 1 : 0], [kern] {
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGroupSmemMax)) == cudaSuccess ? 1 : 0;
+      });
+      if (okReg) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(D.nGroups);
+        cfg.blockDim = dim3(std::max(128, D.maxGroupColourRuns * 32));
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = g_programmatic ? 1 : 0;
+        return cudaLaunchKernelEx(&cfg, kern, D.runs, D.groups, (const float*)D.coef, D.planeStride, (const float*)D.b, D.x, sweeps,
+                                  rhsEarly ? 1 : 0) == cudaSuccess;
+      }
+    }
+  }
   static std::atomic<int> attr[kMaxDevices];
   static const bool init = [] {
     for (auto& a : attr) a.store(kUnset);
@@ -1221,7 +1334,7 @@ void launch_add_correction(double* x, T* e, long long n, int K, int KP, cudaStre
   template bool launch_gs_rows<T, W>(const LevelDev<T>&, int, bool, int, cudaStream_t, int, bool);                       \
   template bool gs_rows_available<T, W>(const LevelDev<T>&);                                                             \
   template size_t gs_rows_smem<T, W>(const LevelDev<T>&);                                                                \
-  template bool launch_gs_groups<T, W>(const LevelDev<T>&, int, bool, int, cudaStream_t);                                \
+  template bool launch_gs_groups<T, W>(const LevelDev<T>&, int, bool, int, cudaStream_t, bool);                          \
   template void launch_residual<T, W>(const ColourRun*, int, const T*, int, const int*, const int*, const T*, const int*, \
                                       int, const T*, const T*, T*, int, cudaStream_t, bool);                             \
   template void launch_restrict<T, W>(const RestrictRun*, int, const int*, const int*, const T*, const int*, int,        \

@@ -76,6 +76,7 @@ struct LevelDev {
   T *x = nullptr, *b = nullptr, *r = nullptr;
   const int* groups = nullptr;  // per chart: first run of each colour [4], run counts [4], texel span [2]
   int nGroups = 0, maxGroupDeep = 0, maxGroupSpan = 0;
+  int maxGroupColourRuns = 0;   // most runs of one colour in one chart
   // fused tile smoother (launch_tile_smooth): tiles ordered by tile colour
   // (tiles of colour c are [tileStart[c], tileStart[c + 1])), segments, FP32
   // coefficient blocks
@@ -126,8 +127,9 @@ size_t gs_rows_smem(const LevelDev<T>& D);
 // the same updates in the same order as launch_gs_colour per colour.  False
 // (nothing launched) when a chart's span does not fit kGroupSmemMax.
 constexpr size_t kGroupSmemMax = 200 * 1024;
+// rhsEarly: the previous launch does not write the level's right-hand side
 template <typename T, int W>
-bool launch_gs_groups(const LevelDev<T>& D, int sweeps, bool reverse, int KP, cudaStream_t s);
+bool launch_gs_groups(const LevelDev<T>& D, int sweeps, bool reverse, int KP, cudaStream_t s, bool rhsEarly = false);
 // Fused smoothing round (tile_smoother.cu): tiles of kTileW x kTileH texels of
 // one chart, a CTA each, `sweeps` 4-colour sweeps in shared memory, x updated
 // in place.  Tiles are ordered by tile colour (tile column parity | tile row

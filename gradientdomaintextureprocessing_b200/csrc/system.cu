@@ -908,6 +908,8 @@ bool DeviceSystem::build_multigrid(Multigrid<T>& mg, int KP) {
         D.nGroups = (int)grp.size() / 10;
         D.maxGroupDeep = maxDeep;
         D.maxGroupSpan = maxSpan;
+        for (int gi = 0; gi < D.nGroups; gi++)
+          for (int c = 0; c < 4; c++) D.maxGroupColourRuns = std::max(D.maxGroupColourRuns, grp[10 * gi + 4 + c]);
       }
     }
     // boundary rows (merged BD + BB, global columns)
@@ -1394,7 +1396,8 @@ void DeviceSystem::vcycle(Multigrid<T>& mg, cudaStream_t s, bool zeroStart) {
       // and written once each per round)
       tile_smooth(mg, D, knobs.tilePostSweeps, true, false, s, profiling_ && l == 0);
     } else if (grouped(D, KP) && post_sweeps(l) > 0) {
-      dev::launch_gs_groups<T, W>(D, post_sweeps(l), true, KP, s);
+      // after the prolongation and the boundary solve, which leave the right-hand side alone
+      dev::launch_gs_groups<T, W>(D, post_sweeps(l), true, KP, s, true);
     } else {
       const bool prof = profiling_ && l == 0 && post_sweeps(l) > 0;
       if (prof) cudaEventRecordWithFlags(profEv_[2], s, cudaEventRecordExternal);
