@@ -120,7 +120,7 @@ struct SolverKnobs {
   int traceLevels = 0;                  // time every level's down / up leg (events in the graph)
   int clusterTexels = 0;                // levels up to this size run in one thread-block cluster (0: off)
   int gridTexels = 0;                   // levels up to this size run in one persistent whole-GPU kernel (0: off)
-  int chartTexels = 2000;               // levels whose largest chart has at most this many deep texels
+  int chartTexels = 1000;               // levels whose largest chart has at most this many deep texels
                                         // smooth all sweeps in one launch, a block per chart (0: off)
   int coarsePreSweeps = 0, coarsePostSweeps = 3;  // sweeps on levels >= coarseFrom (-1: as level 0)
   int coarseFrom = 1;

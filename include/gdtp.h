@@ -250,7 +250,7 @@ int gdtp_residual_static(gdtp_system* s, const double* b_dev, const double* x_de
  * path; takes precedence over "cluster_texels"; 0 = off), "chart_texels"
  * (levels whose largest chart has at most this many deep texels run all sweeps
  * of a smoothing step in one launch, one block per chart with the chart's
- * texels in shared memory; same results; default 2000, 0 = off),
+ * texels in shared memory; same results; default 1000, 0 = off),
  * "trace_levels" (0/1: time every level's legs, arrays "profile.levels" and
  * "profile.cluster"), "krylov" (0/1, default 0: flexible preconditioned
  * conjugate gradients in FP64 around the FP32 V-cycle instead of plain
