@@ -349,10 +349,11 @@ def timed_config(args):
     torch.cuda.set_device(0)
     t0 = time.time()
     if args.config == "geodesics":
-        from gradientdomaintextureprocessing_b200.geodesics import Geodesics
+        from gradientdomaintextureprocessing_b200.geodesics import DEFAULT_SMOOTHING, Geodesics, mean_texel_area
         mesh = meshgen.icosphere_atlas(1024, 1024, subdiv=6, seed=0)
         h = InitializeHierarchy(mesh, levels=4)
-        G = Geodesics(h)
+        t_heat = mean_texel_area(h) if args.geodesic_smoothing == "area" else DEFAULT_SMOOTHING
+        G = Geodesics(h, smoothing=t_heat)
         srcs = np.random.default_rng(0).choice(h.array("deepGlobal"), size=64, replace=False)
         setup_s = time.time() - t0
         for _ in range(args.warmup):
@@ -372,7 +373,8 @@ def timed_config(args):
                "value": n * 64 / t / 1e6, "unit": "Mtexels/s (texels x RHS)", "ms_per_step": t * 1e3,
                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32 V-cycle + f64 refinement",
                "data": "synthetic", "api": "gdtp_geodesic_distance (host sources in, host distances out, wall clock)",
-               "config": {"workload": "icosphere6 1024x1024, 16 charts, 64 sources, t = 1e-3, eps = 1e-6", "texels": n,
+               "config": {"workload": f"icosphere6 1024x1024, 16 charts, 64 sources, t = {t_heat:.4g}"
+                                      f"{' (mean texel area)' if args.geodesic_smoothing == 'area' else ''}, eps = 1e-6", "texels": n,
                           "rhs": 64, "setup_s": round(setup_s, 1)},
                "rel_residual_max": float(max(r["rel_residual_max"] for r in reps)),
                "iterations": int(reps[-1]["iterations"]), "clocks": clocks.summary()}
@@ -460,6 +462,8 @@ def main():
                     help="solver knob for --profile-solves / --trace-levels runs (e.g. tile_texels=1000000)")
     ap.add_argument("--config", choices=["filtering", "geodesics", "lic"], default="filtering",
                     help="geodesics / lic: extra measurement lines for those workloads (1 GPU)")
+    ap.add_argument("--geodesic-smoothing", choices=["default", "area"], default="default",
+                    help="geodesics: heat-step time t, the app's default 1e-3 or the mean texel area")
     args = ap.parse_args()
     if args.serve:
         return serve(args)

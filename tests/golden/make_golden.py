@@ -38,19 +38,32 @@ FIELDS = {"genus2lic512": lambda mesh: meshgen.gaussian_bump_field(mesh, bumps=8
 # heat-method geodesics (the Geodesics app's pipeline): mesh, levels, smoothing weight t, source texel
 GEODESIC = {"geo256": (lambda: meshgen.icosphere_atlas(256, 256, subdiv=5), 4, 1e-3, 12345),
             # the heat-method configuration at full size: only the source and the distances are kept (FP32)
-            "geo1024": (lambda: meshgen.icosphere_atlas(1024, 1024, subdiv=6, seed=0), 4, 1e-3, 100000)}
+            "geo1024": (lambda: meshgen.icosphere_atlas(1024, 1024, subdiv=6, seed=0), 4, 1e-3, 100000),
+            # the benchmark's smoothing time, the mean texel area (None: 1 / texels of the area-normalised mesh);
+            # the mesh is regenerated from its generator by the test, the reference's u, rhs and distances kept
+            "geo256area": (lambda: meshgen.icosphere_atlas(256, 256, subdiv=5), 4, None, 12345)}
 
 
 def make_geodesic(name: str) -> None:
     factory, levels, t, src = GEODESIC[name]
     mesh = factory()
+    if t is None:
+        from gradientdomaintextureprocessing_b200.geodesics import mean_texel_area
+        from gradientdomaintextureprocessing_b200.hierarchy import InitializeHierarchy
+        t = mean_texel_area(InitializeHierarchy(mesh, levels=levels))
     exe = os.path.join(ROOT, "oracle", "_ref", "gdtp_ref")
     with tempfile.TemporaryDirectory() as tmp:
         gdm, out = os.path.join(tmp, "m.gdm"), os.path.join(tmp, "o.gdd")
         meshgen.write_gdm(gdm, mesh)
-        subprocess.run([exe, gdm, out, str(levels), str(t), "0", "1", "geodesic", "1e-6", "", str(src)], check=True,
+        subprocess.run([exe, gdm, out, str(levels), repr(t), "0", "1", "geodesic", "1e-6", "", str(src)], check=True,
                        capture_output=True)
         d = read_dump(out)
+    if name == "geo256area":
+        keep = {"meta/size": d["meta/size"], "L0/counts": d["L0/counts"], "geo/source": d["geo/source"],
+                "geo/weights": d["geo/weights"], "geo/u": d["geo/u"], "geo/rhs": d["geo/rhs"], "geo/dist": d["geo/dist"]}
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k.replace("/", "__"): v for k, v in keep.items()})
+        print(name, sum(v.nbytes for v in keep.values()) / 1e6, "MB raw")
+        return
     if name == "geo1024":  # the mesh is regenerated from its seed by the test
         keep = {"meta/size": d["meta/size"], "L0/counts": d["L0/counts"], "geo/source": d["geo/source"],
                 "geo/weights": d["geo/weights"], "geo/dist": d["geo/dist"].astype(np.float32)}
