@@ -892,11 +892,37 @@ __global__ void k_set_flags(int* __restrict__ flags, unsigned long long mask, in
   if (c < k) flags[c] = int((mask >> c) & 1ull);
 }
 
-// Sum of per-block partials in a fixed order (one block): sums[2K]
+// Sum of per-block partials in a fixed order (one block): sums[2K]; up to
+// kSumWide sums (K <= 4: the solve's right-hand sides) reduced side by side
+constexpr int kSumWide = 8;
 __global__ void k_sum_partials(const double* __restrict__ partials, int nBlocks, int K, double* __restrict__ sums) {
   grid_dependency_wait();
   grid_launch_dependents();
   __shared__ double sh[256];
+  if (2 * K <= kSumWide) {
+    // every sum at once (one tree for all of them): per sum the same thread
+    // partials, in the same order, and the same tree as the loop below
+    __shared__ double shw[kSumWide][256];
+    double s[kSumWide];
+#pragma unroll
+    for (int c = 0; c < kSumWide; c++) s[c] = 0;
+    for (int b = threadIdx.x; b < nBlocks; b += blockDim.x)
+#pragma unroll
+      for (int c = 0; c < kSumWide; c++)
+        if (c < 2 * K) s[c] += partials[(long long)b * 2 * K + c];
+#pragma unroll
+    for (int c = 0; c < kSumWide; c++) shw[c][threadIdx.x] = s[c];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if ((int)threadIdx.x < w)
+#pragma unroll
+        for (int c = 0; c < kSumWide; c++)
+          if (c < 2 * K) shw[c][threadIdx.x] += shw[c][threadIdx.x + w];
+      __syncthreads();
+    }
+    if ((int)threadIdx.x < 2 * K) sums[threadIdx.x] = shw[threadIdx.x][0];
+    return;
+  }
   for (int c = 0; c < 2 * K; c++) {
     double s = 0;
     for (int b = threadIdx.x; b < nBlocks; b += blockDim.x) s += partials[(long long)b * 2 * K + c];
